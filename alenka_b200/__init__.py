@@ -1,0 +1,153 @@
+"""alenka_b200: a B200 (sm_100a) engine for Alenka's columnar scan -> filter -> join ->
+group-by -> order path, behind the reference's own embedding API (alenkaInit /
+alenkaExecute / alenkaClose) and operator entry points.
+
+This module is a thin ctypes binding of the in-tree ``libalenka_b200.so``; there is no
+Python or CPU execution path. Importing it on a machine without the built library raises.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libalenka_b200.so")
+
+ALK_OK = 0
+ALK_ERR_OVERFLOW = 3
+ALK_ERR_UNSUPPORTED = 5
+ALK_SESSION_RESIDENT = 1
+ALK_SESSION_PLAIN = 2
+
+_lib = None
+
+
+class AlenkaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"status {code}: {msg}")
+        self.code = code
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("rows_scanned", ctypes.c_uint64),
+        ("kernels", ctypes.c_uint64),
+        ("h2d_bytes", ctypes.c_uint64),
+        ("d2h_bytes", ctypes.c_uint64),
+        ("plan", ctypes.c_uint32),
+        ("segments_skipped", ctypes.c_uint32),
+        ("hot_kernel_ms", ctypes.c_double),
+        ("hot_kernel_bytes", ctypes.c_uint64),
+        ("hot_kernel_launches", ctypes.c_uint64),
+    ]
+
+
+def _declare(L):
+    c = ctypes
+    vp, u32, u64, i64, i32 = c.c_void_p, c.c_uint32, c.c_uint64, c.c_int64, c.c_int
+    L.alk_session_open.argtypes = [c.c_char_p, u32, c.POINTER(vp)]
+    L.alk_session_execute.argtypes = [vp, c.c_char_p]
+    L.alk_session_error.argtypes = [vp]
+    L.alk_session_error.restype = c.c_char_p
+    L.alk_session_stream.argtypes = [vp]
+    L.alk_session_stream.restype = vp
+    L.alk_session_preload.argtypes = [vp, c.c_char_p]
+    L.alk_session_stats.argtypes = [vp, c.POINTER(Stats)]
+    L.alk_session_set_timing.argtypes = [vp, i32]
+    L.alk_session_close.argtypes = [vp]
+    L.alk_session_close.restype = None
+    L.alk_gen_lineitem_flat.argtypes = [c.c_char_p, u64, u32, u64, i32, c.c_char_p, i32]
+    L.alk_gen_three_way.argtypes = [c.c_char_p, u64, u64, u64, u32, u64, i32, c.c_char_p, i32]
+    L.alk_date_add_days.argtypes = [i64, i64]
+    L.alk_date_add_days.restype = i64
+    L.alk_decode_segment.argtypes = [vp, u32, u32, u32, i64, i64, u32, vp, vp]
+    L.alk_hash_tuples.argtypes = [c.POINTER(vp), u32, u64, u32, vp, vp]
+    L.alk_groupby_hash.argtypes = [c.POINTER(vp), u32, c.POINTER(vp), c.POINTER(c.c_uint8), u32, u64,
+                                   c.POINTER(vp), c.POINTER(vp), vp, c.POINTER(u64), vp]
+    L.alk_sort_perm.argtypes = [c.POINTER(vp), c.POINTER(c.c_uint8), u32, u64, vp, vp]
+    L.alk_sort_perm_u64.argtypes = [vp, u64, vp, vp]
+    L.alk_gather.argtypes = [vp, vp, u64, vp, vp]
+    L.alk_join_build.argtypes = [vp, u64, c.POINTER(vp), vp]
+    L.alk_join_probe.argtypes = [vp, vp, u64, vp, vp, u64, c.POINTER(u64), vp]
+    L.alk_join_free.argtypes = [vp, vp]
+    L.alk_join_free.restype = None
+    L.alk_device_info.argtypes = [c.POINTER(i32), c.POINTER(i32), c.POINTER(i32)]
+    L.alenkaInit.argtypes = [c.POINTER(c.c_char_p)]
+    L.alenkaInit.restype = None
+    L.alenkaExecute.argtypes = [c.c_char_p]
+    L.alenkaClose.argtypes = []
+    L.alenkaClose.restype = None
+
+
+def lib():
+    """The loaded engine library (raises when it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing; build it with python -m alenka_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+class Session:
+    """An engine session over a data directory (data.dictionary + segment files)."""
+
+    def __init__(self, data_dir, resident=True, plain=False):
+        flags = (ALK_SESSION_RESIDENT if resident else 0) | (ALK_SESSION_PLAIN if plain else 0)
+        h = ctypes.c_void_p()
+        rc = lib().alk_session_open(str(data_dir).encode(), flags, ctypes.byref(h))
+        if rc != ALK_OK:
+            raise AlenkaError(rc, "cannot open a session")
+        self._h = h
+
+    def execute(self, script):
+        rc = lib().alk_session_execute(self._h, script.encode())
+        if rc != ALK_OK:
+            raise AlenkaError(rc, lib().alk_session_error(self._h).decode())
+
+    def preload(self, table):
+        rc = lib().alk_session_preload(self._h, table.encode())
+        if rc != ALK_OK:
+            raise AlenkaError(rc, lib().alk_session_error(self._h).decode())
+
+    def stats(self):
+        s = Stats()
+        lib().alk_session_stats(self._h, ctypes.byref(s))
+        return s
+
+    def set_timing(self, on):
+        lib().alk_session_set_timing(self._h, 1 if on else 0)
+
+    @property
+    def stream(self):
+        return lib().alk_session_stream(self._h)
+
+    def close(self):
+        if self._h:
+            lib().alk_session_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def gen_lineitem_flat(data_dir, rows, seg_rows, seed, delta=False):
+    err = ctypes.create_string_buffer(512)
+    rc = lib().alk_gen_lineitem_flat(str(data_dir).encode(), rows, seg_rows, seed, int(delta), err, 512)
+    if rc:
+        raise AlenkaError(rc, err.value.decode())
+
+
+def gen_three_way(data_dir, customers, orders, lineitems, seg_rows, seed, delta=False):
+    err = ctypes.create_string_buffer(512)
+    rc = lib().alk_gen_three_way(str(data_dir).encode(), customers, orders, lineitems, seg_rows, seed,
+                                 int(delta), err, 512)
+    if rc:
+        raise AlenkaError(rc, err.value.decode())
+
+
+def date_add_days(yyyymmdd, days):
+    return lib().alk_date_add_days(yyyymmdd, days)

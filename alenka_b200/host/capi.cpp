@@ -1,0 +1,146 @@
+// C entry points of the embedding layer: alenkaInit / alenkaExecute / alenkaClose /
+// execute_file (alenka.h:30-35, bison.y:295-515) and the explicit session API.
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+
+#include "engine.h"
+
+struct alk_session {
+  std::unique_ptr<alk::Engine> eng;
+  std::string err;
+};
+
+namespace {
+alk_session* g_session = nullptr;
+bool g_verbose = false;
+
+int open_session(const char* dir, uint32_t flags, alk_session** out) {
+  try {
+    auto* s = new alk_session();
+    s->eng = std::make_unique<alk::Engine>(dir ? dir : ".", flags);
+    *out = s;
+    return ALK_OK;
+  } catch (const alk::EngineError& e) {
+    std::fprintf(stderr, "alenka_b200: %s\n", e.what());
+    return e.code;
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int alk_session_open(const char* data_dir, uint32_t flags, alk_session** out) {
+  if (!out) return ALK_ERR_ARG;
+  *out = nullptr;
+  return open_session(data_dir, flags, out);
+}
+
+int alk_session_execute(alk_session* s, const char* script) {
+  if (!s || !script) return ALK_ERR_ARG;
+  int rc = s->eng->execute(script);
+  s->err = s->eng->error();
+  return rc;
+}
+
+const char* alk_session_error(alk_session* s) { return s ? s->err.c_str() : "no session"; }
+
+alk_stream alk_session_stream(alk_session* s) { return s ? (alk_stream)s->eng->stream() : nullptr; }
+
+int alk_session_preload(alk_session* s, const char* table) {
+  if (!s || !table) return ALK_ERR_ARG;
+  int rc = s->eng->preload(table);
+  s->err = s->eng->error();
+  return rc;
+}
+
+int alk_session_stats(alk_session* s, alk_stats* out) {
+  if (!s || !out) return ALK_ERR_ARG;
+  *out = s->eng->stats();
+  return ALK_OK;
+}
+
+int alk_session_set_timing(alk_session* s, int on) {
+  if (!s) return ALK_ERR_ARG;
+  s->eng->set_timing(on != 0);
+  return ALK_OK;
+}
+
+void alk_session_close(alk_session* s) { delete s; }
+
+// The reference's flags (bison.y:306-331): -l MB (segment size for stores), -v,
+// -delta, -ssd, -precision N, -i. Only -v changes this engine's behaviour; the data
+// directory is the current directory as in the reference.
+void alenkaInit(char** av) {
+  if (av)
+    for (int i = 0; av[i]; i++)
+      if (std::strcmp(av[i], "-v") == 0) g_verbose = true;
+  if (!g_session) open_session(".", ALK_SESSION_RESIDENT, &g_session);
+}
+
+int alenkaExecute(char* s) {
+  if (!g_session) alenkaInit(nullptr);
+  if (!g_session || !s) return 1;
+  int rc = g_session->eng->execute(s);
+  if (rc != ALK_OK) std::fprintf(stderr, "alenka_b200: %s\n", g_session->eng->error().c_str());
+  return rc == ALK_OK ? 0 : 1;
+}
+
+void alenkaClose(void) {
+  delete g_session;
+  g_session = nullptr;
+}
+
+int execute_file(int ac, char** av) {
+  if (ac < 2) return 1;
+  std::ifstream f(av[ac - 1]);
+  if (!f) {
+    std::perror(av[ac - 1]);
+    return 1;
+  }
+  std::stringstream ss;
+  ss << f.rdbuf();
+  std::string script = ss.str();
+  for (int i = 1; i < ac - 1; i++)
+    if (std::strcmp(av[i], "-v") == 0) g_verbose = true;
+  alk_session* s = nullptr;
+  if (open_session(".", 0, &s) != ALK_OK) return 1;
+  int rc = s->eng->execute(script);
+  if (rc != ALK_OK) std::fprintf(stderr, "alenka_b200: %s\n", s->eng->error().c_str());
+  delete s;
+  return rc == ALK_OK ? 0 : 1;
+}
+
+}  // extern "C"
+
+// Text rendering of the parsed statements and their queues (front-end tests).
+extern "C" int alk_parse_dump(const char* script, char* out, int out_len) {
+  std::vector<alk::Statement> sts;
+  std::string err;
+  if (!alk::parse_script(script ? script : "", sts, err)) {
+    if (out && out_len > 0) std::snprintf(out, (size_t)out_len, "ERROR %s", err.c_str());
+    return ALK_ERR_PARSE;
+  }
+  static const char* kinds[] = {"FILTER", "SELECT", "JOIN", "ORDER", "STORE", "STORE_BINARY", "DISPLAY", "LOAD", "OTHER"};
+  std::string s;
+  for (auto& st : sts) {
+    s += kinds[(int)st.kind];
+    s += " s=" + st.s + " f=" + st.f + " grp=" + std::to_string(st.grp_cnt) + " sep=" + st.sep + "\n type:";
+    for (auto& x : st.op_type) s += " " + x;
+    s += "\n value:";
+    for (auto& x : st.op_value) s += " " + x;
+    s += "\n nums:";
+    for (auto x : st.op_nums) s += " " + std::to_string(x);
+    s += "\n prec:";
+    for (auto x : st.op_nums_precision) s += " " + std::to_string(x);
+    s += "\n join:";
+    for (size_t i = 0; i < st.op_join.size(); i++) s += " " + st.op_join[i] + "/" + std::string(1, st.join_type[i]);
+    s += " sel=" + std::to_string(st.sel_count) + " tabs=" + std::to_string(st.join_tab_cnt) + " and:";
+    for (auto& kv : st.join_and_cnt) s += " " + std::to_string(kv.first) + "=" + std::to_string(kv.second);
+    s += "\n";
+  }
+  if (out && out_len > 0) std::snprintf(out, (size_t)out_len, "%s", s.c_str());
+  return (int)s.size() < out_len ? ALK_OK : ALK_ERR_OVERFLOW;
+}

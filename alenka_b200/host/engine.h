@@ -1,0 +1,158 @@
+// Host engine: executes Alenka scripts on the B200 through the operator-level C ABI
+// (include/alenka_b200.h). It mirrors the reference's operator layer
+// (emit_filter / emit_select / emit_join / emit_order / emit_store, operators.cu) and
+// its CudaSet column model (cm.h:681-789): base tables backed by segment files,
+// lazily filtered views, and materialized results.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/alenka_b200.h"
+#include "format.h"
+#include "script.h"
+
+namespace alk {
+
+struct EngineError : std::runtime_error {
+  int code;
+  EngineError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// Device buffer owned by the engine stream (stream-ordered allocation).
+class DevBuf {
+ public:
+  DevBuf() = default;
+  DevBuf(size_t bytes, cudaStream_t s);
+  ~DevBuf();
+  DevBuf(DevBuf&& o) noexcept;
+  DevBuf& operator=(DevBuf&& o) noexcept;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  template <class T>
+  T* as() const { return (T*)p_; }
+  size_t bytes() const { return n_; }
+  void reset();
+
+ private:
+  void* p_ = nullptr;
+  size_t n_ = 0;
+  cudaStream_t s_ = nullptr;
+};
+using DevBufP = std::shared_ptr<DevBuf>;
+
+struct ColMeta {
+  int type = 0;        // 0 int/decimal/date/dictionary code, 2 char (codes on device)
+  uint32_t dz = 0;     // decimal_zeroes
+  uint32_t width = 0;  // char width
+  std::string string_map;  // "<table>.<column>" dictionary the codes refer to
+};
+
+struct SegInfo {
+  SegMeta m;
+  size_t file_off = 0;  // payload offset within the cached file image
+};
+
+// One column of a base table: per segment header metadata (zone maps) and the cached
+// images (pinned host) / device residency.
+struct BaseCol {
+  ColMeta meta;
+  std::vector<SegInfo> segs;
+  std::vector<uint8_t*> host_img;     // pinned host copies of the segment files
+  std::vector<size_t> host_len;
+  std::vector<DevBufP> dev;           // device payload (FOR) or expanded int64 (delta)
+  bool headers_read = false;
+  // char dictionaries
+  std::vector<std::string> dict;
+  std::unordered_map<uint64_t, int64_t> hash_to_code;
+  bool dict_loaded = false;
+};
+
+struct Var {
+  enum Kind { Base, Filtered, Mat } kind = Mat;
+  std::string name;
+  std::vector<std::string> columnNames;
+  std::map<std::string, ColMeta> meta;
+  // Base
+  std::string table, load_file_name;
+  uint32_t segCount = 1, maxRecs = 0;
+  uint64_t total = 0;
+  // Filtered (fil_* queues of CudaSet, cm.h:692-698)
+  std::string source;
+  std::vector<std::string> fil_type, fil_value;
+  std::vector<int64_t> fil_nums;
+  std::vector<uint32_t> fil_prec;
+  // Mat
+  uint64_t n = 0;
+  std::map<std::string, DevBufP> data;
+  std::map<std::string, int> grp_type;
+  bool has(const std::string& c) const;
+};
+
+// Materialized rows of a variable for a set of fields.
+struct Rows {
+  uint64_t n = 0;
+  std::map<std::string, DevBufP> col;
+  std::vector<uint64_t> seg_counts;  // surviving rows per source segment (base/filtered)
+  DevBufP seg_of_row;                // u32 source segment of every row (when requested)
+};
+
+class Engine {
+ public:
+  Engine(std::string dir, uint32_t flags);
+  ~Engine();
+  int execute(const std::string& script);
+  const std::string& error() const { return err_; }
+  cudaStream_t stream() const { return stream_; }
+  int preload(const std::string& table);
+  alk_stats stats() const { return stats_; }
+  void set_timing(bool on) { timing_ = on; }
+
+  // ---- used by the planner / operators ----
+  Var* var(const std::string& n);
+  void ensure_base_col(Var* base, const std::string& col, bool device);
+  Rows materialize(Var* v, const std::vector<std::string>& fields, bool want_seg = false);
+  size_t cycle_count(Var* v);
+  uint64_t free_mem() const { return kFreeMem; }
+  // getFreeMem() (cm.cu:3184) pinned to a B200's 180 GB so that segmentation is deterministic.
+  static constexpr uint64_t kFreeMem = 180ull * 1000 * 1000 * 1000;
+
+ private:
+  std::string dir_, err_;
+  uint32_t flags_;
+  cudaStream_t stream_ = nullptr;
+  DataDict dd_;
+  std::map<std::string, std::unique_ptr<Var>> vars_;
+  std::map<std::string, std::shared_ptr<Var>> bases_;  // catalog tables (persist across scripts)
+  std::map<std::string, std::map<std::string, BaseCol>> basecols_;
+  alk_stats stats_{};
+  bool timing_ = false;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+
+  void reset_script_state();
+  Var* base_table(const std::string& t);
+  BaseCol& basecol(Var* base, const std::string& col);
+  void read_headers(Var* base, const std::string& col, BaseCol& bc);
+  void load_dict(Var* base, const std::string& col, BaseCol& bc);
+  std::vector<char> zone_maps(Var* f, Var* src);
+  alk_program compile_filter(Var* f, Var* src, std::vector<std::string>& slots);
+
+  void exec(Statement& st);
+  void emit_filter(Statement& st);
+  void emit_select(Statement& st);
+  void emit_join(Statement& st);
+  void multijoin(Statement& st, const std::string& s, const std::string& j1, const std::string& j2, unsigned tab);
+  void emit_order(Statement& st);
+  void emit_store(Statement& st);
+  bool try_fused(std::vector<Statement>& sts, size_t& i);
+
+  friend struct Planner;
+};
+
+}  // namespace alk

@@ -1,0 +1,968 @@
+// Operator execution of the host engine: emit_filter / emit_select / emit_join /
+// emit_order / emit_store semantics on top of the operator-level C ABI.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+
+#include "../csrc/internal.h"
+#include "engine.h"
+
+namespace alk {
+
+namespace {
+void check(int rc, const char* what) {
+  if (rc != ALK_OK) throw EngineError(rc, std::string(what) + " failed (status " + std::to_string(rc) + ")");
+}
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess)
+    throw EngineError(e == cudaErrorMemoryAllocation ? ALK_ERR_NOMEM : ALK_ERR_CUDA,
+                      std::string(what) + ": " + cudaGetErrorString(e));
+}
+[[noreturn]] void unsupported(const std::string& m) { throw EngineError(ALK_ERR_UNSUPPORTED, m); }
+int64_t pow10u(uint32_t p) { return (int64_t)(unsigned int)std::pow(10.0, (double)p); }
+int64_t wmul(int64_t a, int64_t b) { return (int64_t)((uint64_t)a * (uint64_t)b); }
+int64_t wadd(int64_t a, int64_t b) { return (int64_t)((uint64_t)a + (uint64_t)b); }
+int64_t wsub(int64_t a, int64_t b) { return (int64_t)((uint64_t)a - (uint64_t)b); }
+int64_t sdiv(int64_t a, int64_t b) { return b == 0 ? 0 : (b == -1 ? (int64_t)(0 - (uint64_t)a) : a / b); }
+int64_t arith(const std::string& op, int64_t a, int64_t b) {
+  if (op == "MUL") return wmul(a, b);
+  if (op == "ADD") return wadd(a, b);
+  if (op == "MINUS") return wsub(a, b);
+  return sdiv(a, b);
+}
+uint32_t precision_func(uint32_t& p1, uint32_t& p2, const std::string& op) {  // zone_map.cu:668-712
+  if (op != "DIV") {
+    if (op != "MUL") {
+      uint32_t res = p1;
+      if (p1 > p2) {
+        p2 = p1 - p2;
+        p1 = 0;
+      } else {
+        p1 = p2 - p1;
+        p2 = 0;
+      }
+      return res;
+    }
+    uint32_t res = p1 + p2;
+    p1 = p2 = 0;
+    return res;
+  }
+  if (p1 == p2) {
+    p1 = p1 + 4;
+    p2 = 0;
+    return p1;
+  }
+  if (p1 > p2) {
+    p1 = p1 + (p1 - p2) + 4;
+    p2 = 0;
+    return p1;
+  }
+  p2 = p2 + (p2 - p1) + 4;
+  p1 = 0;
+  return p2;
+}
+template <class S>
+auto pop(S& s) {
+  if (s.empty()) throw EngineError(ALK_ERR_UNSUPPORTED, "malformed postfix program (stack underflow)");
+  auto x = s.back();
+  s.pop_back();
+  return x;
+}
+DevBufP mkbuf(size_t bytes, cudaStream_t s) { return std::make_shared<DevBuf>(bytes, s); }
+
+// Expression tree built by the symbolic select(): columns, constants, binary
+// arithmetic, and aggregate results (Agg leaves refer to an aggregate slot).
+struct Ast;
+using AstP = std::shared_ptr<Ast>;
+struct Ast {
+  enum K { Col, Const, Bin, Agg } k = Const;
+  std::string col;
+  int64_t v = 0;
+  uint8_t op = 0;
+  AstP l, r;
+  int agg = -1;
+};
+AstP mk_col(const std::string& c) {
+  auto a = std::make_shared<Ast>();
+  a->k = Ast::Col;
+  a->col = c;
+  return a;
+}
+AstP mk_const(int64_t v) {
+  auto a = std::make_shared<Ast>();
+  a->k = Ast::Const;
+  a->v = v;
+  return a;
+}
+AstP mk_bin(uint8_t op, AstP l, AstP r) {
+  auto a = std::make_shared<Ast>();
+  a->k = Ast::Bin;
+  a->op = op;
+  a->l = std::move(l);
+  a->r = std::move(r);
+  return a;
+}
+uint8_t vm_op(const std::string& op) {
+  if (op == "MUL") return ALK_OP_MUL;
+  if (op == "ADD") return ALK_OP_ADD;
+  if (op == "MINUS") return ALK_OP_SUB;
+  return ALK_OP_DIV;
+}
+bool has_agg(const AstP& a) {
+  if (!a) return false;
+  if (a->k == Ast::Agg) return true;
+  return has_agg(a->l) || has_agg(a->r);
+}
+bool has_col(const AstP& a) {
+  if (!a) return false;
+  if (a->k == Ast::Col) return true;
+  return has_col(a->l) || has_col(a->r);
+}
+// CudaSet::op(int_type* column1, int_type d, ...) (cm.cu:2480-2556) as a tree.
+AstP ast_op_const(AstP c, int64_t d, const std::string& op, bool reverse, uint32_t p1, uint32_t p2) {
+  int64_t d1 = (int64_t)(unsigned int)d;
+  if (p2) d = wmul(d, pow10u(p2));
+  if (!reverse) {
+    if (op == "MUL") return mk_bin(ALK_OP_MUL, c, mk_const(d1));
+    if (!p1) return mk_bin(vm_op(op), c, mk_const(wmul(d, pow10u(p2))));
+    return mk_bin(vm_op(op), mk_bin(ALK_OP_MUL, c, mk_const(pow10u(p1))), mk_const(d));
+  }
+  AstP x = p1 ? mk_bin(ALK_OP_MUL, c, mk_const(pow10u(p1))) : c;
+  return mk_bin(vm_op(op), mk_const(d), x);
+}
+// CudaSet::op(int_type* column1, int_type* column2, op, 0, p1, p2) (cm.cu:2559-2600)
+AstP ast_op_vec(AstP c1, AstP c2, const std::string& op, uint32_t p1, uint32_t p2) {
+  if (op == "MUL") return mk_bin(ALK_OP_MUL, c1, c2);
+  AstP x = p1 ? mk_bin(ALK_OP_MUL, c1, mk_const(pow10u(p1))) : c1;
+  AstP y = p2 ? mk_bin(ALK_OP_MUL, c2, mk_const(pow10u(p2))) : c2;
+  return mk_bin(vm_op(op), x, y);
+}
+
+// Compile a tree into a register program; leaves are looked up by leaf(name or agg).
+struct Compiler {
+  alk_program p{};
+  uint32_t nconst = 0, live = 0;
+  std::vector<std::string> slots;  // column slots (names or "#agg<i>")
+  Compiler() { std::memset(&p, 0, sizeof(p)); }
+  uint16_t slot(const std::string& n) {
+    auto it = std::find(slots.begin(), slots.end(), n);
+    if (it != slots.end()) return (uint16_t)(it - slots.begin());
+    slots.push_back(n);
+    if (slots.size() > 16) unsupported("expression reads more than 16 columns");
+    return (uint16_t)(slots.size() - 1);
+  }
+  uint16_t konst(int64_t v) {
+    for (uint32_t i = 0; i < nconst; i++)
+      if (p.consts[i] == v) return (uint16_t)i;
+    if (nconst >= ALK_MAX_CONST) unsupported("expression has too many constants");
+    p.consts[nconst] = v;
+    return (uint16_t)nconst++;
+  }
+  // returns (kind, idx)
+  std::pair<uint8_t, uint16_t> gen(const AstP& a) {
+    switch (a->k) {
+      case Ast::Col: return {ALK_K_COL, slot(a->col)};
+      case Ast::Agg: return {ALK_K_COL, slot("#agg" + std::to_string(a->agg))};
+      case Ast::Const: return {ALK_K_CONST, konst(a->v)};
+      default: break;
+    }
+    auto x = gen(a->l);
+    auto y = gen(a->r);
+    if (x.first == ALK_K_REG) live &= ~(1u << x.second);
+    if (y.first == ALK_K_REG) live &= ~(1u << y.second);
+    uint32_t r = 0;
+    while (r < ALK_MAX_REGS && ((live >> r) & 1)) r++;
+    if (r >= ALK_MAX_REGS) unsupported("expression needs more than 8 registers");
+    live |= 1u << r;
+    if (p.n_instr >= ALK_MAX_INSTR) unsupported("expression too long");
+    alk_instr& in = p.ins[p.n_instr++];
+    in.op = a->op;
+    in.dst = (uint8_t)r;
+    in.ka = x.first;
+    in.a = x.second;
+    in.kb = y.first;
+    in.b = y.second;
+    return {ALK_K_REG, (uint16_t)r};
+  }
+  alk_program finish(const AstP& a) {
+    auto res = gen(a);
+    if (res.first != ALK_K_REG) {
+      alk_instr& in = p.ins[p.n_instr++];
+      in.op = ALK_OP_MOV;
+      in.dst = 0;
+      in.ka = in.kb = res.first;
+      in.a = in.b = res.second;
+      res = {ALK_K_REG, 0};
+    }
+    p.result = res.second;
+    return p;
+  }
+};
+
+struct AggSpec {
+  uint8_t kind = ALK_AGG_SUM;  // SUM for SUM and AVG
+  AstP input;                  // null for COUNT
+};
+struct OutSpec {
+  std::string name;
+  int grp_type = 3;  // 0 COUNT, 1 AVG, 2 SUM, 3 none, 4 MIN, 5 MAX (select.cu:838-860)
+  int col_type = 0;  // 0 number, 1 field, 2 vector
+  int64_t num = 0;
+  std::string field;
+  AstP vec;
+  uint32_t prec = 0;
+};
+
+// Symbolic select() (select.cu:359-952): the same stack discipline, producing output
+// column specifications and the aggregate list.
+void compile_select(Statement& st, Var* a, bool grouped, std::vector<OutSpec>& outs, std::vector<AggSpec>& aggs,
+                    bool& one_line) {
+  std::vector<std::string> et, ev;
+  std::vector<AstP> evec;
+  std::vector<int64_t> en;
+  std::vector<uint32_t> ep;
+  size_t iv = 0, in = 0, ip = 0;  // op_value, op_nums, op_nums_precision positions
+  one_line = false;
+  auto is_col = [&](const std::string& s) { return a->has(s); };
+  auto get_dec = [&](const std::string& s) -> uint32_t { return is_col(s) ? a->meta[s].dz : pop(ep); };
+  auto get_vec = [&](const std::string& s) -> AstP { return is_col(s) ? mk_col(s) : pop(evec); };
+  std::string grp_type = "NULL";
+  for (auto& ss : st.op_type) {
+    if (ss == "emit sel_name") {
+      OutSpec o;
+      o.name = st.op_value[iv++];
+      const std::string& g = grp_type;
+      o.grp_type = g == "COUNT" ? 0 : g == "AVG" ? 1 : g == "SUM" ? 2 : g == "MIN" ? 4 : g == "MAX" ? 5 : 3;
+      int kinds = 0;
+      if (!en.empty()) {
+        o.col_type = 0;
+        o.num = pop(en);
+        o.prec = pop(ep);
+        kinds++;
+      }
+      if (!ev.empty() && ev.back() != "") {
+        o.col_type = 1;
+        o.field = pop(ev);
+        o.prec = a->meta[o.field].dz;
+        kinds++;
+      }
+      if (!evec.empty()) {
+        o.col_type = 2;
+        o.vec = pop(evec);
+        o.prec = pop(ep);
+        pop(ev);
+        kinds++;
+      }
+      if (kinds != 1) unsupported("select item " + o.name + " does not reduce to one value");
+      outs.push_back(o);
+      continue;
+    }
+    grp_type = "NULL";
+    if (ss == "DISTINCT" || ss == "YEAR" || ss == "MONTH" || ss == "DAY" || ss == "CAST" || ss == "CASE")
+      unsupported(ss + " in a select list");
+    if (ss == "COUNT" || ss == "SUM" || ss == "AVG" || ss == "MIN" || ss == "MAX") {
+      if (!grouped) one_line = true;
+      grp_type = ss;
+      pop(et);
+      std::string s1v = pop(ev);
+      AggSpec ag;
+      if (ss == "COUNT") {
+        ag.kind = ALK_AGG_COUNT;
+      } else {
+        ag.kind = ss == "MIN" ? ALK_AGG_MIN : (ss == "MAX" ? ALK_AGG_MAX : ALK_AGG_SUM);
+        if (!is_col(s1v)) {
+          ag.input = pop(evec);
+          if (ss != "SUM") ep.push_back(pop(ep));
+        } else {
+          ag.input = mk_col(s1v);
+          ep.push_back(a->meta[s1v].dz);
+        }
+        if (has_agg(ag.input)) unsupported("nested aggregate");
+      }
+      if (ss == "COUNT") ep.push_back(0);
+      auto leaf = std::make_shared<Ast>();
+      leaf->k = Ast::Agg;
+      leaf->agg = (int)aggs.size();
+      aggs.push_back(ag);
+      evec.push_back(leaf);
+      et.push_back("NAME");
+      ev.push_back("");
+      continue;
+    }
+    if (ss == "NAME" || ss == "NUMBER") {
+      et.push_back(ss);
+      if (ss == "NUMBER") {
+        en.push_back(st.op_nums[in]);
+        ep.push_back(st.op_nums_precision[ip++]);
+        in++;
+      } else {
+        ev.push_back(st.op_value[iv++]);
+      }
+      continue;
+    }
+    if (ss == "MUL" || ss == "ADD" || ss == "DIV" || ss == "MINUS") {
+      std::string s1 = pop(et), s2 = pop(et);
+      if (s1 == "NUMBER" && s2 == "NUMBER") {
+        int64_t n1 = pop(en), n2 = pop(en);
+        uint32_t p1 = pop(ep), p2 = pop(ep);
+        ep.push_back(precision_func(p1, p2, ss));
+        if (p1) n1 = wmul(n1, pow10u(p1));
+        if (p2) n2 = wmul(n2, pow10u(p2));
+        evec.push_back(mk_const(arith(ss, n1, n2)));  // top operand first (select.cu:727-736)
+        et.push_back("NAME");
+        ev.push_back("");
+      } else if (s1 == "NAME" && s2 == "NUMBER") {
+        std::string v = pop(ev);
+        int64_t n1 = pop(en);
+        uint32_t p1 = pop(ep);
+        uint32_t p2 = get_dec(v);
+        AstP t = get_vec(v);
+        ep.push_back(precision_func(p2, p1, ss));
+        et.push_back("NAME");
+        ev.push_back("");
+        evec.push_back(ast_op_const(t, n1, ss, true, p2, p1));
+      } else if (s1 == "NUMBER" && s2 == "NAME") {
+        int64_t n1 = pop(en);
+        std::string v = pop(ev);
+        uint32_t p1 = pop(ep);
+        uint32_t p2 = get_dec(v);
+        AstP t = get_vec(v);
+        ep.push_back(precision_func(p2, p1, ss));
+        et.push_back("NAME");
+        ev.push_back("");
+        evec.push_back(ast_op_const(t, n1, ss, false, p2, p1));
+      } else if (s1 == "NAME" && s2 == "NAME") {
+        std::string v1 = pop(ev), v2 = pop(ev);
+        AstP t1 = get_vec(v1);
+        AstP t = get_vec(v2);
+        uint32_t p1 = get_dec(v1), p2 = get_dec(v2);
+        ep.push_back(precision_func(p1, p2, ss));
+        et.push_back("NAME");
+        ev.push_back("");
+        evec.push_back(ast_op_vec(t, t1, ss, p2, p1));
+      } else {
+        unsupported("arithmetic on " + s1 + "/" + s2 + " in a select list");
+      }
+      continue;
+    }
+    unsupported("token " + ss + " in a select list");
+  }
+}
+
+struct GroupOut {
+  uint64_t g = 0;
+  std::vector<DevBufP> keys, vals;
+  DevBufP first;
+};
+}  // namespace
+
+// ------------------------------------------------------------------ FILTER
+// emit_filter (operators.cu:2306-2408): lazy; a filter of a filter appends an AND.
+void Engine::emit_filter(Statement& st) {
+  Var* a = var(st.f);
+  auto b = std::make_unique<Var>();
+  b->kind = Var::Filtered;
+  b->name = st.s;
+  b->columnNames = a->columnNames;
+  b->meta = a->meta;
+  b->fil_type = st.op_type;
+  b->fil_value = st.op_value;
+  b->fil_nums = st.op_nums;
+  b->fil_prec = st.op_nums_precision;
+  if (a->kind == Var::Filtered) {
+    b->source = a->source;
+    b->fil_value.insert(b->fil_value.end(), a->fil_value.begin(), a->fil_value.end());
+    b->fil_type.insert(b->fil_type.end(), a->fil_type.begin(), a->fil_type.end());
+    b->fil_type.push_back("AND");
+    b->fil_nums.insert(b->fil_nums.end(), a->fil_nums.begin(), a->fil_nums.end());
+    b->fil_prec.insert(b->fil_prec.end(), a->fil_prec.begin(), a->fil_prec.end());
+  } else if (a->kind == Var::Base) {
+    b->source = st.f;
+  } else {
+    unsupported("FILTER over a materialized result");
+  }
+  vars_[st.s] = std::move(b);
+}
+
+// ------------------------------------------------------------------ SELECT
+// emit_select (operators.cu:1801-2084) as one global pass: fused scan, expression
+// evaluation, hash aggregation, then the reference's output order (key order for a
+// single-segment source, MurmurHash64A order of the group keys for a multi-segment
+// source, merge.cu:118-203) and count_avg / count_simple (merge.cu:271-496).
+void Engine::emit_select(Statement& st) {
+  Var* a = var(st.f);
+  const int grp_cnt = st.grp_cnt;
+  std::vector<std::string> group_cols(st.op_value.end() - grp_cnt, st.op_value.end());
+  for (auto& g : group_cols)
+    if (!a->has(g)) unsupported("GROUP BY column " + g + " is not a column of " + st.f);
+  std::vector<OutSpec> outs;
+  std::vector<AggSpec> aggs;
+  bool one_line = false;
+  compile_select(st, a, grp_cnt != 0, outs, aggs, one_line);
+  std::set<std::string> field_set;
+  for (auto& v : st.op_value)
+    if (a->has(v)) field_set.insert(v);
+  std::vector<std::string> fields(field_set.begin(), field_set.end());
+  const size_t cycles = cycle_count(a);
+  Rows R = materialize(a, fields, !grp_cnt && one_line);
+  auto out = std::make_unique<Var>();
+  out->kind = Var::Mat;
+  out->name = st.s;
+  // the reference leaves the select-list order reversed when its first segment is empty
+  bool first_empty = !R.seg_counts.empty() && R.seg_counts[0] == 0;
+  if (R.n == 0) {
+    vars_[st.s] = std::move(out);  // no segment produced rows: empty result without columns
+    return;
+  }
+  if (first_empty) std::reverse(outs.begin(), outs.end());
+  // aggregate inputs (row level)
+  std::vector<DevBufP> agg_in(aggs.size());
+  for (size_t k = 0; k < aggs.size(); k++) {
+    if (aggs[k].kind == ALK_AGG_COUNT) continue;
+    const AstP& in = aggs[k].input;
+    if (in->k == Ast::Col) {
+      agg_in[k] = R.col.at(in->col);
+      continue;
+    }
+    Compiler c;
+    alk_program prog = c.finish(in);
+    std::vector<const int64_t*> cols;
+    for (auto& sname : c.slots) cols.push_back(R.col.at(sname)->as<int64_t>());
+    agg_in[k] = mkbuf(R.n * 8, stream_);
+    check(alk_eval(cols.data(), (uint32_t)cols.size(), R.n, &prog, agg_in[k]->as<int64_t>(), (alk_stream)stream_),
+          "expression");
+  }
+  // group keys: GROUP BY columns, or the source segment for aggregate-only selects
+  std::vector<const int64_t*> keys;
+  DevBufP segkey;
+  if (grp_cnt) {
+    for (auto& g : group_cols) keys.push_back(R.col.at(g)->as<int64_t>());
+  } else if (one_line) {
+    segkey = mkbuf(R.n * 8, stream_);
+    check(alk_widen_u32(R.seg_of_row->as<uint32_t>(), R.n, segkey->as<int64_t>(), (alk_stream)stream_), "widen");
+    keys.push_back(segkey->as<int64_t>());
+  }
+  if (keys.empty()) {
+    // projection: one output row per input row
+    out->n = R.n;
+    for (auto& o : outs) {
+      ColMeta m;
+      m.dz = o.prec;
+      DevBufP col;
+      if (o.col_type == 1) {
+        col = R.col.at(o.field);
+        m.string_map = a->meta[o.field].string_map;
+        m.type = 0;
+      } else if (o.col_type == 2) {
+        if (has_agg(o.vec)) unsupported("aggregate in a projection");
+        Compiler c;
+        alk_program prog = c.finish(o.vec);
+        std::vector<const int64_t*> cols;
+        for (auto& sname : c.slots) cols.push_back(R.col.at(sname)->as<int64_t>());
+        col = mkbuf(R.n * 8, stream_);
+        check(alk_eval(cols.data(), (uint32_t)cols.size(), R.n, &prog, col->as<int64_t>(), (alk_stream)stream_),
+              "projection");
+      } else {
+        std::vector<int64_t> h(R.n, (int64_t)(int)o.num);
+        col = mkbuf(R.n * 8, stream_);
+        ck(cudaMemcpyAsync(col->as<void>(), h.data(), R.n * 8, cudaMemcpyHostToDevice, stream_), "const");
+      }
+      out->columnNames.push_back(o.name);
+      out->meta[o.name] = m;
+      out->data[o.name] = col;
+      out->grp_type[o.name] = o.grp_type;
+    }
+    vars_[st.s] = std::move(out);
+    return;
+  }
+  // hash aggregation
+  std::vector<const int64_t*> vals;
+  std::vector<uint8_t> kinds;
+  for (size_t k = 0; k < aggs.size(); k++) {
+    kinds.push_back(aggs[k].kind);
+    vals.push_back(aggs[k].kind == ALK_AGG_COUNT ? nullptr : agg_in[k]->as<int64_t>());
+  }
+  GroupOut G;
+  std::vector<int64_t*> okeys, ovals;
+  for (size_t j = 0; j < keys.size(); j++) {
+    G.keys.push_back(mkbuf(R.n * 8, stream_));
+    okeys.push_back(G.keys.back()->as<int64_t>());
+  }
+  for (size_t k = 0; k < vals.size(); k++) {
+    G.vals.push_back(mkbuf(R.n * 8, stream_));
+    ovals.push_back(G.vals.back()->as<int64_t>());
+  }
+  G.first = mkbuf(R.n * 4, stream_);
+  check(alk_groupby_hash(keys.data(), (uint32_t)keys.size(), vals.data(), kinds.data(), (uint32_t)vals.size(), R.n,
+                         okeys.data(), ovals.data(), G.first->as<uint32_t>(), &G.g, (alk_stream)stream_),
+        "hash group-by");
+  const uint64_t ng = G.g;
+  // output order
+  auto perm = mkbuf(ng * 4, stream_);
+  if (grp_cnt && cycles > 1) {
+    auto h = mkbuf(ng * 8, stream_);
+    std::vector<const int64_t*> kc(okeys.begin(), okeys.end());
+    check(alk_hash_tuples(kc.data(), (uint32_t)kc.size(), ng, kHashSeed, h->as<uint64_t>(), (alk_stream)stream_),
+          "group hash");
+    check(alk_sort_perm_u64(h->as<uint64_t>(), ng, perm->as<uint32_t>(), (alk_stream)stream_), "hash order");
+  } else {
+    std::vector<const int64_t*> kc(okeys.begin(), okeys.end());
+    std::vector<uint8_t> desc(kc.size(), 0);
+    check(alk_sort_perm(kc.data(), desc.data(), (uint32_t)kc.size(), ng, perm->as<uint32_t>(), (alk_stream)stream_),
+          "key order");
+  }
+  auto gathered = [&](const DevBufP& src) {
+    auto d = mkbuf(ng * 8, stream_);
+    check(alk_gather(src->as<int64_t>(), perm->as<uint32_t>(), ng, d->as<int64_t>(), (alk_stream)stream_), "gather");
+    return d;
+  };
+  std::vector<DevBufP> sk, sv;
+  for (auto& k : G.keys) sk.push_back(gathered(k));
+  for (auto& v : G.vals) sv.push_back(gathered(v));
+  DevBufP sfirst;
+  {
+    // first input row of each group, in output order
+    auto f64 = mkbuf(ng * 8, stream_);
+    check(alk_widen_u32(G.first->as<uint32_t>(), ng, f64->as<int64_t>(), (alk_stream)stream_), "widen");
+    sfirst = gathered(f64);
+  }
+  std::vector<std::string> names;
+  std::vector<DevBufP> cols;
+  std::vector<ColMeta> metas;
+  std::vector<int> gtypes;
+  for (auto& o : outs) {
+    ColMeta m;
+    m.dz = o.prec;
+    DevBufP col;
+    if (o.col_type == 1) {
+      auto it = std::find(group_cols.begin(), group_cols.end(), o.field);
+      if (grp_cnt && it != group_cols.end()) {
+        col = sk[it - group_cols.begin()];
+      } else {
+        if (grp_cnt && cycles > 1) unsupported("non-key column " + o.field + " in a multi-segment GROUP BY");
+        // value at the group's first row (segreduce gathers at grp offsets after a stable sort)
+        auto idx32 = mkbuf(ng * 4, stream_);
+        check(alk_narrow_u32(sfirst->as<int64_t>(), ng, idx32->as<uint32_t>(), (alk_stream)stream_), "narrow");
+        col = mkbuf(ng * 8, stream_);
+        check(alk_gather(R.col.at(o.field)->as<int64_t>(), idx32->as<uint32_t>(), ng, col->as<int64_t>(),
+                         (alk_stream)stream_),
+              "gather");
+      }
+      m.string_map = a->meta[o.field].string_map;
+    } else if (o.col_type == 2) {
+      if (has_col(o.vec)) unsupported("row-level expression in a grouped select");
+      if (o.vec->k == Ast::Agg) {
+        col = sv[o.vec->agg];
+      } else {
+        Compiler c;
+        alk_program prog = c.finish(o.vec);
+        std::vector<const int64_t*> cc;
+        for (auto& sname : c.slots) cc.push_back(sv[std::stoi(sname.substr(4))]->as<int64_t>());
+        col = mkbuf(ng * 8, stream_);
+        check(alk_eval(cc.data(), (uint32_t)cc.size(), ng, &prog, col->as<int64_t>(), (alk_stream)stream_),
+              "aggregate expression");
+      }
+    } else {
+      std::vector<int64_t> h(ng, (int64_t)(int)o.num);
+      col = mkbuf(ng * 8, stream_);
+      ck(cudaMemcpyAsync(col->as<void>(), h.data(), ng * 8, cudaMemcpyHostToDevice, stream_), "const");
+    }
+    names.push_back(o.name);
+    cols.push_back(col);
+    metas.push_back(m);
+    gtypes.push_back(o.grp_type);
+  }
+  if (!grp_cnt) {
+    // count_simple (merge.cu:271-311) over the per-segment rows, ordered by segment
+    std::vector<std::vector<int64_t>> h(cols.size(), std::vector<int64_t>(ng));
+    for (size_t c = 0; c < cols.size(); c++)
+      ck(cudaMemcpyAsync(h[c].data(), cols[c]->as<void>(), ng * 8, cudaMemcpyDeviceToHost, stream_), "d2h");
+    ck(cudaStreamSynchronize(stream_), "sync");
+    stats_.d2h_bytes += ng * 8 * cols.size();
+    int64_t count = 0;
+    bool have = false;
+    std::vector<int64_t> res(cols.size());
+    for (size_t c = 0; c < cols.size(); c++) {
+      res[c] = h[c][0];
+      if (gtypes[c] == 0) {
+        count = 0;
+        for (auto x : h[c]) count = wadd(count, x);
+        res[c] = count;
+        have = true;
+      }
+    }
+    for (size_t c = 0; c < cols.size(); c++) {
+      if (gtypes[c] == 1) {
+        if (!have) unsupported("AVG needs a COUNT column in the same select");
+        int64_t s = 0;
+        for (auto x : h[c]) s = wadd(s, x);
+        res[c] = sdiv(s, count);
+      } else if (gtypes[c] == 2) {
+        int64_t s = 0;
+        for (auto x : h[c]) s = wadd(s, x);
+        res[c] = s;
+      }
+    }
+    for (size_t c = 0; c < cols.size(); c++) {
+      auto d = mkbuf(8, stream_);
+      ck(cudaMemcpyAsync(d->as<void>(), &res[c], 8, cudaMemcpyHostToDevice, stream_), "h2d");
+      cols[c] = d;
+    }
+    ck(cudaStreamSynchronize(stream_), "sync");
+    out->n = 1;
+  } else {
+    out->n = ng;
+    // AVG finalisation of count_avg (merge.cu:446-458): (sum*100)/count when the scale
+    // is at most 2 (scale + 2), sum/count otherwise.
+    int countc = -1;
+    for (size_t c = 0; c < cols.size(); c++)
+      if (gtypes[c] == 0) {
+        countc = (int)c;
+        break;
+      }
+    for (size_t c = 0; c < cols.size(); c++) {
+      if (gtypes[c] != 1) continue;
+      if (countc < 0) unsupported("AVG needs a COUNT column in the same select");
+      auto l = mk_col("s");
+      auto r = mk_col("c");
+      AstP e = metas[c].dz <= 2 ? mk_bin(ALK_OP_DIV, mk_bin(ALK_OP_MUL, l, mk_const(100)), r)
+                                : mk_bin(ALK_OP_DIV, l, r);
+      Compiler cc;
+      alk_program prog = cc.finish(e);
+      std::vector<const int64_t*> in;
+      for (auto& sname : cc.slots) in.push_back((sname == "s" ? cols[c] : cols[countc])->as<int64_t>());
+      auto d = mkbuf(ng * 8, stream_);
+      check(alk_eval(in.data(), (uint32_t)in.size(), ng, &prog, d->as<int64_t>(), (alk_stream)stream_), "avg");
+      cols[c] = d;
+      if (metas[c].dz <= 2) metas[c].dz += 2;
+      gtypes[c] = 3;
+    }
+  }
+  for (size_t c = 0; c < cols.size(); c++) {
+    out->columnNames.push_back(names[c]);
+    out->meta[names[c]] = metas[c];
+    out->data[names[c]] = cols[c];
+    out->grp_type[names[c]] = gtypes[c];
+  }
+  vars_[st.s] = std::move(out);
+}
+
+// ------------------------------------------------------------------ JOIN
+// emit_join (operators.cu:797-924): a chain of emit_multijoin steps, then aliases.
+void Engine::emit_join(Statement& st) {
+  std::vector<std::string> op_m = st.op_value;
+  if (st.join_tab_cnt > 1) {
+    size_t oi = 0;
+    for (unsigned i = 1; i <= st.join_tab_cnt; i++) {
+      std::string tab_name = i == st.join_tab_cnt ? st.s : st.s + std::to_string(i);
+      std::string j, j2;
+      if (i == 1) {
+        j2 = st.op_join[oi++];
+        j = st.op_join[oi++];
+      } else {
+        j = oi < st.op_join.size() ? st.op_join[oi++] : st.f;
+        j2 = st.s + std::to_string(i - 1);
+      }
+      multijoin(st, tab_name, j, j2, i);
+      if (i > 1) vars_.erase(st.s + std::to_string(i - 1));
+    }
+  } else {
+    multijoin(st, st.s, st.f, st.op_join.at(0), 1);
+  }
+  Var* r = var(st.s);
+  for (unsigned k = 0; k < st.sel_count; k++) {
+    const std::string& from = op_m[2 * k];
+    const std::string& to = op_m[2 * k + 1];
+    if (from == to) continue;
+    auto it = std::find(r->columnNames.begin(), r->columnNames.end(), from);
+    if (it == r->columnNames.end()) continue;
+    *it = to;
+    r->data[to] = r->data[from];
+    r->data.erase(from);
+    r->meta[to] = r->meta[from];
+  }
+}
+
+// emit_multijoin (operators.cu:940-1582): inner equi-join of a (filtered) left side
+// with a right side; the right side is hashed (MurmurHash64A, linear probing) instead
+// of sorted, so pairs come out as a multiset.
+void Engine::multijoin(Statement& st, const std::string& s, const std::string& j1, const std::string& j2,
+                       unsigned tab) {
+  Var* left = var(j1);
+  Var* right = var(j2);
+  std::vector<std::string> op_sel, op_g;
+  size_t k = 0;
+  for (unsigned i = 0; i < st.sel_count; i++, k += 2) op_sel.push_back(st.op_value.at(k));
+  op_g.assign(st.op_value.begin() + k, st.op_value.end());
+  std::vector<std::string> op_sel_s = op_sel;
+  size_t gi = 0;
+  for (unsigned z = 0; z < st.join_tab_cnt - tab; z++) {
+    unsigned jac = st.join_and_cnt.count(z) ? st.join_and_cnt.at(z) : 0;
+    for (unsigned j = 0; j < jac * 2 + 2; j++) op_sel_s.push_back(op_g.at(gi++));
+  }
+  std::string f1 = op_g.at(gi), f2 = op_g.at(gi + 1);
+  unsigned jac = st.join_and_cnt.count(st.join_tab_cnt - tab) ? st.join_and_cnt.at(st.join_tab_cnt - tab) : 0;
+  if (jac) unsupported("multi-column joins");
+  if (st.join_type.at(tab - 1) != 'I') unsupported("outer / semi / anti joins");
+  auto c = std::make_unique<Var>();
+  c->kind = Var::Mat;
+  c->name = s;
+  for (auto& n : op_sel_s) {
+    if (c->has(n)) continue;
+    if (right->has(n)) c->meta[n] = right->meta[n];
+    else if (left->has(n)) c->meta[n] = left->meta[n];
+    else continue;
+    c->columnNames.push_back(n);
+  }
+  std::string colname1, colname2;
+  if (left->has(f1)) {
+    colname1 = f1;
+    if (!right->has(f2)) throw EngineError(ALK_ERR_ARG, "Couldn't find column " + f2);
+    colname2 = f2;
+  } else if (right->has(f1)) {
+    colname2 = f1;
+    if (!left->has(f2)) throw EngineError(ALK_ERR_ARG, "Couldn't find column " + f2);
+    colname1 = f2;
+  } else {
+    throw EngineError(ALK_ERR_ARG, "Couldn't find column " + f1);
+  }
+  if (left->meta[colname1].type != right->meta[colname2].type) unsupported("join of different column types");
+  std::vector<std::string> rfields, lfields;
+  for (auto& n : c->columnNames)
+    if (!left->has(n) && right->has(n)) rfields.push_back(n);
+  rfields.push_back(colname2);
+  for (auto& n : c->columnNames)
+    if (left->has(n)) lfields.push_back(n);
+  lfields.push_back(colname1);
+  Rows R = materialize(right, rfields);
+  Rows L = materialize(left, lfields);
+  c->n = 0;
+  if (R.n && L.n) {
+    alk_join_table* t = nullptr;
+    check(alk_join_build(R.col.at(colname2)->as<int64_t>(), R.n, &t, (alk_stream)stream_), "join build");
+    struct TableGuard {
+      alk_join_table* t;
+      cudaStream_t s;
+      ~TableGuard() { alk_join_free(t, (alk_stream)s); }
+    } guard{t, stream_};
+    uint64_t cap = std::max<uint64_t>(L.n, 1024), pairs = 0;
+    DevBufP pl, pr;
+    for (int attempt = 0; attempt < 2; attempt++) {
+      pl = mkbuf(cap * 4, stream_);
+      pr = mkbuf(cap * 4, stream_);
+      int rc = alk_join_probe(t, L.col.at(colname1)->as<int64_t>(), L.n, pl->as<uint32_t>(), pr->as<uint32_t>(), cap,
+                              &pairs, (alk_stream)stream_);
+      if (rc == ALK_ERR_OVERFLOW && attempt == 0) {
+        cap = pairs;
+        continue;
+      }
+      check(rc, "join probe");
+      break;
+    }
+    c->n = pairs;
+    for (auto& n : c->columnNames) {
+      bool from_left = left->has(n);
+      const DevBufP& src = from_left ? L.col.at(n) : R.col.at(n);
+      auto d = mkbuf(std::max<uint64_t>(pairs, 1) * 8, stream_);
+      check(alk_gather(src->as<int64_t>(), (from_left ? pl : pr)->as<uint32_t>(), pairs, d->as<int64_t>(),
+                       (alk_stream)stream_),
+            "join gather");
+      c->data[n] = d;
+    }
+    ck(cudaStreamSynchronize(stream_), "join sync");
+  } else {
+    for (auto& n : c->columnNames) c->data[n] = mkbuf(8, stream_);
+  }
+  vars_[s] = std::move(c);
+}
+
+// ------------------------------------------------------------------ ORDER
+// emit_order (operators.cu:1641-1798): stable sort, first key most significant, ties
+// in input order.
+void Engine::emit_order(Statement& st) {
+  Var* a = var(st.f);
+  std::vector<std::string> keys;
+  std::vector<uint8_t> desc;
+  size_t iv = 0;
+  for (auto& t : st.op_type) {
+    if (t == "NAME") {
+      keys.push_back(st.op_value.at(iv++));
+      desc.push_back(0);
+    } else {
+      keys.push_back(t);
+      desc.push_back(st.op_value.at(iv++) == "DESC");
+    }
+    if (!a->has(keys.back())) throw EngineError(ALK_ERR_ARG, "Couldn't find name " + keys.back());
+    if (a->meta[keys.back()].type == 2 || !a->meta[keys.back()].string_map.empty())
+      unsupported("ORDER BY on a char column");
+  }
+  Rows R = materialize(a, a->columnNames);
+  auto b = std::make_unique<Var>();
+  b->kind = Var::Mat;
+  b->name = st.s;
+  b->columnNames = a->columnNames;
+  b->meta = a->meta;
+  b->grp_type = a->grp_type;
+  b->n = R.n;
+  if (R.n) {
+    std::vector<const int64_t*> kc;
+    for (auto& kname : keys) kc.push_back(R.col.at(kname)->as<int64_t>());
+    auto perm = mkbuf(R.n * 4, stream_);
+    check(alk_sort_perm(kc.data(), desc.data(), (uint32_t)kc.size(), R.n, perm->as<uint32_t>(), (alk_stream)stream_),
+          "order");
+    for (auto& n : a->columnNames) {
+      auto d = mkbuf(R.n * 8, stream_);
+      check(alk_gather(R.col.at(n)->as<int64_t>(), perm->as<uint32_t>(), R.n, d->as<int64_t>(), (alk_stream)stream_),
+            "order gather");
+      b->data[n] = d;
+    }
+  } else {
+    for (auto& n : a->columnNames) b->data[n] = mkbuf(8, stream_);
+  }
+  vars_[st.s] = std::move(b);
+}
+
+// ------------------------------------------------------------------ STORE
+// emit_store / CudaSet::Store text output (operators.cu:2410-2444, cm.cu:1479-1560).
+void Engine::emit_store(Statement& st) {
+  Var* a = var(st.s);
+  size_t limit = st.op_nums.empty() ? 0 : (size_t)st.op_nums[0];
+  Rows R = materialize(a, a->columnNames);
+  size_t mcount = (limit != 0 && limit < R.n) ? limit : R.n;
+  std::vector<std::vector<int64_t>> h(a->columnNames.size(), std::vector<int64_t>(mcount));
+  for (size_t c = 0; c < a->columnNames.size(); c++) {
+    if (!mcount) break;
+    ck(cudaMemcpyAsync(h[c].data(), R.col.at(a->columnNames[c])->as<void>(), mcount * 8, cudaMemcpyDeviceToHost,
+                       stream_),
+       "store d2h");
+    stats_.d2h_bytes += mcount * 8;
+  }
+  ck(cudaStreamSynchronize(stream_), "store sync");
+  std::string path = st.f;
+  if (path.empty() || path[0] != '/') path = dir_ + "/" + path;
+  FILE* fp = std::fopen(path.c_str(), "w");
+  if (!fp) throw EngineError(ALK_ERR_IO, "Could not open file " + path);
+  std::vector<const std::vector<std::string>*> dicts(a->columnNames.size(), nullptr);
+  std::vector<uint32_t> widths(a->columnNames.size(), 0);
+  for (size_t c = 0; c < a->columnNames.size(); c++) {
+    const ColMeta& m = a->meta[a->columnNames[c]];
+    if (m.string_map.empty()) continue;
+    auto dot = m.string_map.find('.');
+    Var* b = base_table(m.string_map.substr(0, dot));
+    if (!b) throw EngineError(ALK_ERR_IO, "missing dictionary " + m.string_map);
+    std::string col = m.string_map.substr(dot + 1);
+    BaseCol& bc = basecol(b, col);
+    load_dict(b, col, bc);
+    dicts[c] = &bc.dict;
+    widths[c] = bc.meta.width;
+  }
+  std::string line;
+  for (size_t i = 0; i < mcount; i++) {
+    line.clear();
+    for (size_t c = 0; c < a->columnNames.size(); c++) {
+      const ColMeta& m = a->meta[a->columnNames[c]];
+      int64_t v = h[c][i];
+      if (!dicts[c]) {
+        if (m.dz) {
+          std::string s = std::to_string(v);
+          while (s.size() <= m.dz) s = '0' + s;
+          s.insert(s.size() - m.dz, ".");
+          line += s;
+        } else {
+          line += std::to_string(v);
+        }
+      } else {
+        std::string s = (v >= 0 && (size_t)v < dicts[c]->size()) ? (*dicts[c])[v] : std::string();
+        line += s.substr(0, std::min(s.size(), std::strlen(s.c_str())));
+      }
+      line += st.sep;
+    }
+    if (i != mcount - 1) line += "\n";
+    std::fputs(line.c_str(), fp);
+  }
+  std::fclose(fp);
+}
+
+// ------------------------------------------------------------------ script
+void Engine::exec(Statement& st) {
+  switch (st.kind) {
+    case StmtKind::Filter: emit_filter(st); break;
+    case StmtKind::Select: emit_select(st); break;
+    case StmtKind::Join: emit_join(st); break;
+    case StmtKind::Order: emit_order(st); break;
+    case StmtKind::Store: emit_store(st); break;
+    case StmtKind::Display: break;
+    default: unsupported("statement kind (LOAD / STORE BINARY / catalog commands)");
+  }
+}
+
+void Engine::reset_script_state() {
+  vars_.clear();
+  stats_ = alk_stats{};
+}
+
+int Engine::execute(const std::string& script) {
+  std::vector<Statement> sts;
+  std::string perr;
+  err_.clear();
+  if (!parse_script(script, sts, perr)) {
+    err_ = "parse: " + perr;
+    return ALK_ERR_PARSE;
+  }
+  reset_script_state();
+  uint64_t k0 = g_kernel_launches;
+  int rc = ALK_OK;
+  try {
+    // tables named anywhere in the script (load_vars, operators.cu:2708-2747)
+    std::set<std::string> names;
+    for (auto& st : sts) {
+      names.insert(st.s);
+      names.insert(st.f);
+      for (auto& j : st.op_join) names.insert(j);
+    }
+    for (auto& n : names) {
+      Var* b = base_table(n);
+      if (b) vars_[n] = std::make_unique<Var>(*b);
+    }
+    // last use of every variable (the mystat liveness of pass one)
+    std::map<std::string, size_t> last;
+    for (size_t i = 0; i < sts.size(); i++) {
+      auto& st = sts[i];
+      last[st.s] = std::max(last[st.s], i);
+      if (!st.f.empty() && st.kind != StmtKind::Store) last[st.f] = i;
+      for (auto& j : st.op_join) last[j] = i;
+    }
+    for (size_t i = 0; i < sts.size(); i++) {
+      if (!(flags_ & ALK_SESSION_PLAIN) && try_fused(sts, i)) continue;
+      exec(sts[i]);
+      for (auto it = vars_.begin(); it != vars_.end();) {
+        auto l = last.find(it->first);
+        if (it->second->kind == Var::Mat && (l == last.end() || l->second <= i)) it = vars_.erase(it);
+        else ++it;
+      }
+    }
+    ck(cudaStreamSynchronize(stream_), "script");
+  } catch (const EngineError& e) {
+    err_ = e.what();
+    rc = e.code;
+    cudaStreamSynchronize(stream_);
+  } catch (const std::exception& e) {
+    err_ = e.what();
+    rc = ALK_ERR_ARG;
+    cudaStreamSynchronize(stream_);
+  }
+  vars_.clear();
+  if (!(flags_ & ALK_SESSION_RESIDENT)) {
+    for (auto& t : basecols_)
+      for (auto& c : t.second)
+        for (auto& d : c.second.dev) d.reset();
+  }
+  cudaStreamSynchronize(stream_);
+  stats_.kernels = g_kernel_launches - k0;
+  return rc;
+}
+
+}  // namespace alk

@@ -1,0 +1,49 @@
+// Alenka script front end: lexer + parser producing, per statement, the postfix
+// argument queues that the reference's grammar actions fill before calling an
+// emit_* operator (bison.y:127-287, fl.l:38-133, emit helpers operators.cu:62-360).
+// The queues keep the reference's names and meaning:
+//   op_type / op_value / op_nums / op_nums_f / op_nums_precision  (cm.h:69-77)
+//   op_join / join_type / join_eq_type / sel_count / join_tab_cnt / join_and_cnt
+//   (operators.cu:27-41)
+#pragma once
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+namespace alk {
+
+enum class StmtKind {
+  Filter,       // emit_filter(s, f)              bison.y:140
+  Select,       // emit_select(s, f, grp_cnt)     bison.y:136
+  Join,         // emit_join(s, f, ...)           bison.y:144
+  Order,        // emit_order(s, f, e)            bison.y:142
+  Store,        // emit_store(s, file, sep)       bison.y:146
+  StoreBinary,  // emit_store_binary(s, file, append)  bison.y:148-150
+  Display,      // emit_display(s, sep)           bison.y:156
+  Load,         // emit_load (CSV)                bison.y:138
+  Other         // DESCRIBE / SHOW / DROP / INSERT / DELETE / CREATE
+};
+
+struct Statement {
+  StmtKind kind = StmtKind::Other;
+  std::string s;      // target variable (Store/Display: variable to write)
+  std::string f;      // source variable (Store: output file)
+  std::string sep;    // Store/Display separator
+  int grp_cnt = 0;    // number of GROUP BY columns
+  bool append = false;
+  std::vector<std::string> op_type, op_value;
+  std::vector<int64_t> op_nums;
+  std::vector<double> op_nums_f;
+  std::vector<uint32_t> op_nums_precision;
+  std::vector<std::string> op_join;
+  std::vector<char> join_type, join_eq_type;
+  unsigned sel_count = 0, join_tab_cnt = 0;
+  std::map<unsigned, unsigned> join_and_cnt;
+  int line = 0;
+};
+
+// Parse a whole script. Returns false and sets err ("line N: message") on a syntax error.
+bool parse_script(const std::string& text, std::vector<Statement>& out, std::string& err);
+
+}  // namespace alk

@@ -1,0 +1,62 @@
+"""Benchmark and parity workloads: seeded synthetic tables of the TPC-H-like shapes and
+the Alenka scripts run over them (single-table filter + group-by; the three-way
+filter -> join -> group-by -> order pipeline of the reference's README)."""
+import random
+
+from . import date_add_days, gen_lineitem_flat, gen_three_way
+
+SEGMENTS = ["AUTOMOBILE", "BUILDING", "FURNITURE", "HOUSEHOLD", "MACHINERY"]
+
+
+def flat_cutoff(seed):
+    """Shipdate cutoff near the median of 1992-01-02..1998-12-01 (about 50% selectivity)."""
+    return date_add_days(19950617, random.Random(seed).randint(-30, 30))
+
+
+def flat_script(seed, out="q1.txt"):
+    cut = flat_cutoff(seed)
+    return (f"LF := FILTER lineitem BY l_shipdate < {cut};\n"
+            "R := SELECT l_returnflag AS l_returnflag, l_linestatus AS l_linestatus, "
+            "SUM(l_quantity) AS sum_qty, SUM(l_extendedprice) AS sum_base_price, "
+            "SUM(l_extendedprice*(1-l_discount)) AS sum_disc_price, COUNT(l_orderkey) AS count_order "
+            "FROM LF GROUP BY l_returnflag, l_linestatus;\n"
+            f"STORE R INTO '{out}' USING ('|');\n")
+
+
+def three_way_params(seed):
+    r = random.Random(seed * 7919 + 1)
+    date = date_add_days(19950702, r.randint(-30, 30))
+    return date, SEGMENTS[r.randint(0, 4)]
+
+
+def three_way_script(seed, out="q3.txt", limit=10):
+    date, seg = three_way_params(seed)
+    lim = f" LIMIT {limit}" if limit else ""
+    return (f"OFI := FILTER orders BY o_orderdate < {date};\n"
+            f"CF := FILTER customer BY c_mktsegment == \"{seg}\";\n"
+            f"LF := FILTER lineitem BY l_shipdate > {date};\n"
+            "OLC := SELECT o_orderkey AS o_orderkey, o_orderdate AS o_orderdate, "
+            "o_shippriority AS o_shippriority, l_extendedprice AS price, l_discount AS discount "
+            "FROM LF JOIN OFI ON l_orderkey = o_orderkey JOIN CF ON o_custkey = c_custkey;\n"
+            "F := SELECT o_orderkey AS o_orderkey1, o_orderdate AS orderdate1, o_shippriority AS priority, "
+            "SUM(price*(1-discount)) AS sum_revenue, COUNT(o_orderkey) AS cnt "
+            "FROM OLC GROUP BY o_orderkey, o_orderdate, o_shippriority;\n"
+            "RES := ORDER F BY sum_revenue DESC, orderdate1 ASC;\n"
+            f"STORE RES INTO '{out}' USING ('|'){lim};\n")
+
+
+# Full-size shapes (rows): the single-table workload and the three-way pipeline.
+FLAT_ROWS = 6_000_000
+THREE_WAY = dict(customers=1_500_000, orders=15_000_000, lineitems=60_000_000)
+
+
+def make_flat(data_dir, rows=FLAT_ROWS, seg_rows=2_000_000, seed=1, delta=False):
+    gen_lineitem_flat(data_dir, rows, seg_rows, seed, delta)
+
+
+def make_three_way(data_dir, scale=1.0, seg_rows=10_000_000, seed=1, delta=False):
+    c = max(1, int(THREE_WAY["customers"] * scale))
+    o = max(1, int(THREE_WAY["orders"] * scale))
+    li = max(1, int(THREE_WAY["lineitems"] * scale))
+    gen_three_way(data_dir, c, o, li, seg_rows, seed, delta)
+    return li

@@ -1,0 +1,197 @@
+/*
+ * alenka_b200 — C ABI of the B200 (sm_100a) engine for Alenka's columnar
+ * scan -> filter -> join -> group-by -> order path.
+ *
+ * Two layers, both plain C (pointers, sizes, status codes):
+ *   1. The embedding API a host program binds, with the reference's names and
+ *      meaning (alenka.h:30-35): alenkaInit / alenkaExecute / alenkaClose /
+ *      execute_file, plus explicit-session variants (alk_session_*).
+ *   2. Operator-level entry points, one per reference operator on the path. The
+ *      engine behind layer 1 reaches the GPU only through these.
+ * Every call is asynchronous on the given stream unless it returns a host value;
+ * status 0 = OK. Device pointers are device memory the caller owns unless noted.
+ */
+#ifndef ALENKA_B200_H
+#define ALENKA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* alk_stream; /* a cudaStream_t; NULL = legacy default stream */
+
+/* ---------------------------------------------------------------- status */
+#define ALK_OK 0
+#define ALK_ERR_ARG 1         /* invalid argument */
+#define ALK_ERR_CUDA 2        /* CUDA runtime error (context still usable) */
+#define ALK_ERR_OVERFLOW 3    /* output capacity too small; the required size is returned */
+#define ALK_ERR_TIMEOUT 4     /* a bounded device wait expired */
+#define ALK_ERR_UNSUPPORTED 5 /* script form outside the supported surface */
+#define ALK_ERR_IO 6          /* missing or malformed segment / catalog file */
+#define ALK_ERR_PARSE 7       /* script syntax error */
+#define ALK_ERR_NOMEM 8       /* device allocation failed */
+
+/* ------------------------------------------------- 1. embedding (alenka.h) */
+/* alenkaInit (alenka.h:30): reads the flags of execute_file (bison.y:306-331) from
+ * av (NULL-terminated); the data directory is the current directory. */
+void alenkaInit(char** av);
+/* alenkaExecute (alenka.h:31, bison.y:469-515): runs one script; 0 = success. */
+int alenkaExecute(char* s);
+/* alenkaClose (alenka.h:32): releases the engine. */
+void alenkaClose(void);
+/* execute_file (alenka.h:35, bison.y:295-455): alenka [-l MB] [-v] script.sql */
+int execute_file(int ac, char** av);
+
+/* Explicit sessions: the same engine with a chosen data directory. */
+typedef struct alk_session alk_session;
+/* flags: ALK_SESSION_RESIDENT keeps every loaded column segment in device memory
+ * across scripts (the reference's -i buffers, cm.cu:616-656, one level further). */
+#define ALK_SESSION_RESIDENT 1u
+#define ALK_SESSION_PLAIN 2u  /* operator-at-a-time plan only (no fused pipelines) */
+int alk_session_open(const char* data_dir, uint32_t flags, alk_session** out);
+int alk_session_execute(alk_session* s, const char* script);
+const char* alk_session_error(alk_session* s);
+alk_stream alk_session_stream(alk_session* s);
+/* Pre-load (and pin in device memory) every column of a catalog table. */
+int alk_session_preload(alk_session* s, const char* table);
+/* Statistics of the last script: fact rows scanned, device kernels launched, bytes
+ * copied host->device and device->host, and the plan used (0 plain, 1 fused). */
+typedef struct alk_stats {
+  uint64_t rows_scanned;
+  uint64_t kernels;
+  uint64_t h2d_bytes;
+  uint64_t d2h_bytes;
+  uint32_t plan;
+  uint32_t segments_skipped;
+  double hot_kernel_ms;      /* device time of the dominant kernel (CUDA events) */
+  uint64_t hot_kernel_bytes; /* algorithmic bytes that kernel moves */
+  uint64_t hot_kernel_launches;
+} alk_stats;
+int alk_session_stats(alk_session* s, alk_stats* out);
+/* Enable CUDA-event timing of the dominant kernel (adds two event records per launch). */
+int alk_session_set_timing(alk_session* s, int on);
+void alk_session_close(alk_session* s);
+
+/* ------------------------------------------------- 2. operator entry points */
+
+/* One column of one segment as it sits in device memory. FOR columns keep the
+ * on-disk width (bits 8/16/32/64, value = stored + lower); delta columns are first
+ * expanded with alk_decode_segment and then described with bits=64, lower=0. */
+typedef struct alk_colseg {
+  const void* data;
+  int64_t lower;
+  uint32_t rows;
+  uint32_t bits;
+} alk_colseg;
+
+/* Arrays of device pointers (const int64_t* const* d_cols and the like) are HOST
+ * arrays holding device addresses. */
+
+/* Segment decode, replaces pfor_decompress (compress.cu:180-267): FOR (comp_type 0)
+ * widening and FOR-delta (comp_type 1) MSB-first bit unpacking + prefix sum. d_payload
+ * must be 16-byte aligned and readable up to a multiple of 16 bytes. */
+int alk_decode_segment(const void* d_payload, uint32_t comp_type, uint32_t bits,
+                       uint32_t fit_count, int64_t lower, int64_t start_val, uint32_t rows,
+                       int64_t* d_out, alk_stream stream);
+
+/* MurmurHash64A of n tuples of k int64 keys (row-major tuples built from k column
+ * pointers), seed as given (hash_seed 100, bison.y:304). Replaces the host loop of
+ * add() (merge.cu:118-141) and MurmurHash64A (MurmurHash2_64.cu:201-242). */
+int alk_hash_tuples(const int64_t* const* d_cols, uint32_t k, uint64_t n, uint32_t seed,
+                    uint64_t* d_out, alk_stream stream);
+
+/* Predicate / expression program: a register machine over int64 values that the host
+ * compiles from the reference's postfix queues (filter.cu:133-643, select.cu:359-800,
+ * cm.cu:2250-2655). Operands are registers, columns (slots) or constants. */
+#define ALK_MAX_INSTR 48
+#define ALK_MAX_CONST 48
+#define ALK_MAX_REGS 8
+enum {
+  ALK_OP_ADD = 1, ALK_OP_SUB, ALK_OP_MUL, ALK_OP_DIV,
+  ALK_OP_LT, ALK_OP_GT, ALK_OP_LE, ALK_OP_GE, ALK_OP_EQ, ALK_OP_NE,
+  ALK_OP_AND, ALK_OP_OR, ALK_OP_MOV
+};
+enum { ALK_K_REG = 0, ALK_K_COL = 1, ALK_K_CONST = 2 };
+typedef struct alk_instr {
+  uint8_t op, dst, ka, kb;
+  uint16_t a, b;
+  uint32_t pad;
+} alk_instr;
+typedef struct alk_program {
+  uint32_t n_instr;
+  uint32_t result; /* register holding the result */
+  alk_instr ins[ALK_MAX_INSTR];
+  int64_t consts[ALK_MAX_CONST];
+} alk_program;
+
+/* Fused segment scan, replaces filter_op + filter + copyColumns/mygather
+ * (cm.cu:3609-3666, filter.cu:133-643, cm.cu:3305-3478): for every segment whose
+ * zone-map verdict (seg_mode: 0 skip 'N', 1 all rows 'A', 2 evaluate 'R',
+ * zone_map.cu:720) asks for it, decode the predicate columns, run the predicate and
+ * write the surviving rows' out_cols (decoded to int64) in segment/row order.
+ * cols is a host array [ncols][nseg]; out_cols lists column slots to emit; out_rowid
+ * (optional) receives the row's index within its segment and out_seg (optional) its
+ * segment. seg_counts (optional, device, nseg) receives the per-segment survivors.
+ * Returns the survivor count in *h_count; if it exceeds cap nothing past cap is written
+ * and ALK_ERR_OVERFLOW is returned. Synchronizes the stream. */
+int alk_scan_filter(const alk_colseg* cols, uint32_t ncols, uint32_t nseg,
+                    const uint8_t* seg_mode, const alk_program* pred,
+                    const uint32_t* out_cols, uint32_t nout, int64_t* const* d_out,
+                    uint32_t* d_out_rowid, uint32_t* d_out_seg, uint64_t* d_seg_counts,
+                    uint64_t cap, uint64_t* h_count, alk_stream stream);
+
+/* Expression evaluation over materialized columns, replaces CudaSet::op chains
+ * (cm.cu:2440-2773) as driven by select() (select.cu:700-800). */
+int alk_eval(const int64_t* const* d_cols, uint32_t ncols, uint64_t n, const alk_program* prog,
+             int64_t* d_out, alk_stream stream);
+
+/* Hash group-by with exact int64 aggregates, replaces order_inplace + GroupBy +
+ * segreduce (operators.cu:367-406, cm.cu:910-956, select.cu:499-675).
+ * aggs: per value column ALK_AGG_*; COUNT ignores its column (may be NULL).
+ * Outputs (device, capacity n): group keys [nkeys][G], aggregates [nvals][G], and the
+ * first input row of each group (smallest row index). Group order is unspecified;
+ * *h_groups receives G. Synchronizes the stream. */
+enum { ALK_AGG_SUM = 0, ALK_AGG_COUNT = 1, ALK_AGG_MIN = 2, ALK_AGG_MAX = 3 };
+int alk_groupby_hash(const int64_t* const* d_keys, uint32_t nkeys, const int64_t* const* d_vals,
+                     const uint8_t* aggs, uint32_t nvals, uint64_t n, int64_t* const* d_out_keys,
+                     int64_t* const* d_out_vals, uint32_t* d_out_first, uint64_t* h_groups,
+                     alk_stream stream);
+
+/* Stable multi-key sort permutation, replaces update_permutation (sorts.cu:18-70) as
+ * used by emit_order (operators.cu:1754-1763) and order_inplace: keys[0] is the most
+ * significant; desc[i] != 0 sorts key i descending; ties keep input order. Writes the
+ * permutation (input row index per output position) to d_perm. Synchronizes. */
+int alk_sort_perm(const int64_t* const* d_keys, const uint8_t* desc, uint32_t nkeys, uint64_t n,
+                  uint32_t* d_perm, alk_stream stream);
+/* Same for unsigned 64-bit keys (hash order of merge.cu:147-149). */
+int alk_sort_perm_u64(const uint64_t* d_key, uint64_t n, uint32_t* d_perm, alk_stream stream);
+
+/* Gather, replaces thrust::gather in mygather / apply_permutation (cm.cu:3350,
+ * sorts.cu:87): d_out[i] = d_src[d_idx[i]]. */
+int alk_gather(const int64_t* d_src, const uint32_t* d_idx, uint64_t n, int64_t* d_out,
+               alk_stream stream);
+
+/* Width conversions used by the host engine between index and value columns. */
+int alk_widen_u32(const uint32_t* d_in, uint64_t n, int64_t* d_out, alk_stream stream);
+int alk_narrow_u32(const int64_t* d_in, uint64_t n, uint32_t* d_out, alk_stream stream);
+
+/* Linear-probing hash join on MurmurHash64A keys, replaces the sort-merge join of
+ * emit_multijoin (operators.cu:1117-1283, moderngpu inner_join). Build indexes the
+ * right rows; probe emits every (left row, right row) pair with equal keys. */
+typedef struct alk_join_table alk_join_table;
+int alk_join_build(const int64_t* d_keys, uint64_t n, alk_join_table** out, alk_stream stream);
+/* Writes up to cap pairs; *h_pairs receives the total; ALK_ERR_OVERFLOW if total > cap. */
+int alk_join_probe(const alk_join_table* t, const int64_t* d_keys, uint64_t n, uint32_t* d_left,
+                   uint32_t* d_right, uint64_t cap, uint64_t* h_pairs, alk_stream stream);
+void alk_join_free(alk_join_table* t, alk_stream stream);
+
+/* Device and kernel inventory (for tests): number of sm_100a kernels in this library. */
+int alk_device_info(int* sm_count, int* cc_major, int* cc_minor);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ALENKA_B200_H */
