@@ -473,8 +473,10 @@ __global__ void __launch_bounds__(kT) k_radix_scatter(const uint64_t* keys, cons
 #pragma unroll
       for (int e = 0; e < kRadix; e++)
         if (d == (uint32_t)e) p = pre[e]++;
-      okeys[p] = kk[k];
-      ovals[p] = vv[k];
+      if (p < n) {  // always true for a consistent histogram; guards the write
+        okeys[p] = kk[k];
+        ovals[p] = vv[k];
+      }
     }
   }
 }
@@ -538,6 +540,25 @@ __global__ void __launch_bounds__(kT) k_join_probe(const int64_t* keys, uint64_t
       h = (h + 1) & mask;
     }
   }
+}
+
+// Every operand of a program must name an existing register, column slot or constant:
+// the device code indexes shared arrays with them unchecked.
+bool program_ok(const alk_program* p, uint32_t ncols) {
+  if (p->n_instr > ALK_MAX_INSTR || p->result >= ALK_MAX_REGS) return false;
+  for (uint32_t i = 0; i < p->n_instr; i++) {
+    const alk_instr& in = p->ins[i];
+    if (in.dst >= ALK_MAX_REGS || in.op < ALK_OP_ADD || in.op > ALK_OP_MOV) return false;
+    const uint8_t k[2] = {in.ka, in.kb};
+    const uint16_t x[2] = {in.a, in.b};
+    for (int j = 0; j < 2; j++) {
+      if (k[j] == ALK_K_REG && x[j] >= ALK_MAX_REGS) return false;
+      if (k[j] == ALK_K_COL && x[j] >= ncols) return false;
+      if (k[j] == ALK_K_CONST && x[j] >= ALK_MAX_CONST) return false;
+      if (k[j] > ALK_K_CONST) return false;
+    }
+  }
+  return true;
 }
 
 int grid_for(uint64_t n) {
@@ -656,7 +677,7 @@ int alk_scan_filter(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const
                     uint64_t* h_count, alk_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (!h_count || ncols == 0 || ncols > kMaxCols || nout > kMaxCols) return ALK_ERR_ARG;
-  if (pred && (pred->n_instr > ALK_MAX_INSTR || pred->result >= ALK_MAX_REGS)) return ALK_ERR_ARG;
+  if (pred && !program_ok(pred, ncols)) return ALK_ERR_ARG;
   for (uint32_t o = 0; o < nout; o++)
     if (out_cols[o] >= ncols) return ALK_ERR_ARG;
   *h_count = 0;
@@ -746,7 +767,7 @@ int alk_eval(const int64_t* const* d_cols, uint32_t ncols, uint64_t n, const alk
              alk_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (n == 0) return ALK_OK;
-  if (!prog || ncols > kMaxCols || prog->n_instr > ALK_MAX_INSTR || prog->result >= ALK_MAX_REGS) return ALK_ERR_ARG;
+  if (!prog || ncols > kMaxCols || !program_ok(prog, ncols)) return ALK_ERR_ARG;
   Scratch sc(s);
   cudaError_t e;
   uint8_t* db = sc.get<uint8_t>(sizeof(alk_program) + sizeof(void*) * kMaxCols, &e);

@@ -188,7 +188,11 @@ int alk_join_probe(const alk_join_table* t, const int64_t* d_keys, uint64_t n, u
                    uint32_t* d_right, uint64_t cap, uint64_t* h_pairs, alk_stream stream);
 void alk_join_free(alk_join_table* t, alk_stream stream);
 
-/* Device and kernel inventory (for tests): number of sm_100a kernels in this library. */
+/* Front end: renders the statements and postfix queues the parser produces for a script
+ * (the argument queues of the reference's grammar actions, bison.y:127-287). */
+int alk_parse_dump(const char* script, char* out, int out_len);
+
+/* Device properties of the current device. */
 int alk_device_info(int* sm_count, int* cc_major, int* cc_minor);
 
 #ifdef __cplusplus
