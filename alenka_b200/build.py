@@ -18,7 +18,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SRCS = ["csrc/kernels.cu", "csrc/pipeline.cu"]
 CPP_SRCS = ["host/format.cpp", "host/script.cpp", "host/engine.cpp", "host/engine_ops.cpp",
-            "host/fused.cpp", "host/capi.cpp", "host/gen.cpp"]
+            "host/capi.cpp", "host/gen.cpp"]
 
 
 def _run(cmd):

@@ -479,7 +479,13 @@ int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg
   cudaStream_t s = (cudaStream_t)stream;
   if (!probe || probe_slot < 0 || (uint32_t)probe_slot >= ncols || ncols == 0 || ncols > kMaxCols || nagg > 7)
     return ALK_ERR_ARG;
-  if (acc_stride < probe->v.slot_cap) return ALK_ERR_ARG;
+  {
+    // accumulators are indexed by the probed table's slots: one per inserted key
+    unsigned long long ns = 0;
+    CK(cudaMemcpyAsync(&ns, probe->v.nslots, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (acc_stride < std::min<uint64_t>(ns, probe->v.slot_cap)) return ALK_ERR_ARG;
+  }
   std::vector<alk_program> progs(1 + nagg);
   std::memset(progs.data(), 0, sizeof(alk_program) * progs.size());
   if (pred) progs[0] = *pred;

@@ -144,3 +144,22 @@ extern "C" int alk_parse_dump(const char* script, char* out, int out_len) {
   if (out && out_len > 0) std::snprintf(out, (size_t)out_len, "%s", s.c_str());
   return (int)s.size() < out_len ? ALK_OK : ALK_ERR_OVERFLOW;
 }
+
+// Segment writer (the store side of the format): FOR, or FOR-delta when delta is set and
+// the values are sorted, exactly as pfor_compress / pfor_delta_compress lay them out
+// (compress.cu:271-527). Writes the whole segment file image to out.
+extern "C" int alk_encode_segment(const int64_t* values, uint32_t n, int delta, uint8_t* out, size_t cap,
+                                  size_t* out_len) {
+  if (!values || !out_len || n == 0) return ALK_ERR_ARG;
+  alk::SegMeta m;
+  std::vector<uint8_t> payload;
+  bool sorted = true;
+  for (uint32_t i = 1; i < n && sorted; i++) sorted = values[i - 1] <= values[i];
+  if (delta && sorted) alk::encode_delta(values, n, m, payload);
+  else alk::encode_for(values, n, m, payload);
+  std::vector<uint8_t> img = alk::segment_image(m, payload);
+  *out_len = img.size();
+  if (img.size() > cap || !out) return ALK_ERR_OVERFLOW;
+  std::memcpy(out, img.data(), img.size());
+  return ALK_OK;
+}

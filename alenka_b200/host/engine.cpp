@@ -794,3 +794,65 @@ Rows Engine::materialize(Var* v, const std::vector<std::string>& fields, bool wa
 }
 
 }  // namespace alk
+
+namespace alk {
+
+uint32_t ScanPlan::slot(const std::string& c) {
+  auto it = std::find(slots.begin(), slots.end(), c);
+  if (it != slots.end()) return (uint32_t)(it - slots.begin());
+  slots.push_back(c);
+  if (slots.size() > 16) throw EngineError(ALK_ERR_UNSUPPORTED, "scan reads more than 16 columns");
+  return (uint32_t)slots.size() - 1;
+}
+
+ScanPlan Engine::plan_scan(Var* v) {
+  ScanPlan p;
+  p.src = v->kind == Var::Filtered ? var(v->source) : v;
+  if (p.src->kind != Var::Base) throw EngineError(ALK_ERR_UNSUPPORTED, "scan of a materialized result");
+  p.mode.assign(p.src->segCount, 1);
+  if (v->kind == Var::Filtered) {
+    std::vector<char> zm = zone_maps(v, p.src);
+    p.pred = compile_filter(v, p.src, p.slots);
+    p.has_pred = true;
+    for (uint32_t g = 0; g < p.src->segCount; g++) {
+      p.mode[g] = zm[g] == 'N' ? 0 : (zm[g] == 'A' ? 1 : 2);
+      if (!p.mode[g]) stats_.segments_skipped++;
+    }
+  }
+  return p;
+}
+
+std::vector<alk_colseg> Engine::colsegs(const ScanPlan& p) {
+  Var* src = p.src;
+  std::vector<alk_colseg> cs(p.slots.size() * src->segCount);
+  for (size_t c = 0; c < p.slots.size(); c++) {
+    ensure_base_col(src, p.slots[c], true);
+    BaseCol& bc = basecol(src, p.slots[c]);
+    for (uint32_t g = 0; g < src->segCount; g++) {
+      const SegMeta& m = bc.segs[g].m;
+      alk_colseg& d = cs[c * src->segCount + g];
+      d.data = bc.dev[g]->as<void>();
+      d.rows = m.rec_count;
+      d.lower = m.comp_type == 1 ? 0 : m.orig_lower;
+      d.bits = m.comp_type == 1 ? 64 : m.bits;
+    }
+  }
+  for (uint32_t g = 0; g < src->segCount; g++)
+    if (p.mode[g] && !cs.empty()) stats_.rows_scanned += cs[g].rows;
+  return cs;
+}
+
+uint64_t Engine::scan_bytes(const ScanPlan& p, const std::vector<uint32_t>& used) {
+  uint64_t b = 0;
+  for (uint32_t s : used) {
+    BaseCol& bc = basecol(p.src, p.slots[s]);
+    for (uint32_t g = 0; g < p.src->segCount; g++) {
+      if (!p.mode[g]) continue;
+      const SegMeta& m = bc.segs[g].m;
+      b += (uint64_t)m.rec_count * (m.comp_type == 1 ? 8 : m.bits / 8);
+    }
+  }
+  return b;
+}
+
+}  // namespace alk

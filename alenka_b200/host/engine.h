@@ -95,6 +95,17 @@ struct Var {
   bool has(const std::string& c) const;
 };
 
+// A scan of a base table (or of a filtered view of one): zone-map verdict per segment,
+// the compiled predicate, and the column slots the device code reads.
+struct ScanPlan {
+  Var* src = nullptr;
+  std::vector<std::string> slots;
+  alk_program pred{};
+  bool has_pred = false;
+  std::vector<uint8_t> mode;  // 0 skip, 1 all rows, 2 evaluate
+  uint32_t slot(const std::string& c);
+};
+
 // Materialized rows of a variable for a set of fields.
 struct Rows {
   uint64_t n = 0;
@@ -118,6 +129,11 @@ class Engine {
   Var* var(const std::string& n);
   void ensure_base_col(Var* base, const std::string& col, bool device);
   Rows materialize(Var* v, const std::vector<std::string>& fields, bool want_seg = false);
+  ScanPlan plan_scan(Var* v);
+  // Device descriptors [slots][segments] of a scan (uploads columns on demand).
+  std::vector<alk_colseg> colsegs(const ScanPlan& p);
+  // Bytes one scan reads at the resident widths (segments not skipped).
+  uint64_t scan_bytes(const ScanPlan& p, const std::vector<uint32_t>& used_slots);
   size_t cycle_count(Var* v);
   uint64_t free_mem() const { return kFreeMem; }
   // getFreeMem() (cm.cu:3184) pinned to a B200's 180 GB so that segmentation is deterministic.
@@ -151,6 +167,7 @@ class Engine {
   void emit_order(Statement& st);
   void emit_store(Statement& st);
   bool try_fused(std::vector<Statement>& sts, size_t& i);
+  void run_fused(Statement& J, Statement& F, Statement& O, Statement& S);
 
   friend struct Planner;
 };

@@ -965,4 +965,474 @@ int Engine::execute(const std::string& script) {
   return rc;
 }
 
+// ------------------------------------------------------------------ fused pipelines
+namespace {
+struct FusedFallback : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+[[noreturn]] void fallback(const std::string& why) { throw FusedFallback(why); }
+
+// One emit_multijoin step resolved like operators.cu:961-1033.
+struct StepInfo {
+  std::string left, right, lkey, rkey;
+  std::vector<std::string> out;  // result columns (op_sel_s order, unique)
+};
+
+// Remap column operands of a compiled program from Compiler slot order to the stage's
+// operand numbering (scan slot, or 32 + payload column).
+void remap(alk_program& p, const std::vector<std::string>& names, const std::map<std::string, uint32_t>& where) {
+  for (uint32_t i = 0; i < p.n_instr; i++) {
+    alk_instr& in = p.ins[i];
+    if (in.ka == ALK_K_COL) in.a = (uint16_t)where.at(names.at(in.a));
+    if (in.kb == ALK_K_COL) in.b = (uint16_t)where.at(names.at(in.b));
+  }
+}
+
+struct HtGuard {
+  alk_ht* h = nullptr;
+  cudaStream_t s = nullptr;
+  ~HtGuard() { alk_ht_free(h, (alk_stream)s); }
+};
+}  // namespace
+
+// Recognises  J := SELECT .. FROM fact JOIN d1 ON .. [JOIN d2 ON ..];
+//             F := SELECT .. FROM J GROUP BY ..;  R := ORDER F BY ..;  STORE R .. LIMIT n;
+// where J, F and R feed nothing else, and runs it as build stages over the dimension
+// side(s), one probe-aggregate pass over the fact table and a top-k selection. The
+// result is the reference's: groups equal build rows (the last build key is a group key
+// and unique), F's row order is its group-key order (single-segment source), and ORDER
+// is stable. Any precondition that fails at run time (duplicate build keys, too many
+// ties at the LIMIT boundary) falls back to the operator-at-a-time plan.
+bool Engine::try_fused(std::vector<Statement>& sts, size_t& i) {
+  if (i + 3 >= sts.size()) return false;
+  Statement& J = sts[i];
+  Statement& F = sts[i + 1];
+  Statement& O = sts[i + 2];
+  Statement& S = sts[i + 3];
+  if (J.kind != StmtKind::Join || F.kind != StmtKind::Select || O.kind != StmtKind::Order ||
+      S.kind != StmtKind::Store)
+    return false;
+  if (F.f != J.s || O.f != F.s || S.s != O.s || F.grp_cnt == 0) return false;
+  if (S.op_nums.empty() || S.op_nums[0] <= 0 || S.op_nums[0] > 4096) return false;
+  for (size_t k = 0; k < sts.size(); k++) {
+    if (k >= i && k <= i + 3) continue;
+    for (const std::string* n : {&J.s, &F.s, &O.s}) {
+      if (sts[k].f == *n || sts[k].s == *n) return false;
+      for (auto& j : sts[k].op_join)
+        if (j == *n) return false;
+    }
+  }
+  if (J.join_tab_cnt < 1 || J.join_tab_cnt > 2) return false;
+  for (char t : J.join_type)
+    if (t != 'I') return false;
+  for (auto& kv : J.join_and_cnt)
+    if (kv.second) return false;
+  try {
+    run_fused(J, F, O, S);
+  } catch (const FusedFallback& e) {
+    return false;
+  }
+  stats_.plan = 1;
+  i += 3;
+  return true;
+}
+
+void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
+  cudaStream_t s = stream_;
+  // ---- resolve the join chain (emit_join, operators.cu:832-859)
+  std::vector<std::string> op_sel, op_alias;
+  for (unsigned k = 0; k < J.sel_count; k++) {
+    op_sel.push_back(J.op_value.at(2 * k));
+    op_alias.push_back(J.op_value.at(2 * k + 1));
+  }
+  std::vector<std::string> op_g(J.op_value.begin() + 2 * J.sel_count, J.op_value.end());
+  auto step_cols = [&](unsigned tab, Var* left, const std::vector<std::string>& right_cols, StepInfo& si) {
+    std::vector<std::string> op_sel_s = op_sel;
+    size_t gi = 0;
+    for (unsigned z = 0; z < J.join_tab_cnt - tab; z++)
+      for (unsigned j = 0; j < 2; j++) op_sel_s.push_back(op_g.at(gi++));
+    std::string f1 = op_g.at(gi), f2 = op_g.at(gi + 1);
+    auto rhas = [&](const std::string& c) {
+      return std::find(right_cols.begin(), right_cols.end(), c) != right_cols.end();
+    };
+    for (auto& n : op_sel_s)
+      if (std::find(si.out.begin(), si.out.end(), n) == si.out.end() && (rhas(n) || left->has(n))) si.out.push_back(n);
+    if (left->has(f1) && rhas(f2)) {
+      si.lkey = f1;
+      si.rkey = f2;
+    } else if (rhas(f1) && left->has(f2)) {
+      si.rkey = f1;
+      si.lkey = f2;
+    } else {
+      fallback("join columns");
+    }
+  };
+  Var* fact = var(J.f);
+  Var* d1 = nullptr;
+  Var* d2 = nullptr;  // d2 joins d1 (innermost step) when there are two joins
+  StepInfo st1, st2;
+  if (J.join_tab_cnt == 2) {
+    d2 = var(J.op_join.at(0));
+    d1 = var(J.op_join.at(1));
+    step_cols(1, d1, d2->columnNames, st1);
+    step_cols(2, fact, st1.out, st2);
+  } else {
+    d1 = var(J.op_join.at(0));
+    step_cols(1, fact, d1->columnNames, st2);
+  }
+  for (Var* v : {fact, d1, d2})
+    if (v && v->kind == Var::Mat) fallback("materialized join input");
+  // source table of every result column of J (left side wins, operators.cu:1416)
+  auto origin = [&](const std::string& c) -> Var* {
+    if (fact->has(c)) return fact;
+    if (d1->has(c)) return d1;
+    if (d2 && d2->has(c)) return d2;
+    fallback("column " + c);
+  };
+  // ---- F over J: compile its select list against J's (aliased) columns
+  Var jv;
+  jv.kind = Var::Mat;
+  std::map<std::string, std::string> src_of;  // J alias -> source column
+  for (auto& n : st2.out) {
+    auto it = std::find(op_sel.begin(), op_sel.end(), n);
+    std::string alias = it == op_sel.end() ? n : op_alias[it - op_sel.begin()];
+    jv.columnNames.push_back(alias);
+    jv.meta[alias] = origin(n)->meta[n];
+    src_of[alias] = n;
+  }
+  std::vector<std::string> group_cols(F.op_value.end() - F.grp_cnt, F.op_value.end());
+  for (auto& g : group_cols)
+    if (!jv.has(g) || origin(src_of[g]) == fact) fallback("group key outside the build side");
+  const std::string& build_key = st2.rkey;  // unique key of the last build stage
+  bool key_grouped = false;
+  for (auto& g : group_cols)
+    if (src_of[g] == build_key) key_grouped = true;
+  if (!key_grouped) fallback("build key is not a group key");
+  std::vector<OutSpec> outs;
+  std::vector<AggSpec> aggs;
+  bool one_line = false;
+  try {
+    compile_select(F, &jv, true, outs, aggs, one_line);
+  } catch (const EngineError&) {
+    fallback("select list");
+  }
+  if (aggs.empty() || aggs.size() > 7) fallback("aggregate count");
+  // ---- payload columns carried by the last build stage: every build-side column F uses
+  std::vector<std::string> payload;  // source column names
+  auto need_payload = [&](const std::string& src) {
+    if (origin(src) == fact) return;
+    if (std::find(payload.begin(), payload.end(), src) == payload.end()) payload.push_back(src);
+  };
+  for (auto& g : group_cols) need_payload(src_of[g]);
+  for (auto& o : outs) {
+    if (o.col_type == 1) {
+      if (origin(src_of.at(o.field)) == fact) fallback("fact column outside an aggregate");
+      need_payload(src_of.at(o.field));
+    }
+    if (o.col_type == 2 && has_col(o.vec)) fallback("row-level expression in a grouped select");
+  }
+  std::set<std::string> fact_cols;
+  for (auto& ag : aggs) {
+    if (!ag.input) continue;
+    std::vector<AstP> stack = {ag.input};
+    while (!stack.empty()) {
+      AstP a = stack.back();
+      stack.pop_back();
+      if (!a) continue;
+      if (a->k == Ast::Col) {
+        const std::string& src = src_of.at(a->col);
+        if (origin(src) == fact) fact_cols.insert(src);
+        else need_payload(src);
+      }
+      stack.push_back(a->l);
+      stack.push_back(a->r);
+    }
+  }
+  if (payload.size() > 8) fallback("payload width");
+  // ---- build stages
+  HtGuard ht1, ht2;
+  alk_ht* last = nullptr;
+  std::map<std::string, uint32_t> last_pay;  // payload column index in the last table
+  if (J.join_tab_cnt == 2) {
+    // stage 1: d2 (innermost right) keyed on st1.rkey, carrying the d2 columns needed later
+    ScanPlan p1 = plan_scan(d2);
+    uint32_t k1 = p1.slot(st1.rkey);
+    std::vector<std::string> pay1;
+    for (auto& c : payload)
+      if (origin(c) == d2) pay1.push_back(c);
+    if (d2->has(build_key) && !d1->has(build_key)) pay1.push_back(build_key);
+    std::vector<int32_t> src1;
+    for (auto& c : pay1) src1.push_back((int32_t)p1.slot(c));
+    auto cs1 = colsegs(p1);
+    uint64_t max1 = 0;
+    for (uint32_t g = 0; g < p1.src->segCount; g++)
+      if (p1.mode[g]) max1 += cs1[g].rows;
+    check(alk_ht_create(max1, (uint32_t)pay1.size(), &ht1.h, (alk_stream)s), "hash table");
+    ht1.s = s;
+    check(alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
+                             p1.has_pred ? &p1.pred : nullptr, nullptr, -1, ht1.h, (int32_t)k1, src1.data(),
+                             nullptr, (alk_stream)s),
+          "build stage");
+    int fl = 0;
+    check(alk_ht_info(ht1.h, nullptr, &fl, (alk_stream)s), "hash table");
+    if (fl) fallback("duplicate or overflowing build keys");
+    // stage 2: d1 probes stage 1 on st1.lkey and is keyed on the final build key
+    ScanPlan p2 = plan_scan(d1);
+    uint32_t probe2 = p2.slot(st1.lkey);
+    auto slot_or_pay = [&](const std::string& c) -> int32_t {
+      if (d1->has(c)) return (int32_t)p2.slot(c);
+      auto it = std::find(pay1.begin(), pay1.end(), c);
+      if (it == pay1.end()) fallback("payload routing");
+      return 32 + (int32_t)(it - pay1.begin());
+    };
+    int32_t key2 = slot_or_pay(build_key);
+    if (key2 >= 32) fallback("build key from the inner table");
+    std::vector<int32_t> src2;
+    for (auto& c : payload) {
+      src2.push_back(slot_or_pay(c));
+      last_pay[c] = (uint32_t)src2.size() - 1;
+    }
+    auto cs2 = colsegs(p2);
+    uint64_t max2 = 0;
+    for (uint32_t g = 0; g < p2.src->segCount; g++)
+      if (p2.mode[g]) max2 += cs2[g].rows;
+    check(alk_ht_create(max2, (uint32_t)payload.size(), &ht2.h, (alk_stream)s), "hash table");
+    ht2.s = s;
+    check(alk_pipeline_build(cs2.data(), (uint32_t)p2.slots.size(), p2.src->segCount, p2.mode.data(),
+                             p2.has_pred ? &p2.pred : nullptr, ht1.h, (int32_t)probe2, ht2.h, key2, src2.data(),
+                             nullptr, (alk_stream)s),
+          "build stage");
+    check(alk_ht_info(ht2.h, nullptr, &fl, (alk_stream)s), "hash table");
+    if (fl) fallback("duplicate or overflowing build keys");
+    last = ht2.h;
+  } else {
+    ScanPlan p1 = plan_scan(d1);
+    uint32_t k1 = p1.slot(build_key);
+    std::vector<int32_t> src1;
+    for (auto& c : payload) {
+      src1.push_back((int32_t)p1.slot(c));
+      last_pay[c] = (uint32_t)src1.size() - 1;
+    }
+    auto cs1 = colsegs(p1);
+    uint64_t max1 = 0;
+    for (uint32_t g = 0; g < p1.src->segCount; g++)
+      if (p1.mode[g]) max1 += cs1[g].rows;
+    check(alk_ht_create(max1, (uint32_t)payload.size(), &ht1.h, (alk_stream)s), "hash table");
+    ht1.s = s;
+    check(alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
+                             p1.has_pred ? &p1.pred : nullptr, nullptr, -1, ht1.h, (int32_t)k1, src1.data(),
+                             nullptr, (alk_stream)s),
+          "build stage");
+    int fl = 0;
+    check(alk_ht_info(ht1.h, nullptr, &fl, (alk_stream)s), "hash table");
+    if (fl) fallback("duplicate or overflowing build keys");
+    last = ht1.h;
+  }
+  uint64_t nslots = 0;
+  check(alk_ht_info(last, &nslots, nullptr, (alk_stream)s), "hash table");
+  // ---- probe-aggregate over the fact table
+  ScanPlan pf = plan_scan(fact);
+  uint32_t probe_f = pf.slot(st2.lkey);
+  std::map<std::string, uint32_t> where;  // J alias -> operand index
+  for (auto& alias : jv.columnNames) {
+    const std::string& src = src_of[alias];
+    if (fact_cols.count(src)) where[alias] = pf.slot(src);
+    else if (last_pay.count(src)) where[alias] = 32 + last_pay[src];
+  }
+  std::vector<alk_program> progs(aggs.size());
+  std::vector<uint8_t> kinds(aggs.size());
+  for (size_t g = 0; g < aggs.size(); g++) {
+    kinds[g] = aggs[g].kind;
+    std::memset(&progs[g], 0, sizeof(alk_program));
+    if (aggs[g].kind == ALK_AGG_COUNT) continue;
+    Compiler c;
+    progs[g] = c.finish(aggs[g].input);
+    remap(progs[g], c.slots, where);
+  }
+  auto csf = colsegs(pf);
+  const uint64_t stride = std::max<uint64_t>(nslots, 1);
+  auto acc = mkbuf(stride * 8 * aggs.size(), s);
+  auto cnt = mkbuf(stride * 8, s);
+  for (size_t g = 0; g < aggs.size(); g++) {
+    int64_t init = aggs[g].kind == ALK_AGG_MIN ? INT64_MAX : (aggs[g].kind == ALK_AGG_MAX ? INT64_MIN : 0);
+    check(alk_fill_i64(acc->as<int64_t>() + g * stride, stride, init, (alk_stream)s), "init");
+  }
+  ck(cudaMemsetAsync(cnt->as<void>(), 0, stride * 8, s), "init");
+  alk_event_timer tm{timing_ ? 1 : 0, ev0_, ev1_, 0.0, 0};
+  // the probe-aggregate kernel accumulates into slot-indexed arrays sized for every slot
+  if (nslots) {
+    check(alk_pipeline_probe_agg(csf.data(), (uint32_t)pf.slots.size(), pf.src->segCount, pf.mode.data(),
+                                 pf.has_pred ? &pf.pred : nullptr, last, (int32_t)probe_f, progs.data(), kinds.data(),
+                                 (uint32_t)aggs.size(), acc->as<int64_t>(), stride, cnt->as<uint64_t>(), nullptr,
+                                 (alk_stream)s, &tm),
+          "probe-aggregate");
+  }
+  if (timing_) {
+    stats_.hot_kernel_ms += tm.ms;
+    stats_.hot_kernel_launches += tm.launches;
+    std::vector<uint32_t> all(pf.slots.size());
+    std::iota(all.begin(), all.end(), 0);
+    stats_.hot_kernel_bytes += scan_bytes(pf, all);
+  }
+  // ---- F's columns over slots
+  auto slot_col = [&](const std::string& alias) -> const int64_t* {
+    return alk_ht_payload(last, last_pay.at(src_of.at(alias)));
+  };
+  std::vector<DevBufP> keep;
+  std::vector<const int64_t*> fcol(outs.size());
+  std::vector<ColMeta> fmeta(outs.size());
+  std::vector<int> fgt(outs.size());
+  int countc = -1;
+  for (size_t c = 0; c < outs.size(); c++)
+    if (outs[c].grp_type == 0 && countc < 0) countc = (int)c;
+  for (size_t c = 0; c < outs.size(); c++) {
+    const OutSpec& o = outs[c];
+    fmeta[c].dz = o.prec;
+    fgt[c] = o.grp_type;
+    if (o.col_type == 1) {
+      fcol[c] = slot_col(o.field);
+      fmeta[c].string_map = jv.meta[o.field].string_map;
+    } else if (o.col_type == 2 && o.vec->k == Ast::Agg) {
+      fcol[c] = acc->as<int64_t>() + (size_t)o.vec->agg * stride;
+    } else if (o.col_type == 2) {
+      Compiler cc;
+      alk_program prog = cc.finish(o.vec);
+      std::vector<const int64_t*> in;
+      for (auto& sname : cc.slots) in.push_back(acc->as<int64_t>() + std::stoi(sname.substr(4)) * stride);
+      auto d = mkbuf(stride * 8, s);
+      check(alk_eval(in.data(), (uint32_t)in.size(), nslots, &prog, d->as<int64_t>(), (alk_stream)s), "eval");
+      keep.push_back(d);
+      fcol[c] = d->as<int64_t>();
+    } else {
+      auto d = mkbuf(stride * 8, s);
+      check(alk_fill_i64(d->as<int64_t>(), stride, (int64_t)(int)o.num, (alk_stream)s), "const");
+      keep.push_back(d);
+      fcol[c] = d->as<int64_t>();
+    }
+  }
+  for (size_t c = 0; c < outs.size(); c++) {  // AVG finalisation (merge.cu:446-458)
+    if (fgt[c] != 1) continue;
+    if (countc < 0) fallback("AVG without COUNT");
+    AstP e = fmeta[c].dz <= 2 ? mk_bin(ALK_OP_DIV, mk_bin(ALK_OP_MUL, mk_col("s"), mk_const(100)), mk_col("c"))
+                              : mk_bin(ALK_OP_DIV, mk_col("s"), mk_col("c"));
+    Compiler cc;
+    alk_program prog = cc.finish(e);
+    std::vector<const int64_t*> in;
+    for (auto& sname : cc.slots) in.push_back(sname == "s" ? fcol[c] : fcol[countc]);
+    auto d = mkbuf(stride * 8, s);
+    check(alk_eval(in.data(), (uint32_t)in.size(), nslots, &prog, d->as<int64_t>(), (alk_stream)s), "avg");
+    keep.push_back(d);
+    fcol[c] = d->as<int64_t>();
+    if (fmeta[c].dz <= 2) fmeta[c].dz += 2;
+  }
+  // ---- ORDER keys (operators.cu:1641-1798) and the top-k superset
+  std::vector<int> okey;
+  std::vector<bool> odesc;
+  {
+    size_t iv = 0;
+    for (auto& t : O.op_type) {
+      std::string name = t == "NAME" ? O.op_value.at(iv) : t;
+      bool desc = t != "NAME" && O.op_value.at(iv) == "DESC";
+      iv++;
+      int idx = -1;
+      for (size_t c = 0; c < outs.size(); c++)
+        if (outs[c].name == name) idx = (int)c;
+      if (idx < 0) throw EngineError(ALK_ERR_ARG, "Couldn't find name " + name);
+      if (!fmeta[idx].string_map.empty()) fallback("ORDER BY on a char column");
+      okey.push_back(idx);
+      odesc.push_back(desc);
+    }
+  }
+  if (okey.empty()) fallback("ORDER without keys");
+  const int64_t* rank = fcol[okey[0]];
+  DevBufP rank_buf;
+  if (!odesc[0]) {  // ascending: rank by -1 - v (order reversing, no overflow)
+    AstP e = mk_bin(ALK_OP_SUB, mk_const(-1), mk_col("v"));
+    Compiler cc;
+    alk_program prog = cc.finish(e);
+    const int64_t* in[1] = {rank};
+    rank_buf = mkbuf(stride * 8, s);
+    check(alk_eval(in, 1, nslots, &prog, rank_buf->as<int64_t>(), (alk_stream)s), "rank");
+    rank = rank_buf->as<int64_t>();
+  }
+  const uint32_t limit = (uint32_t)S.op_nums[0];
+  uint64_t ncand = 0;
+  const uint64_t cand_cap = 1 << 16;
+  auto cand = mkbuf(cand_cap * 4, s);
+  int rc = alk_topk_candidates(rank, cnt->as<uint64_t>(), nslots, limit, cand->as<uint32_t>(), cand_cap, &ncand,
+                               (alk_stream)s);
+  if (rc == ALK_ERR_OVERFLOW) fallback("too many ties at the LIMIT boundary");
+  check(rc, "top-k");
+  // gather candidate rows: F columns and group keys
+  std::vector<const int64_t*> gcol;
+  for (auto& g : group_cols) gcol.push_back(slot_col(g));
+  std::vector<std::vector<int64_t>> hf(outs.size(), std::vector<int64_t>(ncand)),
+      hg(gcol.size(), std::vector<int64_t>(ncand));
+  if (ncand) {
+    auto tmp = mkbuf(ncand * 8 * (outs.size() + gcol.size()), s);
+    for (size_t c = 0; c < outs.size() + gcol.size(); c++) {
+      const int64_t* src = c < outs.size() ? fcol[c] : gcol[c - outs.size()];
+      check(alk_gather(src, cand->as<uint32_t>(), ncand, tmp->as<int64_t>() + c * ncand, (alk_stream)s), "gather");
+    }
+    for (size_t c = 0; c < outs.size() + gcol.size(); c++) {
+      auto& dst = c < outs.size() ? hf[c] : hg[c - outs.size()];
+      ck(cudaMemcpyAsync(dst.data(), tmp->as<int64_t>() + c * ncand, ncand * 8, cudaMemcpyDeviceToHost, s), "d2h");
+    }
+    ck(cudaStreamSynchronize(s), "sync");
+    stats_.d2h_bytes += ncand * 8 * (outs.size() + gcol.size());
+  }
+  std::vector<uint32_t> ord(ncand);
+  std::iota(ord.begin(), ord.end(), 0);
+  std::sort(ord.begin(), ord.end(), [&](uint32_t x, uint32_t y) {
+    for (size_t k = 0; k < okey.size(); k++) {
+      int64_t a = hf[okey[k]][x], b = hf[okey[k]][y];
+      if (a != b) return odesc[k] ? a > b : a < b;
+    }
+    for (auto& g : hg)  // F's own row order: group keys ascending
+      if (g[x] != g[y]) return g[x] < g[y];
+    return false;
+  });
+  size_t rows = std::min<size_t>(ncand, limit);
+  // ---- STORE (cm.cu:1479-1560)
+  std::string path = S.f;
+  if (path.empty() || path[0] != '/') path = dir_ + "/" + path;
+  FILE* fp = std::fopen(path.c_str(), "w");
+  if (!fp) throw EngineError(ALK_ERR_IO, "Could not open file " + path);
+  std::vector<const std::vector<std::string>*> dicts(outs.size(), nullptr);
+  for (size_t c = 0; c < outs.size(); c++) {
+    const std::string& sm = fmeta[c].string_map;
+    if (sm.empty()) continue;
+    auto dot = sm.find('.');
+    Var* b = base_table(sm.substr(0, dot));
+    if (!b) throw EngineError(ALK_ERR_IO, "missing dictionary " + sm);
+    BaseCol& bc = basecol(b, sm.substr(dot + 1));
+    load_dict(b, sm.substr(dot + 1), bc);
+    dicts[c] = &bc.dict;
+  }
+  std::string line;
+  for (size_t r = 0; r < rows; r++) {
+    line.clear();
+    for (size_t c = 0; c < outs.size(); c++) {
+      int64_t v = hf[c][ord[r]];
+      if (!dicts[c]) {
+        if (fmeta[c].dz) {
+          std::string t = std::to_string(v);
+          while (t.size() <= fmeta[c].dz) t = '0' + t;
+          t.insert(t.size() - fmeta[c].dz, ".");
+          line += t;
+        } else {
+          line += std::to_string(v);
+        }
+      } else {
+        std::string t = (v >= 0 && (size_t)v < dicts[c]->size()) ? (*dicts[c])[v] : std::string();
+        line += t.substr(0, std::strlen(t.c_str()));
+      }
+      line += S.sep;
+    }
+    if (r + 1 != rows) line += "\n";
+    std::fputs(line.c_str(), fp);
+  }
+  std::fclose(fp);
+}
+
 }  // namespace alk

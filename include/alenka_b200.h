@@ -97,6 +97,12 @@ int alk_decode_segment(const void* d_payload, uint32_t comp_type, uint32_t bits,
                        uint32_t fit_count, int64_t lower, int64_t start_val, uint32_t rows,
                        int64_t* d_out, alk_stream stream);
 
+/* Segment writer (host): one segment file image for n int64 values, FOR or (delta != 0
+ * and sorted values) FOR-delta, laid out as pfor_compress / pfor_delta_compress write it
+ * (compress.cu:271-527). ALK_ERR_OVERFLOW with *out_len set when cap is too small. */
+int alk_encode_segment(const int64_t* values, uint32_t n, int delta, uint8_t* out, size_t cap,
+                       size_t* out_len);
+
 /* MurmurHash64A of n tuples of k int64 keys (row-major tuples built from k column
  * pointers), seed as given (hash_seed 100, bison.y:304). Replaces the host loop of
  * add() (merge.cu:118-141) and MurmurHash64A (MurmurHash2_64.cu:201-242). */
@@ -187,6 +193,51 @@ int alk_join_build(const int64_t* d_keys, uint64_t n, alk_join_table** out, alk_
 int alk_join_probe(const alk_join_table* t, const int64_t* d_keys, uint64_t n, uint32_t* d_left,
                    uint32_t* d_right, uint64_t cap, uint64_t* h_pairs, alk_stream stream);
 void alk_join_free(alk_join_table* t, alk_stream stream);
+
+/* ------------------------------------------------- fused pipeline stages
+ * The filter -> join -> join -> group-by chain of emit_filter / emit_multijoin /
+ * emit_select (operators.cu:797-1582, 1801-2084) as device stages over resident
+ * segments: build stages insert a unique join key with payload columns into a
+ * MurmurHash64A linear-probing table (optionally probing the previous stage's table),
+ * and the probe-aggregate stage accumulates exact int64 aggregates per build row. */
+typedef struct alk_ht alk_ht;
+/* max_keys bounds the inserted keys; npay payload columns (<= 8) per key. */
+int alk_ht_create(uint64_t max_keys, uint32_t npay, alk_ht** out, alk_stream stream);
+void alk_ht_free(alk_ht* h, alk_stream stream);
+/* Inserted keys and flags (1 duplicate key, 2 capacity exceeded, 4 wait expired). */
+int alk_ht_info(const alk_ht* h, uint64_t* nslots, int* flags, alk_stream stream);
+/* Device address of payload column p (slot-indexed). */
+const int64_t* alk_ht_payload(const alk_ht* h, uint32_t p);
+/* Optional CUDA-event timing of the probe-aggregate kernel (cudaEvent_t handles). */
+typedef struct alk_event_timer {
+  int on;
+  void* ev0;
+  void* ev1;
+  double ms;
+  uint64_t launches;
+} alk_event_timer;
+/* Build stage. Program column operands name scan slots (< 32) or, when probing,
+ * payload columns of the probed table (32 + p). pay_src[p] gives each payload column's
+ * source the same way. h_rows_in receives the rows scanned. Synchronizes. */
+int alk_pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                       const alk_program* pred, const alk_ht* probe, int32_t probe_slot, alk_ht* build,
+                       int32_t build_slot, const int32_t* pay_src, uint64_t* h_rows_in, alk_stream stream);
+/* Probe-aggregate stage: for every surviving row whose probe key hits, aggregate
+ * agg_progs[g] (ALK_AGG_SUM / MIN / MAX, or COUNT) into d_acc[g * acc_stride + slot] and
+ * count rows into d_cnt[slot]. Accumulators must be initialised by the caller. */
+int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                           const alk_program* pred, const alk_ht* probe, int32_t probe_slot,
+                           const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg, int64_t* d_acc,
+                           uint64_t acc_stride, uint64_t* d_cnt, uint64_t* h_rows_in, alk_stream stream,
+                           alk_event_timer* timer);
+int alk_fill_i64(int64_t* d, uint64_t n, int64_t v, alk_stream stream);
+/* Top-k candidates for ORDER BY ... LIMIT k (emit_order + Store LIMIT, operators.cu:1641,
+ * cm.cu:1493): every live slot whose ranking value is >= the k-th largest ranking value
+ * (ties included); the caller orders the few candidates with the full key list. */
+int alk_topk_candidates(const int64_t* d_rank, const uint64_t* d_live, uint64_t n, uint32_t k, uint32_t* d_out,
+                        uint64_t cap, uint64_t* h_count, alk_stream stream);
+/* Indices of live (non-zero) slots, unordered. */
+int alk_live_compact(const uint64_t* d_live, uint64_t n, uint32_t* d_out, uint64_t* h_count, alk_stream stream);
 
 /* Front end: renders the statements and postfix queues the parser produces for a script
  * (the argument queues of the reference's grammar actions, bison.y:127-287). */
