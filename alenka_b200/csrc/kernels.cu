@@ -3,6 +3,7 @@
 // group-by, stable LSD radix sort, gather, tuple hashing and the hash join.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "device.cuh"
@@ -641,6 +642,80 @@ int alk_decode_segment(const void* d_payload, uint32_t comp_type, uint32_t bits,
   uint64_t* incls = sc.get<uint64_t>(ntiles, &e);
   CK(e);
   int* err = (int*)(flags + ntiles + 1);
+  CK(cudaMemsetAsync(flags, 0, (ntiles + 2) * sizeof(uint32_t), s));
+  DeltaArgs a{(const unsigned long long*)d_payload, bits, fit_count, lower, start_val, rows, ntiles,
+              flags, aggs, incls, flags + ntiles, err, d_out};
+  int grid = std::min<int>(ntiles, sm_count() * 4);
+  k_decode_delta<<<grid, kT, 0, s>>>(a);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  int h_err = 0;
+  CK(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return h_err;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free decode
+// Look-back state of alk_decode_segment_noalloc lives in this file-scope array instead of
+// memory allocated per call: tile flags plus the tile counter and error word, then the
+// per-tile aggregates and inclusive prefixes. Every device that loads the library holds
+// it until the process exits.
+namespace {
+constexpr uint32_t kNoAllocMaxTiles = 32768;  // 32768 tiles x 2048 rows = 67,108,864 rows
+constexpr size_t kNoAllocFlagBytes = ((kNoAllocMaxTiles + 2) * sizeof(uint32_t) + 255) / 256 * 256;
+constexpr size_t kNoAllocScratchBytes = kNoAllocFlagBytes + 2 * (size_t)kNoAllocMaxTiles * sizeof(uint64_t);
+static __device__ __align__(256) unsigned char g_decode_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+void* g_scratch_addr[kMaxDevices] = {};
+
+// Device address of g_decode_scratch on the current device, looked up once per device
+// (host code cannot use the array's name as a device address).
+int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return alk::cuda_fail(e);
+  if (dev < 0 || dev >= kMaxDevices) return ALK_ERR_ARG;
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_decode_scratch);
+    if (e != cudaSuccess || !p) return alk::cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol);
+    g_scratch_addr[dev] = p;
+  }
+  *out = (unsigned char*)g_scratch_addr[dev];
+  return ALK_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int alk_decode_segment_noalloc(const void* d_payload, uint32_t comp_type, uint32_t bits, uint32_t fit_count,
+                               int64_t lower, int64_t start_val, uint32_t rows, int64_t* d_out, alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (rows == 0) return ALK_OK;
+  if (!d_payload || !d_out) return ALK_ERR_ARG;
+  if (comp_type == 0) {  // FOR widening needs no scratch
+    if (bits != 8 && bits != 16 && bits != 32 && bits != 64) return ALK_ERR_ARG;
+    k_decode_for<<<grid_for(rows), kT, 0, s>>>(d_payload, bits, lower, rows, d_out);
+    alk::g_kernel_launches++;
+    CK(cudaGetLastError());
+    return ALK_OK;
+  }
+  if (comp_type != 1 || bits == 0 || bits > 64 || fit_count != 64 / bits) return ALK_ERR_ARG;
+  const uint32_t ntiles = (rows + kTile - 1) / kTile;
+  if (ntiles > kNoAllocMaxTiles) return ALK_ERR_TOO_LARGE;
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  uint32_t* flags = (uint32_t*)base;
+  uint64_t* aggs = (uint64_t*)(base + kNoAllocFlagBytes);
+  uint64_t* incls = aggs + kNoAllocMaxTiles;
+  int* err = (int*)(flags + ntiles + 1);
+  // tile flags, the tile counter and the error word must start at zero
   CK(cudaMemsetAsync(flags, 0, (ntiles + 2) * sizeof(uint32_t), s));
   DeltaArgs a{(const unsigned long long*)d_payload, bits, fit_count, lower, start_val, rows, ntiles,
               flags, aggs, incls, flags + ntiles, err, d_out};

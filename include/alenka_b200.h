@@ -33,6 +33,7 @@ typedef struct CUstream_st* alk_stream; /* a cudaStream_t; NULL = legacy default
 #define ALK_ERR_IO 6          /* missing or malformed segment / catalog file */
 #define ALK_ERR_PARSE 7       /* script syntax error */
 #define ALK_ERR_NOMEM 8       /* device allocation failed */
+#define ALK_ERR_TOO_LARGE 9   /* input exceeds a fixed-size entry point's stated maximum */
 
 /* ------------------------------------------------- 1. embedding (alenka.h) */
 /* alenkaInit (alenka.h:30): reads the flags of execute_file (bison.y:306-331) from
@@ -96,6 +97,22 @@ typedef struct alk_colseg {
 int alk_decode_segment(const void* d_payload, uint32_t comp_type, uint32_t bits,
                        uint32_t fit_count, int64_t lower, int64_t start_val, uint32_t rows,
                        int64_t* d_out, alk_stream stream);
+
+/* Segment decode that allocates nothing. No counterpart in the reference: this entry point
+ * exists for callers that cannot call cudaMalloc, for example a host that has committed
+ * all device memory to its own pools (as the reference sizes its work to the free memory,
+ * cm.cu:3184, 3565) or a decode path that must never fail or stall on an allocation.
+ * Same arguments and results as alk_decode_segment. FOR segments need no scratch; a
+ * FOR-delta segment keeps its scan state in one fixed device array of the library
+ * (about 0.6 MB per device, held until the process exits), so at most 67,108,864 rows
+ * (32768 tiles of 2048 rows) per call: larger segments return ALK_ERR_TOO_LARGE without
+ * touching the device. The first call on each device looks up that array's device
+ * address (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * Every call on a device shares the array: calls that overlap on the GPU (concurrent
+ * streams, or threads sharing a device) race and must be serialized by the caller. */
+int alk_decode_segment_noalloc(const void* d_payload, uint32_t comp_type, uint32_t bits,
+                               uint32_t fit_count, int64_t lower, int64_t start_val, uint32_t rows,
+                               int64_t* d_out, alk_stream stream);
 
 /* Segment writer (host): one segment file image for n int64 values, FOR or (delta != 0
  * and sorted values) FOR-delta, laid out as pfor_compress / pfor_delta_compress write it
