@@ -32,71 +32,64 @@ int sms() {
   return n;
 }
 
+// Empty key marker: the byte pattern 0x80 repeated (a memset value). Tables whose key
+// range contains it are refused at creation.
+constexpr int64_t kEmptyKey = (int64_t)0x8080808080808080ULL;
+
 struct HtView {
-  uint64_t cap;  // power of two
-  uint32_t* state;
+  uint64_t cap;  // power of two; keys[p] == kEmptyKey marks a free position
   int64_t* key;
-  uint32_t* slot;
   int64_t* payload;  // [npay][slot_cap]
   uint64_t slot_cap;
   uint32_t npay;
   unsigned long long* nslots;
-  int* flags;  // [0] duplicate key, [1] slot overflow, [2] timeout
+  int* flags;  // [0] duplicate key, [1] slot overflow, [2] timeout, [3] key outside the bitmap range
+  // Exact membership bitmap over [kmin, kmin + nbits) of the inserted keys (null when the
+  // key range, known from the build column's zone maps, is too wide).
+  uint32_t* bits;
+  int64_t kmin;
+  uint64_t nbits;
 };
+
+__device__ __forceinline__ bool ht_member(const HtView& h, int64_t k) {
+  const uint64_t o = (uint64_t)k - (uint64_t)h.kmin;
+  if (o >= h.nbits) return false;
+  return (__ldg(h.bits + (o >> 5)) >> (o & 31)) & 1u;
+}
 
 __device__ __forceinline__ int64_t ht_probe(const HtView& h, int64_t k) {
   const uint64_t mask = h.cap - 1;
   uint64_t p = murmur_u64((uint64_t)k) & mask;
   for (uint64_t n = 0; n <= mask; n++) {
-    const uint32_t s = __ldg(h.state + p);
-    if (s == 0) return -1;
-    if (__ldg(h.key + p) == k) return (int64_t)__ldg(h.slot + p);
+    const int64_t v = __ldg(h.key + p);
+    if (v == kEmptyKey) return -1;
+    if (v == k) return (int64_t)p;  // payload and accumulators are indexed by position
     p = (p + 1) & mask;
   }
   return -1;
 }
 
-// Inserts a unique key; returns its payload slot or -1 (duplicate / overflow / timeout,
-// recorded in flags).
+// Inserts a unique key with one compare-and-swap on the key word itself; returns its
+// position, or -1 for a duplicate or a full table (recorded in flags).
 __device__ __forceinline__ int64_t ht_insert(const HtView& h, int64_t k) {
   const uint64_t mask = h.cap - 1;
   uint64_t p = murmur_u64((uint64_t)k) & mask;
-  uint32_t spins = 0;
-  for (uint64_t n = 0; n <= mask;) {
-    uint32_t s = *((volatile uint32_t*)h.state + p);
-    if (s == 0) {
-      if (atomicCAS(h.state + p, 0u, 1u) == 0u) {
-        unsigned long long sl = atomicAdd(h.nslots, 1ull);
-        if (sl >= h.slot_cap) {
-          atomicExch(h.flags + 1, 1);
-          h.key[p] = k;
-          h.slot[p] = 0;
-          __threadfence();
-          atomicExch(h.state + p, 2u);
-          return -1;
-        }
-        h.key[p] = k;
-        h.slot[p] = (uint32_t)sl;
-        __threadfence();
-        atomicExch(h.state + p, 2u);
-        return (int64_t)sl;
+  for (uint64_t n = 0; n <= mask; n++) {
+    const int64_t old =
+        (int64_t)atomicCAS((unsigned long long*)(h.key + p), (unsigned long long)kEmptyKey, (unsigned long long)k);
+    if (old == kEmptyKey) {
+      if (h.bits) {
+        const uint64_t o = (uint64_t)k - (uint64_t)h.kmin;
+        if (o < h.nbits) atomicOr(h.bits + (o >> 5), 1u << (o & 31));
+        else atomicExch(h.flags + 3, 1);
       }
-      continue;
+      return (int64_t)p;
     }
-    if (s == 1) {
-      if (++spins > kSpinLimit) {
-        atomicExch(h.flags + 2, 1);
-        return -1;
-      }
-      continue;
-    }
-    __threadfence();
-    if (__ldcg(h.key + p) == k) {
+    if (old == k) {
       atomicExch(h.flags, 1);  // duplicate build key: the fused plan does not apply
       return -1;
     }
     p = (p + 1) & mask;
-    n++;
   }
   atomicExch(h.flags + 1, 1);
   return -1;
@@ -141,7 +134,7 @@ __global__ void __launch_bounds__(kT) k_stage(StageArgs a) {
       s_res[p] = a.progs[p].result;
     }
   }
-  unsigned long long rows_seen = 0;
+  unsigned long long rows_seen = 0, inserted = 0;
   for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
     __syncthreads();
     const uint32_t seg = a.tile_seg[tile];
@@ -170,6 +163,7 @@ __global__ void __launch_bounds__(kT) k_stage(StageArgs a) {
       if (kBuild) {
         const int64_t sl = ht_insert(a.build, col((uint32_t)a.build_slot));
         if (sl < 0) continue;
+        inserted++;
         for (uint32_t p = 0; p < a.build.npay; p++)
           a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = col((uint32_t)a.pay_src[p]);
       } else {
@@ -190,8 +184,12 @@ __global__ void __launch_bounds__(kT) k_stage(StageArgs a) {
       }
     }
   }
-  for (int o = 16; o; o >>= 1) rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
+  for (int o = 16; o; o >>= 1) {
+    rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
+    inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
+  }
   if ((threadIdx.x & 31) == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
+  if (kBuild && (threadIdx.x & 31) == 0 && inserted) atomicAdd(a.build.nslots, inserted);
 }
 
 __global__ void __launch_bounds__(kT) k_fill_i64(int64_t* p, uint64_t n, int64_t v) {
@@ -262,6 +260,50 @@ __global__ void __launch_bounds__(kT) k_topk_local(const int64_t* rank, const un
     for (; written < k; written++) out[(uint64_t)blockIdx.x * k + written] = INT64_MIN;
 }
 
+// Top-k threshold in one pass for k <= 16: every thread keeps its 16 largest ranking
+// values (with multiplicity) in registers, then the block sorts the 4096 candidates in
+// shared memory and writes its k largest.
+constexpr int kTopK = 16;
+__global__ void __launch_bounds__(kT) k_topk_local16(const int64_t* rank, const unsigned long long* live, uint64_t n,
+                                                     uint32_t k, int64_t* out) {
+  __shared__ int64_t s_v[kT * kTopK];
+  int64_t t[kTopK];
+#pragma unroll
+  for (int i = 0; i < kTopK; i++) t[i] = INT64_MIN;
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
+    if (!live[i]) continue;
+    const int64_t v = rank[i];
+    if (v <= t[kTopK - 1]) continue;
+#pragma unroll
+    for (int q = kTopK - 1; q > 0; q--) {  // insert into the descending list, dropping the smallest
+      const int64_t up = t[q - 1];
+      t[q] = v > up ? up : (v > t[q] ? v : t[q]);
+    }
+    t[0] = v > t[0] ? v : t[0];
+  }
+#pragma unroll
+  for (int i = 0; i < kTopK; i++) s_v[threadIdx.x * kTopK + i] = t[i];
+  __syncthreads();
+  // bitonic sort of kT * kTopK values, descending
+  constexpr int N = kT * kTopK;
+  for (int size = 2; size <= N; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < N / 2; i += kT) {
+        const int lo = 2 * i - (i & (stride - 1));
+        const int hi = lo + stride;
+        const bool desc = (lo & size) == 0;
+        const int64_t a = s_v[lo], b = s_v[hi];
+        if (desc ? a < b : a > b) {
+          s_v[lo] = b;
+          s_v[hi] = a;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x < k) out[(uint64_t)blockIdx.x * k + threadIdx.x] = s_v[threadIdx.x];
+}
+
 // Collect live slots whose ranking value is at least the threshold.
 __global__ void __launch_bounds__(kT) k_topk_collect(const int64_t* rank, const unsigned long long* live, uint64_t n,
                                                      int64_t thr, uint32_t* out, uint64_t cap,
@@ -281,9 +323,526 @@ __global__ void __launch_bounds__(kT) k_live_compact(const unsigned long long* l
   }
 }
 
+// ---------------------------------------------------------------- conjunctive fast path
+// Predicates of the shape AND_i (column_i * mul_i OP const_i), which is what the host
+// compiles for the reference's "column OP constant" filters (filter.cu:473-590), run as
+// straight-line tests over values loaded for the whole item batch at once; probes test
+// the table's exact key bitmap before touching the hash table.
+constexpr int kMaxConj = 4;
+struct Conj {
+  int64_t mul, k;
+  uint32_t slot, op;
+};
+struct FastArgs {
+  StageArgs a;
+  Conj conj[kMaxConj];
+  uint32_t nconj;
+  int need_slot;  // the stage reads the probed table's payload (else membership suffices)
+};
+
+__device__ __forceinline__ bool cmp_apply(uint32_t op, int64_t a, int64_t b) {
+  switch (op) {
+    case ALK_OP_LT: return a < b;
+    case ALK_OP_GT: return a > b;
+    case ALK_OP_LE: return a <= b;
+    case ALK_OP_GE: return a >= b;
+    case ALK_OP_EQ: return a == b;
+    default: return a != b;
+  }
+}
+
+// Values of one column for the thread's items (rows base + k * kT), live items only.
+__device__ __forceinline__ void load_batch(const alk_colseg& d, uint64_t base, uint32_t live, int64_t (&v)[kItems]) {
+  const uint64_t lo = (uint64_t)d.lower;
+  switch (d.bits) {
+    case 8: {
+      const uint8_t* p = (const uint8_t*)d.data + base;
+#pragma unroll
+      for (int k = 0; k < kItems; k++)
+        if ((live >> k) & 1) v[k] = (int64_t)((uint64_t)__ldg(p + k * kT) + lo);
+    } break;
+    case 16: {
+      const uint16_t* p = (const uint16_t*)d.data + base;
+#pragma unroll
+      for (int k = 0; k < kItems; k++)
+        if ((live >> k) & 1) v[k] = (int64_t)((uint64_t)__ldg(p + k * kT) + lo);
+    } break;
+    case 32: {
+      const uint32_t* p = (const uint32_t*)d.data + base;
+#pragma unroll
+      for (int k = 0; k < kItems; k++)
+        if ((live >> k) & 1) v[k] = (int64_t)((uint64_t)__ldg(p + k * kT) + lo);
+    } break;
+    default: {
+      const unsigned long long* p = (const unsigned long long*)d.data + base;
+#pragma unroll
+      for (int k = 0; k < kItems; k++)
+        if ((live >> k) & 1) v[k] = (int64_t)((uint64_t)__ldg(p + k * kT) + lo);
+    } break;
+  }
+}
+
+template <bool kBuild>
+__global__ void __launch_bounds__(kT) k_stage_fast(const __grid_constant__ FastArgs f) {
+  const StageArgs& a = f.a;
+  __shared__ alk_instr s_ins[8][ALK_MAX_INSTR];
+  __shared__ int64_t s_consts[8][ALK_MAX_CONST];
+  __shared__ uint32_t s_n[8], s_res[8];
+  __shared__ int64_t s_regs[ALK_MAX_REGS * kT];
+  __shared__ alk_colseg s_desc[kMaxCols];
+  for (uint32_t p = 1; p < a.nprogs; p++) {
+    for (uint32_t i = threadIdx.x; i < a.progs[p].n_instr; i += kT) s_ins[p][i] = a.progs[p].ins[i];
+    for (uint32_t i = threadIdx.x; i < ALK_MAX_CONST; i += kT) s_consts[p][i] = a.progs[p].consts[i];
+    if (threadIdx.x == 0) {
+      s_n[p] = a.progs[p].n_instr;
+      s_res[p] = a.progs[p].result;
+    }
+  }
+  unsigned long long rows_seen = 0, inserted = 0;
+  for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    __syncthreads();
+    const uint32_t seg = a.tile_seg[tile];
+    const uint32_t row0 = a.tile_row0[tile];
+    if (threadIdx.x < a.ncols) s_desc[threadIdx.x] = a.cols[threadIdx.x * a.nseg + seg];
+    __syncthreads();
+    const uint32_t rows = min((uint32_t)kTile, s_desc[0].rows - row0);
+    const uint64_t base = (uint64_t)row0 + threadIdx.x;
+    uint32_t live = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; k++)
+      if (k * kT + threadIdx.x < rows) live |= 1u << k;
+    rows_seen += __popc(live);
+    if (a.seg_mode[seg] != 1) {
+      for (uint32_t c = 0; c < f.nconj; c++) {
+        const Conj cj = f.conj[c];
+        int64_t v[kItems];
+        load_batch(s_desc[cj.slot], base, live, v);
+#pragma unroll
+        for (int k = 0; k < kItems; k++)
+          if (((live >> k) & 1) && !cmp_apply(cj.op, wrap_mul(v[k], cj.mul), cj.k)) live &= ~(1u << k);
+      }
+    }
+    if (!live) continue;
+    int64_t key[kItems];
+    if (a.probe_slot >= 0) {
+      load_batch(s_desc[a.probe_slot], base, live, key);
+      if (a.probe.bits) {
+#pragma unroll
+        for (int k = 0; k < kItems; k++)
+          if (((live >> k) & 1) && !ht_member(a.probe, key[k])) live &= ~(1u << k);
+      }
+    }
+#pragma unroll 1
+    for (int k = 0; k < kItems; k++) {
+      if (!((live >> k) & 1)) continue;
+      const uint64_t row = base + (uint64_t)k * kT;
+      int64_t j = -1;
+      if (a.probe_slot >= 0 && (f.need_slot || !a.probe.bits)) {
+        j = ht_probe(a.probe, key[k]);
+        if (j < 0) continue;
+      }
+      auto col = [&](uint32_t slot) -> int64_t {
+        if (slot >= 32) return __ldg(a.probe.payload + (uint64_t)(slot - 32) * a.probe.slot_cap + j);
+        const alk_colseg& d = s_desc[slot];
+        return load_for(d.data, d.bits, d.lower, row);
+      };
+      if (kBuild) {
+        const int64_t sl = ht_insert(a.build, col((uint32_t)a.build_slot));
+        if (sl < 0) continue;
+        inserted++;
+        for (uint32_t p = 0; p < a.build.npay; p++)
+          a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = col((uint32_t)a.pay_src[p]);
+      } else {
+        for (uint32_t g = 0; g < a.nagg; g++) {
+          unsigned long long* dst = (unsigned long long*)(a.acc + (uint64_t)g * a.acc_stride + j);
+          const uint8_t kind = a.agg_kind[g];
+          if (kind == ALK_AGG_COUNT) {
+            atomicAdd(dst, 1ull);
+            continue;
+          }
+          const int64_t v = vm_eval<kT>(s_ins[1 + g], s_n[1 + g], s_res[1 + g], s_consts[1 + g],
+                                        s_regs + threadIdx.x, col);
+          if (kind == ALK_AGG_SUM) atomicAdd(dst, (unsigned long long)v);
+          else if (kind == ALK_AGG_MIN) atomicMin((long long*)dst, (long long)v);
+          else atomicMax((long long*)dst, (long long)v);
+        }
+        if (a.cnt) atomicAdd(a.cnt + j, 1ull);
+      }
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
+    inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
+  }
+  if ((threadIdx.x & 31) == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
+  if (kBuild && (threadIdx.x & 31) == 0 && inserted) atomicAdd(a.build.nslots, inserted);
+}
+
+// ---------------------------------------------------------------- TMA-staged stage
+// The same stage with the columns every row needs (conjunct columns and the probe key)
+// brought into shared memory by bulk asynchronous copies (cp.async.bulk, completion on an
+// mbarrier), two tiles in flight per block: the copy engine keeps HBM busy while the
+// block evaluates the previous tile. Columns read only for matching rows (payload,
+// aggregate inputs) are read from global memory.
+constexpr int kStaged = 6;          // staged columns at most
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+struct TmaArgs {
+  FastArgs f;
+  uint32_t nstaged;
+  uint32_t staged_slot[kStaged];  // scan slot of each staged column
+  uint32_t stage_bytes;           // shared bytes of one stage (all staged columns, 2048 rows)
+  int* err;
+};
+
+template <bool kBuild>
+__global__ void __launch_bounds__(kT) k_stage_tma(const __grid_constant__ TmaArgs t) {
+  const FastArgs& f = t.f;
+  const StageArgs& a = f.a;
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  __shared__ alk_instr s_ins[8][ALK_MAX_INSTR];
+  __shared__ int64_t s_consts[8][ALK_MAX_CONST];
+  __shared__ uint32_t s_n[8], s_res[8];
+  __shared__ int64_t s_regs[ALK_MAX_REGS * kT];
+  __shared__ alk_colseg s_desc[2][kMaxCols];
+  __shared__ uint32_t s_off[2][kStaged];  // byte offset of each staged column in a stage buffer
+  __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ int s_abort;
+  for (uint32_t p = 1; p < a.nprogs; p++) {
+    for (uint32_t i = threadIdx.x; i < a.progs[p].n_instr; i += kT) s_ins[p][i] = a.progs[p].ins[i];
+    for (uint32_t i = threadIdx.x; i < ALK_MAX_CONST; i += kT) s_consts[p][i] = a.progs[p].consts[i];
+    if (threadIdx.x == 0) {
+      s_n[p] = a.progs[p].n_instr;
+      s_res[p] = a.progs[p].result;
+    }
+  }
+  // probe key and conjunct columns -> staged index
+  int probe_st = -1;
+  int conj_st[kMaxConj];
+  for (uint32_t c = 0; c < kMaxConj; c++) conj_st[c] = -1;
+  for (uint32_t i = 0; i < t.nstaged; i++) {
+    if (a.probe_slot >= 0 && t.staged_slot[i] == (uint32_t)a.probe_slot) probe_st = (int)i;
+    for (uint32_t c = 0; c < f.nconj; c++)
+      if (t.staged_slot[i] == f.conj[c].slot) conj_st[c] = (int)i;
+  }
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // issue the copies of this block's local tile number `it` into stage it & 1 (thread 0)
+  auto issue = [&](uint32_t it) {
+    const uint32_t tile = blockIdx.x + it * gridDim.x;
+    if (tile >= a.ntiles) return;
+    const uint32_t st = it & 1;
+    const uint32_t seg = a.tile_seg[tile];
+    const uint32_t row0 = a.tile_row0[tile];
+    for (uint32_t c = 0; c < a.ncols; c++) s_desc[st][c] = a.cols[c * a.nseg + seg];
+    const uint32_t rows = min((uint32_t)kTile, s_desc[st][0].rows - row0);
+    uint32_t off = 0, total = 0;
+    for (uint32_t i = 0; i < t.nstaged; i++) {
+      const alk_colseg& d = s_desc[st][t.staged_slot[i]];
+      const uint32_t w = d.bits / 8;
+      const uint32_t bytes = (rows * w + 15) & ~15u;
+      s_off[st][i] = off;
+      off += (kTile * w + 127) & ~127u;
+      total += bytes;
+    }
+    unsigned char* buf = s_dyn + st * t.stage_bytes;
+    mbar_expect_tx(&s_bar[st], total);
+    for (uint32_t i = 0; i < t.nstaged; i++) {
+      const alk_colseg& d = s_desc[st][t.staged_slot[i]];
+      const uint32_t w = d.bits / 8;
+      const uint32_t bytes = (rows * w + 15) & ~15u;
+      bulk_g2s(buf + s_off[st][i], (const unsigned char*)d.data + (uint64_t)row0 * w, bytes, &s_bar[st]);
+    }
+  };
+  if (threadIdx.x == 0) {
+    issue(0);
+    issue(1);
+  }
+  __syncthreads();
+  unsigned long long rows_seen = 0, inserted = 0;
+  uint32_t abort_it = 0;
+  for (uint32_t it = 0;; it++) {
+    const uint32_t tile = blockIdx.x + it * gridDim.x;
+    if (tile >= a.ntiles) break;
+    const uint32_t st = it & 1;
+    // wait for this stage's copies (bounded)
+    if (threadIdx.x == 0) {
+      uint32_t spins = 0;
+      while (!mbar_try_wait(&s_bar[st], (it >> 1) & 1)) {
+        if (++spins > kWaitLimit) {
+          atomicExch(t.err, ALK_ERR_TIMEOUT);
+          s_abort = 1;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __syncthreads();
+    if (s_abort) {
+      abort_it = it;
+      break;
+    }
+    const uint32_t seg = a.tile_seg[tile];
+    const uint32_t row0 = a.tile_row0[tile];
+    const uint32_t rows = min((uint32_t)kTile, s_desc[st][0].rows - row0);
+    const unsigned char* buf = s_dyn + st * t.stage_bytes;
+    auto staged = [&](int i, uint32_t r) -> int64_t {
+      const alk_colseg& d = s_desc[st][t.staged_slot[i]];
+      const unsigned char* p = buf + s_off[st][i];
+      uint64_t x;
+      switch (d.bits) {
+        case 8: x = p[r]; break;
+        case 16: x = ((const uint16_t*)p)[r]; break;
+        case 32: x = ((const uint32_t*)p)[r]; break;
+        default: x = ((const unsigned long long*)p)[r]; break;
+      }
+      return (int64_t)(x + (uint64_t)d.lower);
+    };
+    uint32_t live = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; k++)
+      if (k * kT + threadIdx.x < rows) live |= 1u << k;
+    rows_seen += __popc(live);
+    if (a.seg_mode[seg] != 1) {
+      for (uint32_t c = 0; c < f.nconj; c++) {
+        const Conj cj = f.conj[c];
+#pragma unroll
+        for (int k = 0; k < kItems; k++)
+          if (((live >> k) & 1) &&
+              !cmp_apply(cj.op, wrap_mul(staged(conj_st[c], k * kT + threadIdx.x), cj.mul), cj.k))
+            live &= ~(1u << k);
+      }
+    }
+    int64_t key[kItems];
+    if (live && probe_st >= 0) {
+#pragma unroll
+      for (int k = 0; k < kItems; k++) {
+        key[k] = ((live >> k) & 1) ? staged(probe_st, k * kT + threadIdx.x) : 0;
+        if (((live >> k) & 1) && a.probe.bits && !ht_member(a.probe, key[k])) live &= ~(1u << k);
+      }
+    }
+#pragma unroll 1
+    for (int k = 0; k < kItems; k++) {
+      if (!((live >> k) & 1)) continue;
+      const uint64_t row = (uint64_t)row0 + k * kT + threadIdx.x;
+      int64_t j = -1;
+      if (a.probe_slot >= 0 && (f.need_slot || !a.probe.bits)) {
+        j = ht_probe(a.probe, key[k]);
+        if (j < 0) continue;
+      }
+      auto col = [&](uint32_t slot) -> int64_t {
+        if (slot >= 32) return __ldg(a.probe.payload + (uint64_t)(slot - 32) * a.probe.slot_cap + j);
+        const alk_colseg& d = s_desc[st][slot];
+        return load_for(d.data, d.bits, d.lower, row);
+      };
+      if (kBuild) {
+        const int64_t sl = ht_insert(a.build, col((uint32_t)a.build_slot));
+        if (sl < 0) continue;
+        inserted++;
+        for (uint32_t p = 0; p < a.build.npay; p++)
+          a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = col((uint32_t)a.pay_src[p]);
+      } else {
+        for (uint32_t g = 0; g < a.nagg; g++) {
+          unsigned long long* dst = (unsigned long long*)(a.acc + (uint64_t)g * a.acc_stride + j);
+          const uint8_t kind = a.agg_kind[g];
+          if (kind == ALK_AGG_COUNT) {
+            atomicAdd(dst, 1ull);
+            continue;
+          }
+          const int64_t v = vm_eval<kT>(s_ins[1 + g], s_n[1 + g], s_res[1 + g], s_consts[1 + g],
+                                        s_regs + threadIdx.x, col);
+          if (kind == ALK_AGG_SUM) atomicAdd(dst, (unsigned long long)v);
+          else if (kind == ALK_AGG_MIN) atomicMin((long long*)dst, (long long)v);
+          else atomicMax((long long*)dst, (long long)v);
+        }
+        if (a.cnt) atomicAdd(a.cnt + j, 1ull);
+      }
+    }
+    // every thread is done with this stage: refill it with the tile two ahead
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(it + 2);
+    }
+  }
+  // an aborted block waits (bounded) for the copies still in flight (local tiles abort_it
+  // and abort_it + 1) before it exits
+  if (s_abort && threadIdx.x == 0) {
+    for (uint32_t it = abort_it; it < abort_it + 2; it++) {
+      if (blockIdx.x + it * gridDim.x >= a.ntiles) break;
+      for (uint32_t spins = 0; spins < kWaitLimit && !mbar_try_wait(&s_bar[it & 1], (it >> 1) & 1); spins++)
+        __nanosleep(32);
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
+    inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
+  }
+  if ((threadIdx.x & 31) == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
+  if (kBuild && (threadIdx.x & 31) == 0 && inserted) atomicAdd(a.build.nslots, inserted);
+}
+
+// Host: recognise an AND of (column * mul OP constant) tests in a compiled predicate.
+bool as_conjuncts(const alk_program& p, Conj* out, uint32_t* n) {
+  *n = 0;
+  if (p.n_instr == 0) return true;
+  struct R {
+    int kind = 0;  // 0 unknown, 1 scaled column, 2 conjunct list
+    uint32_t slot = 0;
+    int64_t mul = 1;
+    std::vector<Conj> cj;
+  } r[ALK_MAX_REGS];
+  struct Opd {
+    int kind;  // 0 unknown, 1 scaled column, 2 conjuncts, 3 constant
+    uint32_t slot;
+    int64_t mul, c;
+    const std::vector<Conj>* cj;
+  };
+  auto opd = [&](uint8_t k, uint16_t x) -> Opd {
+    if (k == ALK_K_COL) return {x < 32 ? 1 : 0, x, 1, 0, nullptr};
+    if (k == ALK_K_CONST) return {3, 0, 1, p.consts[x], nullptr};
+    const R& q = r[x];
+    return {q.kind, q.slot, q.mul, 0, &q.cj};
+  };
+  auto mirror = [](uint8_t op) -> uint8_t {
+    switch (op) {
+      case ALK_OP_LT: return ALK_OP_GT;
+      case ALK_OP_GT: return ALK_OP_LT;
+      case ALK_OP_LE: return ALK_OP_GE;
+      case ALK_OP_GE: return ALK_OP_LE;
+      default: return op;
+    }
+  };
+  for (uint32_t i = 0; i < p.n_instr; i++) {
+    const alk_instr& in = p.ins[i];
+    Opd x = opd(in.ka, in.a), y = opd(in.kb, in.b);
+    R res;
+    if (in.op == ALK_OP_MUL && ((x.kind == 1 && y.kind == 3) || (x.kind == 3 && y.kind == 1))) {
+      const Opd& c = x.kind == 1 ? x : y;
+      const Opd& k = x.kind == 3 ? x : y;
+      res.kind = 1;
+      res.slot = c.slot;
+      res.mul = (int64_t)((uint64_t)c.mul * (uint64_t)k.c);
+    } else if (in.op >= ALK_OP_LT && in.op <= ALK_OP_NE && x.kind == 1 && y.kind == 3) {
+      res.kind = 2;
+      res.cj.push_back({x.mul, y.c, x.slot, in.op});
+    } else if (in.op >= ALK_OP_LT && in.op <= ALK_OP_NE && x.kind == 3 && y.kind == 1) {
+      res.kind = 2;
+      res.cj.push_back({y.mul, x.c, y.slot, mirror(in.op)});
+    } else if (in.op == ALK_OP_AND && x.kind == 2 && y.kind == 2) {
+      res.kind = 2;
+      res.cj = *x.cj;
+      res.cj.insert(res.cj.end(), y.cj->begin(), y.cj->end());
+    } else if (in.op == ALK_OP_MOV && (x.kind == 1 || x.kind == 2)) {
+      res.kind = x.kind;
+      res.slot = x.slot;
+      res.mul = x.mul;
+      if (x.cj) res.cj = *x.cj;
+    } else {
+      return false;
+    }
+    r[in.dst] = res;
+  }
+  const R& fin = r[p.result];
+  if (fin.kind != 2 || fin.cj.size() > (size_t)kMaxConj) return false;
+  for (size_t i = 0; i < fin.cj.size(); i++) out[i] = fin.cj[i];
+  *n = (uint32_t)fin.cj.size();
+  return true;
+}
+
 int grid_for(uint64_t n) {
   uint64_t b = (n + kT - 1) / kT;
   return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)sms() * 8));
+}
+
+// Static shared memory of k_stage_tma (programs, registers, descriptors) next to the two
+// dynamic stage buffers; the SM offers 227 KB per block.
+constexpr size_t kTmaStaticSmem = 26 * 1024;
+constexpr size_t kSmemPerBlock = 227 * 1024;
+
+// Launch a stage: the TMA-staged kernel when the predicate is a conjunction and the
+// staged columns fit in shared memory, else the conjunctive kernel with direct loads,
+// else the register-machine kernel. cols is the host descriptor array [ncols][nseg].
+template <bool kBuild>
+cudaError_t launch_stage(const StageArgs& a, const alk_program& pred, int need_slot, const alk_colseg* cols,
+                         const uint8_t* seg_mode, int* d_err, cudaStream_t s, alk_event_timer* timer) {
+  if (!a.ntiles) return cudaSuccess;
+  FastArgs fa;
+  fa.a = a;
+  fa.need_slot = need_slot;
+  const bool conj = as_conjuncts(pred, fa.conj, &fa.nconj);
+  TmaArgs t{};
+  bool tma = false;
+  if (conj) {
+    t.f = fa;
+    t.err = d_err;
+    std::vector<uint32_t> st;
+    auto add = [&](uint32_t sl) {
+      if (std::find(st.begin(), st.end(), sl) == st.end()) st.push_back(sl);
+    };
+    for (uint32_t c = 0; c < fa.nconj; c++) add(fa.conj[c].slot);
+    if (a.probe_slot >= 0) add((uint32_t)a.probe_slot);
+    uint32_t bytes = 0;
+    for (uint32_t sl : st) {
+      uint32_t w = 1;
+      for (uint32_t g = 0; g < a.nseg; g++)
+        if (seg_mode[g]) w = std::max<uint32_t>(w, cols[sl * a.nseg + g].bits / 8);
+      bytes += (kTile * w + 127) & ~127u;
+    }
+    if (!st.empty() && st.size() <= (size_t)kStaged && kTmaStaticSmem + 2 * (size_t)bytes <= kSmemPerBlock) {
+      t.nstaged = (uint32_t)st.size();
+      for (size_t i = 0; i < st.size(); i++) t.staged_slot[i] = st[i];
+      t.stage_bytes = bytes;
+      tma = true;
+    }
+  }
+  int occ = 0;
+  int grid;
+  if (tma) {
+    cudaFuncSetAttribute(k_stage_tma<kBuild>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * t.stage_bytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_tma<kBuild>, kT, 2 * t.stage_bytes);
+  } else if (conj) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_fast<kBuild>, kT, 0);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage<kBuild>, kT, 0);
+  }
+  grid = std::min<int>((int)a.ntiles, sms() * std::max(occ, 1));
+  if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev0, s);
+  if (tma) k_stage_tma<kBuild><<<grid, kT, 2 * t.stage_bytes, s>>>(t);
+  else if (conj) k_stage_fast<kBuild><<<grid, kT, 0, s>>>(fa);
+  else k_stage<kBuild><<<grid, kT, 0, s>>>(a);
+  if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev1, s);
+  alk::g_kernel_launches++;
+  return cudaGetLastError();
 }
 
 bool prog_ok(const alk_program& p, uint32_t ncols, uint32_t npay) {
@@ -317,14 +876,27 @@ struct alk_ht {
 
 extern "C" {
 
-int alk_ht_create(uint64_t max_keys, uint32_t npay, alk_ht** out, alk_stream stream) {
+int alk_ht_create_range(uint64_t max_keys, uint32_t npay, int64_t key_min, int64_t key_max, alk_ht** out,
+                        alk_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (!out || npay > 8 || max_keys >= 0xffffffffull) return ALK_ERR_ARG;
   auto* h = new alk_ht();
   uint64_t cap = 1024;
   while (cap < 2 * max_keys) cap <<= 1;
-  uint64_t slot_cap = std::max<uint64_t>(max_keys, 1);
-  size_t bytes = cap * (4 + 8 + 4) + slot_cap * 8 * npay + 64;
+  const uint64_t slot_cap = cap;  // payload is indexed by table position
+  // exact key bitmap when the key range is at most 2^29 values (64 MB)
+  uint64_t nbits = 0;
+  if (key_max >= key_min) {
+    uint64_t span = (uint64_t)key_max - (uint64_t)key_min + 1;
+    if (span != 0 && span <= (1ull << 29)) nbits = span;
+  }
+  // the empty marker must not be a possible key
+  if (key_max >= key_min && kEmptyKey >= key_min && kEmptyKey <= key_max) {
+    delete h;
+    return ALK_ERR_UNSUPPORTED;
+  }
+  size_t words = (nbits + 31) / 32;
+  size_t bytes = cap * 8 + slot_cap * 8 * npay + 64 + words * 4;
   cudaError_t e = cudaMallocAsync(&h->mem, bytes, s);
   if (e != cudaSuccess) {
     delete h;
@@ -336,18 +908,24 @@ int alk_ht_create(uint64_t max_keys, uint32_t npay, alk_ht** out, alk_stream str
   p += cap * 8;
   h->v.payload = (int64_t*)p;
   p += slot_cap * 8 * npay;
-  h->v.state = (uint32_t*)p;
-  p += cap * 4;
-  h->v.slot = (uint32_t*)p;
-  p += cap * 4;
   h->v.nslots = (unsigned long long*)p;
   h->v.flags = (int*)(p + 8);
   h->v.slot_cap = slot_cap;
   h->v.npay = npay;
-  CK(cudaMemsetAsync(h->v.state, 0, cap * 4, s));
+  CK(cudaMemsetAsync(h->v.key, 0x80, cap * 8, s));  // every key word = kEmptyKey
   CK(cudaMemsetAsync(p, 0, 64, s));
+  if (nbits) {
+    h->v.bits = (uint32_t*)(p + 64);
+    h->v.kmin = key_min;
+    h->v.nbits = nbits;
+    CK(cudaMemsetAsync(h->v.bits, 0, words * 4, s));
+  }
   *out = h;
   return ALK_OK;
+}
+
+int alk_ht_create(uint64_t max_keys, uint32_t npay, alk_ht** out, alk_stream stream) {
+  return alk_ht_create_range(max_keys, npay, 1, 0, out, stream);
 }
 
 void alk_ht_free(alk_ht* h, alk_stream stream) {
@@ -360,14 +938,16 @@ int alk_ht_info(const alk_ht* h, uint64_t* nslots, int* flags, alk_stream stream
   cudaStream_t s = (cudaStream_t)stream;
   if (!h) return ALK_ERR_ARG;
   unsigned long long n = 0;
-  int f[3] = {0, 0, 0};
+  int f[4] = {0, 0, 0, 0};
   CK(cudaMemcpyAsync(&n, h->v.nslots, 8, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(f, h->v.flags, sizeof(f), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   if (nslots) *nslots = std::min<uint64_t>(n, h->v.slot_cap);
-  if (flags) *flags = (f[0] ? 1 : 0) | (f[1] ? 2 : 0) | (f[2] ? 4 : 0);
+  if (flags) *flags = (f[0] ? 1 : 0) | (f[1] ? 2 : 0) | (f[2] ? 4 : 0) | (f[3] ? 8 : 0);
   return ALK_OK;
 }
+
+uint64_t alk_ht_slots(const alk_ht* h) { return h ? h->v.slot_cap : 0; }
 
 const int64_t* alk_ht_payload(const alk_ht* h, uint32_t p) {
   if (!h || p >= h->v.npay) return nullptr;
@@ -446,7 +1026,7 @@ int alk_pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, co
   if (rc) return rc;
   std::memcpy(&hb[off_x], pay_src, 4 * build->v.npay);
   void* db = nullptr;
-  CK(cudaMallocAsync(&db, hb.size() + 16, s));
+  CK(cudaMallocAsync(&db, hb.size() + 32, s));
   CK(cudaMemcpyAsync(db, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
   unsigned long long* rows_in = (unsigned long long*)((uint8_t*)db + ((hb.size() + 7) & ~size_t(7)));
   CK(cudaMemsetAsync(rows_in, 0, 8, s));
@@ -457,18 +1037,20 @@ int alk_pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, co
   a.build_slot = build_slot;
   a.build = build->v;
   a.rows_in = rows_in;
-  if (a.ntiles) {
-    int grid = std::min<int>((int)a.ntiles, sms() * 4);
-    k_stage<true><<<grid, kT, 0, s>>>(a);
-    alk::g_kernel_launches++;
-  }
-  CK(cudaGetLastError());
+  int need_slot = 0;
+  for (uint32_t p = 0; p < build->v.npay; p++)
+    if (pay_src[p] >= 32) need_slot = 1;
+  int* d_err = (int*)(rows_in + 1);
+  CK(cudaMemsetAsync(d_err, 0, 8, s));
+  CK(launch_stage<true>(a, prog, need_slot, cols, seg_mode, d_err, s, nullptr));
   unsigned long long rin = 0;
+  int herr = 0;
   CK(cudaMemcpyAsync(&rin, rows_in, 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, s));
   CK(cudaFreeAsync(db, s));
   CK(cudaStreamSynchronize(s));
   if (h_rows_in) *h_rows_in = rin;
-  return ALK_OK;
+  return herr;
 }
 
 int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
@@ -479,13 +1061,8 @@ int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg
   cudaStream_t s = (cudaStream_t)stream;
   if (!probe || probe_slot < 0 || (uint32_t)probe_slot >= ncols || ncols == 0 || ncols > kMaxCols || nagg > 7)
     return ALK_ERR_ARG;
-  {
-    // accumulators are indexed by the probed table's slots: one per inserted key
-    unsigned long long ns = 0;
-    CK(cudaMemcpyAsync(&ns, probe->v.nslots, 8, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    if (acc_stride < std::min<uint64_t>(ns, probe->v.slot_cap)) return ALK_ERR_ARG;
-  }
+  if (acc_stride < probe->v.slot_cap) return ALK_ERR_ARG;  // accumulators indexed by table position
+
   std::vector<alk_program> progs(1 + nagg);
   std::memset(progs.data(), 0, sizeof(alk_program) * progs.size());
   if (pred) progs[0] = *pred;
@@ -500,7 +1077,7 @@ int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg
   if (rc) return rc;
   std::memcpy(&hb[off_x], agg_kind, nagg);
   void* db = nullptr;
-  CK(cudaMallocAsync(&db, hb.size() + 16, s));
+  CK(cudaMallocAsync(&db, hb.size() + 32, s));
   CK(cudaMemcpyAsync(db, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
   unsigned long long* rows_in = (unsigned long long*)((uint8_t*)db + ((hb.size() + 7) & ~size_t(7)));
   CK(cudaMemsetAsync(rows_in, 0, 8, s));
@@ -514,18 +1091,13 @@ int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg
   a.acc_stride = acc_stride;
   a.cnt = (unsigned long long*)d_cnt;
   a.rows_in = rows_in;
-  if (a.ntiles) {
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage<false>, kT, 0);
-    int grid = std::min<int>((int)a.ntiles, sms() * std::max(occ, 1));
-    if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev0, s);
-    k_stage<false><<<grid, kT, 0, s>>>(a);
-    if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev1, s);
-    alk::g_kernel_launches++;
-  }
-  CK(cudaGetLastError());
+  int* d_err = (int*)(rows_in + 1);
+  CK(cudaMemsetAsync(d_err, 0, 8, s));
+  CK(launch_stage<false>(a, progs[0], 1, cols, seg_mode, d_err, s, timer));
   unsigned long long rin = 0;
+  int herr = 0;
   CK(cudaMemcpyAsync(&rin, rows_in, 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, s));
   CK(cudaFreeAsync(db, s));
   CK(cudaStreamSynchronize(s));
   if (timer && timer->on && a.ntiles) {
@@ -535,7 +1107,7 @@ int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg
     timer->launches++;
   }
   if (h_rows_in) *h_rows_in = rin;
-  return ALK_OK;
+  return herr;
 }
 
 int alk_fill_i64(int64_t* d, uint64_t n, int64_t v, alk_stream stream) {
@@ -552,11 +1124,17 @@ int alk_topk_candidates(const int64_t* d_rank, const uint64_t* d_live, uint64_t 
   if (!h_count || k == 0 || k > 4096) return ALK_ERR_ARG;
   *h_count = 0;
   if (n == 0) return ALK_OK;
-  int blocks = (int)std::min<uint64_t>((n + 1023) / 1024, (uint64_t)sms() * 2);
+  const bool one_pass = k <= (uint32_t)kTopK;
+  const int blocks = one_pass ? (int)std::min<uint64_t>((n + kT - 1) / kT, (uint64_t)sms() * 2)
+                              : (int)std::min<uint64_t>((n + 1023) / 1024, (uint64_t)sms() * 2);
   std::vector<int64_t> best((size_t)blocks * k);
   void* db = nullptr;
   CK(cudaMallocAsync(&db, best.size() * 8 + 16, s));
-  k_topk_local<<<blocks, kT, 0, s>>>(d_rank, (const unsigned long long*)d_live, n, k, (int64_t*)db);
+  if (one_pass) {
+    k_topk_local16<<<blocks, kT, 0, s>>>(d_rank, (const unsigned long long*)d_live, n, k, (int64_t*)db);
+  } else {
+    k_topk_local<<<blocks, kT, 0, s>>>(d_rank, (const unsigned long long*)d_live, n, k, (int64_t*)db);
+  }
   alk::g_kernel_launches++;
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(best.data(), db, best.size() * 8, cudaMemcpyDeviceToHost, s));

@@ -316,7 +316,8 @@ void Engine::ensure_base_col(Var* base, const std::string& col, bool device) {
        "segment upload");
     stats_.h2d_bytes += m.cnt;
     if (m.comp_type == 1) {
-      auto dec = mkbuf((size_t)m.rec_count * 8, stream_);
+      // padded like the FOR payloads: bulk tile copies round their length up to 16 bytes
+      auto dec = mkbuf((size_t)m.rec_count * 8 + 256, stream_);
       check(alk_decode_segment(buf->as<void>(), 1, m.bits, m.fit_count, m.orig_lower, m.start_val, m.rec_count,
                                dec->as<int64_t>(), (alk_stream)stream_),
             "delta decode");

@@ -148,6 +148,9 @@ class Engine {
   std::map<std::string, std::shared_ptr<Var>> bases_;  // catalog tables (persist across scripts)
   std::map<std::string, std::map<std::string, BaseCol>> basecols_;
   alk_stats stats_{};
+  // Exact build-side key counts recorded by previous runs of the same fused stage; they
+  // size the next run's hash table (overflow reruns the stage at the upper bound).
+  std::map<std::string, uint64_t> card_feedback_;
   bool timing_ = false;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
 

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <numeric>
 
 #include "../csrc/internal.h"
@@ -1039,6 +1040,17 @@ bool Engine::try_fused(std::vector<Statement>& sts, size_t& i) {
 
 void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
   cudaStream_t s = stream_;
+  // [min, max] of a base column over every segment, from the segment headers (zone maps)
+  auto range_of = [&](Var* src, const std::string& col) {
+    BaseCol& bc = basecol(src, col);
+    read_headers(src, col, bc);
+    int64_t lo = INT64_MAX, hi = INT64_MIN;
+    for (auto& sg : bc.segs) {
+      lo = std::min(lo, std::min(sg.m.lower, sg.m.upper));
+      hi = std::max(hi, std::max(sg.m.lower, sg.m.upper));
+    }
+    return std::make_pair(lo, hi);
+  };
   // ---- resolve the join chain (emit_join, operators.cu:832-859)
   std::vector<std::string> op_sel, op_alias;
   for (unsigned k = 0; k < J.sel_count; k++) {
@@ -1150,6 +1162,41 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
   }
   if (payload.size() > 8) fallback("payload width");
   // ---- build stages
+  // Each stage's table is sized from the exact key count the previous run of the same
+  // stage recorded (the count the engine learns from its own runs); without one, or
+  // when the table overflows, the stage runs with the exact upper bound (rows scanned).
+  auto build_stage = [&](HtGuard& g, const std::string& sig, uint64_t upper, uint32_t npay,
+                         std::pair<int64_t, int64_t> range, const std::function<void(alk_ht*)>& run) {
+    auto it = card_feedback_.find(sig);
+    uint64_t est = it == card_feedback_.end() ? upper : std::min(upper, it->second + it->second / 4 + 1024);
+    for (int attempt = 0; attempt < 2; attempt++) {
+      if (g.h) alk_ht_free(g.h, (alk_stream)s);
+      g.h = nullptr;
+      g.s = s;
+      check(alk_ht_create_range(est, npay, range.first, range.second, &g.h, (alk_stream)s), "hash table");
+      run(g.h);
+      uint64_t inserted = 0;
+      int fl = 0;
+      check(alk_ht_info(g.h, &inserted, &fl, (alk_stream)s), "hash table");
+      if ((fl & 2) && est < upper) {
+        est = upper;
+        continue;
+      }
+      if (fl) fallback("duplicate build keys or an inconsistent key range");
+      card_feedback_[sig] = inserted;
+      return;
+    }
+  };
+  auto rows_of = [&](const ScanPlan& p, const std::vector<alk_colseg>& cs) {
+    uint64_t n = 0;
+    for (uint32_t g = 0; g < p.src->segCount; g++)
+      if (p.mode[g]) n += cs[g].rows;
+    return n;
+  };
+  auto plan_sig = [&](const ScanPlan& p) {
+    return p.src->table + "|" + std::string((const char*)&p.pred, sizeof(p.pred)) + "|" +
+           std::string((const char*)p.mode.data(), p.mode.size());
+  };
   HtGuard ht1, ht2;
   alk_ht* last = nullptr;
   std::map<std::string, uint32_t> last_pay;  // payload column index in the last table
@@ -1164,18 +1211,13 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     std::vector<int32_t> src1;
     for (auto& c : pay1) src1.push_back((int32_t)p1.slot(c));
     auto cs1 = colsegs(p1);
-    uint64_t max1 = 0;
-    for (uint32_t g = 0; g < p1.src->segCount; g++)
-      if (p1.mode[g]) max1 += cs1[g].rows;
-    check(alk_ht_create(max1, (uint32_t)pay1.size(), &ht1.h, (alk_stream)s), "hash table");
-    ht1.s = s;
-    check(alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
-                             p1.has_pred ? &p1.pred : nullptr, nullptr, -1, ht1.h, (int32_t)k1, src1.data(),
-                             nullptr, (alk_stream)s),
-          "build stage");
-    int fl = 0;
-    check(alk_ht_info(ht1.h, nullptr, &fl, (alk_stream)s), "hash table");
-    if (fl) fallback("duplicate or overflowing build keys");
+    std::string sig1 = plan_sig(p1) + "|" + st1.rkey;
+    build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)pay1.size(), range_of(p1.src, st1.rkey), [&](alk_ht* h) {
+      check(alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
+                               p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h, (int32_t)k1, src1.data(), nullptr,
+                               (alk_stream)s),
+            "build stage");
+    });
     // stage 2: d1 probes stage 1 on st1.lkey and is keyed on the final build key
     ScanPlan p2 = plan_scan(d1);
     uint32_t probe2 = p2.slot(st1.lkey);
@@ -1193,17 +1235,13 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
       last_pay[c] = (uint32_t)src2.size() - 1;
     }
     auto cs2 = colsegs(p2);
-    uint64_t max2 = 0;
-    for (uint32_t g = 0; g < p2.src->segCount; g++)
-      if (p2.mode[g]) max2 += cs2[g].rows;
-    check(alk_ht_create(max2, (uint32_t)payload.size(), &ht2.h, (alk_stream)s), "hash table");
-    ht2.s = s;
-    check(alk_pipeline_build(cs2.data(), (uint32_t)p2.slots.size(), p2.src->segCount, p2.mode.data(),
-                             p2.has_pred ? &p2.pred : nullptr, ht1.h, (int32_t)probe2, ht2.h, key2, src2.data(),
-                             nullptr, (alk_stream)s),
-          "build stage");
-    check(alk_ht_info(ht2.h, nullptr, &fl, (alk_stream)s), "hash table");
-    if (fl) fallback("duplicate or overflowing build keys");
+    std::string sig2 = plan_sig(p2) + "|" + build_key + "|" + sig1;
+    build_stage(ht2, sig2, rows_of(p2, cs2), (uint32_t)payload.size(), range_of(p2.src, build_key), [&](alk_ht* h) {
+      check(alk_pipeline_build(cs2.data(), (uint32_t)p2.slots.size(), p2.src->segCount, p2.mode.data(),
+                               p2.has_pred ? &p2.pred : nullptr, ht1.h, (int32_t)probe2, h, key2, src2.data(),
+                               nullptr, (alk_stream)s),
+            "build stage");
+    });
     last = ht2.h;
   } else {
     ScanPlan p1 = plan_scan(d1);
@@ -1214,22 +1252,16 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
       last_pay[c] = (uint32_t)src1.size() - 1;
     }
     auto cs1 = colsegs(p1);
-    uint64_t max1 = 0;
-    for (uint32_t g = 0; g < p1.src->segCount; g++)
-      if (p1.mode[g]) max1 += cs1[g].rows;
-    check(alk_ht_create(max1, (uint32_t)payload.size(), &ht1.h, (alk_stream)s), "hash table");
-    ht1.s = s;
-    check(alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
-                             p1.has_pred ? &p1.pred : nullptr, nullptr, -1, ht1.h, (int32_t)k1, src1.data(),
-                             nullptr, (alk_stream)s),
-          "build stage");
-    int fl = 0;
-    check(alk_ht_info(ht1.h, nullptr, &fl, (alk_stream)s), "hash table");
-    if (fl) fallback("duplicate or overflowing build keys");
+    std::string sig1 = plan_sig(p1) + "|" + build_key;
+    build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)payload.size(), range_of(p1.src, build_key), [&](alk_ht* h) {
+      check(alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
+                               p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h, (int32_t)k1, src1.data(), nullptr,
+                               (alk_stream)s),
+            "build stage");
+    });
     last = ht1.h;
   }
-  uint64_t nslots = 0;
-  check(alk_ht_info(last, &nslots, nullptr, (alk_stream)s), "hash table");
+  const uint64_t nslots = alk_ht_slots(last);  // accumulators are indexed by table position
   // ---- probe-aggregate over the fact table
   ScanPlan pf = plan_scan(fact);
   uint32_t probe_f = pf.slot(st2.lkey);

@@ -220,9 +220,19 @@ void alk_join_free(alk_join_table* t, alk_stream stream);
 typedef struct alk_ht alk_ht;
 /* max_keys bounds the inserted keys; npay payload columns (<= 8) per key. */
 int alk_ht_create(uint64_t max_keys, uint32_t npay, alk_ht** out, alk_stream stream);
+/* Same, for keys known to lie in [key_min, key_max] (the build column's zone maps): the
+ * table then also keeps an exact membership bitmap of the inserted keys (when the range
+ * spans at most 2^29 values) that probes test before hashing. A key inserted outside
+ * the range sets flag 8. */
+int alk_ht_create_range(uint64_t max_keys, uint32_t npay, int64_t key_min, int64_t key_max, alk_ht** out,
+                        alk_stream stream);
 void alk_ht_free(alk_ht* h, alk_stream stream);
-/* Inserted keys and flags (1 duplicate key, 2 capacity exceeded, 4 wait expired). */
+/* Inserted keys and flags (1 duplicate key, 2 capacity exceeded, 4 wait expired,
+ * 8 key outside the declared range). */
 int alk_ht_info(const alk_ht* h, uint64_t* nslots, int* flags, alk_stream stream);
+/* Slot range of a table: payload columns and per-key accumulators are indexed by the
+ * key's table position, 0 <= slot < alk_ht_slots(h). */
+uint64_t alk_ht_slots(const alk_ht* h);
 /* Device address of payload column p (slot-indexed). */
 const int64_t* alk_ht_payload(const alk_ht* h, uint32_t p);
 /* Optional CUDA-event timing of the probe-aggregate kernel (cudaEvent_t handles). */
