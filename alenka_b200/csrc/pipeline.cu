@@ -95,6 +95,15 @@ __device__ __forceinline__ int64_t ht_insert(const HtView& h, int64_t k) {
   return -1;
 }
 
+// A row that survived a stage's scan: its position and its probe key. The scan kernels
+// stream the columns every row needs and append survivors here; the hit kernel then
+// does the per-row random work (hash probe, payload and aggregate-input loads, atomics)
+// for all survivors in parallel, away from the scan's tile pipeline.
+struct Hit {
+  uint64_t pos;  // segment << 32 | row within the segment
+  int64_t key;   // probe key (0 when the stage probes nothing)
+};
+
 struct StageArgs {
   const alk_colseg* cols;  // [ncols][nseg]
   uint32_t ncols, nseg;
@@ -106,6 +115,7 @@ struct StageArgs {
   uint32_t nprogs;
   int32_t probe_slot;  // fact column probed into probe_ht (-1: none)
   HtView probe;
+  int need_slot;  // the stage reads the probed table's payload (else membership suffices)
   // build stage
   int32_t build_slot;
   HtView build;
@@ -117,24 +127,55 @@ struct StageArgs {
   uint64_t acc_stride;
   unsigned long long* cnt;  // rows per build slot (may be null)
   unsigned long long* rows_in;
+  // survivors of the scan
+  Hit* hits;
+  uint64_t hit_cap;
+  unsigned long long* hit_count;
+  int* err;
 };
 
-template <bool kBuild>
-__global__ void __launch_bounds__(kT) k_stage(StageArgs a) {
-  __shared__ alk_instr s_ins[8][ALK_MAX_INSTR];
-  __shared__ int64_t s_consts[8][ALK_MAX_CONST];
-  __shared__ uint32_t s_n[8], s_res[8];
+// Appends the thread's live items (rows base + k * kT of segment seg) to the hit list with
+// one atomic per warp. Called by all 32 lanes; entries beyond hit_cap are counted but not
+// written (the hit kernel then refuses the whole list).
+__device__ __forceinline__ void emit_hits(const StageArgs& a, uint32_t live, uint32_t seg, uint64_t base,
+                                          const int64_t (&key)[kItems]) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n = __popc(live);
+  uint32_t incl = n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (uint32_t)o) incl += y;
+  }
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+  if (total == 0) return;
+  unsigned long long b = 0;
+  if (lane == 31) b = atomicAdd(a.hit_count, (unsigned long long)total);
+  b = __shfl_sync(0xffffffffu, b, 31);
+  uint64_t p = b + incl - n;
+#pragma unroll
+  for (int k = 0; k < kItems; k++) {
+    if (!((live >> k) & 1)) continue;
+    if (p < a.hit_cap) a.hits[p] = Hit{(uint64_t)seg << 32 | (base + (uint64_t)k * kT), key[k]};
+    p++;
+  }
+}
+
+// Register-machine scan for predicates of any shape: the predicate runs per row, the
+// probe key is tested against the probed table's key bitmap, survivors go to the hit list.
+__global__ void __launch_bounds__(kT) k_stage_scan(const StageArgs a) {
+  __shared__ alk_instr s_ins[ALK_MAX_INSTR];
+  __shared__ int64_t s_consts[ALK_MAX_CONST];
+  __shared__ uint32_t s_n, s_res;
   __shared__ int64_t s_regs[ALK_MAX_REGS * kT];
   __shared__ alk_colseg s_desc[kMaxCols];
-  for (uint32_t p = 0; p < a.nprogs; p++) {
-    for (uint32_t i = threadIdx.x; i < a.progs[p].n_instr; i += kT) s_ins[p][i] = a.progs[p].ins[i];
-    for (uint32_t i = threadIdx.x; i < ALK_MAX_CONST; i += kT) s_consts[p][i] = a.progs[p].consts[i];
-    if (threadIdx.x == 0) {
-      s_n[p] = a.progs[p].n_instr;
-      s_res[p] = a.progs[p].result;
-    }
+  for (uint32_t i = threadIdx.x; i < a.progs[0].n_instr; i += kT) s_ins[i] = a.progs[0].ins[i];
+  for (uint32_t i = threadIdx.x; i < ALK_MAX_CONST; i += kT) s_consts[i] = a.progs[0].consts[i];
+  if (threadIdx.x == 0) {
+    s_n = a.progs[0].n_instr;
+    s_res = a.progs[0].result;
   }
-  unsigned long long rows_seen = 0, inserted = 0;
+  unsigned long long rows_seen = 0;
   for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
     __syncthreads();
     const uint32_t seg = a.tile_seg[tile];
@@ -142,54 +183,103 @@ __global__ void __launch_bounds__(kT) k_stage(StageArgs a) {
     if (threadIdx.x < a.ncols) s_desc[threadIdx.x] = a.cols[threadIdx.x * a.nseg + seg];
     __syncthreads();
     const uint32_t rows = min((uint32_t)kTile, s_desc[0].rows - row0);
-    const bool all = a.seg_mode[seg] == 1 || s_n[0] == 0;
-#pragma unroll 2
+    const bool all = a.seg_mode[seg] == 1 || s_n == 0;
+    const uint64_t base = (uint64_t)row0 + threadIdx.x;
+    uint32_t live = 0;
+    int64_t key[kItems];
+#pragma unroll 1
     for (int k = 0; k < kItems; k++) {
-      const uint32_t r = k * kT + threadIdx.x;
-      if (r >= rows) continue;
-      const uint64_t row = (uint64_t)row0 + r;
+      key[k] = 0;
+      if (k * kT + threadIdx.x >= rows) continue;
+      const uint64_t row = base + (uint64_t)k * kT;
       rows_seen++;
-      int64_t j = -1;
       auto col = [&](uint32_t slot) -> int64_t {
-        if (slot >= 32) return __ldg(a.probe.payload + (uint64_t)(slot - 32) * a.probe.slot_cap + j);
         const alk_colseg& d = s_desc[slot];
         return load_for(d.data, d.bits, d.lower, row);
       };
-      if (!all && vm_eval<kT>(s_ins[0], s_n[0], s_res[0], s_consts[0], s_regs + threadIdx.x, col) == 0) continue;
+      if (!all && vm_eval<kT>(s_ins, s_n, s_res, s_consts, s_regs + threadIdx.x, col) == 0) continue;
       if (a.probe_slot >= 0) {
-        j = ht_probe(a.probe, col((uint32_t)a.probe_slot));
-        if (j < 0) continue;
+        key[k] = col((uint32_t)a.probe_slot);
+        if (a.probe.bits && !ht_member(a.probe, key[k])) continue;
       }
-      if (kBuild) {
-        const int64_t sl = ht_insert(a.build, col((uint32_t)a.build_slot));
-        if (sl < 0) continue;
-        inserted++;
-        for (uint32_t p = 0; p < a.build.npay; p++)
-          a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = col((uint32_t)a.pay_src[p]);
-      } else {
-        for (uint32_t g = 0; g < a.nagg; g++) {
-          unsigned long long* dst = (unsigned long long*)(a.acc + (uint64_t)g * a.acc_stride + j);
-          const uint8_t kind = a.agg_kind[g];
-          if (kind == ALK_AGG_COUNT) {
-            atomicAdd(dst, 1ull);
-            continue;
-          }
-          const int64_t v = vm_eval<kT>(s_ins[1 + g], s_n[1 + g], s_res[1 + g], s_consts[1 + g],
-                                        s_regs + threadIdx.x, col);
-          if (kind == ALK_AGG_SUM) atomicAdd(dst, (unsigned long long)v);
-          else if (kind == ALK_AGG_MIN) atomicMin((long long*)dst, (long long)v);
-          else atomicMax((long long*)dst, (long long)v);
-        }
-        if (a.cnt) atomicAdd(a.cnt + j, 1ull);
+      live |= 1u << k;
+    }
+    emit_hits(a, live, seg, base, key);
+  }
+  for (int o = 16; o; o >>= 1) rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
+  if ((threadIdx.x & 31) == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
+}
+
+// Per-survivor work of a stage, one thread per hit: the hash probe (for the payload
+// position, or for membership when the probed table has no key bitmap), then either the
+// build-side insert with its payload or the aggregate updates. A list that overflowed
+// its capacity is refused as a whole (nothing is applied), so a rerun with a larger list
+// starts from unchanged tables and accumulators.
+template <bool kBuild>
+__global__ void __launch_bounds__(kT) k_stage_hits(const StageArgs a) {
+  __shared__ alk_instr s_ins[8][ALK_MAX_INSTR];
+  __shared__ int64_t s_consts[8][ALK_MAX_CONST];
+  __shared__ uint32_t s_n[8], s_res[8];
+  __shared__ int64_t s_regs[ALK_MAX_REGS * kT];
+  const uint64_t n = *(volatile unsigned long long*)a.hit_count;  // written by the scan kernel
+  if (n > a.hit_cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.err, ALK_ERR_OVERFLOW);
+    return;
+  }
+  if (!kBuild) {
+    for (uint32_t p = 1; p < a.nprogs; p++) {
+      for (uint32_t i = threadIdx.x; i < a.progs[p].n_instr; i += kT) s_ins[p][i] = a.progs[p].ins[i];
+      for (uint32_t i = threadIdx.x; i < ALK_MAX_CONST; i += kT) s_consts[p][i] = a.progs[p].consts[i];
+      if (threadIdx.x == 0) {
+        s_n[p] = a.progs[p].n_instr;
+        s_res[p] = a.progs[p].result;
       }
     }
+    __syncthreads();
   }
-  for (int o = 16; o; o >>= 1) {
-    rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
-    inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
+  unsigned long long inserted = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
+    const Hit h = a.hits[i];
+    const uint32_t seg = (uint32_t)(h.pos >> 32);
+    const uint64_t row = h.pos & 0xffffffffull;
+    int64_t j = -1;
+    if (a.probe_slot >= 0 && (a.need_slot || !a.probe.bits)) {
+      j = ht_probe(a.probe, h.key);
+      if (j < 0) continue;
+    }
+    auto col = [&](uint32_t slot) -> int64_t {
+      if (slot >= 32) return __ldg(a.probe.payload + (uint64_t)(slot - 32) * a.probe.slot_cap + j);
+      const alk_colseg* d = a.cols + (uint64_t)slot * a.nseg + seg;
+      const void* data = (const void*)__ldg((const unsigned long long*)&d->data);
+      return load_for(data, __ldg(&d->bits), (int64_t)__ldg((const long long*)&d->lower), row);
+    };
+    if (kBuild) {
+      const int64_t sl = ht_insert(a.build, col((uint32_t)a.build_slot));
+      if (sl < 0) continue;
+      inserted++;
+      for (uint32_t p = 0; p < a.build.npay; p++)
+        a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = col((uint32_t)a.pay_src[p]);
+    } else {
+      for (uint32_t g = 0; g < a.nagg; g++) {
+        unsigned long long* dst = (unsigned long long*)(a.acc + (uint64_t)g * a.acc_stride + j);
+        const uint8_t kind = a.agg_kind[g];
+        if (kind == ALK_AGG_COUNT) {
+          atomicAdd(dst, 1ull);
+          continue;
+        }
+        const int64_t v =
+            vm_eval<kT>(s_ins[1 + g], s_n[1 + g], s_res[1 + g], s_consts[1 + g], s_regs + threadIdx.x, col);
+        if (kind == ALK_AGG_SUM) atomicAdd(dst, (unsigned long long)v);
+        else if (kind == ALK_AGG_MIN) atomicMin((long long*)dst, (long long)v);
+        else atomicMax((long long*)dst, (long long)v);
+      }
+      if (a.cnt) atomicAdd(a.cnt + j, 1ull);
+    }
   }
-  if ((threadIdx.x & 31) == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
-  if (kBuild && (threadIdx.x & 31) == 0 && inserted) atomicAdd(a.build.nslots, inserted);
+  if (kBuild) {
+    for (int o = 16; o; o >>= 1) inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
+    if ((threadIdx.x & 31) == 0 && inserted) atomicAdd(a.build.nslots, inserted);
+  }
 }
 
 __global__ void __launch_bounds__(kT) k_fill_i64(int64_t* p, uint64_t n, int64_t v) {
@@ -337,7 +427,6 @@ struct FastArgs {
   StageArgs a;
   Conj conj[kMaxConj];
   uint32_t nconj;
-  int need_slot;  // the stage reads the probed table's payload (else membership suffices)
 };
 
 __device__ __forceinline__ bool cmp_apply(uint32_t op, int64_t a, int64_t b) {
@@ -382,23 +471,10 @@ __device__ __forceinline__ void load_batch(const alk_colseg& d, uint64_t base, u
   }
 }
 
-template <bool kBuild>
 __global__ void __launch_bounds__(kT) k_stage_fast(const __grid_constant__ FastArgs f) {
   const StageArgs& a = f.a;
-  __shared__ alk_instr s_ins[8][ALK_MAX_INSTR];
-  __shared__ int64_t s_consts[8][ALK_MAX_CONST];
-  __shared__ uint32_t s_n[8], s_res[8];
-  __shared__ int64_t s_regs[ALK_MAX_REGS * kT];
   __shared__ alk_colseg s_desc[kMaxCols];
-  for (uint32_t p = 1; p < a.nprogs; p++) {
-    for (uint32_t i = threadIdx.x; i < a.progs[p].n_instr; i += kT) s_ins[p][i] = a.progs[p].ins[i];
-    for (uint32_t i = threadIdx.x; i < ALK_MAX_CONST; i += kT) s_consts[p][i] = a.progs[p].consts[i];
-    if (threadIdx.x == 0) {
-      s_n[p] = a.progs[p].n_instr;
-      s_res[p] = a.progs[p].result;
-    }
-  }
-  unsigned long long rows_seen = 0, inserted = 0;
+  unsigned long long rows_seen = 0;
   for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
     __syncthreads();
     const uint32_t seg = a.tile_seg[tile];
@@ -422,9 +498,10 @@ __global__ void __launch_bounds__(kT) k_stage_fast(const __grid_constant__ FastA
           if (((live >> k) & 1) && !cmp_apply(cj.op, wrap_mul(v[k], cj.mul), cj.k)) live &= ~(1u << k);
       }
     }
-    if (!live) continue;
     int64_t key[kItems];
-    if (a.probe_slot >= 0) {
+#pragma unroll
+    for (int k = 0; k < kItems; k++) key[k] = 0;
+    if (live && a.probe_slot >= 0) {
       load_batch(s_desc[a.probe_slot], base, live, key);
       if (a.probe.bits) {
 #pragma unroll
@@ -432,50 +509,10 @@ __global__ void __launch_bounds__(kT) k_stage_fast(const __grid_constant__ FastA
           if (((live >> k) & 1) && !ht_member(a.probe, key[k])) live &= ~(1u << k);
       }
     }
-#pragma unroll 1
-    for (int k = 0; k < kItems; k++) {
-      if (!((live >> k) & 1)) continue;
-      const uint64_t row = base + (uint64_t)k * kT;
-      int64_t j = -1;
-      if (a.probe_slot >= 0 && (f.need_slot || !a.probe.bits)) {
-        j = ht_probe(a.probe, key[k]);
-        if (j < 0) continue;
-      }
-      auto col = [&](uint32_t slot) -> int64_t {
-        if (slot >= 32) return __ldg(a.probe.payload + (uint64_t)(slot - 32) * a.probe.slot_cap + j);
-        const alk_colseg& d = s_desc[slot];
-        return load_for(d.data, d.bits, d.lower, row);
-      };
-      if (kBuild) {
-        const int64_t sl = ht_insert(a.build, col((uint32_t)a.build_slot));
-        if (sl < 0) continue;
-        inserted++;
-        for (uint32_t p = 0; p < a.build.npay; p++)
-          a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = col((uint32_t)a.pay_src[p]);
-      } else {
-        for (uint32_t g = 0; g < a.nagg; g++) {
-          unsigned long long* dst = (unsigned long long*)(a.acc + (uint64_t)g * a.acc_stride + j);
-          const uint8_t kind = a.agg_kind[g];
-          if (kind == ALK_AGG_COUNT) {
-            atomicAdd(dst, 1ull);
-            continue;
-          }
-          const int64_t v = vm_eval<kT>(s_ins[1 + g], s_n[1 + g], s_res[1 + g], s_consts[1 + g],
-                                        s_regs + threadIdx.x, col);
-          if (kind == ALK_AGG_SUM) atomicAdd(dst, (unsigned long long)v);
-          else if (kind == ALK_AGG_MIN) atomicMin((long long*)dst, (long long)v);
-          else atomicMax((long long*)dst, (long long)v);
-        }
-        if (a.cnt) atomicAdd(a.cnt + j, 1ull);
-      }
-    }
+    emit_hits(a, live, seg, base, key);
   }
-  for (int o = 16; o; o >>= 1) {
-    rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
-    inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
-  }
+  for (int o = 16; o; o >>= 1) rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
   if ((threadIdx.x & 31) == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
-  if (kBuild && (threadIdx.x & 31) == 0 && inserted) atomicAdd(a.build.nslots, inserted);
 }
 
 // ---------------------------------------------------------------- TMA-staged stage
@@ -516,30 +553,16 @@ struct TmaArgs {
   uint32_t nstaged;
   uint32_t staged_slot[kStaged];  // scan slot of each staged column
   uint32_t stage_bytes;           // shared bytes of one stage (all staged columns, 2048 rows)
-  int* err;
 };
 
-template <bool kBuild>
 __global__ void __launch_bounds__(kT) k_stage_tma(const __grid_constant__ TmaArgs t) {
   const FastArgs& f = t.f;
   const StageArgs& a = f.a;
   extern __shared__ __align__(128) unsigned char s_dyn[];
-  __shared__ alk_instr s_ins[8][ALK_MAX_INSTR];
-  __shared__ int64_t s_consts[8][ALK_MAX_CONST];
-  __shared__ uint32_t s_n[8], s_res[8];
-  __shared__ int64_t s_regs[ALK_MAX_REGS * kT];
   __shared__ alk_colseg s_desc[2][kMaxCols];
   __shared__ uint32_t s_off[2][kStaged];  // byte offset of each staged column in a stage buffer
   __shared__ __align__(8) uint64_t s_bar[2];
   __shared__ int s_abort;
-  for (uint32_t p = 1; p < a.nprogs; p++) {
-    for (uint32_t i = threadIdx.x; i < a.progs[p].n_instr; i += kT) s_ins[p][i] = a.progs[p].ins[i];
-    for (uint32_t i = threadIdx.x; i < ALK_MAX_CONST; i += kT) s_consts[p][i] = a.progs[p].consts[i];
-    if (threadIdx.x == 0) {
-      s_n[p] = a.progs[p].n_instr;
-      s_res[p] = a.progs[p].result;
-    }
-  }
   // probe key and conjunct columns -> staged index
   int probe_st = -1;
   int conj_st[kMaxConj];
@@ -588,7 +611,7 @@ __global__ void __launch_bounds__(kT) k_stage_tma(const __grid_constant__ TmaArg
     issue(1);
   }
   __syncthreads();
-  unsigned long long rows_seen = 0, inserted = 0;
+  unsigned long long rows_seen = 0;
   uint32_t abort_it = 0;
   for (uint32_t it = 0;; it++) {
     const uint32_t tile = blockIdx.x + it * gridDim.x;
@@ -599,7 +622,7 @@ __global__ void __launch_bounds__(kT) k_stage_tma(const __grid_constant__ TmaArg
       uint32_t spins = 0;
       while (!mbar_try_wait(&s_bar[st], (it >> 1) & 1)) {
         if (++spins > kWaitLimit) {
-          atomicExch(t.err, ALK_ERR_TIMEOUT);
+          atomicExch(a.err, ALK_ERR_TIMEOUT);
           s_abort = 1;
           break;
         }
@@ -643,50 +666,17 @@ __global__ void __launch_bounds__(kT) k_stage_tma(const __grid_constant__ TmaArg
       }
     }
     int64_t key[kItems];
+#pragma unroll
+    for (int k = 0; k < kItems; k++) key[k] = 0;
     if (live && probe_st >= 0) {
 #pragma unroll
       for (int k = 0; k < kItems; k++) {
-        key[k] = ((live >> k) & 1) ? staged(probe_st, k * kT + threadIdx.x) : 0;
-        if (((live >> k) & 1) && a.probe.bits && !ht_member(a.probe, key[k])) live &= ~(1u << k);
+        if (!((live >> k) & 1)) continue;
+        key[k] = staged(probe_st, k * kT + threadIdx.x);
+        if (a.probe.bits && !ht_member(a.probe, key[k])) live &= ~(1u << k);
       }
     }
-#pragma unroll 1
-    for (int k = 0; k < kItems; k++) {
-      if (!((live >> k) & 1)) continue;
-      const uint64_t row = (uint64_t)row0 + k * kT + threadIdx.x;
-      int64_t j = -1;
-      if (a.probe_slot >= 0 && (f.need_slot || !a.probe.bits)) {
-        j = ht_probe(a.probe, key[k]);
-        if (j < 0) continue;
-      }
-      auto col = [&](uint32_t slot) -> int64_t {
-        if (slot >= 32) return __ldg(a.probe.payload + (uint64_t)(slot - 32) * a.probe.slot_cap + j);
-        const alk_colseg& d = s_desc[st][slot];
-        return load_for(d.data, d.bits, d.lower, row);
-      };
-      if (kBuild) {
-        const int64_t sl = ht_insert(a.build, col((uint32_t)a.build_slot));
-        if (sl < 0) continue;
-        inserted++;
-        for (uint32_t p = 0; p < a.build.npay; p++)
-          a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = col((uint32_t)a.pay_src[p]);
-      } else {
-        for (uint32_t g = 0; g < a.nagg; g++) {
-          unsigned long long* dst = (unsigned long long*)(a.acc + (uint64_t)g * a.acc_stride + j);
-          const uint8_t kind = a.agg_kind[g];
-          if (kind == ALK_AGG_COUNT) {
-            atomicAdd(dst, 1ull);
-            continue;
-          }
-          const int64_t v = vm_eval<kT>(s_ins[1 + g], s_n[1 + g], s_res[1 + g], s_consts[1 + g],
-                                        s_regs + threadIdx.x, col);
-          if (kind == ALK_AGG_SUM) atomicAdd(dst, (unsigned long long)v);
-          else if (kind == ALK_AGG_MIN) atomicMin((long long*)dst, (long long)v);
-          else atomicMax((long long*)dst, (long long)v);
-        }
-        if (a.cnt) atomicAdd(a.cnt + j, 1ull);
-      }
-    }
+    emit_hits(a, live, seg, (uint64_t)row0 + threadIdx.x, key);
     // every thread is done with this stage: refill it with the tile two ahead
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -703,12 +693,8 @@ __global__ void __launch_bounds__(kT) k_stage_tma(const __grid_constant__ TmaArg
         __nanosleep(32);
     }
   }
-  for (int o = 16; o; o >>= 1) {
-    rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
-    inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
-  }
+  for (int o = 16; o; o >>= 1) rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
   if ((threadIdx.x & 31) == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
-  if (kBuild && (threadIdx.x & 31) == 0 && inserted) atomicAdd(a.build.nslots, inserted);
 }
 
 // Host: recognise an AND of (column * mul OP constant) tests in a compiled predicate.
@@ -784,27 +770,26 @@ int grid_for(uint64_t n) {
   return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)sms() * 8));
 }
 
-// Static shared memory of k_stage_tma (programs, registers, descriptors) next to the two
-// dynamic stage buffers; the SM offers 227 KB per block.
-constexpr size_t kTmaStaticSmem = 26 * 1024;
+// Static shared memory of k_stage_tma (descriptors, barriers) next to the two dynamic
+// stage buffers; the SM offers 227 KB per block.
+constexpr size_t kTmaStaticSmem = 2 * 1024;
 constexpr size_t kSmemPerBlock = 227 * 1024;
 
-// Launch a stage: the TMA-staged kernel when the predicate is a conjunction and the
-// staged columns fit in shared memory, else the conjunctive kernel with direct loads,
-// else the register-machine kernel. cols is the host descriptor array [ncols][nseg].
+// Launch a stage as two kernels on one stream: the scan (the TMA-staged kernel when the
+// predicate is a conjunction and the staged columns fit in shared memory, else the
+// conjunctive kernel with direct loads, else the register-machine kernel), then the hit
+// kernel over its survivors. cols is the host descriptor array [ncols][nseg].
 template <bool kBuild>
-cudaError_t launch_stage(const StageArgs& a, const alk_program& pred, int need_slot, const alk_colseg* cols,
-                         const uint8_t* seg_mode, int* d_err, cudaStream_t s, alk_event_timer* timer) {
+cudaError_t launch_stage(const StageArgs& a, const alk_program& pred, const alk_colseg* cols,
+                         const uint8_t* seg_mode, cudaStream_t s, alk_event_timer* timer) {
   if (!a.ntiles) return cudaSuccess;
   FastArgs fa;
   fa.a = a;
-  fa.need_slot = need_slot;
   const bool conj = as_conjuncts(pred, fa.conj, &fa.nconj);
   TmaArgs t{};
   bool tma = false;
   if (conj) {
     t.f = fa;
-    t.err = d_err;
     std::vector<uint32_t> st;
     auto add = [&](uint32_t sl) {
       if (std::find(st.begin(), st.end(), sl) == st.end()) st.push_back(sl);
@@ -826,22 +811,24 @@ cudaError_t launch_stage(const StageArgs& a, const alk_program& pred, int need_s
     }
   }
   int occ = 0;
-  int grid;
   if (tma) {
-    cudaFuncSetAttribute(k_stage_tma<kBuild>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * t.stage_bytes);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_tma<kBuild>, kT, 2 * t.stage_bytes);
+    cudaFuncSetAttribute(k_stage_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * t.stage_bytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_tma, kT, 2 * t.stage_bytes);
   } else if (conj) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_fast<kBuild>, kT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_fast, kT, 0);
   } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage<kBuild>, kT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_scan, kT, 0);
   }
-  grid = std::min<int>((int)a.ntiles, sms() * std::max(occ, 1));
+  const int grid = std::min<int>((int)a.ntiles, sms() * std::max(occ, 1));
+  int occ_hits = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_hits, k_stage_hits<kBuild>, kT, 0);
   if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev0, s);
-  if (tma) k_stage_tma<kBuild><<<grid, kT, 2 * t.stage_bytes, s>>>(t);
-  else if (conj) k_stage_fast<kBuild><<<grid, kT, 0, s>>>(fa);
-  else k_stage<kBuild><<<grid, kT, 0, s>>>(a);
+  if (tma) k_stage_tma<<<grid, kT, 2 * t.stage_bytes, s>>>(t);
+  else if (conj) k_stage_fast<<<grid, kT, 0, s>>>(fa);
+  else k_stage_scan<<<grid, kT, 0, s>>>(a);
+  k_stage_hits<kBuild><<<sms() * std::max(occ_hits, 1), kT, 0, s>>>(a);
   if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev1, s);
-  alk::g_kernel_launches++;
+  alk::g_kernel_launches += 2;
   return cudaGetLastError();
 }
 
@@ -1004,9 +991,54 @@ static void patch(StageArgs& a, uint8_t* db) {
   a.progs = (const alk_program*)(db + (uintptr_t)a.progs);
 }
 
+// Uploads a stage's arguments with its counters and hit list in one stream-ordered
+// allocation, runs scan + hit kernels, reads the counters back (one synchronisation).
+// hit_cap 0 (or above the rows scanned) means the rows scanned, which cannot overflow.
+}  // extern "C"
+template <bool kBuild>
+static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* cols, const uint8_t* seg_mode,
+                     const std::vector<uint8_t>& hb, size_t off_x, uint64_t hit_cap, uint64_t* h_rows_in,
+                     uint64_t* h_hits, cudaStream_t s, alk_event_timer* timer) {
+  uint64_t upper = 0;
+  for (uint32_t g = 0; g < a.nseg; g++)
+    if (seg_mode[g]) upper += cols[g].rows;
+  if (hit_cap == 0 || hit_cap > upper) hit_cap = upper;
+  const size_t off_tail = (hb.size() + 15) & ~size_t(15);
+  const size_t off_hits = off_tail + 32;
+  uint8_t* db = nullptr;
+  CK(cudaMallocAsync((void**)&db, off_hits + std::max<uint64_t>(hit_cap, 1) * sizeof(Hit), s));
+  CK(cudaMemcpyAsync(db, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
+  uint8_t* tail = db + off_tail;
+  CK(cudaMemsetAsync(tail, 0, 32, s));
+  patch(a, db);
+  if (kBuild) a.pay_src = (const int32_t*)(db + off_x);
+  else a.agg_kind = db + off_x;
+  a.rows_in = (unsigned long long*)tail;
+  a.hit_count = (unsigned long long*)(tail + 8);
+  a.err = (int*)(tail + 16);
+  a.hits = (Hit*)(db + off_hits);
+  a.hit_cap = hit_cap;
+  CK(launch_stage<kBuild>(a, pred, cols, seg_mode, s, timer));
+  unsigned long long back[3] = {0, 0, 0};
+  CK(cudaMemcpyAsync(back, tail, 24, cudaMemcpyDeviceToHost, s));
+  CK(cudaFreeAsync(db, s));
+  CK(cudaStreamSynchronize(s));
+  if (timer && timer->on && a.ntiles) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, (cudaEvent_t)timer->ev0, (cudaEvent_t)timer->ev1);
+    timer->ms += ms;
+    timer->launches++;
+  }
+  if (h_rows_in) *h_rows_in = back[0];
+  if (h_hits) *h_hits = back[1];
+  return (int)(uint32_t)back[2];
+}
+extern "C" {
+
 int alk_pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
                        const alk_program* pred, const alk_ht* probe, int32_t probe_slot, alk_ht* build,
-                       int32_t build_slot, const int32_t* pay_src, uint64_t* h_rows_in, alk_stream stream) {
+                       int32_t build_slot, const int32_t* pay_src, uint64_t hit_cap, uint64_t* h_rows_in,
+                       uint64_t* h_hits, alk_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (!build || ncols == 0 || ncols > kMaxCols || build_slot < 0 || (uint32_t)build_slot >= ncols) return ALK_ERR_ARG;
   if ((probe_slot >= 0) != (probe != nullptr) || (probe_slot >= 0 && (uint32_t)probe_slot >= ncols))
@@ -1018,46 +1050,27 @@ int alk_pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, co
   }
   alk_program prog{};
   if (pred) prog = *pred;
-  if (!prog_ok(prog, ncols, npay_probe)) return ALK_ERR_ARG;
+  if (!prog_ok(prog, ncols, 0)) return ALK_ERR_ARG;  // the predicate reads scan columns only
   StageArgs a{};
   std::vector<uint8_t> hb;
   size_t off_x;
   int rc = stage_common(cols, ncols, nseg, seg_mode, &prog, 1, hb, a, 4 * 8, &off_x);
   if (rc) return rc;
   std::memcpy(&hb[off_x], pay_src, 4 * build->v.npay);
-  void* db = nullptr;
-  CK(cudaMallocAsync(&db, hb.size() + 32, s));
-  CK(cudaMemcpyAsync(db, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
-  unsigned long long* rows_in = (unsigned long long*)((uint8_t*)db + ((hb.size() + 7) & ~size_t(7)));
-  CK(cudaMemsetAsync(rows_in, 0, 8, s));
-  patch(a, (uint8_t*)db);
-  a.pay_src = (const int32_t*)((uint8_t*)db + off_x);
   a.probe_slot = probe_slot;
   if (probe) a.probe = probe->v;
   a.build_slot = build_slot;
   a.build = build->v;
-  a.rows_in = rows_in;
-  int need_slot = 0;
   for (uint32_t p = 0; p < build->v.npay; p++)
-    if (pay_src[p] >= 32) need_slot = 1;
-  int* d_err = (int*)(rows_in + 1);
-  CK(cudaMemsetAsync(d_err, 0, 8, s));
-  CK(launch_stage<true>(a, prog, need_slot, cols, seg_mode, d_err, s, nullptr));
-  unsigned long long rin = 0;
-  int herr = 0;
-  CK(cudaMemcpyAsync(&rin, rows_in, 8, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, s));
-  CK(cudaFreeAsync(db, s));
-  CK(cudaStreamSynchronize(s));
-  if (h_rows_in) *h_rows_in = rin;
-  return herr;
+    if (pay_src[p] >= 32) a.need_slot = 1;
+  return run_stage<true>(a, prog, cols, seg_mode, hb, off_x, hit_cap, h_rows_in, h_hits, s, nullptr);
 }
 
 int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
                            const alk_program* pred, const alk_ht* probe, int32_t probe_slot,
                            const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg, int64_t* d_acc,
-                           uint64_t acc_stride, uint64_t* d_cnt, uint64_t* h_rows_in, alk_stream stream,
-                           alk_event_timer* timer) {
+                           uint64_t acc_stride, uint64_t* d_cnt, uint64_t hit_cap, uint64_t* h_rows_in,
+                           uint64_t* h_hits, alk_stream stream, alk_event_timer* timer) {
   cudaStream_t s = (cudaStream_t)stream;
   if (!probe || probe_slot < 0 || (uint32_t)probe_slot >= ncols || ncols == 0 || ncols > kMaxCols || nagg > 7)
     return ALK_ERR_ARG;
@@ -1066,48 +1079,27 @@ int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg
   std::vector<alk_program> progs(1 + nagg);
   std::memset(progs.data(), 0, sizeof(alk_program) * progs.size());
   if (pred) progs[0] = *pred;
-  for (uint32_t g = 0; g < nagg; g++)
+  for (uint32_t g = 0; g < nagg; g++) {
+    if (agg_kind[g] > ALK_AGG_MAX) return ALK_ERR_ARG;
     if (agg_kind[g] != ALK_AGG_COUNT) progs[1 + g] = agg_progs[g];
-  for (auto& p : progs)
-    if (!prog_ok(p, ncols, probe->v.npay)) return ALK_ERR_ARG;
+  }
+  for (size_t p = 0; p < progs.size(); p++)
+    if (!prog_ok(progs[p], ncols, p ? probe->v.npay : 0)) return ALK_ERR_ARG;
   StageArgs a{};
   std::vector<uint8_t> hb;
   size_t off_x;
   int rc = stage_common(cols, ncols, nseg, seg_mode, progs.data(), (uint32_t)progs.size(), hb, a, 16, &off_x);
   if (rc) return rc;
   std::memcpy(&hb[off_x], agg_kind, nagg);
-  void* db = nullptr;
-  CK(cudaMallocAsync(&db, hb.size() + 32, s));
-  CK(cudaMemcpyAsync(db, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
-  unsigned long long* rows_in = (unsigned long long*)((uint8_t*)db + ((hb.size() + 7) & ~size_t(7)));
-  CK(cudaMemsetAsync(rows_in, 0, 8, s));
-  patch(a, (uint8_t*)db);
-  a.agg_kind = (const uint8_t*)db + off_x;
   a.probe_slot = probe_slot;
   a.probe = probe->v;
+  a.need_slot = 1;  // accumulators are indexed by the probed key's position
   a.build_slot = -1;
   a.nagg = nagg;
   a.acc = d_acc;
   a.acc_stride = acc_stride;
   a.cnt = (unsigned long long*)d_cnt;
-  a.rows_in = rows_in;
-  int* d_err = (int*)(rows_in + 1);
-  CK(cudaMemsetAsync(d_err, 0, 8, s));
-  CK(launch_stage<false>(a, progs[0], 1, cols, seg_mode, d_err, s, timer));
-  unsigned long long rin = 0;
-  int herr = 0;
-  CK(cudaMemcpyAsync(&rin, rows_in, 8, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, s));
-  CK(cudaFreeAsync(db, s));
-  CK(cudaStreamSynchronize(s));
-  if (timer && timer->on && a.ntiles) {
-    float ms = 0;
-    cudaEventElapsedTime(&ms, (cudaEvent_t)timer->ev0, (cudaEvent_t)timer->ev1);
-    timer->ms += ms;
-    timer->launches++;
-  }
-  if (h_rows_in) *h_rows_in = rin;
-  return herr;
+  return run_stage<false>(a, progs[0], cols, seg_mode, hb, off_x, hit_cap, h_rows_in, h_hits, s, timer);
 }
 
 int alk_fill_i64(int64_t* d, uint64_t n, int64_t v, alk_stream stream) {

@@ -1187,6 +1187,19 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
       return;
     }
   };
+  // Each stage's survivor list is sized the same way from the survivor count its previous
+  // run recorded (rows scanned without one); an overflow reruns it with the exact count.
+  auto with_hits = [&](const std::string& sig, const char* what,
+                       const std::function<int(uint64_t, uint64_t*)>& run) {
+    const std::string key = sig + "#hits";
+    auto it = card_feedback_.find(key);
+    const uint64_t cap = it == card_feedback_.end() ? 0 : it->second + it->second / 4 + 4096;
+    uint64_t hits = 0;
+    int rc = run(cap, &hits);
+    if (rc == ALK_ERR_OVERFLOW) rc = run(hits, &hits);
+    check(rc, what);
+    card_feedback_[key] = hits;
+  };
   auto rows_of = [&](const ScanPlan& p, const std::vector<alk_colseg>& cs) {
     uint64_t n = 0;
     for (uint32_t g = 0; g < p.src->segCount; g++)
@@ -1199,6 +1212,7 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
   };
   HtGuard ht1, ht2;
   alk_ht* last = nullptr;
+  std::string last_sig;  // signature of the stage that built `last`
   std::map<std::string, uint32_t> last_pay;  // payload column index in the last table
   if (J.join_tab_cnt == 2) {
     // stage 1: d2 (innermost right) keyed on st1.rkey, carrying the d2 columns needed later
@@ -1213,10 +1227,11 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     auto cs1 = colsegs(p1);
     std::string sig1 = plan_sig(p1) + "|" + st1.rkey;
     build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)pay1.size(), range_of(p1.src, st1.rkey), [&](alk_ht* h) {
-      check(alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
-                               p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h, (int32_t)k1, src1.data(), nullptr,
-                               (alk_stream)s),
-            "build stage");
+      with_hits(sig1, "build stage", [&](uint64_t cap, uint64_t* hits) {
+        return alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
+                                  p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h, (int32_t)k1, src1.data(), cap,
+                                  nullptr, hits, (alk_stream)s);
+      });
     });
     // stage 2: d1 probes stage 1 on st1.lkey and is keyed on the final build key
     ScanPlan p2 = plan_scan(d1);
@@ -1237,12 +1252,14 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     auto cs2 = colsegs(p2);
     std::string sig2 = plan_sig(p2) + "|" + build_key + "|" + sig1;
     build_stage(ht2, sig2, rows_of(p2, cs2), (uint32_t)payload.size(), range_of(p2.src, build_key), [&](alk_ht* h) {
-      check(alk_pipeline_build(cs2.data(), (uint32_t)p2.slots.size(), p2.src->segCount, p2.mode.data(),
-                               p2.has_pred ? &p2.pred : nullptr, ht1.h, (int32_t)probe2, h, key2, src2.data(),
-                               nullptr, (alk_stream)s),
-            "build stage");
+      with_hits(sig2, "build stage", [&](uint64_t cap, uint64_t* hits) {
+        return alk_pipeline_build(cs2.data(), (uint32_t)p2.slots.size(), p2.src->segCount, p2.mode.data(),
+                                  p2.has_pred ? &p2.pred : nullptr, ht1.h, (int32_t)probe2, h, key2, src2.data(),
+                                  cap, nullptr, hits, (alk_stream)s);
+      });
     });
     last = ht2.h;
+    last_sig = sig2;
   } else {
     ScanPlan p1 = plan_scan(d1);
     uint32_t k1 = p1.slot(build_key);
@@ -1254,12 +1271,14 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     auto cs1 = colsegs(p1);
     std::string sig1 = plan_sig(p1) + "|" + build_key;
     build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)payload.size(), range_of(p1.src, build_key), [&](alk_ht* h) {
-      check(alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
-                               p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h, (int32_t)k1, src1.data(), nullptr,
-                               (alk_stream)s),
-            "build stage");
+      with_hits(sig1, "build stage", [&](uint64_t cap, uint64_t* hits) {
+        return alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
+                                  p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h, (int32_t)k1, src1.data(), cap,
+                                  nullptr, hits, (alk_stream)s);
+      });
     });
     last = ht1.h;
+    last_sig = sig1;
   }
   const uint64_t nslots = alk_ht_slots(last);  // accumulators are indexed by table position
   // ---- probe-aggregate over the fact table
@@ -1293,18 +1312,40 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
   alk_event_timer tm{timing_ ? 1 : 0, ev0_, ev1_, 0.0, 0};
   // the probe-aggregate kernel accumulates into slot-indexed arrays sized for every slot
   if (nslots) {
-    check(alk_pipeline_probe_agg(csf.data(), (uint32_t)pf.slots.size(), pf.src->segCount, pf.mode.data(),
-                                 pf.has_pred ? &pf.pred : nullptr, last, (int32_t)probe_f, progs.data(), kinds.data(),
-                                 (uint32_t)aggs.size(), acc->as<int64_t>(), stride, cnt->as<uint64_t>(), nullptr,
-                                 (alk_stream)s, &tm),
-          "probe-aggregate");
+    with_hits(plan_sig(pf) + "|" + st2.lkey + "|" + last_sig, "probe-aggregate",
+              [&](uint64_t cap, uint64_t* hits) {
+                return alk_pipeline_probe_agg(csf.data(), (uint32_t)pf.slots.size(), pf.src->segCount,
+                                              pf.mode.data(), pf.has_pred ? &pf.pred : nullptr, last, (int32_t)probe_f,
+                                              progs.data(), kinds.data(), (uint32_t)aggs.size(), acc->as<int64_t>(),
+                                              stride, cnt->as<uint64_t>(), cap, nullptr, hits, (alk_stream)s, &tm);
+              });
   }
-  if (timing_) {
+  if (timing_ && nslots) {
     stats_.hot_kernel_ms += tm.ms;
     stats_.hot_kernel_launches += tm.launches;
-    std::vector<uint32_t> all(pf.slots.size());
-    std::iota(all.begin(), all.end(), 0);
-    stats_.hot_kernel_bytes += scan_bytes(pf, all);
+    // Algorithmic bytes: the columns every row needs (predicate and probe key) over all
+    // rows scanned, plus one value of each aggregate input column per survivor.
+    std::set<uint32_t> streamed = {probe_f}, per_hit;
+    auto cols_of = [](const alk_program& p, std::set<uint32_t>& out) {
+      for (uint32_t i = 0; i < p.n_instr; i++) {
+        if (p.ins[i].ka == ALK_K_COL && p.ins[i].a < 32) out.insert(p.ins[i].a);
+        if (p.ins[i].kb == ALK_K_COL && p.ins[i].b < 32) out.insert(p.ins[i].b);
+      }
+    };
+    if (pf.has_pred) cols_of(pf.pred, streamed);
+    for (auto& p : progs) cols_of(p, per_hit);
+    for (uint32_t c : streamed) per_hit.erase(c);
+    const uint64_t hits = card_feedback_[plan_sig(pf) + "|" + st2.lkey + "|" + last_sig + "#hits"];
+    uint64_t hit_bytes = 0;
+    for (uint32_t c : per_hit) {
+      uint32_t w = 1;
+      BaseCol& bc = basecol(pf.src, pf.slots[c]);
+      for (uint32_t g = 0; g < pf.src->segCount; g++)
+        if (pf.mode[g]) w = std::max<uint32_t>(w, bc.segs[g].m.comp_type == 1 ? 8 : bc.segs[g].m.bits / 8);
+      hit_bytes += w;
+    }
+    stats_.hot_kernel_bytes +=
+        scan_bytes(pf, std::vector<uint32_t>(streamed.begin(), streamed.end())) + hits * hit_bytes;
   }
   // ---- F's columns over slots
   auto slot_col = [&](const std::string& alias) -> const int64_t* {

@@ -243,20 +243,29 @@ typedef struct alk_event_timer {
   double ms;
   uint64_t launches;
 } alk_event_timer;
-/* Build stage. Program column operands name scan slots (< 32) or, when probing,
- * payload columns of the probed table (32 + p). pay_src[p] gives each payload column's
- * source the same way. h_rows_in receives the rows scanned. Synchronizes. */
+/* Build stage. The predicate reads scan slots only; payload sources pay_src[p] name scan
+ * slots (< 32) or, when probing, payload columns of the probed table (32 + p).
+ *
+ * Both stages run as a streaming scan that appends surviving rows (predicate true and,
+ * when probing, the key present in the probed table's key bitmap) to a device hit list
+ * of hit_cap entries (16 bytes each; 0 = the rows scanned, which cannot overflow),
+ * followed by one kernel that does the per-survivor work. If more rows survive than
+ * hit_cap, nothing is applied, ALK_ERR_OVERFLOW is returned and *h_hits holds the
+ * exact survivor count for a rerun. h_rows_in receives the rows scanned. Synchronizes. */
 int alk_pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
                        const alk_program* pred, const alk_ht* probe, int32_t probe_slot, alk_ht* build,
-                       int32_t build_slot, const int32_t* pay_src, uint64_t* h_rows_in, alk_stream stream);
+                       int32_t build_slot, const int32_t* pay_src, uint64_t hit_cap, uint64_t* h_rows_in,
+                       uint64_t* h_hits, alk_stream stream);
 /* Probe-aggregate stage: for every surviving row whose probe key hits, aggregate
- * agg_progs[g] (ALK_AGG_SUM / MIN / MAX, or COUNT) into d_acc[g * acc_stride + slot] and
- * count rows into d_cnt[slot]. Accumulators must be initialised by the caller. */
+ * agg_progs[g] (ALK_AGG_SUM / MIN / MAX, or COUNT; column operands: scan slots or probed
+ * payload 32 + p) into d_acc[g * acc_stride + slot] and count rows into d_cnt[slot].
+ * Accumulators must be initialised by the caller. Hit list as for the build stage; the
+ * timer, when on, brackets the scan and hit kernels. */
 int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
                            const alk_program* pred, const alk_ht* probe, int32_t probe_slot,
                            const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg, int64_t* d_acc,
-                           uint64_t acc_stride, uint64_t* d_cnt, uint64_t* h_rows_in, alk_stream stream,
-                           alk_event_timer* timer);
+                           uint64_t acc_stride, uint64_t* d_cnt, uint64_t hit_cap, uint64_t* h_rows_in,
+                           uint64_t* h_hits, alk_stream stream, alk_event_timer* timer);
 int alk_fill_i64(int64_t* d, uint64_t n, int64_t v, alk_stream stream);
 /* Top-k candidates for ORDER BY ... LIMIT k (emit_order + Store LIMIT, operators.cu:1641,
  * cm.cu:1493): every live slot whose ranking value is >= the k-th largest ranking value
