@@ -95,21 +95,20 @@ __device__ __forceinline__ int64_t ht_insert(const HtView& h, int64_t k) {
   return -1;
 }
 
-// A row that survived a stage's scan: its position and its probe key. The scan kernels
-// stream the columns every row needs and append survivors here; the hit kernel then
-// does the per-row random work (hash probe, payload and aggregate-input loads, atomics)
-// for all survivors in parallel, away from the scan's tile pipeline.
-struct Hit {
-  uint64_t pos;  // segment << 32 | row within the segment
-  int64_t key;   // probe key (0 when the stage probes nothing)
-};
+// Rows that survive a stage's scan are appended to a hit list as positions
+// (segment << 32 | row within the segment). The scan kernels stream the columns every row
+// needs; the hit kernel then does the per-row random work (hash probe, payload and
+// aggregate-input loads, atomics) for all survivors in parallel, away from the scan's
+// tile pipeline.
+using Hit = uint64_t;
 
 struct StageArgs {
   const alk_colseg* cols;  // [ncols][nseg]
   uint32_t ncols, nseg;
   const uint8_t* seg_mode;
-  const uint32_t* tile_seg;
-  const uint32_t* tile_row0;
+  // Tiles of kTile rows, numbered across the scanned segments: segment g owns tiles
+  // [seg_tile[g], seg_tile[g + 1]) (none when the zone maps skip it).
+  const uint32_t* seg_tile;  // [nseg + 1]
   uint32_t ntiles;
   const alk_program* progs;  // [0] predicate (n_instr 0 = none), [1 + a] aggregate inputs
   uint32_t nprogs;
@@ -129,37 +128,88 @@ struct StageArgs {
   unsigned long long* rows_in;
   // survivors of the scan
   Hit* hits;
-  uint64_t hit_cap;
-  unsigned long long* hit_count;
+  uint64_t hit_cap;                // entries
+  unsigned long long* hit_count;   // entries reserved (whole chunks)
+  unsigned long long* hit_rows;    // survivors appended
   int* err;
 };
 
-// Appends the thread's live items (rows base + k * kT of segment seg) to the hit list with
-// one atomic per warp. Called by all 32 lanes; entries beyond hit_cap are counted but not
-// written (the hit kernel then refuses the whole list).
-__device__ __forceinline__ void emit_hits(const StageArgs& a, uint32_t live, uint32_t seg, uint64_t base,
-                                          const int64_t (&key)[kItems]) {
+// Segment owning a tile: the g with seg_tile[g] <= tile < seg_tile[g + 1].
+__device__ __forceinline__ uint32_t tile_segment(const uint32_t* seg_tile, uint32_t nseg, uint32_t tile) {
+  uint32_t lo = 0, hi = nseg;  // seg_tile[lo] <= tile < seg_tile[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (seg_tile[mid] <= tile) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Warp-wide exclusive offsets of the lanes' hit counts; returns the warp total. Called by
+// all 32 lanes.
+__device__ __forceinline__ uint32_t warp_offsets(uint32_t n, uint32_t* excl) {
   const uint32_t lane = threadIdx.x & 31;
-  const uint32_t n = __popc(live);
   uint32_t incl = n;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
     if (lane >= (uint32_t)o) incl += y;
   }
-  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-  if (total == 0) return;
-  unsigned long long b = 0;
-  if (lane == 31) b = atomicAdd(a.hit_count, (unsigned long long)total);
-  b = __shfl_sync(0xffffffffu, b, 31);
-  uint64_t p = b + incl - n;
-#pragma unroll
-  for (int k = 0; k < kItems; k++) {
-    if (!((live >> k) & 1)) continue;
-    if (p < a.hit_cap) a.hits[p] = Hit{(uint64_t)seg << 32 | (base + (uint64_t)k * kT), key[k]};
-    p++;
-  }
+  *excl = incl - n;
+  return __shfl_sync(0xffffffffu, incl, 31);
 }
+
+// Each warp appends to chunks of kChunk entries that it reserves with one atomic, so the
+// shared counter sees one atomic per kChunk survivors rather than one per warp and tile.
+// The unused tail of a warp's last chunk holds kNoHit. Entries at or beyond hit_cap are
+// counted but not written (the hit kernel then refuses the whole list), so a list needs
+// room for the survivors plus kChunk entries per warp of the scan.
+constexpr uint32_t kChunk = 128;
+constexpr Hit kNoHit = ~0ull;
+
+struct HitWriter {
+  uint64_t base = 0;            // first entry of the warp's current chunk
+  uint32_t fill = kChunk;       // entries used in it (a full chunk: none reserved yet)
+  unsigned long long rows = 0;  // survivors the warp appended
+
+  // Appends the lanes' live items (rows base_row + k * kStride of segment seg). Warp-wide.
+  template <int kStride>
+  __device__ __forceinline__ void append(const StageArgs& a, uint32_t live, uint32_t seg, uint64_t base_row) {
+    if (!__any_sync(0xffffffffu, live)) return;
+    uint32_t excl;
+    const uint32_t total = warp_offsets(__popc(live), &excl);
+    rows += total;
+    const uint32_t avail = kChunk - fill;
+    unsigned long long nb = 0;
+    if (total > avail) {  // total <= 32 * kItems <= 2 * kChunk: at most two new chunks
+      if ((threadIdx.x & 31) == 0)
+        nb = atomicAdd(a.hit_count, (unsigned long long)(total - avail > kChunk ? 2 * kChunk : kChunk));
+      nb = __shfl_sync(0xffffffffu, nb, 0);
+    }
+    const uint64_t pos0 = (uint64_t)seg << 32 | base_row;
+    uint32_t i = excl;
+    for (uint32_t m = live; m; m &= m - 1, i++) {
+      const uint32_t k = __ffs(m) - 1;
+      const uint64_t slot = i < avail ? base + fill + i : nb + (i - avail);
+      if (slot < a.hit_cap) a.hits[slot] = pos0 + (uint64_t)k * kStride;
+    }
+    if (total > avail) {
+      const uint32_t used = total - avail;  // entries used of the new chunk(s)
+      base = used > kChunk ? nb + kChunk : nb;
+      fill = used > kChunk ? used - kChunk : used;
+    } else {
+      fill += total;
+    }
+  }
+  // Marks the unused tail of the last chunk and publishes the warp's survivor count.
+  // Warp-wide.
+  __device__ __forceinline__ void finish(const StageArgs& a) {
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t i = fill + lane; i < kChunk; i += 32)
+      if (base + i < a.hit_cap) a.hits[base + i] = kNoHit;
+    if (lane == 0 && rows) atomicAdd(a.hit_rows, rows);
+  }
+};
 
 // Register-machine scan for predicates of any shape: the predicate runs per row, the
 // probe key is tested against the probed table's key bitmap, survivors go to the hit list.
@@ -176,20 +226,19 @@ __global__ void __launch_bounds__(kT) k_stage_scan(const StageArgs a) {
     s_res = a.progs[0].result;
   }
   unsigned long long rows_seen = 0;
+  HitWriter hw;
   for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
     __syncthreads();
-    const uint32_t seg = a.tile_seg[tile];
-    const uint32_t row0 = a.tile_row0[tile];
+    const uint32_t seg = tile_segment(a.seg_tile, a.nseg, tile);
+    const uint32_t row0 = (tile - a.seg_tile[seg]) * kTile;
     if (threadIdx.x < a.ncols) s_desc[threadIdx.x] = a.cols[threadIdx.x * a.nseg + seg];
     __syncthreads();
     const uint32_t rows = min((uint32_t)kTile, s_desc[0].rows - row0);
     const bool all = a.seg_mode[seg] == 1 || s_n == 0;
     const uint64_t base = (uint64_t)row0 + threadIdx.x;
     uint32_t live = 0;
-    int64_t key[kItems];
 #pragma unroll 1
     for (int k = 0; k < kItems; k++) {
-      key[k] = 0;
       if (k * kT + threadIdx.x >= rows) continue;
       const uint64_t row = base + (uint64_t)k * kT;
       rows_seen++;
@@ -198,14 +247,12 @@ __global__ void __launch_bounds__(kT) k_stage_scan(const StageArgs a) {
         return load_for(d.data, d.bits, d.lower, row);
       };
       if (!all && vm_eval<kT>(s_ins, s_n, s_res, s_consts, s_regs + threadIdx.x, col) == 0) continue;
-      if (a.probe_slot >= 0) {
-        key[k] = col((uint32_t)a.probe_slot);
-        if (a.probe.bits && !ht_member(a.probe, key[k])) continue;
-      }
+      if (a.probe_slot >= 0 && a.probe.bits && !ht_member(a.probe, col((uint32_t)a.probe_slot))) continue;
       live |= 1u << k;
     }
-    emit_hits(a, live, seg, base, key);
+    hw.append<kT>(a, live, seg, base);
   }
+  hw.finish(a);
   for (int o = 16; o; o >>= 1) rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
   if ((threadIdx.x & 31) == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
 }
@@ -240,19 +287,20 @@ __global__ void __launch_bounds__(kT) k_stage_hits(const StageArgs a) {
   unsigned long long inserted = 0;
   for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
     const Hit h = a.hits[i];
-    const uint32_t seg = (uint32_t)(h.pos >> 32);
-    const uint64_t row = h.pos & 0xffffffffull;
+    if (h == kNoHit) continue;  // unused tail of a warp's last chunk
+    const uint32_t seg = (uint32_t)(h >> 32);
+    const uint64_t row = h & 0xffffffffull;
     int64_t j = -1;
-    if (a.probe_slot >= 0 && (a.need_slot || !a.probe.bits)) {
-      j = ht_probe(a.probe, h.key);
-      if (j < 0) continue;
-    }
     auto col = [&](uint32_t slot) -> int64_t {
       if (slot >= 32) return __ldg(a.probe.payload + (uint64_t)(slot - 32) * a.probe.slot_cap + j);
       const alk_colseg* d = a.cols + (uint64_t)slot * a.nseg + seg;
       const void* data = (const void*)__ldg((const unsigned long long*)&d->data);
       return load_for(data, __ldg(&d->bits), (int64_t)__ldg((const long long*)&d->lower), row);
     };
+    if (a.probe_slot >= 0 && (a.need_slot || !a.probe.bits)) {
+      j = ht_probe(a.probe, col((uint32_t)a.probe_slot));
+      if (j < 0) continue;
+    }
     if (kBuild) {
       const int64_t sl = ht_insert(a.build, col((uint32_t)a.build_slot));
       if (sl < 0) continue;
@@ -360,16 +408,29 @@ __global__ void __launch_bounds__(kT) k_topk_local16(const int64_t* rank, const 
   int64_t t[kTopK];
 #pragma unroll
   for (int i = 0; i < kTopK; i++) t[i] = INT64_MIN;
-  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
-    if (!live[i]) continue;
-    const int64_t v = rank[i];
-    if (v <= t[kTopK - 1]) continue;
+  // kU slots per thread and round, all loads issued before any is used
+  constexpr int kU = 4;
+  const uint64_t step = (uint64_t)gridDim.x * kT * kU;
+  for (uint64_t i0 = blockIdx.x * (uint64_t)kT * kU + threadIdx.x; i0 < n; i0 += step) {
+    unsigned long long l[kU];
+    int64_t r[kU];
 #pragma unroll
-    for (int q = kTopK - 1; q > 0; q--) {  // insert into the descending list, dropping the smallest
-      const int64_t up = t[q - 1];
-      t[q] = v > up ? up : (v > t[q] ? v : t[q]);
+    for (int u = 0; u < kU; u++) {
+      const uint64_t i = i0 + (uint64_t)u * kT;
+      l[u] = i < n ? __ldg(live + i) : 0ull;
+      r[u] = i < n ? __ldg(rank + i) : 0;
     }
-    t[0] = v > t[0] ? v : t[0];
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      const int64_t v = r[u];
+      if (!l[u] || v <= t[kTopK - 1]) continue;
+#pragma unroll
+      for (int q = kTopK - 1; q > 0; q--) {  // insert into the descending list, dropping the smallest
+        const int64_t up = t[q - 1];
+        t[q] = v > up ? up : (v > t[q] ? v : t[q]);
+      }
+      t[0] = v > t[0] ? v : t[0];
+    }
   }
 #pragma unroll
   for (int i = 0; i < kTopK; i++) s_v[threadIdx.x * kTopK + i] = t[i];
@@ -405,6 +466,74 @@ __global__ void __launch_bounds__(kT) k_topk_collect(const int64_t* rank, const 
   }
 }
 
+// Threshold on the device: the k-th largest of the per-block candidate lists (m values,
+// m <= kMergeMax), by a bitonic sort in shared memory.
+constexpr int kMergeThreads = 1024;
+constexpr int kMergeMax = 4096;
+__global__ void __launch_bounds__(kMergeThreads) k_topk_merge(const int64_t* best, uint32_t m, uint32_t k,
+                                                              int64_t* thr) {
+  __shared__ int64_t s_v[kMergeMax];
+  for (uint32_t i = threadIdx.x; i < kMergeMax; i += kMergeThreads) s_v[i] = i < m ? best[i] : INT64_MIN;
+  __syncthreads();
+  for (int size = 2; size <= kMergeMax; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < kMergeMax / 2; i += kMergeThreads) {
+        const int lo = 2 * i - (i & (stride - 1));
+        const int hi = lo + stride;
+        const bool desc = (lo & size) == 0;
+        const int64_t a = s_v[lo], b = s_v[hi];
+        if (desc ? a < b : a > b) {
+          s_v[lo] = b;
+          s_v[hi] = a;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) *thr = s_v[k - 1];
+}
+
+// Collect live slots whose ranking value is at least the device-side threshold.
+__global__ void __launch_bounds__(kT) k_topk_collect_dev(const int64_t* rank, const unsigned long long* live,
+                                                         uint64_t n, const int64_t* thr_p, uint32_t* out,
+                                                         uint64_t cap, unsigned long long* count) {
+  const int64_t thr = *thr_p;
+  constexpr int kU = 4;
+  const uint64_t step = (uint64_t)gridDim.x * kT * kU;
+  for (uint64_t i0 = blockIdx.x * (uint64_t)kT * kU + threadIdx.x; i0 < n; i0 += step) {
+    unsigned long long l[kU];
+    int64_t r[kU];
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      const uint64_t i = i0 + (uint64_t)u * kT;
+      l[u] = i < n ? __ldg(live + i) : 0ull;
+      r[u] = i < n ? __ldg(rank + i) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < kU; u++) {
+      if (!l[u] || r[u] < thr) continue;
+      const unsigned long long p = atomicAdd(count, 1ull);
+      if (p < cap) out[p] = (uint32_t)(i0 + (uint64_t)u * kT);
+    }
+  }
+}
+
+// Rows idx[0 .. min(*count, cap)) of up to kGatherCols int64 columns, column-major into
+// out[c * cap + r].
+constexpr int kGatherCols = 32;
+struct GatherCols {
+  const int64_t* col[kGatherCols];
+};
+__global__ void __launch_bounds__(kT) k_gather_rows(const __grid_constant__ GatherCols g, uint32_t ncols,
+                                                    const uint32_t* idx, const unsigned long long* count,
+                                                    uint64_t cap, int64_t* out) {
+  const uint64_t n = min((uint64_t)*count, cap);
+  for (uint64_t t = blockIdx.x * (uint64_t)kT + threadIdx.x; t < n * ncols; t += (uint64_t)gridDim.x * kT) {
+    const uint64_t c = t / n, r = t - c * n;
+    out[c * cap + r] = g.col[c][idx[r]];
+  }
+}
+
 __global__ void __launch_bounds__(kT) k_live_compact(const unsigned long long* live, uint64_t n, uint32_t* out,
                                                      unsigned long long* count) {
   for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
@@ -427,59 +556,204 @@ struct FastArgs {
   StageArgs a;
   Conj conj[kMaxConj];
   uint32_t nconj;
+  // Per conjunct and segment ([nconj][nseg]), the test rewritten on the stored value x
+  // (value = x + lower): most conjuncts become one unsigned range test on x.
+  const struct ConjSeg* cseg;
+  // Per segment ([nseg]): whether the scan may run in 32-bit arithmetic, and the probe
+  // key's stored-value offset into the probed table's key bitmap.
+  const struct SegPlan* splan;
 };
 
-__device__ __forceinline__ bool cmp_apply(uint32_t op, int64_t a, int64_t b) {
-  switch (op) {
-    case ALK_OP_LT: return a < b;
-    case ALK_OP_GT: return a > b;
-    case ALK_OP_LE: return a <= b;
-    case ALK_OP_GE: return a >= b;
-    case ALK_OP_EQ: return a == b;
-    default: return a != b;
+struct SegPlan {
+  int64_t bit_off;  // bitmap index of a probe key = stored value + bit_off (= lower - kmin)
+  uint32_t narrow;  // every staged column stores <= 32 bits and the 32-bit bitmap index is exact
+  uint32_t pad;
+};
+
+enum : uint32_t { kCjGeneric = 0, kCjIn = 1, kCjOut = 2, kCjNever = 3, kCjAlways = 4 };
+struct ConjSeg {
+  uint64_t lo, span;  // kCjIn: x - lo <= span (unsigned); kCjOut: its negation
+  uint32_t mode, pad;
+};
+
+// Raw-domain form of `(x + lower) * mul OP k` over the stored values x of one segment
+// (0 <= x < 2^bits). Exact whenever mul == 1 and no decoded value can wrap; otherwise
+// the kernels evaluate the conjunct on the decoded value (kCjGeneric).
+ConjSeg conj_seg(const Conj& cj, const alk_colseg& d) {
+  ConjSeg r{0, 0, kCjGeneric, 0};
+  if (cj.mul != 1 || d.bits >= 64) return r;
+  const __int128 xmax = ((__int128)1 << d.bits) - 1;
+  if ((__int128)d.lower + xmax > (__int128)INT64_MAX) return r;
+  const __int128 t = (__int128)cj.k - d.lower;  // value OP k  <=>  x OP t
+  __int128 lo = 0, hi = xmax;
+  bool out = false;
+  switch (cj.op) {
+    case ALK_OP_LT: hi = t - 1; break;
+    case ALK_OP_LE: hi = t; break;
+    case ALK_OP_GT: lo = t + 1; break;
+    case ALK_OP_GE: lo = t; break;
+    case ALK_OP_EQ: lo = hi = t; break;
+    case ALK_OP_NE: lo = hi = t; out = true; break;
+    default: return r;
+  }
+  if (lo < 0) lo = 0;
+  if (hi > xmax) hi = xmax;
+  if (lo > hi) {
+    r.mode = out ? kCjAlways : kCjNever;
+    return r;
+  }
+  r.mode = out ? kCjOut : kCjIn;
+  r.lo = (uint64_t)lo;
+  r.span = (uint64_t)(hi - lo);
+  return r;
+}
+
+template <uint32_t kOp>
+__device__ __forceinline__ uint32_t cmp_items(const uint64_t (&x)[kItems], uint64_t lower, int64_t mul, int64_t c,
+                                              uint32_t live) {
+#pragma unroll
+  for (int k = 0; k < kItems; k++) {
+    const int64_t v = wrap_mul((int64_t)(x[k] + lower), mul);
+    bool ok;
+    if (kOp == ALK_OP_LT) ok = v < c;
+    else if (kOp == ALK_OP_GT) ok = v > c;
+    else if (kOp == ALK_OP_LE) ok = v <= c;
+    else if (kOp == ALK_OP_GE) ok = v >= c;
+    else if (kOp == ALK_OP_EQ) ok = v == c;
+    else ok = v != c;
+    if (!ok) live &= ~(1u << k);
+  }
+  return live;
+}
+
+// Applies one conjunct to the thread's items (stored values x of one segment).
+__device__ __forceinline__ uint32_t conj_filter(const Conj& cj, const ConjSeg& cs, int64_t lower,
+                                                const uint64_t (&x)[kItems], uint32_t live) {
+  switch (cs.mode) {
+    case kCjAlways: return live;
+    case kCjNever: return 0;
+    case kCjIn:
+#pragma unroll
+      for (int k = 0; k < kItems; k++)
+        if (x[k] - cs.lo > cs.span) live &= ~(1u << k);
+      return live;
+    case kCjOut:
+#pragma unroll
+      for (int k = 0; k < kItems; k++)
+        if (x[k] - cs.lo <= cs.span) live &= ~(1u << k);
+      return live;
+    default:
+      switch (cj.op) {
+        case ALK_OP_LT: return cmp_items<ALK_OP_LT>(x, (uint64_t)lower, cj.mul, cj.k, live);
+        case ALK_OP_GT: return cmp_items<ALK_OP_GT>(x, (uint64_t)lower, cj.mul, cj.k, live);
+        case ALK_OP_LE: return cmp_items<ALK_OP_LE>(x, (uint64_t)lower, cj.mul, cj.k, live);
+        case ALK_OP_GE: return cmp_items<ALK_OP_GE>(x, (uint64_t)lower, cj.mul, cj.k, live);
+        case ALK_OP_EQ: return cmp_items<ALK_OP_EQ>(x, (uint64_t)lower, cj.mul, cj.k, live);
+        default: return cmp_items<ALK_OP_NE>(x, (uint64_t)lower, cj.mul, cj.k, live);
+      }
   }
 }
 
-// Values of one column for the thread's items (rows base + k * kT), live items only.
-__device__ __forceinline__ void load_batch(const alk_colseg& d, uint64_t base, uint32_t live, int64_t (&v)[kItems]) {
-  const uint64_t lo = (uint64_t)d.lower;
-  switch (d.bits) {
-    case 8: {
-      const uint8_t* p = (const uint8_t*)d.data + base;
+// Drops the thread's items whose probe key (stored value x + lower) is absent from the
+// probed table's key bitmap.
+__device__ __forceinline__ uint32_t probe_filter(const HtView& h, int64_t lower, const uint64_t (&x)[kItems],
+                                                 uint32_t live) {
+#pragma unroll
+  for (int k = 0; k < kItems; k++)
+    if (((live >> k) & 1) && !ht_member(h, (int64_t)(x[k] + (uint64_t)lower))) live &= ~(1u << k);
+  return live;
+}
+
+// 32-bit forms for segments whose staged columns store at most 32 bits: range tests and
+// bitmap indexes on the stored values need no 64-bit arithmetic.
+__device__ __forceinline__ uint32_t conj_filter32(const Conj& cj, const ConjSeg& cs, int64_t lower,
+                                                  const uint32_t (&x)[kItems], uint32_t live) {
+  const uint32_t lo = (uint32_t)cs.lo, span = (uint32_t)cs.span;
+  switch (cs.mode) {
+    case kCjAlways: return live;
+    case kCjNever: return 0;
+    case kCjIn:
 #pragma unroll
       for (int k = 0; k < kItems; k++)
-        if ((live >> k) & 1) v[k] = (int64_t)((uint64_t)__ldg(p + k * kT) + lo);
+        if (x[k] - lo > span) live &= ~(1u << k);
+      return live;
+    case kCjOut:
+#pragma unroll
+      for (int k = 0; k < kItems; k++)
+        if (x[k] - lo <= span) live &= ~(1u << k);
+      return live;
+    default: {
+      uint64_t w[kItems];
+#pragma unroll
+      for (int k = 0; k < kItems; k++) w[k] = x[k];
+      return conj_filter(cj, cs, lower, w, live);
+    }
+  }
+}
+__device__ __forceinline__ uint32_t probe_filter32(const HtView& h, uint32_t bit_off, const uint32_t (&x)[kItems],
+                                                   uint32_t live) {
+  const uint32_t nbits = (uint32_t)h.nbits;
+#pragma unroll
+  for (int k = 0; k < kItems; k++) {
+    const uint32_t o = x[k] + bit_off;
+    if (((live >> k) & 1) && (o >= nbits || !((__ldg(h.bits + (o >> 5)) >> (o & 31)) & 1u))) live &= ~(1u << k);
+  }
+  return live;
+}
+template <int kStride>
+__device__ __forceinline__ void load_raw32(const void* p, uint32_t bits, uint32_t i0, uint32_t (&x)[kItems]) {
+  switch (bits) {
+    case 8: {
+      const uint8_t* q = (const uint8_t*)p + i0;
+#pragma unroll
+      for (int k = 0; k < kItems; k++) x[k] = q[k * kStride];
     } break;
     case 16: {
-      const uint16_t* p = (const uint16_t*)d.data + base;
+      const uint16_t* q = (const uint16_t*)p + i0;
 #pragma unroll
-      for (int k = 0; k < kItems; k++)
-        if ((live >> k) & 1) v[k] = (int64_t)((uint64_t)__ldg(p + k * kT) + lo);
-    } break;
-    case 32: {
-      const uint32_t* p = (const uint32_t*)d.data + base;
-#pragma unroll
-      for (int k = 0; k < kItems; k++)
-        if ((live >> k) & 1) v[k] = (int64_t)((uint64_t)__ldg(p + k * kT) + lo);
+      for (int k = 0; k < kItems; k++) x[k] = q[k * kStride];
     } break;
     default: {
-      const unsigned long long* p = (const unsigned long long*)d.data + base;
+      const uint32_t* q = (const uint32_t*)p + i0;
 #pragma unroll
-      for (int k = 0; k < kItems; k++)
-        if ((live >> k) & 1) v[k] = (int64_t)((uint64_t)__ldg(p + k * kT) + lo);
+      for (int k = 0; k < kItems; k++) x[k] = q[k * kStride];
     } break;
+  }
+}
+
+// Stored values of one column for the thread's items (elements i0 + k * kStride); from
+// global memory only the live items are read.
+template <bool kGlobal, int kStride, class T>
+__device__ __forceinline__ void load_raw_t(const T* p, uint32_t live, uint64_t (&x)[kItems]) {
+#pragma unroll
+  for (int k = 0; k < kItems; k++) {
+    if (kGlobal) x[k] = ((live >> k) & 1) ? (uint64_t)__ldg(p + k * kStride) : 0;
+    else x[k] = (uint64_t)p[k * kStride];
+  }
+}
+template <bool kGlobal, int kStride = kT>
+__device__ __forceinline__ void load_raw(const void* p, uint32_t bits, uint64_t i0, uint32_t live,
+                                         uint64_t (&x)[kItems]) {
+  switch (bits) {
+    case 8: load_raw_t<kGlobal, kStride>((const uint8_t*)p + i0, live, x); break;
+    case 16: load_raw_t<kGlobal, kStride>((const uint16_t*)p + i0, live, x); break;
+    case 32: load_raw_t<kGlobal, kStride>((const uint32_t*)p + i0, live, x); break;
+    default: load_raw_t<kGlobal, kStride>((const unsigned long long*)p + i0, live, x); break;
   }
 }
 
 __global__ void __launch_bounds__(kT) k_stage_fast(const __grid_constant__ FastArgs f) {
   const StageArgs& a = f.a;
   __shared__ alk_colseg s_desc[kMaxCols];
+  __shared__ ConjSeg s_cs[kMaxConj];
   unsigned long long rows_seen = 0;
+  HitWriter hw;
   for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
     __syncthreads();
-    const uint32_t seg = a.tile_seg[tile];
-    const uint32_t row0 = a.tile_row0[tile];
+    const uint32_t seg = tile_segment(a.seg_tile, a.nseg, tile);
+    const uint32_t row0 = (tile - a.seg_tile[seg]) * kTile;
     if (threadIdx.x < a.ncols) s_desc[threadIdx.x] = a.cols[threadIdx.x * a.nseg + seg];
+    if (threadIdx.x < f.nconj) s_cs[threadIdx.x] = f.cseg[threadIdx.x * a.nseg + seg];
     __syncthreads();
     const uint32_t rows = min((uint32_t)kTile, s_desc[0].rows - row0);
     const uint64_t base = (uint64_t)row0 + threadIdx.x;
@@ -488,41 +762,38 @@ __global__ void __launch_bounds__(kT) k_stage_fast(const __grid_constant__ FastA
     for (int k = 0; k < kItems; k++)
       if (k * kT + threadIdx.x < rows) live |= 1u << k;
     rows_seen += __popc(live);
+    uint64_t x[kItems];
     if (a.seg_mode[seg] != 1) {
       for (uint32_t c = 0; c < f.nconj; c++) {
-        const Conj cj = f.conj[c];
-        int64_t v[kItems];
-        load_batch(s_desc[cj.slot], base, live, v);
-#pragma unroll
-        for (int k = 0; k < kItems; k++)
-          if (((live >> k) & 1) && !cmp_apply(cj.op, wrap_mul(v[k], cj.mul), cj.k)) live &= ~(1u << k);
+        const alk_colseg& d = s_desc[f.conj[c].slot];
+        load_raw<true>(d.data, d.bits, base, live, x);
+        live = conj_filter(f.conj[c], s_cs[c], d.lower, x, live);
       }
     }
-    int64_t key[kItems];
-#pragma unroll
-    for (int k = 0; k < kItems; k++) key[k] = 0;
-    if (live && a.probe_slot >= 0) {
-      load_batch(s_desc[a.probe_slot], base, live, key);
-      if (a.probe.bits) {
-#pragma unroll
-        for (int k = 0; k < kItems; k++)
-          if (((live >> k) & 1) && !ht_member(a.probe, key[k])) live &= ~(1u << k);
-      }
+    if (live && a.probe_slot >= 0 && a.probe.bits) {
+      const alk_colseg& d = s_desc[a.probe_slot];
+      load_raw<true>(d.data, d.bits, base, live, x);
+      live = probe_filter(a.probe, d.lower, x, live);
     }
-    emit_hits(a, live, seg, base, key);
+    hw.append<kT>(a, live, seg, base);
   }
+  hw.finish(a);
   for (int o = 16; o; o >>= 1) rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
   if ((threadIdx.x & 31) == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
 }
 
 // ---------------------------------------------------------------- TMA-staged stage
-// The same stage with the columns every row needs (conjunct columns and the probe key)
-// brought into shared memory by bulk asynchronous copies (cp.async.bulk, completion on an
-// mbarrier), two tiles in flight per block: the copy engine keeps HBM busy while the
-// block evaluates the previous tile. Columns read only for matching rows (payload,
-// aggregate inputs) are read from global memory.
+// The conjunctive scan with the columns every row needs (conjunct columns and the probe
+// key) brought into shared memory by bulk asynchronous copies (cp.async.bulk, completion
+// on a "full" mbarrier). One producer warp keeps kStages tiles in flight per block; kCW
+// consumer warps each evaluate a 256-row slice of a tile and release the stage through
+// an "empty" mbarrier, so no block-wide barrier sits in the loop and a warp waiting on
+// its key-bitmap loads or its hit-list atomic does not hold the others back. Columns read
+// only for surviving rows (payload, aggregate inputs) are left to the hit kernel.
 constexpr int kStaged = 6;          // staged columns at most
 constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr int kCW = kTile / (32 * kItems);   // consumer warps
+constexpr int kTmaThreads = (kCW + 1) * 32;  // + one producer warp
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
@@ -547,154 +818,178 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Bounded wait of one thread for a phase; false when the limit expired.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  for (uint32_t spins = 0; spins < kWaitLimit; spins++) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (spins > 16) __nanosleep(32);
+  }
+  return false;
+}
+// Bounded wait of a whole warp; the outcome is the same in every lane.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity) {
+  bool done = false;
+  for (uint32_t spins = 0; spins < kWaitLimit; spins++) {
+    if (!done) done = mbar_try_wait(bar, parity);
+    if (__all_sync(0xffffffffu, done)) return true;
+    if (spins > 16) __nanosleep(32);
+  }
+  return false;
+}
+
+constexpr uint32_t kStages = 4;  // tiles in flight per block
 
 struct TmaArgs {
   FastArgs f;
   uint32_t nstaged;
   uint32_t staged_slot[kStaged];  // scan slot of each staged column
-  uint32_t stage_bytes;           // shared bytes of one stage (all staged columns, 2048 rows)
+  uint32_t col_off[kStaged];      // byte offset of each staged column in a stage buffer
+  uint32_t stage_bytes;           // shared bytes of one stage (all staged columns, kTile rows)
+  uint32_t conj_st[kMaxConj];     // staged index of each conjunct's column
+  int32_t probe_st;               // staged index of the probe key (-1: no probe)
 };
 
-__global__ void __launch_bounds__(kT) k_stage_tma(const __grid_constant__ TmaArgs t) {
+// Dynamic shared memory of k_stage_tma: kStages stage buffers, then the segment tile
+// prefix, the staged columns' per-segment descriptors and the conjuncts' per-segment
+// raw-domain tests, so that issuing and evaluating a tile read shared memory only.
+__host__ __device__ inline uint32_t tma_tile_table_off(uint32_t stage_bytes) { return kStages * stage_bytes; }
+__host__ __device__ inline uint32_t tma_desc_off(uint32_t stage_bytes, uint32_t nseg) {
+  return (tma_tile_table_off(stage_bytes) + (nseg + 1) * 4 + 15) & ~15u;
+}
+__host__ __device__ inline uint32_t tma_cseg_off(uint32_t stage_bytes, uint32_t nseg, uint32_t nstaged) {
+  return tma_desc_off(stage_bytes, nseg) + nstaged * nseg * (uint32_t)sizeof(alk_colseg);
+}
+__host__ __device__ inline uint32_t tma_splan_off(uint32_t stage_bytes, uint32_t nseg, uint32_t nstaged,
+                                                  uint32_t nconj) {
+  return tma_cseg_off(stage_bytes, nseg, nstaged) + nconj * nseg * (uint32_t)sizeof(ConjSeg);
+}
+__host__ __device__ inline uint32_t tma_smem_bytes(uint32_t stage_bytes, uint32_t nseg, uint32_t nstaged,
+                                                   uint32_t nconj) {
+  return tma_splan_off(stage_bytes, nseg, nstaged, nconj) + nseg * (uint32_t)sizeof(SegPlan);
+}
+
+__global__ void __launch_bounds__(kTmaThreads) k_stage_tma(const __grid_constant__ TmaArgs t) {
   const FastArgs& f = t.f;
   const StageArgs& a = f.a;
   extern __shared__ __align__(128) unsigned char s_dyn[];
-  __shared__ alk_colseg s_desc[2][kMaxCols];
-  __shared__ uint32_t s_off[2][kStaged];  // byte offset of each staged column in a stage buffer
-  __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ __align__(8) uint64_t s_full[kStages], s_empty[kStages];
   __shared__ int s_abort;
-  // probe key and conjunct columns -> staged index
-  int probe_st = -1;
-  int conj_st[kMaxConj];
-  for (uint32_t c = 0; c < kMaxConj; c++) conj_st[c] = -1;
-  for (uint32_t i = 0; i < t.nstaged; i++) {
-    if (a.probe_slot >= 0 && t.staged_slot[i] == (uint32_t)a.probe_slot) probe_st = (int)i;
-    for (uint32_t c = 0; c < f.nconj; c++)
-      if (t.staged_slot[i] == f.conj[c].slot) conj_st[c] = (int)i;
-  }
+  uint32_t* s_tile = (uint32_t*)(s_dyn + tma_tile_table_off(t.stage_bytes));
+  alk_colseg* s_cd = (alk_colseg*)(s_dyn + tma_desc_off(t.stage_bytes, a.nseg));  // [nstaged][nseg]
+  ConjSeg* s_cs = (ConjSeg*)(s_dyn + tma_cseg_off(t.stage_bytes, a.nseg, t.nstaged));  // [nconj][nseg]
+  for (uint32_t i = threadIdx.x; i <= a.nseg; i += kTmaThreads) s_tile[i] = a.seg_tile[i];
+  for (uint32_t i = threadIdx.x; i < t.nstaged * a.nseg; i += kTmaThreads)
+    s_cd[i] = a.cols[t.staged_slot[i / a.nseg] * a.nseg + i % a.nseg];
+  for (uint32_t i = threadIdx.x; i < f.nconj * a.nseg; i += kTmaThreads) s_cs[i] = f.cseg[i];
+  SegPlan* s_sp = (SegPlan*)(s_dyn + tma_splan_off(t.stage_bytes, a.nseg, t.nstaged, f.nconj));  // [nseg]
+  for (uint32_t i = threadIdx.x; i < a.nseg; i += kTmaThreads) s_sp[i] = f.splan[i];
   if (threadIdx.x == 0) {
     s_abort = 0;
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
+    for (uint32_t i = 0; i < kStages; i++) {
+      mbar_init(&s_full[i], 1);
+      mbar_init(&s_empty[i], kCW);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  // issue the copies of this block's local tile number `it` into stage it & 1 (thread 0)
-  auto issue = [&](uint32_t it) {
-    const uint32_t tile = blockIdx.x + it * gridDim.x;
-    if (tile >= a.ntiles) return;
-    const uint32_t st = it & 1;
-    const uint32_t seg = a.tile_seg[tile];
-    const uint32_t row0 = a.tile_row0[tile];
-    for (uint32_t c = 0; c < a.ncols; c++) s_desc[st][c] = a.cols[c * a.nseg + seg];
-    const uint32_t rows = min((uint32_t)kTile, s_desc[st][0].rows - row0);
-    uint32_t off = 0, total = 0;
-    for (uint32_t i = 0; i < t.nstaged; i++) {
-      const alk_colseg& d = s_desc[st][t.staged_slot[i]];
-      const uint32_t w = d.bits / 8;
-      const uint32_t bytes = (rows * w + 15) & ~15u;
-      s_off[st][i] = off;
-      off += (kTile * w + 127) & ~127u;
-      total += bytes;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  volatile int* abort_flag = &s_abort;
+
+  if (warp == kCW) {
+    // ---- producer: one thread issues the bulk copies of the block's tiles
+    if (lane != 0) return;
+    uint32_t issued = 0;
+    for (uint32_t it = 0;; it++) {
+      const uint32_t tile = blockIdx.x + it * gridDim.x;
+      if (tile >= a.ntiles || *abort_flag) break;
+      const uint32_t st = it % kStages;
+      if (it >= kStages && !mbar_wait(&s_empty[st], (it / kStages - 1) & 1)) {
+        atomicExch(a.err, ALK_ERR_TIMEOUT);
+        *abort_flag = 1;
+        break;
+      }
+      const uint32_t seg = tile_segment(s_tile, a.nseg, tile);
+      const uint32_t row0 = (tile - s_tile[seg]) * kTile;
+      const uint32_t rows = min((uint32_t)kTile, s_cd[seg].rows - row0);
+      uint32_t total = 0;
+      for (uint32_t i = 0; i < t.nstaged; i++) total += (rows * (s_cd[i * a.nseg + seg].bits / 8) + 15) & ~15u;
+      unsigned char* buf = s_dyn + st * t.stage_bytes;
+      mbar_expect_tx(&s_full[st], total);
+      for (uint32_t i = 0; i < t.nstaged; i++) {
+        const alk_colseg& d = s_cd[i * a.nseg + seg];
+        const uint32_t w = d.bits / 8;
+        bulk_g2s(buf + t.col_off[i], (const unsigned char*)d.data + (uint64_t)row0 * w, (rows * w + 15) & ~15u,
+                 &s_full[st]);
+      }
+      issued = it + 1;
     }
-    unsigned char* buf = s_dyn + st * t.stage_bytes;
-    mbar_expect_tx(&s_bar[st], total);
-    for (uint32_t i = 0; i < t.nstaged; i++) {
-      const alk_colseg& d = s_desc[st][t.staged_slot[i]];
-      const uint32_t w = d.bits / 8;
-      const uint32_t bytes = (rows * w + 15) & ~15u;
-      bulk_g2s(buf + s_off[st][i], (const unsigned char*)d.data + (uint64_t)row0 * w, bytes, &s_bar[st]);
-    }
-  };
-  if (threadIdx.x == 0) {
-    issue(0);
-    issue(1);
+    // every copy issued has landed before the block may exit (bounded)
+    for (uint32_t it = issued > kStages ? issued - kStages : 0; it < issued; it++)
+      mbar_wait(&s_full[it % kStages], (it / kStages) & 1);
+    return;
   }
-  __syncthreads();
+
+  // ---- consumers: warp `warp` owns rows warp * 256 + k * 32 + lane of every tile
   unsigned long long rows_seen = 0;
-  uint32_t abort_it = 0;
+  HitWriter hw;
+  const uint32_t r0 = warp * (32 * kItems) + lane;
   for (uint32_t it = 0;; it++) {
     const uint32_t tile = blockIdx.x + it * gridDim.x;
-    if (tile >= a.ntiles) break;
-    const uint32_t st = it & 1;
-    // wait for this stage's copies (bounded)
-    if (threadIdx.x == 0) {
-      uint32_t spins = 0;
-      while (!mbar_try_wait(&s_bar[st], (it >> 1) & 1)) {
-        if (++spins > kWaitLimit) {
-          atomicExch(a.err, ALK_ERR_TIMEOUT);
-          s_abort = 1;
-          break;
-        }
-        __nanosleep(32);
+    if (tile >= a.ntiles || __any_sync(0xffffffffu, *abort_flag)) break;
+    const uint32_t st = it % kStages;
+    if (!mbar_wait_warp(&s_full[st], (it / kStages) & 1)) {
+      if (lane == 0) {
+        atomicExch(a.err, ALK_ERR_TIMEOUT);
+        *abort_flag = 1;
       }
-    }
-    __syncthreads();
-    if (s_abort) {
-      abort_it = it;
       break;
     }
-    const uint32_t seg = a.tile_seg[tile];
-    const uint32_t row0 = a.tile_row0[tile];
-    const uint32_t rows = min((uint32_t)kTile, s_desc[st][0].rows - row0);
+    const uint32_t seg = tile_segment(s_tile, a.nseg, tile);
+    const uint32_t row0 = (tile - s_tile[seg]) * kTile;
+    const uint32_t rows = min((uint32_t)kTile, s_cd[seg].rows - row0);
     const unsigned char* buf = s_dyn + st * t.stage_bytes;
-    auto staged = [&](int i, uint32_t r) -> int64_t {
-      const alk_colseg& d = s_desc[st][t.staged_slot[i]];
-      const unsigned char* p = buf + s_off[st][i];
-      uint64_t x;
-      switch (d.bits) {
-        case 8: x = p[r]; break;
-        case 16: x = ((const uint16_t*)p)[r]; break;
-        case 32: x = ((const uint32_t*)p)[r]; break;
-        default: x = ((const unsigned long long*)p)[r]; break;
-      }
-      return (int64_t)(x + (uint64_t)d.lower);
-    };
     uint32_t live = 0;
 #pragma unroll
     for (int k = 0; k < kItems; k++)
-      if (k * kT + threadIdx.x < rows) live |= 1u << k;
+      if (r0 + k * 32 < rows) live |= 1u << k;
     rows_seen += __popc(live);
-    if (a.seg_mode[seg] != 1) {
+    const SegPlan sp = s_sp[seg];
+    if (sp.narrow) {
+      uint32_t x[kItems];
       for (uint32_t c = 0; c < f.nconj; c++) {
-        const Conj cj = f.conj[c];
-#pragma unroll
-        for (int k = 0; k < kItems; k++)
-          if (((live >> k) & 1) &&
-              !cmp_apply(cj.op, wrap_mul(staged(conj_st[c], k * kT + threadIdx.x), cj.mul), cj.k))
-            live &= ~(1u << k);
+        const alk_colseg& d = s_cd[t.conj_st[c] * a.nseg + seg];
+        load_raw32<32>(buf + t.col_off[t.conj_st[c]], d.bits, r0, x);
+        live = conj_filter32(f.conj[c], s_cs[c * a.nseg + seg], d.lower, x, live);
+      }
+      if (t.probe_st >= 0 && a.probe.bits) {
+        const alk_colseg& d = s_cd[t.probe_st * a.nseg + seg];
+        load_raw32<32>(buf + t.col_off[t.probe_st], d.bits, r0, x);
+        live = probe_filter32(a.probe, (uint32_t)sp.bit_off, x, live);
+      }
+    } else {
+      uint64_t x[kItems];
+      for (uint32_t c = 0; c < f.nconj; c++) {
+        const alk_colseg& d = s_cd[t.conj_st[c] * a.nseg + seg];
+        load_raw<false, 32>(buf + t.col_off[t.conj_st[c]], d.bits, r0, live, x);
+        live = conj_filter(f.conj[c], s_cs[c * a.nseg + seg], d.lower, x, live);
+      }
+      if (t.probe_st >= 0 && a.probe.bits) {
+        const alk_colseg& d = s_cd[t.probe_st * a.nseg + seg];
+        load_raw<false, 32>(buf + t.col_off[t.probe_st], d.bits, r0, live, x);
+        live = probe_filter(a.probe, d.lower, x, live);
       }
     }
-    int64_t key[kItems];
-#pragma unroll
-    for (int k = 0; k < kItems; k++) key[k] = 0;
-    if (live && probe_st >= 0) {
-#pragma unroll
-      for (int k = 0; k < kItems; k++) {
-        if (!((live >> k) & 1)) continue;
-        key[k] = staged(probe_st, k * kT + threadIdx.x);
-        if (a.probe.bits && !ht_member(a.probe, key[k])) live &= ~(1u << k);
-      }
-    }
-    emit_hits(a, live, seg, (uint64_t)row0 + threadIdx.x, key);
-    // every thread is done with this stage: refill it with the tile two ahead
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(it + 2);
-    }
+    // the slice's values are in registers: release the stage to the producer
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&s_empty[st]);
+    hw.append<32>(a, live, seg, (uint64_t)row0 + r0);
   }
-  // an aborted block waits (bounded) for the copies still in flight (local tiles abort_it
-  // and abort_it + 1) before it exits
-  if (s_abort && threadIdx.x == 0) {
-    for (uint32_t it = abort_it; it < abort_it + 2; it++) {
-      if (blockIdx.x + it * gridDim.x >= a.ntiles) break;
-      for (uint32_t spins = 0; spins < kWaitLimit && !mbar_try_wait(&s_bar[it & 1], (it >> 1) & 1); spins++)
-        __nanosleep(32);
-    }
-  }
+  hw.finish(a);
   for (int o = 16; o; o >>= 1) rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
-  if ((threadIdx.x & 31) == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
+  if (lane == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
 }
 
 // Host: recognise an AND of (column * mul OP constant) tests in a compiled predicate.
@@ -770,22 +1065,21 @@ int grid_for(uint64_t n) {
   return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)sms() * 8));
 }
 
-// Static shared memory of k_stage_tma (descriptors, barriers) next to the two dynamic
-// stage buffers; the SM offers 227 KB per block.
+// Static shared memory of k_stage_tma (barriers) next to its dynamic stage buffers and
+// tables; the SM offers 227 KB per block.
 constexpr size_t kTmaStaticSmem = 2 * 1024;
 constexpr size_t kSmemPerBlock = 227 * 1024;
 
 // Launch a stage as two kernels on one stream: the scan (the TMA-staged kernel when the
 // predicate is a conjunction and the staged columns fit in shared memory, else the
 // conjunctive kernel with direct loads, else the register-machine kernel), then the hit
-// kernel over its survivors. cols is the host descriptor array [ncols][nseg].
+// kernel over its survivors. cols is the host descriptor array [ncols][nseg]; fa holds
+// the device arguments and, when conj, the predicate's conjuncts.
 template <bool kBuild>
-cudaError_t launch_stage(const StageArgs& a, const alk_program& pred, const alk_colseg* cols,
-                         const uint8_t* seg_mode, cudaStream_t s, alk_event_timer* timer) {
+cudaError_t launch_stage(const FastArgs& fa, bool conj, const alk_colseg* cols, const uint8_t* seg_mode,
+                         cudaStream_t s, alk_event_timer* timer) {
+  const StageArgs& a = fa.a;
   if (!a.ntiles) return cudaSuccess;
-  FastArgs fa;
-  fa.a = a;
-  const bool conj = as_conjuncts(pred, fa.conj, &fa.nconj);
   TmaArgs t{};
   bool tma = false;
   if (conj) {
@@ -796,34 +1090,51 @@ cudaError_t launch_stage(const StageArgs& a, const alk_program& pred, const alk_
     };
     for (uint32_t c = 0; c < fa.nconj; c++) add(fa.conj[c].slot);
     if (a.probe_slot >= 0) add((uint32_t)a.probe_slot);
+    // bulk copies need 16-byte aligned sources (row0 * width is a multiple of kTile)
+    bool aligned = true;
     uint32_t bytes = 0;
-    for (uint32_t sl : st) {
+    for (size_t i = 0; i < st.size() && i < (size_t)kStaged; i++) {
       uint32_t w = 1;
-      for (uint32_t g = 0; g < a.nseg; g++)
-        if (seg_mode[g]) w = std::max<uint32_t>(w, cols[sl * a.nseg + g].bits / 8);
+      for (uint32_t g = 0; g < a.nseg; g++) {
+        if (!seg_mode[g]) continue;
+        const alk_colseg& d = cols[st[i] * a.nseg + g];
+        w = std::max<uint32_t>(w, d.bits / 8);
+        if ((uintptr_t)d.data & 15) aligned = false;
+      }
+      t.col_off[i] = bytes;
       bytes += (kTile * w + 127) & ~127u;
     }
-    if (!st.empty() && st.size() <= (size_t)kStaged && kTmaStaticSmem + 2 * (size_t)bytes <= kSmemPerBlock) {
+    if (!st.empty() && st.size() <= (size_t)kStaged && aligned &&
+        kTmaStaticSmem + tma_smem_bytes(bytes, a.nseg, (uint32_t)st.size(), fa.nconj) <= kSmemPerBlock) {
       t.nstaged = (uint32_t)st.size();
-      for (size_t i = 0; i < st.size(); i++) t.staged_slot[i] = st[i];
+      t.probe_st = -1;
+      for (size_t i = 0; i < st.size(); i++) {
+        t.staged_slot[i] = st[i];
+        if (a.probe_slot >= 0 && st[i] == (uint32_t)a.probe_slot) t.probe_st = (int32_t)i;
+        for (uint32_t c = 0; c < fa.nconj; c++)
+          if (fa.conj[c].slot == st[i]) t.conj_st[c] = (uint32_t)i;
+      }
       t.stage_bytes = bytes;
       tma = true;
     }
   }
   int occ = 0;
+  const uint32_t tma_smem = tma ? tma_smem_bytes(t.stage_bytes, a.nseg, t.nstaged, fa.nconj) : 0;
   if (tma) {
-    cudaFuncSetAttribute(k_stage_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * t.stage_bytes);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_tma, kT, 2 * t.stage_bytes);
+    cudaFuncSetAttribute(k_stage_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem);
+    cudaFuncSetAttribute(k_stage_tma, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_tma, kTmaThreads, tma_smem);
   } else if (conj) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_fast, kT, 0);
   } else {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_scan, kT, 0);
   }
-  const int grid = std::min<int>((int)a.ntiles, sms() * std::max(occ, 1));
+  // at most 8 blocks per SM of 8 appending warps each: the hit list's chunk slack assumes it
+  const int grid = std::min<int>((int)a.ntiles, sms() * std::min(std::max(occ, 1), 8));
   int occ_hits = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_hits, k_stage_hits<kBuild>, kT, 0);
   if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev0, s);
-  if (tma) k_stage_tma<<<grid, kT, 2 * t.stage_bytes, s>>>(t);
+  if (tma) k_stage_tma<<<grid, kTmaThreads, tma_smem, s>>>(t);
   else if (conj) k_stage_fast<<<grid, kT, 0, s>>>(fa);
   else k_stage_scan<<<grid, kT, 0, s>>>(a);
   k_stage_hits<kBuild><<<sms() * std::max(occ_hits, 1), kT, 0, s>>>(a);
@@ -936,6 +1247,8 @@ int alk_ht_info(const alk_ht* h, uint64_t* nslots, int* flags, alk_stream stream
 
 uint64_t alk_ht_slots(const alk_ht* h) { return h ? h->v.slot_cap : 0; }
 
+const int64_t* alk_ht_keys(const alk_ht* h) { return h ? h->v.key : nullptr; }
+
 const int64_t* alk_ht_payload(const alk_ht* h, uint32_t p) {
   if (!h || p >= h->v.npay) return nullptr;
   return h->v.payload + (uint64_t)p * h->v.slot_cap;
@@ -944,31 +1257,32 @@ const int64_t* alk_ht_payload(const alk_ht* h, uint32_t p) {
 static int stage_common(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
                         const alk_program* progs, uint32_t nprogs, std::vector<uint8_t>& hb, StageArgs& a,
                         size_t extra_bytes, size_t* off_extra) {
-  std::vector<uint32_t> tseg, trow;
+  if (nseg == 0) return ALK_ERR_ARG;
+  std::vector<uint32_t> seg_tile(nseg + 1, 0);
+  uint64_t ntiles = 0;
   for (uint32_t g = 0; g < nseg; g++) {
+    seg_tile[g] = (uint32_t)ntiles;
     if (seg_mode[g] == 0) continue;
-    uint32_t rows = cols[g].rows;
-    for (uint32_t c = 1; c < ncols; c++)
-      if (cols[c * nseg + g].rows != rows) return ALK_ERR_ARG;
-    for (uint32_t r = 0; r < rows; r += kTile) {
-      tseg.push_back(g);
-      trow.push_back(r);
+    const uint32_t rows = cols[g].rows;
+    for (uint32_t c = 0; c < ncols; c++) {
+      const alk_colseg& d = cols[c * nseg + g];
+      if (d.rows != rows || !(d.bits == 8 || d.bits == 16 || d.bits == 32 || d.bits == 64)) return ALK_ERR_ARG;
+      if (rows && !d.data) return ALK_ERR_ARG;
     }
+    ntiles += (rows + kTile - 1) / kTile;
   }
-  a.ntiles = (uint32_t)tseg.size();
+  if (ntiles >= 0xffffffffull) return ALK_ERR_TOO_LARGE;
+  seg_tile[nseg] = (uint32_t)ntiles;
+  a.ntiles = (uint32_t)ntiles;
   size_t off_cols = 0;
   size_t off_mode = off_cols + sizeof(alk_colseg) * ncols * nseg;
-  size_t off_tseg = (off_mode + nseg + 15) & ~size_t(15);
-  size_t off_trow = off_tseg + 4 * tseg.size();
-  size_t off_prog = (off_trow + 4 * trow.size() + 15) & ~size_t(15);
+  size_t off_tile = (off_mode + nseg + 15) & ~size_t(15);
+  size_t off_prog = (off_tile + 4 * (nseg + 1) + 15) & ~size_t(15);
   size_t off_x = (off_prog + sizeof(alk_program) * nprogs + 15) & ~size_t(15);
   hb.assign(off_x + extra_bytes + 16, 0);
   std::memcpy(&hb[off_cols], cols, sizeof(alk_colseg) * ncols * nseg);
   std::memcpy(&hb[off_mode], seg_mode, nseg);
-  if (!tseg.empty()) {
-    std::memcpy(&hb[off_tseg], tseg.data(), 4 * tseg.size());
-    std::memcpy(&hb[off_trow], trow.data(), 4 * trow.size());
-  }
+  std::memcpy(&hb[off_tile], seg_tile.data(), 4 * (nseg + 1));
   std::memcpy(&hb[off_prog], progs, sizeof(alk_program) * nprogs);
   a.ncols = ncols;
   a.nseg = nseg;
@@ -977,8 +1291,7 @@ static int stage_common(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, c
   // device offsets are patched by the caller once the buffer exists
   a.cols = (const alk_colseg*)(uintptr_t)off_cols;
   a.seg_mode = (const uint8_t*)(uintptr_t)off_mode;
-  a.tile_seg = (const uint32_t*)(uintptr_t)off_tseg;
-  a.tile_row0 = (const uint32_t*)(uintptr_t)off_trow;
+  a.seg_tile = (const uint32_t*)(uintptr_t)off_tile;
   a.progs = (const alk_program*)(uintptr_t)off_prog;
   return ALK_OK;
 }
@@ -986,8 +1299,7 @@ static int stage_common(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, c
 static void patch(StageArgs& a, uint8_t* db) {
   a.cols = (const alk_colseg*)(db + (uintptr_t)a.cols);
   a.seg_mode = db + (uintptr_t)a.seg_mode;
-  a.tile_seg = (const uint32_t*)(db + (uintptr_t)a.tile_seg);
-  a.tile_row0 = (const uint32_t*)(db + (uintptr_t)a.tile_row0);
+  a.seg_tile = (const uint32_t*)(db + (uintptr_t)a.seg_tile);
   a.progs = (const alk_program*)(db + (uintptr_t)a.progs);
 }
 
@@ -998,16 +1310,57 @@ static void patch(StageArgs& a, uint8_t* db) {
 template <bool kBuild>
 static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* cols, const uint8_t* seg_mode,
                      const std::vector<uint8_t>& hb, size_t off_x, uint64_t hit_cap, uint64_t* h_rows_in,
-                     uint64_t* h_hits, cudaStream_t s, alk_event_timer* timer) {
+                     uint64_t* h_hits, alk_stage_status* h_status, cudaStream_t s, alk_event_timer* timer) {
   uint64_t upper = 0;
   for (uint32_t g = 0; g < a.nseg; g++)
     if (seg_mode[g]) upper += cols[g].rows;
   if (hit_cap == 0 || hit_cap > upper) hit_cap = upper;
-  const size_t off_tail = (hb.size() + 15) & ~size_t(15);
+  // room for the survivors plus the unused tail of every scan warp's last chunk
+  hit_cap += std::min<uint64_t>(a.ntiles, (uint64_t)sms() * 8) * 8 * kChunk;
+  // conjunctive predicates: per conjunct and segment, the raw-domain test (segments the
+  // zone maps pass whole need none)
+  FastArgs fa{};
+  const bool conj = as_conjuncts(pred, fa.conj, &fa.nconj);
+  std::vector<ConjSeg> cs;
+  if (conj) {
+    cs.resize((size_t)fa.nconj * a.nseg);
+    for (uint32_t c = 0; c < fa.nconj; c++)
+      for (uint32_t g = 0; g < a.nseg; g++)
+        cs[c * a.nseg + g] = seg_mode[g] == 1 ? ConjSeg{0, 0, kCjAlways, 0}
+                                              : conj_seg(fa.conj[c], cols[fa.conj[c].slot * a.nseg + g]);
+  }
+  // per segment: 32-bit evaluation when every staged column stores <= 32 bits and the
+  // stored probe key maps to its bitmap index without leaving 32-bit arithmetic
+  std::vector<SegPlan> sp(a.nseg, SegPlan{0, 0, 0});
+  for (uint32_t g = 0; g < a.nseg; g++) {
+    bool narrow = conj;
+    for (uint32_t c = 0; conj && c < fa.nconj; c++)
+      if (cols[fa.conj[c].slot * a.nseg + g].bits > 32) narrow = false;
+    if (a.probe_slot >= 0) {
+      const alk_colseg& d = cols[a.probe_slot * a.nseg + g];
+      if (d.bits > 32) narrow = false;
+      if (a.probe.bits) {
+        const __int128 off = (__int128)d.lower - a.probe.kmin;
+        const __int128 xmax = ((__int128)1 << std::min<uint32_t>(d.bits, 64)) - 1;
+        const __int128 two32 = (__int128)1 << 32;
+        const bool fits = (off >= 0 && off + xmax < two32) || (off < 0 && -off <= two32 - (__int128)a.probe.nbits);
+        if (!fits) narrow = false;
+        else sp[g].bit_off = (int64_t)off;
+      }
+    }
+    sp[g].narrow = narrow ? 1 : 0;
+  }
+  const size_t off_cs = (hb.size() + 15) & ~size_t(15);
+  const size_t off_sp = (off_cs + cs.size() * sizeof(ConjSeg) + 15) & ~size_t(15);
+  const size_t off_tail = (off_sp + sp.size() * sizeof(SegPlan) + 15) & ~size_t(15);
   const size_t off_hits = off_tail + 32;
+  std::vector<uint8_t> up(off_tail, 0);
+  std::memcpy(up.data(), hb.data(), hb.size());
+  if (!cs.empty()) std::memcpy(up.data() + off_cs, cs.data(), cs.size() * sizeof(ConjSeg));
+  std::memcpy(up.data() + off_sp, sp.data(), sp.size() * sizeof(SegPlan));
   uint8_t* db = nullptr;
   CK(cudaMallocAsync((void**)&db, off_hits + std::max<uint64_t>(hit_cap, 1) * sizeof(Hit), s));
-  CK(cudaMemcpyAsync(db, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(db, up.data(), up.size(), cudaMemcpyHostToDevice, s));
   uint8_t* tail = db + off_tail;
   CK(cudaMemsetAsync(tail, 0, 32, s));
   patch(a, db);
@@ -1016,11 +1369,22 @@ static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* co
   a.rows_in = (unsigned long long*)tail;
   a.hit_count = (unsigned long long*)(tail + 8);
   a.err = (int*)(tail + 16);
+  a.hit_rows = (unsigned long long*)(tail + 24);
   a.hits = (Hit*)(db + off_hits);
   a.hit_cap = hit_cap;
-  CK(launch_stage<kBuild>(a, pred, cols, seg_mode, s, timer));
-  unsigned long long back[3] = {0, 0, 0};
-  CK(cudaMemcpyAsync(back, tail, 24, cudaMemcpyDeviceToHost, s));
+  fa.a = a;
+  fa.cseg = (const ConjSeg*)(db + off_cs);
+  fa.splan = (const SegPlan*)(db + off_sp);
+  CK(launch_stage<kBuild>(fa, conj, cols, seg_mode, s, timer));
+  static_assert(sizeof(alk_stage_status) == 32, "status mirrors the counters after the arguments");
+  if (h_status) {  // asynchronous: the counters land in the caller's (pinned) status
+    if (timer && timer->on && a.ntiles) timer->launches++;
+    CK(cudaMemcpyAsync(h_status, tail, 32, cudaMemcpyDeviceToHost, s));
+    CK(cudaFreeAsync(db, s));
+    return ALK_OK;
+  }
+  unsigned long long back[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(back, tail, 32, cudaMemcpyDeviceToHost, s));
   CK(cudaFreeAsync(db, s));
   CK(cudaStreamSynchronize(s));
   if (timer && timer->on && a.ntiles) {
@@ -1030,15 +1394,15 @@ static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* co
     timer->launches++;
   }
   if (h_rows_in) *h_rows_in = back[0];
-  if (h_hits) *h_hits = back[1];
+  if (h_hits) *h_hits = back[3];
   return (int)(uint32_t)back[2];
 }
 extern "C" {
 
-int alk_pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
-                       const alk_program* pred, const alk_ht* probe, int32_t probe_slot, alk_ht* build,
-                       int32_t build_slot, const int32_t* pay_src, uint64_t hit_cap, uint64_t* h_rows_in,
-                       uint64_t* h_hits, alk_stream stream) {
+static int pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                          const alk_program* pred, const alk_ht* probe, int32_t probe_slot, alk_ht* build,
+                          int32_t build_slot, const int32_t* pay_src, uint64_t hit_cap, uint64_t* h_rows_in,
+                          uint64_t* h_hits, alk_stage_status* h_status, alk_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (!build || ncols == 0 || ncols > kMaxCols || build_slot < 0 || (uint32_t)build_slot >= ncols) return ALK_ERR_ARG;
   if ((probe_slot >= 0) != (probe != nullptr) || (probe_slot >= 0 && (uint32_t)probe_slot >= ncols))
@@ -1056,21 +1420,39 @@ int alk_pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, co
   size_t off_x;
   int rc = stage_common(cols, ncols, nseg, seg_mode, &prog, 1, hb, a, 4 * 8, &off_x);
   if (rc) return rc;
-  std::memcpy(&hb[off_x], pay_src, 4 * build->v.npay);
+  if (build->v.npay) std::memcpy(&hb[off_x], pay_src, 4 * build->v.npay);
   a.probe_slot = probe_slot;
   if (probe) a.probe = probe->v;
   a.build_slot = build_slot;
   a.build = build->v;
   for (uint32_t p = 0; p < build->v.npay; p++)
     if (pay_src[p] >= 32) a.need_slot = 1;
-  return run_stage<true>(a, prog, cols, seg_mode, hb, off_x, hit_cap, h_rows_in, h_hits, s, nullptr);
+  return run_stage<true>(a, prog, cols, seg_mode, hb, off_x, hit_cap, h_rows_in, h_hits, h_status, s, nullptr);
 }
 
-int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
-                           const alk_program* pred, const alk_ht* probe, int32_t probe_slot,
-                           const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg, int64_t* d_acc,
-                           uint64_t acc_stride, uint64_t* d_cnt, uint64_t hit_cap, uint64_t* h_rows_in,
-                           uint64_t* h_hits, alk_stream stream, alk_event_timer* timer) {
+int alk_pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                       const alk_program* pred, const alk_ht* probe, int32_t probe_slot, alk_ht* build,
+                       int32_t build_slot, const int32_t* pay_src, uint64_t hit_cap, uint64_t* h_rows_in,
+                       uint64_t* h_hits, alk_stream stream) {
+  return pipeline_build(cols, ncols, nseg, seg_mode, pred, probe, probe_slot, build, build_slot, pay_src, hit_cap,
+                        h_rows_in, h_hits, nullptr, stream);
+}
+
+int alk_pipeline_build_async(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                             const alk_program* pred, const alk_ht* probe, int32_t probe_slot, alk_ht* build,
+                             int32_t build_slot, const int32_t* pay_src, uint64_t hit_cap,
+                             alk_stage_status* h_status, alk_stream stream) {
+  if (!h_status) return ALK_ERR_ARG;
+  return pipeline_build(cols, ncols, nseg, seg_mode, pred, probe, probe_slot, build, build_slot, pay_src, hit_cap,
+                        nullptr, nullptr, h_status, stream);
+}
+
+static int pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                              const alk_program* pred, const alk_ht* probe, int32_t probe_slot,
+                              const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg, int64_t* d_acc,
+                              uint64_t acc_stride, uint64_t* d_cnt, uint64_t hit_cap, uint64_t* h_rows_in,
+                              uint64_t* h_hits, alk_stage_status* h_status, alk_stream stream,
+                              alk_event_timer* timer) {
   cudaStream_t s = (cudaStream_t)stream;
   if (!probe || probe_slot < 0 || (uint32_t)probe_slot >= ncols || ncols == 0 || ncols > kMaxCols || nagg > 7)
     return ALK_ERR_ARG;
@@ -1099,7 +1481,33 @@ int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg
   a.acc = d_acc;
   a.acc_stride = acc_stride;
   a.cnt = (unsigned long long*)d_cnt;
-  return run_stage<false>(a, progs[0], cols, seg_mode, hb, off_x, hit_cap, h_rows_in, h_hits, s, timer);
+  return run_stage<false>(a, progs[0], cols, seg_mode, hb, off_x, hit_cap, h_rows_in, h_hits, h_status, s, timer);
+}
+
+int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                           const alk_program* pred, const alk_ht* probe, int32_t probe_slot,
+                           const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg, int64_t* d_acc,
+                           uint64_t acc_stride, uint64_t* d_cnt, uint64_t hit_cap, uint64_t* h_rows_in,
+                           uint64_t* h_hits, alk_stream stream, alk_event_timer* timer) {
+  return pipeline_probe_agg(cols, ncols, nseg, seg_mode, pred, probe, probe_slot, agg_progs, agg_kind, nagg, d_acc,
+                            acc_stride, d_cnt, hit_cap, h_rows_in, h_hits, nullptr, stream, timer);
+}
+
+int alk_pipeline_probe_agg_async(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                                 const alk_program* pred, const alk_ht* probe, int32_t probe_slot,
+                                 const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg,
+                                 int64_t* d_acc, uint64_t acc_stride, uint64_t* d_cnt, uint64_t hit_cap,
+                                 alk_stage_status* h_status, alk_stream stream, alk_event_timer* timer) {
+  if (!h_status) return ALK_ERR_ARG;
+  return pipeline_probe_agg(cols, ncols, nseg, seg_mode, pred, probe, probe_slot, agg_progs, agg_kind, nagg, d_acc,
+                            acc_stride, d_cnt, hit_cap, nullptr, nullptr, h_status, stream, timer);
+}
+
+int alk_ht_info_async(const alk_ht* h, alk_ht_status* h_out, alk_stream stream) {
+  if (!h || !h_out) return ALK_ERR_ARG;
+  static_assert(sizeof(alk_ht_status) == 24, "inserted count followed by the four flags");
+  CK(cudaMemcpyAsync(h_out, h->v.nslots, 24, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  return ALK_OK;
 }
 
 int alk_fill_i64(int64_t* d, uint64_t n, int64_t v, alk_stream stream) {
@@ -1144,6 +1552,42 @@ int alk_topk_candidates(const int64_t* d_rank, const uint64_t* d_live, uint64_t 
   CK(cudaStreamSynchronize(s));
   *h_count = c;
   return c > cap ? ALK_ERR_OVERFLOW : ALK_OK;
+}
+
+int alk_topk_select(const int64_t* d_rank, const uint64_t* d_live, uint64_t n, uint32_t k, uint32_t* d_out,
+                    uint64_t cap, uint64_t* d_count, alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!d_count || !d_out || k == 0 || k > (uint32_t)kTopK) return ALK_ERR_ARG;
+  CK(cudaMemsetAsync(d_count, 0, 8, s));
+  if (n == 0) return ALK_OK;
+  const int blocks = (int)std::min<uint64_t>((n + kT - 1) / kT, (uint64_t)kMergeMax / k);
+  int64_t* db = nullptr;
+  CK(cudaMallocAsync((void**)&db, ((size_t)blocks * k + 1) * 8, s));
+  k_topk_local16<<<blocks, kT, 0, s>>>(d_rank, (const unsigned long long*)d_live, n, k, db);
+  k_topk_merge<<<1, kMergeThreads, 0, s>>>(db, (uint32_t)blocks * k, k, db + (size_t)blocks * k);
+  k_topk_collect_dev<<<grid_for(n), kT, 0, s>>>(d_rank, (const unsigned long long*)d_live, n,
+                                                db + (size_t)blocks * k, d_out, cap,
+                                                (unsigned long long*)d_count);
+  alk::g_kernel_launches += 3;
+  CK(cudaGetLastError());
+  CK(cudaFreeAsync(db, s));
+  return ALK_OK;
+}
+
+int alk_gather_rows(const int64_t* const* d_cols, uint32_t ncols, const uint32_t* d_idx, const uint64_t* d_count,
+                    uint64_t cap, int64_t* d_out, alk_stream stream) {
+  if (ncols == 0 || ncols > (uint32_t)kGatherCols || !d_idx || !d_count || !d_out) return ALK_ERR_ARG;
+  if (cap == 0) return ALK_OK;
+  GatherCols g{};
+  for (uint32_t c = 0; c < ncols; c++) {
+    if (!d_cols[c]) return ALK_ERR_ARG;
+    g.col[c] = d_cols[c];
+  }
+  k_gather_rows<<<grid_for(cap * ncols), kT, 0, (cudaStream_t)stream>>>(
+      g, ncols, d_idx, (const unsigned long long*)d_count, cap, d_out);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  return ALK_OK;
 }
 
 int alk_live_compact(const uint64_t* d_live, uint64_t n, uint32_t* d_out, uint64_t* h_count, alk_stream stream) {

@@ -223,7 +223,21 @@ Engine::~Engine() {
   cudaStreamSynchronize(stream_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
+  if (pin_) cudaFreeHost(pin_);
   cudaStreamDestroy(stream_);
+}
+
+void* Engine::pinned(size_t bytes) {
+  if (bytes > pin_n_) {
+    cudaStreamSynchronize(stream_);  // the old buffer may still be a copy destination
+    if (pin_) cudaFreeHost(pin_);
+    pin_ = nullptr;
+    pin_n_ = 0;
+    const size_t n = std::max<size_t>(bytes, 1 << 20);
+    ck(cudaMallocHost(&pin_, n), "pinned staging buffer");
+    pin_n_ = n;
+  }
+  return pin_;
 }
 
 Var* Engine::var(const std::string& n) {

@@ -153,6 +153,11 @@ class Engine {
   std::map<std::string, uint64_t> card_feedback_;
   bool timing_ = false;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  // Pinned host staging for device->host results (a pageable destination would make
+  // every copy wait for the stream).
+  void* pin_ = nullptr;
+  size_t pin_n_ = 0;
+  void* pinned(size_t bytes);
 
   void reset_script_state();
   Var* base_table(const std::string& t);

@@ -972,6 +972,8 @@ struct FusedFallback : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 [[noreturn]] void fallback(const std::string& why) { throw FusedFallback(why); }
+// A stage overflowed the size its recorded counts gave it; the counts are now exact.
+struct RerunFused {};
 
 // One emit_multijoin step resolved like operators.cu:961-1033.
 struct StepInfo {
@@ -1028,10 +1030,16 @@ bool Engine::try_fused(std::vector<Statement>& sts, size_t& i) {
     if (t != 'I') return false;
   for (auto& kv : J.join_and_cnt)
     if (kv.second) return false;
-  try {
-    run_fused(J, F, O, S);
-  } catch (const FusedFallback& e) {
-    return false;
+  for (int attempt = 0;; attempt++) {
+    try {
+      run_fused(J, F, O, S);
+      break;
+    } catch (const FusedFallback& e) {
+      return false;
+    } catch (const RerunFused&) {
+      // a rerun uses the exact counts the overflowing stage reported
+      if (attempt >= 2) return false;
+    }
   }
   stats_.plan = 1;
   i += 3;
@@ -1135,11 +1143,14 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     if (origin(src) == fact) return;
     if (std::find(payload.begin(), payload.end(), src) == payload.end()) payload.push_back(src);
   };
-  for (auto& g : group_cols) need_payload(src_of[g]);
+  // Group and output columns that are the last table's build key read its key column;
+  // the key is carried as payload only when an aggregate input reads it.
+  for (auto& g : group_cols)
+    if (src_of[g] != build_key) need_payload(src_of[g]);
   for (auto& o : outs) {
     if (o.col_type == 1) {
       if (origin(src_of.at(o.field)) == fact) fallback("fact column outside an aggregate");
-      need_payload(src_of.at(o.field));
+      if (src_of.at(o.field) != build_key) need_payload(src_of.at(o.field));
     }
     if (o.col_type == 2 && has_col(o.vec)) fallback("row-level expression in a grouped select");
   }
@@ -1162,43 +1173,72 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
   }
   if (payload.size() > 8) fallback("payload width");
   // ---- build stages
-  // Each stage's table is sized from the exact key count the previous run of the same
-  // stage recorded (the count the engine learns from its own runs); without one, or
-  // when the table overflows, the stage runs with the exact upper bound (rows scanned).
+  // Stage sizes come from the exact counts the previous run of the same stage recorded
+  // (the counts the engine learns from its own runs): hash tables from the inserted key
+  // count, survivor lists from the survivor count; without a record, the exact upper
+  // bound (rows scanned). The stages run without host synchronisation. Their counters
+  // are checked once the query's result is back, and a stage that overflowed makes the
+  // whole query run again with the counts it reported.
+  struct FusedStatus {
+    alk_stage_status st[3];
+    alk_ht_status ht[2];
+  };
+  const uint64_t kSmallCand = 1024;  // candidate rows returned with the first copy
+  const size_t nback_max = outs.size() + group_cols.size();
+  uint8_t* pin = (uint8_t*)pinned(sizeof(FusedStatus) + 8 + kSmallCand * 8 * nback_max);
+  FusedStatus* fs = (FusedStatus*)pin;
+  std::memset(fs, 0, sizeof(FusedStatus));
+  struct Pending {
+    std::string sig;
+    int st, ht;
+    uint64_t upper;
+  };
+  std::vector<Pending> pending;
+  auto hit_cap_for = [&](const std::string& sig) -> uint64_t {
+    auto it = card_feedback_.find(sig + "#hits");
+    return it == card_feedback_.end() ? 0 : it->second + it->second / 4 + 4096;
+  };
   auto build_stage = [&](HtGuard& g, const std::string& sig, uint64_t upper, uint32_t npay,
-                         std::pair<int64_t, int64_t> range, const std::function<void(alk_ht*)>& run) {
+                         std::pair<int64_t, int64_t> range, int idx,
+                         const std::function<int(alk_ht*, uint64_t, alk_stage_status*)>& run) {
     auto it = card_feedback_.find(sig);
-    uint64_t est = it == card_feedback_.end() ? upper : std::min(upper, it->second + it->second / 4 + 1024);
-    for (int attempt = 0; attempt < 2; attempt++) {
-      if (g.h) alk_ht_free(g.h, (alk_stream)s);
-      g.h = nullptr;
-      g.s = s;
-      check(alk_ht_create_range(est, npay, range.first, range.second, &g.h, (alk_stream)s), "hash table");
-      run(g.h);
-      uint64_t inserted = 0;
-      int fl = 0;
-      check(alk_ht_info(g.h, &inserted, &fl, (alk_stream)s), "hash table");
-      if ((fl & 2) && est < upper) {
-        est = upper;
+    const uint64_t est = it == card_feedback_.end() ? upper : std::min(upper, it->second + it->second / 4 + 1024);
+    g.s = s;
+    check(alk_ht_create_range(est, npay, range.first, range.second, &g.h, (alk_stream)s), "hash table");
+    check(run(g.h, hit_cap_for(sig), &fs->st[idx]), "build stage");
+    check(alk_ht_info_async(g.h, &fs->ht[idx], (alk_stream)s), "hash table");
+    pending.push_back({sig, idx, idx, upper});
+  };
+  // After the query's one synchronisation: record what every stage counted, or, when a
+  // stage overflowed, keep the counts up to that stage and drop the later stages' records
+  // (they ran on incomplete input) before running the query again.
+  auto verify = [&]() {
+    bool rerun = false;
+    for (auto& p : pending) {
+      if (rerun) {
+        card_feedback_.erase(p.sig);
+        card_feedback_.erase(p.sig + "#hits");
         continue;
       }
-      if (fl) fallback("duplicate build keys or an inconsistent key range");
-      card_feedback_[sig] = inserted;
-      return;
+      const alk_stage_status& st = fs->st[p.st];
+      if (st.err != ALK_OK && st.err != ALK_ERR_OVERFLOW) throw EngineError(st.err, "fused stage: wait expired");
+      card_feedback_[p.sig + "#hits"] = st.hits;
+      if (st.err == ALK_ERR_OVERFLOW) {
+        rerun = true;  // nothing of this stage was applied; its table count means nothing
+        continue;
+      }
+      if (p.ht < 0) continue;
+      const alk_ht_status& h = fs->ht[p.ht];
+      if (h.flags[1]) {
+        card_feedback_[p.sig] = p.upper;
+        rerun = true;
+      } else if (h.flags[0] || h.flags[3]) {
+        fallback("duplicate build keys or an inconsistent key range");
+      } else {
+        card_feedback_[p.sig] = h.inserted;
+      }
     }
-  };
-  // Each stage's survivor list is sized the same way from the survivor count its previous
-  // run recorded (rows scanned without one); an overflow reruns it with the exact count.
-  auto with_hits = [&](const std::string& sig, const char* what,
-                       const std::function<int(uint64_t, uint64_t*)>& run) {
-    const std::string key = sig + "#hits";
-    auto it = card_feedback_.find(key);
-    const uint64_t cap = it == card_feedback_.end() ? 0 : it->second + it->second / 4 + 4096;
-    uint64_t hits = 0;
-    int rc = run(cap, &hits);
-    if (rc == ALK_ERR_OVERFLOW) rc = run(hits, &hits);
-    check(rc, what);
-    card_feedback_[key] = hits;
+    if (rerun) throw RerunFused();
   };
   auto rows_of = [&](const ScanPlan& p, const std::vector<alk_colseg>& cs) {
     uint64_t n = 0;
@@ -1226,13 +1266,12 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     for (auto& c : pay1) src1.push_back((int32_t)p1.slot(c));
     auto cs1 = colsegs(p1);
     std::string sig1 = plan_sig(p1) + "|" + st1.rkey;
-    build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)pay1.size(), range_of(p1.src, st1.rkey), [&](alk_ht* h) {
-      with_hits(sig1, "build stage", [&](uint64_t cap, uint64_t* hits) {
-        return alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
-                                  p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h, (int32_t)k1, src1.data(), cap,
-                                  nullptr, hits, (alk_stream)s);
-      });
-    });
+    build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)pay1.size(), range_of(p1.src, st1.rkey), 0,
+                [&](alk_ht* h, uint64_t cap, alk_stage_status* st) {
+                  return alk_pipeline_build_async(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount,
+                                                  p1.mode.data(), p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h,
+                                                  (int32_t)k1, src1.data(), cap, st, (alk_stream)s);
+                });
     // stage 2: d1 probes stage 1 on st1.lkey and is keyed on the final build key
     ScanPlan p2 = plan_scan(d1);
     uint32_t probe2 = p2.slot(st1.lkey);
@@ -1251,13 +1290,12 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     }
     auto cs2 = colsegs(p2);
     std::string sig2 = plan_sig(p2) + "|" + build_key + "|" + sig1;
-    build_stage(ht2, sig2, rows_of(p2, cs2), (uint32_t)payload.size(), range_of(p2.src, build_key), [&](alk_ht* h) {
-      with_hits(sig2, "build stage", [&](uint64_t cap, uint64_t* hits) {
-        return alk_pipeline_build(cs2.data(), (uint32_t)p2.slots.size(), p2.src->segCount, p2.mode.data(),
-                                  p2.has_pred ? &p2.pred : nullptr, ht1.h, (int32_t)probe2, h, key2, src2.data(),
-                                  cap, nullptr, hits, (alk_stream)s);
-      });
-    });
+    build_stage(ht2, sig2, rows_of(p2, cs2), (uint32_t)payload.size(), range_of(p2.src, build_key), 1,
+                [&](alk_ht* h, uint64_t cap, alk_stage_status* st) {
+                  return alk_pipeline_build_async(cs2.data(), (uint32_t)p2.slots.size(), p2.src->segCount,
+                                                  p2.mode.data(), p2.has_pred ? &p2.pred : nullptr, ht1.h,
+                                                  (int32_t)probe2, h, key2, src2.data(), cap, st, (alk_stream)s);
+                });
     last = ht2.h;
     last_sig = sig2;
   } else {
@@ -1270,13 +1308,12 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     }
     auto cs1 = colsegs(p1);
     std::string sig1 = plan_sig(p1) + "|" + build_key;
-    build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)payload.size(), range_of(p1.src, build_key), [&](alk_ht* h) {
-      with_hits(sig1, "build stage", [&](uint64_t cap, uint64_t* hits) {
-        return alk_pipeline_build(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount, p1.mode.data(),
-                                  p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h, (int32_t)k1, src1.data(), cap,
-                                  nullptr, hits, (alk_stream)s);
-      });
-    });
+    build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)payload.size(), range_of(p1.src, build_key), 0,
+                [&](alk_ht* h, uint64_t cap, alk_stage_status* st) {
+                  return alk_pipeline_build_async(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount,
+                                                  p1.mode.data(), p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h,
+                                                  (int32_t)k1, src1.data(), cap, st, (alk_stream)s);
+                });
     last = ht1.h;
     last_sig = sig1;
   }
@@ -1311,17 +1348,21 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
   ck(cudaMemsetAsync(cnt->as<void>(), 0, stride * 8, s), "init");
   alk_event_timer tm{timing_ ? 1 : 0, ev0_, ev1_, 0.0, 0};
   // the probe-aggregate kernel accumulates into slot-indexed arrays sized for every slot
+  const std::string sigf = plan_sig(pf) + "|" + st2.lkey + "|" + last_sig;
   if (nslots) {
-    with_hits(plan_sig(pf) + "|" + st2.lkey + "|" + last_sig, "probe-aggregate",
-              [&](uint64_t cap, uint64_t* hits) {
-                return alk_pipeline_probe_agg(csf.data(), (uint32_t)pf.slots.size(), pf.src->segCount,
-                                              pf.mode.data(), pf.has_pred ? &pf.pred : nullptr, last, (int32_t)probe_f,
-                                              progs.data(), kinds.data(), (uint32_t)aggs.size(), acc->as<int64_t>(),
-                                              stride, cnt->as<uint64_t>(), cap, nullptr, hits, (alk_stream)s, &tm);
-              });
+    check(alk_pipeline_probe_agg_async(csf.data(), (uint32_t)pf.slots.size(), pf.src->segCount, pf.mode.data(),
+                                       pf.has_pred ? &pf.pred : nullptr, last, (int32_t)probe_f, progs.data(),
+                                       kinds.data(), (uint32_t)aggs.size(), acc->as<int64_t>(), stride,
+                                       cnt->as<uint64_t>(), hit_cap_for(sigf), &fs->st[2], (alk_stream)s, &tm),
+          "probe-aggregate");
+    pending.push_back({sigf, 2, -1, 0});
   }
-  if (timing_ && nslots) {
-    stats_.hot_kernel_ms += tm.ms;
+  // device time and algorithmic bytes of the probe-aggregate stage (read after the sync)
+  auto record_timing = [&]() {
+    if (!timing_ || !nslots || !tm.launches) return;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    stats_.hot_kernel_ms += ms;
     stats_.hot_kernel_launches += tm.launches;
     // Algorithmic bytes: the columns every row needs (predicate and probe key) over all
     // rows scanned, plus one value of each aggregate input column per survivor.
@@ -1335,7 +1376,7 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     if (pf.has_pred) cols_of(pf.pred, streamed);
     for (auto& p : progs) cols_of(p, per_hit);
     for (uint32_t c : streamed) per_hit.erase(c);
-    const uint64_t hits = card_feedback_[plan_sig(pf) + "|" + st2.lkey + "|" + last_sig + "#hits"];
+    const uint64_t hits = fs->st[2].hits;
     uint64_t hit_bytes = 0;
     for (uint32_t c : per_hit) {
       uint32_t w = 1;
@@ -1346,10 +1387,12 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     }
     stats_.hot_kernel_bytes +=
         scan_bytes(pf, std::vector<uint32_t>(streamed.begin(), streamed.end())) + hits * hit_bytes;
-  }
+  };
   // ---- F's columns over slots
   auto slot_col = [&](const std::string& alias) -> const int64_t* {
-    return alk_ht_payload(last, last_pay.at(src_of.at(alias)));
+    const std::string& src = src_of.at(alias);
+    if (src == build_key && !last_pay.count(src)) return alk_ht_keys(last);
+    return alk_ht_payload(last, last_pay.at(src));
   };
   std::vector<DevBufP> keep;
   std::vector<const int64_t*> fcol(outs.size());
@@ -1432,16 +1475,60 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
   uint64_t ncand = 0;
   const uint64_t cand_cap = 1 << 16;
   auto cand = mkbuf(cand_cap * 4, s);
-  int rc = alk_topk_candidates(rank, cnt->as<uint64_t>(), nslots, limit, cand->as<uint32_t>(), cand_cap, &ncand,
-                               (alk_stream)s);
-  if (rc == ALK_ERR_OVERFLOW) fallback("too many ties at the LIMIT boundary");
-  check(rc, "top-k");
-  // gather candidate rows: F columns and group keys
+  // the candidate rows come back with F's columns followed by the group keys
   std::vector<const int64_t*> gcol;
   for (auto& g : group_cols) gcol.push_back(slot_col(g));
-  std::vector<std::vector<int64_t>> hf(outs.size(), std::vector<int64_t>(ncand)),
-      hg(gcol.size(), std::vector<int64_t>(ncand));
-  if (ncand) {
+  std::vector<const int64_t*> back_cols(fcol);
+  back_cols.insert(back_cols.end(), gcol.begin(), gcol.end());
+  const size_t nback = back_cols.size();
+  std::vector<std::vector<int64_t>> hf(outs.size()), hg(gcol.size());
+  bool fetched = false;
+  if (limit <= 16 && nback <= 32) {
+    // threshold, candidates and their rows on the device; one copy back, the query's only
+    // synchronisation
+    const uint64_t small = kSmallCand;
+    auto dcount = mkbuf(8, s);
+    auto tmp = mkbuf(small * 8 * nback, s);
+    check(alk_topk_select(rank, cnt->as<uint64_t>(), nslots, limit, cand->as<uint32_t>(), cand_cap,
+                          dcount->as<uint64_t>(), (alk_stream)s),
+          "top-k");
+    check(alk_gather_rows(back_cols.data(), (uint32_t)nback, cand->as<uint32_t>(), dcount->as<uint64_t>(), small,
+                          tmp->as<int64_t>(), (alk_stream)s),
+          "gather");
+    uint8_t* res = pin + sizeof(FusedStatus);
+    ck(cudaMemcpyAsync(res, dcount->as<void>(), 8, cudaMemcpyDeviceToHost, s), "d2h");
+    ck(cudaMemcpyAsync(res + 8, tmp->as<void>(), small * 8 * nback, cudaMemcpyDeviceToHost, s), "d2h");
+    ck(cudaStreamSynchronize(s), "sync");
+    verify();
+    record_timing();
+    std::memcpy(&ncand, res, 8);
+    stats_.d2h_bytes += 8 + small * 8 * nback;
+    if (ncand > cand_cap) fallback("too many ties at the LIMIT boundary");
+    if (ncand <= small) {
+      const int64_t* rowsb = (const int64_t*)(res + 8);
+      for (size_t c = 0; c < nback; c++) {
+        auto& dst = c < outs.size() ? hf[c] : hg[c - outs.size()];
+        dst.assign(rowsb + c * small, rowsb + c * small + ncand);
+      }
+      fetched = true;
+    }
+  } else {
+    int rc = alk_topk_candidates(rank, cnt->as<uint64_t>(), nslots, limit, cand->as<uint32_t>(), cand_cap, &ncand,
+                                 (alk_stream)s);
+    verify();
+    record_timing();
+    if (rc == ALK_ERR_OVERFLOW) fallback("too many ties at the LIMIT boundary");
+    check(rc, "top-k");
+  }
+  // An empty join leaves the reference's SELECT a column-less set (emit_select,
+  // operators.cu:1847-1856), in which ORDER BY cannot find its first key.
+  if (ncand == 0) {
+    const std::string& t0 = O.op_type.at(0);
+    throw EngineError(ALK_ERR_ARG, "Couldn't find name " + (t0 == "NAME" ? O.op_value.at(0) : t0));
+  }
+  if (!fetched) {
+    for (auto& v : hf) v.resize(ncand);
+    for (auto& v : hg) v.resize(ncand);
     auto tmp = mkbuf(ncand * 8 * (outs.size() + gcol.size()), s);
     for (size_t c = 0; c < outs.size() + gcol.size(); c++) {
       const int64_t* src = c < outs.size() ? fcol[c] : gcol[c - outs.size()];

@@ -80,7 +80,11 @@ void alk_session_close(alk_session* s);
 
 /* One column of one segment as it sits in device memory. FOR columns keep the
  * on-disk width (bits 8/16/32/64, value = stored + lower); delta columns are first
- * expanded with alk_decode_segment and then described with bits=64, lower=0. */
+ * expanded with alk_decode_segment and then described with bits=64, lower=0.
+ * Kernels read whole 16-byte units: data must stay readable up to the next multiple
+ * of 16 bytes past rows * bits / 8 (the session loaders pad every payload by 256
+ * bytes), and the fused stages stage 16-byte aligned columns through shared memory
+ * with bulk copies (unaligned columns take a direct-load kernel instead). */
 typedef struct alk_colseg {
   const void* data;
   int64_t lower;
@@ -233,6 +237,9 @@ int alk_ht_info(const alk_ht* h, uint64_t* nslots, int* flags, alk_stream stream
 /* Slot range of a table: payload columns and per-key accumulators are indexed by the
  * key's table position, 0 <= slot < alk_ht_slots(h). */
 uint64_t alk_ht_slots(const alk_ht* h);
+/* Device address of the key column (slot-indexed; free slots hold the byte pattern 0x80
+ * repeated, 0x8080808080808080). */
+const int64_t* alk_ht_keys(const alk_ht* h);
 /* Device address of payload column p (slot-indexed). */
 const int64_t* alk_ht_payload(const alk_ht* h, uint32_t p);
 /* Optional CUDA-event timing of the probe-aggregate kernel (cudaEvent_t handles). */
@@ -246,11 +253,12 @@ typedef struct alk_event_timer {
 /* Build stage. The predicate reads scan slots only; payload sources pay_src[p] name scan
  * slots (< 32) or, when probing, payload columns of the probed table (32 + p).
  *
- * Both stages run as a streaming scan that appends surviving rows (predicate true and,
- * when probing, the key present in the probed table's key bitmap) to a device hit list
- * of hit_cap entries (16 bytes each; 0 = the rows scanned, which cannot overflow),
- * followed by one kernel that does the per-survivor work. If more rows survive than
- * hit_cap, nothing is applied, ALK_ERR_OVERFLOW is returned and *h_hits holds the
+ * Both stages run as a streaming scan that appends the positions of surviving rows
+ * (predicate true and, when probing, the key present in the probed table's key bitmap)
+ * to a device hit list sized for hit_cap survivors (8 bytes each, plus a fixed slack for
+ * the scan warps' partly filled chunks; 0 = the rows scanned, which cannot overflow),
+ * followed by one kernel that does the per-survivor work. If more rows survive than the
+ * list holds, nothing is applied, ALK_ERR_OVERFLOW is returned and *h_hits holds the
  * exact survivor count for a rerun. h_rows_in receives the rows scanned. Synchronizes. */
 int alk_pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
                        const alk_program* pred, const alk_ht* probe, int32_t probe_slot, alk_ht* build,
@@ -266,12 +274,49 @@ int alk_pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t nseg
                            const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg, int64_t* d_acc,
                            uint64_t acc_stride, uint64_t* d_cnt, uint64_t hit_cap, uint64_t* h_rows_in,
                            uint64_t* h_hits, alk_stream stream, alk_event_timer* timer);
+/* Asynchronous stages: the same work, with no host synchronisation. The counters arrive
+ * in *h_status (host memory; pinned for the copy to be asynchronous) once the stream
+ * reaches the end of the stage: err is ALK_OK, ALK_ERR_OVERFLOW (nothing applied; hits is
+ * the exact survivor count) or ALK_ERR_TIMEOUT. Argument errors are returned at once. */
+typedef struct alk_stage_status {
+  uint64_t rows_in;  /* rows scanned */
+  uint64_t reserved; /* hit-list entries reserved */
+  int32_t err;
+  int32_t pad;
+  uint64_t hits;     /* survivors of the scan */
+} alk_stage_status;
+int alk_pipeline_build_async(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                             const alk_program* pred, const alk_ht* probe, int32_t probe_slot, alk_ht* build,
+                             int32_t build_slot, const int32_t* pay_src, uint64_t hit_cap,
+                             alk_stage_status* h_status, alk_stream stream);
+int alk_pipeline_probe_agg_async(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                                 const alk_program* pred, const alk_ht* probe, int32_t probe_slot,
+                                 const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg,
+                                 int64_t* d_acc, uint64_t acc_stride, uint64_t* d_cnt, uint64_t hit_cap,
+                                 alk_stage_status* h_status, alk_stream stream, alk_event_timer* timer);
+/* alk_ht_info without synchronising: inserted keys and the four flags (duplicate key,
+ * capacity exceeded, wait expired, key outside the declared range; non-zero = set) land
+ * in *h_out when the stream reaches this point. */
+typedef struct alk_ht_status {
+  uint64_t inserted;
+  int32_t flags[4];
+} alk_ht_status;
+int alk_ht_info_async(const alk_ht* h, alk_ht_status* h_out, alk_stream stream);
 int alk_fill_i64(int64_t* d, uint64_t n, int64_t v, alk_stream stream);
 /* Top-k candidates for ORDER BY ... LIMIT k (emit_order + Store LIMIT, operators.cu:1641,
  * cm.cu:1493): every live slot whose ranking value is >= the k-th largest ranking value
  * (ties included); the caller orders the few candidates with the full key list. */
 int alk_topk_candidates(const int64_t* d_rank, const uint64_t* d_live, uint64_t n, uint32_t k, uint32_t* d_out,
                         uint64_t cap, uint64_t* h_count, alk_stream stream);
+/* The same selection without a host round trip (k <= 16): the threshold is computed on
+ * the device and the candidate count is written to device memory d_count (candidates
+ * beyond cap are counted, not written). Asynchronous on the stream. */
+int alk_topk_select(const int64_t* d_rank, const uint64_t* d_live, uint64_t n, uint32_t k, uint32_t* d_out,
+                    uint64_t cap, uint64_t* d_count, alk_stream stream);
+/* d_out[c * cap + r] = d_cols[c][d_idx[r]] for r < min(*d_count, cap) and c < ncols (<= 32);
+ * the row count is read on the device. Asynchronous on the stream. */
+int alk_gather_rows(const int64_t* const* d_cols, uint32_t ncols, const uint32_t* d_idx, const uint64_t* d_count,
+                    uint64_t cap, int64_t* d_out, alk_stream stream);
 /* Indices of live (non-zero) slots, unordered. */
 int alk_live_compact(const uint64_t* d_live, uint64_t n, uint32_t* d_out, uint64_t* h_count, alk_stream stream);
 

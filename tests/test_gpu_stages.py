@@ -1,0 +1,197 @@
+"""Fused-stage entry points through the C ABI, checked against numpy on the same inputs:
+the build stage's survivor list (overflow applies nothing and reports the exact survivor
+count; a rerun with that count succeeds), the asynchronous status form, the exact key
+bitmap under a key range, and the device-side top-k selection and row gather (ties
+included). Integer results: compared exactly."""
+import ctypes as c
+
+import numpy as np
+import pytest
+
+import alenka_b200 as ab
+
+pytestmark = pytest.mark.gpu
+
+ALK_OK, ALK_ERR_OVERFLOW = 0, 3
+
+
+class ColSeg(c.Structure):
+    _fields_ = [("data", c.c_void_p), ("lower", c.c_int64), ("rows", c.c_uint32), ("bits", c.c_uint32)]
+
+
+class StageStatus(c.Structure):
+    _fields_ = [("rows_in", c.c_uint64), ("reserved", c.c_uint64), ("err", c.c_int32), ("pad", c.c_int32),
+                ("hits", c.c_uint64)]
+
+
+class HtStatus(c.Structure):
+    _fields_ = [("inserted", c.c_uint64), ("flags", c.c_int32 * 4)]
+
+
+def _lib():
+    L = ab.lib()
+    vp, u32, u64, i32, i64 = c.c_void_p, c.c_uint32, c.c_uint64, c.c_int32, c.c_int64
+    L.alk_ht_create_range.argtypes = [u64, u32, i64, i64, c.POINTER(vp), vp]
+    L.alk_ht_free.argtypes = [vp, vp]
+    L.alk_ht_free.restype = None
+    L.alk_ht_info.argtypes = [vp, c.POINTER(u64), c.POINTER(c.c_int), vp]
+    L.alk_ht_info_async.argtypes = [vp, c.POINTER(HtStatus), vp]
+    L.alk_ht_slots.argtypes = [vp]
+    L.alk_ht_slots.restype = u64
+    L.alk_ht_payload.argtypes = [vp, u32]
+    L.alk_ht_payload.restype = vp
+    L.alk_ht_keys.argtypes = [vp]
+    L.alk_ht_keys.restype = vp
+    L.alk_pipeline_build.argtypes = [c.POINTER(ColSeg), u32, u32, c.POINTER(c.c_uint8), vp, vp, i32, vp, i32,
+                                     c.POINTER(i32), u64, c.POINTER(u64), c.POINTER(u64), vp]
+    L.alk_pipeline_build_async.argtypes = [c.POINTER(ColSeg), u32, u32, c.POINTER(c.c_uint8), vp, vp, i32, vp, i32,
+                                           c.POINTER(i32), u64, c.POINTER(StageStatus), vp]
+    L.alk_topk_select.argtypes = [vp, vp, u64, u32, vp, u64, vp, vp]
+    L.alk_gather_rows.argtypes = [c.POINTER(vp), u32, vp, vp, u64, vp, vp]
+    return L
+
+
+def _column(values, bits=32):
+    """A FOR column segment on the device: stored = value - min, at `bits` width, padded."""
+    import torch
+    lo = int(values.min())
+    dt = {8: np.uint8, 16: np.uint16, 32: np.uint32, 64: np.uint64}[bits]
+    raw = (values - lo).astype(dt)
+    pad = np.zeros(len(raw) * raw.itemsize + 256, dtype=np.uint8)
+    pad[:len(raw) * raw.itemsize] = raw.view(np.uint8)
+    t = torch.from_numpy(pad).cuda()
+    return t, ColSeg(t.data_ptr(), lo, len(values), bits)
+
+
+def test_build_hit_list_overflow_then_exact_rerun():
+    import torch
+    L = _lib()
+    n = 2_000_000
+    keys = np.random.default_rng(3).permutation(n).astype(np.int64) * 3 + 11
+    buf, cs = _column(keys)
+    cols = (ColSeg * 1)(cs)
+    mode = (c.c_uint8 * 1)(2)
+    ht = c.c_void_p()
+    assert L.alk_ht_create_range(n, 0, int(keys.min()), int(keys.max()), c.byref(ht), None) == ALK_OK
+    try:
+        rows_in, hits = c.c_uint64(), c.c_uint64()
+        rc = L.alk_pipeline_build(cols, 1, 1, mode, None, None, -1, ht, 0, None, 1, c.byref(rows_in), c.byref(hits),
+                                  None)
+        assert rc == ALK_ERR_OVERFLOW
+        assert hits.value == n and rows_in.value == n
+        ins, fl = c.c_uint64(), c.c_int()
+        assert L.alk_ht_info(ht, c.byref(ins), c.byref(fl), None) == ALK_OK
+        assert ins.value == 0 and fl.value == 0  # nothing applied
+        rc = L.alk_pipeline_build(cols, 1, 1, mode, None, None, -1, ht, 0, None, hits.value, c.byref(rows_in),
+                                  c.byref(hits), None)
+        assert rc == ALK_OK and hits.value == n
+        assert L.alk_ht_info(ht, c.byref(ins), c.byref(fl), None) == ALK_OK
+        assert ins.value == n and fl.value == 0
+    finally:
+        L.alk_ht_free(ht, None)
+        torch.cuda.synchronize()
+    del buf
+
+
+class Instr(c.Structure):
+    _fields_ = [("op", c.c_uint8), ("dst", c.c_uint8), ("ka", c.c_uint8), ("kb", c.c_uint8), ("a", c.c_uint16),
+                ("b", c.c_uint16), ("pad", c.c_uint32)]
+
+
+class Program(c.Structure):
+    _fields_ = [("n_instr", c.c_uint32), ("result", c.c_uint32), ("ins", Instr * 48), ("consts", c.c_int64 * 48)]
+
+
+ALK_OP_LT, ALK_OP_GE, ALK_OP_AND = 5, 8, 11
+ALK_K_REG, ALK_K_COL, ALK_K_CONST = 0, 1, 2
+
+
+def _range_pred(slot, lo, hi):
+    """lo <= column(slot) < hi as a compiled program (two conjuncts)."""
+    p = Program()
+    p.n_instr, p.result = 3, 2
+    p.consts[0], p.consts[1] = lo, hi
+    p.ins[0] = Instr(ALK_OP_GE, 0, ALK_K_COL, ALK_K_CONST, slot, 0, 0)
+    p.ins[1] = Instr(ALK_OP_LT, 1, ALK_K_COL, ALK_K_CONST, slot, 1, 0)
+    p.ins[2] = Instr(ALK_OP_AND, 2, ALK_K_REG, ALK_K_REG, 0, 1, 0)
+    return p
+
+
+@pytest.mark.parametrize("bits", [16, 32, 64])
+def test_build_async_status_and_payload(bits):
+    import torch
+    L = _lib()
+    rng = np.random.default_rng(5)
+    n = 300_000
+    keys = rng.permutation(n).astype(np.int64) + 1000
+    vals = rng.integers(-20_000, 40_000, n).astype(np.int64)
+    kb, ks = _column(keys)
+    vb, vs = _column(vals, bits)
+    cols = (ColSeg * 2)(ks, vs)
+    mode = (c.c_uint8 * 1)(2)
+    prog = _range_pred(1, -5_000, 30_000)
+    sel = (vals >= -5_000) & (vals < 30_000)
+    ht = c.c_void_p()
+    assert L.alk_ht_create_range(n, 1, 1000, 1000 + n - 1, c.byref(ht), None) == ALK_OK
+    status, hst = StageStatus(), HtStatus()
+    pay = (c.c_int32 * 1)(1)
+    try:
+        rc = L.alk_pipeline_build_async(cols, 2, 1, mode, c.byref(prog), None, -1, ht, 0, pay, 0, c.byref(status),
+                                        None)
+        assert rc == ALK_OK
+        assert L.alk_ht_info_async(ht, c.byref(hst), None) == ALK_OK
+        torch.cuda.synchronize()
+        assert status.err == ALK_OK and status.rows_in == n and status.hits == int(sel.sum())
+        assert hst.inserted == int(sel.sum()) and list(hst.flags) == [0, 0, 0, 0]
+        # keys and payload by table position (gathered with the identity permutation):
+        # every inserted key carries its own row's value
+        slots = L.alk_ht_slots(ht)
+        got = torch.empty(2 * slots, dtype=torch.int64, device="cuda")
+        ident = torch.arange(slots, dtype=torch.int32, device="cuda")
+        cnt = torch.tensor([slots], dtype=torch.int64, device="cuda")
+        colp = (c.c_void_p * 2)(L.alk_ht_keys(ht), L.alk_ht_payload(ht, 0))
+        assert L.alk_gather_rows(colp, 2, ident.data_ptr(), cnt.data_ptr(), slots, got.data_ptr(), None) == ALK_OK
+        torch.cuda.synchronize()
+        tk, tv = got.cpu().numpy()[:slots], got.cpu().numpy()[slots:]
+        occ = tk != np.int64(np.uint64(0x8080808080808080).view(np.int64))
+        assert dict(zip(tk[occ].tolist(), tv[occ].tolist())) == dict(zip(keys[sel].tolist(), vals[sel].tolist()))
+    finally:
+        L.alk_ht_free(ht, None)
+        torch.cuda.synchronize()
+    del kb, vb
+
+
+@pytest.mark.parametrize("k", [1, 10, 16])
+def test_topk_select_and_gather_rows(k):
+    import torch
+    L = _lib()
+    rng = np.random.default_rng(k)
+    n = 1_000_003
+    rank = rng.integers(-5000, 5000, n).astype(np.int64)  # many ties
+    live = (rng.random(n) < 0.3).astype(np.uint64) * rng.integers(1, 9, n).astype(np.uint64)
+    other = rng.integers(0, 1 << 40, n).astype(np.int64)
+    d_rank = torch.from_numpy(rank).cuda()
+    d_live = torch.from_numpy(live.view(np.int64)).cuda()
+    d_other = torch.from_numpy(other).cuda()
+    cap = 1 << 16
+    d_out = torch.zeros(cap, dtype=torch.int32, device="cuda")
+    d_cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    assert L.alk_topk_select(d_rank.data_ptr(), d_live.data_ptr(), n, k, d_out.data_ptr(), cap, d_cnt.data_ptr(),
+                             None) == ALK_OK
+    small = 4096
+    d_rows = torch.zeros(2 * small, dtype=torch.int64, device="cuda")
+    cols = (c.c_void_p * 2)(d_rank.data_ptr(), d_other.data_ptr())
+    assert L.alk_gather_rows(cols, 2, d_out.data_ptr(), d_cnt.data_ptr(), small, d_rows.data_ptr(), None) == ALK_OK
+    torch.cuda.synchronize()
+    m = int(d_cnt.item())
+    lv = rank[live != 0]
+    thr = np.sort(lv)[::-1][k - 1]
+    want = np.nonzero((live != 0) & (rank >= thr))[0]
+    assert m == len(want)
+    got = np.sort(d_out.cpu().numpy()[:m].astype(np.int64))
+    assert np.array_equal(got, want)
+    rows = d_rows.cpu().numpy()
+    idx = d_out.cpu().numpy()[:min(m, small)].astype(np.int64)
+    assert np.array_equal(rows[:len(idx)], rank[idx])
+    assert np.array_equal(rows[small:small + len(idx)], other[idx])
