@@ -302,11 +302,19 @@ __global__ void __launch_bounds__(kT) k_stage_hits(const StageArgs a) {
       if (j < 0) continue;
     }
     if (kBuild) {
-      const int64_t sl = ht_insert(a.build, col((uint32_t)a.build_slot));
+      // the key and every payload value are loaded before the insert, so that one
+      // round trip covers them all
+      const int64_t key = col((uint32_t)a.build_slot);
+      int64_t pv[8];
+#pragma unroll
+      for (uint32_t p = 0; p < 8; p++)
+        if (p < a.build.npay) pv[p] = col((uint32_t)a.pay_src[p]);
+      const int64_t sl = ht_insert(a.build, key);
       if (sl < 0) continue;
       inserted++;
-      for (uint32_t p = 0; p < a.build.npay; p++)
-        a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = col((uint32_t)a.pay_src[p]);
+#pragma unroll
+      for (uint32_t p = 0; p < 8; p++)
+        if (p < a.build.npay) a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = pv[p];
     } else {
       for (uint32_t g = 0; g < a.nagg; g++) {
         unsigned long long* dst = (unsigned long long*)(a.acc + (uint64_t)g * a.acc_stride + j);
@@ -402,9 +410,65 @@ __global__ void __launch_bounds__(kT) k_topk_local(const int64_t* rank, const un
 // values (with multiplicity) in registers, then the block sorts the 4096 candidates in
 // shared memory and writes its k largest.
 constexpr int kTopK = 16;
+
+// Inserts v into a descending register list, dropping the smallest.
+__device__ __forceinline__ void top16_insert(int64_t (&t)[kTopK], int64_t v) {
+  if (v <= t[kTopK - 1]) return;
+#pragma unroll
+  for (int q = kTopK - 1; q > 0; q--) {
+    const int64_t up = t[q - 1];
+    t[q] = v > up ? up : (v > t[q] ? v : t[q]);
+  }
+  t[0] = v > t[0] ? v : t[0];
+}
+
+// The warp's 16 largest values (with multiplicity) out of its lanes' descending lists:
+// 16 rounds of a warp maximum over the list heads, the winning lane popping its head.
+// Lane r < 16 returns the r-th largest. Warp-wide.
+__device__ __forceinline__ int64_t warp_top16(int64_t (&t)[kTopK]) {
+  const uint32_t lane = threadIdx.x & 31;
+  int64_t mine = INT64_MIN;
+#pragma unroll 1
+  for (int r = 0; r < kTopK; r++) {
+    int64_t m = t[0];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      const int64_t x = __shfl_xor_sync(0xffffffffu, m, o);
+      m = x > m ? x : m;
+    }
+    const uint32_t win = __ffs(__ballot_sync(0xffffffffu, t[0] == m)) - 1;
+    if (lane == (uint32_t)r) mine = m;
+    if (lane == win) {
+#pragma unroll
+      for (int q = 0; q < kTopK - 1; q++) t[q] = t[q + 1];
+      t[kTopK - 1] = INT64_MIN;
+    }
+  }
+  return mine;
+}
+
+// The block's 16 largest: warp lists through shared memory, merged by warp 0.
+template <int kThreads>
+__device__ __forceinline__ void block_top16(int64_t (&t)[kTopK], int64_t* s_w, int64_t* out16) {
+  constexpr int kWarps = kThreads / 32;
+  static_assert(kWarps * kTopK <= 32 * kTopK, "warp 0 holds at most 16 values per lane");
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t w = warp_top16(t);
+  if (lane < (uint32_t)kTopK) s_w[warp * kTopK + lane] = w;
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int i = 0; i < kTopK; i++) t[i] = INT64_MIN;
+    for (int i = lane; i < kWarps * kTopK; i += 32) top16_insert(t, s_w[i]);
+    const int64_t b = warp_top16(t);
+    if (lane < (uint32_t)kTopK) out16[lane] = b;
+  }
+}
+
 __global__ void __launch_bounds__(kT) k_topk_local16(const int64_t* rank, const unsigned long long* live, uint64_t n,
                                                      uint32_t k, int64_t* out) {
-  __shared__ int64_t s_v[kT * kTopK];
+  __shared__ int64_t s_w[(kT / 32) * kTopK];
+  __shared__ int64_t s_best[kTopK];
   int64_t t[kTopK];
 #pragma unroll
   for (int i = 0; i < kTopK; i++) t[i] = INT64_MIN;
@@ -421,38 +485,12 @@ __global__ void __launch_bounds__(kT) k_topk_local16(const int64_t* rank, const 
       r[u] = i < n ? __ldg(rank + i) : 0;
     }
 #pragma unroll
-    for (int u = 0; u < kU; u++) {
-      const int64_t v = r[u];
-      if (!l[u] || v <= t[kTopK - 1]) continue;
-#pragma unroll
-      for (int q = kTopK - 1; q > 0; q--) {  // insert into the descending list, dropping the smallest
-        const int64_t up = t[q - 1];
-        t[q] = v > up ? up : (v > t[q] ? v : t[q]);
-      }
-      t[0] = v > t[0] ? v : t[0];
-    }
+    for (int u = 0; u < kU; u++)
+      if (l[u]) top16_insert(t, r[u]);
   }
-#pragma unroll
-  for (int i = 0; i < kTopK; i++) s_v[threadIdx.x * kTopK + i] = t[i];
+  block_top16<kT>(t, s_w, s_best);
   __syncthreads();
-  // bitonic sort of kT * kTopK values, descending
-  constexpr int N = kT * kTopK;
-  for (int size = 2; size <= N; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int i = threadIdx.x; i < N / 2; i += kT) {
-        const int lo = 2 * i - (i & (stride - 1));
-        const int hi = lo + stride;
-        const bool desc = (lo & size) == 0;
-        const int64_t a = s_v[lo], b = s_v[hi];
-        if (desc ? a < b : a > b) {
-          s_v[lo] = b;
-          s_v[hi] = a;
-        }
-      }
-      __syncthreads();
-    }
-  }
-  if (threadIdx.x < k) out[(uint64_t)blockIdx.x * k + threadIdx.x] = s_v[threadIdx.x];
+  if (threadIdx.x < k) out[(uint64_t)blockIdx.x * k + threadIdx.x] = s_best[threadIdx.x];
 }
 
 // Collect live slots whose ranking value is at least the threshold.
@@ -467,30 +505,20 @@ __global__ void __launch_bounds__(kT) k_topk_collect(const int64_t* rank, const 
 }
 
 // Threshold on the device: the k-th largest of the per-block candidate lists (m values,
-// m <= kMergeMax), by a bitonic sort in shared memory.
+// m <= kMergeMax).
 constexpr int kMergeThreads = 1024;
 constexpr int kMergeMax = 4096;
 __global__ void __launch_bounds__(kMergeThreads) k_topk_merge(const int64_t* best, uint32_t m, uint32_t k,
                                                               int64_t* thr) {
-  __shared__ int64_t s_v[kMergeMax];
-  for (uint32_t i = threadIdx.x; i < kMergeMax; i += kMergeThreads) s_v[i] = i < m ? best[i] : INT64_MIN;
+  __shared__ int64_t s_w[(kMergeThreads / 32) * kTopK];
+  __shared__ int64_t s_best[kTopK];
+  int64_t t[kTopK];
+#pragma unroll
+  for (int i = 0; i < kTopK; i++) t[i] = INT64_MIN;
+  for (uint32_t i = threadIdx.x; i < m; i += kMergeThreads) top16_insert(t, best[i]);
+  block_top16<kMergeThreads>(t, s_w, s_best);
   __syncthreads();
-  for (int size = 2; size <= kMergeMax; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int i = threadIdx.x; i < kMergeMax / 2; i += kMergeThreads) {
-        const int lo = 2 * i - (i & (stride - 1));
-        const int hi = lo + stride;
-        const bool desc = (lo & size) == 0;
-        const int64_t a = s_v[lo], b = s_v[hi];
-        if (desc ? a < b : a > b) {
-          s_v[lo] = b;
-          s_v[hi] = a;
-        }
-      }
-      __syncthreads();
-    }
-  }
-  if (threadIdx.x == 0) *thr = s_v[k - 1];
+  if (threadIdx.x == 0) *thr = s_best[k - 1];
 }
 
 // Collect live slots whose ranking value is at least the device-side threshold.
@@ -565,9 +593,12 @@ struct FastArgs {
 };
 
 struct SegPlan {
-  int64_t bit_off;  // bitmap index of a probe key = stored value + bit_off (= lower - kmin)
-  uint32_t narrow;  // every staged column stores <= 32 bits and the 32-bit bitmap index is exact
-  uint32_t pad;
+  uint32_t narrow;  // every staged column stores <= 32 bits: 32-bit evaluation
+  // probe key x (stored value) against the key bitmap, in 32 bits: member when
+  // x - xlo <= xspan (unsigned) and bit (x - xlo + boff) is set; kmember 0: no stored
+  // value of the segment lies in the bitmap's key range
+  uint32_t kmember;
+  uint32_t xlo, xspan, boff, pad;
 };
 
 enum : uint32_t { kCjGeneric = 0, kCjIn = 1, kCjOut = 2, kCjNever = 3, kCjAlways = 4 };
@@ -690,13 +721,18 @@ __device__ __forceinline__ uint32_t conj_filter32(const Conj& cj, const ConjSeg&
     }
   }
 }
-__device__ __forceinline__ uint32_t probe_filter32(const HtView& h, uint32_t bit_off, const uint32_t (&x)[kItems],
+__device__ __forceinline__ uint32_t probe_filter32(const HtView& h, const SegPlan& sp, const uint32_t (&x)[kItems],
                                                    uint32_t live) {
-  const uint32_t nbits = (uint32_t)h.nbits;
+  if (!sp.kmember) return 0;
 #pragma unroll
   for (int k = 0; k < kItems; k++) {
-    const uint32_t o = x[k] + bit_off;
-    if (((live >> k) & 1) && (o >= nbits || !((__ldg(h.bits + (o >> 5)) >> (o & 31)) & 1u))) live &= ~(1u << k);
+    const uint32_t d = x[k] - sp.xlo;
+    if (d > sp.xspan) {
+      live &= ~(1u << k);
+      continue;
+    }
+    const uint32_t o = d + sp.boff;
+    if (((live >> k) & 1) && !((__ldg(h.bits + (o >> 5)) >> (o & 31)) & 1u)) live &= ~(1u << k);
   }
   return live;
 }
@@ -840,7 +876,7 @@ __device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity) {
   return false;
 }
 
-constexpr uint32_t kStages = 4;  // tiles in flight per block
+constexpr uint32_t kMaxStages = 4;  // tiles in flight per block, at most
 
 struct TmaArgs {
   FastArgs f;
@@ -848,47 +884,70 @@ struct TmaArgs {
   uint32_t staged_slot[kStaged];  // scan slot of each staged column
   uint32_t col_off[kStaged];      // byte offset of each staged column in a stage buffer
   uint32_t stage_bytes;           // shared bytes of one stage (all staged columns, kTile rows)
+  uint32_t nst;                   // stages in flight (2 .. kMaxStages)
   uint32_t conj_st[kMaxConj];     // staged index of each conjunct's column
   int32_t probe_st;               // staged index of the probe key (-1: no probe)
+  // Build stage whose key and payload are all scan columns: the consumers insert their
+  // survivors straight from the staged tile (no hit list).
+  uint32_t inline_build;
+  uint32_t key_st;     // staged index of the build key
+  uint32_t pay_st[8];  // staged index of each payload column
 };
 
-// Dynamic shared memory of k_stage_tma: kStages stage buffers, then the segment tile
-// prefix, the staged columns' per-segment descriptors and the conjuncts' per-segment
-// raw-domain tests, so that issuing and evaluating a tile read shared memory only.
-__host__ __device__ inline uint32_t tma_tile_table_off(uint32_t stage_bytes) { return kStages * stage_bytes; }
-__host__ __device__ inline uint32_t tma_desc_off(uint32_t stage_bytes, uint32_t nseg) {
-  return (tma_tile_table_off(stage_bytes) + (nseg + 1) * 4 + 15) & ~15u;
+// Dynamic shared memory of k_stage_tma: nst stage buffers, then the segment tile prefix,
+// the staged columns' per-segment descriptors, the conjuncts' per-segment raw-domain
+// tests and the per-segment plans, so that issuing and evaluating a tile read shared
+// memory only.
+__host__ __device__ inline uint32_t tma_tile_table_off(uint32_t stage_bytes, uint32_t nst) {
+  return nst * stage_bytes;
 }
-__host__ __device__ inline uint32_t tma_cseg_off(uint32_t stage_bytes, uint32_t nseg, uint32_t nstaged) {
-  return tma_desc_off(stage_bytes, nseg) + nstaged * nseg * (uint32_t)sizeof(alk_colseg);
+__host__ __device__ inline uint32_t tma_desc_off(uint32_t stage_bytes, uint32_t nst, uint32_t nseg) {
+  return (tma_tile_table_off(stage_bytes, nst) + (nseg + 1) * 4 + 15) & ~15u;
 }
-__host__ __device__ inline uint32_t tma_splan_off(uint32_t stage_bytes, uint32_t nseg, uint32_t nstaged,
-                                                  uint32_t nconj) {
-  return tma_cseg_off(stage_bytes, nseg, nstaged) + nconj * nseg * (uint32_t)sizeof(ConjSeg);
+__host__ __device__ inline uint32_t tma_cseg_off(uint32_t stage_bytes, uint32_t nst, uint32_t nseg, uint32_t nstaged) {
+  return tma_desc_off(stage_bytes, nst, nseg) + nstaged * nseg * (uint32_t)sizeof(alk_colseg);
 }
-__host__ __device__ inline uint32_t tma_smem_bytes(uint32_t stage_bytes, uint32_t nseg, uint32_t nstaged,
-                                                   uint32_t nconj) {
-  return tma_splan_off(stage_bytes, nseg, nstaged, nconj) + nseg * (uint32_t)sizeof(SegPlan);
+__host__ __device__ inline uint32_t tma_splan_off(uint32_t stage_bytes, uint32_t nst, uint32_t nseg,
+                                                  uint32_t nstaged, uint32_t nconj) {
+  return tma_cseg_off(stage_bytes, nst, nseg, nstaged) + nconj * nseg * (uint32_t)sizeof(ConjSeg);
+}
+__host__ __device__ inline uint32_t tma_smem_bytes(uint32_t stage_bytes, uint32_t nst, uint32_t nseg,
+                                                   uint32_t nstaged, uint32_t nconj) {
+  return tma_splan_off(stage_bytes, nst, nseg, nstaged, nconj) + nseg * (uint32_t)sizeof(SegPlan);
+}
+
+// Decoded value of row r of a staged column.
+__device__ __forceinline__ int64_t staged_value(const unsigned char* p, const alk_colseg& d, uint32_t r) {
+  uint64_t x;
+  switch (d.bits) {
+    case 8: x = p[r]; break;
+    case 16: x = ((const uint16_t*)p)[r]; break;
+    case 32: x = ((const uint32_t*)p)[r]; break;
+    default: x = ((const unsigned long long*)p)[r]; break;
+  }
+  return (int64_t)(x + (uint64_t)d.lower);
 }
 
 __global__ void __launch_bounds__(kTmaThreads) k_stage_tma(const __grid_constant__ TmaArgs t) {
   const FastArgs& f = t.f;
   const StageArgs& a = f.a;
+  const uint32_t nst = t.nst;
   extern __shared__ __align__(128) unsigned char s_dyn[];
-  __shared__ __align__(8) uint64_t s_full[kStages], s_empty[kStages];
+  __shared__ __align__(8) uint64_t s_full[kMaxStages], s_empty[kMaxStages];
   __shared__ int s_abort;
-  uint32_t* s_tile = (uint32_t*)(s_dyn + tma_tile_table_off(t.stage_bytes));
-  alk_colseg* s_cd = (alk_colseg*)(s_dyn + tma_desc_off(t.stage_bytes, a.nseg));  // [nstaged][nseg]
-  ConjSeg* s_cs = (ConjSeg*)(s_dyn + tma_cseg_off(t.stage_bytes, a.nseg, t.nstaged));  // [nconj][nseg]
+  __shared__ uint16_t s_rows[kCW * 32 * kItems];  // per consumer warp: survivors of its slice (inline build)
+  uint32_t* s_tile = (uint32_t*)(s_dyn + tma_tile_table_off(t.stage_bytes, nst));
+  alk_colseg* s_cd = (alk_colseg*)(s_dyn + tma_desc_off(t.stage_bytes, nst, a.nseg));  // [nstaged][nseg]
+  ConjSeg* s_cs = (ConjSeg*)(s_dyn + tma_cseg_off(t.stage_bytes, nst, a.nseg, t.nstaged));  // [nconj][nseg]
   for (uint32_t i = threadIdx.x; i <= a.nseg; i += kTmaThreads) s_tile[i] = a.seg_tile[i];
   for (uint32_t i = threadIdx.x; i < t.nstaged * a.nseg; i += kTmaThreads)
     s_cd[i] = a.cols[t.staged_slot[i / a.nseg] * a.nseg + i % a.nseg];
   for (uint32_t i = threadIdx.x; i < f.nconj * a.nseg; i += kTmaThreads) s_cs[i] = f.cseg[i];
-  SegPlan* s_sp = (SegPlan*)(s_dyn + tma_splan_off(t.stage_bytes, a.nseg, t.nstaged, f.nconj));  // [nseg]
+  SegPlan* s_sp = (SegPlan*)(s_dyn + tma_splan_off(t.stage_bytes, nst, a.nseg, t.nstaged, f.nconj));  // [nseg]
   for (uint32_t i = threadIdx.x; i < a.nseg; i += kTmaThreads) s_sp[i] = f.splan[i];
   if (threadIdx.x == 0) {
     s_abort = 0;
-    for (uint32_t i = 0; i < kStages; i++) {
+    for (uint32_t i = 0; i < nst; i++) {
       mbar_init(&s_full[i], 1);
       mbar_init(&s_empty[i], kCW);
     }
@@ -905,8 +964,8 @@ __global__ void __launch_bounds__(kTmaThreads) k_stage_tma(const __grid_constant
     for (uint32_t it = 0;; it++) {
       const uint32_t tile = blockIdx.x + it * gridDim.x;
       if (tile >= a.ntiles || *abort_flag) break;
-      const uint32_t st = it % kStages;
-      if (it >= kStages && !mbar_wait(&s_empty[st], (it / kStages - 1) & 1)) {
+      const uint32_t st = it % nst;
+      if (it >= nst && !mbar_wait(&s_empty[st], (it / nst - 1) & 1)) {
         atomicExch(a.err, ALK_ERR_TIMEOUT);
         *abort_flag = 1;
         break;
@@ -927,20 +986,20 @@ __global__ void __launch_bounds__(kTmaThreads) k_stage_tma(const __grid_constant
       issued = it + 1;
     }
     // every copy issued has landed before the block may exit (bounded)
-    for (uint32_t it = issued > kStages ? issued - kStages : 0; it < issued; it++)
-      mbar_wait(&s_full[it % kStages], (it / kStages) & 1);
+    for (uint32_t it = issued > nst ? issued - nst : 0; it < issued; it++)
+      mbar_wait(&s_full[it % nst], (it / nst) & 1);
     return;
   }
 
   // ---- consumers: warp `warp` owns rows warp * 256 + k * 32 + lane of every tile
-  unsigned long long rows_seen = 0;
+  unsigned long long rows_seen = 0, inserted = 0, survivors = 0;  // survivors: inline builds
   HitWriter hw;
   const uint32_t r0 = warp * (32 * kItems) + lane;
   for (uint32_t it = 0;; it++) {
     const uint32_t tile = blockIdx.x + it * gridDim.x;
     if (tile >= a.ntiles || __any_sync(0xffffffffu, *abort_flag)) break;
-    const uint32_t st = it % kStages;
-    if (!mbar_wait_warp(&s_full[st], (it / kStages) & 1)) {
+    const uint32_t st = it % nst;
+    if (!mbar_wait_warp(&s_full[st], (it / nst) & 1)) {
       if (lane == 0) {
         atomicExch(a.err, ALK_ERR_TIMEOUT);
         *abort_flag = 1;
@@ -967,7 +1026,7 @@ __global__ void __launch_bounds__(kTmaThreads) k_stage_tma(const __grid_constant
       if (t.probe_st >= 0 && a.probe.bits) {
         const alk_colseg& d = s_cd[t.probe_st * a.nseg + seg];
         load_raw32<32>(buf + t.col_off[t.probe_st], d.bits, r0, x);
-        live = probe_filter32(a.probe, (uint32_t)sp.bit_off, x, live);
+        live = probe_filter32(a.probe, sp, x, live);
       }
     } else {
       uint64_t x[kItems];
@@ -982,14 +1041,62 @@ __global__ void __launch_bounds__(kTmaThreads) k_stage_tma(const __grid_constant
         live = probe_filter(a.probe, d.lower, x, live);
       }
     }
+    if (t.inline_build) {
+      // insert the survivors from the staged tile, then release it; the warp's survivors
+      // are first compacted so that all lanes insert at once (one compare-and-swap round
+      // trip per 32 survivors)
+      survivors += __popc(live);
+      uint32_t excl;
+      const uint32_t total = __any_sync(0xffffffffu, live) ? warp_offsets(__popc(live), &excl) : 0;
+      uint16_t* wl = s_rows + warp * (32 * kItems);
+      uint32_t q = excl;
+      for (uint32_t m = total ? live : 0; m; m &= m - 1, q++) wl[q] = (uint16_t)(r0 + (__ffs(m) - 1) * 32);
+      __syncwarp();
+      // rounds of 32 survivors; the last round's values are read into registers and the
+      // stage is released before its inserts, so the producer refills it meanwhile
+      for (uint32_t j0 = 0; j0 < total; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        const bool mine = j < total;
+        int64_t key = 0, pv[8];
+        if (mine) {
+          const uint32_t r = wl[j];
+          key = staged_value(buf + t.col_off[t.key_st], s_cd[t.key_st * a.nseg + seg], r);
+#pragma unroll
+          for (uint32_t p = 0; p < 8; p++)
+            if (p < a.build.npay)
+              pv[p] = staged_value(buf + t.col_off[t.pay_st[p]], s_cd[t.pay_st[p] * a.nseg + seg], r);
+        }
+        if (j0 + 32 >= total) {
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&s_empty[st]);
+        }
+        const int64_t sl = mine ? ht_insert(a.build, key) : -1;
+        if (sl >= 0) {
+          inserted++;
+#pragma unroll
+          for (uint32_t p = 0; p < 8; p++)
+            if (p < a.build.npay) a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = pv[p];
+        }
+        __syncwarp();
+      }
+      __syncwarp();  // the survivor list is rewritten by the next tile
+      if (total == 0 && lane == 0) mbar_arrive(&s_empty[st]);
+      continue;
+    }
     // the slice's values are in registers: release the stage to the producer
     __syncwarp();
     if (lane == 0) mbar_arrive(&s_empty[st]);
     hw.append<32>(a, live, seg, (uint64_t)row0 + r0);
   }
   hw.finish(a);
-  for (int o = 16; o; o >>= 1) rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
+  for (int o = 16; o; o >>= 1) {
+    rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
+    inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
+    survivors += __shfl_xor_sync(0xffffffffu, survivors, o);
+  }
   if (lane == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
+  if (lane == 0 && inserted) atomicAdd(a.build.nslots, inserted);
+  if (lane == 0 && survivors) atomicAdd(a.hit_rows, survivors);
 }
 
 // Host: recognise an AND of (column * mul OP constant) tests in a compiled predicate.
@@ -1067,8 +1174,9 @@ int grid_for(uint64_t n) {
 
 // Static shared memory of k_stage_tma (barriers) next to its dynamic stage buffers and
 // tables; the SM offers 227 KB per block.
-constexpr size_t kTmaStaticSmem = 2 * 1024;
+constexpr size_t kTmaStaticSmem = 6 * 1024;
 constexpr size_t kSmemPerBlock = 227 * 1024;
+constexpr size_t kSmemPerSM = 228 * 1024;
 
 // Launch a stage as two kernels on one stream: the scan (the TMA-staged kernel when the
 // predicate is a conjunction and the staged columns fit in shared memory, else the
@@ -1077,49 +1185,65 @@ constexpr size_t kSmemPerBlock = 227 * 1024;
 // the device arguments and, when conj, the predicate's conjuncts.
 template <bool kBuild>
 cudaError_t launch_stage(const FastArgs& fa, bool conj, const alk_colseg* cols, const uint8_t* seg_mode,
-                         cudaStream_t s, alk_event_timer* timer) {
+                         const int32_t* h_pay_src, cudaStream_t s, alk_event_timer* timer) {
   const StageArgs& a = fa.a;
   if (!a.ntiles) return cudaSuccess;
   TmaArgs t{};
   bool tma = false;
-  if (conj) {
+  uint32_t tma_smem = 0;
+  // Stage the columns every row needs (and, for an inline build, the key and payload),
+  // with as many tiles in flight as keep 3 blocks per SM (2 at least).
+  auto plan = [&](bool with_build) -> bool {
+    t = TmaArgs{};
     t.f = fa;
     std::vector<uint32_t> st;
-    auto add = [&](uint32_t sl) {
-      if (std::find(st.begin(), st.end(), sl) == st.end()) st.push_back(sl);
+    auto add = [&](uint32_t sl) -> uint32_t {
+      auto it = std::find(st.begin(), st.end(), sl);
+      if (it != st.end()) return (uint32_t)(it - st.begin());
+      st.push_back(sl);
+      return (uint32_t)st.size() - 1;
     };
-    for (uint32_t c = 0; c < fa.nconj; c++) add(fa.conj[c].slot);
-    if (a.probe_slot >= 0) add((uint32_t)a.probe_slot);
+    for (uint32_t c = 0; c < fa.nconj; c++) t.conj_st[c] = add(fa.conj[c].slot);
+    t.probe_st = a.probe_slot >= 0 ? (int32_t)add((uint32_t)a.probe_slot) : -1;
+    if (with_build) {
+      t.inline_build = 1;
+      t.key_st = add((uint32_t)a.build_slot);
+      for (uint32_t p = 0; p < a.build.npay; p++) t.pay_st[p] = add((uint32_t)h_pay_src[p]);
+    }
+    if (st.empty() || st.size() > (size_t)kStaged) return false;
     // bulk copies need 16-byte aligned sources (row0 * width is a multiple of kTile)
-    bool aligned = true;
     uint32_t bytes = 0;
-    for (size_t i = 0; i < st.size() && i < (size_t)kStaged; i++) {
+    for (size_t i = 0; i < st.size(); i++) {
       uint32_t w = 1;
       for (uint32_t g = 0; g < a.nseg; g++) {
         if (!seg_mode[g]) continue;
         const alk_colseg& d = cols[st[i] * a.nseg + g];
         w = std::max<uint32_t>(w, d.bits / 8);
-        if ((uintptr_t)d.data & 15) aligned = false;
+        if ((uintptr_t)d.data & 15) return false;
       }
       t.col_off[i] = bytes;
+      t.staged_slot[i] = st[i];
       bytes += (kTile * w + 127) & ~127u;
     }
-    if (!st.empty() && st.size() <= (size_t)kStaged && aligned &&
-        kTmaStaticSmem + tma_smem_bytes(bytes, a.nseg, (uint32_t)st.size(), fa.nconj) <= kSmemPerBlock) {
-      t.nstaged = (uint32_t)st.size();
-      t.probe_st = -1;
-      for (size_t i = 0; i < st.size(); i++) {
-        t.staged_slot[i] = st[i];
-        if (a.probe_slot >= 0 && st[i] == (uint32_t)a.probe_slot) t.probe_st = (int32_t)i;
-        for (uint32_t c = 0; c < fa.nconj; c++)
-          if (fa.conj[c].slot == st[i]) t.conj_st[c] = (uint32_t)i;
+    t.nstaged = (uint32_t)st.size();
+    t.stage_bytes = bytes;
+    for (t.nst = kMaxStages; t.nst >= 2; t.nst--) {
+      const size_t need = kTmaStaticSmem + tma_smem_bytes(bytes, t.nst, a.nseg, t.nstaged, fa.nconj);
+      const bool three_fit = 3 * (need + 1024) <= kSmemPerSM;  // 1 KB per block is reserved
+      if (need <= kSmemPerBlock && (three_fit || t.nst == 2)) {
+        tma_smem = tma_smem_bytes(bytes, t.nst, a.nseg, t.nstaged, fa.nconj);
+        return true;
       }
-      t.stage_bytes = bytes;
-      tma = true;
     }
+    return false;
+  };
+  if (conj) {
+    // an inline build needs every payload value from the scan and the probe (if any)
+    // settled by the exact key bitmap
+    const bool can_inline = kBuild && h_pay_src && !a.need_slot && (a.probe_slot < 0 || a.probe.bits);
+    tma = (can_inline && plan(true)) || plan(false);
   }
   int occ = 0;
-  const uint32_t tma_smem = tma ? tma_smem_bytes(t.stage_bytes, a.nseg, t.nstaged, fa.nconj) : 0;
   if (tma) {
     cudaFuncSetAttribute(k_stage_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem);
     cudaFuncSetAttribute(k_stage_tma, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
@@ -1137,9 +1261,9 @@ cudaError_t launch_stage(const FastArgs& fa, bool conj, const alk_colseg* cols, 
   if (tma) k_stage_tma<<<grid, kTmaThreads, tma_smem, s>>>(t);
   else if (conj) k_stage_fast<<<grid, kT, 0, s>>>(fa);
   else k_stage_scan<<<grid, kT, 0, s>>>(a);
-  k_stage_hits<kBuild><<<sms() * std::max(occ_hits, 1), kT, 0, s>>>(a);
+  if (!(tma && t.inline_build)) k_stage_hits<kBuild><<<sms() * std::max(occ_hits, 1), kT, 0, s>>>(a);
   if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev1, s);
-  alk::g_kernel_launches += 2;
+  alk::g_kernel_launches += (tma && t.inline_build) ? 1 : 2;
   return cudaGetLastError();
 }
 
@@ -1331,7 +1455,7 @@ static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* co
   }
   // per segment: 32-bit evaluation when every staged column stores <= 32 bits and the
   // stored probe key maps to its bitmap index without leaving 32-bit arithmetic
-  std::vector<SegPlan> sp(a.nseg, SegPlan{0, 0, 0});
+  std::vector<SegPlan> sp(a.nseg, SegPlan{0, 0, 0, 0, 0, 0});
   for (uint32_t g = 0; g < a.nseg; g++) {
     bool narrow = conj;
     for (uint32_t c = 0; conj && c < fa.nconj; c++)
@@ -1339,13 +1463,18 @@ static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* co
     if (a.probe_slot >= 0) {
       const alk_colseg& d = cols[a.probe_slot * a.nseg + g];
       if (d.bits > 32) narrow = false;
-      if (a.probe.bits) {
-        const __int128 off = (__int128)d.lower - a.probe.kmin;
-        const __int128 xmax = ((__int128)1 << std::min<uint32_t>(d.bits, 64)) - 1;
-        const __int128 two32 = (__int128)1 << 32;
-        const bool fits = (off >= 0 && off + xmax < two32) || (off < 0 && -off <= two32 - (__int128)a.probe.nbits);
-        if (!fits) narrow = false;
-        else sp[g].bit_off = (int64_t)off;
+      if (narrow && a.probe.bits) {
+        // stored values x in [0, 2^bits) whose key x + lower lies in [kmin, kmin + nbits)
+        const __int128 blo = (__int128)a.probe.kmin - d.lower;  // x of the first bitmap key
+        const __int128 xmax = ((__int128)1 << d.bits) - 1;
+        const __int128 lo = std::max<__int128>(blo, 0);
+        const __int128 hi = std::min<__int128>(blo + (__int128)a.probe.nbits - 1, xmax);
+        if (lo <= hi) {
+          sp[g].kmember = 1;
+          sp[g].xlo = (uint32_t)lo;
+          sp[g].xspan = (uint32_t)(hi - lo);
+          sp[g].boff = (uint32_t)(lo - blo);  // < nbits <= 2^29
+        }
       }
     }
     sp[g].narrow = narrow ? 1 : 0;
@@ -1375,7 +1504,7 @@ static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* co
   fa.a = a;
   fa.cseg = (const ConjSeg*)(db + off_cs);
   fa.splan = (const SegPlan*)(db + off_sp);
-  CK(launch_stage<kBuild>(fa, conj, cols, seg_mode, s, timer));
+  CK(launch_stage<kBuild>(fa, conj, cols, seg_mode, kBuild ? (const int32_t*)(hb.data() + off_x) : nullptr, s, timer));
   static_assert(sizeof(alk_stage_status) == 32, "status mirrors the counters after the arguments");
   if (h_status) {  // asynchronous: the counters land in the caller's (pinned) status
     if (timer && timer->on && a.ntiles) timer->launches++;

@@ -64,10 +64,45 @@ def _column(values, bits=32):
 
 
 def test_build_hit_list_overflow_then_exact_rerun():
+    # a predicate that is not a conjunction runs on the register-machine scan, which
+    # hands its survivors to the hit kernel through the survivor list
     import torch
     L = _lib()
     n = 2_000_000
     keys = np.random.default_rng(3).permutation(n).astype(np.int64) * 3 + 11
+    buf, cs = _column(keys)
+    cols = (ColSeg * 1)(cs)
+    mode = (c.c_uint8 * 1)(2)
+    pred = _or_pred(0, 0)  # key >= 0 OR key < 0: every row
+    ht = c.c_void_p()
+    assert L.alk_ht_create_range(n, 0, int(keys.min()), int(keys.max()), c.byref(ht), None) == ALK_OK
+    try:
+        rows_in, hits = c.c_uint64(), c.c_uint64()
+        rc = L.alk_pipeline_build(cols, 1, 1, mode, c.byref(pred), None, -1, ht, 0, None, 1, c.byref(rows_in),
+                                  c.byref(hits), None)
+        assert rc == ALK_ERR_OVERFLOW
+        assert hits.value == n and rows_in.value == n
+        ins, fl = c.c_uint64(), c.c_int()
+        assert L.alk_ht_info(ht, c.byref(ins), c.byref(fl), None) == ALK_OK
+        assert ins.value == 0 and fl.value == 0  # nothing applied
+        rc = L.alk_pipeline_build(cols, 1, 1, mode, c.byref(pred), None, -1, ht, 0, None, hits.value,
+                                  c.byref(rows_in), c.byref(hits), None)
+        assert rc == ALK_OK and hits.value == n
+        assert L.alk_ht_info(ht, c.byref(ins), c.byref(fl), None) == ALK_OK
+        assert ins.value == n and fl.value == 0
+    finally:
+        L.alk_ht_free(ht, None)
+        torch.cuda.synchronize()
+    del buf
+
+
+def test_build_inline_from_staged_tile():
+    # no predicate and no probe: the TMA-staged scan inserts its rows itself (no survivor
+    # list, so no list capacity applies); a duplicate key is reported
+    import torch
+    L = _lib()
+    n = 2_000_000
+    keys = np.random.default_rng(4).permutation(n).astype(np.int64) * 3 + 11
     buf, cs = _column(keys)
     cols = (ColSeg * 1)(cs)
     mode = (c.c_uint8 * 1)(2)
@@ -77,16 +112,16 @@ def test_build_hit_list_overflow_then_exact_rerun():
         rows_in, hits = c.c_uint64(), c.c_uint64()
         rc = L.alk_pipeline_build(cols, 1, 1, mode, None, None, -1, ht, 0, None, 1, c.byref(rows_in), c.byref(hits),
                                   None)
-        assert rc == ALK_ERR_OVERFLOW
-        assert hits.value == n and rows_in.value == n
+        assert rc == ALK_OK and rows_in.value == n
         ins, fl = c.c_uint64(), c.c_int()
         assert L.alk_ht_info(ht, c.byref(ins), c.byref(fl), None) == ALK_OK
-        assert ins.value == 0 and fl.value == 0  # nothing applied
-        rc = L.alk_pipeline_build(cols, 1, 1, mode, None, None, -1, ht, 0, None, hits.value, c.byref(rows_in),
-                                  c.byref(hits), None)
-        assert rc == ALK_OK and hits.value == n
-        assert L.alk_ht_info(ht, c.byref(ins), c.byref(fl), None) == ALK_OK
         assert ins.value == n and fl.value == 0
+        # the same keys again: every insert meets its duplicate
+        rc = L.alk_pipeline_build(cols, 1, 1, mode, None, None, -1, ht, 0, None, 0, c.byref(rows_in), c.byref(hits),
+                                  None)
+        assert rc == ALK_OK
+        assert L.alk_ht_info(ht, c.byref(ins), c.byref(fl), None) == ALK_OK
+        assert ins.value == n and (fl.value & 1)
     finally:
         L.alk_ht_free(ht, None)
         torch.cuda.synchronize()
@@ -114,6 +149,20 @@ def _range_pred(slot, lo, hi):
     p.ins[0] = Instr(ALK_OP_GE, 0, ALK_K_COL, ALK_K_CONST, slot, 0, 0)
     p.ins[1] = Instr(ALK_OP_LT, 1, ALK_K_COL, ALK_K_CONST, slot, 1, 0)
     p.ins[2] = Instr(ALK_OP_AND, 2, ALK_K_REG, ALK_K_REG, 0, 1, 0)
+    return p
+
+
+ALK_OP_OR = 12
+
+
+def _or_pred(slot, c0):
+    """column(slot) >= c0 OR column(slot) < c0 (true for every row; not a conjunction)."""
+    p = Program()
+    p.n_instr, p.result = 3, 2
+    p.consts[0] = c0
+    p.ins[0] = Instr(ALK_OP_GE, 0, ALK_K_COL, ALK_K_CONST, slot, 0, 0)
+    p.ins[1] = Instr(ALK_OP_LT, 1, ALK_K_COL, ALK_K_CONST, slot, 0, 0)
+    p.ins[2] = Instr(ALK_OP_OR, 2, ALK_K_REG, ALK_K_REG, 0, 1, 0)
     return p
 
 
