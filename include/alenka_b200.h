@@ -324,6 +324,18 @@ int alk_live_compact(const uint64_t* d_live, uint64_t n, uint32_t* d_out, uint64
  * (the argument queues of the reference's grammar actions, bison.y:127-287). */
 int alk_parse_dump(const char* script, char* out, int out_len);
 
+/* Seeded synthetic tables in the reference's on-disk format (no counterpart in the
+ * reference, which loads text files): the single-table lineitem shape and the
+ * customer/orders/lineitem shape of the three-way pipeline, in segments of seg_rows
+ * rows (0: one segment), FOR or (delta != 0) FOR-delta for sorted integer columns.
+ * 0 on success; a message is written into err (err_len bytes) otherwise. */
+int alk_gen_lineitem_flat(const char* dir, uint64_t rows, uint32_t seg_rows, uint64_t seed, int delta,
+                          char* err, int err_len);
+int alk_gen_three_way(const char* dir, uint64_t customers, uint64_t orders, uint64_t lineitems,
+                      uint32_t seg_rows, uint64_t seed, int delta, char* err, int err_len);
+/* A yyyymmdd date value moved by a number of days (proleptic Gregorian). */
+int64_t alk_date_add_days(int64_t yyyymmdd_value, int64_t days);
+
 /* Device properties of the current device. */
 int alk_device_info(int* sm_count, int* cc_major, int* cc_minor);
 
