@@ -16,6 +16,7 @@ ALK_ERR_OVERFLOW = 3
 ALK_ERR_UNSUPPORTED = 5
 ALK_SESSION_RESIDENT = 1
 ALK_SESSION_PLAIN = 2
+ALK_SESSION_NOGRAPH = 4
 
 _lib = None
 
@@ -37,6 +38,7 @@ class Stats(ctypes.Structure):
         ("hot_kernel_ms", ctypes.c_double),
         ("hot_kernel_bytes", ctypes.c_uint64),
         ("hot_kernel_launches", ctypes.c_uint64),
+        ("query_device_ms", ctypes.c_double),
     ]
 
 
@@ -92,8 +94,9 @@ def lib():
 class Session:
     """An engine session over a data directory (data.dictionary + segment files)."""
 
-    def __init__(self, data_dir, resident=True, plain=False):
-        flags = (ALK_SESSION_RESIDENT if resident else 0) | (ALK_SESSION_PLAIN if plain else 0)
+    def __init__(self, data_dir, resident=True, plain=False, graphs=True):
+        flags = ((ALK_SESSION_RESIDENT if resident else 0) | (ALK_SESSION_PLAIN if plain else 0)
+                 | (0 if graphs else ALK_SESSION_NOGRAPH))
         h = ctypes.c_void_p()
         rc = lib().alk_session_open(str(data_dir).encode(), flags, ctypes.byref(h))
         if rc != ALK_OK:

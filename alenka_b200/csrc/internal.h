@@ -3,10 +3,19 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace alk {
 int cuda_fail(cudaError_t e);
 void set_last_cuda_error(cudaError_t e);
 const char* last_cuda_error();
 // sm_100a kernel launches issued by this library since load (statistics).
 extern uint64_t g_kernel_launches;
+
+// Source pointer for a host-to-device upload of `bytes` from `host`: the caller's buffer,
+// or, while the stream is being captured into a CUDA graph, a pinned copy that must live
+// as long as the graph. Such copies are listed in capture_host_buffers() (this thread);
+// whoever ends the capture takes them over and frees them (cudaFreeHost) with the graph.
+const void* upload_source(const void* host, size_t bytes, cudaStream_t s, cudaError_t* err);
+std::vector<void*>& capture_host_buffers();
 }  // namespace alk

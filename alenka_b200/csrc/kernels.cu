@@ -586,6 +586,23 @@ void set_last_cuda_error(cudaError_t e) { g_last_cuda = e; }
 const char* last_cuda_error() { return cudaGetErrorString(g_last_cuda); }
 uint64_t g_kernel_launches = 0;
 
+std::vector<void*>& capture_host_buffers() {
+  static thread_local std::vector<void*> v;
+  return v;
+}
+
+const void* upload_source(const void* host, size_t bytes, cudaStream_t s, cudaError_t* err) {
+  *err = cudaSuccess;
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &st) != cudaSuccess || st != cudaStreamCaptureStatusActive) return host;
+  void* p = nullptr;
+  *err = cudaMallocHost(&p, bytes ? bytes : 1);
+  if (*err != cudaSuccess) return nullptr;
+  std::memcpy(p, host, bytes);
+  capture_host_buffers().push_back(p);
+  return p;
+}
+
 // Stream-ordered scratch owned by one entry-point call.
 struct Scratch {
   cudaStream_t s;
@@ -850,12 +867,13 @@ int alk_eval(const int64_t* const* d_cols, uint32_t ncols, uint64_t n, const alk
   std::vector<uint8_t> hb(sizeof(alk_program) + sizeof(void*) * kMaxCols, 0);
   std::memcpy(hb.data(), prog, sizeof(alk_program));
   if (ncols) std::memcpy(hb.data() + sizeof(alk_program), d_cols, sizeof(void*) * ncols);
-  CK(cudaMemcpyAsync(db, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
+  const void* src = alk::upload_source(hb.data(), hb.size(), s, &e);
+  CK(e);
+  CK(cudaMemcpyAsync(db, src, hb.size(), cudaMemcpyHostToDevice, s));
   k_eval<<<grid_for(n), kT, 0, s>>>((const int64_t* const*)(db + sizeof(alk_program)), ncols, n,
                                     (const alk_program*)db, d_out);
   alk::g_kernel_launches++;
   CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(s));
   return ALK_OK;
 }
 

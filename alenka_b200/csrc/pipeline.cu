@@ -1257,12 +1257,16 @@ cudaError_t launch_stage(const FastArgs& fa, bool conj, const alk_colseg* cols, 
   const int grid = std::min<int>((int)a.ntiles, sms() * std::min(std::max(occ, 1), 8));
   int occ_hits = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_hits, k_stage_hits<kBuild>, kT, 0);
-  if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev0, s);
+  // inside a stream capture the timing events become event-record nodes of the graph
+  cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+  if (timer && timer->on) cudaStreamIsCapturing(s, &cst);
+  const unsigned evflags = cst == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
+  if (timer && timer->on) cudaEventRecordWithFlags((cudaEvent_t)timer->ev0, s, evflags);
   if (tma) k_stage_tma<<<grid, kTmaThreads, tma_smem, s>>>(t);
   else if (conj) k_stage_fast<<<grid, kT, 0, s>>>(fa);
   else k_stage_scan<<<grid, kT, 0, s>>>(a);
   if (!(tma && t.inline_build)) k_stage_hits<kBuild><<<sms() * std::max(occ_hits, 1), kT, 0, s>>>(a);
-  if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev1, s);
+  if (timer && timer->on) cudaEventRecordWithFlags((cudaEvent_t)timer->ev1, s, evflags);
   alk::g_kernel_launches += (tma && t.inline_build) ? 1 : 2;
   return cudaGetLastError();
 }
@@ -1489,7 +1493,10 @@ static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* co
   std::memcpy(up.data() + off_sp, sp.data(), sp.size() * sizeof(SegPlan));
   uint8_t* db = nullptr;
   CK(cudaMallocAsync((void**)&db, off_hits + std::max<uint64_t>(hit_cap, 1) * sizeof(Hit), s));
-  CK(cudaMemcpyAsync(db, up.data(), up.size(), cudaMemcpyHostToDevice, s));
+  cudaError_t ue;
+  const void* src = alk::upload_source(up.data(), up.size(), s, &ue);
+  CK(ue);
+  CK(cudaMemcpyAsync(db, src, up.size(), cudaMemcpyHostToDevice, s));
   uint8_t* tail = db + off_tail;
   CK(cudaMemsetAsync(tail, 0, 32, s));
   patch(a, db);

@@ -3,6 +3,8 @@
 // execution. All device work goes through the operator-level C ABI.
 #include "engine.h"
 
+#include "../csrc/internal.h"
+
 #include <algorithm>
 #include <array>
 #include <climits>
@@ -15,7 +17,10 @@ namespace alk {
 
 namespace {
 void check(int rc, const char* what) {
-  if (rc != ALK_OK) throw EngineError(rc, std::string(what) + " failed (status " + std::to_string(rc) + ")");
+  if (rc == ALK_OK) return;
+  std::string m = std::string(what) + " failed (status " + std::to_string(rc) + ")";
+  if (rc == ALK_ERR_CUDA || rc == ALK_ERR_NOMEM) m += std::string(": ") + alk::last_cuda_error();
+  throw EngineError(rc, m);
 }
 void ck(cudaError_t e, const char* what) {
   if (e != cudaSuccess)
@@ -206,6 +211,8 @@ Engine::Engine(std::string dir, uint32_t flags) : dir_(std::move(dir)), flags_(f
   }
   cudaEventCreate(&ev0_);
   cudaEventCreate(&ev1_);
+  cudaEventCreate(&evq0_);
+  cudaEventCreate(&evq1_);
   std::string e;
   load_data_dict(dir_ + "/data.dictionary", dd_, e);
 }
@@ -223,6 +230,8 @@ Engine::~Engine() {
   cudaStreamSynchronize(stream_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
+  if (evq0_) cudaEventDestroy(evq0_);
+  if (evq1_) cudaEventDestroy(evq1_);
   if (pin_) cudaFreeHost(pin_);
   cudaStreamDestroy(stream_);
 }

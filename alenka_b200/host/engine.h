@@ -114,6 +114,30 @@ struct Rows {
   DevBufP seg_of_row;                // u32 source segment of every row (when requested)
 };
 
+// A fused stage whose counters are checked after the query's synchronisation.
+struct FusedPending {
+  std::string sig;  // stage signature (table, compiled predicate, zone-map verdicts, key)
+  int st, ht;       // index of its alk_stage_status / alk_ht_status (ht -1: none)
+  uint64_t upper;   // exact upper bound of its key count (rows scanned)
+};
+
+// What the fused plan needs after the device work: counters to check, the ORDER keys
+// and the STORE. A captured graph keeps one, so that a replay skips the planning.
+struct FusedTail {
+  std::vector<FusedPending> pending;
+  bool timed = false;                           // the probe-aggregate stage carries timing events
+  uint64_t streamed_bytes = 0, hit_bytes = 0;   // its algorithmic bytes: all rows, per survivor
+  size_t nouts = 0, ngroups = 0;                // F's columns, then the group keys, come back
+  std::vector<int> okey;
+  std::vector<bool> odesc;
+  std::vector<ColMeta> fmeta;
+  uint32_t limit = 0;
+  uint64_t small = 0, cand_cap = 0;             // rows returned with the first copy; candidate cap
+  std::string first_key, path, sep;
+  uint64_t kernels = 0, d2h = 0, rows = 0;      // statistics of one execution
+};
+struct FusedGraph;
+
 class Engine {
  public:
   Engine(std::string dir, uint32_t flags);
@@ -153,6 +177,7 @@ class Engine {
   std::map<std::string, uint64_t> card_feedback_;
   bool timing_ = false;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaEvent_t evq0_ = nullptr, evq1_ = nullptr;  // around a fused query's device work
   // Pinned host staging for device->host results (a pageable destination would make
   // every copy wait for the stream).
   void* pin_ = nullptr;
@@ -175,7 +200,18 @@ class Engine {
   void emit_order(Statement& st);
   void emit_store(Statement& st);
   bool try_fused(std::vector<Statement>& sts, size_t& i);
-  void run_fused(Statement& J, Statement& F, Statement& O, Statement& S);
+  void run_fused(Statement& J, Statement& F, Statement& O, Statement& S, const std::string& gkey);
+  // After the synchronisation: check the stages, record their counts, store the rows.
+  void finish_fused(const FusedTail& t);
+  void store_fused_rows(const FusedTail& t, std::vector<std::vector<int64_t>>& hf,
+                        std::vector<std::vector<int64_t>>& hg, uint64_t ncand);
+  // Fused queries captured as CUDA graphs, by script text and statement (resident
+  // sessions; captured on a query's second successful run, replayed from the third).
+  std::map<std::string, std::shared_ptr<FusedGraph>> fused_graphs_;
+  std::set<std::string> fused_seen_;
+  std::set<std::string> fused_nograph_;  // queries whose capture failed
+  std::string cur_script_;
+  bool big_fetch_ = false;  // bring every candidate back (ties beyond the first copy)
 
   friend struct Planner;
 };

@@ -15,7 +15,10 @@ namespace alk {
 
 namespace {
 void check(int rc, const char* what) {
-  if (rc != ALK_OK) throw EngineError(rc, std::string(what) + " failed (status " + std::to_string(rc) + ")");
+  if (rc == ALK_OK) return;
+  std::string m = std::string(what) + " failed (status " + std::to_string(rc) + ")";
+  if (rc == ALK_ERR_CUDA || rc == ALK_ERR_NOMEM) m += std::string(": ") + alk::last_cuda_error();
+  throw EngineError(rc, m);
 }
 void ck(cudaError_t e, const char* what) {
   if (e != cudaSuccess)
@@ -914,6 +917,7 @@ int Engine::execute(const std::string& script) {
     return ALK_ERR_PARSE;
   }
   reset_script_state();
+  cur_script_ = script;
   uint64_t k0 = g_kernel_launches;
   int rc = ALK_OK;
   try {
@@ -972,8 +976,66 @@ struct FusedFallback : std::runtime_error {
   using std::runtime_error::runtime_error;
 };
 [[noreturn]] void fallback(const std::string& why) { throw FusedFallback(why); }
-// A stage overflowed the size its recorded counts gave it; the counts are now exact.
-struct RerunFused {};
+// A stage overflowed the size its recorded counts gave it (the counts are now exact),
+// or (big) more candidates tie at the LIMIT boundary than the first copy brought back.
+struct RerunFused {
+  bool big = false;
+};
+
+// Counters of the fused stages, copied into pinned host memory ahead of the result rows.
+struct FusedStatus {
+  alk_stage_status st[3];  // build stage 1, build stage 2, probe-aggregate
+  alk_ht_status ht[2];
+};
+constexpr uint64_t kSmallCand = 1024;     // candidate rows returned with the first copy
+constexpr uint64_t kCandCap = 1 << 16;    // candidates at most (more ties: operator plan)
+
+// RAII for a stream capture: a capture that does not reach its end (an exception) is
+// ended and discarded, with the pinned uploads it made.
+struct CaptureGuard {
+  cudaStream_t s = nullptr;
+  bool active = false;
+  void begin(cudaStream_t st) {
+    alk::capture_host_buffers().clear();
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+      s = st;
+      active = true;
+    }
+  }
+  // ends the capture and returns the graph (null on failure); the pinned uploads move to `bufs`
+  cudaGraph_t end(std::vector<void*>& bufs) {
+    cudaGraph_t g = nullptr;
+    if (!active) return nullptr;
+    active = false;
+    if (cudaStreamEndCapture(s, &g) != cudaSuccess) g = nullptr;
+    bufs.swap(alk::capture_host_buffers());
+    alk::capture_host_buffers().clear();
+    return g;
+  }
+  ~CaptureGuard() {
+    if (!active) return;
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(s, &g);
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    for (void* p : alk::capture_host_buffers()) cudaFreeHost(p);
+    alk::capture_host_buffers().clear();
+  }
+};
+}  // namespace
+
+// An instantiated fused query with the host state its replays need.
+struct FusedGraph {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<void*> host_bufs;  // pinned uploads the graph copies from
+  FusedTail tail;
+  ~FusedGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (void* p : host_bufs) cudaFreeHost(p);
+  }
+};
+
+namespace {
 
 // One emit_multijoin step resolved like operators.cu:961-1033.
 struct StepInfo {
@@ -994,7 +1056,11 @@ void remap(alk_program& p, const std::vector<std::string>& names, const std::map
 struct HtGuard {
   alk_ht* h = nullptr;
   cudaStream_t s = nullptr;
-  ~HtGuard() { alk_ht_free(h, (alk_stream)s); }
+  void release() {
+    alk_ht_free(h, (alk_stream)s);
+    h = nullptr;
+  }
+  ~HtGuard() { release(); }
 };
 }  // namespace
 
@@ -1030,24 +1096,67 @@ bool Engine::try_fused(std::vector<Statement>& sts, size_t& i) {
     if (t != 'I') return false;
   for (auto& kv : J.join_and_cnt)
     if (kv.second) return false;
+  // graphs only where every input stays resident between queries
+  const std::string gkey = ((flags_ & ALK_SESSION_RESIDENT) && !(flags_ & ALK_SESSION_NOGRAPH))
+                               ? cur_script_ + "\n#" + std::to_string(i)
+                               : std::string();
+  big_fetch_ = false;
   for (int attempt = 0;; attempt++) {
+    // this run would capture the query into a graph (its second successful run)
+    const bool capturing = !gkey.empty() && fused_seen_.count(gkey) && !fused_graphs_.count(gkey) &&
+                           !fused_nograph_.count(gkey);
     try {
-      run_fused(J, F, O, S);
+      run_fused(J, F, O, S, fused_nograph_.count(gkey) ? std::string() : gkey);
       break;
+    } catch (const EngineError& e) {
+      if (!capturing) throw;
+      // the query could not be captured: it runs without a graph from now on
+      cudaGetLastError();
+      fused_nograph_.insert(gkey);
+      if (attempt >= 2) throw;
     } catch (const FusedFallback& e) {
+      big_fetch_ = false;
       return false;
-    } catch (const RerunFused&) {
-      // a rerun uses the exact counts the overflowing stage reported
-      if (attempt >= 2) return false;
+    } catch (const RerunFused& r) {
+      // a rerun uses the exact counts the overflowing stage reported, or fetches every
+      // tied candidate
+      fused_graphs_.erase(gkey);
+      fused_seen_.erase(gkey);
+      if (r.big) big_fetch_ = true;
+      if (attempt >= 2) {
+        big_fetch_ = false;
+        return false;
+      }
     }
   }
-  stats_.plan = 1;
+  big_fetch_ = false;
+  stats_.plan = std::max<uint32_t>(stats_.plan, 1);
   i += 3;
   return true;
 }
 
-void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
+void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, const std::string& gkey) {
   cudaStream_t s = stream_;
+  // a captured graph of this very query: replay it and do the host part
+  if (!gkey.empty() && !big_fetch_) {
+    auto it = fused_graphs_.find(gkey);
+    if (it != fused_graphs_.end()) {
+      std::shared_ptr<FusedGraph> g = it->second;
+      cudaEventRecord(evq0_, s);
+      ck(cudaGraphLaunch(g->exec, s), "graph launch");
+      cudaEventRecord(evq1_, s);
+      ck(cudaStreamSynchronize(s), "sync");
+      float qms = 0;
+      if (cudaEventElapsedTime(&qms, evq0_, evq1_) == cudaSuccess) stats_.query_device_ms += qms;
+      g_kernel_launches += g->tail.kernels;
+      stats_.d2h_bytes += g->tail.d2h;
+      stats_.rows_scanned += g->tail.rows;
+      finish_fused(g->tail);
+      stats_.plan = 2;
+      return;
+    }
+  }
+  const uint64_t rows_before = stats_.rows_scanned;
   // [min, max] of a base column over every segment, from the segment headers (zone maps)
   auto range_of = [&](Var* src, const std::string& col) {
     BaseCol& bc = basecol(src, col);
@@ -1179,21 +1288,22 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
   // bound (rows scanned). The stages run without host synchronisation. Their counters
   // are checked once the query's result is back, and a stage that overflowed makes the
   // whole query run again with the counts it reported.
-  struct FusedStatus {
-    alk_stage_status st[3];
-    alk_ht_status ht[2];
-  };
-  const uint64_t kSmallCand = 1024;  // candidate rows returned with the first copy
+  FusedTail tail;
+  tail.small = big_fetch_ ? kCandCap : kSmallCand;
+  tail.cand_cap = kCandCap;
   const size_t nback_max = outs.size() + group_cols.size();
-  uint8_t* pin = (uint8_t*)pinned(sizeof(FusedStatus) + 8 + kSmallCand * 8 * nback_max);
+  uint8_t* pin = (uint8_t*)pinned(sizeof(FusedStatus) + 8 + tail.small * 8 * nback_max);
   FusedStatus* fs = (FusedStatus*)pin;
   std::memset(fs, 0, sizeof(FusedStatus));
-  struct Pending {
-    std::string sig;
-    int st, ht;
-    uint64_t upper;
-  };
-  std::vector<Pending> pending;
+  // On a query's second successful run in a resident session, its device work (from here
+  // to the copies of the result) is captured into a CUDA graph and replayed afterwards.
+  CaptureGuard cap;
+  // the device-side top-k (LIMIT <= 16) keeps the query free of host round trips
+  const bool fast = S.op_nums[0] <= 16 && nback_max <= 32;
+  const bool capture = fast && !gkey.empty() && !big_fetch_ && fused_seen_.count(gkey);
+  const uint64_t k_before = g_kernel_launches;
+  if (capture) cap.begin(s);
+  else cudaEventRecord(evq0_, s);
   auto hit_cap_for = [&](const std::string& sig) -> uint64_t {
     auto it = card_feedback_.find(sig + "#hits");
     return it == card_feedback_.end() ? 0 : it->second + it->second / 4 + 4096;
@@ -1207,38 +1317,7 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     check(alk_ht_create_range(est, npay, range.first, range.second, &g.h, (alk_stream)s), "hash table");
     check(run(g.h, hit_cap_for(sig), &fs->st[idx]), "build stage");
     check(alk_ht_info_async(g.h, &fs->ht[idx], (alk_stream)s), "hash table");
-    pending.push_back({sig, idx, idx, upper});
-  };
-  // After the query's one synchronisation: record what every stage counted, or, when a
-  // stage overflowed, keep the counts up to that stage and drop the later stages' records
-  // (they ran on incomplete input) before running the query again.
-  auto verify = [&]() {
-    bool rerun = false;
-    for (auto& p : pending) {
-      if (rerun) {
-        card_feedback_.erase(p.sig);
-        card_feedback_.erase(p.sig + "#hits");
-        continue;
-      }
-      const alk_stage_status& st = fs->st[p.st];
-      if (st.err != ALK_OK && st.err != ALK_ERR_OVERFLOW) throw EngineError(st.err, "fused stage: wait expired");
-      card_feedback_[p.sig + "#hits"] = st.hits;
-      if (st.err == ALK_ERR_OVERFLOW) {
-        rerun = true;  // nothing of this stage was applied; its table count means nothing
-        continue;
-      }
-      if (p.ht < 0) continue;
-      const alk_ht_status& h = fs->ht[p.ht];
-      if (h.flags[1]) {
-        card_feedback_[p.sig] = p.upper;
-        rerun = true;
-      } else if (h.flags[0] || h.flags[3]) {
-        fallback("duplicate build keys or an inconsistent key range");
-      } else {
-        card_feedback_[p.sig] = h.inserted;
-      }
-    }
-    if (rerun) throw RerunFused();
+    tail.pending.push_back({sig, idx, idx, upper});
   };
   auto rows_of = [&](const ScanPlan& p, const std::vector<alk_colseg>& cs) {
     uint64_t n = 0;
@@ -1346,7 +1425,8 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     check(alk_fill_i64(acc->as<int64_t>() + g * stride, stride, init, (alk_stream)s), "init");
   }
   ck(cudaMemsetAsync(cnt->as<void>(), 0, stride * 8, s), "init");
-  alk_event_timer tm{timing_ ? 1 : 0, ev0_, ev1_, 0.0, 0};
+  // events bracket the probe-aggregate stage when timing is on, and always in a graph
+  alk_event_timer tm{(timing_ || capture) ? 1 : 0, ev0_, ev1_, 0.0, 0};
   // the probe-aggregate kernel accumulates into slot-indexed arrays sized for every slot
   const std::string sigf = plan_sig(pf) + "|" + st2.lkey + "|" + last_sig;
   if (nslots) {
@@ -1355,17 +1435,13 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
                                        kinds.data(), (uint32_t)aggs.size(), acc->as<int64_t>(), stride,
                                        cnt->as<uint64_t>(), hit_cap_for(sigf), &fs->st[2], (alk_stream)s, &tm),
           "probe-aggregate");
-    pending.push_back({sigf, 2, -1, 0});
+    tail.pending.push_back({sigf, 2, -1, 0});
+    tail.timed = tm.launches > 0;
   }
-  // device time and algorithmic bytes of the probe-aggregate stage (read after the sync)
-  auto record_timing = [&]() {
-    if (!timing_ || !nslots || !tm.launches) return;
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ev0_, ev1_);
-    stats_.hot_kernel_ms += ms;
-    stats_.hot_kernel_launches += tm.launches;
-    // Algorithmic bytes: the columns every row needs (predicate and probe key) over all
-    // rows scanned, plus one value of each aggregate input column per survivor.
+  // algorithmic bytes of the probe-aggregate stage: the columns every row needs
+  // (predicate and probe key) over all rows scanned, plus one value of each aggregate
+  // input column per survivor
+  {
     std::set<uint32_t> streamed = {probe_f}, per_hit;
     auto cols_of = [](const alk_program& p, std::set<uint32_t>& out) {
       for (uint32_t i = 0; i < p.n_instr; i++) {
@@ -1376,18 +1452,15 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     if (pf.has_pred) cols_of(pf.pred, streamed);
     for (auto& p : progs) cols_of(p, per_hit);
     for (uint32_t c : streamed) per_hit.erase(c);
-    const uint64_t hits = fs->st[2].hits;
-    uint64_t hit_bytes = 0;
     for (uint32_t c : per_hit) {
       uint32_t w = 1;
       BaseCol& bc = basecol(pf.src, pf.slots[c]);
       for (uint32_t g = 0; g < pf.src->segCount; g++)
         if (pf.mode[g]) w = std::max<uint32_t>(w, bc.segs[g].m.comp_type == 1 ? 8 : bc.segs[g].m.bits / 8);
-      hit_bytes += w;
+      tail.hit_bytes += w;
     }
-    stats_.hot_kernel_bytes +=
-        scan_bytes(pf, std::vector<uint32_t>(streamed.begin(), streamed.end())) + hits * hit_bytes;
-  };
+    tail.streamed_bytes = scan_bytes(pf, std::vector<uint32_t>(streamed.begin(), streamed.end()));
+  }
   // ---- F's columns over slots
   auto slot_col = [&](const std::string& alias) -> const int64_t* {
     const std::string& src = src_of.at(alias);
@@ -1472,75 +1545,165 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
     rank = rank_buf->as<int64_t>();
   }
   const uint32_t limit = (uint32_t)S.op_nums[0];
-  uint64_t ncand = 0;
-  const uint64_t cand_cap = 1 << 16;
-  auto cand = mkbuf(cand_cap * 4, s);
   // the candidate rows come back with F's columns followed by the group keys
   std::vector<const int64_t*> gcol;
   for (auto& g : group_cols) gcol.push_back(slot_col(g));
   std::vector<const int64_t*> back_cols(fcol);
   back_cols.insert(back_cols.end(), gcol.begin(), gcol.end());
   const size_t nback = back_cols.size();
-  std::vector<std::vector<int64_t>> hf(outs.size()), hg(gcol.size());
-  bool fetched = false;
-  if (limit <= 16 && nback <= 32) {
+  tail.nouts = outs.size();
+  tail.ngroups = gcol.size();
+  tail.okey = okey;
+  tail.odesc = odesc;
+  tail.fmeta = fmeta;
+  tail.limit = limit;
+  tail.first_key = O.op_type.at(0) == "NAME" ? O.op_value.at(0) : O.op_type.at(0);
+  tail.path = S.f;
+  tail.sep = S.sep;
+  auto cand = mkbuf(kCandCap * 4, s);
+  if (fast) {
     // threshold, candidates and their rows on the device; one copy back, the query's only
     // synchronisation
-    const uint64_t small = kSmallCand;
     auto dcount = mkbuf(8, s);
-    auto tmp = mkbuf(small * 8 * nback, s);
-    check(alk_topk_select(rank, cnt->as<uint64_t>(), nslots, limit, cand->as<uint32_t>(), cand_cap,
+    auto tmp = mkbuf(tail.small * 8 * nback, s);
+    check(alk_topk_select(rank, cnt->as<uint64_t>(), nslots, limit, cand->as<uint32_t>(), kCandCap,
                           dcount->as<uint64_t>(), (alk_stream)s),
           "top-k");
-    check(alk_gather_rows(back_cols.data(), (uint32_t)nback, cand->as<uint32_t>(), dcount->as<uint64_t>(), small,
-                          tmp->as<int64_t>(), (alk_stream)s),
+    check(alk_gather_rows(back_cols.data(), (uint32_t)nback, cand->as<uint32_t>(), dcount->as<uint64_t>(),
+                          tail.small, tmp->as<int64_t>(), (alk_stream)s),
           "gather");
     uint8_t* res = pin + sizeof(FusedStatus);
     ck(cudaMemcpyAsync(res, dcount->as<void>(), 8, cudaMemcpyDeviceToHost, s), "d2h");
-    ck(cudaMemcpyAsync(res + 8, tmp->as<void>(), small * 8 * nback, cudaMemcpyDeviceToHost, s), "d2h");
-    ck(cudaStreamSynchronize(s), "sync");
-    verify();
-    record_timing();
-    std::memcpy(&ncand, res, 8);
-    stats_.d2h_bytes += 8 + small * 8 * nback;
-    if (ncand > cand_cap) fallback("too many ties at the LIMIT boundary");
-    if (ncand <= small) {
-      const int64_t* rowsb = (const int64_t*)(res + 8);
-      for (size_t c = 0; c < nback; c++) {
-        auto& dst = c < outs.size() ? hf[c] : hg[c - outs.size()];
-        dst.assign(rowsb + c * small, rowsb + c * small + ncand);
+    ck(cudaMemcpyAsync(res + 8, tmp->as<void>(), tail.small * 8 * nback, cudaMemcpyDeviceToHost, s), "d2h");
+    tail.d2h = 8 + tail.small * 8 * nback;
+    stats_.d2h_bytes += tail.d2h;
+    // every device buffer of the query is released in stream order before the
+    // synchronisation (a captured graph owns all of them)
+    dcount.reset();
+    tmp.reset();
+    cand.reset();
+    rank_buf.reset();
+    keep.clear();
+    acc.reset();
+    cnt.reset();
+    ht2.release();
+    ht1.release();
+    tail.kernels = g_kernel_launches - k_before;
+    tail.rows = stats_.rows_scanned - rows_before;
+    if (capture) {
+      auto g = std::make_shared<FusedGraph>();
+      g->tail = tail;
+      cudaGraph_t graph = cap.end(g->host_bufs);
+      const bool ok = graph && cudaGraphInstantiate(&g->exec, graph, 0) == cudaSuccess;
+      if (graph) cudaGraphDestroy(graph);
+      if (!ok) {
+        cudaGetLastError();
+        throw EngineError(ALK_ERR_CUDA, "capture of the fused query into a CUDA graph failed");
       }
-      fetched = true;
+      cudaEventRecord(evq0_, s);
+      ck(cudaGraphLaunch(g->exec, s), "graph launch");
+      fused_graphs_[gkey] = g;
     }
-  } else {
-    int rc = alk_topk_candidates(rank, cnt->as<uint64_t>(), nslots, limit, cand->as<uint32_t>(), cand_cap, &ncand,
-                                 (alk_stream)s);
-    verify();
-    record_timing();
-    if (rc == ALK_ERR_OVERFLOW) fallback("too many ties at the LIMIT boundary");
-    check(rc, "top-k");
+    cudaEventRecord(evq1_, s);
+    ck(cudaStreamSynchronize(s), "sync");
+    float qms = 0;
+    if (cudaEventElapsedTime(&qms, evq0_, evq1_) == cudaSuccess) stats_.query_device_ms += qms;
+    finish_fused(tail);
+    if (!gkey.empty()) fused_seen_.insert(gkey);
+    return;
   }
-  // An empty join leaves the reference's SELECT a column-less set (emit_select,
-  // operators.cu:1847-1856), in which ORDER BY cannot find its first key.
-  if (ncand == 0) {
-    const std::string& t0 = O.op_type.at(0);
-    throw EngineError(ALK_ERR_ARG, "Couldn't find name " + (t0 == "NAME" ? O.op_value.at(0) : t0));
-  }
-  if (!fetched) {
-    for (auto& v : hf) v.resize(ncand);
-    for (auto& v : hg) v.resize(ncand);
-    auto tmp = mkbuf(ncand * 8 * (outs.size() + gcol.size()), s);
-    for (size_t c = 0; c < outs.size() + gcol.size(); c++) {
-      const int64_t* src = c < outs.size() ? fcol[c] : gcol[c - outs.size()];
-      check(alk_gather(src, cand->as<uint32_t>(), ncand, tmp->as<int64_t>() + c * ncand, (alk_stream)s), "gather");
-    }
-    for (size_t c = 0; c < outs.size() + gcol.size(); c++) {
+  // LIMIT above 16: the top-k threshold through the host, then every candidate's row
+  uint64_t ncand = 0;
+  int rc = alk_topk_candidates(rank, cnt->as<uint64_t>(), nslots, limit, cand->as<uint32_t>(), kCandCap, &ncand,
+                               (alk_stream)s);
+  tail.small = 0;
+  finish_fused(tail);  // checks the stages (no rows in pinned memory)
+  if (rc == ALK_ERR_OVERFLOW) fallback("too many ties at the LIMIT boundary");
+  check(rc, "top-k");
+  if (ncand == 0) throw EngineError(ALK_ERR_ARG, "Couldn't find name " + tail.first_key);
+  std::vector<std::vector<int64_t>> hf(outs.size(), std::vector<int64_t>(ncand)),
+      hg(gcol.size(), std::vector<int64_t>(ncand));
+  {
+    auto tmp = mkbuf(ncand * 8 * nback, s);
+    for (size_t c = 0; c < nback; c++)
+      check(alk_gather(back_cols[c], cand->as<uint32_t>(), ncand, tmp->as<int64_t>() + c * ncand, (alk_stream)s),
+            "gather");
+    for (size_t c = 0; c < nback; c++) {
       auto& dst = c < outs.size() ? hf[c] : hg[c - outs.size()];
       ck(cudaMemcpyAsync(dst.data(), tmp->as<int64_t>() + c * ncand, ncand * 8, cudaMemcpyDeviceToHost, s), "d2h");
     }
     ck(cudaStreamSynchronize(s), "sync");
-    stats_.d2h_bytes += ncand * 8 * (outs.size() + gcol.size());
+    stats_.d2h_bytes += ncand * 8 * nback;
   }
+  store_fused_rows(tail, hf, hg, ncand);
+}
+
+// After the query's one synchronisation: record what every stage counted, or, when a
+// stage overflowed, keep the counts up to that stage and drop the later stages' records
+// (they ran on incomplete input) and run the query again; then the probe-aggregate
+// stage's device time, and (t.small > 0) the rows from pinned memory into the STORE.
+void Engine::finish_fused(const FusedTail& t) {
+  const FusedStatus* fs = (const FusedStatus*)pin_;
+  bool rerun = false;
+  for (auto& p : t.pending) {
+    if (rerun) {
+      card_feedback_.erase(p.sig);
+      card_feedback_.erase(p.sig + "#hits");
+      continue;
+    }
+    const alk_stage_status& st = fs->st[p.st];
+    if (st.err != ALK_OK && st.err != ALK_ERR_OVERFLOW) throw EngineError(st.err, "fused stage: wait expired");
+    card_feedback_[p.sig + "#hits"] = st.hits;
+    if (st.err == ALK_ERR_OVERFLOW) {
+      rerun = true;  // nothing of this stage was applied; its table count means nothing
+      continue;
+    }
+    if (p.ht < 0) continue;
+    const alk_ht_status& h = fs->ht[p.ht];
+    if (h.flags[1]) {
+      card_feedback_[p.sig] = p.upper;
+      rerun = true;
+    } else if (h.flags[0] || h.flags[3]) {
+      fallback("duplicate build keys or an inconsistent key range");
+    } else {
+      card_feedback_[p.sig] = h.inserted;
+    }
+  }
+  if (rerun) throw RerunFused();
+  if (timing_ && t.timed) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    stats_.hot_kernel_ms += ms;
+    stats_.hot_kernel_launches += 1;
+    stats_.hot_kernel_bytes += t.streamed_bytes + fs->st[2].hits * t.hit_bytes;
+  }
+  if (!t.small) return;
+  const uint8_t* res = (const uint8_t*)pin_ + sizeof(FusedStatus);
+  uint64_t ncand = 0;
+  std::memcpy(&ncand, res, 8);
+  if (ncand > t.cand_cap) fallback("too many ties at the LIMIT boundary");
+  // An empty join leaves the reference's SELECT a column-less set (emit_select,
+  // operators.cu:1847-1856), in which ORDER BY cannot find its first key.
+  if (ncand == 0) throw EngineError(ALK_ERR_ARG, "Couldn't find name " + t.first_key);
+  if (ncand > t.small) throw RerunFused{true};
+  const int64_t* rowsb = (const int64_t*)(res + 8);
+  std::vector<std::vector<int64_t>> hf(t.nouts), hg(t.ngroups);
+  for (size_t c = 0; c < t.nouts + t.ngroups; c++) {
+    auto& dst = c < t.nouts ? hf[c] : hg[c - t.nouts];
+    dst.assign(rowsb + c * t.small, rowsb + c * t.small + ncand);
+  }
+  store_fused_rows(t, hf, hg, ncand);
+}
+
+// ORDER of the candidates with the full key list (ties: F's group-key order), then STORE
+// ... LIMIT (cm.cu:1479-1560).
+void Engine::store_fused_rows(const FusedTail& t, std::vector<std::vector<int64_t>>& hf,
+                              std::vector<std::vector<int64_t>>& hg, uint64_t ncand) {
+  const auto& okey = t.okey;
+  const auto& odesc = t.odesc;
+  const auto& fmeta = t.fmeta;
+  const size_t nouts = t.nouts;
+  const uint32_t limit = t.limit;
   std::vector<uint32_t> ord(ncand);
   std::iota(ord.begin(), ord.end(), 0);
   std::sort(ord.begin(), ord.end(), [&](uint32_t x, uint32_t y) {
@@ -1554,12 +1717,12 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
   });
   size_t rows = std::min<size_t>(ncand, limit);
   // ---- STORE (cm.cu:1479-1560)
-  std::string path = S.f;
+  std::string path = t.path;
   if (path.empty() || path[0] != '/') path = dir_ + "/" + path;
   FILE* fp = std::fopen(path.c_str(), "w");
   if (!fp) throw EngineError(ALK_ERR_IO, "Could not open file " + path);
-  std::vector<const std::vector<std::string>*> dicts(outs.size(), nullptr);
-  for (size_t c = 0; c < outs.size(); c++) {
+  std::vector<const std::vector<std::string>*> dicts(nouts, nullptr);
+  for (size_t c = 0; c < nouts; c++) {
     const std::string& sm = fmeta[c].string_map;
     if (sm.empty()) continue;
     auto dot = sm.find('.');
@@ -1572,22 +1735,22 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S) {
   std::string line;
   for (size_t r = 0; r < rows; r++) {
     line.clear();
-    for (size_t c = 0; c < outs.size(); c++) {
+    for (size_t c = 0; c < nouts; c++) {
       int64_t v = hf[c][ord[r]];
       if (!dicts[c]) {
         if (fmeta[c].dz) {
-          std::string t = std::to_string(v);
-          while (t.size() <= fmeta[c].dz) t = '0' + t;
-          t.insert(t.size() - fmeta[c].dz, ".");
-          line += t;
+          std::string d = std::to_string(v);
+          while (d.size() <= fmeta[c].dz) d = '0' + d;
+          d.insert(d.size() - fmeta[c].dz, ".");
+          line += d;
         } else {
           line += std::to_string(v);
         }
       } else {
-        std::string t = (v >= 0 && (size_t)v < dicts[c]->size()) ? (*dicts[c])[v] : std::string();
-        line += t.substr(0, std::strlen(t.c_str()));
+        std::string d = (v >= 0 && (size_t)v < dicts[c]->size()) ? (*dicts[c])[v] : std::string();
+        line += d.substr(0, std::strlen(d.c_str()));
       }
-      line += S.sep;
+      line += t.sep;
     }
     if (r + 1 != rows) line += "\n";
     std::fputs(line.c_str(), fp);

@@ -87,6 +87,60 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+class NvmlClockSampler:
+    """SM clock, power and throttle reasons read through NVML every 2 ms during the timed
+    region (the region lasts tens of milliseconds, below nvidia-smi's polling period).
+    Read-only: no setting of the GPU is changed."""
+
+    def __init__(self, gpu_index):
+        import pynvml
+        self.n = pynvml
+        pynvml.nvmlInit()
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        idx = int(vis.split(",")[gpu_index]) if vis and vis.split(",")[gpu_index].strip().isdigit() else gpu_index
+        self.h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+        self.samples, self.reasons = [], 0
+        self.stop_flag = threading.Event()
+
+    def _run(self):
+        n = self.n
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append(n.nvmlDeviceGetClockInfo(self.h, n.NVML_CLOCK_SM))
+                self.reasons |= n.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def start(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+
+    def stop(self):
+        self.stop_flag.set()
+        self.t.join()
+        n = self.n
+        names = {n.nvmlClocksEventReasonHwSlowdown: "hw_slowdown",
+                 n.nvmlClocksEventReasonHwThermalSlowdown: "hw_thermal_slowdown",
+                 n.nvmlClocksEventReasonSwThermalSlowdown: "sw_thermal_slowdown",
+                 n.nvmlClocksEventReasonSwPowerCap: "sw_power_cap",
+                 n.nvmlClocksEventReasonHwPowerBrakeSlowdown: "hw_power_brake_slowdown"}
+        try:
+            mx = n.nvmlDeviceGetMaxClockInfo(self.h, n.NVML_CLOCK_SM)
+        except Exception:
+            mx = None
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": mx,
+                "reasons": sorted(v for k, v in names.items() if self.reasons & k), "samples": len(self.samples),
+                "source": "nvml, 2 ms"}
+
+
+def clock_sampler(gpu_index):
+    try:
+        return NvmlClockSampler(gpu_index)
+    except Exception:
+        return ClockSampler(gpu_index)
+
+
 def measured_peak_hbm():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -174,7 +228,8 @@ def timed_steps(sess, script, steps, torch, dist):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    acc = {"kernels": 0, "h2d": 0, "d2h": 0, "rows": 0, "hot_ms": 0.0, "hot_bytes": 0, "hot_launches": 0, "plan": 0}
+    acc = {"kernels": 0, "h2d": 0, "d2h": 0, "rows": 0, "hot_ms": 0.0, "hot_bytes": 0, "hot_launches": 0, "plan": 0,
+           "query_dev_ms": 0.0}
     for _ in range(steps):
         sess.execute(script)
         st = sess.stats()
@@ -186,6 +241,7 @@ def timed_steps(sess, script, steps, torch, dist):
         acc["hot_bytes"] += st.hot_kernel_bytes
         acc["hot_launches"] += st.hot_kernel_launches
         acc["plan"] = st.plan
+        acc["query_dev_ms"] += st.query_device_ms
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
@@ -208,6 +264,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fused-only", action="store_true",
                     help="time only the resident fused plan (profiling runs)")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="run every query without CUDA-graph replay (same kernels; for ncu, whose per-kernel "
+                         "replay does not handle graph memory nodes)")
     args = ap.parse_args()
     world = _env_int("WORLD_SIZE", 1)
     rank = _env_int("RANK", 0)
@@ -235,24 +294,25 @@ def main():
     args.warmup = max(args.warmup, 3)
 
     # device-resident fused plan (value) ------------------------------------------------
-    sess = ab.Session(d, resident=True)
+    sess = ab.Session(d, resident=True, graphs=not args.no_graphs)
     for t in ("lineitem", "orders", "customer"):
         sess.preload(t)
     for _ in range(args.warmup):
         sess.execute(script)
     sess.set_timing(True)
-    clk = ClockSampler(local)
+    clk = clock_sampler(local)
     clk.start()
     ms, acc = timed_steps(sess, script, args.steps, torch, dist)
     clocks = clk.stop()
     sess.set_timing(False)
     value = fact_rows * world / (ms / 1000.0)
-    plan = "fused" if acc["plan"] == 1 else "operator-at-a-time"
+    plan = {0: "operator-at-a-time", 1: "fused", 2: "fused, replayed from its CUDA graph"}.get(acc["plan"], "?")
 
     if args.fused_only:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "rows/s", "ms_per_step": ms,
-                              "plan": plan, "gpu_launches": acc["kernels"]}), flush=True)
+                              "plan": plan, "gpu_launches": acc["kernels"],
+                              "device_ms_per_step": acc["query_dev_ms"] / args.steps}), flush=True)
         sess.close()
         return
     # plain operator-at-a-time GPU path, resident (the baseline the fused plan is compared to)
@@ -280,9 +340,12 @@ def main():
         achieved = per_launch_bytes / (per_launch_ms / 1000.0) / 1e9
         hot = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                "traffic": profiled_traffic("probe_aggregate_lineitem_three_way.md"),
-               "kernel": "k_stage<false> (probe-aggregate over lineitem)",
+               "kernel": "probe-aggregate stage over lineitem: k_stage_tma (TMA-staged streaming scan) + "
+                         "k_stage_hits<false> (per-survivor probe and aggregates), timed together",
+               "algorithmic_bytes": "rows x (l_shipdate + l_orderkey stored widths) + survivors x "
+                                    "(l_extendedprice + l_discount stored widths)",
                "algorithmic_bytes_per_launch": int(per_launch_bytes), "avg_launch_ms": per_launch_ms,
-               "peak_source": f"{peak_kind} hbm_gbs"}
+               "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth measured on this pool)"}
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         try:
@@ -299,6 +362,7 @@ def main():
                        "fact_rows_per_step": fact_rows, "plan": plan, "parallelism": f"replicas x{world}",
                        "plain_gpu_rows_per_s": fact_rows * world / (pms / 1000.0),
                        "fused_vs_plain": pms / ms,
+                       "device_ms_per_step": acc["query_dev_ms"] / args.steps,
                        "l2": "inputs larger than L2 (lineitem columns 660 MB compressed, resident)"},
             "e2e": {"value": fact_rows * world / (ems / 1000.0), "unit": "rows/s",
                     "h2d_bytes_per_step": eacc["h2d"] // args.steps, "d2h_bytes_per_step": eacc["d2h"] // args.steps},

@@ -51,7 +51,8 @@ typedef struct alk_session alk_session;
 /* flags: ALK_SESSION_RESIDENT keeps every loaded column segment in device memory
  * across scripts (the reference's -i buffers, cm.cu:616-656, one level further). */
 #define ALK_SESSION_RESIDENT 1u
-#define ALK_SESSION_PLAIN 2u  /* operator-at-a-time plan only (no fused pipelines) */
+#define ALK_SESSION_PLAIN 2u    /* operator-at-a-time plan only (no fused pipelines) */
+#define ALK_SESSION_NOGRAPH 4u  /* fused queries are never captured into CUDA graphs */
 int alk_session_open(const char* data_dir, uint32_t flags, alk_session** out);
 int alk_session_execute(alk_session* s, const char* script);
 const char* alk_session_error(alk_session* s);
@@ -59,7 +60,8 @@ alk_stream alk_session_stream(alk_session* s);
 /* Pre-load (and pin in device memory) every column of a catalog table. */
 int alk_session_preload(alk_session* s, const char* table);
 /* Statistics of the last script: fact rows scanned, device kernels launched, bytes
- * copied host->device and device->host, and the plan used (0 plain, 1 fused). */
+ * copied host->device and device->host, and the plan used (0 plain, 1 fused, 2 fused and
+ * replayed from the CUDA graph captured on an earlier run of the same script). */
 typedef struct alk_stats {
   uint64_t rows_scanned;
   uint64_t kernels;
@@ -70,6 +72,7 @@ typedef struct alk_stats {
   double hot_kernel_ms;      /* device time of the dominant kernel (CUDA events) */
   uint64_t hot_kernel_bytes; /* algorithmic bytes that kernel moves */
   uint64_t hot_kernel_launches;
+  double query_device_ms;    /* device time of the fused query (events around its device work) */
 } alk_stats;
 int alk_session_stats(alk_session* s, alk_stats* out);
 /* Enable CUDA-event timing of the dominant kernel (adds two event records per launch). */
@@ -171,7 +174,8 @@ int alk_scan_filter(const alk_colseg* cols, uint32_t ncols, uint32_t nseg,
                     uint64_t cap, uint64_t* h_count, alk_stream stream);
 
 /* Expression evaluation over materialized columns, replaces CudaSet::op chains
- * (cm.cu:2440-2773) as driven by select() (select.cu:700-800). */
+ * (cm.cu:2440-2773) as driven by select() (select.cu:700-800). Asynchronous on the
+ * stream (d_cols is read before the call returns). */
 int alk_eval(const int64_t* const* d_cols, uint32_t ncols, uint64_t n, const alk_program* prog,
              int64_t* d_out, alk_stream stream);
 

@@ -219,6 +219,32 @@ def test_fused_predicates_all_groups(three_way):
     assert o == g
 
 
+def test_fused_graph_capture_and_replay(three_way):
+    """A resident session runs a fused query normally, captures it into a CUDA graph on its
+    second run and replays the graph from the third; every run must store the oracle's
+    rows. A second script interleaved with the first keeps its own graph."""
+    scripts = [wl.three_way_script(7, out="rep_a.txt"), _three_way_with(*FUSED_PREDICATES["ge_le"])]
+    outs = ["rep_a.txt", "fx.txt"]
+    want = []
+    for sc, o in zip(scripts, outs):
+        _oracle.execute(three_way, sc.replace(o, "oracle_" + o))
+        want.append(_read(os.path.join(three_way, "oracle_" + o)))
+    with ab.Session(three_way, resident=True) as s:
+        s.set_timing(True)
+        for run in range(4):
+            for sc, o, w in zip(scripts, outs, want):
+                p = os.path.join(three_way, o)
+                if os.path.exists(p):
+                    os.remove(p)
+                s.execute(sc)
+                assert _read(p) == w, (o, run)
+                st = s.stats()
+                # plan 1: fused (runs 0 and 1, the second one captured), 2: replayed graph
+                assert st.plan == (2 if run >= 2 else 1), (o, run, st.plan)
+                assert st.kernels > 0 and st.rows_scanned > 0
+                assert st.hot_kernel_launches == 1 and st.hot_kernel_ms > 0
+
+
 def test_join_multiset(three_way):
     script = ("OFI := FILTER orders BY o_orderdate < 19950101;\n"
               "CF := FILTER customer BY c_mktsegment == \"BUILDING\";\n"
