@@ -49,6 +49,10 @@ struct HtView {
   uint32_t* bits;
   int64_t kmin;
   uint64_t nbits;
+  // Dense (rank-addressed) table: a key's slot is its rank among the keys present, the
+  // popcount of the bitmap below it (rank[w] = set bits in words < w). Keys and payload
+  // are dense over slots [0, nslots); cap is then the slot capacity. Null: hash table.
+  uint32_t* rank;
 };
 
 __device__ __forceinline__ bool ht_member(const HtView& h, int64_t k) {
@@ -57,7 +61,21 @@ __device__ __forceinline__ bool ht_member(const HtView& h, int64_t k) {
   return (__ldg(h.bits + (o >> 5)) >> (o & 31)) & 1u;
 }
 
+// Slot of a present key of a dense table (the caller knows the key is present).
+__device__ __forceinline__ int64_t rank_slot(const HtView& h, int64_t k) {
+  const uint64_t o = (uint64_t)k - (uint64_t)h.kmin;
+  const uint32_t w = __ldg(h.bits + (o >> 5));
+  return (int64_t)__ldg(h.rank + (o >> 5)) + __popc(w & ((1u << (o & 31)) - 1u));
+}
+
 __device__ __forceinline__ int64_t ht_probe(const HtView& h, int64_t k) {
+  if (h.rank) {
+    const uint64_t o = (uint64_t)k - (uint64_t)h.kmin;
+    if (o >= h.nbits) return -1;
+    const uint32_t w = __ldg(h.bits + (o >> 5));
+    if (!((w >> (o & 31)) & 1u)) return -1;
+    return (int64_t)__ldg(h.rank + (o >> 5)) + __popc(w & ((1u << (o & 31)) - 1u));
+  }
   const uint64_t mask = h.cap - 1;
   uint64_t p = murmur_u64((uint64_t)k) & mask;
   for (uint64_t n = 0; n <= mask; n++) {
@@ -127,11 +145,17 @@ struct StageArgs {
   unsigned long long* cnt;  // rows per build slot (may be null)
   unsigned long long* rows_in;
   // survivors of the scan
-  Hit* hits;
+  Hit* hits;                       // entries of hit_words words: [position, (key, payload...)]
   uint64_t hit_cap;                // entries
+  uint32_t hit_words;              // 1: positions; 2 + npay: dense-build records
   unsigned long long* hit_count;   // entries reserved (whole chunks)
   unsigned long long* hit_rows;    // survivors appended
   int* err;
+  // dense-build rank prefix over the key bitmap: per-tile set-bit counts and their
+  // exclusive bases
+  uint64_t* rk_aggs;
+  uint64_t* rk_incls;
+  uint32_t rk_tiles;
 };
 
 // Segment owning a tile: the g with seg_tile[g] <= tile < seg_tile[g + 1].
@@ -172,33 +196,43 @@ struct HitWriter {
   uint32_t fill = kChunk;       // entries used in it (a full chunk: none reserved yet)
   unsigned long long rows = 0;  // survivors the warp appended
 
-  // Appends the lanes' live items (rows base_row + k * kStride of segment seg). Warp-wide.
+  // Where the warp's next `total` entries go (total <= 2 * kChunk): entry i of them at
+  // entry index i < avail ? b0 + i : nb + (i - avail). Warp-wide.
+  struct Room {
+    uint64_t b0;
+    uint32_t avail;
+    unsigned long long nb;
+    __device__ __forceinline__ uint64_t at(uint32_t i) const { return i < avail ? b0 + i : nb + (i - avail); }
+  };
+  __device__ __forceinline__ Room reserve(const StageArgs& a, uint32_t total) {
+    rows += total;
+    Room r{base + fill, kChunk - fill, 0};
+    if (total > r.avail) {  // at most two new chunks, contiguous
+      if ((threadIdx.x & 31) == 0)
+        r.nb = atomicAdd(a.hit_count, (unsigned long long)(total - r.avail > kChunk ? 2 * kChunk : kChunk));
+      r.nb = __shfl_sync(0xffffffffu, r.nb, 0);
+      const uint32_t used = total - r.avail;  // entries used of the new chunk(s)
+      base = used > kChunk ? r.nb + kChunk : r.nb;
+      fill = used > kChunk ? used - kChunk : used;
+    } else {
+      fill += total;
+    }
+    return r;
+  }
+  // Appends the lanes' live items as positions (rows base_row + k * kStride of segment
+  // seg). Warp-wide.
   template <int kStride>
   __device__ __forceinline__ void append(const StageArgs& a, uint32_t live, uint32_t seg, uint64_t base_row) {
     if (!__any_sync(0xffffffffu, live)) return;
     uint32_t excl;
     const uint32_t total = warp_offsets(__popc(live), &excl);
-    rows += total;
-    const uint32_t avail = kChunk - fill;
-    unsigned long long nb = 0;
-    if (total > avail) {  // total <= 32 * kItems <= 2 * kChunk: at most two new chunks
-      if ((threadIdx.x & 31) == 0)
-        nb = atomicAdd(a.hit_count, (unsigned long long)(total - avail > kChunk ? 2 * kChunk : kChunk));
-      nb = __shfl_sync(0xffffffffu, nb, 0);
-    }
+    const Room r = reserve(a, total);
     const uint64_t pos0 = (uint64_t)seg << 32 | base_row;
     uint32_t i = excl;
     for (uint32_t m = live; m; m &= m - 1, i++) {
       const uint32_t k = __ffs(m) - 1;
-      const uint64_t slot = i < avail ? base + fill + i : nb + (i - avail);
-      if (slot < a.hit_cap) a.hits[slot] = pos0 + (uint64_t)k * kStride;
-    }
-    if (total > avail) {
-      const uint32_t used = total - avail;  // entries used of the new chunk(s)
-      base = used > kChunk ? nb + kChunk : nb;
-      fill = used > kChunk ? used - kChunk : used;
-    } else {
-      fill += total;
+      const uint64_t e = r.at(i);
+      if (e < a.hit_cap) a.hits[e * a.hit_words] = pos0 + (uint64_t)k * kStride;
     }
   }
   // Marks the unused tail of the last chunk and publishes the warp's survivor count.
@@ -206,7 +240,7 @@ struct HitWriter {
   __device__ __forceinline__ void finish(const StageArgs& a) {
     const uint32_t lane = threadIdx.x & 31;
     for (uint32_t i = fill + lane; i < kChunk; i += 32)
-      if (base + i < a.hit_cap) a.hits[base + i] = kNoHit;
+      if (base + i < a.hit_cap) a.hits[(base + i) * a.hit_words] = kNoHit;
     if (lane == 0 && rows) atomicAdd(a.hit_rows, rows);
   }
 };
@@ -286,7 +320,8 @@ __global__ void __launch_bounds__(kT) k_stage_hits(const StageArgs a) {
   }
   unsigned long long inserted = 0;
   for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
-    const Hit h = a.hits[i];
+    const Hit* e = a.hits + i * a.hit_words;
+    const Hit h = e[0];
     if (h == kNoHit) continue;  // unused tail of a warp's last chunk
     const uint32_t seg = (uint32_t)(h >> 32);
     const uint64_t row = h & 0xffffffffull;
@@ -297,6 +332,35 @@ __global__ void __launch_bounds__(kT) k_stage_hits(const StageArgs a) {
       const void* data = (const void*)__ldg((const unsigned long long*)&d->data);
       return load_for(data, __ldg(&d->bits), (int64_t)__ldg((const long long*)&d->lower), row);
     };
+    if (kBuild && a.build.rank) {
+      // dense build: the key's rank is its slot; the record carries key and payload, or
+      // they are read at the survivor's position
+      int64_t key, pv[8];
+      if (a.hit_words > 1) {
+        key = (int64_t)e[1];
+#pragma unroll
+        for (uint32_t p = 0; p < 8; p++)
+          if (p < a.build.npay) pv[p] = (int64_t)e[2 + p];
+      } else {
+        if (a.probe_slot >= 0 && (a.need_slot || !a.probe.bits)) {  // as the bitmap pass did
+          j = ht_probe(a.probe, col((uint32_t)a.probe_slot));
+          if (j < 0) continue;
+        }
+        key = col((uint32_t)a.build_slot);
+#pragma unroll
+        for (uint32_t p = 0; p < 8; p++)
+          if (p < a.build.npay) pv[p] = col((uint32_t)a.pay_src[p]);
+      }
+      const uint64_t o = (uint64_t)key - (uint64_t)a.build.kmin;
+      if (o >= a.build.nbits) continue;  // flagged by the bitmap pass
+      const int64_t sl = rank_slot(a.build, key);
+      if ((uint64_t)sl >= a.build.cap) continue;  // more keys than slots: flagged by the prefix pass
+      a.build.key[sl] = key;
+#pragma unroll
+      for (uint32_t p = 0; p < 8; p++)
+        if (p < a.build.npay) a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = pv[p];
+      continue;
+    }
     if (a.probe_slot >= 0 && (a.need_slot || !a.probe.bits)) {
       j = ht_probe(a.probe, col((uint32_t)a.probe_slot));
       if (j < 0) continue;
@@ -335,6 +399,97 @@ __global__ void __launch_bounds__(kT) k_stage_hits(const StageArgs a) {
   if (kBuild) {
     for (int o = 16; o; o >>= 1) inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
     if ((threadIdx.x & 31) == 0 && inserted) atomicAdd(a.build.nslots, inserted);
+  }
+}
+
+// Dense build from a list of survivor positions: set each survivor's key bit (a bit found
+// set already is a duplicate key; a key outside the bitmap range is flagged).
+__global__ void __launch_bounds__(kT) k_rank_mark(const StageArgs a) {
+  const uint64_t n = *(volatile unsigned long long*)a.hit_count;
+  if (n > a.hit_cap) return;  // the scatter pass reports the overflow
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
+    const Hit h = a.hits[i * a.hit_words];
+    if (h == kNoHit) continue;
+    const uint32_t seg = (uint32_t)(h >> 32);
+    const uint64_t row = h & 0xffffffffull;
+    auto col = [&](uint32_t slot) -> int64_t {
+      const alk_colseg* d = a.cols + (uint64_t)slot * a.nseg + seg;
+      const void* data = (const void*)__ldg((const unsigned long long*)&d->data);
+      return load_for(data, __ldg(&d->bits), (int64_t)__ldg((const long long*)&d->lower), row);
+    };
+    if (a.probe_slot >= 0 && !a.probe.bits && ht_probe(a.probe, col((uint32_t)a.probe_slot)) < 0) continue;
+    const int64_t key = col((uint32_t)a.build_slot);
+    const uint64_t o = (uint64_t)key - (uint64_t)a.build.kmin;
+    if (o >= a.build.nbits) {
+      atomicExch(a.build.flags + 3, 1);
+      continue;
+    }
+    const uint32_t bit = 1u << (o & 31);
+    if (atomicOr(a.build.bits + (o >> 5), bit) & bit) atomicExch(a.build.flags, 1);
+  }
+}
+
+// rank[w] = set bits in words < w of the dense table's bitmap, as a three-pass scan over
+// tiles of 2048 words: tile sums, one block's scan of the sums, then each tile's ranks.
+// The total is the key count. A key count above the slot capacity is flagged, and, for
+// survivors recorded by the scan (one record per survivor, every one a member), a key
+// count below the survivor count means duplicate keys.
+constexpr uint32_t kRankTile = kT * 8;
+__device__ __forceinline__ uint64_t rank_tile_counts(const HtView& h, uint32_t tile, uint32_t (&c)[8]) {
+  const uint64_t nwords = (h.nbits + 31) / 32;
+  const uint64_t w0 = (uint64_t)tile * kRankTile + (uint64_t)threadIdx.x * 8;  // blocked
+  uint64_t sum = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    c[k] = w0 + k < nwords ? (uint32_t)__popc(h.bits[w0 + k]) : 0u;
+    sum += c[k];
+  }
+  return sum;
+}
+__global__ void __launch_bounds__(kT) k_rank_sums(const StageArgs a) {
+  __shared__ uint64_t s_warp[kT / 32 + 1];
+  uint32_t c[8];
+  const uint64_t sum = rank_tile_counts(a.build, blockIdx.x, c);
+  uint64_t tot;
+  block_excl_scan<kT>(sum, s_warp, &tot);
+  if (threadIdx.x == 0) a.rk_aggs[blockIdx.x] = tot;
+}
+constexpr int kRankScanThreads = 1024;
+__global__ void __launch_bounds__(kRankScanThreads) k_rank_scan_sums(const StageArgs a) {
+  __shared__ uint64_t s_warp[kRankScanThreads / 32 + 1];
+  const HtView& h = a.build;
+  const uint32_t per = (a.rk_tiles + kRankScanThreads - 1) / kRankScanThreads;  // consecutive tiles per thread
+  const uint32_t t0 = threadIdx.x * per;
+  uint64_t sum = 0;
+  for (uint32_t i = 0; i < per; i++)
+    if (t0 + i < a.rk_tiles) sum += a.rk_aggs[t0 + i];
+  uint64_t tot;
+  uint64_t run = block_excl_scan<kRankScanThreads>(sum, s_warp, &tot);
+  for (uint32_t i = 0; i < per; i++) {
+    if (t0 + i >= a.rk_tiles) break;
+    const uint64_t v = a.rk_aggs[t0 + i];
+    a.rk_incls[t0 + i] = run;  // exclusive base of the tile
+    run += v;
+  }
+  if (threadIdx.x == 0) {
+    *h.nslots = tot;
+    if (tot > h.cap) atomicExch(h.flags + 1, 1);
+    if (a.hit_words > 1 && *(volatile unsigned long long*)a.hit_rows != tot) atomicExch(h.flags, 1);
+  }
+}
+__global__ void __launch_bounds__(kT) k_rank_write(const StageArgs a) {
+  __shared__ uint64_t s_warp[kT / 32 + 1];
+  const HtView& h = a.build;
+  const uint64_t nwords = (h.nbits + 31) / 32;
+  uint32_t c[8];
+  const uint64_t sum = rank_tile_counts(h, blockIdx.x, c);
+  uint64_t tot;
+  uint64_t r = a.rk_incls[blockIdx.x] + block_excl_scan<kT>(sum, s_warp, &tot);
+  const uint64_t w0 = (uint64_t)blockIdx.x * kRankTile + (uint64_t)threadIdx.x * 8;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    if (w0 + k < nwords) h.rank[w0 + k] = (uint32_t)r;
+    r += c[k];
   }
 }
 
@@ -1044,14 +1199,38 @@ __global__ void __launch_bounds__(kTmaThreads) k_stage_tma(const __grid_constant
     if (t.inline_build) {
       // insert the survivors from the staged tile, then release it; the warp's survivors
       // are first compacted so that all lanes insert at once (one compare-and-swap round
-      // trip per 32 survivors)
-      survivors += __popc(live);
+      // trip per 32 survivors). A dense table takes records instead: the key's bit is set
+      // and [position, key, payload] goes to the survivor list, for the rank passes.
+      const bool dense = a.build.rank != nullptr;
+      if (!dense) survivors += __popc(live);
       uint32_t excl;
       const uint32_t total = __any_sync(0xffffffffu, live) ? warp_offsets(__popc(live), &excl) : 0;
       uint16_t* wl = s_rows + warp * (32 * kItems);
       uint32_t q = excl;
       for (uint32_t m = total ? live : 0; m; m &= m - 1, q++) wl[q] = (uint16_t)(r0 + (__ffs(m) - 1) * 32);
       __syncwarp();
+      if (dense) {
+        const HitWriter::Room room = total ? hw.reserve(a, total) : HitWriter::Room{0, 0, 0};
+        for (uint32_t j = lane; j < total; j += 32) {
+          const uint32_t r = wl[j];
+          const int64_t key = staged_value(buf + t.col_off[t.key_st], s_cd[t.key_st * a.nseg + seg], r);
+          const uint64_t o = (uint64_t)key - (uint64_t)a.build.kmin;
+          if (o < a.build.nbits) atomicOr(a.build.bits + (o >> 5), 1u << (o & 31));
+          else atomicExch(a.build.flags + 3, 1);
+          const uint64_t e = room.at(j);
+          if (e >= a.hit_cap) continue;
+          Hit* rec = a.hits + e * a.hit_words;
+          rec[0] = (uint64_t)seg << 32 | (uint64_t)(row0 + r);
+          rec[1] = (uint64_t)key;
+#pragma unroll
+          for (uint32_t p = 0; p < 8; p++)
+            if (p < a.build.npay)
+              rec[2 + p] = (uint64_t)staged_value(buf + t.col_off[t.pay_st[p]], s_cd[t.pay_st[p] * a.nseg + seg], r);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&s_empty[st]);
+        continue;
+      }
       // rounds of 32 survivors; the last round's values are read into registers and the
       // stage is released before its inserts, so the producer refills it meanwhile
       for (uint32_t j0 = 0; j0 < total; j0 += 32) {
@@ -1184,9 +1363,9 @@ constexpr size_t kSmemPerSM = 228 * 1024;
 // kernel over its survivors. cols is the host descriptor array [ncols][nseg]; fa holds
 // the device arguments and, when conj, the predicate's conjuncts.
 template <bool kBuild>
-cudaError_t launch_stage(const FastArgs& fa, bool conj, const alk_colseg* cols, const uint8_t* seg_mode,
+cudaError_t launch_stage(FastArgs fa, bool conj, const alk_colseg* cols, const uint8_t* seg_mode,
                          const int32_t* h_pay_src, cudaStream_t s, alk_event_timer* timer) {
-  const StageArgs& a = fa.a;
+  StageArgs& a = fa.a;
   if (!a.ntiles) return cudaSuccess;
   TmaArgs t{};
   bool tma = false;
@@ -1243,6 +1422,11 @@ cudaError_t launch_stage(const FastArgs& fa, bool conj, const alk_colseg* cols, 
     const bool can_inline = kBuild && h_pay_src && !a.need_slot && (a.probe_slot < 0 || a.probe.bits);
     tma = (can_inline && plan(true)) || plan(false);
   }
+  const bool inline_build = tma && t.inline_build;
+  const bool dense = kBuild && a.build.rank != nullptr;
+  // a dense build staged inline records [position, key, payload] per survivor
+  a.hit_words = dense && inline_build ? 2 + a.build.npay : 1;
+  t.f.a.hit_words = a.hit_words;
   int occ = 0;
   if (tma) {
     cudaFuncSetAttribute(k_stage_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem);
@@ -1265,9 +1449,26 @@ cudaError_t launch_stage(const FastArgs& fa, bool conj, const alk_colseg* cols, 
   if (tma) k_stage_tma<<<grid, kTmaThreads, tma_smem, s>>>(t);
   else if (conj) k_stage_fast<<<grid, kT, 0, s>>>(fa);
   else k_stage_scan<<<grid, kT, 0, s>>>(a);
-  if (!(tma && t.inline_build)) k_stage_hits<kBuild><<<sms() * std::max(occ_hits, 1), kT, 0, s>>>(a);
+  uint32_t launches = 1;
+  const int hits_grid = sms() * std::max(occ_hits, 1);
+  if (dense) {
+    // dense build: key bits (from positions, when the scan did not set them), the rank
+    // prefix, then the scatter of keys and payload to their ranks
+    if (!inline_build) {
+      k_rank_mark<<<hits_grid, kT, 0, s>>>(a);
+      launches++;
+    }
+    k_rank_sums<<<a.rk_tiles, kT, 0, s>>>(a);
+    k_rank_scan_sums<<<1, kRankScanThreads, 0, s>>>(a);
+    k_rank_write<<<a.rk_tiles, kT, 0, s>>>(a);
+    k_stage_hits<kBuild><<<hits_grid, kT, 0, s>>>(a);
+    launches += 4;
+  } else if (!inline_build) {
+    k_stage_hits<kBuild><<<hits_grid, kT, 0, s>>>(a);
+    launches++;
+  }
   if (timer && timer->on) cudaEventRecordWithFlags((cudaEvent_t)timer->ev1, s, evflags);
-  alk::g_kernel_launches += (tma && t.inline_build) ? 1 : 2;
+  alk::g_kernel_launches += launches;
   return cudaGetLastError();
 }
 
@@ -1346,6 +1547,41 @@ int alk_ht_create_range(uint64_t max_keys, uint32_t npay, int64_t key_min, int64
     h->v.nbits = nbits;
     CK(cudaMemsetAsync(h->v.bits, 0, words * 4, s));
   }
+  *out = h;
+  return ALK_OK;
+}
+
+int alk_ht_create_dense(uint64_t max_keys, uint32_t npay, int64_t key_min, int64_t key_max, alk_ht** out,
+                        alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!out || npay > 8 || max_keys >= 0xffffffffull || key_max < key_min) return ALK_ERR_ARG;
+  const uint64_t span = (uint64_t)key_max - (uint64_t)key_min + 1;
+  if (span == 0 || span > (1ull << 29)) return ALK_ERR_UNSUPPORTED;  // no exact bitmap
+  const uint64_t cap = std::max<uint64_t>(max_keys, 1);  // slots are ranks: no spare room
+  const size_t words = (span + 31) / 32;
+  const size_t off_pay = cap * 8;
+  const size_t off_ctr = off_pay + cap * 8 * npay;
+  const size_t off_bits = off_ctr + 64;
+  const size_t off_rank = off_bits + ((words * 4 + 15) & ~size_t(15));
+  auto* h = new alk_ht();
+  cudaError_t e = cudaMallocAsync(&h->mem, off_rank + words * 4, s);
+  if (e != cudaSuccess) {
+    delete h;
+    return alk::cuda_fail(e);
+  }
+  uint8_t* p = (uint8_t*)h->mem;
+  h->v.cap = cap;
+  h->v.key = (int64_t*)p;
+  h->v.payload = (int64_t*)(p + off_pay);
+  h->v.slot_cap = cap;
+  h->v.npay = npay;
+  h->v.nslots = (unsigned long long*)(p + off_ctr);
+  h->v.flags = (int*)(p + off_ctr + 8);
+  h->v.bits = (uint32_t*)(p + off_bits);
+  h->v.kmin = key_min;
+  h->v.nbits = span;
+  h->v.rank = (uint32_t*)(p + off_rank);
+  CK(cudaMemsetAsync(p + off_ctr, 0, 64 + ((words * 4 + 15) & ~size_t(15)), s));  // counters and bitmap
   *out = h;
   return ALK_OK;
 }
@@ -1485,20 +1721,28 @@ static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* co
   }
   const size_t off_cs = (hb.size() + 15) & ~size_t(15);
   const size_t off_sp = (off_cs + cs.size() * sizeof(ConjSeg) + 15) & ~size_t(15);
+  // zeroed tail: the stage counters, then (dense build) the look-back state of the rank
+  // prefix; the survivor list follows, in entries of up to wmax words
+  const bool dense = kBuild && a.build.rank != nullptr;
+  const uint32_t wmax = dense ? 2 + a.build.npay : 1;
+  const uint32_t rk_tiles = dense ? (uint32_t)(((a.build.nbits + 31) / 32 + kRankTile - 1) / kRankTile) : 0;
   const size_t off_tail = (off_sp + sp.size() * sizeof(SegPlan) + 15) & ~size_t(15);
-  const size_t off_hits = off_tail + 32;
+  const size_t off_rk_aggs = 32;
+  const size_t off_rk_incls = off_rk_aggs + 8 * (size_t)rk_tiles;
+  const size_t tail_bytes = off_rk_incls + 8 * (size_t)rk_tiles;
+  const size_t off_hits = (off_tail + tail_bytes + 255) & ~size_t(255);
   std::vector<uint8_t> up(off_tail, 0);
   std::memcpy(up.data(), hb.data(), hb.size());
   if (!cs.empty()) std::memcpy(up.data() + off_cs, cs.data(), cs.size() * sizeof(ConjSeg));
   std::memcpy(up.data() + off_sp, sp.data(), sp.size() * sizeof(SegPlan));
   uint8_t* db = nullptr;
-  CK(cudaMallocAsync((void**)&db, off_hits + std::max<uint64_t>(hit_cap, 1) * sizeof(Hit), s));
+  CK(cudaMallocAsync((void**)&db, off_hits + std::max<uint64_t>(hit_cap, 1) * wmax * sizeof(Hit), s));
   cudaError_t ue;
   const void* src = alk::upload_source(up.data(), up.size(), s, &ue);
   CK(ue);
   CK(cudaMemcpyAsync(db, src, up.size(), cudaMemcpyHostToDevice, s));
   uint8_t* tail = db + off_tail;
-  CK(cudaMemsetAsync(tail, 0, 32, s));
+  CK(cudaMemsetAsync(tail, 0, tail_bytes, s));
   patch(a, db);
   if (kBuild) a.pay_src = (const int32_t*)(db + off_x);
   else a.agg_kind = db + off_x;
@@ -1506,8 +1750,12 @@ static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* co
   a.hit_count = (unsigned long long*)(tail + 8);
   a.err = (int*)(tail + 16);
   a.hit_rows = (unsigned long long*)(tail + 24);
+  a.rk_aggs = (uint64_t*)(tail + off_rk_aggs);
+  a.rk_incls = (uint64_t*)(tail + off_rk_incls);
+  a.rk_tiles = rk_tiles;
   a.hits = (Hit*)(db + off_hits);
   a.hit_cap = hit_cap;
+  a.hit_words = 1;
   fa.a = a;
   fa.cseg = (const ConjSeg*)(db + off_cs);
   fa.splan = (const SegPlan*)(db + off_sp);

@@ -1314,7 +1314,12 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     auto it = card_feedback_.find(sig);
     const uint64_t est = it == card_feedback_.end() ? upper : std::min(upper, it->second + it->second / 4 + 1024);
     g.s = s;
-    check(alk_ht_create_range(est, npay, range.first, range.second, &g.h, (alk_stream)s), "hash table");
+    // a key range of at most 2^29 values (the zone maps) takes the dense, rank-addressed
+    // table; wider ranges the hash table
+    const bool dense = range.second >= range.first &&
+                       (uint64_t)range.second - (uint64_t)range.first < (1ull << 29);
+    if (dense) check(alk_ht_create_dense(est, npay, range.first, range.second, &g.h, (alk_stream)s), "dense table");
+    else check(alk_ht_create_range(est, npay, range.first, range.second, &g.h, (alk_stream)s), "hash table");
     check(run(g.h, hit_cap_for(sig), &fs->st[idx]), "build stage");
     check(alk_ht_info_async(g.h, &fs->ht[idx], (alk_stream)s), "hash table");
     tail.pending.push_back({sig, idx, idx, upper});

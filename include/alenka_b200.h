@@ -234,6 +234,14 @@ int alk_ht_create(uint64_t max_keys, uint32_t npay, alk_ht** out, alk_stream str
  * the range sets flag 8. */
 int alk_ht_create_range(uint64_t max_keys, uint32_t npay, int64_t key_min, int64_t key_max, alk_ht** out,
                         alk_stream stream);
+/* Dense (rank-addressed) build table for keys known to lie in [key_min, key_max], a
+ * range of at most 2^29 values (from the build column's zone maps): a build stage sets the
+ * keys' bits in an exact bitmap, a prefix pass ranks them, and a key's slot is its rank
+ * among the keys present, so keys, payload and per-key accumulators are dense over
+ * [0, inserted) with no hashing. max_keys is the slot capacity (more distinct keys set
+ * flag 2, capacity exceeded). ALK_ERR_UNSUPPORTED for a wider range. */
+int alk_ht_create_dense(uint64_t max_keys, uint32_t npay, int64_t key_min, int64_t key_max, alk_ht** out,
+                        alk_stream stream);
 void alk_ht_free(alk_ht* h, alk_stream stream);
 /* Inserted keys and flags (1 duplicate key, 2 capacity exceeded, 4 wait expired,
  * 8 key outside the declared range). */
@@ -241,8 +249,9 @@ int alk_ht_info(const alk_ht* h, uint64_t* nslots, int* flags, alk_stream stream
 /* Slot range of a table: payload columns and per-key accumulators are indexed by the
  * key's table position, 0 <= slot < alk_ht_slots(h). */
 uint64_t alk_ht_slots(const alk_ht* h);
-/* Device address of the key column (slot-indexed; free slots hold the byte pattern 0x80
- * repeated, 0x8080808080808080). */
+/* Device address of the key column (slot-indexed; free slots of a hash table hold the
+ * byte pattern 0x80 repeated, 0x8080808080808080; a dense table's slots at and beyond
+ * its key count are undefined). */
 const int64_t* alk_ht_keys(const alk_ht* h);
 /* Device address of payload column p (slot-indexed). */
 const int64_t* alk_ht_payload(const alk_ht* h, uint32_t p);
