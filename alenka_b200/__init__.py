@@ -39,6 +39,9 @@ class Stats(ctypes.Structure):
         ("hot_kernel_bytes", ctypes.c_uint64),
         ("hot_kernel_launches", ctypes.c_uint64),
         ("query_device_ms", ctypes.c_double),
+        ("reserved_bytes", ctypes.c_uint64),
+        ("card_estimates", ctypes.c_uint32),
+        ("card_reruns", ctypes.c_uint32),
     ]
 
 
@@ -72,6 +75,23 @@ def _declare(L):
     L.alk_join_free.argtypes = [vp, vp]
     L.alk_join_free.restype = None
     L.alk_device_info.argtypes = [c.POINTER(i32), c.POINTER(i32), c.POINTER(i32)]
+    fp = c.POINTER(c.c_float)
+    L.alk_mlp_param_count.restype = u32
+    L.alk_mlp_create.argtypes = [u64, c.POINTER(vp), vp]
+    L.alk_mlp_free.argtypes = [vp, vp]
+    L.alk_mlp_free.restype = None
+    L.alk_mlp_set_params.argtypes = [vp, fp, vp]
+    L.alk_mlp_params.argtypes = [vp, fp, c.POINTER(c.c_uint16), vp]
+    L.alk_mlp_forward.argtypes = [vp, vp, u64, vp, vp]
+    L.alk_mlp_gradients.argtypes = [vp, vp, vp, vp, u64, vp, fp, vp]
+    L.alk_mlp_train.argtypes = [vp, vp, vp, vp, u64, u32, u32, c.c_float, fp, vp]
+    L.alk_card_hist16.argtypes = [vp, i64, i64, vp, vp]
+    L.alk_card_count.argtypes = [vp, u32, u32, vp, vp, vp, i32, i32, i64, i64, c.POINTER(u64), vp]
+    L.alk_session_card_mode.argtypes = [vp, i32, i32]
+    L.alk_session_card_records.argtypes = [vp, fp, fp, fp, u64, c.POINTER(u64)]
+    L.alk_session_card_train.argtypes = [vp, u64, u64, u32, u32, c.c_float, u64, fp]
+    L.alk_session_card_predict.argtypes = [vp, fp, u64, fp]
+    L.alk_session_card_forget.argtypes = [vp]
     L.alenkaInit.argtypes = [c.POINTER(c.c_char_p)]
     L.alenkaInit.restype = None
     L.alenkaExecute.argtypes = [c.c_char_p]
@@ -120,6 +140,43 @@ class Session:
 
     def set_timing(self, on):
         lib().alk_session_set_timing(self._h, 1 if on else 0)
+
+    # ---- learned cardinality estimator
+    def card_mode(self, record=False, use=False):
+        lib().alk_session_card_mode(self._h, 1 if record else 0, 1 if use else 0)
+
+    def card_records(self):
+        """(features [n, 64], log-fraction targets [n, 3], target masks [n, 3]) as numpy."""
+        import numpy as np
+        n = ctypes.c_uint64()
+        lib().alk_session_card_records(self._h, None, None, None, 0, ctypes.byref(n))
+        x = np.zeros((n.value, 64), np.float32)
+        y = np.zeros((n.value, 3), np.float32)
+        m = np.zeros((n.value, 3), np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        lib().alk_session_card_records(self._h, x.ctypes.data_as(fp), y.ctypes.data_as(fp), m.ctypes.data_as(fp),
+                                       n.value, ctypes.byref(n))
+        return x, y, m
+
+    def card_train(self, first, count, epochs=30, batch=256, lr=1e-3, seed=1):
+        loss = ctypes.c_float()
+        rc = lib().alk_session_card_train(self._h, first, count, epochs, batch, lr, seed, ctypes.byref(loss))
+        if rc != ALK_OK:
+            raise AlenkaError(rc, lib().alk_session_error(self._h).decode())
+        return loss.value
+
+    def card_predict(self, x):
+        import numpy as np
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.zeros((x.shape[0], 3), np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        rc = lib().alk_session_card_predict(self._h, x.ctypes.data_as(fp), x.shape[0], y.ctypes.data_as(fp))
+        if rc != ALK_OK:
+            raise AlenkaError(rc, "estimator prediction failed")
+        return y
+
+    def card_forget(self):
+        lib().alk_session_card_forget(self._h)
 
     @property
     def stream(self):

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "alenka_b200.h"
+
 #include <vector>
 
 namespace alk {
@@ -18,4 +20,13 @@ extern uint64_t g_kernel_launches;
 // whoever ends the capture takes them over and frees them (cudaFreeHost) with the graph.
 const void* upload_source(const void* host, size_t bytes, cudaStream_t s, cudaError_t* err);
 std::vector<void*>& capture_host_buffers();
+
+// A filter program as a conjunction of single-column tests `value * mul OP k` (OP one of
+// the comparison opcodes); false when the program has another form. An empty program is
+// the empty conjunction.
+struct CardConj {
+  int64_t mul, k;
+  uint32_t slot, op;
+};
+bool program_conjuncts(const alk_program& p, std::vector<CardConj>& out);
 }  // namespace alk

@@ -291,6 +291,62 @@ __global__ void __launch_bounds__(kT) k_stage_scan(const StageArgs a) {
   if ((threadIdx.x & 31) == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
 }
 
+// Exact counts of one segment for the cardinality estimator's records (and the exact
+// counting pass that replaces an estimate): rows passing the predicate, of those the rows
+// whose probe key is in the probed table, and of those the distinct values of a key column
+// (first settings of a bit in a bitmap over the key's range, cleared before the launch).
+__global__ void __launch_bounds__(kT) k_card_count(const StageArgs a, uint32_t seg, int32_t key_slot, int64_t kmin,
+                                                   uint64_t nbits, uint32_t* bitmap, unsigned long long* out) {
+  __shared__ alk_instr s_ins[ALK_MAX_INSTR];
+  __shared__ int64_t s_consts[ALK_MAX_CONST];
+  __shared__ int64_t s_regs[ALK_MAX_REGS * kT];
+  __shared__ alk_colseg s_desc[kMaxCols];
+  for (uint32_t i = threadIdx.x; i < a.progs[0].n_instr; i += kT) s_ins[i] = a.progs[0].ins[i];
+  for (uint32_t i = threadIdx.x; i < ALK_MAX_CONST; i += kT) s_consts[i] = a.progs[0].consts[i];
+  if (threadIdx.x < a.ncols) s_desc[threadIdx.x] = a.cols[threadIdx.x * a.nseg + seg];
+  __syncthreads();
+  const uint32_t n_ins = a.progs[0].n_instr, res = a.progs[0].result;
+  const bool all = a.seg_mode[seg] == 1 || n_ins == 0;
+  unsigned long long c_pass = 0, c_join = 0, c_new = 0;
+  for (uint32_t tile = a.seg_tile[seg] + blockIdx.x; tile < a.seg_tile[seg + 1]; tile += gridDim.x) {
+    const uint32_t row0 = (tile - a.seg_tile[seg]) * kTile;
+    const uint32_t rows = min((uint32_t)kTile, s_desc[0].rows - row0);
+#pragma unroll 1
+    for (int k = 0; k < kItems; k++) {
+      if (k * kT + threadIdx.x >= rows) continue;
+      const uint64_t row = (uint64_t)row0 + threadIdx.x + (uint64_t)k * kT;
+      auto col = [&](uint32_t slot) -> int64_t {
+        const alk_colseg& d = s_desc[slot];
+        return load_for(d.data, d.bits, d.lower, row);
+      };
+      if (!all && vm_eval<kT>(s_ins, n_ins, res, s_consts, s_regs + threadIdx.x, col) == 0) continue;
+      c_pass++;
+      if (a.probe_slot >= 0) {
+        const int64_t pk = col((uint32_t)a.probe_slot);
+        if (a.probe.bits ? !ht_member(a.probe, pk) : ht_probe(a.probe, pk) < 0) continue;
+      }
+      c_join++;
+      if (key_slot >= 0 && nbits) {
+        const uint64_t o = (uint64_t)col((uint32_t)key_slot) - (uint64_t)kmin;
+        if (o < nbits) {
+          const uint32_t bit = 1u << (o & 31);
+          if (!(atomicOr(bitmap + (o >> 5), bit) & bit)) c_new++;
+        }
+      }
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    c_pass += __shfl_xor_sync(0xffffffffu, c_pass, o);
+    c_join += __shfl_xor_sync(0xffffffffu, c_join, o);
+    c_new += __shfl_xor_sync(0xffffffffu, c_new, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (c_pass) atomicAdd(out, c_pass);
+    if (c_join) atomicAdd(out + 1, c_join);
+    if (c_new) atomicAdd(out + 2, c_new);
+  }
+}
+
 // Per-survivor work of a stage, one thread per hit: the hash probe (for the payload
 // position, or for membership when the probed table has no key bitmap), then either the
 // build-side insert with its payload or the aggregate updates. A list that overflowed
@@ -1499,6 +1555,7 @@ bool prog_ok(const alk_program& p, uint32_t ncols, uint32_t npay) {
 struct alk_ht {
   HtView v{};
   void* mem = nullptr;
+  size_t bytes = 0;  // device bytes held
 };
 
 extern "C" {
@@ -1529,6 +1586,7 @@ int alk_ht_create_range(uint64_t max_keys, uint32_t npay, int64_t key_min, int64
     delete h;
     return alk::cuda_fail(e);
   }
+  h->bytes = bytes;
   uint8_t* p = (uint8_t*)h->mem;
   h->v.cap = cap;
   h->v.key = (int64_t*)p;
@@ -1569,6 +1627,7 @@ int alk_ht_create_dense(uint64_t max_keys, uint32_t npay, int64_t key_min, int64
     delete h;
     return alk::cuda_fail(e);
   }
+  h->bytes = off_rank + words * 4;
   uint8_t* p = (uint8_t*)h->mem;
   h->v.cap = cap;
   h->v.key = (int64_t*)p;
@@ -1610,6 +1669,8 @@ int alk_ht_info(const alk_ht* h, uint64_t* nslots, int* flags, alk_stream stream
 }
 
 uint64_t alk_ht_slots(const alk_ht* h) { return h ? h->v.slot_cap : 0; }
+
+uint64_t alk_ht_bytes(const alk_ht* h) { return h ? h->bytes : 0; }
 
 const int64_t* alk_ht_keys(const alk_ht* h) { return h ? h->v.key : nullptr; }
 
@@ -1990,6 +2051,73 @@ int alk_live_compact(const uint64_t* d_live, uint64_t n, uint32_t* d_out, uint64
   CK(cudaFreeAsync(db, s));
   CK(cudaStreamSynchronize(s));
   *h_count = c;
+  return ALK_OK;
+}
+
+}  // extern "C"
+
+namespace alk {
+bool program_conjuncts(const alk_program& p, std::vector<CardConj>& out) {
+  Conj cj[kMaxConj];
+  uint32_t n = 0;
+  out.clear();
+  if (!as_conjuncts(p, cj, &n)) return false;
+  for (uint32_t i = 0; i < n; i++) out.push_back({cj[i].mul, cj[i].k, cj[i].slot, cj[i].op});
+  return true;
+}
+}  // namespace alk
+
+extern "C" {
+
+int alk_card_count(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                   const alk_program* pred, const alk_ht* probe, int32_t probe_slot, int32_t key_slot,
+                   int64_t key_min, int64_t key_max, uint64_t* h_counts, alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!h_counts || ncols == 0 || ncols > kMaxCols) return ALK_ERR_ARG;
+  if ((probe_slot >= 0) != (probe != nullptr) || (probe_slot >= 0 && (uint32_t)probe_slot >= ncols))
+    return ALK_ERR_ARG;
+  if (key_slot >= 0 && (uint32_t)key_slot >= ncols) return ALK_ERR_ARG;
+  alk_program prog{};
+  if (pred) prog = *pred;
+  if (!prog_ok(prog, ncols, 0)) return ALK_ERR_ARG;
+  StageArgs a{};
+  std::vector<uint8_t> hb;
+  size_t off_x;
+  int rc = stage_common(cols, ncols, nseg, seg_mode, &prog, 1, hb, a, 0, &off_x);
+  if (rc) return rc;
+  a.probe_slot = probe_slot;
+  if (probe) a.probe = probe->v;
+  // distinct values are counted when the key range is known and at most 2^30 values
+  uint64_t nbits = 0;
+  if (key_slot >= 0 && key_max >= key_min) {
+    const uint64_t span = (uint64_t)key_max - (uint64_t)key_min + 1;
+    if (span != 0 && span <= (1ull << 30)) nbits = span;
+  }
+  const size_t off_cnt = (hb.size() + 255) & ~size_t(255);
+  const size_t off_bits = off_cnt + ((24 * (size_t)nseg + 255) & ~size_t(255));
+  const size_t words = (nbits + 31) / 32;
+  uint8_t* db = nullptr;
+  CK(cudaMallocAsync((void**)&db, off_bits + words * 4 + 16, s));
+  CK(cudaMemcpyAsync(db, hb.data(), hb.size(), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(db + off_cnt, 0, 24 * (size_t)nseg, s));
+  std::vector<uint32_t> seg_tile(nseg + 1);
+  std::memcpy(seg_tile.data(), hb.data() + (uintptr_t)a.seg_tile, 4 * (nseg + 1));  // offsets before patch()
+  patch(a, db);
+  for (uint32_t g = 0; g < nseg; g++) {
+    const uint32_t tiles = seg_tile[g + 1] - seg_tile[g];
+    if (!seg_mode[g] || tiles == 0) continue;
+    if (nbits) CK(cudaMemsetAsync(db + off_bits, 0, words * 4, s));
+    k_card_count<<<std::min<uint32_t>(tiles, (uint32_t)sms() * 4), kT, 0, s>>>(
+        a, g, nbits ? key_slot : -1, key_min, nbits, (uint32_t*)(db + off_bits),
+        (unsigned long long*)(db + off_cnt) + 3 * g);
+    alk::g_kernel_launches++;
+    CK(cudaGetLastError());
+  }
+  CK(cudaMemcpyAsync(h_counts, db + off_cnt, 24 * (size_t)nseg, cudaMemcpyDeviceToHost, s));
+  CK(cudaFreeAsync(db, s));
+  CK(cudaStreamSynchronize(s));
+  if (!nbits)
+    for (uint32_t g = 0; g < nseg; g++) h_counts[3 * g + 2] = ~0ull;
   return ALK_OK;
 }
 

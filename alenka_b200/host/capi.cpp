@@ -68,6 +68,39 @@ int alk_session_set_timing(alk_session* s, int on) {
   return ALK_OK;
 }
 
+int alk_session_card_mode(alk_session* s, int record, int use) {
+  if (!s) return ALK_ERR_ARG;
+  return s->eng->card_mode(record != 0, use != 0);
+}
+
+int alk_session_card_records(alk_session* s, float* h_x, float* h_y, float* h_mask, uint64_t cap, uint64_t* h_n) {
+  if (!s || !h_n) return ALK_ERR_ARG;
+  *h_n = s->eng->card_records(h_x, h_y, h_mask, cap);
+  return ALK_OK;
+}
+
+int alk_session_card_train(alk_session* s, uint64_t first, uint64_t count, uint32_t epochs, uint32_t batch,
+                           float lr, uint64_t seed, float* h_loss) {
+  if (!s || batch == 0) return ALK_ERR_ARG;
+  return s->eng->card_train(first, count, epochs, batch, lr, seed, h_loss);
+}
+
+int alk_session_card_predict(alk_session* s, const float* h_x, uint64_t n, float* h_y) {
+  if (!s || (n && (!h_x || !h_y))) return ALK_ERR_ARG;
+  try {
+    s->eng->card_forward(h_x, n, h_y);
+  } catch (const alk::EngineError& e) {
+    return e.code;
+  }
+  return ALK_OK;
+}
+
+int alk_session_card_forget(alk_session* s) {
+  if (!s) return ALK_ERR_ARG;
+  s->eng->card_forget();
+  return ALK_OK;
+}
+
 void alk_session_close(alk_session* s) { delete s; }
 
 // The reference's flags (bison.y:306-331): -l MB (segment size for stores), -v,

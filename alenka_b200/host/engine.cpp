@@ -227,6 +227,7 @@ Engine::~Engine() {
     }
   basecols_.clear();
   bases_.clear();
+  if (card_mlp_) alk_mlp_free(card_mlp_, (alk_stream)stream_);
   cudaStreamSynchronize(stream_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);

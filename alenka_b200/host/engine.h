@@ -6,6 +6,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <map>
 #include <memory>
 #include <set>
@@ -138,6 +139,22 @@ struct FusedTail {
 };
 struct FusedGraph;
 
+// One fused stage as the cardinality estimator sees it: the scan, what it probes, and the
+// key column whose distinct values it counts (the build key, or the probe-aggregate
+// stage's group key).
+struct CardStage {
+  const ScanPlan* p = nullptr;
+  const std::vector<alk_colseg>* cs = nullptr;
+  int kind = 0;  // 0 build, 1 build probing another table, 2 probe-aggregate
+  int32_t probe_slot = -1;
+  const alk_ht* probe = nullptr;
+  double probe_fill = 0;  // fraction of the probed table's key range present
+  std::pair<int64_t, int64_t> probe_range{0, -1};
+  int32_t key_slot = -1;
+  std::pair<int64_t, int64_t> key_range{0, -1};
+  const ScanPlan* up = nullptr;  // the scan that built the probed table
+};
+
 class Engine {
  public:
   Engine(std::string dir, uint32_t flags);
@@ -148,6 +165,13 @@ class Engine {
   int preload(const std::string& table);
   alk_stats stats() const { return stats_; }
   void set_timing(bool on) { timing_ = on; }
+  // learned cardinality estimator (session side)
+  int card_mode(bool record, bool use);
+  uint64_t card_records(float* x, float* y, float* m, uint64_t cap) const;
+  int card_train(uint64_t first, uint64_t count, uint32_t epochs, uint32_t batch, float lr, uint64_t seed,
+                 float* loss);
+  void card_forward(const float* h_x, uint64_t n, float* h_y);
+  void card_forget();
 
   // ---- used by the planner / operators ----
   Var* var(const std::string& n);
@@ -212,6 +236,19 @@ class Engine {
   std::set<std::string> fused_nograph_;  // queries whose capture failed
   std::string cur_script_;
   bool big_fetch_ = false;  // bring every candidate back (ties beyond the first copy)
+
+  // ---- learned cardinality estimator
+  bool card_record_ = false, card_use_ = false;
+  alk_mlp* card_mlp_ = nullptr;
+  std::vector<float> card_x_, card_y_, card_m_;  // records: features, targets, target masks
+  std::map<std::string, std::vector<std::array<float, 16>>> card_hist_;  // "table.column" -> per segment
+  const std::vector<std::array<float, 16>>& card_hist(const ScanPlan& p, const std::vector<alk_colseg>& cs,
+                                                      uint32_t slot);
+  std::vector<float> card_features(const CardStage& st);
+  void card_record(const CardStage& st);
+  // Estimated survivors (after the probe) and distinct keys of a stage; false when the
+  // estimator is off or untrained.
+  bool card_estimate(const CardStage& st, uint64_t* hits, uint64_t* keys);
 
   friend struct Planner;
 };

@@ -1120,6 +1120,7 @@ bool Engine::try_fused(std::vector<Statement>& sts, size_t& i) {
     } catch (const RerunFused& r) {
       // a rerun uses the exact counts the overflowing stage reported, or fetches every
       // tied candidate
+      stats_.card_reruns++;
       fused_graphs_.erase(gkey);
       fused_seen_.erase(gkey);
       if (r.big) big_fetch_ = true;
@@ -1300,7 +1301,7 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
   CaptureGuard cap;
   // the device-side top-k (LIMIT <= 16) keeps the query free of host round trips
   const bool fast = S.op_nums[0] <= 16 && nback_max <= 32;
-  const bool capture = fast && !gkey.empty() && !big_fetch_ && fused_seen_.count(gkey);
+  const bool capture = fast && !gkey.empty() && !big_fetch_ && !card_record_ && fused_seen_.count(gkey);
   const uint64_t k_before = g_kernel_launches;
   if (capture) cap.begin(s);
   else cudaEventRecord(evq0_, s);
@@ -1308,11 +1309,22 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     auto it = card_feedback_.find(sig + "#hits");
     return it == card_feedback_.end() ? 0 : it->second + it->second / 4 + 4096;
   };
+  // A stage without recorded counts is sized by the learned estimator when it is on;
+  // returns the fraction of the key range the table is expected to hold (the exact
+  // fraction when recording), a feature of the stage that probes it.
   auto build_stage = [&](HtGuard& g, const std::string& sig, uint64_t upper, uint32_t npay,
-                         std::pair<int64_t, int64_t> range, int idx,
-                         const std::function<int(alk_ht*, uint64_t, alk_stage_status*)>& run) {
+                         std::pair<int64_t, int64_t> range, int idx, const CardStage& cst,
+                         const std::function<int(alk_ht*, uint64_t, alk_stage_status*)>& run) -> double {
     auto it = card_feedback_.find(sig);
-    const uint64_t est = it == card_feedback_.end() ? upper : std::min(upper, it->second + it->second / 4 + 1024);
+    uint64_t est = it == card_feedback_.end() ? upper : std::min(upper, it->second + it->second / 4 + 1024);
+    uint64_t hcap = hit_cap_for(sig);
+    uint64_t e_hits = 0, e_keys = 0;
+    if (it == card_feedback_.end() && !card_feedback_.count(sig + "#hits") &&
+        card_estimate(cst, &e_hits, &e_keys)) {
+      est = std::min(upper, e_keys + e_keys / 4 + 1024);
+      hcap = std::min(upper, e_hits + e_hits / 4 + 4096);
+    }
+    if (card_record_) card_record(cst);
     g.s = s;
     // a key range of at most 2^29 values (the zone maps) takes the dense, rank-addressed
     // table; wider ranges the hash table
@@ -1320,9 +1332,18 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
                        (uint64_t)range.second - (uint64_t)range.first < (1ull << 29);
     if (dense) check(alk_ht_create_dense(est, npay, range.first, range.second, &g.h, (alk_stream)s), "dense table");
     else check(alk_ht_create_range(est, npay, range.first, range.second, &g.h, (alk_stream)s), "hash table");
-    check(run(g.h, hit_cap_for(sig), &fs->st[idx]), "build stage");
+    check(run(g.h, hcap, &fs->st[idx]), "build stage");
     check(alk_ht_info_async(g.h, &fs->ht[idx], (alk_stream)s), "hash table");
     tail.pending.push_back({sig, idx, idx, upper});
+    stats_.reserved_bytes += alk_ht_bytes(g.h) + (hcap ? hcap : upper) * 8 * (dense ? 2 + npay : 1);
+    const double span = range.second >= range.first ? (double)range.second - (double)range.first + 1.0 : 0.0;
+    if (span <= 0) return 0.0;
+    if (card_record_) {
+      uint64_t n = 0;
+      check(alk_ht_info(g.h, &n, nullptr, (alk_stream)s), "hash table");
+      return std::min(1.0, (double)n / span);
+    }
+    return std::min(1.0, (double)est / span);
   };
   auto rows_of = [&](const ScanPlan& p, const std::vector<alk_colseg>& cs) {
     uint64_t n = 0;
@@ -1338,6 +1359,9 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
   alk_ht* last = nullptr;
   std::string last_sig;  // signature of the stage that built `last`
   std::map<std::string, uint32_t> last_pay;  // payload column index in the last table
+  double last_fill = 0;                      // fraction of its key range the last table holds
+  std::pair<int64_t, int64_t> last_range;    // and that key range
+  ScanPlan last_scan;                        // the scan that built it
   if (J.join_tab_cnt == 2) {
     // stage 1: d2 (innermost right) keyed on st1.rkey, carrying the d2 columns needed later
     ScanPlan p1 = plan_scan(d2);
@@ -1350,7 +1374,12 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     for (auto& c : pay1) src1.push_back((int32_t)p1.slot(c));
     auto cs1 = colsegs(p1);
     std::string sig1 = plan_sig(p1) + "|" + st1.rkey;
-    build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)pay1.size(), range_of(p1.src, st1.rkey), 0,
+    CardStage c1;
+    c1.p = &p1;
+    c1.cs = &cs1;
+    c1.key_slot = (int32_t)k1;
+    c1.key_range = range_of(p1.src, st1.rkey);
+    const double fill1 = build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)pay1.size(), range_of(p1.src, st1.rkey), 0, c1,
                 [&](alk_ht* h, uint64_t cap, alk_stage_status* st) {
                   return alk_pipeline_build_async(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount,
                                                   p1.mode.data(), p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h,
@@ -1374,7 +1403,18 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     }
     auto cs2 = colsegs(p2);
     std::string sig2 = plan_sig(p2) + "|" + build_key + "|" + sig1;
-    build_stage(ht2, sig2, rows_of(p2, cs2), (uint32_t)payload.size(), range_of(p2.src, build_key), 1,
+    CardStage c2;
+    c2.p = &p2;
+    c2.cs = &cs2;
+    c2.kind = 1;
+    c2.probe_slot = (int32_t)probe2;
+    c2.probe = ht1.h;
+    c2.probe_fill = fill1;
+    c2.probe_range = range_of(p1.src, st1.rkey);
+    c2.up = &p1;
+    c2.key_slot = key2;
+    c2.key_range = range_of(p2.src, build_key);
+    last_fill = build_stage(ht2, sig2, rows_of(p2, cs2), (uint32_t)payload.size(), range_of(p2.src, build_key), 1, c2,
                 [&](alk_ht* h, uint64_t cap, alk_stage_status* st) {
                   return alk_pipeline_build_async(cs2.data(), (uint32_t)p2.slots.size(), p2.src->segCount,
                                                   p2.mode.data(), p2.has_pred ? &p2.pred : nullptr, ht1.h,
@@ -1382,6 +1422,8 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
                 });
     last = ht2.h;
     last_sig = sig2;
+    last_range = c2.key_range;
+    last_scan = p2;
   } else {
     ScanPlan p1 = plan_scan(d1);
     uint32_t k1 = p1.slot(build_key);
@@ -1392,7 +1434,12 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     }
     auto cs1 = colsegs(p1);
     std::string sig1 = plan_sig(p1) + "|" + build_key;
-    build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)payload.size(), range_of(p1.src, build_key), 0,
+    CardStage c1;
+    c1.p = &p1;
+    c1.cs = &cs1;
+    c1.key_slot = (int32_t)k1;
+    c1.key_range = range_of(p1.src, build_key);
+    last_fill = build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)payload.size(), range_of(p1.src, build_key), 0, c1,
                 [&](alk_ht* h, uint64_t cap, alk_stage_status* st) {
                   return alk_pipeline_build_async(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount,
                                                   p1.mode.data(), p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h,
@@ -1400,6 +1447,8 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
                 });
     last = ht1.h;
     last_sig = sig1;
+    last_range = c1.key_range;
+    last_scan = p1;
   }
   const uint64_t nslots = alk_ht_slots(last);  // accumulators are indexed by table position
   // ---- probe-aggregate over the fact table
@@ -1435,10 +1484,27 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
   // the probe-aggregate kernel accumulates into slot-indexed arrays sized for every slot
   const std::string sigf = plan_sig(pf) + "|" + st2.lkey + "|" + last_sig;
   if (nslots) {
+    CardStage cf;
+    cf.p = &pf;
+    cf.cs = &csf;
+    cf.kind = 2;
+    cf.probe_slot = (int32_t)probe_f;
+    cf.probe = last;
+    cf.probe_fill = last_fill;
+    cf.probe_range = last_range;
+    cf.key_slot = (int32_t)probe_f;
+    cf.key_range = last_range;
+    cf.up = &last_scan;
+    const uint64_t upper_f = rows_of(pf, csf);
+    uint64_t hcap = hit_cap_for(sigf), e_hits = 0, e_keys = 0;
+    if (!card_feedback_.count(sigf + "#hits") && card_estimate(cf, &e_hits, &e_keys))
+      hcap = std::min(upper_f, e_hits + e_hits / 4 + 4096);
+    if (card_record_) card_record(cf);
+    stats_.reserved_bytes += (hcap ? hcap : upper_f) * 8;
     check(alk_pipeline_probe_agg_async(csf.data(), (uint32_t)pf.slots.size(), pf.src->segCount, pf.mode.data(),
                                        pf.has_pred ? &pf.pred : nullptr, last, (int32_t)probe_f, progs.data(),
                                        kinds.data(), (uint32_t)aggs.size(), acc->as<int64_t>(), stride,
-                                       cnt->as<uint64_t>(), hit_cap_for(sigf), &fs->st[2], (alk_stream)s, &tm),
+                                       cnt->as<uint64_t>(), hcap, &fs->st[2], (alk_stream)s, &tm),
           "probe-aggregate");
     tail.pending.push_back({sigf, 2, -1, 0});
     tail.timed = tm.launches > 0;

@@ -45,6 +45,33 @@ def three_way_script(seed, out="q3.txt", limit=10):
             f"STORE RES INTO '{out}' USING ('|'){lim};\n")
 
 
+def card_script(seed, out="qc.txt"):
+    """A three-way query of the README shape with seeded comparison operators and
+    constants on all three tables (the estimator's training and test queries): dates
+    anywhere in the 7-year range, any of <, <=, >, >=, sometimes a second lineitem
+    conjunct on the discount, and == or != on the market segment."""
+    r = random.Random(seed * 104729 + 3)
+    ops = ["<", "<=", ">", ">="]
+    ld = date_add_days(19920102, r.randint(0, 2540))
+    od = date_add_days(19920102, r.randint(0, 2540))
+    lf = f"l_shipdate {r.choice(ops)} {ld}"
+    if r.random() < 0.3:
+        lf += f" AND l_discount {r.choice(ops)} {r.randint(0, 10) / 100:.2f}"
+    of = f"o_orderdate {r.choice(ops)} {od}"
+    cf = f"c_mktsegment {r.choice(['==', '!='])} \"{SEGMENTS[r.randint(0, 4)]}\""
+    return (f"OFI := FILTER orders BY {of};\n"
+            f"CF := FILTER customer BY {cf};\n"
+            f"LF := FILTER lineitem BY {lf};\n"
+            "OLC := SELECT o_orderkey AS o_orderkey, o_orderdate AS o_orderdate, "
+            "o_shippriority AS o_shippriority, l_extendedprice AS price, l_discount AS discount "
+            "FROM LF JOIN OFI ON l_orderkey = o_orderkey JOIN CF ON o_custkey = c_custkey;\n"
+            "F := SELECT o_orderkey AS o_orderkey1, o_orderdate AS orderdate1, o_shippriority AS priority, "
+            "SUM(price*(1-discount)) AS sum_revenue, COUNT(o_orderkey) AS cnt "
+            "FROM OLC GROUP BY o_orderkey, o_orderdate, o_shippriority;\n"
+            "RES := ORDER F BY sum_revenue DESC, orderdate1 ASC;\n"
+            f"STORE RES INTO '{out}' USING ('|') LIMIT 10;\n")
+
+
 # Full-size shapes (rows): the single-table workload and the three-way pipeline.
 FLAT_ROWS = 6_000_000
 THREE_WAY = dict(customers=1_500_000, orders=15_000_000, lineitems=60_000_000)

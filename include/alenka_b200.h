@@ -73,6 +73,9 @@ typedef struct alk_stats {
   uint64_t hot_kernel_bytes; /* algorithmic bytes that kernel moves */
   uint64_t hot_kernel_launches;
   double query_device_ms;    /* device time of the fused query (events around its device work) */
+  uint64_t reserved_bytes;   /* survivor-list and hash-table bytes the fused stages reserved */
+  uint32_t card_estimates;   /* fused stages sized by the learned estimator */
+  uint32_t card_reruns;      /* fused query runs repeated because a size was too small */
 } alk_stats;
 int alk_session_stats(alk_session* s, alk_stats* out);
 /* Enable CUDA-event timing of the dominant kernel (adds two event records per launch). */
@@ -249,6 +252,8 @@ int alk_ht_info(const alk_ht* h, uint64_t* nslots, int* flags, alk_stream stream
 /* Slot range of a table: payload columns and per-key accumulators are indexed by the
  * key's table position, 0 <= slot < alk_ht_slots(h). */
 uint64_t alk_ht_slots(const alk_ht* h);
+/* Device bytes the table holds (keys, payload, bitmap, rank). */
+uint64_t alk_ht_bytes(const alk_ht* h);
 /* Device address of the key column (slot-indexed; free slots of a hash table hold the
  * byte pattern 0x80 repeated, 0x8080808080808080; a dense table's slots at and beyond
  * its key count are undefined). */
@@ -348,6 +353,70 @@ int alk_gen_three_way(const char* dir, uint64_t customers, uint64_t orders, uint
                       uint32_t seg_rows, uint64_t seed, int delta, char* err, int err_len);
 /* A yyyymmdd date value moved by a number of days (proleptic Gregorian). */
 int64_t alk_date_add_days(int64_t yyyymmdd_value, int64_t days);
+
+/* ------------------------------------------ 4. learned cardinality estimator
+ * No counterpart in the reference, which sizes every buffer from the free device memory
+ * (getFreeMem, cm.cu:3184) and the rows scanned. A small MLP, 64 -> 128 -> 128 -> 3 with
+ * ReLU, BF16 weights and FP32 accumulation, predicts per (stage, segment) three log
+ * fractions: the rows passing the filter (of the rows), the rows passing the join probe
+ * (of those) and the distinct key values (of those). The fused plan sizes its survivor
+ * lists and hash tables from them on a query's first run; a size that proves too small
+ * makes the query run again with the exact counts (the estimate steers the plan, never
+ * the answer). */
+#define ALK_CARD_FEATURES 64
+#define ALK_CARD_HIDDEN 128
+#define ALK_CARD_OUTPUTS 3
+typedef struct alk_mlp alk_mlp;
+/* Parameters in order W1[128][64], b1[128], W2[128][128], b2[128], W3[3][128], b3[3]. */
+uint32_t alk_mlp_param_count(void);
+/* Seeded initialisation (uniform, fan-in scaled; zero biases). Synchronizes the stream. */
+int alk_mlp_create(uint64_t seed, alk_mlp** out, alk_stream stream);
+void alk_mlp_free(alk_mlp* m, alk_stream stream);
+/* Replace the FP32 master parameters (h_master, alk_mlp_param_count() floats); the BF16
+ * weights are their round-to-nearest-even copies. Synchronizes the stream. */
+int alk_mlp_set_params(alk_mlp* m, const float* h_master, alk_stream stream);
+/* Copies of the FP32 master parameters and of their BF16 copies (either may be NULL). */
+int alk_mlp_params(const alk_mlp* m, float* h_master, uint16_t* h_bf16, alk_stream stream);
+/* d_y[n][3] = MLP(d_x[n][64]) with the BF16 weights. Asynchronous. */
+int alk_mlp_forward(alk_mlp* m, const float* d_x, uint64_t n, float* d_y, alk_stream stream);
+/* Gradient of the masked mean squared error sum((y - t)^2 * mask) / n with respect to the
+ * parameters (layout above; bias gradients included), into d_grad; *h_loss = the loss.
+ * The forward pass uses the BF16 weights. Synchronizes the stream. */
+int alk_mlp_gradients(alk_mlp* m, const float* d_x, const float* d_t, const float* d_mask, uint64_t n,
+                      float* d_grad, float* h_loss, alk_stream stream);
+/* Adam (beta 0.9 / 0.999, eps 1e-8) over mini-batches of `batch` rows in order, for
+ * `epochs` passes; *h_loss = mean loss of the last pass. Synchronizes the stream. */
+int alk_mlp_train(alk_mlp* m, const float* d_x, const float* d_t, const float* d_mask, uint64_t n, uint32_t epochs,
+                  uint32_t batch, float lr, float* h_loss, alk_stream stream);
+/* 16 equal-width bins of a column segment's values over [lo, hi] (values outside go to
+ * the end bins) into d_hist16[16]. Asynchronous. */
+int alk_card_hist16(const alk_colseg* seg, int64_t lo, int64_t hi, uint32_t* d_hist16, alk_stream stream);
+/* Exact per-segment counts of a stage (the estimator's labels and the exact counting
+ * pass): h_counts[3 * g] rows of segment g passing pred, [3 * g + 1] of those whose
+ * probe_slot value is a key of probe (all of them without a probe), [3 * g + 2] distinct
+ * key_slot values among those (UINT64_MAX when key_slot < 0 or the range [key_min,
+ * key_max] is wider than 2^30). Segments with seg_mode 0 count 0. Synchronizes. */
+int alk_card_count(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                   const alk_program* pred, const alk_ht* probe, int32_t probe_slot, int32_t key_slot,
+                   int64_t key_min, int64_t key_max, uint64_t* h_counts, alk_stream stream);
+
+/* Session side. record: every fused query also runs the exact counting pass of each stage
+ * and keeps one record (features, log-fraction targets, target mask) per scanned segment;
+ * such runs are not captured into CUDA graphs. use: stages without recorded counts are
+ * sized by the estimator (when one is trained). */
+int alk_session_card_mode(alk_session* s, int record, int use);
+/* Records kept so far: *h_n = their number; up to cap of them are copied (features
+ * [cap][64], targets [cap][3], masks [cap][3]; NULL pointers skip a copy). */
+int alk_session_card_records(alk_session* s, float* h_x, float* h_y, float* h_mask, uint64_t cap, uint64_t* h_n);
+/* Train the session's estimator (created from seed on first use) on records
+ * [first, first + count), shuffled by seed, with alk_mlp_train. */
+int alk_session_card_train(alk_session* s, uint64_t first, uint64_t count, uint32_t epochs, uint32_t batch,
+                           float lr, uint64_t seed, float* h_loss);
+/* Estimator outputs for n feature rows (host arrays). */
+int alk_session_card_predict(alk_session* s, const float* h_x, uint64_t n, float* h_y);
+/* Forget the exact counts recorded by earlier runs and the captured graphs, so that the
+ * next run of a query is a first run again. */
+int alk_session_card_forget(alk_session* s);
 
 /* Device properties of the current device. */
 int alk_device_info(int* sm_count, int* cc_major, int* cc_minor);

@@ -210,6 +210,60 @@ def test_build_async_status_and_payload(bits):
     del kb, vb
 
 
+@pytest.mark.parametrize("route", ["records", "positions"])
+@pytest.mark.parametrize("dup", [False, True])
+def test_dense_build(route, dup):
+    """Dense (rank-addressed) table: slots are the keys' ranks, so the key column comes out
+    sorted and each key carries its row's payload. 'records': no predicate, so the
+    TMA-staged scan records [position, key, payload] itself; 'positions': a predicate that
+    is not a conjunction runs the register-machine scan, then the bitmap pass. A repeated
+    key is reported as a duplicate on either route."""
+    import torch
+    L = _lib()
+    L.alk_ht_create_dense.argtypes = [c.c_uint64, c.c_uint32, c.c_int64, c.c_int64, c.POINTER(c.c_void_p),
+                                      c.c_void_p]
+    rng = np.random.default_rng(11)
+    n = 300_000
+    keys = rng.permutation(n).astype(np.int64) * 3 + 11
+    if dup:
+        keys[-1] = keys[0]
+    vals = rng.integers(0, 1 << 30, n).astype(np.int64)
+    kb, ks = _column(keys)
+    vb, vs = _column(vals)
+    cols = (ColSeg * 2)(ks, vs)
+    mode = (c.c_uint8 * 1)(2)
+    pred = _or_pred(1, 0) if route == "positions" else None
+    ht = c.c_void_p()
+    assert L.alk_ht_create_dense(n + 16, 1, int(keys.min()), int(keys.max()), c.byref(ht), None) == ALK_OK
+    pay = (c.c_int32 * 1)(1)
+    try:
+        rows_in, hits = c.c_uint64(), c.c_uint64()
+        rc = L.alk_pipeline_build(cols, 2, 1, mode, c.byref(pred) if pred else None, None, -1, ht, 0, pay, 0,
+                                  c.byref(rows_in), c.byref(hits), None)
+        assert rc == ALK_OK and rows_in.value == n
+        ins, fl = c.c_uint64(), c.c_int()
+        assert L.alk_ht_info(ht, c.byref(ins), c.byref(fl), None) == ALK_OK
+        distinct = np.unique(keys)
+        assert ins.value == len(distinct)
+        assert (fl.value & 1) == (1 if dup else 0)
+        if dup:
+            return
+        got = torch.empty(2 * n, dtype=torch.int64, device="cuda")
+        ident = torch.arange(n, dtype=torch.int32, device="cuda")
+        cnt = torch.tensor([n], dtype=torch.int64, device="cuda")
+        colp = (c.c_void_p * 2)(L.alk_ht_keys(ht), L.alk_ht_payload(ht, 0))
+        assert L.alk_gather_rows(colp, 2, ident.data_ptr(), cnt.data_ptr(), n, got.data_ptr(), None) == ALK_OK
+        torch.cuda.synchronize()
+        tk, tv = got.cpu().numpy()[:n], got.cpu().numpy()[n:]
+        order = np.argsort(keys)
+        assert np.array_equal(tk, keys[order])  # slot = rank of the key
+        assert np.array_equal(tv, vals[order])
+    finally:
+        L.alk_ht_free(ht, None)
+        torch.cuda.synchronize()
+    del kb, vb
+
+
 @pytest.mark.parametrize("k", [1, 10, 16])
 def test_topk_select_and_gather_rows(k):
     import torch
