@@ -45,6 +45,10 @@ class Stats(ctypes.Structure):
     ]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("consumer_warps", ctypes.c_uint32), ("stages", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32)]
+
+
 def _declare(L):
     c = ctypes
     vp, u32, u64, i64, i32 = c.c_void_p, c.c_uint32, c.c_uint64, c.c_int64, c.c_int
@@ -87,6 +91,8 @@ def _declare(L):
     L.alk_mlp_train.argtypes = [vp, vp, vp, vp, u64, u32, u32, c.c_float, fp, vp]
     L.alk_card_hist16.argtypes = [vp, i64, i64, vp, vp]
     L.alk_card_count.argtypes = [vp, u32, u32, vp, vp, vp, i32, i32, i64, i64, c.POINTER(u64), vp]
+    L.alk_session_execute_batch.argtypes = [vp, c.POINTER(c.c_char_p), u32]
+    L.alk_session_tuning.argtypes = [vp, c.POINTER(Tuning), i32]
     L.alk_session_card_mode.argtypes = [vp, i32, i32]
     L.alk_session_card_records.argtypes = [vp, fp, fp, fp, u64, c.POINTER(u64)]
     L.alk_session_card_train.argtypes = [vp, u64, u64, u32, u32, c.c_float, u64, fp]
@@ -140,6 +146,20 @@ class Session:
 
     def set_timing(self, on):
         lib().alk_session_set_timing(self._h, 1 if on else 0)
+
+    def execute_batch(self, scripts):
+        """Runs the scripts with one batched launch for their dense group-bys."""
+        arr = (ctypes.c_char_p * len(scripts))(*[x.encode() for x in scripts])
+        rc = lib().alk_session_execute_batch(self._h, arr, len(scripts))
+        if rc != ALK_OK:
+            raise AlenkaError(rc, lib().alk_session_error(self._h).decode())
+
+    def tuning(self, autotune=None):
+        """Launch shape of the last batched group-by; autotune True/False switches the
+        autotuner."""
+        t = Tuning()
+        lib().alk_session_tuning(self._h, ctypes.byref(t), -1 if autotune is None else int(bool(autotune)))
+        return (t.consumer_warps, t.stages, t.blocks_per_sm)
 
     # ---- learned cardinality estimator
     def card_mode(self, record=False, use=False):

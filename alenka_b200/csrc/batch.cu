@@ -1,0 +1,466 @@
+// Batched filter + group-by: many queries of the single-table FILTER -> SELECT ... GROUP BY
+// shape (the reference runs each as emit_filter + emit_select, operators.cu:2306 and
+// :1801, one query at a time) in one persistent launch over a work list of (query,
+// segment) items. Each block takes a contiguous range of the list's tiles, so it meets
+// few query boundaries. One producer warp stages a tile's columns into shared memory with
+// bulk copies; consumer warps evaluate the query's conjuncts on the stored values, form
+// the group slot from small-domain key columns (dense: slot = sum (key - min) * stride)
+// and fold each aggregate input, a product of two affine column terms, into accumulators
+// private to each thread. A warp folds its lanes' accumulators into the query's global
+// accumulators when it moves to another query and at the end.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "internal.h"
+#include "scan.cuh"
+
+namespace {
+constexpr int kGbCols = 8;
+constexpr int kGbAggs = 8;
+constexpr uint32_t kGbMaxStages = 4;
+
+struct GbQuery {
+  uint32_t ncols, nconj, nkeys, nagg;
+  Conj conj[kMaxConj];  // slot: the query's column index
+  int32_t key_col[2];
+  int64_t key_min[2];
+  uint64_t key_mul[2];
+  uint64_t key_span[2];
+  uint32_t nslots, nacc;  // nacc = nagg + 1: the row count is the last accumulator
+  alk_gb_agg agg[kGbAggs];
+  int64_t* acc;  // [nacc][nslots]
+};
+struct GbItem {
+  uint32_t query, mode, rows, pad;
+  alk_colseg col[kGbCols];
+  ConjSeg cs[kMaxConj];
+};
+struct GbArgs {
+  const GbItem* items;
+  const uint32_t* item_tile;  // [nitems + 1]: item i owns tiles [item_tile[i], item_tile[i + 1])
+  uint32_t nitems, ntiles;
+  const GbQuery* queries;
+  uint32_t nst, stage_bytes;  // stages in flight, bytes of one stage
+  uint32_t cw;                // consumer warps; a tile is cw * 256 rows
+  uint32_t max_acc;           // private accumulators per thread
+  unsigned long long* item_rows;  // survivors per item
+  int* err;
+};
+
+__device__ __forceinline__ uint32_t find_item(const uint32_t* item_tile, uint32_t n, uint32_t tile) {
+  uint32_t lo = 0, hi = n;  // item_tile[lo] <= tile < item_tile[hi]
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(item_tile + mid) <= tile) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int64_t stored_at(const unsigned char* p, uint32_t bits, uint32_t r) {
+  switch (bits) {
+    case 8: return p[r];
+    case 16: return ((const uint16_t*)p)[r];
+    case 32: return ((const uint32_t*)p)[r];
+    default: return ((const int64_t*)p)[r];
+  }
+}
+
+// A warp folds its lanes' private accumulators (slot-major, [acc][lane]) into the
+// query's global accumulators and clears them.
+__device__ void gb_flush(const GbQuery& q, int64_t* priv, uint32_t lane) {
+  for (uint32_t j = 0; j < q.nslots * q.nacc; j++) {
+    const uint32_t a = j % q.nacc, slot = j / q.nacc;
+    const uint32_t kind = a < q.nagg ? q.agg[a].kind : (uint32_t)ALK_AGG_COUNT;
+    int64_t v = priv[j * 32 + lane];
+    priv[j * 32 + lane] = kind == ALK_AGG_MIN ? INT64_MAX : kind == ALK_AGG_MAX ? INT64_MIN : 0;
+    for (int o = 16; o; o >>= 1) {
+      const int64_t w = __shfl_xor_sync(0xffffffffu, v, o);
+      v = kind == ALK_AGG_MIN ? min(v, w) : kind == ALK_AGG_MAX ? max(v, w) : (int64_t)((uint64_t)v + (uint64_t)w);
+    }
+    if (lane == 0) {
+      int64_t* dst = q.acc + (size_t)a * q.nslots + slot;
+      if (kind == ALK_AGG_MIN) {
+        if (v != INT64_MAX) atomicMin((long long*)dst, (long long)v);
+      } else if (kind == ALK_AGG_MAX) {
+        if (v != INT64_MIN) atomicMax((long long*)dst, (long long)v);
+      } else if (v) {
+        atomicAdd((unsigned long long*)dst, (unsigned long long)v);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void gb_clear(const GbQuery& q, int64_t* priv, uint32_t lane) {
+  for (uint32_t j = 0; j < q.nslots * q.nacc; j++) {
+    const uint32_t a = j % q.nacc;
+    const uint32_t kind = a < q.nagg ? q.agg[a].kind : (uint32_t)ALK_AGG_COUNT;
+    priv[j * 32 + lane] = kind == ALK_AGG_MIN ? INT64_MAX : kind == ALK_AGG_MAX ? INT64_MIN : 0;
+  }
+}
+
+__global__ void k_gb_tma(const __grid_constant__ GbArgs g) {
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  __shared__ __align__(8) uint64_t s_full[kGbMaxStages], s_empty[kGbMaxStages];
+  __shared__ uint32_t s_item[kGbMaxStages];
+  __shared__ int s_abort;
+  const uint32_t nst = g.nst, cw = g.cw;
+  const uint32_t tile_rows = cw * 32 * kItems;
+  if (threadIdx.x == 0) {
+    s_abort = 0;
+    for (uint32_t i = 0; i < nst; i++) {
+      mbar_init(&s_full[i], 1);
+      mbar_init(&s_empty[i], cw);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  volatile int* abort_flag = &s_abort;
+  // this block's contiguous range of the work list's tiles
+  const uint32_t t0 = (uint32_t)((uint64_t)blockIdx.x * g.ntiles / gridDim.x);
+  const uint32_t t1 = (uint32_t)((uint64_t)(blockIdx.x + 1) * g.ntiles / gridDim.x);
+
+  if (warp == cw) {
+    // ---- producer: one thread issues the bulk copies
+    if (lane != 0) return;
+    uint32_t issued = 0;
+    for (uint32_t it = 0; t0 + it < t1; it++) {
+      if (*abort_flag) break;
+      const uint32_t tile = t0 + it, st = it % nst;
+      if (it >= nst && !mbar_wait(&s_empty[st], (it / nst - 1) & 1)) {
+        atomicExch(g.err, ALK_ERR_TIMEOUT);
+        *abort_flag = 1;
+        break;
+      }
+      const uint32_t i = find_item(g.item_tile, g.nitems, tile);
+      const GbItem& item = g.items[i];
+      const GbQuery& q = g.queries[item.query];
+      const uint32_t row0 = (tile - __ldg(g.item_tile + i)) * tile_rows;
+      const uint32_t rows = min(tile_rows, item.rows - row0);
+      s_item[st] = i;
+      uint32_t total = 0;
+      for (uint32_t c = 0; c < q.ncols; c++) total += (rows * (item.col[c].bits / 8) + 15) & ~15u;
+      unsigned char* buf = s_dyn + (size_t)st * g.stage_bytes;
+      mbar_expect_tx(&s_full[st], total);
+      uint32_t off = 0;
+      for (uint32_t c = 0; c < q.ncols; c++) {
+        const uint32_t w = item.col[c].bits / 8, n = (rows * w + 15) & ~15u;
+        bulk_g2s(buf + off, (const unsigned char*)item.col[c].data + (uint64_t)row0 * w, n, &s_full[st]);
+        off += n;
+      }
+      issued = it + 1;
+    }
+    for (uint32_t it = issued > nst ? issued - nst : 0; it < issued; it++)
+      mbar_wait(&s_full[it % nst], (it / nst) & 1);
+    return;
+  }
+
+  // ---- consumers: warp `warp` owns rows warp * 256 + k * 32 + lane of every tile
+  int64_t* priv = (int64_t*)(s_dyn + (size_t)nst * g.stage_bytes) + (size_t)warp * g.max_acc * 32;
+  // the warp's copies of its current query and item descriptors
+  GbQuery& q = ((GbQuery*)(s_dyn + (size_t)nst * g.stage_bytes + (size_t)cw * g.max_acc * 32 * 8))[warp];
+  GbItem& item = ((GbItem*)((unsigned char*)(&q - warp) + sizeof(GbQuery) * cw))[warp];
+  uint32_t cur_q = 0xffffffffu, cur_item = 0xffffffffu;
+  unsigned long long surv = 0;  // survivors of cur_item seen by this warp (warp-uniform)
+  const uint32_t r0 = warp * (32 * kItems) + lane;
+  for (uint32_t it = 0; t0 + it < t1; it++) {
+    if (__any_sync(0xffffffffu, *abort_flag)) break;
+    const uint32_t st = it % nst;
+    if (!mbar_wait_warp(&s_full[st], (it / nst) & 1)) {
+      if (lane == 0) {
+        atomicExch(g.err, ALK_ERR_TIMEOUT);
+        *abort_flag = 1;
+      }
+      break;
+    }
+    const uint32_t i = s_item[st];
+    if (i != cur_item) {
+      if (cur_item != 0xffffffffu && lane == 0 && surv) atomicAdd(g.item_rows + cur_item, surv);
+      surv = 0;
+      cur_item = i;
+      __syncwarp();
+      for (uint32_t w = lane; w < sizeof(GbItem) / 4; w += 32) ((uint32_t*)&item)[w] = ((const uint32_t*)(g.items + i))[w];
+      __syncwarp();
+      const uint32_t qi = item.query;
+      if (qi != cur_q) {
+        if (cur_q != 0xffffffffu) gb_flush(q, priv, lane);
+        __syncwarp();
+        for (uint32_t w = lane; w < sizeof(GbQuery) / 4; w += 32)
+          ((uint32_t*)&q)[w] = ((const uint32_t*)(g.queries + qi))[w];
+        __syncwarp();
+        gb_clear(q, priv, lane);
+        cur_q = qi;
+      }
+    }
+    const uint32_t row0 = (it + t0 - __ldg(g.item_tile + i)) * tile_rows;
+    const uint32_t rows = min(tile_rows, item.rows - row0);
+    const unsigned char* buf = s_dyn + (size_t)st * g.stage_bytes;
+    // staged column offsets of this tile
+    uint32_t coff[kGbCols];
+    {
+      uint32_t off = 0;
+#pragma unroll
+      for (int c = 0; c < kGbCols; c++) {
+        coff[c] = off;
+        if (c < (int)q.ncols) off += (rows * (item.col[c].bits / 8) + 15) & ~15u;
+      }
+    }
+    uint32_t live = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; k++)
+      if (r0 + k * 32 < rows) live |= 1u << k;
+    if (item.mode != 1) {
+      for (uint32_t c = 0; c < q.nconj && live; c++) {
+        const uint32_t col = q.conj[c].slot;
+        const alk_colseg& d = item.col[col];
+        if (d.bits <= 32) {
+          uint32_t x[kItems];
+          load_raw32<32>(buf + coff[col], d.bits, r0, x);
+          live = conj_filter32(q.conj[c], item.cs[c], d.lower, x, live);
+        } else {
+          uint64_t x[kItems];
+          load_raw<false, 32>(buf + coff[col], d.bits, r0, live, x);
+          live = conj_filter(q.conj[c], item.cs[c], d.lower, x, live);
+        }
+      }
+    }
+    surv += __reduce_add_sync(0xffffffffu, (unsigned)__popc(live));
+    // fold the survivors
+    for (uint32_t m = live; m; m &= m - 1) {
+      const uint32_t r = r0 + (__ffs(m) - 1) * 32;
+      uint64_t slot = 0;
+      bool ok = true;
+      for (uint32_t j = 0; j < q.nkeys; j++) {
+        const alk_colseg& d = item.col[q.key_col[j]];
+        const uint64_t o = (uint64_t)(stored_at(buf + coff[q.key_col[j]], d.bits, r) + d.lower) - (uint64_t)q.key_min[j];
+        ok = ok && o < q.key_span[j];
+        slot += o * q.key_mul[j];
+      }
+      if (!ok) {  // a key outside the range the zone maps gave: the plan is wrong
+        atomicExch(g.err, ALK_ERR_ARG);
+        continue;
+      }
+      int64_t* p = priv + (size_t)slot * q.nacc * 32 + lane;
+      for (uint32_t a = 0; a < q.nagg; a++) {
+        const alk_gb_agg& ag = q.agg[a];
+        if (ag.kind == ALK_AGG_COUNT) {
+          p[a * 32] += 1;
+          continue;
+        }
+        const alk_colseg& da = item.col[ag.a];
+        int64_t v = stored_at(buf + coff[ag.a], da.bits, r) + da.lower;
+        if (ag.am != 1 || ag.ac != 0) v = (int64_t)((uint64_t)v * (uint64_t)ag.am + (uint64_t)ag.ac);
+        if (ag.b >= 0) {
+          const alk_colseg& db = item.col[ag.b];
+          const int64_t w = stored_at(buf + coff[ag.b], db.bits, r) + db.lower;
+          v = (int64_t)((uint64_t)v * ((uint64_t)w * (uint64_t)ag.bm + (uint64_t)ag.bc));
+        }
+        int64_t& acc = p[a * 32];
+        if (ag.kind == ALK_AGG_MIN) acc = min(acc, v);
+        else if (ag.kind == ALK_AGG_MAX) acc = max(acc, v);
+        else acc = (int64_t)((uint64_t)acc + (uint64_t)v);
+      }
+      p[q.nagg * 32] += 1;
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&s_empty[st]);
+  }
+  if (cur_q != 0xffffffffu) gb_flush(q, priv, lane);
+  if (cur_item != 0xffffffffu && lane == 0 && surv) atomicAdd(g.item_rows + cur_item, surv);
+}
+
+__global__ void k_gb_init(int64_t* acc, uint64_t nslots, const uint32_t* kinds, uint32_t nacc) {
+  const uint64_t n = nslots * nacc;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t k = kinds[i / nslots];
+    acc[i] = k == ALK_AGG_MIN ? INT64_MAX : k == ALK_AGG_MAX ? INT64_MIN : 0;
+  }
+}
+
+int sms_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+}  // namespace
+
+#define CK(x)                                         \
+  do {                                                \
+    cudaError_t e_ = (x);                             \
+    if (e_ != cudaSuccess) return alk::cuda_fail(e_); \
+  } while (0)
+
+extern "C" {
+
+int alk_batch_groupby(const alk_gb_query* qs, uint32_t nq, const alk_gb_tuning* tune, alk_gb_tuning* used,
+                      alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!qs || nq == 0) return ALK_ERR_ARG;
+  std::vector<GbQuery> hq(nq);
+  std::vector<GbItem> items;
+  std::vector<uint32_t> item_tile;
+  std::vector<uint32_t> kinds_all;
+  std::vector<std::pair<uint32_t, uint32_t>> item_src;  // (query, segment) of each item
+  uint32_t max_acc = 1, max_stage = 16;
+  const uint32_t cw = tune && tune->consumer_warps ? tune->consumer_warps : 8;
+  if (cw != 4 && cw != 8) return ALK_ERR_ARG;
+  const uint32_t tile_rows = cw * 32 * kItems;
+  uint64_t ntiles = 0;
+  for (uint32_t qi = 0; qi < nq; qi++) {
+    const alk_gb_query& a = qs[qi];
+    GbQuery& q = hq[qi];
+    std::memset(&q, 0, sizeof(q));
+    if (a.ncols == 0 || a.ncols > kGbCols || a.nkeys > 2 || a.nagg > kGbAggs || !a.cols || !a.d_acc) return ALK_ERR_ARG;
+    q.ncols = a.ncols;
+    q.nkeys = a.nkeys;
+    q.nagg = a.nagg;
+    uint64_t nslots = 1;
+    for (int j = (int)a.nkeys - 1; j >= 0; j--) {
+      if (a.key_col[j] < 0 || (uint32_t)a.key_col[j] >= a.ncols || a.key_max[j] < a.key_min[j]) return ALK_ERR_ARG;
+      const uint64_t span = (uint64_t)a.key_max[j] - (uint64_t)a.key_min[j] + 1;
+      if (span == 0 || span > 4096) return ALK_ERR_UNSUPPORTED;
+      q.key_col[j] = a.key_col[j];
+      q.key_min[j] = a.key_min[j];
+      q.key_span[j] = span;
+      q.key_mul[j] = nslots;
+      nslots *= span;
+    }
+    q.nslots = (uint32_t)nslots;
+    q.nacc = a.nagg + 1;
+    if (nslots * q.nacc > 64) return ALK_ERR_UNSUPPORTED;  // private accumulators per thread
+    max_acc = std::max<uint32_t>(max_acc, (uint32_t)(nslots * q.nacc));
+    for (uint32_t k = 0; k < a.nagg; k++) {
+      const alk_gb_agg& ag = a.agg[k];
+      if (ag.kind > ALK_AGG_MAX) return ALK_ERR_ARG;
+      if (ag.kind != ALK_AGG_COUNT && (ag.a < 0 || (uint32_t)ag.a >= a.ncols || ag.b >= (int32_t)a.ncols))
+        return ALK_ERR_ARG;
+      q.agg[k] = ag;
+    }
+    q.acc = a.d_acc;
+    // the filter as conjuncts on the query's columns
+    alk_program prog{};
+    if (a.pred) prog = *a.pred;
+    std::vector<alk::CardConj> cj;
+    if (!alk::program_conjuncts(prog, cj) || cj.size() > (size_t)kMaxConj) return ALK_ERR_UNSUPPORTED;
+    q.nconj = (uint32_t)cj.size();
+    for (uint32_t c = 0; c < q.nconj; c++) {
+      if (cj[c].slot >= a.ncols) return ALK_ERR_ARG;
+      q.conj[c] = Conj{cj[c].mul, cj[c].k, cj[c].slot, cj[c].op};
+    }
+    for (uint32_t k = 0; k <= a.nagg; k++) kinds_all.push_back(k < a.nagg ? a.agg[k].kind : ALK_AGG_COUNT);
+    // work items: the scanned segments
+    for (uint32_t gi = 0; gi < a.nseg; gi++) {
+      const uint8_t mode = a.seg_mode ? a.seg_mode[gi] : 2;
+      if (mode == 0) continue;
+      GbItem it;
+      std::memset(&it, 0, sizeof(it));
+      it.query = qi;
+      it.mode = mode;
+      it.rows = a.cols[gi].rows;
+      uint32_t stage = 0;
+      for (uint32_t c = 0; c < a.ncols; c++) {
+        const alk_colseg& d = a.cols[(size_t)c * a.nseg + gi];
+        if (d.rows != it.rows || !(d.bits == 8 || d.bits == 16 || d.bits == 32 || d.bits == 64)) return ALK_ERR_ARG;
+        if (d.rows && (!d.data || ((uintptr_t)d.data & 15))) return ALK_ERR_ARG;  // bulk copies: 16-byte aligned
+        it.col[c] = d;
+        stage += (tile_rows * (d.bits / 8) + 15) & ~15u;
+      }
+      for (uint32_t c = 0; c < q.nconj; c++) it.cs[c] = conj_seg(q.conj[c], it.col[q.conj[c].slot]);
+      if (it.rows == 0) continue;
+      item_src.push_back({qi, gi});
+      max_stage = std::max(max_stage, stage);
+      item_tile.push_back((uint32_t)ntiles);
+      ntiles += (it.rows + tile_rows - 1) / tile_rows;
+      items.push_back(it);
+    }
+  }
+  if (ntiles >= 0xffffffffull) return ALK_ERR_TOO_LARGE;
+  item_tile.push_back((uint32_t)ntiles);
+  const uint32_t nitems = (uint32_t)items.size();
+  // device copies: queries, items, item tiles, kinds, item survivor counts, error flag
+  const size_t o_q = 0;
+  const size_t o_items = (o_q + sizeof(GbQuery) * nq + 255) & ~size_t(255);
+  const size_t o_tile = (o_items + sizeof(GbItem) * nitems + 255) & ~size_t(255);
+  const size_t o_kinds = (o_tile + 4 * item_tile.size() + 255) & ~size_t(255);
+  const size_t o_rows = (o_kinds + 4 * kinds_all.size() + 255) & ~size_t(255);
+  const size_t o_err = o_rows + 8 * (size_t)std::max<uint32_t>(nitems, 1);
+  const size_t bytes = o_err + 16;
+  std::vector<uint8_t> hb(o_rows, 0);
+  std::memcpy(&hb[o_q], hq.data(), sizeof(GbQuery) * nq);
+  if (nitems) std::memcpy(&hb[o_items], items.data(), sizeof(GbItem) * nitems);
+  std::memcpy(&hb[o_tile], item_tile.data(), 4 * item_tile.size());
+  std::memcpy(&hb[o_kinds], kinds_all.data(), 4 * kinds_all.size());
+  uint8_t* db = nullptr;
+  CK(cudaMallocAsync((void**)&db, bytes, s));
+  cudaError_t ue;
+  const void* src = alk::upload_source(hb.data(), hb.size(), s, &ue);
+  CK(ue);
+  CK(cudaMemcpyAsync(db, src, hb.size(), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(db + o_rows, 0, bytes - o_rows, s));
+  // accumulators: every query's [nacc][nslots] starts at the identity of its aggregate
+  {
+    size_t k0 = 0;
+    for (uint32_t qi = 0; qi < nq; qi++) {
+      k_gb_init<<<std::max<uint32_t>(1, std::min<uint32_t>((hq[qi].nslots * hq[qi].nacc + 255) / 256, 64)), 256, 0,
+                  s>>>(hq[qi].acc, hq[qi].nslots, (const uint32_t*)(db + o_kinds) + k0, hq[qi].nacc);
+      k0 += hq[qi].nacc;
+      alk::g_kernel_launches++;
+    }
+    CK(cudaGetLastError());
+  }
+  GbArgs g{};
+  g.items = (const GbItem*)(db + o_items);
+  g.item_tile = (const uint32_t*)(db + o_tile);
+  g.nitems = nitems;
+  g.ntiles = (uint32_t)ntiles;
+  g.queries = (const GbQuery*)(db + o_q);
+  g.nst = tune && tune->stages ? std::min<uint32_t>(tune->stages, kGbMaxStages) : 3;
+  g.cw = cw;
+  g.stage_bytes = (max_stage + 127) & ~127u;
+  g.max_acc = max_acc;
+  g.item_rows = (unsigned long long*)(db + o_rows);
+  g.err = (int*)(db + o_err);
+  const size_t smem =
+      (size_t)g.nst * g.stage_bytes + (size_t)cw * max_acc * 32 * 8 + (sizeof(GbQuery) + sizeof(GbItem)) * cw;
+  int rc = ALK_OK;
+  if (ntiles) {
+    CK(cudaFuncSetAttribute(k_gb_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_gb_tma, (int)(cw + 1) * 32, smem));
+    if (occ < 1) {
+      cudaFreeAsync(db, s);
+      return ALK_ERR_UNSUPPORTED;
+    }
+    const uint32_t per_sm = tune && tune->blocks_per_sm ? std::min<uint32_t>(tune->blocks_per_sm, occ) : occ;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)sms_count() * per_sm);
+    k_gb_tma<<<grid, (cw + 1) * 32, smem, s>>>(g);
+    alk::g_kernel_launches++;
+    CK(cudaGetLastError());
+    if (used) {
+      used->consumer_warps = cw;
+      used->stages = g.nst;
+      used->blocks_per_sm = per_sm;
+    }
+  }
+  int herr = 0;
+  std::vector<uint64_t> irows(nitems);
+  CK(cudaMemcpyAsync(&herr, db + o_err, 4, cudaMemcpyDeviceToHost, s));
+  if (nitems) CK(cudaMemcpyAsync(irows.data(), db + o_rows, 8 * (size_t)nitems, cudaMemcpyDeviceToHost, s));
+  CK(cudaFreeAsync(db, s));
+  CK(cudaStreamSynchronize(s));
+  for (uint32_t qi = 0; qi < nq; qi++)
+    if (qs[qi].h_seg_rows) std::fill(qs[qi].h_seg_rows, qs[qi].h_seg_rows + qs[qi].nseg, 0);
+  for (uint32_t i = 0; i < nitems; i++)
+    if (qs[item_src[i].first].h_seg_rows) qs[item_src[i].first].h_seg_rows[item_src[i].second] = irows[i];
+  if (herr) rc = herr;
+  return rc;
+}
+
+}  // extern "C"

@@ -68,6 +68,25 @@ int alk_session_set_timing(alk_session* s, int on) {
   return ALK_OK;
 }
 
+int alk_session_execute_batch(alk_session* s, const char* const* scripts, uint32_t n) {
+  if (!s || (n && !scripts)) return ALK_ERR_ARG;
+  std::vector<std::string> v;
+  for (uint32_t i = 0; i < n; i++) {
+    if (!scripts[i]) return ALK_ERR_ARG;
+    v.emplace_back(scripts[i]);
+  }
+  int rc = s->eng->execute_batch(v);
+  s->err = s->eng->error();
+  return rc;
+}
+
+int alk_session_tuning(alk_session* s, alk_gb_tuning* out, int autotune) {
+  if (!s) return ALK_ERR_ARG;
+  if (out) *out = s->eng->last_tuning();
+  if (autotune >= 0) s->eng->set_autotune(autotune != 0);
+  return ALK_OK;
+}
+
 int alk_session_card_mode(alk_session* s, int record, int use) {
   if (!s) return ALK_ERR_ARG;
   return s->eng->card_mode(record != 0, use != 0);

@@ -138,6 +138,7 @@ struct FusedTail {
   uint64_t kernels = 0, d2h = 0, rows = 0;      // statistics of one execution
 };
 struct FusedGraph;
+struct SelectCtx;
 
 // One fused stage as the cardinality estimator sees it: the scan, what it probes, and the
 // key column whose distinct values it counts (the build key, or the probe-aggregate
@@ -160,6 +161,9 @@ class Engine {
   Engine(std::string dir, uint32_t flags);
   ~Engine();
   int execute(const std::string& script);
+  int execute_batch(const std::vector<std::string>& scripts);
+  const alk_gb_tuning& last_tuning() const { return last_tuning_; }
+  void set_autotune(bool on) { autotune_ = on; }
   const std::string& error() const { return err_; }
   cudaStream_t stream() const { return stream_; }
   int preload(const std::string& table);
@@ -209,6 +213,8 @@ class Engine {
   void* pinned(size_t bytes);
 
   void reset_script_state();
+  void begin_script(const std::vector<Statement>& sts, std::map<std::string, size_t>& last);
+  void drop_dead(const std::map<std::string, size_t>& last, size_t i);
   Var* base_table(const std::string& t);
   BaseCol& basecol(Var* base, const std::string& col);
   void read_headers(Var* base, const std::string& col, BaseCol& bc);
@@ -219,6 +225,13 @@ class Engine {
   void exec(Statement& st);
   void emit_filter(Statement& st);
   void emit_select(Statement& st);
+  void select_output(SelectCtx& c);
+  // Dense group-by of a FILTER -> SELECT ... GROUP BY over a base table (small key
+  // domains, conjunctive filter, affine-product aggregates): false when the SELECT has
+  // another form. Batches run many prepared selects in one launch.
+  bool dense_select_prepare(Statement& st, SelectCtx& c);
+  void dense_select_run(const std::vector<SelectCtx*>& cs);
+  void dense_select_finish(SelectCtx& c);
   void emit_join(Statement& st);
   void multijoin(Statement& st, const std::string& s, const std::string& j1, const std::string& j2, unsigned tab);
   void emit_order(Statement& st);
@@ -236,6 +249,10 @@ class Engine {
   std::set<std::string> fused_nograph_;  // queries whose capture failed
   std::string cur_script_;
   bool big_fetch_ = false;  // bring every candidate back (ties beyond the first copy)
+  // batched group-by launch shapes by workload signature (autotuned), and the last used
+  std::map<std::string, alk_gb_tuning> gb_tune_;
+  alk_gb_tuning last_tuning_{};
+  bool autotune_ = true;
 
   // ---- learned cardinality estimator
   bool card_record_ = false, card_use_ = false;

@@ -363,6 +363,29 @@ struct GroupOut {
 };
 }  // namespace
 
+// One SELECT's state between its aggregation and its output columns; for the dense
+// (batched) group-by also the scan and the accumulators.
+struct SelectCtx {
+  Statement* st = nullptr;
+  Var* a = nullptr;
+  int grp_cnt = 0;
+  std::vector<std::string> group_cols;
+  std::vector<OutSpec> outs;
+  std::vector<AggSpec> aggs;
+  size_t cycles = 1;
+  GroupOut G;
+  std::vector<int64_t*> okeys;
+  const Rows* R = nullptr;
+  std::unique_ptr<Var> out;
+  // dense group-by
+  ScanPlan plan;
+  std::vector<alk_colseg> cs;
+  alk_gb_query q{};
+  DevBufP acc;
+  std::vector<uint64_t> seg_rows;
+  std::vector<int64_t> kmin, kspan;
+};
+
 // ------------------------------------------------------------------ FILTER
 // emit_filter (operators.cu:2306-2408): lazy; a filter of a filter appends an AND.
 void Engine::emit_filter(Statement& st) {
@@ -397,6 +420,14 @@ void Engine::emit_filter(Statement& st) {
 // single-segment source, MurmurHash64A order of the group keys for a multi-segment
 // source, merge.cu:118-203) and count_avg / count_simple (merge.cu:271-496).
 void Engine::emit_select(Statement& st) {
+  {
+    SelectCtx c;
+    if (dense_select_prepare(st, c)) {
+      dense_select_run({&c});
+      dense_select_finish(c);
+      return;
+    }
+  }
   Var* a = var(st.f);
   const int grp_cnt = st.grp_cnt;
   std::vector<std::string> group_cols(st.op_value.end() - grp_cnt, st.op_value.end());
@@ -503,6 +534,33 @@ void Engine::emit_select(Statement& st) {
   check(alk_groupby_hash(keys.data(), (uint32_t)keys.size(), vals.data(), kinds.data(), (uint32_t)vals.size(), R.n,
                          okeys.data(), ovals.data(), G.first->as<uint32_t>(), &G.g, (alk_stream)stream_),
         "hash group-by");
+  SelectCtx c;
+  c.st = &st;
+  c.a = a;
+  c.grp_cnt = grp_cnt;
+  c.group_cols = group_cols;
+  c.outs = std::move(outs);
+  c.cycles = cycles;
+  c.G = std::move(G);
+  c.okeys = okeys;
+  c.R = &R;
+  c.out = std::move(out);
+  select_output(c);
+}
+
+// The grouped part of emit_select (select.cu:359-952 and the merge of merge.cu): output
+// order of the groups (key order for one segment, MurmurHash64A order of the key tuple
+// across segments), the output columns, count_simple / count_avg finalisation.
+void Engine::select_output(SelectCtx& c) {
+  Statement& st = *c.st;
+  Var* a = c.a;
+  const int grp_cnt = c.grp_cnt;
+  const std::vector<std::string>& group_cols = c.group_cols;
+  std::vector<OutSpec>& outs = c.outs;
+  const size_t cycles = c.cycles;
+  GroupOut& G = c.G;
+  std::vector<int64_t*>& okeys = c.okeys;
+  std::unique_ptr<Var>& out = c.out;
   const uint64_t ng = G.g;
   // output order
   auto perm = mkbuf(ng * 4, stream_);
@@ -547,6 +605,8 @@ void Engine::emit_select(Statement& st) {
         col = sk[it - group_cols.begin()];
       } else {
         if (grp_cnt && cycles > 1) unsupported("non-key column " + o.field + " in a multi-segment GROUP BY");
+        if (!c.R) unsupported("non-key column " + o.field + " in a dense GROUP BY");
+        const Rows& R = *c.R;
         // value at the group's first row (segreduce gathers at grp offsets after a stable sort)
         auto idx32 = mkbuf(ng * 4, stream_);
         check(alk_narrow_u32(sfirst->as<int64_t>(), ng, idx32->as<uint32_t>(), (alk_stream)stream_), "narrow");
@@ -652,6 +712,303 @@ void Engine::emit_select(Statement& st) {
     out->grp_type[names[c]] = gtypes[c];
   }
   vars_[st.s] = std::move(out);
+}
+
+// ------------------------------------------------------------------ dense group-by
+namespace {
+// An aggregate input as (am * A + ac) * (bm * B + bc) in wrapping int64 arithmetic: the
+// ring identities hold modulo 2^64, so this form equals the expression tree's value
+// whenever the tree uses only +, - and * (no division).
+struct Sym {
+  int kind = 0;  // 0 constant, 1 affine term, 2 product of two affine terms
+  int64_t c = 0;
+  std::string a, b;
+  int64_t am = 0, ac = 0, bm = 0, bc = 0;
+};
+int64_t u_add(int64_t x, int64_t y) { return (int64_t)((uint64_t)x + (uint64_t)y); }
+int64_t u_sub(int64_t x, int64_t y) { return (int64_t)((uint64_t)x - (uint64_t)y); }
+int64_t u_mul(int64_t x, int64_t y) { return (int64_t)((uint64_t)x * (uint64_t)y); }
+bool sym_of(const AstP& e, Sym& out) {
+  if (!e) return false;
+  if (e->k == Ast::Const) {
+    out = Sym{};
+    out.c = e->v;
+    return true;
+  }
+  if (e->k == Ast::Col) {
+    out = Sym{};
+    out.kind = 1;
+    out.a = e->col;
+    out.am = 1;
+    return true;
+  }
+  if (e->k != Ast::Bin) return false;
+  Sym x, y;
+  if (!sym_of(e->l, x) || !sym_of(e->r, y)) return false;
+  out = Sym{};
+  switch (e->op) {
+    case ALK_OP_ADD:
+    case ALK_OP_SUB: {
+      const bool sub = e->op == ALK_OP_SUB;
+      if (x.kind == 0 && y.kind == 0) {
+        out.c = sub ? u_sub(x.c, y.c) : u_add(x.c, y.c);
+        return true;
+      }
+      if (x.kind == 1 && y.kind == 0) {
+        out = x;
+        out.ac = sub ? u_sub(x.ac, y.c) : u_add(x.ac, y.c);
+        return true;
+      }
+      if (x.kind == 0 && y.kind == 1) {
+        out = y;
+        out.am = sub ? u_sub(0, y.am) : y.am;
+        out.ac = sub ? u_sub(x.c, y.ac) : u_add(x.c, y.ac);
+        return true;
+      }
+      if (x.kind == 1 && y.kind == 1 && x.a == y.a) {
+        out = x;
+        out.am = sub ? u_sub(x.am, y.am) : u_add(x.am, y.am);
+        out.ac = sub ? u_sub(x.ac, y.ac) : u_add(x.ac, y.ac);
+        return true;
+      }
+      return false;
+    }
+    case ALK_OP_MUL: {
+      if (x.kind == 0 && y.kind == 0) {
+        out.c = u_mul(x.c, y.c);
+        return true;
+      }
+      if (x.kind == 0) std::swap(x, y);  // constant on the right
+      if (y.kind == 0 && x.kind == 1) {
+        out = x;
+        out.am = u_mul(x.am, y.c);
+        out.ac = u_mul(x.ac, y.c);
+        return true;
+      }
+      if (y.kind == 0 && x.kind == 2) {
+        out = x;
+        out.am = u_mul(x.am, y.c);
+        out.ac = u_mul(x.ac, y.c);
+        return true;
+      }
+      if (x.kind == 1 && y.kind == 1) {
+        out.kind = 2;
+        out.a = x.a;
+        out.am = x.am;
+        out.ac = x.ac;
+        out.b = y.a;
+        out.bm = y.am;
+        out.bc = y.ac;
+        return true;
+      }
+      return false;
+    }
+    default: return false;
+  }
+}
+}  // namespace
+
+bool Engine::dense_select_prepare(Statement& st, SelectCtx& c) {
+  if ((flags_ & ALK_SESSION_PLAIN) || !st.grp_cnt) return false;
+  Var* a = vars_.count(st.f) ? var(st.f) : nullptr;
+  if (!a || (a->kind != Var::Filtered && a->kind != Var::Base)) return false;
+  if (a->kind == Var::Filtered && var(a->source)->kind != Var::Base) return false;
+  c.st = &st;
+  c.a = a;
+  c.grp_cnt = st.grp_cnt;
+  c.group_cols.assign(st.op_value.end() - st.grp_cnt, st.op_value.end());
+  if (c.group_cols.size() > 2) return false;
+  for (auto& g : c.group_cols)
+    if (!a->has(g) || a->meta[g].type > 2) return false;
+  bool one_line = false;
+  compile_select(st, a, true, c.outs, c.aggs, one_line);
+  for (auto& o : c.outs) {
+    if (o.col_type == 1 && std::find(c.group_cols.begin(), c.group_cols.end(), o.field) == c.group_cols.end())
+      return false;
+    if (o.col_type == 2 && has_col(o.vec)) return false;
+  }
+  if (c.aggs.size() > 8) return false;
+  std::vector<Sym> sym(c.aggs.size());
+  for (size_t k = 0; k < c.aggs.size(); k++)
+    if (c.aggs[k].kind != ALK_AGG_COUNT && !sym_of(c.aggs[k].input, sym[k])) return false;
+  c.cycles = cycle_count(a);
+  const uint32_t skipped = stats_.segments_skipped;
+  c.plan = plan_scan(a);
+  auto fail = [&]() {
+    stats_.segments_skipped = skipped;  // the operator plan scans again
+    return false;
+  };
+  if (c.plan.has_pred) {
+    std::vector<CardConj> cj;
+    if (!program_conjuncts(c.plan.pred, cj) || cj.size() > 4) return fail();
+  }
+  Var* src = c.plan.src;
+  alk_gb_query& q = c.q;
+  std::memset(&q, 0, sizeof(q));
+  q.nkeys = (uint32_t)c.group_cols.size();
+  uint64_t nslots = 1;
+  c.kmin.assign(q.nkeys, 0);
+  c.kspan.assign(q.nkeys, 0);
+  for (uint32_t j = 0; j < q.nkeys; j++) {
+    q.key_col[j] = (int32_t)c.plan.slot(c.group_cols[j]);
+    BaseCol& bc = basecol(src, c.group_cols[j]);
+    read_headers(src, c.group_cols[j], bc);
+    int64_t lo = INT64_MAX, hi = INT64_MIN;
+    for (uint32_t g = 0; g < src->segCount; g++) {
+      if (!c.plan.mode[g]) continue;
+      lo = std::min(lo, std::min(bc.segs[g].m.lower, bc.segs[g].m.upper));
+      hi = std::max(hi, std::max(bc.segs[g].m.lower, bc.segs[g].m.upper));
+    }
+    if (hi < lo) lo = hi = 0;  // nothing scanned
+    const uint64_t span = (uint64_t)hi - (uint64_t)lo + 1;
+    if (span == 0 || span > 64) return fail();
+    q.key_min[j] = lo;
+    q.key_max[j] = hi;
+    c.kmin[j] = lo;
+    c.kspan[j] = (int64_t)span;
+    nslots *= span;
+  }
+  q.nagg = (uint32_t)c.aggs.size();
+  if (nslots * (q.nagg + 1) > 64) return fail();
+  for (size_t k = 0; k < c.aggs.size(); k++) {
+    alk_gb_agg& g = q.agg[k];
+    g.kind = c.aggs[k].kind;
+    g.a = q.key_col[0] >= 0 && q.nkeys ? q.key_col[0] : 0;
+    g.b = -1;
+    g.am = 1;
+    if (g.kind == ALK_AGG_COUNT) continue;
+    const Sym& y = sym[k];
+    if (y.kind == 0) {  // a constant input
+      g.am = 0;
+      g.ac = y.c;
+      continue;
+    }
+    g.a = (int32_t)c.plan.slot(y.a);
+    g.am = y.am;
+    g.ac = y.ac;
+    if (y.kind == 2) {
+      g.b = (int32_t)c.plan.slot(y.b);
+      g.bm = y.bm;
+      g.bc = y.bc;
+    }
+  }
+  if (c.plan.slots.size() > 8) return fail();
+  for (auto& n : c.plan.slots)
+    if (src->meta[n].type > 2) return fail();
+  c.cs = colsegs(c.plan);
+  for (auto& d : c.cs)
+    if (d.rows && ((uintptr_t)d.data & 15)) return fail();
+  q.cols = c.cs.data();
+  q.ncols = (uint32_t)c.plan.slots.size();
+  q.nseg = src->segCount;
+  q.seg_mode = c.plan.mode.data();
+  q.pred = c.plan.has_pred ? &c.plan.pred : nullptr;
+  c.acc = mkbuf(nslots * (q.nagg + 1) * 8, stream_);
+  q.d_acc = c.acc->as<int64_t>();
+  c.seg_rows.assign(src->segCount, 0);
+  q.h_seg_rows = c.seg_rows.data();
+  return true;
+}
+
+// One launch for every prepared select. The launch shape (consumer warps, tiles in
+// flight, blocks per SM) is autotuned per workload signature: the first batch of a
+// signature runs under each candidate shape (every run is complete and exact; the last
+// one's results stand) and the fastest shape is kept for later batches.
+void Engine::dense_select_run(const std::vector<SelectCtx*>& cs) {
+  std::vector<alk_gb_query> qs;
+  std::string sig = std::to_string(cs.size());
+  uint64_t rows = 0;
+  for (auto* c : cs) {
+    qs.push_back(c->q);
+    sig += "|" + std::to_string(c->q.ncols) + "," + std::to_string(c->q.nagg) + "," + std::to_string(c->q.nkeys);
+    for (uint32_t k = 0; k < c->q.ncols; k++) sig += ":" + std::to_string(c->cs[(size_t)k * c->q.nseg].bits);
+    for (uint32_t g = 0; g < c->q.nseg; g++)
+      if (c->q.seg_mode[g]) rows += c->cs[g].rows;
+  }
+  auto it = gb_tune_.find(sig);
+  alk_gb_tuning best{};
+  if (it != gb_tune_.end()) {
+    best = it->second;
+  } else if (rows >= (64ull << 20) && autotune_) {
+    // candidates, timed with events around the launch on the engine stream
+    float best_ms = 1e30f;
+    for (uint32_t cw : {8u, 4u})
+      for (uint32_t nst : {2u, 3u, 4u})
+        for (uint32_t bps : {1u, 2u, 3u, 4u}) {
+          alk_gb_tuning t{cw, nst, bps}, used{};
+          cudaEventRecord(ev0_, stream_);
+          int rc = alk_batch_groupby(qs.data(), (uint32_t)qs.size(), &t, &used, (alk_stream)stream_);
+          cudaEventRecord(ev1_, stream_);
+          if (rc == ALK_ERR_UNSUPPORTED) continue;
+          check(rc, "batched group-by");
+          if (used.blocks_per_sm != bps) continue;  // capped by shared memory: a duplicate
+          ck(cudaEventSynchronize(ev1_), "sync");
+          float ms = 0;
+          cudaEventElapsedTime(&ms, ev0_, ev1_);
+          if (ms < best_ms) {
+            best_ms = ms;
+            best = used;
+          }
+        }
+    gb_tune_[sig] = best;
+  }
+  alk_gb_tuning used{};
+  check(alk_batch_groupby(qs.data(), (uint32_t)qs.size(), best.consumer_warps ? &best : nullptr, &used,
+                          (alk_stream)stream_),
+        "batched group-by");
+  last_tuning_ = used;
+}
+
+void Engine::dense_select_finish(SelectCtx& c) {
+  Statement& st = *c.st;
+  auto out = std::make_unique<Var>();
+  out->kind = Var::Mat;
+  out->name = st.s;
+  uint64_t n = 0;
+  for (auto r : c.seg_rows) n += r;
+  if (n == 0) {  // no segment produced rows: empty result without columns
+    vars_[st.s] = std::move(out);
+    return;
+  }
+  // the reference leaves the select-list order reversed when its first segment is empty
+  if (c.seg_rows[0] == 0) std::reverse(c.outs.begin(), c.outs.end());
+  const alk_gb_query& q = c.q;
+  uint64_t nslots = 1;
+  for (uint32_t j = 0; j < q.nkeys; j++) nslots *= (uint64_t)c.kspan[j];
+  const uint32_t nacc = q.nagg + 1;
+  std::vector<int64_t> h(nslots * nacc);
+  ck(cudaMemcpyAsync(h.data(), c.acc->as<void>(), h.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h");
+  ck(cudaStreamSynchronize(stream_), "sync");
+  stats_.d2h_bytes += h.size() * 8;
+  std::vector<std::vector<int64_t>> keys(q.nkeys), vals(q.nagg);
+  for (uint64_t sl = 0; sl < nslots; sl++) {
+    if (h[(size_t)q.nagg * nslots + sl] == 0) continue;  // no row in this slot
+    uint64_t rest = sl;
+    for (int j = (int)q.nkeys - 1; j >= 0; j--) {  // slot = sum (key - min) * stride, last key fastest
+      keys[j].push_back(c.kmin[j] + (int64_t)(rest % (uint64_t)c.kspan[j]));
+      rest /= (uint64_t)c.kspan[j];
+    }
+    for (uint32_t k = 0; k < q.nagg; k++) vals[k].push_back(h[(size_t)k * nslots + sl]);
+  }
+  const uint64_t ng = keys.empty() ? 0 : keys[0].size();
+  GroupOut& G = c.G;
+  G.g = ng;
+  auto upload = [&](const std::vector<int64_t>& v) {
+    auto d = mkbuf(std::max<uint64_t>(v.size(), 1) * 8, stream_);
+    if (!v.empty())
+      ck(cudaMemcpyAsync(d->as<void>(), v.data(), v.size() * 8, cudaMemcpyHostToDevice, stream_), "h2d");
+    stats_.h2d_bytes += v.size() * 8;
+    return d;
+  };
+  for (auto& k : keys) G.keys.push_back(upload(k));
+  for (auto& v : vals) G.vals.push_back(upload(v));
+  G.first = mkbuf(std::max<uint64_t>(ng, 1) * 4, stream_);
+  ck(cudaMemsetAsync(G.first->as<void>(), 0, std::max<uint64_t>(ng, 1) * 4, stream_), "init");
+  for (auto& k : G.keys) c.okeys.push_back(k->as<int64_t>());
+  c.out = std::move(out);
+  stats_.plan = std::max<uint32_t>(stats_.plan, 1);
+  select_output(c);
+  ck(cudaStreamSynchronize(stream_), "sync");  // host vectors above were copy sources
 }
 
 // ------------------------------------------------------------------ JOIN
@@ -908,6 +1265,141 @@ void Engine::reset_script_state() {
   stats_ = alk_stats{};
 }
 
+// Variables of the catalog tables a script names (load_vars, operators.cu:2708-2747) and
+// the last statement that uses every variable (the liveness of the reference's pass one).
+void Engine::begin_script(const std::vector<Statement>& sts, std::map<std::string, size_t>& last) {
+  std::set<std::string> names;
+  for (auto& st : sts) {
+    names.insert(st.s);
+    names.insert(st.f);
+    for (auto& j : st.op_join) names.insert(j);
+  }
+  for (auto& n : names) {
+    Var* b = base_table(n);
+    if (b) vars_[n] = std::make_unique<Var>(*b);
+  }
+  for (size_t i = 0; i < sts.size(); i++) {
+    auto& st = sts[i];
+    last[st.s] = std::max(last[st.s], i);
+    if (!st.f.empty() && st.kind != StmtKind::Store) last[st.f] = i;
+    for (auto& j : st.op_join) last[j] = i;
+  }
+}
+
+void Engine::drop_dead(const std::map<std::string, size_t>& last, size_t i) {
+  for (auto it = vars_.begin(); it != vars_.end();) {
+    auto l = last.find(it->first);
+    if (it->second->kind == Var::Mat && (l == last.end() || l->second <= i)) it = vars_.erase(it);
+    else ++it;
+  }
+}
+
+// Many scripts with one launch for their group-bys: each script runs up to its first
+// SELECT that the dense group-by takes, every such SELECT then runs in one batched
+// launch, and each script continues from there. Scripts without one run as usual.
+int Engine::execute_batch(const std::vector<std::string>& scripts) {
+  struct Run {
+    std::vector<Statement> sts;
+    std::map<std::string, size_t> last;
+    std::map<std::string, std::unique_ptr<Var>> vars;
+    std::string text;
+    size_t i = 0;
+    bool pending = false;
+    SelectCtx c;
+    int rc = ALK_OK;
+    std::string err;
+  };
+  err_.clear();
+  stats_ = alk_stats{};
+  const uint64_t k0 = g_kernel_launches;
+  std::vector<std::unique_ptr<Run>> runs;
+  auto fail = [&](Run& r, int rc, const std::string& m) {
+    r.rc = rc;
+    r.err = m;
+    r.pending = false;
+    cudaStreamSynchronize(stream_);
+  };
+  // phase 1: every script up to its dense group-by
+  for (auto& text : scripts) {
+    runs.push_back(std::make_unique<Run>());
+    Run& r = *runs.back();
+    r.text = text;
+    std::string perr;
+    if (!parse_script(text, r.sts, perr)) {
+      fail(r, ALK_ERR_PARSE, "parse: " + perr);
+      continue;
+    }
+    vars_.clear();
+    cur_script_ = text;
+    try {
+      begin_script(r.sts, r.last);
+      for (; r.i < r.sts.size(); r.i++) {
+        if (r.sts[r.i].kind == StmtKind::Select && dense_select_prepare(r.sts[r.i], r.c)) {
+          r.pending = true;
+          break;
+        }
+        if (!(flags_ & ALK_SESSION_PLAIN) && try_fused(r.sts, r.i)) continue;
+        exec(r.sts[r.i]);
+        drop_dead(r.last, r.i);
+      }
+    } catch (const EngineError& e) {
+      fail(r, e.code, e.what());
+    } catch (const std::exception& e) {
+      fail(r, ALK_ERR_ARG, e.what());
+    }
+    r.vars = std::move(vars_);
+    vars_.clear();
+  }
+  // phase 2: one launch
+  std::vector<SelectCtx*> batch;
+  for (auto& r : runs)
+    if (r->pending) batch.push_back(&r->c);
+  if (!batch.empty()) {
+    try {
+      dense_select_run(batch);
+    } catch (const EngineError& e) {
+      for (auto& r : runs)
+        if (r->pending) fail(*r, e.code, e.what());
+    }
+  }
+  // phase 3: the rest of every script that waited
+  for (auto& rp : runs) {
+    Run& r = *rp;
+    if (!r.pending) continue;
+    vars_ = std::move(r.vars);
+    cur_script_ = r.text;
+    try {
+      dense_select_finish(r.c);
+      drop_dead(r.last, r.i);
+      for (r.i++; r.i < r.sts.size(); r.i++) {
+        if (!(flags_ & ALK_SESSION_PLAIN) && try_fused(r.sts, r.i)) continue;
+        exec(r.sts[r.i]);
+        drop_dead(r.last, r.i);
+      }
+      ck(cudaStreamSynchronize(stream_), "script");
+    } catch (const EngineError& e) {
+      fail(r, e.code, e.what());
+    } catch (const std::exception& e) {
+      fail(r, ALK_ERR_ARG, e.what());
+    }
+    vars_.clear();
+  }
+  int rc = ALK_OK;
+  for (size_t k = 0; k < runs.size(); k++)
+    if (runs[k]->rc != ALK_OK && rc == ALK_OK) {
+      rc = runs[k]->rc;
+      err_ = "script " + std::to_string(k) + ": " + runs[k]->err;
+    }
+  if (!(flags_ & ALK_SESSION_RESIDENT)) {
+    for (auto& t : basecols_)
+      for (auto& c : t.second)
+        for (auto& d : c.second.dev) d.reset();
+  }
+  cudaStreamSynchronize(stream_);
+  stats_.kernels = g_kernel_launches - k0;
+  return rc;
+}
+
 int Engine::execute(const std::string& script) {
   std::vector<Statement> sts;
   std::string perr;
@@ -921,33 +1413,12 @@ int Engine::execute(const std::string& script) {
   uint64_t k0 = g_kernel_launches;
   int rc = ALK_OK;
   try {
-    // tables named anywhere in the script (load_vars, operators.cu:2708-2747)
-    std::set<std::string> names;
-    for (auto& st : sts) {
-      names.insert(st.s);
-      names.insert(st.f);
-      for (auto& j : st.op_join) names.insert(j);
-    }
-    for (auto& n : names) {
-      Var* b = base_table(n);
-      if (b) vars_[n] = std::make_unique<Var>(*b);
-    }
-    // last use of every variable (the mystat liveness of pass one)
     std::map<std::string, size_t> last;
-    for (size_t i = 0; i < sts.size(); i++) {
-      auto& st = sts[i];
-      last[st.s] = std::max(last[st.s], i);
-      if (!st.f.empty() && st.kind != StmtKind::Store) last[st.f] = i;
-      for (auto& j : st.op_join) last[j] = i;
-    }
+    begin_script(sts, last);
     for (size_t i = 0; i < sts.size(); i++) {
       if (!(flags_ & ALK_SESSION_PLAIN) && try_fused(sts, i)) continue;
       exec(sts[i]);
-      for (auto it = vars_.begin(); it != vars_.end();) {
-        auto l = last.find(it->first);
-        if (it->second->kind == Var::Mat && (l == last.end() || l->second <= i)) it = vars_.erase(it);
-        else ++it;
-      }
+      drop_dead(last, i);
     }
     ck(cudaStreamSynchronize(stream_), "script");
   } catch (const EngineError& e) {

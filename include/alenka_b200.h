@@ -354,6 +354,53 @@ int alk_gen_three_way(const char* dir, uint64_t customers, uint64_t orders, uint
 /* A yyyymmdd date value moved by a number of days (proleptic Gregorian). */
 int64_t alk_date_add_days(int64_t yyyymmdd_value, int64_t days);
 
+/* ------------------------------------------ batched filter + group-by
+ * Many queries of the single-table shape FILTER t BY <conjunction> -> SELECT keys,
+ * aggregates FROM it GROUP BY keys (each of which the reference runs as emit_filter +
+ * emit_select, operators.cu:2306 and :1801) in one persistent launch over a work list of
+ * (query, segment) items. Group keys are at most two columns whose value ranges (from the
+ * zone maps) give a dense slot space; every aggregate input is a product of two affine
+ * column terms, value = (am * A + ac) * (bm * B + bc) in wrapping int64 arithmetic (b < 0:
+ * the second factor is 1), which covers columns and the decimal forms such as
+ * price * (1 - discount). */
+typedef struct alk_gb_agg {
+  int64_t am, ac, bm, bc;
+  int32_t a, b;   /* query column indexes (b < 0: no second factor) */
+  uint32_t kind;  /* ALK_AGG_SUM / COUNT / MIN / MAX */
+  uint32_t pad;
+} alk_gb_agg;
+typedef struct alk_gb_query {
+  const alk_colseg* cols;  /* [ncols][nseg]; 16-byte aligned, readable to the next 16 bytes */
+  uint32_t ncols, nseg;    /* ncols <= 8 */
+  const uint8_t* seg_mode; /* per segment: 0 skip, 1 every row passes, 2 evaluate (NULL: 2) */
+  const alk_program* pred; /* a conjunction of column comparisons, or NULL */
+  uint32_t nkeys;          /* 0..2 */
+  int32_t key_col[2];
+  int64_t key_min[2], key_max[2]; /* key value ranges; slots = product of the spans */
+  uint32_t nagg;                  /* <= 8 */
+  alk_gb_agg agg[8];
+  int64_t* d_acc;       /* device [nagg + 1][slots]: the aggregates, then the row count */
+  uint64_t* h_seg_rows; /* optional host [nseg]: rows passing the filter per segment */
+} alk_gb_query;
+/* Launch shape: consumer warps per block (4 or 8; a tile is 256 rows per warp), tiles in
+ * flight per block (2..4), blocks per SM (capped by shared memory); 0 = default. */
+typedef struct alk_gb_tuning {
+  uint32_t consumer_warps, stages, blocks_per_sm;
+} alk_gb_tuning;
+/* Runs the queries (accumulators initialised here) and synchronizes the stream. slots *
+ * (nagg + 1) <= 64 per query (accumulators private to each thread); a larger slot space or
+ * a filter that is not a conjunction returns ALK_ERR_UNSUPPORTED. *used = the shape run. */
+int alk_batch_groupby(const alk_gb_query* queries, uint32_t nq, const alk_gb_tuning* tune, alk_gb_tuning* used,
+                      alk_stream stream);
+/* Runs n scripts with one batched launch for their group-bys: every script runs up to
+ * its first SELECT ... GROUP BY of the dense form, those run together, then every script
+ * continues. Results are those of running the scripts one at a time. Returns the first
+ * failing script's status (alk_session_error names it); the others still run. */
+int alk_session_execute_batch(alk_session* s, const char* const* scripts, uint32_t n);
+/* *out = the launch shape of the last batched group-by; autotune 0/1 turns the per-
+ * workload autotuner off/on (-1 leaves it). */
+int alk_session_tuning(alk_session* s, alk_gb_tuning* out, int autotune);
+
 /* ------------------------------------------ 4. learned cardinality estimator
  * No counterpart in the reference, which sizes every buffer from the free device memory
  * (getFreeMem, cm.cu:3184) and the rows scanned. A small MLP, 64 -> 128 -> 128 -> 3 with
