@@ -93,6 +93,9 @@ def _declare(L):
     L.alk_card_count.argtypes = [vp, u32, u32, vp, vp, vp, i32, i32, i64, i64, c.POINTER(u64), vp]
     L.alk_session_execute_batch.argtypes = [vp, c.POINTER(c.c_char_p), u32]
     L.alk_session_tuning.argtypes = [vp, c.POINTER(Tuning), i32]
+    L.alk_session_gen_flat_resident.argtypes = [vp, c.c_char_p, c.POINTER(u32), u32, u64, u64]
+    L.alk_gen_flat_value.argtypes = [u64, i32, u64]
+    L.alk_gen_flat_value.restype = i64
     L.alk_session_card_mode.argtypes = [vp, i32, i32]
     L.alk_session_card_records.argtypes = [vp, fp, fp, fp, u64, c.POINTER(u64)]
     L.alk_session_card_train.argtypes = [vp, u64, u64, u32, u32, c.c_float, u64, fp]
@@ -151,6 +154,13 @@ class Session:
         """Runs the scripts with one batched launch for their dense group-bys."""
         arr = (ctypes.c_char_p * len(scripts))(*[x.encode() for x in scripts])
         rc = lib().alk_session_execute_batch(self._h, arr, len(scripts))
+        if rc != ALK_OK:
+            raise AlenkaError(rc, lib().alk_session_error(self._h).decode())
+
+    def gen_flat_resident(self, table, seg_rows, seed, row_base=0):
+        """Generate a lineitem-shaped table in device memory (segments of seg_rows rows)."""
+        arr = (ctypes.c_uint32 * len(seg_rows))(*seg_rows)
+        rc = lib().alk_session_gen_flat_resident(self._h, table.encode(), arr, len(seg_rows), seed, row_base)
         if rc != ALK_OK:
             raise AlenkaError(rc, lib().alk_session_error(self._h).decode())
 

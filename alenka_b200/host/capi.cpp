@@ -80,6 +80,14 @@ int alk_session_execute_batch(alk_session* s, const char* const* scripts, uint32
   return rc;
 }
 
+int alk_session_gen_flat_resident(alk_session* s, const char* table, const uint32_t* seg_rows, uint32_t nseg,
+                                  uint64_t seed, uint64_t row_base) {
+  if (!s || !table || !seg_rows || nseg == 0) return ALK_ERR_ARG;
+  int rc = s->eng->gen_resident_flat(table, std::vector<uint32_t>(seg_rows, seg_rows + nseg), seed, row_base);
+  s->err = s->eng->error();
+  return rc;
+}
+
 int alk_session_tuning(alk_session* s, alk_gb_tuning* out, int autotune) {
   if (!s) return ALK_ERR_ARG;
   if (out) *out = s->eng->last_tuning();

@@ -69,6 +69,7 @@ struct BaseCol {
   std::vector<size_t> host_len;
   std::vector<DevBufP> dev;           // device payload (FOR) or expanded int64 (delta)
   bool headers_read = false;
+  bool device_only = false;  // generated in device memory: no files, never released
   // char dictionaries
   std::vector<std::string> dict;
   std::unordered_map<uint64_t, int64_t> hash_to_code;
@@ -162,6 +163,9 @@ class Engine {
   ~Engine();
   int execute(const std::string& script);
   int execute_batch(const std::vector<std::string>& scripts);
+  // A lineitem-shaped table generated in device memory (segments of the given sizes).
+  int gen_resident_flat(const std::string& table, const std::vector<uint32_t>& seg_rows, uint64_t seed,
+                        uint64_t row_base);
   const alk_gb_tuning& last_tuning() const { return last_tuning_; }
   void set_autotune(bool on) { autotune_ = on; }
   const std::string& error() const { return err_; }

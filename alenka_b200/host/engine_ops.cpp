@@ -1393,7 +1393,8 @@ int Engine::execute_batch(const std::vector<std::string>& scripts) {
   if (!(flags_ & ALK_SESSION_RESIDENT)) {
     for (auto& t : basecols_)
       for (auto& c : t.second)
-        for (auto& d : c.second.dev) d.reset();
+        if (!c.second.device_only)
+          for (auto& d : c.second.dev) d.reset();
   }
   cudaStreamSynchronize(stream_);
   stats_.kernels = g_kernel_launches - k0;
@@ -1434,7 +1435,8 @@ int Engine::execute(const std::string& script) {
   if (!(flags_ & ALK_SESSION_RESIDENT)) {
     for (auto& t : basecols_)
       for (auto& c : t.second)
-        for (auto& d : c.second.dev) d.reset();
+        if (!c.second.device_only)
+          for (auto& d : c.second.dev) d.reset();
   }
   cudaStreamSynchronize(stream_);
   stats_.kernels = g_kernel_launches - k0;

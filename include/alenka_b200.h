@@ -351,6 +351,23 @@ int alk_gen_lineitem_flat(const char* dir, uint64_t rows, uint32_t seg_rows, uin
                           char* err, int err_len);
 int alk_gen_three_way(const char* dir, uint64_t customers, uint64_t orders, uint64_t lineitems,
                       uint32_t seg_rows, uint64_t seed, int delta, char* err, int err_len);
+/* The single-table lineitem shape generated in device memory, segment by segment, as a
+ * function of (seed, column, row_base + row): l_orderkey (4 rows per key), l_quantity
+ * U[1,50], l_extendedprice U[90000,10500000], l_discount U[0,10], l_shipdate uniform
+ * over 1992-01-02..1998-12-01, l_returnflag codes of {A,N,R}, l_linestatus codes of
+ * {F,O}. minmax: per segment and column (7) the [min, max] pair; write: the stored
+ * values into cols [7][nseg] (data, lower = the minimum, bits set by the caller). */
+int alk_gen_flat_minmax(uint64_t seed, uint64_t row_base, const uint32_t* seg_rows, uint32_t nseg, int64_t* h_minmax,
+                        alk_stream stream);
+int alk_gen_flat_write(uint64_t seed, uint64_t row_base, const uint32_t* seg_rows, uint32_t nseg,
+                       const alk_colseg* cols, alk_stream stream);
+/* One generated value (host side, for checks). */
+int64_t alk_gen_flat_value(uint64_t seed, int col, uint64_t row);
+/* Registers such a table in the session's catalog with every segment resident (no
+ * files; exact per-segment zone maps; the file encoder's widths). */
+int alk_session_gen_flat_resident(alk_session* s, const char* table, const uint32_t* seg_rows, uint32_t nseg,
+                                  uint64_t seed, uint64_t row_base);
+
 /* A yyyymmdd date value moved by a number of days (proleptic Gregorian). */
 int64_t alk_date_add_days(int64_t yyyymmdd_value, int64_t days);
 

@@ -117,3 +117,57 @@ def test_batch_tuning_reported(flats):
         s.execute_batch([wl.flat_script(i, out=f"t{i}.txt") for i in range(4)])
         cw, stages, bps = s.tuning()
         assert cw in (4, 8) and 2 <= stages <= 4 and bps >= 1
+
+
+# ------------------------------------------------------- tables generated on the device
+
+def _np_gen(seed, col, rows):
+    """numpy restatement of the device generator (splitmix64 of seed, column, row)."""
+    import numpy as np
+    with np.errstate(over="ignore"):
+        r = rows.astype(np.uint64)
+        x = (np.uint64(seed) * np.uint64(0x100000001b3) + np.uint64(col) * np.uint64(0x9e3779b97f4a7c15)
+             + r * np.uint64(0xd1b54a32d192ed03))
+        z = x + np.uint64(0x9e3779b97f4a7c15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xbf58476d1ce4e5b9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94d049bb133111eb)
+        h = z ^ (z >> np.uint64(31))
+    if col == 1:
+        return 1 + (h % np.uint64(50)).astype(np.int64)
+    if col == 4:
+        days = 8036 + (h % np.uint64(10561 - 8036 + 1)).astype(np.int64)
+        return np.array([int(str(np.datetime64("1970-01-01") + np.timedelta64(int(d), "D")).replace("-", ""))
+                         for d in days])
+    if col == 5:
+        return (h % np.uint64(3)).astype(np.int64)
+    raise ValueError(col)
+
+
+def test_device_generated_table_values_and_groupby():
+    import tempfile
+    import numpy as np
+    segs = [100_000, 37, 250_001]
+    n = sum(segs)
+    rows = np.arange(n)
+    qty, ship, flag = _np_gen(9, 1, rows), _np_gen(9, 4, rows), _np_gen(9, 5, rows)
+    assert all(ab.lib().alk_gen_flat_value(9, c, 12345) == int(v[12345]) for c, v in ((1, qty), (4, ship), (5, flag)))
+    cut = 19950617
+    script = ("LF := FILTER gl BY l_shipdate < %d;\n"
+              "R := SELECT l_returnflag AS f, SUM(l_quantity) AS q, COUNT(l_orderkey) AS c FROM LF "
+              "GROUP BY l_returnflag;\nSTORE R INTO 'gr.txt' USING ('|');\n" % cut)
+    outs = {}
+    with tempfile.TemporaryDirectory() as d:
+        for plain in (True, False):
+            with ab.Session(d, plain=plain) as s:
+                s.gen_flat_resident("gl", segs, 9)
+                s.execute(script)
+                assert s.stats().plan == (0 if plain else 1)
+                outs[plain] = open(os.path.join(d, "gr.txt"), "rb").read()
+    assert outs[True] == outs[False]
+    got = {}
+    for line in outs[True].decode().splitlines():
+        f, q, c = line.split("|")[:3]
+        got[f] = (int(q), int(c))
+    m = ship < cut
+    want = {k: (int(qty[m & (flag == i)].sum()), int((m & (flag == i)).sum())) for i, k in enumerate("ANR")}
+    assert got == want
