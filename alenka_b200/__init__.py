@@ -42,6 +42,7 @@ class Stats(ctypes.Structure):
         ("reserved_bytes", ctypes.c_uint64),
         ("card_estimates", ctypes.c_uint32),
         ("card_reruns", ctypes.c_uint32),
+        ("batch_host_ms", ctypes.c_double * 3),
     ]
 
 
@@ -93,6 +94,7 @@ def _declare(L):
     L.alk_card_count.argtypes = [vp, u32, u32, vp, vp, vp, i32, i32, i64, i64, c.POINTER(u64), vp]
     L.alk_session_execute_batch.argtypes = [vp, c.POINTER(c.c_char_p), u32]
     L.alk_session_tuning.argtypes = [vp, c.POINTER(Tuning), i32]
+    L.alk_session_set_plain.argtypes = [vp, i32]
     L.alk_session_gen_flat_resident.argtypes = [vp, c.c_char_p, c.POINTER(u32), u32, u64, u64]
     L.alk_gen_flat_value.argtypes = [u64, i32, u64]
     L.alk_gen_flat_value.restype = i64
@@ -163,6 +165,9 @@ class Session:
         rc = lib().alk_session_gen_flat_resident(self._h, table.encode(), arr, len(seg_rows), seed, row_base)
         if rc != ALK_OK:
             raise AlenkaError(rc, lib().alk_session_error(self._h).decode())
+
+    def set_plain(self, on):
+        lib().alk_session_set_plain(self._h, 1 if on else 0)
 
     def tuning(self, autotune=None):
         """Launch shape of the last batched group-by; autotune True/False switches the

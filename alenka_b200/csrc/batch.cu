@@ -58,15 +58,6 @@ __device__ __forceinline__ uint32_t find_item(const uint32_t* item_tile, uint32_
   return lo;
 }
 
-__device__ __forceinline__ int64_t stored_at(const unsigned char* p, uint32_t bits, uint32_t r) {
-  switch (bits) {
-    case 8: return p[r];
-    case 16: return ((const uint16_t*)p)[r];
-    case 32: return ((const uint32_t*)p)[r];
-    default: return ((const int64_t*)p)[r];
-  }
-}
-
 // A warp folds its lanes' private accumulators (slot-major, [acc][lane]) into the
 // query's global accumulators and clears them.
 __device__ void gb_flush(const GbQuery& q, int64_t* priv, uint32_t lane) {
@@ -103,7 +94,9 @@ __device__ __forceinline__ void gb_clear(const GbQuery& q, int64_t* priv, uint32
 __global__ void k_gb_tma(const __grid_constant__ GbArgs g) {
   extern __shared__ __align__(128) unsigned char s_dyn[];
   __shared__ __align__(8) uint64_t s_full[kGbMaxStages], s_empty[kGbMaxStages];
-  __shared__ uint32_t s_item[kGbMaxStages];
+  __shared__ uint32_t s_item[kGbMaxStages];           // item of the tile in each stage
+  __shared__ uint32_t s_rows[kGbMaxStages];           // its rows
+  __shared__ uint32_t s_coff[kGbMaxStages][kGbCols];  // its staged column offsets
   __shared__ int s_abort;
   const uint32_t nst = g.nst, cw = g.cw;
   const uint32_t tile_rows = cw * 32 * kItems;
@@ -126,6 +119,26 @@ __global__ void k_gb_tma(const __grid_constant__ GbArgs g) {
     // ---- producer: one thread issues the bulk copies
     if (lane != 0) return;
     uint32_t issued = 0;
+    // the block's tiles are contiguous: the item is found once and then advanced, with
+    // its copy sources kept in registers; each stage carries the tile's item, rows and
+    // column offsets for the consumers
+    uint32_t i = t0 < t1 ? find_item(g.item_tile, g.nitems, t0) : 0;
+    uint32_t first = 0, next = 0, irows = 0, ncols = 0;
+    const unsigned char* src[kGbCols];
+    uint32_t width[kGbCols];
+    auto load_item = [&]() {
+      first = __ldg(g.item_tile + i);
+      next = __ldg(g.item_tile + i + 1);
+      const GbItem& item = g.items[i];
+      irows = item.rows;
+      ncols = g.queries[item.query].ncols;
+#pragma unroll
+      for (int c = 0; c < kGbCols; c++) {
+        src[c] = c < (int)ncols ? (const unsigned char*)item.col[c].data : nullptr;
+        width[c] = c < (int)ncols ? item.col[c].bits / 8 : 0;
+      }
+    };
+    if (t0 < t1) load_item();
     for (uint32_t it = 0; t0 + it < t1; it++) {
       if (*abort_flag) break;
       const uint32_t tile = t0 + it, st = it % nst;
@@ -134,21 +147,27 @@ __global__ void k_gb_tma(const __grid_constant__ GbArgs g) {
         *abort_flag = 1;
         break;
       }
-      const uint32_t i = find_item(g.item_tile, g.nitems, tile);
-      const GbItem& item = g.items[i];
-      const GbQuery& q = g.queries[item.query];
-      const uint32_t row0 = (tile - __ldg(g.item_tile + i)) * tile_rows;
-      const uint32_t rows = min(tile_rows, item.rows - row0);
+      while (tile >= next && i + 1 < g.nitems) {
+        i++;
+        load_item();
+      }
+      const uint32_t row0 = (tile - first) * tile_rows;
+      const uint32_t rows = min(tile_rows, irows - row0);
       s_item[st] = i;
+      s_rows[st] = rows;
       uint32_t total = 0;
-      for (uint32_t c = 0; c < q.ncols; c++) total += (rows * (item.col[c].bits / 8) + 15) & ~15u;
+#pragma unroll
+      for (int c = 0; c < kGbCols; c++) {
+        s_coff[st][c] = total;
+        total += (rows * width[c] + 15) & ~15u;
+      }
       unsigned char* buf = s_dyn + (size_t)st * g.stage_bytes;
       mbar_expect_tx(&s_full[st], total);
-      uint32_t off = 0;
-      for (uint32_t c = 0; c < q.ncols; c++) {
-        const uint32_t w = item.col[c].bits / 8, n = (rows * w + 15) & ~15u;
-        bulk_g2s(buf + off, (const unsigned char*)item.col[c].data + (uint64_t)row0 * w, n, &s_full[st]);
-        off += n;
+#pragma unroll
+      for (int c = 0; c < kGbCols; c++) {
+        if (c >= (int)ncols) break;
+        const uint32_t n = (rows * width[c] + 15) & ~15u;
+        bulk_g2s(buf + s_coff[st][c], src[c] + (uint64_t)row0 * width[c], n, &s_full[st]);
       }
       issued = it + 1;
     }
@@ -194,19 +213,9 @@ __global__ void k_gb_tma(const __grid_constant__ GbArgs g) {
         cur_q = qi;
       }
     }
-    const uint32_t row0 = (it + t0 - __ldg(g.item_tile + i)) * tile_rows;
-    const uint32_t rows = min(tile_rows, item.rows - row0);
+    const uint32_t rows = s_rows[st];
     const unsigned char* buf = s_dyn + (size_t)st * g.stage_bytes;
-    // staged column offsets of this tile
-    uint32_t coff[kGbCols];
-    {
-      uint32_t off = 0;
-#pragma unroll
-      for (int c = 0; c < kGbCols; c++) {
-        coff[c] = off;
-        if (c < (int)q.ncols) off += (rows * (item.col[c].bits / 8) + 15) & ~15u;
-      }
-    }
+    const uint32_t* coff = s_coff[st];  // staged column offsets of this tile
     uint32_t live = 0;
 #pragma unroll
     for (int k = 0; k < kItems; k++)
@@ -227,42 +236,80 @@ __global__ void k_gb_tma(const __grid_constant__ GbArgs g) {
       }
     }
     surv += __reduce_add_sync(0xffffffffu, (unsigned)__popc(live));
-    // fold the survivors
-    for (uint32_t m = live; m; m &= m - 1) {
-      const uint32_t r = r0 + (__ffs(m) - 1) * 32;
-      uint64_t slot = 0;
-      bool ok = true;
+    // fold the survivors a column at a time over the thread's 8 rows: the group slot in
+    // 32-bit arithmetic (stored key + (segment base - key minimum), each below its span),
+    // then every aggregate input into the slot's accumulators, private to the lane
+    if (live) {
+      uint32_t slot[kItems];
+#pragma unroll
+      for (int k = 0; k < kItems; k++) slot[k] = 0;
       for (uint32_t j = 0; j < q.nkeys; j++) {
         const alk_colseg& d = item.col[q.key_col[j]];
-        const uint64_t o = (uint64_t)(stored_at(buf + coff[q.key_col[j]], d.bits, r) + d.lower) - (uint64_t)q.key_min[j];
-        ok = ok && o < q.key_span[j];
-        slot += o * q.key_mul[j];
+        const uint32_t kd = (uint32_t)((uint64_t)d.lower - (uint64_t)q.key_min[j]);
+        const uint32_t span = (uint32_t)q.key_span[j], mul = (uint32_t)q.key_mul[j];
+        uint32_t x[kItems];
+        if (d.bits > 32) {  // the low word suffices: the offset from the minimum is below the span
+          uint64_t w[kItems];
+          load_raw<false, 32>(buf + coff[q.key_col[j]], d.bits, r0, live, w);
+#pragma unroll
+          for (int k = 0; k < kItems; k++) x[k] = (uint32_t)w[k];
+        } else {
+          load_raw32<32>(buf + coff[q.key_col[j]], d.bits, r0, x);
+        }
+#pragma unroll
+        for (int k = 0; k < kItems; k++) {
+          const uint32_t o = x[k] + kd;
+          if (o >= span && ((live >> k) & 1)) {  // outside the zone maps' range: the plan is wrong
+            atomicExch(g.err, ALK_ERR_ARG);
+            live &= ~(1u << k);
+          }
+          slot[k] += o * mul;
+        }
       }
-      if (!ok) {  // a key outside the range the zone maps gave: the plan is wrong
-        atomicExch(g.err, ALK_ERR_ARG);
-        continue;
-      }
-      int64_t* p = priv + (size_t)slot * q.nacc * 32 + lane;
-      for (uint32_t a = 0; a < q.nagg; a++) {
-        const alk_gb_agg& ag = q.agg[a];
-        if (ag.kind == ALK_AGG_COUNT) {
-          p[a * 32] += 1;
+      const uint32_t nagg = q.nagg, stride = q.nacc * 32;
+      int64_t* base = priv + lane;
+      for (uint32_t a = 0; a < nagg; a++) {
+        const uint32_t kind = q.agg[a].kind;
+        int64_t* pa = base + a * 32;
+        if (kind == ALK_AGG_COUNT) {
+#pragma unroll
+          for (int k = 0; k < kItems; k++)
+            if ((live >> k) & 1) pa[slot[k] * stride] += 1;
           continue;
         }
-        const alk_colseg& da = item.col[ag.a];
-        int64_t v = stored_at(buf + coff[ag.a], da.bits, r) + da.lower;
-        if (ag.am != 1 || ag.ac != 0) v = (int64_t)((uint64_t)v * (uint64_t)ag.am + (uint64_t)ag.ac);
-        if (ag.b >= 0) {
-          const alk_colseg& db = item.col[ag.b];
-          const int64_t w = stored_at(buf + coff[ag.b], db.bits, r) + db.lower;
-          v = (int64_t)((uint64_t)v * ((uint64_t)w * (uint64_t)ag.bm + (uint64_t)ag.bc));
+        const int32_t ca = q.agg[a].a, cb = q.agg[a].b;
+        const uint64_t am = (uint64_t)q.agg[a].am, ac = (uint64_t)q.agg[a].ac;
+        const uint64_t la = (uint64_t)item.col[ca].lower;
+        uint64_t v[kItems];
+        load_raw<false, 32>(buf + coff[ca], item.col[ca].bits, r0, live, v);
+        if (am == 1 && ac == 0) {
+#pragma unroll
+          for (int k = 0; k < kItems; k++) v[k] += la;
+        } else {
+#pragma unroll
+          for (int k = 0; k < kItems; k++) v[k] = (v[k] + la) * am + ac;
         }
-        int64_t& acc = p[a * 32];
-        if (ag.kind == ALK_AGG_MIN) acc = min(acc, v);
-        else if (ag.kind == ALK_AGG_MAX) acc = max(acc, v);
-        else acc = (int64_t)((uint64_t)acc + (uint64_t)v);
+        if (cb >= 0) {
+          const uint64_t bm = (uint64_t)q.agg[a].bm, bc = (uint64_t)q.agg[a].bc;
+          const uint64_t lb = (uint64_t)item.col[cb].lower;
+          uint64_t w[kItems];
+          load_raw<false, 32>(buf + coff[cb], item.col[cb].bits, r0, live, w);
+#pragma unroll
+          for (int k = 0; k < kItems; k++) v[k] *= (w[k] + lb) * bm + bc;
+        }
+#pragma unroll
+        for (int k = 0; k < kItems; k++) {
+          if (!((live >> k) & 1)) continue;
+          int64_t& acc = pa[slot[k] * stride];
+          if (kind == ALK_AGG_MIN) acc = min(acc, (int64_t)v[k]);
+          else if (kind == ALK_AGG_MAX) acc = max(acc, (int64_t)v[k]);
+          else acc = (int64_t)((uint64_t)acc + v[k]);
+        }
       }
-      p[q.nagg * 32] += 1;
+      int64_t* pc = base + nagg * 32;
+#pragma unroll
+      for (int k = 0; k < kItems; k++)
+        if ((live >> k) & 1) pc[slot[k] * stride] += 1;
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&s_empty[st]);
@@ -300,7 +347,7 @@ int sms_count() {
 extern "C" {
 
 int alk_batch_groupby(const alk_gb_query* qs, uint32_t nq, const alk_gb_tuning* tune, alk_gb_tuning* used,
-                      alk_stream stream) {
+                      alk_event_timer* timer, alk_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (!qs || nq == 0) return ALK_ERR_ARG;
   std::vector<GbQuery> hq(nq);
@@ -440,7 +487,9 @@ int alk_batch_groupby(const alk_gb_query* qs, uint32_t nq, const alk_gb_tuning* 
     }
     const uint32_t per_sm = tune && tune->blocks_per_sm ? std::min<uint32_t>(tune->blocks_per_sm, occ) : occ;
     const uint32_t grid = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)sms_count() * per_sm);
+    if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev0, s);
     k_gb_tma<<<grid, (cw + 1) * 32, smem, s>>>(g);
+    if (timer && timer->on) cudaEventRecord((cudaEvent_t)timer->ev1, s);
     alk::g_kernel_launches++;
     CK(cudaGetLastError());
     if (used) {
@@ -459,6 +508,12 @@ int alk_batch_groupby(const alk_gb_query* qs, uint32_t nq, const alk_gb_tuning* 
     if (qs[qi].h_seg_rows) std::fill(qs[qi].h_seg_rows, qs[qi].h_seg_rows + qs[qi].nseg, 0);
   for (uint32_t i = 0; i < nitems; i++)
     if (qs[item_src[i].first].h_seg_rows) qs[item_src[i].first].h_seg_rows[item_src[i].second] = irows[i];
+  if (timer && timer->on && ntiles) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, (cudaEvent_t)timer->ev0, (cudaEvent_t)timer->ev1);
+    timer->ms += ms;
+    timer->launches++;
+  }
   if (herr) rc = herr;
   return rc;
 }

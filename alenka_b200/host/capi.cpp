@@ -88,6 +88,12 @@ int alk_session_gen_flat_resident(alk_session* s, const char* table, const uint3
   return rc;
 }
 
+int alk_session_set_plain(alk_session* s, int on) {
+  if (!s) return ALK_ERR_ARG;
+  s->eng->set_plain(on != 0);
+  return ALK_OK;
+}
+
 int alk_session_tuning(alk_session* s, alk_gb_tuning* out, int autotune) {
   if (!s) return ALK_ERR_ARG;
   if (out) *out = s->eng->last_tuning();

@@ -731,8 +731,18 @@ Rows Engine::materialize(Var* v, const std::vector<std::string>& fields, bool wa
   Rows r;
   if (v->kind == Var::Mat) {
     r.n = v->n;
-    for (auto& fl : fields)
-      if (v->has(fl)) r.col[fl] = v->data.at(fl);
+    for (auto& fl : fields) {
+      if (!v->has(fl)) continue;
+      if (!v->data.count(fl) && v->host.count(fl)) {  // a host-held small result column
+        const auto& h = v->host.at(fl);
+        auto d = mkbuf(std::max<size_t>(h.size(), 1) * 8, stream_);
+        if (!h.empty())
+          ck(cudaMemcpyAsync(d->as<void>(), h.data(), h.size() * 8, cudaMemcpyHostToDevice, stream_), "h2d");
+        stats_.h2d_bytes += h.size() * 8;
+        v->data[fl] = d;
+      }
+      r.col[fl] = v->data.at(fl);
+    }
     r.seg_counts = {v->n};
     if (want_seg) {
       r.seg_of_row = mkbuf(std::max<uint64_t>(v->n, 1) * 4, stream_);

@@ -93,6 +93,8 @@ struct Var {
   // Mat
   uint64_t n = 0;
   std::map<std::string, DevBufP> data;
+  // host copies of small results (dense group-by); data gets a column on first use
+  std::map<std::string, std::vector<int64_t>> host;
   std::map<std::string, int> grp_type;
   bool has(const std::string& c) const;
 };
@@ -168,6 +170,7 @@ class Engine {
                         uint64_t row_base);
   const alk_gb_tuning& last_tuning() const { return last_tuning_; }
   void set_autotune(bool on) { autotune_ = on; }
+  void set_plain(bool on) { flags_ = on ? (flags_ | ALK_SESSION_PLAIN) : (flags_ & ~ALK_SESSION_PLAIN); }
   const std::string& error() const { return err_; }
   cudaStream_t stream() const { return stream_; }
   int preload(const std::string& table);

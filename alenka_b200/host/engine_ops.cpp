@@ -1,6 +1,7 @@
 // Operator execution of the host engine: emit_filter / emit_select / emit_join /
 // emit_order / emit_store semantics on top of the operator-level C ABI.
 #include <algorithm>
+#include <chrono>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -382,6 +383,7 @@ struct SelectCtx {
   std::vector<alk_colseg> cs;
   alk_gb_query q{};
   DevBufP acc;
+  std::vector<int64_t> hacc;  // the accumulators on the host
   std::vector<uint64_t> seg_rows;
   std::vector<int64_t> kmin, kspan;
 };
@@ -716,6 +718,43 @@ void Engine::select_output(SelectCtx& c) {
 
 // ------------------------------------------------------------------ dense group-by
 namespace {
+// The device register machine's arithmetic (wrapping; x / 0 = 0; INT64_MIN / -1 wraps),
+// for the few rows of a dense group-by result.
+int64_t host_mul(int64_t a, int64_t b) { return (int64_t)((uint64_t)a * (uint64_t)b); }
+int64_t host_div(int64_t a, int64_t b) {
+  if (b == 0) return 0;
+  if (b == -1) return (int64_t)(0 - (uint64_t)a);
+  return a / b;
+}
+int64_t host_apply(uint8_t op, int64_t a, int64_t b) {
+  switch (op) {
+    case ALK_OP_ADD: return (int64_t)((uint64_t)a + (uint64_t)b);
+    case ALK_OP_SUB: return (int64_t)((uint64_t)a - (uint64_t)b);
+    case ALK_OP_MUL: return host_mul(a, b);
+    case ALK_OP_DIV: return host_div(a, b);
+    case ALK_OP_LT: return a < b;
+    case ALK_OP_GT: return a > b;
+    case ALK_OP_LE: return a <= b;
+    case ALK_OP_GE: return a >= b;
+    case ALK_OP_EQ: return a == b;
+    case ALK_OP_NE: return a != b;
+    case ALK_OP_AND: return (a != 0) && (b != 0);
+    case ALK_OP_OR: return (a != 0) || (b != 0);
+    default: return a;
+  }
+}
+void host_eval(const alk_program& p, const std::vector<const int64_t*>& cols, uint64_t n, int64_t* out) {
+  int64_t regs[ALK_MAX_REGS];
+  for (uint64_t i = 0; i < n; i++) {
+    for (uint32_t pc = 0; pc < p.n_instr; pc++) {
+      const alk_instr& in = p.ins[pc];
+      const int64_t a = in.ka == ALK_K_REG ? regs[in.a] : (in.ka == ALK_K_COL ? cols[in.a][i] : p.consts[in.a]);
+      const int64_t b = in.kb == ALK_K_REG ? regs[in.b] : (in.kb == ALK_K_COL ? cols[in.b][i] : p.consts[in.b]);
+      regs[in.dst] = host_apply(in.op, a, b);
+    }
+    out[i] = regs[p.result];
+  }
+}
 // An aggregate input as (am * A + ac) * (bm * B + bc) in wrapping int64 arithmetic: the
 // ring identities hold modulo 2^64, so this form equals the expression tree's value
 // whenever the tree uses only +, - and * (no division).
@@ -937,7 +976,7 @@ void Engine::dense_select_run(const std::vector<SelectCtx*>& cs) {
         for (uint32_t bps : {1u, 2u, 3u, 4u}) {
           alk_gb_tuning t{cw, nst, bps}, used{};
           cudaEventRecord(ev0_, stream_);
-          int rc = alk_batch_groupby(qs.data(), (uint32_t)qs.size(), &t, &used, (alk_stream)stream_);
+          int rc = alk_batch_groupby(qs.data(), (uint32_t)qs.size(), &t, &used, nullptr, (alk_stream)stream_);
           cudaEventRecord(ev1_, stream_);
           if (rc == ALK_ERR_UNSUPPORTED) continue;
           check(rc, "batched group-by");
@@ -953,10 +992,32 @@ void Engine::dense_select_run(const std::vector<SelectCtx*>& cs) {
     gb_tune_[sig] = best;
   }
   alk_gb_tuning used{};
-  check(alk_batch_groupby(qs.data(), (uint32_t)qs.size(), best.consumer_warps ? &best : nullptr, &used,
+  alk_event_timer tm{timing_ ? 1 : 0, ev0_, ev1_, 0.0, 0};
+  check(alk_batch_groupby(qs.data(), (uint32_t)qs.size(), best.consumer_warps ? &best : nullptr, &used, &tm,
                           (alk_stream)stream_),
         "batched group-by");
   last_tuning_ = used;
+  // every select's accumulators back in one synchronisation
+  for (auto* c : cs) {
+    c->hacc.resize(c->acc->bytes() / 8);
+    ck(cudaMemcpyAsync(c->hacc.data(), c->acc->as<void>(), c->hacc.size() * 8, cudaMemcpyDeviceToHost, stream_),
+       "d2h");
+    stats_.d2h_bytes += c->hacc.size() * 8;
+  }
+  ck(cudaStreamSynchronize(stream_), "sync");
+  for (auto* c : cs) c->acc.reset();
+  if (tm.launches) {
+    // algorithmic bytes: every scanned row's stored values of the columns the queries read
+    uint64_t bytes = 0;
+    for (auto* c : cs)
+      for (uint32_t k = 0; k < c->q.ncols; k++)
+        for (uint32_t g = 0; g < c->q.nseg; g++)
+          if (c->q.seg_mode[g])
+            bytes += (uint64_t)c->cs[(size_t)k * c->q.nseg + g].rows * (c->cs[(size_t)k * c->q.nseg + g].bits / 8);
+    stats_.hot_kernel_ms += tm.ms;
+    stats_.hot_kernel_launches += tm.launches;
+    stats_.hot_kernel_bytes += bytes;
+  }
 }
 
 void Engine::dense_select_finish(SelectCtx& c) {
@@ -976,10 +1037,8 @@ void Engine::dense_select_finish(SelectCtx& c) {
   uint64_t nslots = 1;
   for (uint32_t j = 0; j < q.nkeys; j++) nslots *= (uint64_t)c.kspan[j];
   const uint32_t nacc = q.nagg + 1;
-  std::vector<int64_t> h(nslots * nacc);
-  ck(cudaMemcpyAsync(h.data(), c.acc->as<void>(), h.size() * 8, cudaMemcpyDeviceToHost, stream_), "d2h");
-  ck(cudaStreamSynchronize(stream_), "sync");
-  stats_.d2h_bytes += h.size() * 8;
+  const std::vector<int64_t>& h = c.hacc;  // copied back by dense_select_run
+  if (h.size() < nslots * nacc) throw EngineError(ALK_ERR_ARG, "dense group-by: accumulators missing");
   std::vector<std::vector<int64_t>> keys(q.nkeys), vals(q.nagg);
   for (uint64_t sl = 0; sl < nslots; sl++) {
     if (h[(size_t)q.nagg * nslots + sl] == 0) continue;  // no row in this slot
@@ -991,24 +1050,88 @@ void Engine::dense_select_finish(SelectCtx& c) {
     for (uint32_t k = 0; k < q.nagg; k++) vals[k].push_back(h[(size_t)k * nslots + sl]);
   }
   const uint64_t ng = keys.empty() ? 0 : keys[0].size();
-  GroupOut& G = c.G;
-  G.g = ng;
-  auto upload = [&](const std::vector<int64_t>& v) {
-    auto d = mkbuf(std::max<uint64_t>(v.size(), 1) * 8, stream_);
-    if (!v.empty())
-      ck(cudaMemcpyAsync(d->as<void>(), v.data(), v.size() * 8, cudaMemcpyHostToDevice, stream_), "h2d");
-    stats_.h2d_bytes += v.size() * 8;
-    return d;
+  // output order (as select_output): MurmurHash64A of the key tuple across segments,
+  // stable; key order within one segment
+  std::vector<uint32_t> perm(ng);
+  std::iota(perm.begin(), perm.end(), 0);
+  if (c.cycles > 1) {
+    std::vector<uint64_t> hs(ng);
+    std::vector<int64_t> tuple(q.nkeys);
+    for (uint64_t g = 0; g < ng; g++) {
+      for (uint32_t j = 0; j < q.nkeys; j++) tuple[j] = keys[j][g];
+      hs[g] = murmur64a(tuple.data(), (int)(8 * q.nkeys), kHashSeed);
+    }
+    std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) { return hs[x] < hs[y]; });
+  } else {
+    std::stable_sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
+      for (uint32_t j = 0; j < q.nkeys; j++)
+        if (keys[j][x] != keys[j][y]) return keys[j][x] < keys[j][y];
+      return false;
+    });
+  }
+  auto permuted = [&](const std::vector<int64_t>& v) {
+    std::vector<int64_t> o(ng);
+    for (uint64_t g = 0; g < ng; g++) o[g] = v[perm[g]];
+    return o;
   };
-  for (auto& k : keys) G.keys.push_back(upload(k));
-  for (auto& v : vals) G.vals.push_back(upload(v));
-  G.first = mkbuf(std::max<uint64_t>(ng, 1) * 4, stream_);
-  ck(cudaMemsetAsync(G.first->as<void>(), 0, std::max<uint64_t>(ng, 1) * 4, stream_), "init");
-  for (auto& k : G.keys) c.okeys.push_back(k->as<int64_t>());
-  c.out = std::move(out);
+  std::vector<std::vector<int64_t>> sk, sv;
+  for (auto& k : keys) sk.push_back(permuted(k));
+  for (auto& v : vals) sv.push_back(permuted(v));
+  // output columns (select_output's rules, evaluated on the host for the few groups)
+  std::vector<std::string> names;
+  std::vector<std::vector<int64_t>> cols;
+  std::vector<ColMeta> metas;
+  std::vector<int> gtypes;
+  for (auto& o : c.outs) {
+    ColMeta m;
+    m.dz = o.prec;
+    std::vector<int64_t> col;
+    if (o.col_type == 1) {
+      auto it = std::find(c.group_cols.begin(), c.group_cols.end(), o.field);
+      col = sk[it - c.group_cols.begin()];
+      m.string_map = c.a->meta[o.field].string_map;
+    } else if (o.col_type == 2 && o.vec->k == Ast::Agg) {
+      col = sv[o.vec->agg];
+    } else if (o.col_type == 2) {
+      Compiler cc;
+      alk_program prog = cc.finish(o.vec);
+      std::vector<const int64_t*> in;
+      for (auto& sname : cc.slots) in.push_back(sv[std::stoi(sname.substr(4))].data());
+      col.resize(ng);
+      host_eval(prog, in, ng, col.data());
+    } else {
+      col.assign(ng, (int64_t)(int)o.num);
+    }
+    names.push_back(o.name);
+    cols.push_back(std::move(col));
+    metas.push_back(m);
+    gtypes.push_back(o.grp_type);
+  }
+  // AVG finalisation of count_avg (merge.cu:446-458)
+  int countc = -1;
+  for (size_t k = 0; k < cols.size(); k++)
+    if (gtypes[k] == 0) {
+      countc = (int)k;
+      break;
+    }
+  for (size_t k = 0; k < cols.size(); k++) {
+    if (gtypes[k] != 1) continue;
+    if (countc < 0) unsupported("AVG needs a COUNT column in the same select");
+    for (uint64_t g = 0; g < ng; g++)
+      cols[k][g] = metas[k].dz <= 2 ? host_div(host_mul(cols[k][g], 100), cols[countc][g])
+                                    : host_div(cols[k][g], cols[countc][g]);
+    if (metas[k].dz <= 2) metas[k].dz += 2;
+    gtypes[k] = 3;
+  }
+  out->n = ng;
+  for (size_t k = 0; k < cols.size(); k++) {
+    out->columnNames.push_back(names[k]);
+    out->meta[names[k]] = metas[k];
+    out->grp_type[names[k]] = gtypes[k];
+    out->host[names[k]] = std::move(cols[k]);
+  }
+  vars_[st.s] = std::move(out);
   stats_.plan = std::max<uint32_t>(stats_.plan, 1);
-  select_output(c);
-  ck(cudaStreamSynchronize(stream_), "sync");  // host vectors above were copy sources
 }
 
 // ------------------------------------------------------------------ JOIN
@@ -1191,17 +1314,29 @@ void Engine::emit_order(Statement& st) {
 void Engine::emit_store(Statement& st) {
   Var* a = var(st.s);
   size_t limit = st.op_nums.empty() ? 0 : (size_t)st.op_nums[0];
-  Rows R = materialize(a, a->columnNames);
-  size_t mcount = (limit != 0 && limit < R.n) ? limit : R.n;
-  std::vector<std::vector<int64_t>> h(a->columnNames.size(), std::vector<int64_t>(mcount));
-  for (size_t c = 0; c < a->columnNames.size(); c++) {
-    if (!mcount) break;
-    ck(cudaMemcpyAsync(h[c].data(), R.col.at(a->columnNames[c])->as<void>(), mcount * 8, cudaMemcpyDeviceToHost,
-                       stream_),
-       "store d2h");
-    stats_.d2h_bytes += mcount * 8;
+  bool on_host = a->kind == Var::Mat;
+  for (auto& c : a->columnNames) on_host = on_host && a->host.count(c);
+  std::vector<std::vector<int64_t>> h(a->columnNames.size());
+  size_t mcount = 0;
+  if (on_host) {  // a small result already on the host
+    mcount = (limit != 0 && limit < a->n) ? limit : a->n;
+    for (size_t c = 0; c < a->columnNames.size(); c++) {
+      const auto& src = a->host.at(a->columnNames[c]);
+      h[c].assign(src.begin(), src.begin() + mcount);
+    }
+  } else {
+    Rows R = materialize(a, a->columnNames);
+    mcount = (limit != 0 && limit < R.n) ? limit : R.n;
+    for (size_t c = 0; c < a->columnNames.size(); c++) {
+      h[c].resize(mcount);
+      if (!mcount) continue;
+      ck(cudaMemcpyAsync(h[c].data(), R.col.at(a->columnNames[c])->as<void>(), mcount * 8, cudaMemcpyDeviceToHost,
+                         stream_),
+         "store d2h");
+      stats_.d2h_bytes += mcount * 8;
+    }
+    ck(cudaStreamSynchronize(stream_), "store sync");
   }
-  ck(cudaStreamSynchronize(stream_), "store sync");
   std::string path = st.f;
   if (path.empty() || path[0] != '/') path = dir_ + "/" + path;
   FILE* fp = std::fopen(path.c_str(), "w");
@@ -1319,6 +1454,10 @@ int Engine::execute_batch(const std::vector<std::string>& scripts) {
     r.pending = false;
     cudaStreamSynchronize(stream_);
   };
+  auto wall = [] {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  };
+  const double w0 = wall();
   // phase 1: every script up to its dense group-by
   for (auto& text : scripts) {
     runs.push_back(std::make_unique<Run>());
@@ -1350,6 +1489,7 @@ int Engine::execute_batch(const std::vector<std::string>& scripts) {
     r.vars = std::move(vars_);
     vars_.clear();
   }
+  const double w1 = wall();
   // phase 2: one launch
   std::vector<SelectCtx*> batch;
   for (auto& r : runs)
@@ -1362,6 +1502,7 @@ int Engine::execute_batch(const std::vector<std::string>& scripts) {
         if (r->pending) fail(*r, e.code, e.what());
     }
   }
+  const double w2 = wall();
   // phase 3: the rest of every script that waited
   for (auto& rp : runs) {
     Run& r = *rp;
@@ -1384,6 +1525,9 @@ int Engine::execute_batch(const std::vector<std::string>& scripts) {
     }
     vars_.clear();
   }
+  stats_.batch_host_ms[0] = w1 - w0;
+  stats_.batch_host_ms[1] = w2 - w1;
+  stats_.batch_host_ms[2] = wall() - w2;
   int rc = ALK_OK;
   for (size_t k = 0; k < runs.size(); k++)
     if (runs[k]->rc != ALK_OK && rc == ALK_OK) {

@@ -13,9 +13,9 @@ def flat_cutoff(seed):
     return date_add_days(19950617, random.Random(seed).randint(-30, 30))
 
 
-def flat_script(seed, out="q1.txt"):
+def flat_script(seed, out="q1.txt", table="lineitem"):
     cut = flat_cutoff(seed)
-    return (f"LF := FILTER lineitem BY l_shipdate < {cut};\n"
+    return (f"LF := FILTER {table} BY l_shipdate < {cut};\n"
             "R := SELECT l_returnflag AS l_returnflag, l_linestatus AS l_linestatus, "
             "SUM(l_quantity) AS sum_qty, SUM(l_extendedprice) AS sum_base_price, "
             "SUM(l_extendedprice*(1-l_discount)) AS sum_disc_price, COUNT(l_orderkey) AS count_order "
@@ -70,6 +70,24 @@ def card_script(seed, out="qc.txt"):
             "FROM OLC GROUP BY o_orderkey, o_orderdate, o_shippriority;\n"
             "RES := ORDER F BY sum_revenue DESC, orderdate1 ASC;\n"
             f"STORE RES INTO '{out}' USING ('|') LIMIT 10;\n")
+
+
+def batched_layout(queries=256, total_rows=6_000_000_000, seed=1, median=4_000_000, sigma=1.0,
+                   lo=1_000_000, hi=32_000_000):
+    """Segment sizes of the batched workload: lognormal (median 4M rows, clipped to
+    [1M, 32M]) drawn until the total is reached, dealt to the queries' tables in turn.
+    Returns one list of segment sizes per query (empty when the total ran out first)."""
+    import math
+    r = random.Random(seed * 7 + 5)
+    tables = [[] for _ in range(queries)]
+    total, i = 0, 0
+    while total < total_rows:
+        n = int(min(hi, max(lo, math.exp(math.log(median) + sigma * r.gauss(0.0, 1.0)))))
+        n = min(n, total_rows - total)
+        tables[i % queries].append(n)
+        total += n
+        i += 1
+    return tables
 
 
 # Full-size shapes (rows): the single-table workload and the three-way pipeline.

@@ -252,6 +252,96 @@ def timed_steps(sess, script, steps, torch, dist):
     return ms, acc
 
 
+def _steps(sess, fn, steps, torch):
+    """steps calls of fn bracketed by synchronize, timed with CUDA events on the session's
+    stream; returns (ms per step, summed stats)."""
+    stream = torch.cuda.ExternalStream(sess.stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    acc = {"kernels": 0, "hot_ms": 0.0, "hot_bytes": 0, "hot_launches": 0, "plan": 0, "rows": 0}
+    for _ in range(steps):
+        fn()
+        st = sess.stats()
+        acc["kernels"] += st.kernels
+        acc["hot_ms"] += st.hot_kernel_ms
+        acc["hot_bytes"] += st.hot_kernel_bytes
+        acc["hot_launches"] += st.hot_kernel_launches
+        acc["plan"] = st.plan
+        acc["rows"] += st.rows_scanned
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, acc
+
+
+def run_batched(args, torch):
+    """Many queries of the single-table filter + group-by family over tables generated in
+    device memory (lognormal segment sizes), one batch per step; beside it the same
+    scripts one at a time on the dense path and on the plain operator path."""
+    import alenka_b200 as ab
+    from alenka_b200 import workloads as wl
+    total = int(6_000_000_000 * args.scale)
+    layout = [t for t in wl.batched_layout(args.queries, total, args.seed) if t]
+    rows = sum(sum(t) for t in layout)
+    d = tempfile.mkdtemp(prefix="alenka_batched_")
+    sess = ab.Session(d, resident=True)
+    if args.no_autotune:
+        sess.tuning(autotune=False)
+    t0 = time.perf_counter()
+    for q, segs in enumerate(layout):
+        sess.gen_flat_resident(f"li{q:03d}", segs, args.seed * 1000 + q)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    scripts = [wl.flat_script(args.seed * 1000 + q, out=f"bq{q:03d}.txt", table=f"li{q:03d}")
+               for q in range(len(layout))]
+    for _ in range(args.warmup):
+        sess.execute_batch(scripts)
+    sess.set_timing(True)
+    clk = clock_sampler(0)
+    clk.start()
+    ms, acc = _steps(sess, lambda: sess.execute_batch(scripts), args.steps, torch)
+    clocks = clk.stop()
+    sess.set_timing(False)
+    tuning = sess.tuning()
+    host_ms = list(sess.stats().batch_host_ms)
+    one_ms = plain_ms = float("nan")
+    if not args.batched_only:
+        for sc in scripts[:4]:
+            sess.execute(sc)
+        one_ms, _ = _steps(sess, lambda: [sess.execute(sc) for sc in scripts], 1, torch)
+        sess.set_plain(True)
+        for sc in scripts[:2]:
+            sess.execute(sc)
+        plain_ms, _ = _steps(sess, lambda: [sess.execute(sc) for sc in scripts], 1, torch)
+    sess.close()
+    peak, peak_kind = measured_peak_hbm()
+    hot = None
+    if acc["hot_launches"]:
+        pl_bytes = acc["hot_bytes"] / acc["hot_launches"]
+        pl_ms = acc["hot_ms"] / acc["hot_launches"]
+        achieved = pl_bytes / (pl_ms / 1000.0) / 1e9
+        hot = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+               "traffic": profiled_traffic("batched_groupby_flat.md"),
+               "kernel": "k_gb_tma (batched filter + dense group-by, one launch per batch)",
+               "algorithmic_bytes": "scanned rows x stored widths of the columns the queries read",
+               "algorithmic_bytes_per_launch": int(pl_bytes), "avg_launch_ms": pl_ms,
+               "peak_source": f"{peak_kind} hbm_gbs"}
+    print(json.dumps({
+        "metric": "fact rows/s, batched filter + group-by (single-table family)", "value": rows / (ms / 1000.0),
+        "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (generated in device memory)",
+        "config": {"workload": f"{len(layout)} queries over {rows} lineitem rows in "
+                               f"{sum(len(t) for t in layout)} lognormal segments (median 4M, 1M-32M)",
+                   "launch_shape": {"consumer_warps": tuning[0], "stages": tuning[1], "blocks_per_sm": tuning[2]},
+                   "one_at_a_time_dense_rows_per_s": rows / (one_ms / 1000.0),
+                   "plain_gpu_rows_per_s": rows / (plain_ms / 1000.0),
+                   "batched_vs_plain": plain_ms / ms, "generation_s": gen_s,
+                   "host_ms_plan_launch_finish": host_ms, "l2": "inputs larger than L2"},
+        "e2e": None, "gpu_launches": acc["kernels"], "roofline": hot, "cpu_baseline": None, "clocks": clocks,
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -264,6 +354,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fused-only", action="store_true",
                     help="time only the resident fused plan (profiling runs)")
+    ap.add_argument("--workload", default="three_way", choices=["three_way", "batched"],
+                    help="three_way: the filter -> join -> group-by pipeline (default); batched: many "
+                         "single-table filter + group-by queries per step")
+    ap.add_argument("--queries", type=int, default=256)
+    ap.add_argument("--batched-only", action="store_true", help="batched workload: skip the one-at-a-time runs")
+    ap.add_argument("--no-autotune", action="store_true", help="batched workload: default launch shape")
     ap.add_argument("--no-graphs", action="store_true",
                     help="run every query without CUDA-graph replay (same kernels; for ncu, whose per-kernel "
                          "replay does not handle graph memory nodes)")
@@ -276,6 +372,10 @@ def main():
         return
     import torch
     torch.cuda.set_device(local)
+    if args.workload == "batched":
+        if rank == 0:
+            run_batched(args, torch)
+        return
     dist = None
     if world > 1:
         import datetime

@@ -76,6 +76,7 @@ typedef struct alk_stats {
   uint64_t reserved_bytes;   /* survivor-list and hash-table bytes the fused stages reserved */
   uint32_t card_estimates;   /* fused stages sized by the learned estimator */
   uint32_t card_reruns;      /* fused query runs repeated because a size was too small */
+  double batch_host_ms[3];   /* batches: wall time of planning, the batched launch, the rest */
 } alk_stats;
 int alk_session_stats(alk_session* s, alk_stats* out);
 /* Enable CUDA-event timing of the dominant kernel (adds two event records per launch). */
@@ -399,6 +400,8 @@ typedef struct alk_gb_query {
   int64_t* d_acc;       /* device [nagg + 1][slots]: the aggregates, then the row count */
   uint64_t* h_seg_rows; /* optional host [nseg]: rows passing the filter per segment */
 } alk_gb_query;
+/* timer (optional): events around the group-by kernel; its time and launch count are
+ * added to it. */
 /* Launch shape: consumer warps per block (4 or 8; a tile is 256 rows per warp), tiles in
  * flight per block (2..4), blocks per SM (capped by shared memory); 0 = default. */
 typedef struct alk_gb_tuning {
@@ -408,12 +411,14 @@ typedef struct alk_gb_tuning {
  * (nagg + 1) <= 64 per query (accumulators private to each thread); a larger slot space or
  * a filter that is not a conjunction returns ALK_ERR_UNSUPPORTED. *used = the shape run. */
 int alk_batch_groupby(const alk_gb_query* queries, uint32_t nq, const alk_gb_tuning* tune, alk_gb_tuning* used,
-                      alk_stream stream);
+                      alk_event_timer* timer, alk_stream stream);
 /* Runs n scripts with one batched launch for their group-bys: every script runs up to
  * its first SELECT ... GROUP BY of the dense form, those run together, then every script
  * continues. Results are those of running the scripts one at a time. Returns the first
  * failing script's status (alk_session_error names it); the others still run. */
 int alk_session_execute_batch(alk_session* s, const char* const* scripts, uint32_t n);
+/* Switches the session between the operator-at-a-time plan (on) and the fused plans. */
+int alk_session_set_plain(alk_session* s, int on);
 /* *out = the launch shape of the last batched group-by; autotune 0/1 turns the per-
  * workload autotuner off/on (-1 leaves it). */
 int alk_session_tuning(alk_session* s, alk_gb_tuning* out, int autotune);
