@@ -715,7 +715,7 @@ __global__ void __launch_bounds__(kT) k_topk_collect(const int64_t* rank, const 
 
 // Threshold on the device: the k-th largest of the per-block candidate lists (m values,
 // m <= kMergeMax).
-constexpr int kMergeThreads = 1024;
+constexpr int kMergeThreads = 256;
 constexpr int kMergeMax = 4096;
 __global__ void __launch_bounds__(kMergeThreads) k_topk_merge(const int64_t* best, uint32_t m, uint32_t k,
                                                               int64_t* thr) {
@@ -807,27 +807,47 @@ struct SegPlan {
 
 // Drops the thread's items whose probe key (stored value x + lower) is absent from the
 // probed table's key bitmap.
+// The key-bitmap tests load all of the thread's bitmap words before testing any: the
+// loads are independent round trips to L2, issued back to back (an item already dropped
+// reads word 0 and is not tested).
 __device__ __forceinline__ uint32_t probe_filter(const HtView& h, int64_t lower, const uint64_t (&x)[kItems],
                                                  uint32_t live) {
+  uint64_t o[kItems];
+  uint32_t w[kItems];
+#pragma unroll
+  for (int k = 0; k < kItems; k++) {
+    o[k] = x[k] + (uint64_t)lower - (uint64_t)h.kmin;
+    if (!(((live >> k) & 1) && o[k] < h.nbits)) {
+      live &= ~(1u << k);
+      o[k] = 0;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kItems; k++) w[k] = __ldg(h.bits + (o[k] >> 5));
 #pragma unroll
   for (int k = 0; k < kItems; k++)
-    if (((live >> k) & 1) && !ht_member(h, (int64_t)(x[k] + (uint64_t)lower))) live &= ~(1u << k);
+    if (!((w[k] >> (o[k] & 31)) & 1u)) live &= ~(1u << k);
   return live;
 }
 
 __device__ __forceinline__ uint32_t probe_filter32(const HtView& h, const SegPlan& sp, const uint32_t (&x)[kItems],
                                                    uint32_t live) {
   if (!sp.kmember) return 0;
+  uint32_t o[kItems], w[kItems];
 #pragma unroll
   for (int k = 0; k < kItems; k++) {
     const uint32_t d = x[k] - sp.xlo;
-    if (d > sp.xspan) {
+    o[k] = d + sp.boff;
+    if (!(((live >> k) & 1) && d <= sp.xspan)) {
       live &= ~(1u << k);
-      continue;
+      o[k] = 0;
     }
-    const uint32_t o = d + sp.boff;
-    if (((live >> k) & 1) && !((__ldg(h.bits + (o >> 5)) >> (o & 31)) & 1u)) live &= ~(1u << k);
   }
+#pragma unroll
+  for (int k = 0; k < kItems; k++) w[k] = __ldg(h.bits + (o[k] >> 5));
+#pragma unroll
+  for (int k = 0; k < kItems; k++)
+    if (!((w[k] >> (o[k] & 31)) & 1u)) live &= ~(1u << k);
   return live;
 }
 __global__ void __launch_bounds__(kT) k_stage_fast(const __grid_constant__ FastArgs f) {
@@ -1800,7 +1820,10 @@ int alk_topk_select(const int64_t* d_rank, const uint64_t* d_live, uint64_t n, u
   if (!d_count || !d_out || k == 0 || k > (uint32_t)kTopK) return ALK_ERR_ARG;
   CK(cudaMemsetAsync(d_count, 0, 8, s));
   if (n == 0) return ALK_OK;
-  const int blocks = (int)std::min<uint64_t>((n + kT - 1) / kT, (uint64_t)kMergeMax / k);
+  // a few blocks per SM, each over a strided share of the slots: the merge of their lists
+  // stays short
+  const int blocks = (int)std::min<uint64_t>(std::min<uint64_t>((n + kT - 1) / kT, (uint64_t)kMergeMax / k),
+                                             (uint64_t)sms() * 4);
   int64_t* db = nullptr;
   CK(cudaMallocAsync((void**)&db, ((size_t)blocks * k + 1) * 8, s));
   k_topk_local16<<<blocks, kT, 0, s>>>(d_rank, (const unsigned long long*)d_live, n, k, db);
