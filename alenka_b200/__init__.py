@@ -43,6 +43,8 @@ class Stats(ctypes.Structure):
         ("card_estimates", ctypes.c_uint32),
         ("card_reruns", ctypes.c_uint32),
         ("batch_host_ms", ctypes.c_double * 3),
+        ("sort_groupbys", ctypes.c_uint32),
+        ("pad_", ctypes.c_uint32),
     ]
 
 
@@ -95,6 +97,7 @@ def _declare(L):
     L.alk_session_execute_batch.argtypes = [vp, c.POINTER(c.c_char_p), u32]
     L.alk_session_tuning.argtypes = [vp, c.POINTER(Tuning), i32]
     L.alk_session_set_plain.argtypes = [vp, i32]
+    L.alk_session_set_groupby.argtypes = [vp, i32]
     L.alk_session_gen_flat_resident.argtypes = [vp, c.c_char_p, c.POINTER(u32), u32, u64, u64]
     L.alk_gen_flat_value.argtypes = [u64, i32, u64]
     L.alk_gen_flat_value.restype = i64
@@ -165,6 +168,11 @@ class Session:
         rc = lib().alk_session_gen_flat_resident(self._h, table.encode(), arr, len(seg_rows), seed, row_base)
         if rc != ALK_OK:
             raise AlenkaError(rc, lib().alk_session_error(self._h).decode())
+
+    def set_groupby(self, mode):
+        """0: hash or sort by the expected group count; 1: hash; 2: sort."""
+        if lib().alk_session_set_groupby(self._h, int(mode)) != ALK_OK:
+            raise AlenkaError(1, "bad group-by mode")
 
     def set_plain(self, on):
         lib().alk_session_set_plain(self._h, 1 if on else 0)

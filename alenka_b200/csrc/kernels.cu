@@ -568,6 +568,148 @@ int grid_for(uint64_t n) {
   return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, lim));
 }
 
+
+// ------------------------------------------------------------ sort-based group-by
+// Rows in key order (the identity when the input already is, else a stable permutation)
+// are cut into tiles of kSegTile rows; thread t of a tile owns rows t*kSegItems ..
+// t*kSegItems + kSegItems - 1. A row heads a group when its key tuple differs from the
+// previous row's. Group g = (heads up to and including the row) - 1.
+constexpr int kSegItems = 8;
+constexpr int kSegTile = kT * kSegItems;
+
+struct SegGbArgs {
+  const int64_t* const* keys;
+  uint32_t nkeys;
+  const int64_t* const* vals;
+  const uint8_t* aggs;
+  uint32_t nvals;
+  uint64_t n;
+  const uint32_t* perm;  // null: identity
+  unsigned long long* tile_heads;  // [ntiles]: heads per tile, then their exclusive prefix
+  unsigned long long* flags;       // [0] rows out of key order (the check), [1] groups
+};
+
+__device__ __forceinline__ uint64_t seg_row(const SegGbArgs& a, uint64_t i) { return a.perm ? a.perm[i] : i; }
+
+__device__ __forceinline__ bool seg_head(const SegGbArgs& a, uint64_t i) {
+  if (i == 0) return true;
+  const uint64_t r = seg_row(a, i), q = seg_row(a, i - 1);
+  for (uint32_t j = 0; j < a.nkeys; j++)
+    if (__ldg(a.keys[j] + r) != __ldg(a.keys[j] + q)) return true;
+  return false;
+}
+
+// Rows where the key tuple decreases (lexicographic, signed): zero means already in order.
+__global__ void __launch_bounds__(kT) k_seg_check(const SegGbArgs a) {
+  unsigned long long bad = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x + 1; i < a.n; i += (uint64_t)gridDim.x * kT) {
+    for (uint32_t j = 0; j < a.nkeys; j++) {
+      const int64_t x = __ldg(a.keys[j] + i - 1), y = __ldg(a.keys[j] + i);
+      if (x != y) {
+        bad += x > y;
+        break;
+      }
+    }
+  }
+  for (int o = 16; o; o >>= 1) bad += __shfl_xor_sync(0xffffffffu, bad, o);
+  if ((threadIdx.x & 31) == 0 && bad) atomicAdd(a.flags, bad);
+}
+
+__global__ void __launch_bounds__(kT) k_seg_count(const SegGbArgs a) {
+  __shared__ unsigned long long s_warp[kT / 32 + 1];
+  const uint64_t t = blockIdx.x;
+  const uint64_t i0 = t * kSegTile + (uint64_t)threadIdx.x * kSegItems;
+  unsigned long long c = 0;
+  for (int k = 0; k < kSegItems; k++)
+    if (i0 + k < a.n && seg_head(a, i0 + k)) c++;
+  unsigned long long tot;
+  block_excl_scan<kT>(c, s_warp, &tot);
+  if (threadIdx.x == 0) a.tile_heads[t] = tot;
+}
+
+// exclusive prefix of the tile counts, one block; flags[1] = groups
+__global__ void __launch_bounds__(1024) k_seg_scan(const SegGbArgs a, uint64_t ntiles) {
+  __shared__ unsigned long long s_warp[1024 / 32 + 1];
+  unsigned long long carry = 0;
+  for (uint64_t b = 0; b < ntiles; b += 1024) {
+    const uint64_t i = b + threadIdx.x;
+    const unsigned long long v = i < ntiles ? a.tile_heads[i] : 0;
+    unsigned long long tot;
+    const unsigned long long ex = block_excl_scan<1024>(v, s_warp, &tot);
+    if (i < ntiles) a.tile_heads[i] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) a.flags[1] = carry;
+}
+
+__device__ __forceinline__ void seg_apply(int64_t* dst, uint8_t kind, int64_t v) {
+  if (kind == ALK_AGG_MIN) atomicMin((long long*)dst, (long long)v);
+  else if (kind == ALK_AGG_MAX) atomicMax((long long*)dst, (long long)v);
+  else atomicAdd((unsigned long long*)dst, (unsigned long long)v);
+}
+
+// Group index of every row; head rows write their keys and first row; every row's values
+// are folded in registers while the thread's group does not change, then applied with
+// one atomic per (thread, group, value).
+__global__ void __launch_bounds__(kT) k_seg_reduce(const SegGbArgs a, int64_t* const* out_keys,
+                                                   int64_t* const* out_vals, uint32_t* out_first) {
+  __shared__ unsigned long long s_warp[kT / 32 + 1];
+  const uint64_t t = blockIdx.x;
+  const uint64_t i0 = t * kSegTile + (uint64_t)threadIdx.x * kSegItems;
+  uint32_t heads = 0;
+  unsigned long long c = 0;
+  for (int k = 0; k < kSegItems; k++)
+    if (i0 + k < a.n && seg_head(a, i0 + k)) {
+      heads |= 1u << k;
+      c++;
+    }
+  unsigned long long tot;
+  const unsigned long long ex = block_excl_scan<kT>(c, s_warp, &tot);
+  // group of the thread's first row: heads before it, minus one
+  long long g = (long long)(a.tile_heads[t] + ex) - 1;
+  int64_t acc[kMaxVals];
+  long long cur = -1;
+  for (int k = 0; k < kSegItems; k++) {
+    const uint64_t i = i0 + k;
+    if (i >= a.n) break;
+    const uint64_t r = seg_row(a, i);
+    if ((heads >> k) & 1) {
+      g++;
+      for (uint32_t j = 0; j < a.nkeys; j++) out_keys[j][g] = __ldg(a.keys[j] + r);
+      out_first[g] = (uint32_t)r;
+    }
+    if (g != cur) {
+      if (cur >= 0)
+        for (uint32_t v = 0; v < a.nvals; v++) seg_apply(out_vals[v] + cur, a.aggs[v], acc[v]);
+      cur = g;
+      for (uint32_t v = 0; v < a.nvals; v++)
+        acc[v] = a.aggs[v] == ALK_AGG_COUNT ? 1 : __ldg(a.vals[v] + r);
+      continue;
+    }
+    for (uint32_t v = 0; v < a.nvals; v++) {
+      const uint8_t kind = a.aggs[v];
+      if (kind == ALK_AGG_COUNT) {
+        acc[v] += 1;
+        continue;
+      }
+      const int64_t x = __ldg(a.vals[v] + r);
+      acc[v] = kind == ALK_AGG_MIN ? min(acc[v], x)
+             : kind == ALK_AGG_MAX ? max(acc[v], x)
+                                   : (int64_t)((uint64_t)acc[v] + (uint64_t)x);
+    }
+  }
+  if (cur >= 0)
+    for (uint32_t v = 0; v < a.nvals; v++) seg_apply(out_vals[v] + cur, a.aggs[v], acc[v]);
+}
+
+__global__ void __launch_bounds__(kT) k_seg_init(int64_t* const* out_vals, const uint8_t* aggs, uint32_t nvals,
+                                                 uint64_t g) {
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < g * nvals; i += (uint64_t)gridDim.x * kT) {
+    const uint32_t v = (uint32_t)(i / g);
+    const uint8_t k = aggs[v];
+    out_vals[v][i - (uint64_t)v * g] = k == ALK_AGG_MIN ? INT64_MAX : k == ALK_AGG_MAX ? INT64_MIN : 0;
+  }
+}
 }  // namespace
 
 #define CK(x)                                           \
@@ -882,6 +1024,78 @@ int alk_gather(const int64_t* d_src, const uint32_t* d_idx, uint64_t n, int64_t*
   k_gather<<<grid_for(n), kT, 0, (cudaStream_t)stream>>>(d_src, d_idx, n, d_out);
   alk::g_kernel_launches++;
   CK(cudaGetLastError());
+  return ALK_OK;
+}
+
+int alk_groupby_sort(const int64_t* const* d_keys, uint32_t nkeys, const int64_t* const* d_vals,
+                     const uint8_t* aggs, uint32_t nvals, uint64_t n, int64_t* const* d_out_keys,
+                     int64_t* const* d_out_vals, uint32_t* d_out_first, uint64_t* h_groups, int* h_was_sorted,
+                     alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!h_groups || nkeys == 0 || nkeys > kMaxKeys || nvals > kMaxVals || n > 0xffffffffull) return ALK_ERR_ARG;
+  *h_groups = 0;
+  if (h_was_sorted) *h_was_sorted = 1;
+  if (n == 0) return ALK_OK;
+  Scratch sc(s);
+  cudaError_t e;
+  const size_t ptr_bytes = sizeof(void*) * (kMaxKeys + kMaxVals) * 2 + 64;
+  uint8_t* db = sc.get<uint8_t>(ptr_bytes, &e);
+  CK(e);
+  const uint64_t ntiles = (n + kSegTile - 1) / kSegTile;
+  unsigned long long* tiles = sc.get<unsigned long long>(ntiles, &e);
+  CK(e);
+  unsigned long long* flags = sc.get<unsigned long long>(2, &e);
+  CK(e);
+  std::vector<uint8_t> hb(ptr_bytes, 0);
+  const size_t o_keys = 0, o_vals = o_keys + sizeof(void*) * kMaxKeys, o_okeys = o_vals + sizeof(void*) * kMaxVals,
+               o_ovals = o_okeys + sizeof(void*) * kMaxKeys, o_aggs = o_ovals + sizeof(void*) * kMaxVals;
+  std::memcpy(&hb[o_keys], d_keys, sizeof(void*) * nkeys);
+  if (nvals) {
+    std::memcpy(&hb[o_vals], d_vals, sizeof(void*) * nvals);
+    std::memcpy(&hb[o_ovals], d_out_vals, sizeof(void*) * nvals);
+    std::memcpy(&hb[o_aggs], aggs, nvals);
+  }
+  std::memcpy(&hb[o_okeys], d_out_keys, sizeof(void*) * nkeys);
+  CK(cudaMemcpyAsync(db, hb.data(), ptr_bytes, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(flags, 0, 16, s));
+  SegGbArgs a{(const int64_t* const*)(db + o_keys), nkeys, (const int64_t* const*)(db + o_vals), db + o_aggs, nvals,
+              n, nullptr, tiles, flags};
+  // 1. already in key order?
+  k_seg_check<<<grid_for(n), kT, 0, s>>>(a);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  unsigned long long bad = 0;
+  CK(cudaMemcpyAsync(&bad, flags, 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  uint32_t* perm = nullptr;
+  if (bad) {  // 2. a stable sort on the key tuple
+    if (h_was_sorted) *h_was_sorted = 0;
+    perm = sc.get<uint32_t>(n, &e);
+    CK(e);
+    std::vector<uint8_t> desc(nkeys, 0);
+    int rc = alk_sort_perm(d_keys, desc.data(), nkeys, n, perm, stream);
+    if (rc) return rc;
+    a.perm = perm;
+  }
+  // 3. heads per tile, their prefix, the group count
+  k_seg_count<<<(unsigned)ntiles, kT, 0, s>>>(a);
+  k_seg_scan<<<1, 1024, 0, s>>>(a, ntiles);
+  alk::g_kernel_launches += 2;
+  CK(cudaGetLastError());
+  unsigned long long g = 0;
+  CK(cudaMemcpyAsync(&g, flags + 1, 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  // 4. identities, then the reduction
+  if (nvals) {
+    k_seg_init<<<grid_for(g * nvals), kT, 0, s>>>((int64_t* const*)(db + o_ovals), db + o_aggs, nvals, g);
+    alk::g_kernel_launches++;
+  }
+  k_seg_reduce<<<(unsigned)ntiles, kT, 0, s>>>(a, (int64_t* const*)(db + o_okeys), (int64_t* const*)(db + o_ovals),
+                                                d_out_first);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  *h_groups = g;
   return ALK_OK;
 }
 

@@ -88,6 +88,12 @@ int alk_session_gen_flat_resident(alk_session* s, const char* table, const uint3
   return rc;
 }
 
+int alk_session_set_groupby(alk_session* s, int mode) {
+  if (!s || mode < 0 || mode > 2) return ALK_ERR_ARG;
+  s->eng->set_groupby_mode(mode);
+  return ALK_OK;
+}
+
 int alk_session_set_plain(alk_session* s, int on) {
   if (!s) return ALK_ERR_ARG;
   s->eng->set_plain(on != 0);

@@ -170,6 +170,8 @@ class Engine {
                         uint64_t row_base);
   const alk_gb_tuning& last_tuning() const { return last_tuning_; }
   void set_autotune(bool on) { autotune_ = on; }
+  // group-by form: 0 chosen by the expected group count, 1 hash, 2 sort
+  void set_groupby_mode(int m) { groupby_mode_ = m; }
   void set_plain(bool on) { flags_ = on ? (flags_ | ALK_SESSION_PLAIN) : (flags_ & ~ALK_SESSION_PLAIN); }
   const std::string& error() const { return err_; }
   cudaStream_t stream() const { return stream_; }
@@ -260,6 +262,9 @@ class Engine {
   std::map<std::string, alk_gb_tuning> gb_tune_;
   alk_gb_tuning last_tuning_{};
   bool autotune_ = true;
+  int groupby_mode_ = 0;
+  static constexpr uint64_t kHashGroupsMax = 1ull << 22;
+  uint64_t expected_groups(Var* a, const std::vector<std::string>& group_cols, uint64_t n);
 
   // ---- learned cardinality estimator
   bool card_record_ = false, card_use_ = false;

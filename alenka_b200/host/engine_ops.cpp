@@ -533,9 +533,22 @@ void Engine::emit_select(Statement& st) {
     ovals.push_back(G.vals.back()->as<int64_t>());
   }
   G.first = mkbuf(R.n * 4, stream_);
-  check(alk_groupby_hash(keys.data(), (uint32_t)keys.size(), vals.data(), kinds.data(), (uint32_t)vals.size(), R.n,
-                         okeys.data(), ovals.data(), G.first->as<uint32_t>(), &G.g, (alk_stream)stream_),
-        "hash group-by");
+  // hash or sort: the expected group count decides (groups beyond kHashGroupsMax take the
+  // reference's sort-based form, which skips the sort when the rows are in key order)
+  const uint64_t groups = grp_cnt ? expected_groups(a, group_cols, R.n) : R.n;
+  const bool sorted_gb = groupby_mode_ == 2 || (groupby_mode_ == 0 && groups > kHashGroupsMax);
+  if (sorted_gb) {
+    int in_order = 0;
+    check(alk_groupby_sort(keys.data(), (uint32_t)keys.size(), vals.data(), kinds.data(), (uint32_t)vals.size(), R.n,
+                           okeys.data(), ovals.data(), G.first->as<uint32_t>(), &G.g, &in_order,
+                           (alk_stream)stream_),
+          "sort group-by");
+    stats_.sort_groupbys++;
+  } else {
+    check(alk_groupby_hash(keys.data(), (uint32_t)keys.size(), vals.data(), kinds.data(), (uint32_t)vals.size(), R.n,
+                           okeys.data(), ovals.data(), G.first->as<uint32_t>(), &G.g, (alk_stream)stream_),
+          "hash group-by");
+  }
   SelectCtx c;
   c.st = &st;
   c.a = a;
@@ -846,6 +859,51 @@ bool sym_of(const AstP& e, Sym& out) {
   }
 }
 }  // namespace
+
+// Expected group count of a GROUP BY over n rows: the learned estimator's distinct-key
+// prediction when it is trained and enabled (single-key group-bys over a base table),
+// else the exact bound the zone maps give (the product of the key ranges), at most n.
+uint64_t Engine::expected_groups(Var* a, const std::vector<std::string>& group_cols, uint64_t n) {
+  Var* src = a->kind == Var::Filtered ? var(a->source) : a;
+  if (src->kind != Var::Base) return n;
+  for (auto& g : group_cols)
+    if (!src->has(g) || src->meta[g].type > 2) return n;
+  if (card_use_ && card_mlp_ && group_cols.size() == 1) {
+    const alk_stats saved = stats_;  // the estimate's scan plan is not a scan of the query
+    uint64_t hits = 0, keys = 0;
+    ScanPlan p = plan_scan(a);
+    CardStage cst;
+    cst.p = &p;
+    cst.key_slot = (int32_t)p.slot(group_cols[0]);
+    auto cs = colsegs(p);
+    cst.cs = &cs;
+    BaseCol& bc = basecol(src, group_cols[0]);
+    read_headers(src, group_cols[0], bc);
+    int64_t lo = INT64_MAX, hi = INT64_MIN;
+    for (auto& sg : bc.segs) {
+      lo = std::min(lo, std::min(sg.m.lower, sg.m.upper));
+      hi = std::max(hi, std::max(sg.m.lower, sg.m.upper));
+    }
+    cst.key_range = {lo, hi};
+    const bool ok = card_estimate(cst, &hits, &keys);
+    const uint32_t estimates = stats_.card_estimates;
+    stats_ = saved;
+    stats_.card_estimates = estimates;
+    if (ok) return std::min<uint64_t>(n, keys);
+  }
+  long double bound = 1;
+  for (auto& g : group_cols) {
+    BaseCol& bc = basecol(src, g);
+    read_headers(src, g, bc);
+    int64_t lo = INT64_MAX, hi = INT64_MIN;
+    for (auto& sg : bc.segs) {
+      lo = std::min(lo, std::min(sg.m.lower, sg.m.upper));
+      hi = std::max(hi, std::max(sg.m.lower, sg.m.upper));
+    }
+    bound *= (long double)((uint64_t)hi - (uint64_t)lo) + 1.0L;
+  }
+  return bound < (long double)n ? (uint64_t)bound : n;
+}
 
 bool Engine::dense_select_prepare(Statement& st, SelectCtx& c) {
   if ((flags_ & ALK_SESSION_PLAIN) || !st.grp_cnt) return false;

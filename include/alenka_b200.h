@@ -77,6 +77,8 @@ typedef struct alk_stats {
   uint32_t card_estimates;   /* fused stages sized by the learned estimator */
   uint32_t card_reruns;      /* fused query runs repeated because a size was too small */
   double batch_host_ms[3];   /* batches: wall time of planning, the batched launch, the rest */
+  uint32_t sort_groupbys;    /* group-bys that took the sort-based form */
+  uint32_t pad_;
 } alk_stats;
 int alk_session_stats(alk_session* s, alk_stats* out);
 /* Enable CUDA-event timing of the dominant kernel (adds two event records per launch). */
@@ -190,6 +192,16 @@ int alk_eval(const int64_t* const* d_cols, uint32_t ncols, uint64_t n, const alk
  * first input row of each group (smallest row index). Group order is unspecified;
  * *h_groups receives G. Synchronizes the stream. */
 enum { ALK_AGG_SUM = 0, ALK_AGG_COUNT = 1, ALK_AGG_MIN = 2, ALK_AGG_MAX = 3 };
+/* Sort-based group-by, the reference's own form (stable sort on the keys, head flags,
+ * segmented reduction: operators.cu:367-406, select.cu:499-675), for key spaces too large
+ * for a hash table sized by the rows to pay: the input is first checked for key order
+ * (lexicographic, signed) and sorted (stable LSD radix) only when it is not; groups come
+ * out in key order. Same arguments and outputs as alk_groupby_hash; *h_was_sorted (may be
+ * NULL) = 1 when no sort was needed. Synchronizes the stream. */
+int alk_groupby_sort(const int64_t* const* d_keys, uint32_t nkeys, const int64_t* const* d_vals,
+                     const uint8_t* aggs, uint32_t nvals, uint64_t n, int64_t* const* d_out_keys,
+                     int64_t* const* d_out_vals, uint32_t* d_out_first, uint64_t* h_groups, int* h_was_sorted,
+                     alk_stream stream);
 int alk_groupby_hash(const int64_t* const* d_keys, uint32_t nkeys, const int64_t* const* d_vals,
                      const uint8_t* aggs, uint32_t nvals, uint64_t n, int64_t* const* d_out_keys,
                      int64_t* const* d_out_vals, uint32_t* d_out_first, uint64_t* h_groups,
@@ -417,6 +429,10 @@ int alk_batch_groupby(const alk_gb_query* queries, uint32_t nq, const alk_gb_tun
  * continues. Results are those of running the scripts one at a time. Returns the first
  * failing script's status (alk_session_error names it); the others still run. */
 int alk_session_execute_batch(alk_session* s, const char* const* scripts, uint32_t n);
+/* Group-by form of the operator path: 0 chosen by the expected group count (the learned
+ * estimator's when it is on, else the zone maps' bound; above 2^22 groups the sort-based
+ * form), 1 always hash, 2 always sort. */
+int alk_session_set_groupby(alk_session* s, int mode);
 /* Switches the session between the operator-at-a-time plan (on) and the fused plans. */
 int alk_session_set_plain(alk_session* s, int on);
 /* *out = the launch shape of the last batched group-by; autotune 0/1 turns the per-
