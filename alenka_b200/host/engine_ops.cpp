@@ -2,6 +2,9 @@
 // emit_order / emit_store semantics on top of the operator-level C ABI.
 #include <algorithm>
 #include <chrono>
+#include <thread>
+#include <string_view>
+#include <charconv>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -537,6 +540,7 @@ void Engine::emit_select(Statement& st) {
   // reference's sort-based form, which skips the sort when the rows are in key order)
   const uint64_t groups = grp_cnt ? expected_groups(a, group_cols, R.n) : R.n;
   const bool sorted_gb = groupby_mode_ == 2 || (groupby_mode_ == 0 && groups > kHashGroupsMax);
+  if (timing_) cudaEventRecord(ev0_, stream_);
   if (sorted_gb) {
     int in_order = 0;
     check(alk_groupby_sort(keys.data(), (uint32_t)keys.size(), vals.data(), kinds.data(), (uint32_t)vals.size(), R.n,
@@ -548,6 +552,15 @@ void Engine::emit_select(Statement& st) {
     check(alk_groupby_hash(keys.data(), (uint32_t)keys.size(), vals.data(), kinds.data(), (uint32_t)vals.size(), R.n,
                            okeys.data(), ovals.data(), G.first->as<uint32_t>(), &G.g, (alk_stream)stream_),
           "hash group-by");
+  }
+  if (timing_) {  // the group-by's own device time (both forms synchronize before returning)
+    cudaEventRecord(ev1_, stream_);
+    cudaEventSynchronize(ev1_);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    stats_.hot_kernel_ms += ms;
+    stats_.hot_kernel_launches += 1;
+    stats_.hot_kernel_bytes += R.n * 8 * (keys.size() + vals.size());
   }
   SelectCtx c;
   c.st = &st;
@@ -1413,30 +1426,45 @@ void Engine::emit_store(Statement& st) {
     dicts[c] = &bc.dict;
     widths[c] = bc.meta.width;
   }
-  std::string line;
-  for (size_t i = 0; i < mcount; i++) {
-    line.clear();
-    for (size_t c = 0; c < a->columnNames.size(); c++) {
-      const ColMeta& m = a->meta[a->columnNames[c]];
-      int64_t v = h[c][i];
-      if (!dicts[c]) {
-        if (m.dz) {
-          std::string s = std::to_string(v);
-          while (s.size() <= m.dz) s = '0' + s;
-          s.insert(s.size() - m.dz, ".");
-          line += s;
+  // rows formatted in parallel chunks (integers through std::to_chars), written in order
+  auto format_rows = [&](size_t r0, size_t r1, std::string& out) {
+    char num[32];
+    for (size_t i = r0; i < r1; i++) {
+      for (size_t c = 0; c < a->columnNames.size(); c++) {
+        const ColMeta& m = a->meta[a->columnNames[c]];
+        const int64_t v = h[c][i];
+        if (!dicts[c]) {
+          const auto res = std::to_chars(num, num + sizeof(num), v);
+          std::string_view d(num, (size_t)(res.ptr - num));
+          if (m.dz) {
+            std::string sd(d);
+            while (sd.size() <= m.dz) sd = '0' + sd;
+            sd.insert(sd.size() - m.dz, ".");
+            out += sd;
+          } else {
+            out += d;
+          }
         } else {
-          line += std::to_string(v);
+          const std::string& sv = (v >= 0 && (size_t)v < dicts[c]->size()) ? (*dicts[c])[v] : std::string();
+          out.append(sv.data(), std::min(sv.size(), std::strlen(sv.c_str())));
         }
-      } else {
-        std::string s = (v >= 0 && (size_t)v < dicts[c]->size()) ? (*dicts[c])[v] : std::string();
-        line += s.substr(0, std::min(s.size(), std::strlen(s.c_str())));
+        out += st.sep;
       }
-      line += st.sep;
+      if (i != mcount - 1) out += "\n";
     }
-    if (i != mcount - 1) line += "\n";
-    std::fputs(line.c_str(), fp);
+  };
+  const size_t nthreads =
+      std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), mcount / 65536));
+  std::vector<std::string> parts(nthreads);
+  if (nthreads == 1) {
+    format_rows(0, mcount, parts[0]);
+  } else {
+    std::vector<std::thread> ths;
+    for (size_t t = 0; t < nthreads; t++)
+      ths.emplace_back(format_rows, mcount * t / nthreads, mcount * (t + 1) / nthreads, std::ref(parts[t]));
+    for (auto& th : ths) th.join();
   }
+  for (auto& part : parts) std::fwrite(part.data(), 1, part.size(), fp);
   std::fclose(fp);
 }
 

@@ -342,6 +342,44 @@ def run_batched(args, torch):
     }), flush=True)
 
 
+def run_groupby_high(args, torch):
+    """The high-cardinality group-by: FILTER lineitem BY l_shipdate < d; GROUP BY
+    l_orderkey over a lineitem-shaped table generated in device memory (600M rows, 4 rows
+    per key), timed in its hash form and its sort-based form (in key order: no sort), and
+    in the form the engine picks from the expected group count."""
+    import alenka_b200 as ab
+    from alenka_b200 import workloads as wl
+    rows = int(600_000_000 * args.scale)
+    seg = 10_000_000
+    segs = [seg] * (rows // seg) + ([rows % seg] if rows % seg else [])
+    d = tempfile.mkdtemp(prefix="alenka_gbhigh_")
+    sess = ab.Session(d, resident=True)
+    sess.gen_flat_resident("lineitem", segs, args.seed)
+    cut = wl.flat_cutoff(args.seed)
+    script = (f"LF := FILTER lineitem BY l_shipdate < {cut};\n"
+              "R := SELECT l_orderkey AS k, SUM(l_quantity) AS q, SUM(l_extendedprice*(1-l_discount)) AS rev, "
+              "COUNT(l_orderkey) AS c FROM LF GROUP BY l_orderkey;\n"
+              "STORE R INTO 'gbh.txt' USING ('|');\n")
+    out = {}
+    for name, mode in (("auto", 0), ("hash", 1), ("sort", 2)):
+        sess.set_groupby(mode)
+        for _ in range(max(1, args.warmup // 2)):
+            sess.execute(script)
+        sess.set_timing(True)
+        ms, acc = _steps(sess, lambda: sess.execute(script), max(1, args.steps // 4), torch)
+        sess.set_timing(False)
+        gb_ms = acc["hot_ms"] / max(1, acc["hot_launches"])
+        out[name] = {"ms_per_query": ms, "rows_per_s": rows / (ms / 1000.0), "groupby_ms": gb_ms,
+                     "groupby_rows_per_s": rows / (gb_ms / 1000.0) if gb_ms else None,
+                     "sort_form": bool(sess.stats().sort_groupbys)}
+    sess.close()
+    print(json.dumps({"metric": "fact rows/s, filter + GROUP BY l_orderkey (high cardinality)",
+                      "value": out["auto"]["rows_per_s"], "unit": "rows/s", "n_gpus": 1, "dtype": "int64",
+                      "data": "synthetic (generated in device memory)",
+                      "config": {"workload": f"lineitem {rows} rows, {len(segs)} segments, ~{rows // 4} keys",
+                                 "forms": out}}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -354,7 +392,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fused-only", action="store_true",
                     help="time only the resident fused plan (profiling runs)")
-    ap.add_argument("--workload", default="three_way", choices=["three_way", "batched"],
+    ap.add_argument("--workload", default="three_way", choices=["three_way", "batched", "groupby_high"],
                     help="three_way: the filter -> join -> group-by pipeline (default); batched: many "
                          "single-table filter + group-by queries per step")
     ap.add_argument("--queries", type=int, default=256)
@@ -372,9 +410,9 @@ def main():
         return
     import torch
     torch.cuda.set_device(local)
-    if args.workload == "batched":
+    if args.workload in ("batched", "groupby_high"):
         if rank == 0:
-            run_batched(args, torch)
+            (run_batched if args.workload == "batched" else run_groupby_high)(args, torch)
         return
     dist = None
     if world > 1:
