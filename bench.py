@@ -161,6 +161,18 @@ def profiled_traffic(name):
     return None
 
 
+def profiled_traffic_rows(name):
+    """Rows the profiled launch covered, when the summary states them (for scaling)."""
+    p = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(p):
+            if line.strip().startswith("traffic_rows_per_launch:"):
+                return int(line.split(":")[1].strip())
+    except OSError:
+        pass
+    return None
+
+
 def ensure_data(base, scale, seed):
     from alenka_b200 import workloads as wl
     d = os.path.join(base, f"threeway_s{scale}_seed{seed}")
@@ -321,7 +333,9 @@ def run_batched(args, torch):
         pl_ms = acc["hot_ms"] / acc["hot_launches"]
         achieved = pl_bytes / (pl_ms / 1000.0) / 1e9
         hot = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-               "traffic": profiled_traffic("batched_groupby_flat.md"),
+               "traffic": (profiled_traffic("batched_groupby_flat.md") * rows // profiled_traffic_rows(
+                   "batched_groupby_flat.md")) if profiled_traffic_rows("batched_groupby_flat.md") else None,
+               "traffic_note": "ncu capture at 120M rows, scaled by rows to this batch",
                "kernel": "k_gb_tma (batched filter + dense group-by, one launch per batch)",
                "algorithmic_bytes": "scanned rows x stored widths of the columns the queries read",
                "algorithmic_bytes_per_launch": int(pl_bytes), "avg_launch_ms": pl_ms,
