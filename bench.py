@@ -258,10 +258,15 @@ def timed_steps(sess, script, steps, torch, dist):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist, torch, "cuda")
     return ms, acc
+
+
+def max_over_ranks(ms, dist, torch, device):
+    """The slowest rank's milliseconds: every replica's step must be done for the job's."""
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def _steps(sess, fn, steps, torch):

@@ -198,3 +198,37 @@ def test_oracle_three_way_matches_numpy(tmp_path):
     for line, (k, (r, c)) in zip(got, rows):
         f = line.split("|")
         assert int(f[0]) == k and int(f[1]) == odate[k] and int(f[3].replace(".", "")) == r and int(f[4]) == c
+
+
+def _replica_rank(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # each replica reports its own time; the job's time is the slowest replica's
+        ms = bench.max_over_ranks(1.0 + rank * 2.5, dist, torch, "cpu")
+        q.put((rank, ms))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_replica_timing_is_max_over_ranks_gloo():
+    """The N>1 bench path (replicas, no data-path collective): the per-step time every
+    rank prints is the maximum over ranks, computed with the same all-reduce on gloo."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_replica_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    got = sorted(q.get(timeout=10) for _ in range(2))
+    assert got == [(0, 3.5), (1, 3.5)]
