@@ -1285,6 +1285,9 @@ void Engine::multijoin(Statement& st, const std::string& s, const std::string& j
     throw EngineError(ALK_ERR_ARG, "Couldn't find column " + f1);
   }
   if (left->meta[colname1].type != right->meta[colname2].type) unsupported("join of different column types");
+  // char keys are dictionary codes: codes of two different dictionaries do not compare
+  if (left->meta[colname1].type == 2 && left->meta[colname1].string_map != right->meta[colname2].string_map)
+    unsupported("join on char columns of different dictionaries");
   std::vector<std::string> rfields, lfields;
   for (auto& n : c->columnNames)
     if (!left->has(n) && right->has(n)) rfields.push_back(n);
@@ -1937,6 +1940,10 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
   for (auto& g : group_cols)
     if (!jv.has(g) || origin(src_of[g]) == fact) fallback("group key outside the build side");
   const std::string& build_key = st2.rkey;  // unique key of the last build stage
+  for (const StepInfo* sp : {&st1, &st2})  // the stages join on integer key values
+    if ((sp->rkey.size() && origin(sp->rkey)->meta[sp->rkey].type == 2) ||
+        (sp->lkey.size() && origin(sp->lkey)->meta[sp->lkey].type == 2))
+      fallback("join on char columns");
   bool key_grouped = false;
   for (auto& g : group_cols)
     if (src_of[g] == build_key) key_grouped = true;
