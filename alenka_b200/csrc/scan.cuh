@@ -200,10 +200,12 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 // Bounded wait of one thread for a phase; false when the limit expired.
+// (Used by the producers, which mostly wait for a consumer to free a stage: they back
+// off quickly so that their polling takes few issue slots from the consumers.)
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   for (uint32_t spins = 0; spins < kWaitLimit; spins++) {
     if (mbar_try_wait(bar, parity)) return true;
-    if (spins > 16) __nanosleep(32);
+    if (spins > 2) __nanosleep(128);
   }
   return false;
 }
