@@ -106,6 +106,8 @@ def _declare(L):
     L.alk_session_card_train.argtypes = [vp, u64, u64, u32, u32, c.c_float, u64, fp]
     L.alk_session_card_predict.argtypes = [vp, fp, u64, fp]
     L.alk_session_card_forget.argtypes = [vp]
+    L.alk_session_card_save.argtypes = [vp, c.c_char_p]
+    L.alk_session_card_load.argtypes = [vp, c.c_char_p]
     L.alenkaInit.argtypes = [c.POINTER(c.c_char_p)]
     L.alenkaInit.restype = None
     L.alenkaExecute.argtypes = [c.c_char_p]
@@ -217,6 +219,16 @@ class Session:
         if rc != ALK_OK:
             raise AlenkaError(rc, "estimator prediction failed")
         return y
+
+    def card_save(self, path):
+        rc = lib().alk_session_card_save(self._h, str(path).encode())
+        if rc != ALK_OK:
+            raise AlenkaError(rc, lib().alk_session_error(self._h).decode())
+
+    def card_load(self, path):
+        rc = lib().alk_session_card_load(self._h, str(path).encode())
+        if rc != ALK_OK:
+            raise AlenkaError(rc, lib().alk_session_error(self._h).decode())
 
     def card_forget(self):
         lib().alk_session_card_forget(self._h)

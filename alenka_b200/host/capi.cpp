@@ -134,6 +134,20 @@ int alk_session_card_predict(alk_session* s, const float* h_x, uint64_t n, float
   return ALK_OK;
 }
 
+int alk_session_card_save(alk_session* s, const char* path) {
+  if (!s || !path) return ALK_ERR_ARG;
+  int rc = s->eng->card_save(path);
+  s->err = s->eng->error();
+  return rc;
+}
+
+int alk_session_card_load(alk_session* s, const char* path) {
+  if (!s || !path) return ALK_ERR_ARG;
+  int rc = s->eng->card_load(path);
+  s->err = s->eng->error();
+  return rc;
+}
+
 int alk_session_card_forget(alk_session* s) {
   if (!s) return ALK_ERR_ARG;
   s->eng->card_forget();

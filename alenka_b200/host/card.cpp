@@ -6,6 +6,7 @@
 // with the exact counts, so results never depend on it.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <numeric>
 #include <random>
@@ -331,6 +332,59 @@ int Engine::card_train(uint64_t first, uint64_t count, uint32_t epochs, uint32_t
     return e.code;
   }
   return ALK_OK;
+}
+
+// The trained network as a file: "ALKMLP1\0", the parameter count (u32), then the FP32
+// master parameters.
+int Engine::card_save(const std::string& path) {
+  if (!card_mlp_) {
+    err_ = "the cardinality estimator is not trained";
+    return ALK_ERR_ARG;
+  }
+  const uint32_t n = alk_mlp_param_count();
+  std::vector<float> p(n);
+  int rc = alk_mlp_params(card_mlp_, p.data(), nullptr, (alk_stream)stream_);
+  if (rc) return rc;
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) {
+    err_ = "cannot write " + path;
+    return ALK_ERR_IO;
+  }
+  const char magic[8] = {'A', 'L', 'K', 'M', 'L', 'P', '1', 0};
+  bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(&n, 4, 1, f) == 1 && std::fwrite(p.data(), 4, n, f) == n;
+  ok = std::fclose(f) == 0 && ok;
+  if (!ok) {
+    err_ = "cannot write " + path;
+    return ALK_ERR_IO;
+  }
+  return ALK_OK;
+}
+
+int Engine::card_load(const std::string& path) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) {
+    err_ = "cannot read " + path;
+    return ALK_ERR_IO;
+  }
+  char magic[8] = {0};
+  uint32_t n = 0;
+  std::vector<float> p;
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "ALKMLP1", 8) == 0 &&
+            std::fread(&n, 4, 1, f) == 1 && n == alk_mlp_param_count();
+  if (ok) {
+    p.resize(n);
+    ok = std::fread(p.data(), 4, n, f) == n;
+  }
+  std::fclose(f);
+  if (!ok) {
+    err_ = path + ": not an estimator file of this network";
+    return ALK_ERR_IO;
+  }
+  if (!card_mlp_) {
+    int rc = alk_mlp_create(1, &card_mlp_, (alk_stream)stream_);
+    if (rc) return rc;
+  }
+  return alk_mlp_set_params(card_mlp_, p.data(), (alk_stream)stream_);
 }
 
 void Engine::card_forget() {

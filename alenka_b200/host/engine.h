@@ -185,6 +185,8 @@ class Engine {
                  float* loss);
   void card_forward(const float* h_x, uint64_t n, float* h_y);
   void card_forget();
+  int card_save(const std::string& path);
+  int card_load(const std::string& path);
 
   // ---- used by the planner / operators ----
   Var* var(const std::string& n);

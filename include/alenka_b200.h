@@ -499,6 +499,10 @@ int alk_session_card_train(alk_session* s, uint64_t first, uint64_t count, uint3
                            float lr, uint64_t seed, float* h_loss);
 /* Estimator outputs for n feature rows (host arrays). */
 int alk_session_card_predict(alk_session* s, const float* h_x, uint64_t n, float* h_y);
+/* The trained estimator to a file and back (FP32 master parameters), so that a session
+ * can use a network trained in another one. */
+int alk_session_card_save(alk_session* s, const char* path);
+int alk_session_card_load(alk_session* s, const char* path);
 /* Forget the exact counts recorded by earlier runs and the captured graphs, so that the
  * next run of a query is a first run again. */
 int alk_session_card_forget(alk_session* s);

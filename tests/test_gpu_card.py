@@ -308,3 +308,25 @@ def test_record_mode_keeps_results_exact(card_tables):
             s.execute(script)
             assert s.stats().plan == 1
         assert open(os.path.join(d, "qr.txt"), "rb").read() == want
+
+
+def test_estimator_save_and_load(card_tables, tmp_path):
+    d = card_tables
+    with ab.Session(d) as s:
+        s.card_mode(record=True)
+        for q in range(40):
+            _run(s, wl.card_script(5000 + q, out="qs.txt"))
+        x, _, _ = s.card_records()
+        s.card_train(0, len(x), epochs=3, batch=128, lr=1e-3, seed=9)
+        want = s.card_predict(x[:500])
+        f = tmp_path / "card.bin"
+        s.card_save(f)
+    with ab.Session(d) as s2:
+        with pytest.raises(ab.AlenkaError):
+            s2.card_predict(x[:10])  # nothing trained or loaded yet
+        s2.card_load(f)
+        np.testing.assert_array_equal(s2.card_predict(x[:500]), want)
+        bad = tmp_path / "bad.bin"
+        bad.write_bytes(b"not a network")
+        with pytest.raises(ab.AlenkaError):
+            s2.card_load(bad)
