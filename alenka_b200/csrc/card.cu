@@ -3,7 +3,7 @@
 // trained on the GPU by these kernels (forward, backward, Adam). The network predicts
 // per-segment log-selectivities that size the fused stages' tables and survivor lists
 // on a query's first run; the exact counts the stages report remain the fallback and
-// the judge of its error. No counterpart in the reference (it sizes from the free
+// the measure of its error. No counterpart in the reference (it sizes from the free
 // memory, cm.cu:3184).
 #include <cuda_bf16.h>
 
