@@ -318,11 +318,15 @@ __global__ void k_gb_tma(const __grid_constant__ GbArgs g) {
   if (cur_item != 0xffffffffu && lane == 0 && surv) atomicAdd(g.item_rows + cur_item, surv);
 }
 
-__global__ void k_gb_init(int64_t* acc, uint64_t nslots, const uint32_t* kinds, uint32_t nacc) {
-  const uint64_t n = nslots * nacc;
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t k = kinds[i / nslots];
-    acc[i] = k == ALK_AGG_MIN ? INT64_MAX : k == ALK_AGG_MAX ? INT64_MIN : 0;
+// Every query's accumulators [nacc][nslots] at the identity of their aggregate: one
+// launch for the batch, query blockIdx.y.
+__global__ void k_gb_init(const GbQuery* queries) {
+  const GbQuery& q = queries[blockIdx.y];
+  const uint32_t n = q.nslots * q.nacc;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t a = i / q.nslots;
+    const uint32_t k = a < q.nagg ? q.agg[a].kind : (uint32_t)ALK_AGG_COUNT;
+    q.acc[i] = k == ALK_AGG_MIN ? INT64_MAX : k == ALK_AGG_MAX ? INT64_MIN : 0;
   }
 }
 
@@ -353,7 +357,6 @@ int alk_batch_groupby(const alk_gb_query* qs, uint32_t nq, const alk_gb_tuning* 
   std::vector<GbQuery> hq(nq);
   std::vector<GbItem> items;
   std::vector<uint32_t> item_tile;
-  std::vector<uint32_t> kinds_all;
   std::vector<std::pair<uint32_t, uint32_t>> item_src;  // (query, segment) of each item
   uint32_t max_acc = 1, max_stage = 16;
   const uint32_t cw = tune && tune->consumer_warps ? tune->consumer_warps : 8;
@@ -401,7 +404,6 @@ int alk_batch_groupby(const alk_gb_query* qs, uint32_t nq, const alk_gb_tuning* 
       if (cj[c].slot >= a.ncols) return ALK_ERR_ARG;
       q.conj[c] = Conj{cj[c].mul, cj[c].k, cj[c].slot, cj[c].op};
     }
-    for (uint32_t k = 0; k <= a.nagg; k++) kinds_all.push_back(k < a.nagg ? a.agg[k].kind : ALK_AGG_COUNT);
     // work items: the scanned segments
     for (uint32_t gi = 0; gi < a.nseg; gi++) {
       const uint8_t mode = a.seg_mode ? a.seg_mode[gi] : 2;
@@ -431,19 +433,17 @@ int alk_batch_groupby(const alk_gb_query* qs, uint32_t nq, const alk_gb_tuning* 
   if (ntiles >= 0xffffffffull) return ALK_ERR_TOO_LARGE;
   item_tile.push_back((uint32_t)ntiles);
   const uint32_t nitems = (uint32_t)items.size();
-  // device copies: queries, items, item tiles, kinds, item survivor counts, error flag
+  // device copies: queries, items, item tiles, item survivor counts, error flag
   const size_t o_q = 0;
   const size_t o_items = (o_q + sizeof(GbQuery) * nq + 255) & ~size_t(255);
   const size_t o_tile = (o_items + sizeof(GbItem) * nitems + 255) & ~size_t(255);
-  const size_t o_kinds = (o_tile + 4 * item_tile.size() + 255) & ~size_t(255);
-  const size_t o_rows = (o_kinds + 4 * kinds_all.size() + 255) & ~size_t(255);
+  const size_t o_rows = (o_tile + 4 * item_tile.size() + 255) & ~size_t(255);
   const size_t o_err = o_rows + 8 * (size_t)std::max<uint32_t>(nitems, 1);
   const size_t bytes = o_err + 16;
   std::vector<uint8_t> hb(o_rows, 0);
   std::memcpy(&hb[o_q], hq.data(), sizeof(GbQuery) * nq);
   if (nitems) std::memcpy(&hb[o_items], items.data(), sizeof(GbItem) * nitems);
   std::memcpy(&hb[o_tile], item_tile.data(), 4 * item_tile.size());
-  std::memcpy(&hb[o_kinds], kinds_all.data(), 4 * kinds_all.size());
   uint8_t* db = nullptr;
   CK(cudaMallocAsync((void**)&db, bytes, s));
   cudaError_t ue;
@@ -453,13 +453,10 @@ int alk_batch_groupby(const alk_gb_query* qs, uint32_t nq, const alk_gb_tuning* 
   CK(cudaMemsetAsync(db + o_rows, 0, bytes - o_rows, s));
   // accumulators: every query's [nacc][nslots] starts at the identity of its aggregate
   {
-    size_t k0 = 0;
-    for (uint32_t qi = 0; qi < nq; qi++) {
-      k_gb_init<<<std::max<uint32_t>(1, std::min<uint32_t>((hq[qi].nslots * hq[qi].nacc + 255) / 256, 64)), 256, 0,
-                  s>>>(hq[qi].acc, hq[qi].nslots, (const uint32_t*)(db + o_kinds) + k0, hq[qi].nacc);
-      k0 += hq[qi].nacc;
-      alk::g_kernel_launches++;
-    }
+    uint32_t most = 1;
+    for (uint32_t qi = 0; qi < nq; qi++) most = std::max(most, hq[qi].nslots * hq[qi].nacc);
+    k_gb_init<<<dim3((most + 255) / 256, nq), 256, 0, s>>>((const GbQuery*)(db + o_q));
+    alk::g_kernel_launches++;
     CK(cudaGetLastError());
   }
   GbArgs g{};

@@ -385,7 +385,7 @@ struct SelectCtx {
   ScanPlan plan;
   std::vector<alk_colseg> cs;
   alk_gb_query q{};
-  DevBufP acc;
+  size_t acc_words = 0;       // accumulators: slots x (aggregates + 1)
   std::vector<int64_t> hacc;  // the accumulators on the host
   std::vector<uint64_t> seg_rows;
   std::vector<int64_t> kmin, kspan;
@@ -1013,8 +1013,7 @@ bool Engine::dense_select_prepare(Statement& st, SelectCtx& c) {
   q.nseg = src->segCount;
   q.seg_mode = c.plan.mode.data();
   q.pred = c.plan.has_pred ? &c.plan.pred : nullptr;
-  c.acc = mkbuf(nslots * (q.nagg + 1) * 8, stream_);
-  q.d_acc = c.acc->as<int64_t>();
+  c.acc_words = nslots * (q.nagg + 1);  // the accumulators live in the batch's arena
   c.seg_rows.assign(src->segCount, 0);
   q.h_seg_rows = c.seg_rows.data();
   return true;
@@ -1025,6 +1024,15 @@ bool Engine::dense_select_prepare(Statement& st, SelectCtx& c) {
 // signature runs under each candidate shape (every run is complete and exact; the last
 // one's results stand) and the fastest shape is kept for later batches.
 void Engine::dense_select_run(const std::vector<SelectCtx*>& cs) {
+  // every select's accumulators in one device buffer: one allocation, one copy back
+  size_t total = 0;
+  std::vector<size_t> at(cs.size());
+  for (size_t i = 0; i < cs.size(); i++) {
+    at[i] = total;
+    total += cs[i]->acc_words;
+  }
+  auto arena = mkbuf(std::max<size_t>(total, 1) * 8, stream_);
+  for (size_t i = 0; i < cs.size(); i++) cs[i]->q.d_acc = arena->as<int64_t>() + at[i];
   std::vector<alk_gb_query> qs;
   std::string sig = std::to_string(cs.size());
   uint64_t rows = 0;
@@ -1068,15 +1076,15 @@ void Engine::dense_select_run(const std::vector<SelectCtx*>& cs) {
                           (alk_stream)stream_),
         "batched group-by");
   last_tuning_ = used;
-  // every select's accumulators back in one synchronisation
-  for (auto* c : cs) {
-    c->hacc.resize(c->acc->bytes() / 8);
-    ck(cudaMemcpyAsync(c->hacc.data(), c->acc->as<void>(), c->hacc.size() * 8, cudaMemcpyDeviceToHost, stream_),
-       "d2h");
-    stats_.d2h_bytes += c->hacc.size() * 8;
-  }
+  // every select's accumulators back in one copy and one synchronisation
+  std::vector<int64_t> all(total);
+  if (total) ck(cudaMemcpyAsync(all.data(), arena->as<void>(), total * 8, cudaMemcpyDeviceToHost, stream_), "d2h");
+  stats_.d2h_bytes += total * 8;
   ck(cudaStreamSynchronize(stream_), "sync");
-  for (auto* c : cs) c->acc.reset();
+  for (size_t i = 0; i < cs.size(); i++) {
+    const size_t n = (i + 1 < cs.size() ? at[i + 1] : total) - at[i];
+    cs[i]->hacc.assign(all.begin() + at[i], all.begin() + at[i] + n);
+  }
   if (tm.launches) {
     // algorithmic bytes: every scanned row's stored values of the columns the queries read
     uint64_t bytes = 0;
