@@ -28,6 +28,8 @@ struct GbQuery {
   uint64_t key_mul[2];
   uint64_t key_span[2];
   uint32_t nslots, nacc;  // nacc = nagg + 1: the row count is the last accumulator
+  int32_t count_agg;      // an aggregate that is COUNT (it doubles as the row count), or -1
+  uint32_t pad;
   alk_gb_agg agg[kGbAggs];
   int64_t* acc;  // [nacc][nslots]
 };
@@ -43,7 +45,7 @@ struct GbArgs {
   const GbQuery* queries;
   uint32_t nst, stage_bytes;  // stages in flight, bytes of one stage
   uint32_t cw;                // consumer warps; a tile is cw * 256 rows
-  uint32_t max_acc;           // private accumulators per thread
+  uint32_t max_acc;           // private accumulators per thread: (slots + 1) x (aggregates + 1)
   unsigned long long* item_rows;  // survivors per item
   int* err;
 };
@@ -64,8 +66,9 @@ __device__ void gb_flush(const GbQuery& q, int64_t* priv, uint32_t lane) {
   for (uint32_t j = 0; j < q.nslots * q.nacc; j++) {
     const uint32_t a = j % q.nacc, slot = j / q.nacc;
     const uint32_t kind = a < q.nagg ? q.agg[a].kind : (uint32_t)ALK_AGG_COUNT;
-    int64_t v = priv[j * 32 + lane];
-    priv[j * 32 + lane] = kind == ALK_AGG_MIN ? INT64_MAX : kind == ALK_AGG_MAX ? INT64_MIN : 0;
+    // a query with a COUNT aggregate keeps no separate row count: it is that aggregate
+    const uint32_t src = (a == q.nagg && q.count_agg >= 0) ? j - a + (uint32_t)q.count_agg : j;
+    int64_t v = priv[src * 32 + lane];  // gb_clear resets the accumulators for the next query
     for (int o = 16; o; o >>= 1) {
       const int64_t w = __shfl_xor_sync(0xffffffffu, v, o);
       v = kind == ALK_AGG_MIN ? min(v, w) : kind == ALK_AGG_MAX ? max(v, w) : (int64_t)((uint64_t)v + (uint64_t)w);
@@ -239,7 +242,7 @@ __global__ void k_gb_tma(const __grid_constant__ GbArgs g) {
     // fold the survivors a column at a time over the thread's 8 rows: the group slot in
     // 32-bit arithmetic (stored key + (segment base - key minimum), each below its span),
     // then every aggregate input into the slot's accumulators, private to the lane
-    if (live) {
+    if (__any_sync(0xffffffffu, live)) {
       uint32_t slot[kItems];
 #pragma unroll
       for (int k = 0; k < kItems; k++) slot[k] = 0;
@@ -256,25 +259,30 @@ __global__ void k_gb_tma(const __grid_constant__ GbArgs g) {
         } else {
           load_raw32<32>(buf + coff[q.key_col[j]], d.bits, r0, x);
         }
+        uint32_t bad = 0;
 #pragma unroll
         for (int k = 0; k < kItems; k++) {
           const uint32_t o = x[k] + kd;
-          if (o >= span && ((live >> k) & 1)) {  // outside the zone maps' range: the plan is wrong
-            atomicExch(g.err, ALK_ERR_ARG);
-            live &= ~(1u << k);
-          }
+          bad |= (o >= span ? 1u : 0u) << k;
           slot[k] += o * mul;
+        }
+        bad &= live;
+        if (bad) {  // a key outside the zone maps' range: the plan is wrong
+          atomicExch(g.err, ALK_ERR_ARG);
+          live &= ~bad;
         }
       }
       const uint32_t nagg = q.nagg, stride = q.nacc * 32;
       int64_t* base = priv + lane;
+      // rows that did not pass update the spare slot (index nslots): no branch per row
+#pragma unroll
+      for (int k = 0; k < kItems; k++) slot[k] = ((live >> k) & 1) ? slot[k] * stride : q.nslots * stride;
       for (uint32_t a = 0; a < nagg; a++) {
         const uint32_t kind = q.agg[a].kind;
         int64_t* pa = base + a * 32;
         if (kind == ALK_AGG_COUNT) {
 #pragma unroll
-          for (int k = 0; k < kItems; k++)
-            if ((live >> k) & 1) pa[slot[k] * stride] += 1;
+          for (int k = 0; k < kItems; k++) pa[slot[k]] += 1;
           continue;
         }
         const int32_t ca = q.agg[a].a, cb = q.agg[a].b;
@@ -297,19 +305,22 @@ __global__ void k_gb_tma(const __grid_constant__ GbArgs g) {
 #pragma unroll
           for (int k = 0; k < kItems; k++) v[k] *= (w[k] + lb) * bm + bc;
         }
+        if (kind == ALK_AGG_MIN) {
 #pragma unroll
-        for (int k = 0; k < kItems; k++) {
-          if (!((live >> k) & 1)) continue;
-          int64_t& acc = pa[slot[k] * stride];
-          if (kind == ALK_AGG_MIN) acc = min(acc, (int64_t)v[k]);
-          else if (kind == ALK_AGG_MAX) acc = max(acc, (int64_t)v[k]);
-          else acc = (int64_t)((uint64_t)acc + v[k]);
+          for (int k = 0; k < kItems; k++) pa[slot[k]] = min(pa[slot[k]], (int64_t)v[k]);
+        } else if (kind == ALK_AGG_MAX) {
+#pragma unroll
+          for (int k = 0; k < kItems; k++) pa[slot[k]] = max(pa[slot[k]], (int64_t)v[k]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < kItems; k++) pa[slot[k]] = (int64_t)((uint64_t)pa[slot[k]] + v[k]);
         }
       }
-      int64_t* pc = base + nagg * 32;
+      if (q.count_agg < 0) {
+        int64_t* pc = base + nagg * 32;
 #pragma unroll
-      for (int k = 0; k < kItems; k++)
-        if ((live >> k) & 1) pc[slot[k] * stride] += 1;
+        for (int k = 0; k < kItems; k++) pc[slot[k]] += 1;
+      }
     }
     __syncwarp();
     if (lane == 0) mbar_arrive(&s_empty[st]);
@@ -384,8 +395,13 @@ int alk_batch_groupby(const alk_gb_query* qs, uint32_t nq, const alk_gb_tuning* 
     }
     q.nslots = (uint32_t)nslots;
     q.nacc = a.nagg + 1;
+    q.count_agg = -1;
+    for (uint32_t k = 0; k < a.nagg; k++)
+      if (a.agg[k].kind == ALK_AGG_COUNT && q.count_agg < 0) q.count_agg = (int32_t)k;
     if (nslots * q.nacc > 64) return ALK_ERR_UNSUPPORTED;  // private accumulators per thread
-    max_acc = std::max<uint32_t>(max_acc, (uint32_t)(nslots * q.nacc));
+    // one more slot per lane takes the updates of rows that did not pass, so that the
+    // updates need no branch
+    max_acc = std::max<uint32_t>(max_acc, (uint32_t)((nslots + 1) * q.nacc));
     for (uint32_t k = 0; k < a.nagg; k++) {
       const alk_gb_agg& ag = a.agg[k];
       if (ag.kind > ALK_AGG_MAX) return ALK_ERR_ARG;
