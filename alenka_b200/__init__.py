@@ -96,6 +96,7 @@ def _declare(L):
     L.alk_card_count.argtypes = [vp, u32, u32, vp, vp, vp, i32, i32, i64, i64, c.POINTER(u64), vp]
     L.alk_session_execute_batch.argtypes = [vp, c.POINTER(c.c_char_p), u32]
     L.alk_session_tuning.argtypes = [vp, c.POINTER(Tuning), i32]
+    L.alk_session_set_tuning.argtypes = [vp, c.POINTER(Tuning)]
     L.alk_session_set_plain.argtypes = [vp, i32]
     L.alk_session_set_groupby.argtypes = [vp, i32]
     L.alk_session_gen_flat_resident.argtypes = [vp, c.c_char_p, c.POINTER(u32), u32, u64, u64]
@@ -185,6 +186,14 @@ class Session:
         t = Tuning()
         lib().alk_session_tuning(self._h, ctypes.byref(t), -1 if autotune is None else int(bool(autotune)))
         return (t.consumer_warps, t.stages, t.blocks_per_sm)
+
+    def set_tuning(self, shape=None):
+        """Fixes the batched group-by's launch shape (consumer_warps, stages,
+        blocks_per_sm); None returns to the autotuner."""
+        t = Tuning(*shape) if shape else None
+        rc = lib().alk_session_set_tuning(self._h, ctypes.byref(t) if t else None)
+        if rc:
+            raise AlenkaError(rc, "bad launch shape %r" % (shape,))
 
     # ---- learned cardinality estimator
     def card_mode(self, record=False, use=False):

@@ -107,6 +107,13 @@ int alk_session_tuning(alk_session* s, alk_gb_tuning* out, int autotune) {
   return ALK_OK;
 }
 
+int alk_session_set_tuning(alk_session* s, const alk_gb_tuning* shape) {
+  if (!s) return ALK_ERR_ARG;
+  if (shape && shape->consumer_warps && shape->consumer_warps != 4 && shape->consumer_warps != 8) return ALK_ERR_ARG;
+  s->eng->set_tuning(shape ? *shape : alk_gb_tuning{});
+  return ALK_OK;
+}
+
 int alk_session_card_mode(alk_session* s, int record, int use) {
   if (!s) return ALK_ERR_ARG;
   return s->eng->card_mode(record != 0, use != 0);

@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <array>
+#include <functional>
 #include <map>
 #include <memory>
 #include <set>
@@ -170,6 +171,7 @@ class Engine {
                         uint64_t row_base);
   const alk_gb_tuning& last_tuning() const { return last_tuning_; }
   void set_autotune(bool on) { autotune_ = on; }
+  void set_tuning(const alk_gb_tuning& t) { fixed_tuning_ = t; }
   // group-by form: 0 chosen by the expected group count, 1 hash, 2 sort
   void set_groupby_mode(int m) { groupby_mode_ = m; }
   void set_plain(bool on) { flags_ = on ? (flags_ | ALK_SESSION_PLAIN) : (flags_ & ~ALK_SESSION_PLAIN); }
@@ -259,11 +261,22 @@ class Engine {
   std::set<std::string> fused_seen_;
   std::set<std::string> fused_nograph_;  // queries whose capture failed
   std::string cur_script_;
+  // a batch's final STOREs: formatted at once, written together after the batch (the
+  // file creations dominate a small result's store) on several threads
+  struct PendingWrite {
+    std::string path, data;
+    size_t run;
+  };
+  std::vector<PendingWrite>* deferred_writes_ = nullptr;
+  size_t deferred_run_ = 0;
+  void write_files(const std::vector<PendingWrite>& writes,
+                   const std::function<void(size_t, const std::string&)>& failed);
   bool big_fetch_ = false;  // bring every candidate back (ties beyond the first copy)
   // batched group-by launch shapes by workload signature (autotuned), and the last used
   std::map<std::string, alk_gb_tuning> gb_tune_;
   alk_gb_tuning last_tuning_{};
   bool autotune_ = true;
+  alk_gb_tuning fixed_tuning_{};  // consumer_warps 0: not fixed
   int groupby_mode_ = 0;
   static constexpr uint64_t kHashGroupsMax = 1ull << 22;
   uint64_t expected_groups(Var* a, const std::vector<std::string>& group_cols, uint64_t n);

@@ -1,6 +1,7 @@
 // Operator execution of the host engine: emit_filter / emit_select / emit_join /
 // emit_order / emit_store semantics on top of the operator-level C ABI.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <thread>
 #include <string_view>
@@ -1045,7 +1046,9 @@ void Engine::dense_select_run(const std::vector<SelectCtx*>& cs) {
   }
   auto it = gb_tune_.find(sig);
   alk_gb_tuning best{};
-  if (it != gb_tune_.end()) {
+  if (fixed_tuning_.consumer_warps) {
+    best = fixed_tuning_;
+  } else if (it != gb_tune_.end()) {
     best = it->second;
   } else if (rows >= (64ull << 20) && autotune_) {
     // candidates, timed with events around the launch on the engine stream
@@ -1421,8 +1424,11 @@ void Engine::emit_store(Statement& st) {
   }
   std::string path = st.f;
   if (path.empty() || path[0] != '/') path = dir_ + "/" + path;
-  FILE* fp = std::fopen(path.c_str(), "w");
-  if (!fp) throw EngineError(ALK_ERR_IO, "Could not open file " + path);
+  FILE* fp = nullptr;
+  if (!deferred_writes_) {
+    fp = std::fopen(path.c_str(), "w");
+    if (!fp) throw EngineError(ALK_ERR_IO, "Could not open file " + path);
+  }
   std::vector<const std::vector<std::string>*> dicts(a->columnNames.size(), nullptr);
   std::vector<uint32_t> widths(a->columnNames.size(), 0);
   for (size_t c = 0; c < a->columnNames.size(); c++) {
@@ -1474,6 +1480,12 @@ void Engine::emit_store(Statement& st) {
     for (size_t t = 0; t < nthreads; t++)
       ths.emplace_back(format_rows, mcount * t / nthreads, mcount * (t + 1) / nthreads, std::ref(parts[t]));
     for (auto& th : ths) th.join();
+  }
+  if (deferred_writes_) {
+    PendingWrite w{path, std::string(), deferred_run_};
+    for (auto& part : parts) w.data += part;
+    deferred_writes_->push_back(std::move(w));
+    return;
   }
   for (auto& part : parts) std::fwrite(part.data(), 1, part.size(), fp);
   std::fclose(fp);
@@ -1529,6 +1541,39 @@ void Engine::drop_dead(const std::map<std::string, size_t>& last, size_t i) {
 // Many scripts with one launch for their group-bys: each script runs up to its first
 // SELECT that the dense group-by takes, every such SELECT then runs in one batched
 // launch, and each script continues from there. Scripts without one run as usual.
+// Writes the files on up to 16 threads; writes to one path stay in order on one thread.
+void Engine::write_files(const std::vector<PendingWrite>& writes,
+                         const std::function<void(size_t, const std::string&)>& failed) {
+  std::map<std::string, std::vector<size_t>> by_path;
+  for (size_t k = 0; k < writes.size(); k++) by_path[writes[k].path].push_back(k);
+  std::vector<const std::vector<size_t>*> groups;
+  for (auto& p : by_path) groups.push_back(&p.second);
+  std::vector<char> ok(writes.size(), 1);
+  std::atomic<size_t> next{0};
+  auto worker = [&] {
+    for (size_t g; (g = next.fetch_add(1)) < groups.size();)
+      for (size_t k : *groups[g]) {
+        FILE* fp = std::fopen(writes[k].path.c_str(), "w");
+        if (!fp) {
+          ok[k] = 0;
+          continue;
+        }
+        std::fwrite(writes[k].data.data(), 1, writes[k].data.size(), fp);
+        std::fclose(fp);
+      }
+  };
+  const size_t nth = std::min<size_t>(groups.size(), std::min<size_t>(16, std::max(1u, std::thread::hardware_concurrency())));
+  if (nth <= 1) {
+    worker();
+  } else {
+    std::vector<std::thread> ths;
+    for (size_t t = 0; t < nth; t++) ths.emplace_back(worker);
+    for (auto& th : ths) th.join();
+  }
+  for (size_t k = 0; k < writes.size(); k++)
+    if (!ok[k]) failed(writes[k].run, writes[k].path);
+}
+
 int Engine::execute_batch(const std::vector<std::string>& scripts) {
   struct Run {
     std::vector<Statement> sts;
@@ -1600,9 +1645,11 @@ int Engine::execute_batch(const std::vector<std::string>& scripts) {
     }
   }
   const double w2 = wall();
-  // phase 3: the rest of every script that waited
-  for (auto& rp : runs) {
-    Run& r = *rp;
+  // phase 3: the rest of every script that waited; a script's last statement, when it
+  // is a STORE, leaves its file to be written after the loop
+  std::vector<PendingWrite> writes;
+  for (size_t k = 0; k < runs.size(); k++) {
+    Run& r = *runs[k];
     if (!r.pending) continue;
     vars_ = std::move(r.vars);
     cur_script_ = r.text;
@@ -1611,7 +1658,11 @@ int Engine::execute_batch(const std::vector<std::string>& scripts) {
       drop_dead(r.last, r.i);
       for (r.i++; r.i < r.sts.size(); r.i++) {
         if (!(flags_ & ALK_SESSION_PLAIN) && try_fused(r.sts, r.i)) continue;
+        const bool defer = r.i + 1 == r.sts.size() && r.sts[r.i].kind == StmtKind::Store;
+        deferred_writes_ = defer ? &writes : nullptr;
+        deferred_run_ = k;
         exec(r.sts[r.i]);
+        deferred_writes_ = nullptr;
         drop_dead(r.last, r.i);
       }
       ck(cudaStreamSynchronize(stream_), "script");
@@ -1620,8 +1671,12 @@ int Engine::execute_batch(const std::vector<std::string>& scripts) {
     } catch (const std::exception& e) {
       fail(r, ALK_ERR_ARG, e.what());
     }
+    deferred_writes_ = nullptr;
     vars_.clear();
   }
+  write_files(writes, [&](size_t run, const std::string& path) {
+    fail(*runs[run], ALK_ERR_IO, "Could not open file " + path);
+  });
   stats_.batch_host_ms[0] = w1 - w0;
   stats_.batch_host_ms[1] = w2 - w1;
   stats_.batch_host_ms[2] = wall() - w2;

@@ -304,6 +304,8 @@ def run_batched(args, torch):
     sess = ab.Session(d, resident=True)
     if args.no_autotune:
         sess.tuning(autotune=False)
+    if args.launch_shape:
+        sess.set_tuning(tuple(int(v) for v in args.launch_shape.split(",")))
     t0 = time.perf_counter()
     for q, segs in enumerate(layout):
         sess.gen_flat_resident(f"li{q:03d}", segs, args.seed * 1000 + q)
@@ -417,6 +419,8 @@ def main():
     ap.add_argument("--queries", type=int, default=256)
     ap.add_argument("--batched-only", action="store_true", help="batched workload: skip the one-at-a-time runs")
     ap.add_argument("--no-autotune", action="store_true", help="batched workload: default launch shape")
+    ap.add_argument("--launch-shape", default=None,
+                    help="batched workload: fixed launch shape 'consumer_warps,stages,blocks_per_sm'")
     ap.add_argument("--no-graphs", action="store_true",
                     help="run every query without CUDA-graph replay (same kernels; for ncu, whose per-kernel "
                          "replay does not handle graph memory nodes)")

@@ -438,6 +438,10 @@ int alk_session_set_plain(alk_session* s, int on);
 /* *out = the launch shape of the last batched group-by; autotune 0/1 turns the per-
  * workload autotuner off/on (-1 leaves it). */
 int alk_session_tuning(alk_session* s, alk_gb_tuning* out, int autotune);
+/* Fixes the launch shape of later batched group-bys (*shape with consumer_warps 0, or
+ * NULL, returns to the autotuner or the default); a shape that shared memory cannot hold
+ * is reduced as the launch reports in alk_session_tuning. */
+int alk_session_set_tuning(alk_session* s, const alk_gb_tuning* shape);
 
 /* ------------------------------------------ 4. learned cardinality estimator
  * No counterpart in the reference, which sizes every buffer from the free device memory

@@ -171,3 +171,39 @@ def test_device_generated_table_values_and_groupby():
     m = ship < cut
     want = {k: (int(qty[m & (flag == i)].sum()), int((m & (flag == i)).sum())) for i, k in enumerate("ANR")}
     assert got == want
+
+
+def test_batch_fixed_launch_shape(flats):
+    d = flats[2]
+    scripts = [wl.flat_script(40 + i, out=f"fx{i}.txt") for i in range(3)]
+    want = []
+    for i, sc in enumerate(scripts):
+        _oracle.execute(d, sc.replace(f"fx{i}.txt", f"oracle_fx{i}.txt"))
+        want.append(_read(os.path.join(d, f"oracle_fx{i}.txt")))
+    with ab.Session(d) as s:
+        with pytest.raises(ab.AlenkaError):
+            s.set_tuning((5, 2, 1))  # 4 or 8 consumer warps only
+        for shape in ((4, 2, 2), (8, 4, 1)):
+            s.set_tuning(shape)
+            s.execute_batch(scripts)
+            assert s.tuning() == shape
+            for i, w in enumerate(want):
+                assert _read(os.path.join(d, f"fx{i}.txt")) == w
+
+
+def test_batch_store_failures_and_shared_paths(flats):
+    """The final STOREs of a batch are written after it: an unwritable path still fails
+    its own script, and two scripts storing into one file leave the later one's rows."""
+    d = flats[1]
+    first = wl.flat_script(61, out="same.txt")
+    second = wl.flat_script(62, out="same.txt")
+    unwritable = wl.flat_script(63, out="no_such_dir/x.txt")
+    other = wl.flat_script(64, out="o64.txt")
+    _oracle.execute(d, second.replace("same.txt", "oracle_same.txt"))
+    _oracle.execute(d, other.replace("o64.txt", "oracle_o64.txt"))
+    with ab.Session(d) as s:
+        with pytest.raises(ab.AlenkaError) as e:
+            s.execute_batch([first, unwritable, second, other])
+        assert "script 1" in str(e.value) and "Could not open file" in str(e.value)
+    assert _read(os.path.join(d, "same.txt")) == _read(os.path.join(d, "oracle_same.txt"))
+    assert _read(os.path.join(d, "o64.txt")) == _read(os.path.join(d, "oracle_o64.txt"))
