@@ -29,7 +29,7 @@ struct GbQuery {
   uint64_t key_span[2];
   uint32_t nslots, nacc;  // nacc = nagg + 1: the row count is the last accumulator
   int32_t count_agg;      // an aggregate that is COUNT (it doubles as the row count), or -1
-  uint32_t pad;
+  uint32_t npriv;         // private words per slot: nagg with a COUNT aggregate, else nacc
   alk_gb_agg agg[kGbAggs];
   int64_t* acc;  // [nacc][nslots]
 };
@@ -67,8 +67,8 @@ __device__ void gb_flush(const GbQuery& q, int64_t* priv, uint32_t lane) {
     const uint32_t a = j % q.nacc, slot = j / q.nacc;
     const uint32_t kind = a < q.nagg ? q.agg[a].kind : (uint32_t)ALK_AGG_COUNT;
     // a query with a COUNT aggregate keeps no separate row count: it is that aggregate
-    const uint32_t src = (a == q.nagg && q.count_agg >= 0) ? j - a + (uint32_t)q.count_agg : j;
-    int64_t v = priv[src * 32 + lane];  // gb_clear resets the accumulators for the next query
+    const uint32_t w = (a == q.nagg && q.count_agg >= 0) ? (uint32_t)q.count_agg : a;
+    int64_t v = priv[(slot * q.npriv + w) * 32 + lane];  // gb_clear resets them for the next query
     for (int o = 16; o; o >>= 1) {
       const int64_t w = __shfl_xor_sync(0xffffffffu, v, o);
       v = kind == ALK_AGG_MIN ? min(v, w) : kind == ALK_AGG_MAX ? max(v, w) : (int64_t)((uint64_t)v + (uint64_t)w);
@@ -87,8 +87,8 @@ __device__ void gb_flush(const GbQuery& q, int64_t* priv, uint32_t lane) {
 }
 
 __device__ __forceinline__ void gb_clear(const GbQuery& q, int64_t* priv, uint32_t lane) {
-  for (uint32_t j = 0; j < q.nslots * q.nacc; j++) {
-    const uint32_t a = j % q.nacc;
+  for (uint32_t j = 0; j < q.nslots * q.npriv; j++) {
+    const uint32_t a = j % q.npriv;
     const uint32_t kind = a < q.nagg ? q.agg[a].kind : (uint32_t)ALK_AGG_COUNT;
     priv[j * 32 + lane] = kind == ALK_AGG_MIN ? INT64_MAX : kind == ALK_AGG_MAX ? INT64_MIN : 0;
   }
@@ -272,7 +272,7 @@ __global__ void k_gb_tma(const __grid_constant__ GbArgs g) {
           live &= ~bad;
         }
       }
-      const uint32_t nagg = q.nagg, stride = q.nacc * 32;
+      const uint32_t nagg = q.nagg, stride = q.npriv * 32;
       int64_t* base = priv + lane;
       // rows that did not pass update the spare slot (index nslots): no branch per row
 #pragma unroll
@@ -401,7 +401,8 @@ int alk_batch_groupby(const alk_gb_query* qs, uint32_t nq, const alk_gb_tuning* 
     if (nslots * q.nacc > 64) return ALK_ERR_UNSUPPORTED;  // private accumulators per thread
     // one more slot per lane takes the updates of rows that did not pass, so that the
     // updates need no branch
-    max_acc = std::max<uint32_t>(max_acc, (uint32_t)((nslots + 1) * q.nacc));
+    q.npriv = q.count_agg >= 0 ? a.nagg : q.nacc;
+    max_acc = std::max<uint32_t>(max_acc, (uint32_t)((nslots + 1) * q.npriv));
     for (uint32_t k = 0; k < a.nagg; k++) {
       const alk_gb_agg& ag = a.agg[k];
       if (ag.kind > ALK_AGG_MAX) return ALK_ERR_ARG;
