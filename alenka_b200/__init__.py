@@ -17,6 +17,7 @@ ALK_ERR_UNSUPPORTED = 5
 ALK_SESSION_RESIDENT = 1
 ALK_SESSION_PLAIN = 2
 ALK_SESSION_NOGRAPH = 4
+ALK_SESSION_DELTA = 8
 
 _lib = None
 
@@ -131,9 +132,9 @@ def lib():
 class Session:
     """An engine session over a data directory (data.dictionary + segment files)."""
 
-    def __init__(self, data_dir, resident=True, plain=False, graphs=True):
+    def __init__(self, data_dir, resident=True, plain=False, graphs=True, delta=False):
         flags = ((ALK_SESSION_RESIDENT if resident else 0) | (ALK_SESSION_PLAIN if plain else 0)
-                 | (0 if graphs else ALK_SESSION_NOGRAPH))
+                 | (0 if graphs else ALK_SESSION_NOGRAPH) | (ALK_SESSION_DELTA if delta else 0))
         h = ctypes.c_void_p()
         rc = lib().alk_session_open(str(data_dir).encode(), flags, ctypes.byref(h))
         if rc != ALK_OK:

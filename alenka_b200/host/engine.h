@@ -249,6 +249,8 @@ class Engine {
   void multijoin(Statement& st, const std::string& s, const std::string& j1, const std::string& j2, unsigned tab);
   void emit_order(Statement& st);
   void emit_store(Statement& st);
+  void emit_store_binary(Statement& st);
+  std::map<std::string, uint32_t> cnt_counts_;  // largest payload written per column file prefix
   bool try_fused(std::vector<Statement>& sts, size_t& i);
   void run_fused(Statement& J, Statement& F, Statement& O, Statement& S, const std::string& gkey);
   // After the synchronisation: check the stages, record their counts, store the rows.

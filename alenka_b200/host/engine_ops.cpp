@@ -1491,6 +1491,72 @@ void Engine::emit_store(Statement& st) {
   std::fclose(fp);
 }
 
+// STORE v INTO 'name' [APPEND] [LIMIT n] BINARY: the binary branch of CudaSet::Store
+// (cm.cu:1040-1240) under emit_store_binary (operators.cu:2446-2515). Every column of v
+// becomes one more segment file <name>.<column>.<segment>, encoded on the device in the
+// reference's byte format (FOR; FOR-delta for sorted columns when the session has the
+// delta switch), then the column headers (writeHeader, cm.cu:1251-1263) and the table's
+// catalog entry (cm.cu:1686-1701, saved as save_col_data does). A result with columns
+// and no rows writes the headers only (cm.cu:1481-1486); an empty select result has no
+// columns and writes nothing. SORT SEGMENTS BY / PRESORTED BY and char columns are
+// outside the supported surface.
+void Engine::emit_store_binary(Statement& st) {
+  Var* a = var(st.s);
+  if (st.store_sort) unsupported("STORE BINARY with SORT SEGMENTS BY / PRESORTED BY");
+  for (auto& c : a->columnNames)
+    if (a->meta[c].type != 0 || !a->meta[c].string_map.empty()) unsupported("STORE BINARY of char columns");
+  if (st.f.empty() || st.f.find('/') != std::string::npos) unsupported("STORE BINARY outside the data directory");
+  Rows R = materialize(a, a->columnNames);
+  const size_t limit = st.op_nums.empty() ? 0 : (size_t)st.op_nums[0];
+  const uint64_t n = (limit != 0 && limit < R.n) ? limit : R.n;
+  if (n > UINT32_MAX) unsupported("a segment of more than 2^32 - 1 rows");
+  const std::string base = dir_ + "/" + st.f;
+  uint64_t total = n;
+  uint32_t seg = 0, max_recs = (uint32_t)n;
+  if (st.append) {  // continue the table: its header gives the segment count (cm.cu:1050-1060)
+    ColHeader h;
+    std::string e;
+    if (!a->columnNames.empty() && read_col_header(base + "." + a->columnNames[0] + ".header", h, e)) {
+      seg = h.segs;
+      total += h.total;
+      max_recs = std::max(max_recs, h.max_recs);
+    }
+  }
+  if (n == 0) {
+    for (auto& c : a->columnNames) {
+      const std::string prefix = base + "." + c;
+      if (!write_col_header(prefix + ".header", ColHeader{total, seg, max_recs, cnt_counts_[prefix]}))
+        throw EngineError(ALK_ERR_IO, "Could not write " + prefix + ".header");
+    }
+    return;
+  }
+  const size_t cap = kSegHeadBytes + (size_t)n * 8 + kSegTailBytes + 8;
+  auto img = mkbuf(cap, stream_);
+  std::vector<uint8_t> host;
+  for (auto& c : a->columnNames) {
+    size_t len = 0;
+    check(alk_encode_segment_device(R.col.at(c)->as<int64_t>(), (uint32_t)n, (flags_ & ALK_SESSION_DELTA) ? 2 : 0,
+                                    img->as<void>(), cap, &len, (alk_stream)stream_),
+          "segment writer");
+    host.resize(len);
+    ck(cudaMemcpyAsync(host.data(), img->as<void>(), len, cudaMemcpyDeviceToHost, stream_), "segment d2h");
+    ck(cudaStreamSynchronize(stream_), "segment d2h");
+    stats_.d2h_bytes += len;
+    const std::string prefix = base + "." + c;
+    if (!write_file(prefix + "." + std::to_string(seg), host.data(), len))
+      throw EngineError(ALK_ERR_IO, "Could not write " + prefix + "." + std::to_string(seg));
+    uint32_t cnt = 0;
+    std::memcpy(&cnt, host.data(), 4);
+    cnt_counts_[prefix] = std::max(cnt_counts_[prefix], cnt);
+    if (!write_col_header(prefix + ".header", ColHeader{total, seg + 1, max_recs, cnt_counts_[prefix]}))
+      throw EngineError(ALK_ERR_IO, "Could not write " + prefix + ".header");
+  }
+  for (auto& c : a->columnNames) dd_[st.f][c] = ColData{0, a->meta[c].dz};
+  if (!save_data_dict(dir_ + "/data.dictionary", dd_)) throw EngineError(ALK_ERR_IO, "Could not write data.dictionary");
+  bases_.erase(st.f);  // the table is read afresh by the next statement that names it
+  basecols_.erase(st.f);
+}
+
 // ------------------------------------------------------------------ script
 void Engine::exec(Statement& st) {
   switch (st.kind) {
@@ -1499,8 +1565,9 @@ void Engine::exec(Statement& st) {
     case StmtKind::Join: emit_join(st); break;
     case StmtKind::Order: emit_order(st); break;
     case StmtKind::Store: emit_store(st); break;
+    case StmtKind::StoreBinary: emit_store_binary(st); break;
     case StmtKind::Display: break;
-    default: unsupported("statement kind (LOAD / STORE BINARY / catalog commands)");
+    default: unsupported("statement kind (LOAD / catalog commands)");
   }
 }
 

@@ -20,13 +20,14 @@ void wr(std::vector<uint8_t>& out, T v) {
   const uint8_t* p = reinterpret_cast<const uint8_t*>(&v);
   out.insert(out.end(), p, p + sizeof(T));
 }
+}  // namespace
+
 // Bits needed for a value range, computed as the reference does in double precision:
 // (unsigned int)ceil(log2((double)((max - min) + 1))) (compress.cu:296, compress.cu:459).
 uint32_t range_bits(int64_t lo, int64_t hi) {
   int64_t span = (int64_t)((uint64_t)hi - (uint64_t)lo + 1ULL);
   return (uint32_t)std::ceil(std::log2((double)span));
 }
-}  // namespace
 
 bool parse_segment(const uint8_t* buf, size_t len, SegMeta& m, const uint8_t** payload,
                    std::string& err) {

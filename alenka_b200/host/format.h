@@ -46,6 +46,9 @@ bool write_file(const std::string& path, const void* data, size_t len, bool appe
 void encode_for(const int64_t* v, uint32_t n, SegMeta& m, std::vector<uint8_t>& payload);
 void encode_delta(const int64_t* v, uint32_t n, SegMeta& m, std::vector<uint8_t>& payload);
 std::vector<uint8_t> segment_image(const SegMeta& m, const std::vector<uint8_t>& payload);
+// Packed width of a value range as the reference computes it (double-precision log2);
+// shared by the host and the device segment writers so both pick the same width.
+uint32_t range_bits(int64_t lo, int64_t hi);
 
 struct ColHeader {
   uint64_t total = 0;

@@ -551,6 +551,7 @@ class Parser {
 
   void sort_def() {
     if (is_kw("SORT")) {
+      cur_->store_sort = true;
       take();
       expect_kw("SEGMENTS");
       expect_kw("BY");
@@ -561,6 +562,7 @@ class Parser {
         expect_int();
       }
     } else if (is_kw("PRESORTED")) {
+      cur_->store_sort = true;
       take();
       expect_kw("BY");
       expect(T::Name, "column");

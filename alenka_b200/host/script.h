@@ -32,6 +32,7 @@ struct Statement {
   std::string sep;    // Store/Display separator
   int grp_cnt = 0;    // number of GROUP BY columns
   bool append = false;
+  bool store_sort = false;  // STORE ... BINARY with SORT SEGMENTS BY / PRESORTED BY
   std::vector<std::string> op_type, op_value;
   std::vector<int64_t> op_nums;
   std::vector<double> op_nums_f;

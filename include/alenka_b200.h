@@ -53,6 +53,8 @@ typedef struct alk_session alk_session;
 #define ALK_SESSION_RESIDENT 1u
 #define ALK_SESSION_PLAIN 2u    /* operator-at-a-time plan only (no fused pipelines) */
 #define ALK_SESSION_NOGRAPH 4u  /* fused queries are never captured into CUDA graphs */
+#define ALK_SESSION_DELTA 8u    /* STORE BINARY writes sorted columns FOR-delta (the
+                                   reference's delta switch, compress.cu:428-444) */
 int alk_session_open(const char* data_dir, uint32_t flags, alk_session** out);
 int alk_session_execute(alk_session* s, const char* script);
 const char* alk_session_error(alk_session* s);
@@ -132,6 +134,16 @@ int alk_decode_segment_noalloc(const void* d_payload, uint32_t comp_type, uint32
  * (compress.cu:271-527). ALK_ERR_OVERFLOW with *out_len set when cap is too small. */
 int alk_encode_segment(const int64_t* values, uint32_t n, int delta, uint8_t* out, size_t cap,
                        size_t* out_len);
+/* Segment writer (device): the same image as alk_encode_segment, built on the device
+ * from n int64 values in device memory into d_image (device memory, 8-byte aligned):
+ * the GPU form of pfor_compress / pfor_delta_compress (compress.cu:271-527) behind
+ * CudaSet::Store's binary branch (cm.cu:1040-1240). mode 0 FOR, 1 FOR-delta, 2 FOR-delta
+ * when the values are sorted (the reference's delta switch, compress.cu:428-444), else
+ * FOR. *h_len = the image size; ALK_ERR_OVERFLOW when cap is too small (with *h_len a
+ * size that suffices). d_image holds working statistics until the header is written;
+ * nothing is allocated. Returns after the image is complete (stream synchronized). */
+int alk_encode_segment_device(const int64_t* d_values, uint32_t n, int mode, void* d_image, size_t cap,
+                              size_t* h_len, alk_stream stream);
 
 /* MurmurHash64A of n tuples of k int64 keys (row-major tuples built from k column
  * pointers), seed as given (hash_seed 100, bison.y:304). Replaces the host loop of
