@@ -1530,16 +1530,27 @@ void Engine::emit_store_binary(Statement& st) {
     }
     return;
   }
-  const size_t cap = kSegHeadBytes + (size_t)n * 8 + kSegTailBytes + 8;
-  auto img = mkbuf(cap, stream_);
+  // every column's segment image in one call of the device writer
+  const size_t ncol = a->columnNames.size();
+  const size_t cap = (kSegHeadBytes + (size_t)n * 8 + kSegTailBytes + 255) & ~size_t(255);
+  auto imgs = mkbuf(cap * ncol, stream_);
+  std::vector<const int64_t*> src(ncol);
+  std::vector<uint32_t> counts(ncol, (uint32_t)n);
+  std::vector<void*> dst(ncol);
+  std::vector<size_t> caps(ncol, cap), lens(ncol, 0);
+  for (size_t k = 0; k < ncol; k++) {
+    src[k] = R.col.at(a->columnNames[k])->as<int64_t>();
+    dst[k] = imgs->as<uint8_t>() + k * cap;
+  }
+  check(alk_encode_segments_device(src.data(), counts.data(), (uint32_t)ncol, (flags_ & ALK_SESSION_DELTA) ? 2 : 0,
+                                   dst.data(), caps.data(), lens.data(), (alk_stream)stream_),
+        "segment writer");
   std::vector<uint8_t> host;
-  for (auto& c : a->columnNames) {
-    size_t len = 0;
-    check(alk_encode_segment_device(R.col.at(c)->as<int64_t>(), (uint32_t)n, (flags_ & ALK_SESSION_DELTA) ? 2 : 0,
-                                    img->as<void>(), cap, &len, (alk_stream)stream_),
-          "segment writer");
+  for (size_t k = 0; k < ncol; k++) {
+    const std::string& c = a->columnNames[k];
+    const size_t len = lens[k];
     host.resize(len);
-    ck(cudaMemcpyAsync(host.data(), img->as<void>(), len, cudaMemcpyDeviceToHost, stream_), "segment d2h");
+    ck(cudaMemcpyAsync(host.data(), dst[k], len, cudaMemcpyDeviceToHost, stream_), "segment d2h");
     ck(cudaStreamSynchronize(stream_), "segment d2h");
     stats_.d2h_bytes += len;
     const std::string prefix = base + "." + c;

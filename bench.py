@@ -401,6 +401,131 @@ def run_groupby_high(args, torch):
                                  "forms": out}}), flush=True)
 
 
+def run_encode(args, torch):
+    """The segment writer behind STORE ... BINARY: a lineitem-shaped result of 60M rows and
+    five numeric columns (l_orderkey in order, l_quantity, l_extendedprice, l_discount,
+    l_shipdate) encoded into segment images of 10M rows per column, FOR or FOR-delta as the
+    reference's delta switch picks. One step is one call of the batched device writer
+    (alk_encode_segments_device, mode 2) over every segment of every column; e2e adds the
+    upload of the values from pinned host memory and the download of every image."""
+    import ctypes
+    import numpy as np
+    import alenka_b200 as ab
+    L = ab.lib()
+    L.alk_encode_segment_device.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p,
+                                            ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), ctypes.c_void_p]
+    L.alk_encode_segment.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+    vp = ctypes.c_void_p
+    L.alk_encode_segments_device.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_int, vp, vp, vp, vp]
+    rows = int(60_000_000 * args.scale)
+    seg = min(10_000_000, rows)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(args.seed)
+
+    def rnd(lo, hi):
+        return torch.randint(lo, hi + 1, (rows,), device="cuda", generator=g, dtype=torch.int64)
+    cols = {"l_orderkey": torch.cumsum(rnd(0, 1), 0) * 4 + 1, "l_quantity": rnd(1, 50),
+            "l_extendedprice": rnd(90_000, 10_500_000), "l_discount": rnd(0, 10),
+            "l_shipdate": rnd(19_920_102, 19_981_201)}
+    segs = [(c, s0, min(seg, rows - s0)) for c in cols for s0 in range(0, rows, seg)]
+    k = len(segs)
+    cap = (24 + 8 * seg + 32 + 255) // 256 * 256
+    imgs = torch.empty(k * cap // 8, dtype=torch.int64, device="cuda")
+    ln = ctypes.c_size_t()
+    P = ctypes.c_void_p * k
+    d_imgs = P(*[imgs.data_ptr() + i * cap for i in range(k)])
+    counts = (ctypes.c_uint32 * k)(*[n for _, _, n in segs])
+    caps = (ctypes.c_size_t * k)(*([cap] * k))
+    lens = (ctypes.c_size_t * k)()
+
+    def encode(src):
+        rc = L.alk_encode_segments_device(src, counts, k, 2, d_imgs, caps, lens, None)
+        if rc:
+            raise RuntimeError(f"segment writer: status {rc}")
+        return sum(lens)
+    src_dev = P(*[cols[c].data_ptr() + 8 * s0 for c, s0, _ in segs])
+
+    def step():
+        return encode(src_dev)
+    args.warmup = max(args.warmup, 3)
+    for _ in range(args.warmup):
+        img_bytes = step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = clock_sampler(0)
+    clk.start()
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    in_bytes = 8 * rows * len(cols)
+    alg = in_bytes + img_bytes
+    # end to end: values from pinned host memory, every image back to pinned host memory
+    host_cols = {c: t.cpu().pin_memory() for c, t in cols.items()}
+    stage = {c: torch.empty_like(t) for c, t in cols.items()}
+    src_stage = P(*[stage[c].data_ptr() + 8 * s0 for c, s0, _ in segs])
+    host_img = torch.empty(k * cap, dtype=torch.uint8).pin_memory()
+    img_u8 = imgs.view(torch.uint8)
+
+    def e2e_step():
+        for c in cols:
+            stage[c].copy_(host_cols[c], non_blocking=True)
+        encode(src_stage)
+        for i in range(k):
+            host_img[i * cap:i * cap + lens[i]].copy_(img_u8[i * cap:i * cap + lens[i]], non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_step()
+    e2e_steps = max(1, args.steps // 2)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    cpu = None
+    if not args.no_cpu_baseline:  # the host writer (pinned to the reference's own files), one core
+        n_cpu = min(rows, 4_000_000)
+        sample = {c: np.ascontiguousarray(host_cols[c][:n_cpu].numpy()) for c in cols}
+        out = ctypes.create_string_buffer(24 + 8 * n_cpu + 64)
+        t0 = time.perf_counter()
+        for c in cols:
+            v = sample[c]
+            rc = L.alk_encode_segment(v.ctypes.data, n_cpu, 1, out, len(out), ctypes.byref(ln))
+            if rc:
+                raise RuntimeError(f"host segment writer: status {rc}")
+        dt = time.perf_counter() - t0
+        cpu = {"value": n_cpu / dt, "unit": "rows/s", "cores": 1, "kind": "port",
+               "sample": f"{n_cpu} rows x {len(cols)} columns, one segment per column (host writer)"}
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg / (ms / 1000.0) / 1e9
+    traffic = profiled_traffic("encode_segment_lineitem.md")
+    trows = profiled_traffic_rows("encode_segment_lineitem.md")
+    print(json.dumps({
+        "metric": "rows/s written as segment images (STORE BINARY of 5 numeric lineitem columns)",
+        "value": rows / (ms / 1000.0), "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int64",
+        "data": "synthetic (seeded, generated in device memory)",
+        "config": {"workload": f"{rows} rows x {len(cols)} columns in segments of {seg} rows "
+                               f"({len(segs)} segment images, {img_bytes} bytes)",
+                   "l2": "inputs larger than L2"},
+        "e2e": {"value": rows / (e2e_ms / 1000.0), "unit": "rows/s", "h2d_bytes_per_step": in_bytes,
+                "d2h_bytes_per_step": img_bytes},
+        "gpu_launches": 4 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": (traffic * rows // trows) if traffic and trows else None,
+                     "traffic_note": "ncu capture of one step at a smaller size, scaled by rows",
+                     "kernel": "k_enc_stats_batch + k_enc_pack_batch (the whole step: 4 launches, 1 synchronisation)",
+                     "algorithmic_bytes": "8 B per value read + the image bytes written",
+                     "algorithmic_bytes_per_step": alg, "peak_source": f"{peak_kind} hbm_gbs"},
+        "cpu_baseline": cpu, "clocks": clocks,
+    }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -413,7 +538,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--fused-only", action="store_true",
                     help="time only the resident fused plan (profiling runs)")
-    ap.add_argument("--workload", default="three_way", choices=["three_way", "batched", "groupby_high"],
+    ap.add_argument("--workload", default="three_way", choices=["three_way", "batched", "groupby_high", "encode"],
                     help="three_way: the filter -> join -> group-by pipeline (default); batched: many "
                          "single-table filter + group-by queries per step")
     ap.add_argument("--queries", type=int, default=256)
@@ -433,9 +558,9 @@ def main():
         return
     import torch
     torch.cuda.set_device(local)
-    if args.workload in ("batched", "groupby_high"):
+    if args.workload in ("batched", "groupby_high", "encode"):
         if rank == 0:
-            (run_batched if args.workload == "batched" else run_groupby_high)(args, torch)
+            {"batched": run_batched, "groupby_high": run_groupby_high, "encode": run_encode}[args.workload](args, torch)
         return
     dist = None
     if world > 1:

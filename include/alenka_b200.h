@@ -144,6 +144,14 @@ int alk_encode_segment(const int64_t* values, uint32_t n, int delta, uint8_t* ou
  * nothing is allocated. Returns after the image is complete (stream synchronized). */
 int alk_encode_segment_device(const int64_t* d_values, uint32_t n, int mode, void* d_image, size_t cap,
                               size_t* h_len, alk_stream stream);
+/* Segment writer (device), many segments per call: segment i is n[i] values at
+ * d_values[i] written into d_images[i] (device memory, 8-byte aligned, caps[i] bytes, at
+ * least 24 + 8 n[i] + 32: the image is written before its size is known). The same images
+ * as alk_encode_segment_device, for all segments with four launches and one stream
+ * synchronisation; h_lens[i] = the image size. Host arrays of count entries. Used by
+ * STORE ... BINARY for all columns of a result at once (cm.cu:1040-1240). */
+int alk_encode_segments_device(const int64_t* const* d_values, const uint32_t* n, uint32_t count, int mode,
+                               void* const* d_images, const size_t* caps, size_t* h_lens, alk_stream stream);
 
 /* MurmurHash64A of n tuples of k int64 keys (row-major tuples built from k column
  * pointers), seed as given (hash_seed 100, bison.y:304). Replaces the host loop of

@@ -155,3 +155,88 @@ def test_large_segment_round_trip_on_device():
     assert L.alk_decode_segment(d_pay.data_ptr(), 0, bits, 64 // bits, lower, 0, n, d_out.data_ptr(), None) == 0
     torch.cuda.synchronize()
     assert torch.equal(d_out.cpu(), torch.from_numpy(v))
+
+
+def batch_images(arrays, mode):
+    """(status, [image bytes]) of the batched device writer over numpy int64 arrays."""
+    import torch
+    L = ab.lib()
+    vp = ctypes.c_void_p
+    L.alk_encode_segments_device.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_int, vp, vp, vp, vp]
+    k = len(arrays)
+    d_vals = [torch.from_numpy(np.ascontiguousarray(a, dtype=np.int64)).cuda() if len(a) else
+              torch.zeros(1, dtype=torch.int64, device="cuda") for a in arrays]
+    caps = [24 + 8 * len(a) + 32 for a in arrays]
+    d_imgs = [torch.full((c // 8 + 2,), -1, dtype=torch.int64, device="cuda") for c in caps]
+    P = ctypes.c_void_p * k
+    ptrs = P(*[t.data_ptr() for t in d_vals])
+    imgs = P(*[t.data_ptr() for t in d_imgs])
+    ns = (ctypes.c_uint32 * k)(*[len(a) for a in arrays])
+    cp = (ctypes.c_size_t * k)(*caps)
+    lens = (ctypes.c_size_t * k)()
+    torch.cuda.synchronize()
+    rc = L.alk_encode_segments_device(ptrs, ns, k, mode, imgs, cp, lens, None)
+    torch.cuda.synchronize()
+    if rc:
+        return rc, list(lens)
+    return 0, [d_imgs[i].cpu().numpy().view(np.uint8)[:lens[i]].tobytes() for i in range(k)]
+
+
+def _edge_ranges():
+    """Value and difference ranges at and around every power of two: the batched plan
+    computes widths exactly up to 2^46 and leaves the rest to the single-segment path."""
+    out = []
+    for kk in range(1, 63):
+        for span in (1 << kk) - 1, 1 << kk, (1 << kk) + 1:
+            out.append(np.array([0, span - 1], dtype=np.int64))          # value range: span
+            out.append(np.array([5, 5, 5 + span - 1], dtype=np.int64))   # difference range: span
+    return out
+
+
+@pytest.mark.parametrize("mode", [0, 2])
+def test_batched_writer_matches_host_writer(mode):
+    inputs = [v for _, v in _inputs()] + [np.zeros(0, np.int64)] + _edge_ranges()
+    for name, v in _reference_values():
+        inputs.append(v)
+    rc, imgs = batch_images(inputs, mode)
+    assert rc == 0
+    for v, img in zip(inputs, imgs):
+        if len(v) == 0:
+            assert len(img) == 56
+            continue
+        assert img == host_image(v, 1 if mode == 2 else 0), len(v)
+
+
+def _reference_values():
+    return [(name, _case(name)[1]) for name in CASES]
+
+
+def test_batched_writer_reference_files_and_forced_delta():
+    seg = {name: _case(name) for name in CASES}
+    rc, imgs = batch_images([seg[n][1] for n in CASES], 2)
+    assert rc == 0
+    for n, img in zip(CASES, imgs):
+        if n.startswith("delta"):
+            assert img == seg[n][0], n
+    r = np.random.default_rng(8)
+    vals = [r.integers(-(1 << 40), 1 << 40, n) for n in (1, 2, 3, 8191, 8192, 8193, 50_000)]
+    rc, imgs = batch_images(vals, 1)
+    assert rc == 0
+    for v, img in zip(vals, imgs):
+        assert np.array_equal(oracle_decode(img), v)
+
+
+def test_batched_writer_needs_room_for_the_largest_image():
+    import torch
+    L = ab.lib()
+    vp = ctypes.c_void_p
+    L.alk_encode_segments_device.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_int, vp, vp, vp, vp]
+    d_v = torch.arange(100, dtype=torch.int64, device="cuda")
+    d_img = torch.zeros(256, dtype=torch.int64, device="cuda")
+    ptrs = (ctypes.c_void_p * 1)(d_v.data_ptr())
+    imgs = (ctypes.c_void_p * 1)(d_img.data_ptr())
+    ns = (ctypes.c_uint32 * 1)(100)
+    cp = (ctypes.c_size_t * 1)(24 + 100 + 32)  # the FOR image would fit, the largest would not
+    lens = (ctypes.c_size_t * 1)()
+    assert L.alk_encode_segments_device(ptrs, ns, 1, 0, imgs, cp, lens, None) == 3
+    assert lens[0] == 24 + 800 + 32
