@@ -68,6 +68,7 @@ def _declare(L):
     L.alk_session_close.argtypes = [vp]
     L.alk_session_close.restype = None
     L.alk_gen_lineitem_flat.argtypes = [c.c_char_p, u64, u32, u64, i32, c.c_char_p, i32]
+    L.alk_gen_names.argtypes = [c.c_char_p, u64, u32, u32, u64, c.c_char_p, i32]
     L.alk_gen_three_way.argtypes = [c.c_char_p, u64, u64, u64, u32, u64, i32, c.c_char_p, i32]
     L.alk_date_add_days.argtypes = [i64, i64]
     L.alk_date_add_days.restype = i64
@@ -262,6 +263,13 @@ class Session:
 def gen_lineitem_flat(data_dir, rows, seg_rows, seed, delta=False):
     err = ctypes.create_string_buffer(512)
     rc = lib().alk_gen_lineitem_flat(str(data_dir).encode(), rows, seg_rows, seed, int(delta), err, 512)
+    if rc:
+        raise AlenkaError(rc, err.value.decode())
+
+
+def gen_names(data_dir, rows, distinct, seg_rows, seed):
+    err = ctypes.create_string_buffer(512)
+    rc = lib().alk_gen_names(str(data_dir).encode(), rows, distinct, seg_rows, seed, err, 512)
     if rc:
         raise AlenkaError(rc, err.value.decode())
 

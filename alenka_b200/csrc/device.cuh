@@ -73,6 +73,11 @@ __device__ __forceinline__ int64_t vm_apply(uint8_t op, int64_t a, int64_t b) {
     case ALK_OP_NE: return a != b;
     case ALK_OP_AND: return (a != 0) && (b != 0);
     case ALK_OP_OR: return (a != 0) || (b != 0);
+    case ALK_OP_INSET: {  // b: device address of [n, bits...]
+      const uint32_t* set = (const uint32_t*)(uintptr_t)b;
+      const uint64_t n = __ldg(set);
+      return (uint64_t)a < n ? (__ldg(set + 1 + ((uint64_t)a >> 5)) >> (a & 31)) & 1 : 0;
+    }
     default: return a;  // MOV
   }
 }

@@ -1347,7 +1347,8 @@ bool prog_ok(const alk_program& p, uint32_t ncols, uint32_t npay) {
   if (p.n_instr > ALK_MAX_INSTR || p.result >= ALK_MAX_REGS) return false;
   for (uint32_t i = 0; i < p.n_instr; i++) {
     const alk_instr& in = p.ins[i];
-    if (in.dst >= ALK_MAX_REGS || in.op < ALK_OP_ADD || in.op > ALK_OP_MOV) return false;
+    if (in.dst >= ALK_MAX_REGS || in.op < ALK_OP_ADD || in.op > ALK_OP_INSET) return false;
+    if (in.op == ALK_OP_INSET && in.kb != ALK_K_CONST) return false;  // the set's address
     const uint8_t k[2] = {in.ka, in.kb};
     const uint16_t x[2] = {in.a, in.b};
     for (int j = 0; j < 2; j++) {

@@ -367,6 +367,33 @@ void Engine::load_dict(Var* base, const std::string& col, BaseCol& bc) {
   bc.dict_loaded = true;
 }
 
+// The codes of a char column whose dictionary entries match a LIKE pattern, on the
+// device as [count, bits...]; kept per pattern with the column (the reference keeps its
+// match list per column too, map_res in filter.cu:454-500).
+DevBufP Engine::like_set(Var* base, const std::string& col, const std::string& pattern) {
+  BaseCol& bc = basecol(base, col);
+  auto it = bc.like_sets.find(pattern);
+  if (it != bc.like_sets.end()) return it->second;
+  if (pattern.size() >= 256) unsupported("a LIKE pattern of 256 bytes or more");
+  load_dict(base, col, bc);
+  const uint32_t w = bc.meta.width;
+  const uint64_t count = bc.dict.size();
+  std::string raw;
+  raw.reserve(count * w);
+  for (auto& s : bc.dict) raw += s;
+  auto d_dict = mkbuf(std::max<size_t>(raw.size(), 1), stream_);
+  if (!raw.empty())
+    ck(cudaMemcpyAsync(d_dict->as<void>(), raw.data(), raw.size(), cudaMemcpyHostToDevice, stream_), "dictionary h2d");
+  stats_.h2d_bytes += raw.size();
+  auto set = mkbuf((1 + (count + 31) / 32) * 4, stream_);
+  check(alk_like_dictionary(d_dict->as<char>(), w, count, pattern.data(), (uint32_t)pattern.size(),
+                            set->as<uint32_t>(), (alk_stream)stream_),
+        "LIKE");
+  ck(cudaStreamSynchronize(stream_), "LIKE");  // the dictionary copy is released here
+  bc.like_sets[pattern] = set;
+  return set;
+}
+
 int Engine::preload(const std::string& table) {
   try {
     Var* b = base_table(table);
@@ -658,8 +685,15 @@ alk_program Engine::compile_filter(Var* f, Var* src, std::vector<std::string>& s
         std::string v1 = pop(ev), v2 = pop(ev);
         if (s1 == "NAME") std::swap(v1, v2);  // v1 literal, v2 column
         if (v2.find('.') != std::string::npos) unsupported("bitmap-index predicates");
-        if (cmp != 4 && cmp != 3) unsupported("string comparison other than == / !=");
+        if (cmp != 4 && cmp != 3 && cmp != 7) unsupported("string comparison other than == / != / LIKE");
         if (!src->has(v2) || src->meta[v2].type != 2) unsupported("string compared with a non-char column");
+        if (cmp == 7) {
+          // LIKE: the dictionary entries that match, as a set of codes (filter.cu:454-500)
+          const DevBufP set = like_set(src, v2, v1);
+          bools.push_back(b.emit(ALK_OP_INSET, slot(v2), b.konst((int64_t)(uintptr_t)set->as<void>())));
+          et.push_back("NAME");
+          continue;
+        }
         // .hash rows equal MurmurHash64A(literal padded to the width)/2 exactly when the
         // row's dictionary code is the literal's code (cm.cu:1806-1819, filter.cu:428-449)
         BaseCol& bc = basecol(src, v2);

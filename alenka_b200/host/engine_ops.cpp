@@ -767,6 +767,7 @@ int64_t host_apply(uint8_t op, int64_t a, int64_t b) {
     case ALK_OP_NE: return a != b;
     case ALK_OP_AND: return (a != 0) && (b != 0);
     case ALK_OP_OR: return (a != 0) || (b != 0);
+    case ALK_OP_INSET: throw EngineError(ALK_ERR_UNSUPPORTED, "a code-set test outside a filter");
     default: return a;
   }
 }

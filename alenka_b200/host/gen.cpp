@@ -197,6 +197,37 @@ bool gen_three_way(const std::string& dir, uint64_t customers, uint64_t orders, 
   return save_data_dict(dir + "/data.dictionary", dd);
 }
 
+// Names workload for string predicates: table "names" with n_key (1..rows) and n_name,
+// a char(12) column drawn from `distinct` generated strings over the letters A, B, X and
+// the characters '.', '%', '_' (lengths 0 to 12, so some fill the width and carry no
+// terminator): the cases that the LIKE matcher's wildcards and its '?'-against-'.' rule
+// tell apart.
+bool gen_names(const std::string& dir, uint64_t rows, uint32_t distinct, uint32_t seg_rows, uint64_t seed,
+               std::string& err) {
+  DataDict dd;
+  std::string e2;
+  load_data_dict(dir + "/data.dictionary", dd, e2);
+  const char alphabet[] = "ABXAB.%_";
+  Rng r(mix(seed, 41));
+  std::vector<std::string> vocab(std::max<uint32_t>(distinct, 1));
+  for (auto& w : vocab) {
+    const int64_t len = r.uniform(0, 12);
+    for (int64_t k = 0; k < len; k++) w.push_back(alphabet[r.uniform(0, 7)]);
+  }
+  std::vector<ColumnSpec> spec = {{"n_key", 0, 0, 0, false}, {"n_name", 2, 0, 12, false}};
+  std::vector<std::vector<int64_t>> ints(2);
+  std::vector<std::vector<char>> chars(2);
+  ints[0].resize(rows);
+  chars[1].assign(rows * 12, 0);
+  for (uint64_t i = 0; i < rows; i++) {
+    ints[0][i] = (int64_t)i + 1;
+    const std::string& w = vocab[r.uniform(0, (int64_t)vocab.size() - 1)];
+    std::memcpy(&chars[1][i * 12], w.data(), w.size());
+  }
+  if (!write_table(dir, "names", spec, ints, chars, rows, seg_rows, dd, err)) return false;
+  return save_data_dict(dir + "/data.dictionary", dd);
+}
+
 }  // namespace alk
 
 extern "C" {
@@ -213,6 +244,13 @@ int alk_gen_three_way(const char* dir, uint64_t customers, uint64_t orders, uint
                       uint32_t seg_rows, uint64_t seed, int delta, char* err, int err_len) {
   std::string e;
   bool ok = alk::gen_three_way(dir, customers, orders, lineitems, seg_rows, seed, delta != 0, e);
+  if (!ok && err && err_len > 0) std::snprintf(err, (size_t)err_len, "%s", e.c_str());
+  return ok ? 0 : 1;
+}
+int alk_gen_names(const char* dir, uint64_t rows, uint32_t distinct, uint32_t seg_rows, uint64_t seed, char* err,
+                  int err_len) {
+  std::string e;
+  bool ok = alk::gen_names(dir, rows, distinct, seg_rows, seed, e);
   if (!ok && err && err_len > 0) std::snprintf(err, (size_t)err_len, "%s", e.c_str());
   return ok ? 0 : 1;
 }

@@ -168,7 +168,12 @@ int alk_hash_tuples(const int64_t* const* d_cols, uint32_t k, uint64_t n, uint32
 enum {
   ALK_OP_ADD = 1, ALK_OP_SUB, ALK_OP_MUL, ALK_OP_DIV,
   ALK_OP_LT, ALK_OP_GT, ALK_OP_LE, ALK_OP_GE, ALK_OP_EQ, ALK_OP_NE,
-  ALK_OP_AND, ALK_OP_OR, ALK_OP_MOV
+  ALK_OP_AND, ALK_OP_OR, ALK_OP_MOV,
+  /* a in a set of codes: b is a constant holding a device pointer to uint32 words, word 0
+   * the set's size n in bits, then the bits; 1 when 0 <= a < n and bit a is set. The
+   * LIKE of a char column compiles to it (filter.cu:454-500: the dictionary entries
+   * that match, then each row's code looked up). */
+  ALK_OP_INSET
 };
 enum { ALK_K_REG = 0, ALK_K_COL = 1, ALK_K_CONST = 2 };
 typedef struct alk_instr {
@@ -182,6 +187,14 @@ typedef struct alk_program {
   alk_instr ins[ALK_MAX_INSTR];
   int64_t consts[ALK_MAX_CONST];
 } alk_program;
+
+/* LIKE over a char column's dictionary (gpu_regex, filter.cu:67-129, run over the
+ * dictionary file as filter.cu:454-500 does): entry k of `count` fixed-width entries at
+ * d_dict (device) matches the pattern ('%' any run, '?' any character but '.', others
+ * themselves; pattern_len < 256). d_bits (device, 1 + ceil(count / 32) words) receives
+ * count in word 0 and bit k set for each match: the set ALK_OP_INSET tests. */
+int alk_like_dictionary(const char* d_dict, uint32_t width, uint64_t count, const char* pattern,
+                        uint32_t pattern_len, uint32_t* d_bits, alk_stream stream);
 
 /* Fused segment scan, replaces filter_op + filter + copyColumns/mygather
  * (cm.cu:3609-3666, filter.cu:133-643, cm.cu:3305-3478): for every segment whose
@@ -384,6 +397,10 @@ int alk_gen_lineitem_flat(const char* dir, uint64_t rows, uint32_t seg_rows, uin
                           char* err, int err_len);
 int alk_gen_three_way(const char* dir, uint64_t customers, uint64_t orders, uint64_t lineitems,
                       uint32_t seg_rows, uint64_t seed, int delta, char* err, int err_len);
+/* Table "names" for string predicates: n_key 1..rows and n_name char(12) drawn from
+ * `distinct` generated strings over A, B, X, '.', '%', '_' (lengths 0-12). */
+int alk_gen_names(const char* dir, uint64_t rows, uint32_t distinct, uint32_t seg_rows, uint64_t seed, char* err,
+                  int err_len);
 /* The single-table lineitem shape generated in device memory, segment by segment, as a
  * function of (seed, column, row_base + row): l_orderkey (4 rows per key), l_quantity
  * U[1,50], l_extendedprice U[90000,10500000], l_discount U[0,10], l_shipdate uniform

@@ -12,8 +12,12 @@ OUT="$HERE/_ref"
 [ -d "$REF" ] || { echo "reference sources not present; skipping"; exit 0; }
 mkdir -p "$OUT"
 FLAGS="-std=c++17 -O1 -DTHRUST_DEVICE_SYSTEM=THRUST_DEVICE_SYSTEM_CPP -DTHRUST_HOST_SYSTEM=THRUST_HOST_SYSTEM_CPP"
+# the LIKE matcher (struct gpu_regex, filter.cu) is self-contained: its lines are cut from
+# the reference file into the build folder and compiled for the host with the rest
+sed -n '/^struct gpu_regex/,/^};/p' "$REF/filter.cu" > "$OUT/gpu_regex.inc"
 g++ $FLAGS -I"$HERE/ref_shim" -I/usr/local/cuda/include -include "$HERE/ref_shim/cuda_host_shim.h" \
-  -include algorithm -DREF_COMPRESS_CU="\"$REF/compress.cu\"" -c "$HERE/ref_driver.cpp" -o "$OUT/ref_driver.o"
+  -include algorithm -DREF_COMPRESS_CU="\"$REF/compress.cu\"" -DREF_GPU_REGEX="\"$OUT/gpu_regex.inc\"" \
+  -c "$HERE/ref_driver.cpp" -o "$OUT/ref_driver.o"
 g++ -O1 -include cstddef -x c++ -c "$REF/MurmurHash2_64.cu" -o "$OUT/murmur.o"
 g++ -o "$OUT/ref_driver" "$OUT/ref_driver.o" "$OUT/murmur.o"
 echo "built $OUT/ref_driver"

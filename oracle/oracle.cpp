@@ -28,6 +28,49 @@
 #include "../alenka_b200/host/script.h"
 
 namespace orc {
+
+// LIKE as gpu_regex (filter.cu:67-129) matches one fixed-width dictionary entry: '%' any
+// run of characters, '?' any character except '.', every other pattern character
+// itself. An entry ends at its first NUL or at the width; at most `width` characters are
+// examined in all, counting each retry one character further after a '%'. pat is
+// NUL-terminated.
+bool like_match(const char* entry, uint32_t width, const char* pat) {
+  bool after_pct = false;
+  uint32_t seen = 0;
+  const char* from = entry;  // where the current attempt starts in the entry
+  const char* pfrom = pat;   // and in the pattern
+  for (;;) {
+    const char* s = from;
+    const char* p = pfrom;
+    int how = 0;  // 0 entry exhausted (or the count reached), 1 a '%' restarts, 2 mismatch
+    while (seen < width && *s) {
+      if (*p == '%') {
+        after_pct = true;
+        from = s;
+        pfrom = p + 1;
+        while (*pfrom == '%') ++pfrom;
+        if (!*pfrom) return true;
+        how = 1;
+        break;
+      }
+      if (*p == '?' ? *s == '.' : *s != *p) {
+        how = 2;
+        break;
+      }
+      ++s;
+      ++p;
+      ++seen;
+    }
+    if (how == 1) continue;
+    if (how == 0) {
+      while (*p == '%') ++p;
+      return *p == 0;
+    }
+    if (!after_pct) return false;
+    ++from;
+    ++seen;
+  }
+}
 using std::map;
 using std::set;
 using std::string;
@@ -649,8 +692,27 @@ class Engine {
           string v1 = pop(exe_value), v2 = pop(exe_value);
           if (s1 == "NAME" && s2 == "STRING") std::swap(v1, v2);  // v1 literal, v2 column
           if (v2.find('.') != string::npos) throw Error("bitmap-index predicates are not supported");
-          if (cmp == 7) throw Error("LIKE is not supported");
           const ColInfo& ci = a->info.at(v2);
+          if (cmp == 7) {
+            // LIKE: every dictionary entry is matched once and a row passes when its
+            // code is among the matches (filter.cu:454-500)
+            const auto& dict = file(a->load_file_name + "." + v2);
+            const uint32_t w = ci.char_size;
+            const size_t entries = w ? dict.size() / w : 0;
+            std::vector<char> pat(std::max<size_t>(w, v1.size()) + 1, '\0');
+            std::memcpy(pat.data(), v1.data(), v1.size());
+            std::vector<char> hit(entries);
+            for (size_t k = 0; k < entries; k++)
+              hit[k] = like_match((const char*)dict.data() + k * w, w, pat.data());
+            const Vec& codes = cols.at(v2);
+            for (size_t i = 0; i < n; i++) {
+              const i64 c = codes[i];
+              (*res)[i] = (c >= 0 && (size_t)c < entries && hit[c]) ? 1 : 0;
+            }
+            exe_type.push_back("NAME");
+            bools.push_back(res);
+            continue;
+          }
           string lit = v1;
           while (lit.size() < ci.char_size) lit.push_back('\0');
           uint64_t hv = murmur(lit.data(), (int)lit.size(), alk::kHashSeed) / 2;
@@ -1658,6 +1720,10 @@ int oracle_execute(const char* dir, const char* script, int threads, char* err, 
   }
   return 0;
 }
+int oracle_like(const char* entry, uint32_t width, const char* pattern) {
+  return orc::like_match(entry, width, pattern) ? 1 : 0;
+}
+
 int64_t oracle_decode_segment(const uint8_t* image, size_t len, int64_t* out, size_t out_cap) {
   orc::Decoded d;
   if (!orc::decode_image(image, len, d)) return -1;

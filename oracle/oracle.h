@@ -20,6 +20,9 @@ int oracle_execute(const char* dir, const char* script, int threads, char* err, 
 // Decode one segment file image into int64 values (pfor_decompress, compress.cu:180-267).
 // Returns the row count, or -1 on a malformed image.
 int64_t oracle_decode_segment(const uint8_t* image, size_t len, int64_t* out, size_t out_cap);
+/* 1 when the fixed-width entry matches the NUL-terminated LIKE pattern (gpu_regex,
+ * filter.cu:67-129). */
+int oracle_like(const char* entry, uint32_t width, const char* pattern);
 uint64_t oracle_murmur64a(const void* key, int len, uint32_t seed);
 // Rows scanned by the last oracle_execute (fact rows of every segment visited).
 uint64_t oracle_rows_scanned(void);

@@ -6,7 +6,12 @@
 //                            sets, each with the values pfor_decompress (compress.cu:180)
 //                            reads back
 //   ref_driver murmur <file> MurmurHash64A (MurmurHash2_64.cu:201) of seeded byte strings
+//   ref_driver like <file>   the reference's LIKE matcher (struct gpu_regex, filter.cu:67-129)
+//                            over a fixed set of dictionary entries and patterns
 #include REF_COMPRESS_CU
+#ifdef REF_GPU_REGEX
+#include REF_GPU_REGEX
+#endif
 
 #include <cstdint>
 #include <cstdio>
@@ -101,10 +106,55 @@ static int do_murmur(const std::string& path) {
   return 0;
 }
 
+#ifdef REF_GPU_REGEX
+// Entries of a char column of width 12 (NUL padded; one fills the width) and LIKE
+// patterns shorter than the width, as filter.cu passes them: the entries back to back,
+// the pattern in a zeroed buffer of the column width, len = {width}.
+static int do_like(const std::string& path) {
+  const unsigned int width = 12;
+  const char* entries[] = {"AUTOMOBILE", "BUILDING", "FURNITURE", "HOUSEHOLD", "MACHINERY", "A.B", "A.BC",
+                           "ABC", "abc.def", "%PCT", "100%", "", "X", "XYZXYZXYZXYZ", "..", "a_b", "AAB",
+                           "ABAB", "MACHINE.RY", "ABABABABABA", "BA", "AXBXC"};
+  const char* patterns[] = {"%", "%%", "", "A%", "%A", "%A%", "A?C", "A?B", "???", "?%", "%?", "%.%",
+                            "%B%I%", "BUILDING", "BUILDING%", "BUILD", "%ING", "%Y", "_", "a_b", "X%Z",
+                            "XYZ%XYZ", "%XYZ", "?.?", "A%B%", "%AB", "A%%B", "100%", "%PCT", "%%PCT", "M%Y",
+                            "MACHINE%RY", "M?CHINE.RY", "%BA", "%ABA", "A%C", "%B%C", "?B%", "AB?B", "%?%?"};
+  const size_t ne = sizeof(entries) / sizeof(entries[0]), np = sizeof(patterns) / sizeof(patterns[0]);
+  std::vector<char> src(ne * width, 0);
+  for (size_t i = 0; i < ne; i++) std::memcpy(&src[i * width], entries[i], std::min<size_t>(width, std::strlen(entries[i])));
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) return 1;
+  std::fprintf(f, "width %u\n", width);
+  for (size_t i = 0; i < ne; i++) {
+    std::fprintf(f, "entry ");
+    for (unsigned int k = 0; k < width; k++) std::fprintf(f, "%02x", (unsigned char)src[i * width + k]);
+    std::fprintf(f, "\n");
+  }
+  for (size_t j = 0; j < np; j++) {
+    std::vector<char> pat(width, 0);
+    std::memcpy(pat.data(), patterns[j], std::strlen(patterns[j]));
+    std::vector<char> dest(ne, 0);
+    unsigned int len = width;
+    gpu_regex m(src.data(), pat.data(), (bool*)dest.data(), &len);
+    for (size_t i = 0; i < ne; i++) m(i);
+    std::fprintf(f, "pattern %s ", std::strlen(patterns[j]) ? "" : "-");
+    for (size_t k = 0; k < std::strlen(patterns[j]); k++) std::fprintf(f, "%02x", (unsigned char)patterns[j][k]);
+    std::fprintf(f, " ");
+    for (size_t i = 0; i < ne; i++) std::fprintf(f, "%d", dest[i] ? 1 : 0);
+    std::fprintf(f, "\n");
+  }
+  std::fclose(f);
+  return 0;
+}
+#endif
+
 int main(int argc, char** argv) {
   if (argc < 3) return 2;
   std::string mode = argv[1];
   if (mode == "codec") return do_codec(argv[2]);
   if (mode == "murmur") return do_murmur(argv[2]);
+#ifdef REF_GPU_REGEX
+  if (mode == "like") return do_like(argv[2]);
+#endif
   return 2;
 }

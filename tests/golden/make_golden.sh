@@ -5,6 +5,7 @@
 #   ref_codec/<case>.values  the values encoded (the reference's pfor_decompress
 #                            returns exactly these; the driver checks it)
 #   murmur64a.txt            "<seed> <hex bytes|-> <MurmurHash64A>" lines
+#   like_gpu_regex.txt       the reference's LIKE matcher over fixed entries and patterns
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
 ROOT=$(cd "$HERE/../.." && pwd)
@@ -18,5 +19,6 @@ done
 mkdir -p "$HERE/ref_codec"
 cp "$TMP"/*.seg "$TMP"/*.values "$HERE/ref_codec/"
 "$ROOT/oracle/_ref/ref_driver" murmur "$HERE/murmur64a.txt"
+"$ROOT/oracle/_ref/ref_driver" like "$HERE/like_gpu_regex.txt"
 rm -rf "$TMP"
 echo "golden vectors written to $HERE"

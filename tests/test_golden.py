@@ -88,3 +88,29 @@ def test_gpu_decode_matches_reference(name):
     torch.cuda.synchronize()
     assert rc == 0
     assert np.array_equal(d_out.cpu().numpy()[:rec], vals)
+
+
+def like_golden():
+    """(width, entries as bytes, [(pattern bytes, [0/1 per entry])]) written by the
+    reference's own LIKE matcher (gpu_regex, filter.cu:67-129) via make_golden.sh."""
+    width, entries, cases = 0, [], []
+    for ln in open(os.path.join(GOLD, "like_gpu_regex.txt")).read().splitlines():
+        f = ln.split()
+        if f[0] == "width":
+            width = int(f[1])
+        elif f[0] == "entry":
+            entries.append(bytes.fromhex(f[1]))
+        elif f[0] == "pattern":
+            pat = b"" if f[1] == "-" else bytes.fromhex(f[1])
+            cases.append((pat, [int(c) for c in f[2]]))
+    return width, entries, cases
+
+
+def test_oracle_like_matches_reference():
+    width, entries, cases = like_golden()
+    assert width == 12 and len(entries) == 22 and len(cases) == 40
+    L = _oracle.lib()
+    L.oracle_like.argtypes = [ctypes.c_char_p, ctypes.c_uint32, ctypes.c_char_p]
+    for pat, want in cases:
+        got = [L.oracle_like(e, width, pat + b"\0") for e in entries]
+        assert got == want, pat
