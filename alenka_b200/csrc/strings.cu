@@ -1,4 +1,4 @@
-// LIKE on char columns. The reference evaluates LIKE once per dictionary entry with
+// String predicates and ordering on char columns. LIKE: The reference evaluates LIKE once per dictionary entry with
 // gpu_regex (filter.cu:67-129) over the column's dictionary file, keeps the matching
 // codes, and then tests each row's code against them (filter.cu:454-500). Here the
 // matches become a bitmap over the codes, built by one thread per entry, and the rows'
@@ -75,7 +75,26 @@ __global__ void k_like_dict(const __grid_constant__ LikeArgs a) {
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.bits[0] = (uint32_t)a.count;
 }
+__global__ void k_code_lookup(const int64_t* __restrict__ codes, uint64_t n, const int64_t* __restrict__ table,
+                              uint64_t table_n, int64_t* __restrict__ out) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int64_t c = codes[i];
+    out[i] = (c >= 0 && (uint64_t)c < table_n) ? __ldg(table + c) : -1;
+  }
+}
 }  // namespace
+
+extern "C" int alk_code_lookup(const int64_t* d_codes, uint64_t n, const int64_t* d_table, uint64_t table_n,
+                               int64_t* d_out, alk_stream stream) {
+  if (n == 0) return ALK_OK;
+  if (!d_codes || !d_table || !d_out) return ALK_ERR_ARG;
+  const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148ull * 8));
+  k_code_lookup<<<grid, 256, 0, (cudaStream_t)stream>>>(d_codes, n, d_table, table_n, d_out);
+  alk::g_kernel_launches++;
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? ALK_OK : alk::cuda_fail(e);
+}
 
 extern "C" int alk_like_dictionary(const char* d_dict, uint32_t width, uint64_t count, const char* pattern,
                                    uint32_t pattern_len, uint32_t* d_bits, alk_stream stream) {

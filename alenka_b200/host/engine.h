@@ -76,6 +76,7 @@ struct BaseCol {
   std::unordered_map<uint64_t, int64_t> hash_to_code;
   bool dict_loaded = false;
   std::map<std::string, DevBufP> like_sets;  // LIKE pattern -> its matching codes [n, bits]
+  DevBufP ranks;                             // entry -> dense rank in byte order (ORDER BY)
 };
 
 struct Var {
@@ -252,6 +253,7 @@ class Engine {
   void emit_store(Statement& st);
   void emit_store_binary(Statement& st);
   DevBufP like_set(Var* base, const std::string& col, const std::string& pattern);
+  const DevBufP& dict_ranks(const ColMeta& m);
   std::map<std::string, uint32_t> cnt_counts_;  // largest payload written per column file prefix
   bool try_fused(std::vector<Statement>& sts, size_t& i);
   void run_fused(Statement& J, Statement& F, Statement& O, Statement& S, const std::string& gkey);

@@ -1366,8 +1366,6 @@ void Engine::emit_order(Statement& st) {
       desc.push_back(st.op_value.at(iv++) == "DESC");
     }
     if (!a->has(keys.back())) throw EngineError(ALK_ERR_ARG, "Couldn't find name " + keys.back());
-    if (a->meta[keys.back()].type == 2 || !a->meta[keys.back()].string_map.empty())
-      unsupported("ORDER BY on a char column");
   }
   Rows R = materialize(a, a->columnNames);
   auto b = std::make_unique<Var>();
@@ -1379,7 +1377,25 @@ void Engine::emit_order(Statement& st) {
   b->n = R.n;
   if (R.n) {
     std::vector<const int64_t*> kc;
-    for (auto& kname : keys) kc.push_back(R.col.at(kname)->as<int64_t>());
+    std::vector<DevBufP> ranked;  // char keys: each row's dictionary code replaced by its rank
+    for (auto& kname : keys) {
+      const ColMeta& m = a->meta[kname];
+      if (m.type != 2 && m.string_map.empty()) {
+        kc.push_back(R.col.at(kname)->as<int64_t>());
+        continue;
+      }
+      // the reference sorts the strings themselves, bytes compared unsigned over the full
+      // width, stably (update_char_permutation cm.cu:4218, str_sort
+      // strings_sort_device.cu:125): the same order as the entries' ranks in the sorted
+      // dictionary, equal strings sharing a rank
+      const DevBufP& rank = dict_ranks(m);
+      auto key = mkbuf(R.n * 8, stream_);
+      check(alk_code_lookup(R.col.at(kname)->as<int64_t>(), R.n, rank->as<int64_t>(), rank->bytes() / 8,
+                            key->as<int64_t>(), (alk_stream)stream_),
+            "order char key");
+      ranked.push_back(key);
+      kc.push_back(key->as<int64_t>());
+    }
     auto perm = mkbuf(R.n * 4, stream_);
     check(alk_sort_perm(kc.data(), desc.data(), (uint32_t)kc.size(), R.n, perm->as<uint32_t>(), (alk_stream)stream_),
           "order");
@@ -1393,6 +1409,36 @@ void Engine::emit_order(Statement& st) {
     for (auto& n : a->columnNames) b->data[n] = mkbuf(8, stream_);
   }
   vars_[st.s] = std::move(b);
+}
+
+// Dense ranks of a char column's dictionary entries in byte order (unsigned, full
+// width), on the device, kept with the column.
+const DevBufP& Engine::dict_ranks(const ColMeta& m) {
+  const auto dot = m.string_map.find('.');
+  Var* b = dot == std::string::npos ? nullptr : base_table(m.string_map.substr(0, dot));
+  if (!b) throw EngineError(ALK_ERR_IO, "missing dictionary " + m.string_map);
+  BaseCol& bc = basecol(b, m.string_map.substr(dot + 1));
+  if (bc.ranks) return bc.ranks;
+  load_dict(b, m.string_map.substr(dot + 1), bc);
+  const size_t n = bc.dict.size();
+  std::vector<uint32_t> order(n);
+  std::iota(order.begin(), order.end(), 0u);
+  auto less = [&](uint32_t x, uint32_t y) {
+    return std::memcmp(bc.dict[x].data(), bc.dict[y].data(), bc.dict[x].size()) < 0;
+  };
+  std::stable_sort(order.begin(), order.end(), less);
+  std::vector<int64_t> rank(std::max<size_t>(n, 1), 0);
+  int64_t r = 0;
+  for (size_t i = 0; i < n; i++) {
+    if (i && less(order[i - 1], order[i])) r++;
+    rank[order[i]] = r;
+  }
+  bc.ranks = mkbuf(rank.size() * 8, stream_);
+  ck(cudaMemcpyAsync(bc.ranks->as<void>(), rank.data(), rank.size() * 8, cudaMemcpyHostToDevice, stream_),
+     "ranks h2d");
+  ck(cudaStreamSynchronize(stream_), "ranks h2d");
+  stats_.h2d_bytes += rank.size() * 8;
+  return bc.ranks;
 }
 
 // ------------------------------------------------------------------ STORE

@@ -195,6 +195,12 @@ typedef struct alk_program {
  * count in word 0 and bit k set for each match: the set ALK_OP_INSET tests. */
 int alk_like_dictionary(const char* d_dict, uint32_t width, uint64_t count, const char* pattern,
                         uint32_t pattern_len, uint32_t* d_bits, alk_stream stream);
+/* d_out[i] = d_table[d_codes[i]] for codes in [0, table_n), else -1: a char column's
+ * dictionary codes mapped to their entries' ranks in byte order, which ORDER BY sorts
+ * (update_char_permutation cm.cu:4218 sorts the strings themselves; the order is the
+ * same). */
+int alk_code_lookup(const int64_t* d_codes, uint64_t n, const int64_t* d_table, uint64_t table_n, int64_t* d_out,
+                    alk_stream stream);
 
 /* Fused segment scan, replaces filter_op + filter + copyColumns/mygather
  * (cm.cu:3609-3666, filter.cu:133-643, cm.cu:3305-3478): for every segment whose

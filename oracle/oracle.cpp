@@ -1622,10 +1622,26 @@ class Engine {
     vector<u32> perm(s.n);
     std::iota(perm.begin(), perm.end(), 0);
     for (size_t k = keys.size(); k-- > 0;) {
-      if (a->info[keys[k]].type == 2 || !a->info[keys[k]].string_map.empty())
-        throw Error("ORDER BY on a char column is not supported by the oracle");
-      const Vec& key = s.c.at(keys[k]);
       bool desc = dirs[k] == "DESC";
+      if (a->info[keys[k]].type == 2 || !a->info[keys[k]].string_map.empty()) {
+        // the rows' strings read from the dictionary by code and sorted stably as unsigned
+        // bytes over the column width (update_char_permutation cm.cu:4218, str_sort
+        // strings_sort_device.cu:125)
+        const string& sm = a->info[keys[k]].string_map;
+        const auto& dict = file(sm);
+        auto pos = sm.find_last_of('/');
+        string base = pos == string::npos ? sm : sm.substr(pos + 1);
+        auto dot = base.find('.');
+        const u32 w = dd_[base.substr(0, dot)][base.substr(dot + 1)].col_length;
+        const Vec& code = s.c.at(keys[k]);
+        auto str = [&](u32 r) { return dict.data() + (size_t)code[r] * w; };
+        __gnu_parallel::stable_sort(perm.begin(), perm.end(), [&](u32 x, u32 y) {
+          const int c = std::memcmp(str(x), str(y), w);
+          return desc ? c > 0 : c < 0;
+        });
+        continue;
+      }
+      const Vec& key = s.c.at(keys[k]);
       __gnu_parallel::stable_sort(perm.begin(), perm.end(), [&](u32 x, u32 y) {
         return desc ? key[x] > key[y] : key[x] < key[y];
       });
