@@ -267,6 +267,7 @@ class Engine {
   std::set<std::string> fused_seen_;
   std::set<std::string> fused_nograph_;  // queries whose capture failed
   std::string cur_script_;
+  std::unordered_map<std::string, std::vector<Statement>> parsed_;  // script text -> statements
   // a batch's final STOREs: formatted at once, written together after the batch (the
   // file creations dominate a small result's store) on several threads
   struct PendingWrite {

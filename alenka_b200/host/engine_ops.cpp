@@ -1826,9 +1826,17 @@ int Engine::execute(const std::string& script) {
   std::vector<Statement> sts;
   std::string perr;
   err_.clear();
-  if (!parse_script(script, sts, perr)) {
-    err_ = "parse: " + perr;
-    return ALK_ERR_PARSE;
+  // a script seen before is not parsed again: each run works on a copy of its statements
+  auto pc = parsed_.find(script);
+  if (pc != parsed_.end()) {
+    sts = pc->second;
+  } else {
+    if (!parse_script(script, sts, perr)) {
+      err_ = "parse: " + perr;
+      return ALK_ERR_PARSE;
+    }
+    if (parsed_.size() >= 256) parsed_.clear();
+    parsed_.emplace(script, sts);
   }
   reset_script_state();
   cur_script_ = script;
