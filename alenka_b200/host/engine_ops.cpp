@@ -1471,11 +1471,6 @@ void Engine::emit_store(Statement& st) {
   }
   std::string path = st.f;
   if (path.empty() || path[0] != '/') path = dir_ + "/" + path;
-  FILE* fp = nullptr;
-  if (!deferred_writes_) {
-    fp = std::fopen(path.c_str(), "w");
-    if (!fp) throw EngineError(ALK_ERR_IO, "Could not open file " + path);
-  }
   std::vector<const std::vector<std::string>*> dicts(a->columnNames.size(), nullptr);
   std::vector<uint32_t> widths(a->columnNames.size(), 0);
   for (size_t c = 0; c < a->columnNames.size(); c++) {
@@ -1534,8 +1529,13 @@ void Engine::emit_store(Statement& st) {
     deferred_writes_->push_back(std::move(w));
     return;
   }
-  for (auto& part : parts) std::fwrite(part.data(), 1, part.size(), fp);
-  std::fclose(fp);
+  std::string all;
+  if (parts.size() == 1) {
+    all.swap(parts[0]);
+  } else {
+    for (auto& part : parts) all += part;
+  }
+  if (!write_file(path, all.data(), all.size())) throw EngineError(ALK_ERR_IO, "Could not open file " + path);
 }
 
 // STORE v INTO 'name' [APPEND] [LIMIT n] BINARY: the binary branch of CudaSet::Store
@@ -1678,13 +1678,7 @@ void Engine::write_files(const std::vector<PendingWrite>& writes,
   auto worker = [&] {
     for (size_t g; (g = next.fetch_add(1)) < groups.size();)
       for (size_t k : *groups[g]) {
-        FILE* fp = std::fopen(writes[k].path.c_str(), "w");
-        if (!fp) {
-          ok[k] = 0;
-          continue;
-        }
-        std::fwrite(writes[k].data.data(), 1, writes[k].data.size(), fp);
-        std::fclose(fp);
+        if (!write_file(writes[k].path, writes[k].data.data(), writes[k].data.size())) ok[k] = 0;
       }
   };
   const size_t nth = std::min<size_t>(groups.size(), std::min<size_t>(16, std::max(1u, std::thread::hardware_concurrency())));
@@ -2696,8 +2690,6 @@ void Engine::store_fused_rows(const FusedTail& t, std::vector<std::vector<int64_
   // ---- STORE (cm.cu:1479-1560)
   std::string path = t.path;
   if (path.empty() || path[0] != '/') path = dir_ + "/" + path;
-  FILE* fp = std::fopen(path.c_str(), "w");
-  if (!fp) throw EngineError(ALK_ERR_IO, "Could not open file " + path);
   std::vector<const std::vector<std::string>*> dicts(nouts, nullptr);
   for (size_t c = 0; c < nouts; c++) {
     const std::string& sm = fmeta[c].string_map;
@@ -2709,7 +2701,7 @@ void Engine::store_fused_rows(const FusedTail& t, std::vector<std::vector<int64_
     load_dict(b, sm.substr(dot + 1), bc);
     dicts[c] = &bc.dict;
   }
-  std::string line;
+  std::string line, all;
   for (size_t r = 0; r < rows; r++) {
     line.clear();
     for (size_t c = 0; c < nouts; c++) {
@@ -2730,9 +2722,9 @@ void Engine::store_fused_rows(const FusedTail& t, std::vector<std::vector<int64_
       line += t.sep;
     }
     if (r + 1 != rows) line += "\n";
-    std::fputs(line.c_str(), fp);
+    all += line;
   }
-  std::fclose(fp);
+  if (!write_file(path, all.data(), all.size())) throw EngineError(ALK_ERR_IO, "Could not open file " + path);
 }
 
 }  // namespace alk
