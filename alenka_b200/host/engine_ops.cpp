@@ -1249,7 +1249,12 @@ void Engine::emit_join(Statement& st) {
     *it = to;
     r->data[to] = r->data[from];
     r->data.erase(from);
+    // the rename carries the type and the decimal flag but not decimal_zeroes
+    // (operators.cu:877-906): the alias keeps its previous scale, 0 for a new name, and
+    // that scale is what later arithmetic (get_decimals, cm.cu:4371) and STORE use
+    uint32_t dz_to = r->meta.count(to) ? r->meta[to].dz : 0;
     r->meta[to] = r->meta[from];
+    r->meta[to].dz = dz_to;
   }
 }
 
@@ -2124,6 +2129,12 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     std::string alias = it == op_sel.end() ? n : op_alias[it - op_sel.begin()];
     jv.columnNames.push_back(alias);
     jv.meta[alias] = origin(n)->meta[n];
+    if (alias != n) {
+      // an aliased join column keeps the alias's scale, not its own (operators.cu:877-906):
+      // the scale of a selected column of that name, else 0
+      bool named = std::find(st2.out.begin(), st2.out.end(), alias) != st2.out.end();
+      jv.meta[alias].dz = named ? origin(alias)->meta[alias].dz : 0;
+    }
     src_of[alias] = n;
   }
   std::vector<std::string> group_cols(F.op_value.end() - F.grp_cnt, F.op_value.end());

@@ -1,12 +1,15 @@
 #!/bin/bash
-# Builds oracle/_ref/ref_driver from the reference's own sources in place
-# (/root/reference/compress.cu and MurmurHash2_64.cu) for the CPU: Thrust's CPP device
-# system plus the host shims in oracle/ref_shim (CUDA runtime calls -> host memory,
-# the absent moderngpu headers, Thrust 2.x's removed pinned_allocator). Outputs go to
-# oracle/_ref only. The rest of the reference (the operators) needs moderngpu, which
-# the reference does not vendor, and is not built.
+# Builds, from the reference's own sources in place (ALENKA_REF, default
+# /root/reference), for the CPU:
+#   oracle/_ref/ref_driver  its codec (compress.cu), MurmurHash64A and LIKE matcher,
+#                           driven by oracle/ref_driver.cpp to write golden vectors
+#   oracle/_ref/alenka_ref  the whole reference CLI (bison front end, operators, codec)
+#                           under Thrust's OpenMP device system (oracle/ref.mk)
+# The host shims in oracle/ref_shim stand in for the CUDA runtime calls (host memory),
+# Thrust 2.x's removed pinned_allocator and the moderngpu primitives the reference does
+# not vendor. Outputs go to oracle/_ref only.
 set -e
-REF=${REF:-/root/reference}
+REF=${ALENKA_REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 [ -d "$REF" ] || { echo "reference sources not present; skipping"; exit 0; }
@@ -21,3 +24,6 @@ g++ $FLAGS -I"$HERE/ref_shim" -I/usr/local/cuda/include -include "$HERE/ref_shim
 g++ -O1 -include cstddef -x c++ -c "$REF/MurmurHash2_64.cu" -o "$OUT/murmur.o"
 g++ -o "$OUT/ref_driver" "$OUT/ref_driver.o" "$OUT/murmur.o"
 echo "built $OUT/ref_driver"
+# the whole reference (bison front end, operators, codec) for the CPU: oracle/_ref/alenka_ref
+make -s -j"$(nproc)" -f "$HERE/ref.mk" REF="$REF"
+echo "built $OUT/alenka_ref"

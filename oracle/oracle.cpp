@@ -1489,7 +1489,13 @@ class Engine {
       *it = to;
       r->h[to] = std::move(r->h[from]);
       r->h.erase(from);
+      // the rename carries type and the decimal flag but not decimal_zeroes
+      // (operators.cu:877-906): an aliased decimal column of a join result keeps the
+      // alias's previous scale, 0 for a new name, for printing and for arithmetic
+      // (get_decimals, cm.cu:4371)
+      u32 dz_to = r->info.count(to) ? r->info[to].dz : 0;
       r->info[to] = r->info[from];
+      r->info[to].dz = dz_to;
     }
   }
 

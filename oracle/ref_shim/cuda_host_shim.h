@@ -1,5 +1,6 @@
-// Host stand-ins for the CUDA runtime calls the reference codec makes, so that
-// compress.cu runs on the CPU with Thrust's CPP device system.
+// Host stand-ins for the CUDA runtime calls the reference makes, so that its sources
+// (codec, operators, front end) build for the CPU with Thrust's host device systems
+// (CPP or OMP): device memory becomes host memory. Test infrastructure only.
 #pragma once
 #include <cstdlib>
 #include <cstring>
@@ -10,6 +11,7 @@ typedef int cudaError_t;
 enum { cudaSuccess = 0 };
 enum cudaMemcpyKind { cudaMemcpyHostToHost, cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, cudaMemcpyDeviceToDevice };
 inline int cudaMalloc(void** p, size_t n) { *p = std::malloc(n ? n : 1); return 0; }
+template <class T> inline int cudaMalloc(T** p, size_t n) { return cudaMalloc((void**)p, n); }
 inline int cudaFree(void* p) { std::free(p); return 0; }
 inline int cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind) { std::memmove(d, s, n); return 0; }
 inline int cudaMemset(void* d, int v, size_t n) { std::memset(d, v, n); return 0; }
@@ -17,6 +19,7 @@ inline int cudaThreadSynchronize() { return 0; }
 inline int cudaDeviceSynchronize() { return 0; }
 inline const char* cudaGetErrorString(int) { return "shim"; }
 inline int cudaHostAlloc(void** p, size_t n, unsigned) { *p = std::malloc(n ? n : 1); return 0; }
+template <class T> inline int cudaHostAlloc(T** p, size_t n, unsigned f) { return cudaHostAlloc((void**)p, n, f); }
 inline int cudaFreeHost(void* p) { std::free(p); return 0; }
 inline int cudaMemGetInfo(size_t* f, size_t* t) { *f = *t = (size_t)180 << 30; return 0; }
 #define cudaHostAllocDefault 0

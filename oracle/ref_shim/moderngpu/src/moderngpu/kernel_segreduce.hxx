@@ -1,10 +1,3 @@
-// Stand-in for the moderngpu header the reference includes (moderngpu is not vendored).
-// Only the names cm.h mentions are declared; nothing here is called by the codec.
+// moderngpu header name the reference includes; the host restatement is in mgpu_host.hxx.
 #pragma once
-namespace mgpu {
-struct standard_context_t {};
-template <class T> struct plus_t {};
-template <class T> struct minimum_t {};
-template <class T> struct maximum_t {};
-template <class T> struct less_t {};
-}  // namespace mgpu
+#include "mgpu_host.hxx"

@@ -1,6 +1,7 @@
 #!/bin/bash
 # Regenerates the golden vectors from the reference's own code: builds
-# oracle/_ref/ref_driver from /root/reference (oracle/build_ref.sh), then writes
+# oracle/_ref/ref_driver from the reference sources (oracle/build_ref.sh; ALENKA_REF
+# names the checkout), then writes
 #   ref_codec/<case>.seg     segment files written by the reference's pfor_compress
 #   ref_codec/<case>.values  the values encoded (the reference's pfor_decompress
 #                            returns exactly these; the driver checks it)
