@@ -794,7 +794,8 @@ int alk_decode_segment(const void* d_payload, uint32_t comp_type, uint32_t bits,
   if (comp_type != 1 || bits == 0 || bits > 64 || fit_count != 64 / bits) return ALK_ERR_ARG;
   Scratch sc(s);
   cudaError_t e;
-  uint32_t ntiles = (rows + kTile - 1) / kTile;
+  // in 64 bits: rows + kTile - 1 wraps in 32 bits for rows near 2^32
+  const uint32_t ntiles = (uint32_t)(((uint64_t)rows + kTile - 1) / kTile);
   uint32_t* flags = sc.get<uint32_t>(ntiles + 2, &e);
   CK(e);
   uint64_t* aggs = sc.get<uint64_t>(ntiles, &e);
@@ -833,7 +834,9 @@ std::mutex g_scratch_mu;
 void* g_scratch_addr[kMaxDevices] = {};
 
 // Device address of g_decode_scratch on the current device, looked up once per device
-// (host code cannot use the array's name as a device address).
+// (host code cannot use the array's name as a device address) and kept for the life of
+// the process: a device reset (cudaDeviceReset) after the first call is not supported,
+// because the array may then live at another address.
 int noalloc_scratch(unsigned char** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -866,8 +869,9 @@ int alk_decode_segment_noalloc(const void* d_payload, uint32_t comp_type, uint32
     return ALK_OK;
   }
   if (comp_type != 1 || bits == 0 || bits > 64 || fit_count != 64 / bits) return ALK_ERR_ARG;
-  const uint32_t ntiles = (rows + kTile - 1) / kTile;
-  if (ntiles > kNoAllocMaxTiles) return ALK_ERR_TOO_LARGE;
+  // the row count is tested before any tile arithmetic, so no count wraps past the limit
+  if ((uint64_t)rows > (uint64_t)kNoAllocMaxTiles * kTile) return ALK_ERR_TOO_LARGE;
+  const uint32_t ntiles = (uint32_t)(((uint64_t)rows + kTile - 1) / kTile);
   unsigned char* base = nullptr;
   int rc = noalloc_scratch(&base);
   if (rc) return rc;

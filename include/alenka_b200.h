@@ -115,14 +115,15 @@ int alk_decode_segment(const void* d_payload, uint32_t comp_type, uint32_t bits,
 
 /* Segment decode that allocates nothing. No counterpart in the reference: this entry point
  * exists for callers that cannot call cudaMalloc, for example a host that has committed
- * all device memory to its own pools (as the reference sizes its work to the free memory,
- * cm.cu:3184, 3565) or a decode path that must never fail or stall on an allocation.
+ * all device memory to its own pools or a decode path that must never fail or stall on
+ * an allocation.
  * Same arguments and results as alk_decode_segment. FOR segments need no scratch; a
  * FOR-delta segment keeps its scan state in one fixed device array of the library
  * (about 0.6 MB per device, held until the process exits), so at most 67,108,864 rows
  * (32768 tiles of 2048 rows) per call: larger segments return ALK_ERR_TOO_LARGE without
  * touching the device. The first call on each device looks up that array's device
- * address (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * address (cudaGetSymbolAddress) and keeps it, so make that first call before any stream
+ * capture, and do not reset the device (cudaDeviceReset) after it.
  * Every call on a device shares the array: calls that overlap on the GPU (concurrent
  * streams, or threads sharing a device) race and must be serialized by the caller. */
 int alk_decode_segment_noalloc(const void* d_payload, uint32_t comp_type, uint32_t bits,

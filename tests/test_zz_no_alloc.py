@@ -83,13 +83,42 @@ def test_noalloc_matches_allocating_decode_twice_in_a_row():
             assert np.array_equal(got, want), (name, call)
 
 
-def test_noalloc_rejects_segments_above_its_maximum():
+@pytest.mark.parametrize("rows", [MAX_ROWS + 1, 0xFFFFFFFF, 0xFFFFF801])
+def test_noalloc_rejects_segments_above_its_maximum(rows):
+    # 0xFFFFFFFF and 0xFFFFF801 would wrap a 32-bit tile count to 0; both must be refused
     import torch
     L = _lib()
     payload = torch.zeros(4096, dtype=torch.uint8, device="cuda")
     out = torch.full((8,), -7, dtype=torch.int64, device="cuda")
     torch.cuda.synchronize()
-    rc = L.alk_decode_segment_noalloc(payload.data_ptr(), 1, 2, 32, 0, 0, MAX_ROWS + 1, out.data_ptr(), None)
+    rc = L.alk_decode_segment_noalloc(payload.data_ptr(), 1, 2, 32, 0, 0, rows, out.data_ptr(), None)
     torch.cuda.synchronize()
     assert rc == ALK_ERR_TOO_LARGE
     assert (out.cpu().numpy() == -7).all()
+
+
+def test_noalloc_accepts_exactly_its_maximum_and_allocates_nothing():
+    """MAX_ROWS rows of a 1-bit FOR-delta segment (an 8 MB payload, a 512 MB output):
+    accepted and decoded exactly, twice, with the device's free memory unchanged across
+    the warm calls."""
+    import torch
+    L = _lib()
+    rng = np.random.default_rng(77)
+    steps = rng.integers(0, 2, MAX_ROWS, dtype=np.int64)
+    steps[0] = 0
+    values = np.cumsum(steps) + 1000
+    meta, payload = _segment(values, True)
+    assert meta["comp"] == 1 and meta["bits"] == 1 and meta["rows"] == MAX_ROWS
+    out = torch.full((MAX_ROWS,), -7, dtype=torch.int64, device="cuda")
+    args = (payload.data_ptr(), meta["comp"], meta["bits"], meta["fit"], meta["lower"], meta["start"],
+            meta["rows"], out.data_ptr(), None)
+    assert L.alk_decode_segment_noalloc(*args) == 0  # first call: looks up the array's address
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    for call in range(2):
+        out.fill_(-7)
+        torch.cuda.synchronize()
+        assert L.alk_decode_segment_noalloc(*args) == 0, call
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free_before, call
+        assert np.array_equal(out.cpu().numpy(), values), call
