@@ -1384,11 +1384,12 @@ int alk_ht_create_range(uint64_t max_keys, uint32_t npay, int64_t key_min, int64
   uint64_t cap = 1024;
   while (cap < 2 * max_keys) cap <<= 1;
   const uint64_t slot_cap = cap;  // payload is indexed by table position
-  // exact key bitmap when the key range is at most 2^29 values (64 MB)
+  // exact key bitmap when the key range is below 2^32 values (at most 512 MB); bit
+  // offsets then fit the 32-bit probe path
   uint64_t nbits = 0;
   if (key_max >= key_min) {
     uint64_t span = (uint64_t)key_max - (uint64_t)key_min + 1;
-    if (span != 0 && span <= (1ull << 29)) nbits = span;
+    if (span != 0 && span <= ALK_DENSE_MAX_SPAN) nbits = span;
   }
   // the empty marker must not be a possible key
   if (key_max >= key_min && kEmptyKey >= key_min && kEmptyKey <= key_max) {
@@ -1430,7 +1431,7 @@ int alk_ht_create_dense(uint64_t max_keys, uint32_t npay, int64_t key_min, int64
   cudaStream_t s = (cudaStream_t)stream;
   if (!out || npay > 8 || max_keys >= 0xffffffffull || key_max < key_min) return ALK_ERR_ARG;
   const uint64_t span = (uint64_t)key_max - (uint64_t)key_min + 1;
-  if (span == 0 || span > (1ull << 29)) return ALK_ERR_UNSUPPORTED;  // no exact bitmap
+  if (span == 0 || span > ALK_DENSE_MAX_SPAN) return ALK_ERR_UNSUPPORTED;  // no exact bitmap
   const uint64_t cap = std::max<uint64_t>(max_keys, 1);  // slots are ranks: no spare room
   const size_t words = (span + 31) / 32;
   const size_t off_pay = cap * 8;
@@ -1590,7 +1591,7 @@ static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* co
           sp[g].kmember = 1;
           sp[g].xlo = (uint32_t)lo;
           sp[g].xspan = (uint32_t)(hi - lo);
-          sp[g].boff = (uint32_t)(lo - blo);  // < nbits <= 2^29
+          sp[g].boff = (uint32_t)(lo - blo);  // < nbits < 2^32
         }
       }
     }

@@ -2237,10 +2237,11 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     }
     if (card_record_) card_record(cst);
     g.s = s;
-    // a key range of at most 2^29 values (the zone maps) takes the dense, rank-addressed
-    // table; wider ranges the hash table
+    // a key range below 2^32 values (the zone maps) takes the dense, rank-addressed
+    // table (a bitmap of span/8 bytes plus a u32 rank per bitmap word: 150 MB for the
+    // 600M-wide o_orderkey range of a 150M-row orders table); wider ranges the hash table
     const bool dense = range.second >= range.first &&
-                       (uint64_t)range.second - (uint64_t)range.first < (1ull << 29);
+                       (uint64_t)range.second - (uint64_t)range.first < ALK_DENSE_MAX_SPAN;
     if (dense) check(alk_ht_create_dense(est, npay, range.first, range.second, &g.h, (alk_stream)s), "dense table");
     else check(alk_ht_create_range(est, npay, range.first, range.second, &g.h, (alk_stream)s), "hash table");
     check(run(g.h, hcap, &fs->st[idx]), "build stage");

@@ -284,14 +284,18 @@ void alk_join_free(alk_join_table* t, alk_stream stream);
 typedef struct alk_ht alk_ht;
 /* max_keys bounds the inserted keys; npay payload columns (<= 8) per key. */
 int alk_ht_create(uint64_t max_keys, uint32_t npay, alk_ht** out, alk_stream stream);
+/* Widest key range (values) that gets an exact key bitmap: bit offsets stay below 2^32,
+ * and the bitmap takes at most 512 MB. */
+#define ALK_DENSE_MAX_SPAN 0xFFFFFFFFull
 /* Same, for keys known to lie in [key_min, key_max] (the build column's zone maps): the
  * table then also keeps an exact membership bitmap of the inserted keys (when the range
- * spans at most 2^29 values) that probes test before hashing. A key inserted outside
- * the range sets flag 8. */
+ * spans at most ALK_DENSE_MAX_SPAN values) that probes test before hashing. A key
+ * inserted outside the range sets flag 8. */
 int alk_ht_create_range(uint64_t max_keys, uint32_t npay, int64_t key_min, int64_t key_max, alk_ht** out,
                         alk_stream stream);
 /* Dense (rank-addressed) build table for keys known to lie in [key_min, key_max], a
- * range of at most 2^29 values (from the build column's zone maps): a build stage sets the
+ * range of at most ALK_DENSE_MAX_SPAN values (from the build column's zone maps): a build
+ * stage sets the
  * keys' bits in an exact bitmap, a prefix pass ranks them, and a key's slot is its rank
  * among the keys present, so keys, payload and per-key accumulators are dense over
  * [0, inserted) with no hashing. max_keys is the slot capacity (more distinct keys set
