@@ -233,6 +233,20 @@ struct HitWriter {
       if (e < a.hit_cap) a.hits[e * a.hit_words] = pos0 + (uint64_t)k * kStride;
     }
   }
+  // Appends the lanes' live items as positions row0 + k of segment seg, where each lane
+  // owns the consecutive rows row0 .. row0 + 7 (blocked layout). Warp-wide.
+  __device__ __forceinline__ void append_blocked(const StageArgs& a, uint32_t live, uint32_t seg, uint32_t row0) {
+    if (!__any_sync(0xffffffffu, live)) return;
+    uint32_t excl;
+    const uint32_t total = warp_offsets(__popc(live), &excl);
+    const Room r = reserve(a, total);
+    const uint64_t pos0 = (uint64_t)seg << 32 | row0;
+    uint32_t i = excl;
+    for (uint32_t m = live; m; m &= m - 1, i++) {
+      const uint64_t e = r.at(i);
+      if (e < a.hit_cap) a.hits[e * a.hit_words] = pos0 + (uint32_t)(__ffs(m) - 1);
+    }
+  }
   // Marks the unused tail of the last chunk and publishes the warp's survivor count.
   // Warp-wide.
   __device__ __forceinline__ void finish(const StageArgs& a) {
@@ -838,13 +852,11 @@ __device__ __forceinline__ uint32_t probe_filter32(const HtView& h, const SegPla
   for (int k = 0; k < kItems; k++) {
     const uint32_t d = x[k] - sp.xlo;
     o[k] = d + sp.boff;
-    if (!(((live >> k) & 1) && d <= sp.xspan)) {
-      live &= ~(1u << k);
-      o[k] = 0;
-    }
+    if (d > sp.xspan) live &= ~(1u << k);
   }
+  // only live items load their word (predicated loads: no memory access for the others)
 #pragma unroll
-  for (int k = 0; k < kItems; k++) w[k] = __ldg(h.bits + (o[k] >> 5));
+  for (int k = 0; k < kItems; k++) w[k] = ((live >> k) & 1) ? __ldg(h.bits + (o[k] >> 5)) : 0u;
 #pragma unroll
   for (int k = 0; k < kItems; k++)
     if (!((w[k] >> (o[k] & 31)) & 1u)) live &= ~(1u << k);
@@ -1149,6 +1161,208 @@ __global__ void __launch_bounds__(kTmaThreads) k_stage_tma(const __grid_constant
   if (lane == 0 && survivors) atomicAdd(a.hit_rows, survivors);
 }
 
+// ---------------------------------------------------------------- blocked vector-load stage
+// The conjunctive scan when every scanned segment stores its tested columns in at most 32
+// bits. Each thread owns 8 consecutive rows of a 2048-row tile and reads every column it
+// tests with one or two 16-byte loads (one 8-byte load for an 8-bit column), so a warp's
+// loads cover whole sectors, there is no staging copy or handshake, and a row costs a few
+// instructions: the shipdate-and-key-bitmap scan of a 600M-row fact table reads at about
+// the copy bandwidth of HBM. Survivors are appended to the hit list as positions, or, for
+// an inline build, go straight to the build table (a hash insert, or a dense table's key
+// bit and record); their key and payload values are read per survivor.
+constexpr uint32_t kVecRows = kItems;  // consecutive rows per thread per tile
+static_assert(kT * kVecRows == kTile, "a tile is one block of rows per thread");
+
+// Stored values of rows row0 .. row0 + n - 1 (n <= 8) of a column of at most 32 bits; the
+// full block reads 8 rows with vector loads (row0 is a multiple of 8, so the addresses
+// are aligned when the column's base is), a segment's last partial block reads row by row.
+__device__ __forceinline__ void load8_narrow(const void* p, uint32_t bits, uint32_t row0, uint32_t n,
+                                             uint32_t (&x)[kVecRows]) {
+  if (n == kVecRows) {
+    if (bits == 8) {
+      const uint2 v = __ldcs((const uint2*)((const uint8_t*)p + row0));
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        x[k] = (v.x >> (8 * k)) & 0xffu;
+        x[4 + k] = (v.y >> (8 * k)) & 0xffu;
+      }
+    } else if (bits == 16) {
+      const uint4 v = __ldcs((const uint4*)((const uint16_t*)p + row0));
+      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        x[2 * k] = w[k] & 0xffffu;
+        x[2 * k + 1] = w[k] >> 16;
+      }
+    } else {
+      const uint4* q = (const uint4*)((const uint32_t*)p + row0);
+      const uint4 u = __ldcs(q), v = __ldcs(q + 1);
+      x[0] = u.x, x[1] = u.y, x[2] = u.z, x[3] = u.w;
+      x[4] = v.x, x[5] = v.y, x[6] = v.z, x[7] = v.w;
+    }
+    return;
+  }
+#pragma unroll
+  for (uint32_t k = 0; k < kVecRows; k++) {
+    x[k] = 0;
+    if (k < n) {
+      const uint32_t r = row0 + k;
+      x[k] = bits == 8 ? __ldg((const uint8_t*)p + r) : bits == 16 ? __ldg((const uint16_t*)p + r)
+                                                                   : __ldg((const uint32_t*)p + r);
+    }
+  }
+}
+
+// kMode: 0 survivors to the hit list, 1 inline dense build, 2 inline hash build.
+// kConj: the predicate's conjuncts. A block's tiles advance by gridDim.x, so each thread
+// follows its segment incrementally and keeps the segment's column descriptors, conjunct
+// tests and probe plan in registers (no per-tile table lookups).
+template <int kMode, int kConj>
+__global__ void __launch_bounds__(kT) k_stage_vec(const __grid_constant__ TmaArgs t) {
+  const FastArgs& f = t.f;
+  const StageArgs& a = f.a;
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  // the per-segment tables of k_stage_tma's layout, with no stage buffers in front
+  uint32_t* s_tile = (uint32_t*)(s_dyn + tma_tile_table_off(0, 0));
+  alk_colseg* s_cd = (alk_colseg*)(s_dyn + tma_desc_off(0, 0, a.nseg));  // [nstaged][nseg]
+  ConjSeg* s_cs = (ConjSeg*)(s_dyn + tma_cseg_off(0, 0, a.nseg, t.nstaged));  // [nconj][nseg]
+  SegPlan* s_sp = (SegPlan*)(s_dyn + tma_splan_off(0, 0, a.nseg, t.nstaged, f.nconj));  // [nseg]
+  for (uint32_t i = threadIdx.x; i <= a.nseg; i += kT) s_tile[i] = a.seg_tile[i];
+  for (uint32_t i = threadIdx.x; i < t.nstaged * a.nseg; i += kT)
+    s_cd[i] = a.cols[t.staged_slot[i / a.nseg] * a.nseg + i % a.nseg];
+  for (uint32_t i = threadIdx.x; i < f.nconj * a.nseg; i += kT) s_cs[i] = f.cseg[i];
+  for (uint32_t i = threadIdx.x; i < a.nseg; i += kT) s_sp[i] = f.splan[i];
+  __syncthreads();
+  unsigned long long rows_seen = 0, inserted = 0, survivors = 0;
+  HitWriter hw;
+  const bool probe = t.probe_st >= 0 && a.probe.bits;
+  // the current segment, in registers
+  uint32_t seg = 0, seg_end = 0, tile0 = 0, nrows = 0;
+  const void* cdata[kConj > 0 ? kConj : 1];
+  uint32_t cbits[kConj > 0 ? kConj : 1];
+  int64_t clower[kConj > 0 ? kConj : 1];
+  ConjSeg ccs[kConj > 0 ? kConj : 1];
+  const void* pdata = nullptr;
+  uint32_t pbits = 0;
+  SegPlan sp{};
+  bool first = true;
+  for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    if (first || tile >= seg_end) {
+      if (first) seg = tile_segment(s_tile, a.nseg, tile);
+      while (tile >= s_tile[seg + 1]) seg++;
+      first = false;
+      tile0 = s_tile[seg];
+      seg_end = s_tile[seg + 1];
+#pragma unroll
+      for (int c = 0; c < kConj; c++) {
+        const alk_colseg& d = s_cd[t.conj_st[c] * a.nseg + seg];
+        cdata[c] = d.data;
+        cbits[c] = d.bits;
+        clower[c] = d.lower;
+        ccs[c] = s_cs[c * a.nseg + seg];
+      }
+      nrows = s_cd[seg].rows;
+      if (probe) {
+        const alk_colseg& d = s_cd[t.probe_st * a.nseg + seg];
+        pdata = d.data;
+        pbits = d.bits;
+        sp = s_sp[seg];
+      }
+    }
+    const uint32_t row0 = (tile - tile0) * kTile + threadIdx.x * kVecRows;
+    const uint32_t n = row0 < nrows ? min(kVecRows, nrows - row0) : 0u;
+    uint32_t live = (1u << n) - 1u;
+    rows_seen += n;
+    uint32_t x[kVecRows];
+#pragma unroll
+    for (int c = 0; c < kConj; c++) {
+      if (live) {
+        load8_narrow(cdata[c], cbits[c], row0, n, x);
+        live = conj_filter32(f.conj[c], ccs[c], clower[c], x, live);
+      }
+    }
+    if (live && probe) {
+      load8_narrow(pdata, pbits, row0, n, x);
+      live = probe_filter32(a.probe, sp, x, live);
+    }
+    if (kMode == 0) {
+      hw.append_blocked(a, live, seg, row0);
+      continue;
+    }
+    // inline build: key and payload of each survivor read at its row
+    const alk_colseg& kd = s_cd[t.key_st * a.nseg + seg];
+    if (kMode == 1) {
+      uint32_t excl;
+      const uint32_t total = __any_sync(0xffffffffu, live) ? warp_offsets(__popc(live), &excl) : 0;
+      if (!total) continue;
+      const HitWriter::Room room = hw.reserve(a, total);
+      uint32_t i = excl;
+      for (uint32_t m = live; m; m &= m - 1, i++) {
+        const uint32_t r = row0 + (uint32_t)(__ffs(m) - 1);
+        const int64_t key = load_for(kd.data, kd.bits, kd.lower, r);
+        const uint64_t o = (uint64_t)key - (uint64_t)a.build.kmin;
+        if (o < a.build.nbits) atomicOr(a.build.bits + (o >> 5), 1u << (o & 31));
+        else atomicExch(a.build.flags + 3, 1);
+        const uint64_t e = room.at(i);
+        if (e >= a.hit_cap) continue;
+        Hit* rec = a.hits + e * a.hit_words;
+        rec[0] = (uint64_t)seg << 32 | (uint64_t)r;
+        rec[1] = (uint64_t)key;
+#pragma unroll
+        for (uint32_t p = 0; p < 8; p++)
+          if (p < a.build.npay) {
+            const alk_colseg& pd = s_cd[t.pay_st[p] * a.nseg + seg];
+            rec[2 + p] = (uint64_t)load_for(pd.data, pd.bits, pd.lower, r);
+          }
+      }
+      continue;
+    }
+    survivors += __popc(live);
+    for (uint32_t m = live; m; m &= m - 1) {
+      const uint32_t r = row0 + (uint32_t)(__ffs(m) - 1);
+      const int64_t key = load_for(kd.data, kd.bits, kd.lower, r);
+      int64_t pv[8];
+#pragma unroll
+      for (uint32_t p = 0; p < 8; p++)
+        if (p < a.build.npay) {
+          const alk_colseg& pd = s_cd[t.pay_st[p] * a.nseg + seg];
+          pv[p] = load_for(pd.data, pd.bits, pd.lower, r);
+        }
+      const int64_t sl = ht_insert(a.build, key);
+      if (sl < 0) continue;
+      inserted++;
+#pragma unroll
+      for (uint32_t p = 0; p < 8; p++)
+        if (p < a.build.npay) a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = pv[p];
+    }
+  }
+  hw.finish(a);
+  for (int o = 16; o; o >>= 1) {
+    rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
+    inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
+    survivors += __shfl_xor_sync(0xffffffffu, survivors, o);
+  }
+  const uint32_t lane = threadIdx.x & 31;
+  if (lane == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
+  if (lane == 0 && inserted) atomicAdd(a.build.nslots, inserted);
+  if (lane == 0 && survivors) atomicAdd(a.hit_rows, survivors);
+}
+
+// The blocked kernel for a mode and conjunct count (0 .. kMaxConj).
+template <int kMode>
+using VecKernel = void (*)(const TmaArgs);
+template <int kMode>
+VecKernel<kMode> vec_kernel_for(uint32_t nconj) {
+  switch (nconj) {
+    case 0: return k_stage_vec<kMode, 0>;
+    case 1: return k_stage_vec<kMode, 1>;
+    case 2: return k_stage_vec<kMode, 2>;
+    case 3: return k_stage_vec<kMode, 3>;
+    default: return k_stage_vec<kMode, 4>;
+  }
+}
+static_assert(kMaxConj == 4, "one blocked kernel per conjunct count");
+
 // Host: recognise an AND of (column * mul OP constant) tests in a compiled predicate.
 bool as_conjuncts(const alk_program& p, Conj* out, uint32_t* n) {
   *n = 0;
@@ -1234,19 +1448,20 @@ constexpr size_t kSmemPerSM = 228 * 1024;
 // kernel over its survivors. cols is the host descriptor array [ncols][nseg]; fa holds
 // the device arguments and, when conj, the predicate's conjuncts.
 template <bool kBuild>
-cudaError_t launch_stage(FastArgs fa, bool conj, const alk_colseg* cols, const uint8_t* seg_mode,
+cudaError_t launch_stage(FastArgs fa, bool conj, bool narrow_all, const alk_colseg* cols, const uint8_t* seg_mode,
                          const int32_t* h_pay_src, cudaStream_t s, alk_event_timer* timer) {
   StageArgs& a = fa.a;
   if (!a.ntiles) return cudaSuccess;
   TmaArgs t{};
-  bool tma = false;
-  uint32_t tma_smem = 0;
-  // Stage the columns every row needs (and, for an inline build, the key and payload),
-  // with as many tiles in flight as keep 3 blocks per SM (2 at least).
-  auto plan = [&](bool with_build) -> bool {
+  bool tma = false, vec = false;
+  uint32_t tma_smem = 0, vec_smem = 0;
+  // The columns every row needs (conjunct columns and the probe key) and, for an inline
+  // build, the key and payload: their descriptors go to shared memory.
+  std::vector<uint32_t> st;
+  auto plan_cols = [&](bool with_build) -> bool {
     t = TmaArgs{};
     t.f = fa;
-    std::vector<uint32_t> st;
+    st.clear();
     auto add = [&](uint32_t sl) -> uint32_t {
       auto it = std::find(st.begin(), st.end(), sl);
       if (it != st.end()) return (uint32_t)(it - st.begin());
@@ -1261,6 +1476,29 @@ cudaError_t launch_stage(FastArgs fa, bool conj, const alk_colseg* cols, const u
       for (uint32_t p = 0; p < a.build.npay; p++) t.pay_st[p] = add((uint32_t)h_pay_src[p]);
     }
     if (st.empty() || st.size() > (size_t)kStaged) return false;
+    for (size_t i = 0; i < st.size(); i++) t.staged_slot[i] = st[i];
+    t.nstaged = (uint32_t)st.size();
+    return true;
+  };
+  // Blocked vector loads: every scanned segment narrow, and the columns read for every
+  // row aligned for 16-byte (8-bit columns: 8-byte) loads.
+  auto plan_vec = [&](bool with_build) -> bool {
+    if (!plan_cols(with_build)) return false;
+    std::vector<uint32_t> tested;
+    for (uint32_t c = 0; c < fa.nconj; c++) tested.push_back(t.conj_st[c]);
+    if (t.probe_st >= 0 && a.probe.bits) tested.push_back((uint32_t)t.probe_st);
+    for (uint32_t i : tested)
+      for (uint32_t g = 0; g < a.nseg; g++) {
+        if (!seg_mode[g]) continue;
+        const alk_colseg& d = cols[st[i] * a.nseg + g];
+        if (d.bits > 32 || ((uintptr_t)d.data & (d.bits == 8 ? 7u : 15u))) return false;
+      }
+    vec_smem = tma_smem_bytes(0, 0, a.nseg, t.nstaged, fa.nconj);
+    return vec_smem + kTmaStaticSmem <= kSmemPerBlock;
+  };
+  // Staged tiles, with as many tiles in flight as keep 3 blocks per SM (2 at least).
+  auto plan = [&](bool with_build) -> bool {
+    if (!plan_cols(with_build)) return false;
     // bulk copies need 16-byte aligned sources (row0 * width is a multiple of kTile)
     uint32_t bytes = 0;
     for (size_t i = 0; i < st.size(); i++) {
@@ -1272,10 +1510,8 @@ cudaError_t launch_stage(FastArgs fa, bool conj, const alk_colseg* cols, const u
         if ((uintptr_t)d.data & 15) return false;
       }
       t.col_off[i] = bytes;
-      t.staged_slot[i] = st[i];
       bytes += (kTile * w + 127) & ~127u;
     }
-    t.nstaged = (uint32_t)st.size();
     t.stage_bytes = bytes;
     for (t.nst = kMaxStages; t.nst >= 2; t.nst--) {
       const size_t need = kTmaStaticSmem + tma_smem_bytes(bytes, t.nst, a.nseg, t.nstaged, fa.nconj);
@@ -1291,15 +1527,23 @@ cudaError_t launch_stage(FastArgs fa, bool conj, const alk_colseg* cols, const u
     // an inline build needs every payload value from the scan and the probe (if any)
     // settled by the exact key bitmap
     const bool can_inline = kBuild && h_pay_src && !a.need_slot && (a.probe_slot < 0 || a.probe.bits);
-    tma = (can_inline && plan(true)) || plan(false);
+    if (narrow_all) vec = (can_inline && plan_vec(true)) || plan_vec(false);
+    if (!vec) tma = (can_inline && plan(true)) || plan(false);
   }
-  const bool inline_build = tma && t.inline_build;
+  const bool inline_build = (tma || vec) && t.inline_build;
   const bool dense = kBuild && a.build.rank != nullptr;
   // a dense build staged inline records [position, key, payload] per survivor
   a.hit_words = dense && inline_build ? 2 + a.build.npay : 1;
   t.f.a.hit_words = a.hit_words;
   int occ = 0;
-  if (tma) {
+  // the blocked kernel's mode: hit list, inline dense build, inline hash build
+  void (*vec_kernel)(const TmaArgs) = !inline_build ? vec_kernel_for<0>(fa.nconj)
+                                      : dense         ? vec_kernel_for<1>(fa.nconj)
+                                                      : vec_kernel_for<2>(fa.nconj);
+  if (vec) {
+    cudaFuncSetAttribute(vec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, vec_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, vec_kernel, kT, vec_smem);
+  } else if (tma) {
     cudaFuncSetAttribute(k_stage_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, tma_smem);
     cudaFuncSetAttribute(k_stage_tma, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage_tma, kTmaThreads, tma_smem);
@@ -1317,7 +1561,8 @@ cudaError_t launch_stage(FastArgs fa, bool conj, const alk_colseg* cols, const u
   if (timer && timer->on) cudaStreamIsCapturing(s, &cst);
   const unsigned evflags = cst == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
   if (timer && timer->on) cudaEventRecordWithFlags((cudaEvent_t)timer->ev0, s, evflags);
-  if (tma) k_stage_tma<<<grid, kTmaThreads, tma_smem, s>>>(t);
+  if (vec) vec_kernel<<<grid, kT, vec_smem, s>>>(t);
+  else if (tma) k_stage_tma<<<grid, kTmaThreads, tma_smem, s>>>(t);
   else if (conj) k_stage_fast<<<grid, kT, 0, s>>>(fa);
   else k_stage_scan<<<grid, kT, 0, s>>>(a);
   uint32_t launches = 1;
@@ -1637,7 +1882,11 @@ static int run_stage(StageArgs& a, const alk_program& pred, const alk_colseg* co
   fa.a = a;
   fa.cseg = (const ConjSeg*)(db + off_cs);
   fa.splan = (const SegPlan*)(db + off_sp);
-  CK(launch_stage<kBuild>(fa, conj, cols, seg_mode, kBuild ? (const int32_t*)(hb.data() + off_x) : nullptr, s, timer));
+  bool narrow_all = true;
+  for (uint32_t g = 0; g < a.nseg; g++)
+    if (seg_mode[g] && !sp[g].narrow) narrow_all = false;
+  CK(launch_stage<kBuild>(fa, conj, narrow_all, cols, seg_mode, kBuild ? (const int32_t*)(hb.data() + off_x) : nullptr,
+                          s, timer));
   static_assert(sizeof(alk_stage_status) == 32, "status mirrors the counters after the arguments");
   if (h_status) {  // asynchronous: the counters land in the caller's (pinned) status
     if (timer && timer->on && a.ntiles) timer->launches++;
