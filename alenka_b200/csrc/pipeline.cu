@@ -503,13 +503,23 @@ __global__ void __launch_bounds__(kT) k_rank_mark(const StageArgs a) {
 // survivors recorded by the scan (one record per survivor, every one a member), a key
 // count below the survivor count means duplicate keys.
 constexpr uint32_t kRankTile = kT * 8;
+// The thread's 8 consecutive bitmap words (two 16-byte loads; the bitmap and the rank
+// array of a dense table start on 16-byte boundaries) and their set-bit counts.
 __device__ __forceinline__ uint64_t rank_tile_counts(const HtView& h, uint32_t tile, uint32_t (&c)[8]) {
   const uint64_t nwords = (h.nbits + 31) / 32;
   const uint64_t w0 = (uint64_t)tile * kRankTile + (uint64_t)threadIdx.x * 8;  // blocked
+  uint32_t w[8];
+  if (w0 + 8 <= nwords) {
+    const uint4 p = ((const uint4*)(h.bits + w0))[0], q = ((const uint4*)(h.bits + w0))[1];
+    w[0] = p.x, w[1] = p.y, w[2] = p.z, w[3] = p.w, w[4] = q.x, w[5] = q.y, w[6] = q.z, w[7] = q.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; k++) w[k] = w0 + k < nwords ? h.bits[w0 + k] : 0u;
+  }
   uint64_t sum = 0;
 #pragma unroll
   for (int k = 0; k < 8; k++) {
-    c[k] = w0 + k < nwords ? (uint32_t)__popc(h.bits[w0 + k]) : 0u;
+    c[k] = (uint32_t)__popc(w[k]);
     sum += c[k];
   }
   return sum;
@@ -554,10 +564,19 @@ __global__ void __launch_bounds__(kT) k_rank_write(const StageArgs a) {
   uint64_t tot;
   uint64_t r = a.rk_incls[blockIdx.x] + block_excl_scan<kT>(sum, s_warp, &tot);
   const uint64_t w0 = (uint64_t)blockIdx.x * kRankTile + (uint64_t)threadIdx.x * 8;
+  uint32_t rk[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) {
-    if (w0 + k < nwords) h.rank[w0 + k] = (uint32_t)r;
+    rk[k] = (uint32_t)r;
     r += c[k];
+  }
+  if (w0 + 8 <= nwords) {
+    ((uint4*)(h.rank + w0))[0] = make_uint4(rk[0], rk[1], rk[2], rk[3]);
+    ((uint4*)(h.rank + w0))[1] = make_uint4(rk[4], rk[5], rk[6], rk[7]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+      if (w0 + k < nwords) h.rank[w0 + k] = rk[k];
   }
 }
 
@@ -1296,24 +1315,37 @@ __global__ void __launch_bounds__(kT) k_stage_vec(const __grid_constant__ TmaArg
       const uint32_t total = __any_sync(0xffffffffu, live) ? warp_offsets(__popc(live), &excl) : 0;
       if (!total) continue;
       const HitWriter::Room room = hw.reserve(a, total);
-      uint32_t i = excl;
-      for (uint32_t m = live; m; m &= m - 1, i++) {
-        const uint32_t r = row0 + (uint32_t)(__ffs(m) - 1);
-        const int64_t key = load_for(kd.data, kd.bits, kd.lower, r);
-        const uint64_t o = (uint64_t)key - (uint64_t)a.build.kmin;
-        if (o < a.build.nbits) atomicOr(a.build.bits + (o >> 5), 1u << (o & 31));
-        else atomicExch(a.build.flags + 3, 1);
-        const uint64_t e = room.at(i);
-        if (e >= a.hit_cap) continue;
-        Hit* rec = a.hits + e * a.hit_words;
-        rec[0] = (uint64_t)seg << 32 | (uint64_t)r;
-        rec[1] = (uint64_t)key;
+      // record fields one column at a time: the key (with its bit), then each payload
+      // column; a column of at most 32 bits whose base is aligned is read for the
+      // thread's 8 rows with vector loads, a wider one row by row
+      for (uint32_t f = 0; f < 1 + a.build.npay; f++) {
+        const alk_colseg& d = f == 0 ? kd : s_cd[t.pay_st[f - 1] * a.nseg + seg];
+        const bool vec_col = d.bits <= 32 && !((uintptr_t)d.data & (d.bits == 8 ? 7u : 15u));
+        uint32_t v[kVecRows];
+        if (live && vec_col) load8_narrow(d.data, d.bits, row0, n, v);
+        uint32_t i = excl;
+        for (uint32_t m = live; m; m &= m - 1, i++) {
+          const uint32_t k = (uint32_t)(__ffs(m) - 1);
+          const uint32_t r = row0 + k;
+          uint32_t vk = 0;
 #pragma unroll
-        for (uint32_t p = 0; p < 8; p++)
-          if (p < a.build.npay) {
-            const alk_colseg& pd = s_cd[t.pay_st[p] * a.nseg + seg];
-            rec[2 + p] = (uint64_t)load_for(pd.data, pd.bits, pd.lower, r);
+          for (uint32_t q = 0; q < kVecRows; q++)
+            if (q == k) vk = v[q];
+          const int64_t val = vec_col ? (int64_t)((uint64_t)vk + (uint64_t)d.lower) : load_for(d.data, d.bits, d.lower, r);
+          const uint64_t e = room.at(i);
+          if (f == 0) {
+            const uint64_t o = (uint64_t)val - (uint64_t)a.build.kmin;
+            if (o < a.build.nbits) atomicOr(a.build.bits + (o >> 5), 1u << (o & 31));
+            else atomicExch(a.build.flags + 3, 1);
+            if (e < a.hit_cap) {
+              Hit* rec = a.hits + e * a.hit_words;
+              rec[0] = (uint64_t)seg << 32 | (uint64_t)r;
+              rec[1] = (uint64_t)val;
+            }
+          } else if (e < a.hit_cap) {
+            a.hits[e * a.hit_words + 1 + f] = (uint64_t)val;
           }
+        }
       }
       continue;
     }
@@ -1681,7 +1713,7 @@ int alk_ht_create_dense(uint64_t max_keys, uint32_t npay, int64_t key_min, int64
   const size_t words = (span + 31) / 32;
   const size_t off_pay = cap * 8;
   const size_t off_ctr = off_pay + cap * 8 * npay;
-  const size_t off_bits = off_ctr + 64;
+  const size_t off_bits = (off_ctr + 64 + 15) & ~size_t(15);  // 16-byte aligned (vector loads)
   const size_t off_rank = off_bits + ((words * 4 + 15) & ~size_t(15));
   auto* h = new alk_ht();
   cudaError_t e = cudaMallocAsync(&h->mem, off_rank + words * 4, s);
@@ -1702,7 +1734,7 @@ int alk_ht_create_dense(uint64_t max_keys, uint32_t npay, int64_t key_min, int64
   h->v.kmin = key_min;
   h->v.nbits = span;
   h->v.rank = (uint32_t*)(p + off_rank);
-  CK(cudaMemsetAsync(p + off_ctr, 0, 64 + ((words * 4 + 15) & ~size_t(15)), s));  // counters and bitmap
+  CK(cudaMemsetAsync(p + off_ctr, 0, off_rank - off_ctr, s));  // counters and bitmap
   *out = h;
   return ALK_OK;
 }
