@@ -214,12 +214,25 @@ def _save_catalog(path, cat):
 
 
 def _write(d, name, cols, columns, rows, seg_rows, cat):
+    """columns: name -> array over all rows, or a function (begin, end) -> that slice
+    (so that large tables are produced one segment at a time)."""
     t = _Table(d, name, cols)
     seg_rows = seg_rows or rows
     for b in range(0, rows, seg_rows):
         e = min(rows, b + seg_rows)
-        t.segment({k: v[b:e] for k, v in columns.items()})
+        t.segment({k: (v(b, e) if callable(v) else v[b:e]) for k, v in columns.items()})
     t.finish(cat)
+
+
+def _order_counts(state, rows):
+    """Prefix ends of the per-order row counts (1-7, one draw per order) until they cover
+    rows: cum[k] = rows of orders 0..k."""
+    k = rows // 4 + 64
+    while True:
+        cum = np.cumsum(_uniform(state, 0, k, 1, 7))
+        if int(cum[-1]) >= rows:
+            return cum
+        k *= 2
 
 
 SEGMENTS = [b"AUTOMOBILE", b"BUILDING", b"FURNITURE", b"HOUSEHOLD", b"MACHINERY"]
@@ -244,23 +257,21 @@ def three_way(d, customers, orders, lineitems, seg_rows, seed):
     odays = _uniform(_mix(seed, 22), 0, orders, d0, d0 + 7 * 365 - 1)
     _write(d, "orders", [("o_orderkey", 0, 0, 0), ("o_custkey", 0, 0, 0), ("o_orderdate", 0, 0, 0),
                          ("o_shippriority", 0, 0, 0)],
-           {"o_orderkey": 4 * np.arange(1, orders + 1, dtype=np.int64),
-            "o_custkey": _uniform(_mix(seed, 21), 0, orders, 1, customers),
-            "o_orderdate": yyyymmdd(odays), "o_shippriority": np.zeros(orders, dtype=np.int64)},
+           {"o_orderkey": lambda b, e: 4 * np.arange(b + 1, e + 1, dtype=np.int64),
+            "o_custkey": lambda b, e: _uniform(_mix(seed, 21), b, e - b, 1, customers),
+            "o_orderdate": lambda b, e: yyyymmdd(odays[b:e]),
+            "o_shippriority": lambda b, e: np.zeros(e - b, dtype=np.int64)},
            orders, seg_rows, cat)
-    k = lineitems // 4 + 64
-    while True:
-        counts = _uniform(_mix(seed, 31), 0, k, 1, 7)
-        if int(counts.sum()) >= lineitems:
-            break
-        k *= 2
-    order_of_row = np.repeat(np.arange(k, dtype=np.int64) % orders, counts)[:lineitems]
+    cum = _order_counts(_mix(seed, 31), lineitems)
+
+    def order_of(b, e):  # the order a lineitem row belongs to; the order list wraps around
+        return np.searchsorted(cum, np.arange(b, e, dtype=np.int64), side="right") % orders
     _write(d, "lineitem", [("l_orderkey", 0, 0, 0), ("l_shipdate", 0, 0, 0), ("l_extendedprice", 1, 2, 0),
                            ("l_discount", 1, 2, 0)],
-           {"l_orderkey": 4 * (order_of_row + 1),
-            "l_shipdate": yyyymmdd(odays[order_of_row] + _uniform(_mix(seed, 32), 0, lineitems, 1, 121)),
-            "l_extendedprice": _uniform(_mix(seed, 33), 0, lineitems, 90000, 10500000),
-            "l_discount": _uniform(_mix(seed, 34), 0, lineitems, 0, 10)},
+           {"l_orderkey": lambda b, e: 4 * (order_of(b, e) + 1),
+            "l_shipdate": lambda b, e: yyyymmdd(odays[order_of(b, e)] + _uniform(_mix(seed, 32), b, e - b, 1, 121)),
+            "l_extendedprice": lambda b, e: _uniform(_mix(seed, 33), b, e - b, 90000, 10500000),
+            "l_discount": lambda b, e: _uniform(_mix(seed, 34), b, e - b, 0, 10)},
            lineitems, seg_rows, cat)
     _save_catalog(os.path.join(d, "data.dictionary"), cat)
 
@@ -270,13 +281,8 @@ def lineitem_flat(d, rows, seg_rows, seed):
     cents U[90000,10500000], discount U[0,10], shipdate uniform over 1992-01-02..1998-12-01,
     returnflag in {A,N,R}, linestatus in {F,O}."""
     cat = _load_catalog(os.path.join(d, "data.dictionary"))
-    k = rows // 4 + 64
-    while True:
-        counts = _uniform(_mix(seed, 1), 0, k, 1, 7)
-        if int(counts.sum()) >= rows:
-            break
-        k *= 2
-    keys = np.repeat(np.arange(1, k + 1, dtype=np.int64), counts)[:rows]
+    cum = _order_counts(_mix(seed, 1), rows)
+    keys = np.searchsorted(cum, np.arange(rows, dtype=np.int64), side="right") + 1
     d0 = int(days_from_civil(np.int64(1992), np.int64(1), np.int64(2)))
     d1 = int(days_from_civil(np.int64(1998), np.int64(12), np.int64(1)))
     flags = np.frombuffer(b"ANR", dtype=np.uint8)[_uniform(_mix(seed, 6), 0, rows, 0, 2)].reshape(rows, 1)

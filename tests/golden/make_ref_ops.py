@@ -7,8 +7,10 @@ input files, and what the reference stored (the file itself when small, else its
 SHA-256 and line count) or the fatal error it stopped with. tests/test_ref_golden.py
 checks the oracle (CPU) and the engine (GPU) against this manifest.
 
-    python tests/golden/make_ref_ops.py            # all cases
-    python tests/golden/make_ref_ops.py --small    # cases below 1M rows only
+    python tests/golden/make_ref_ops.py                   # all cases
+    python tests/golden/make_ref_ops.py --small           # cases below 1M rows only
+    python tests/golden/make_ref_ops.py --only <dataset>  # one dataset's cases
+The 600M-row dataset needs about 10 GB of disk and a few minutes of the reference.
 """
 import hashlib
 import json
@@ -65,17 +67,18 @@ def run_reference(d, script, out):
 
 def main():
     small = "--small" in sys.argv
+    only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else None
     if not os.path.exists(REF):
         sys.exit("oracle/_ref/alenka_ref is missing: run oracle/build_ref.sh first")
     os.makedirs(OUT, exist_ok=True)
     manifest = {"reference": "oracle/_ref/alenka_ref (reference sources, Thrust OpenMP backend)", "cases": []}
     old = {}
     mpath = os.path.join(OUT, "manifest.json")
-    if small and os.path.exists(mpath):
+    if (small or only) and os.path.exists(mpath):
         old = {c["name"]: c for c in json.load(open(mpath))["cases"]}
     for ds_name, ds in ref_cases.DATASETS.items():
         cases = [c for c in ref_cases.CASES if c["dataset"] == ds_name]
-        if small and ds["rows"] >= 1_000_000:
+        if (small and ds["rows"] >= 1_000_000) or (only and ds_name != only):
             manifest["cases"] += [old[c["name"]] for c in cases if c["name"] in old]
             continue
         d = tempfile.mkdtemp(prefix="golden_" + ds_name + "_")

@@ -7,7 +7,8 @@ which write the same bytes); their digest is part of the manifest. Scripts are l
 text with seed-drawn constants, in the shapes of the benchmark workloads: the
 single-table FILTER + GROUP BY (config 1, also at its stated 6M rows), the three-way
 FILTER -> JOIN -> JOIN -> GROUP BY -> ORDER of the reference's README (config 2, also at
-its stated 60M / 15M / 1.5M rows), and operator scripts around them."""
+its stated 60M / 15M / 1.5M rows, and at the benchmark's 600M / 150M / 15M), and operator
+scripts around them."""
 import random
 
 SEGMENTS = ["AUTOMOBILE", "BUILDING", "FURNITURE", "HOUSEHOLD", "MACHINERY"]
@@ -27,6 +28,10 @@ DATASETS = {
     "config1": {"kind": "flat", "rows": 6_000_000, "seg_rows": 2_000_000, "seed": 1},
     "config2": {"kind": "three_way", "customers": 1_500_000, "orders": 15_000_000, "rows": 60_000_000,
                 "seg_rows": 10_000_000, "seed": 1},
+    # the headline instance: the three-way pipeline at lineitem 600M / orders 150M /
+    # customer 15M (the benchmark's default tables)
+    "headline600": {"kind": "three_way", "customers": 15_000_000, "orders": 150_000_000, "rows": 600_000_000,
+                    "seg_rows": 10_000_000, "seed": 1},
 }
 
 
@@ -196,6 +201,8 @@ def _cases():
     c.append({"name": "config1_q1_s1", "dataset": "config1", "script": flat_script(1, "q1.txt"), "out": "q1.txt"})
     c.append({"name": "config2_q3_s1", "dataset": "config2", "script": three_way_script(1, "q3.txt"), "out": "q3.txt"})
     c.append({"name": "config2_q3_all_groups", "dataset": "config2", "script": three_way_script(1, "q3.txt", limit=0),
+              "out": "q3.txt"})
+    c.append({"name": "headline600_q3_s1", "dataset": "headline600", "script": three_way_script(1, "q3.txt"),
               "out": "q3.txt"})
     return c
 
