@@ -750,6 +750,8 @@ __global__ void __launch_bounds__(kT) k_topk_collect(const int64_t* rank, const 
 // m <= kMergeMax).
 constexpr int kMergeThreads = 256;
 constexpr int kMergeMax = 4096;
+// slots the sampled top-k selection collects at or above its threshold, at most
+constexpr uint64_t kTopKCollect = 1 << 16;
 __global__ void __launch_bounds__(kMergeThreads) k_topk_merge(const int64_t* best, uint32_t m, uint32_t k,
                                                               int64_t* thr) {
   __shared__ int64_t s_w[(kMergeThreads / 32) * kTopK];
@@ -785,6 +787,101 @@ __global__ void __launch_bounds__(kT) k_topk_collect_dev(const int64_t* rank, co
       const unsigned long long p = atomicAdd(count, 1ull);
       if (p < cap) out[p] = (uint32_t)(i0 + (uint64_t)u * kT);
     }
+  }
+}
+
+// Sampled threshold for the top-k selection: per block, the k largest ranking values
+// among the live slots i * kSampleStride (a thread holds a few samples, so its list
+// inserts are few). The k-th largest of a sample is at most the k-th largest of all
+// slots, so every slot at or above the true threshold is at or above the sample's.
+constexpr uint32_t kSampleStride = 64;
+__global__ void __launch_bounds__(kT) k_topk_sample(const int64_t* rank, const unsigned long long* live, uint64_t n,
+                                                    uint32_t k, int64_t* out) {
+  __shared__ int64_t s_w[(kT / 32) * kTopK];
+  __shared__ int64_t s_best[kTopK];
+  int64_t t[kTopK];
+#pragma unroll
+  for (int i = 0; i < kTopK; i++) t[i] = INT64_MIN;
+  const uint64_t ns = (n + kSampleStride - 1) / kSampleStride;
+  for (uint64_t j = blockIdx.x * (uint64_t)kT + threadIdx.x; j < ns; j += (uint64_t)gridDim.x * kT) {
+    const uint64_t i = j * kSampleStride;
+    if (__ldg(live + i)) top16_insert(t, __ldg(rank + i));
+  }
+  block_top16<kT>(t, s_w, s_best);
+  __syncthreads();
+  if (threadIdx.x < k) out[(uint64_t)blockIdx.x * k + threadIdx.x] = s_best[threadIdx.x];
+}
+
+// Exact selection among the slots collected at or above the sampled threshold: their k-th
+// largest value is the true threshold (they include every slot at or above it), and the
+// ones at or above it are the result. When more slots were collected than fit (ties at
+// the sampled threshold), *fallback is set and the exact full pass runs instead.
+__global__ void __launch_bounds__(kMergeThreads) k_topk_refine(const int64_t* rank, const uint32_t* cand,
+                                                               const unsigned long long* ncand, uint64_t cap,
+                                                               uint32_t k, uint32_t* out, uint64_t out_cap,
+                                                               unsigned long long* count, int* fallback) {
+  __shared__ int64_t s_w[(kMergeThreads / 32) * kTopK];
+  __shared__ int64_t s_best[kTopK];
+  const unsigned long long m = *ncand;
+  if (m > cap) {
+    if (threadIdx.x == 0) *fallback = 1;
+    return;
+  }
+  int64_t t[kTopK];
+#pragma unroll
+  for (int i = 0; i < kTopK; i++) t[i] = INT64_MIN;
+  for (uint64_t i = threadIdx.x; i < m; i += kMergeThreads) top16_insert(t, rank[cand[i]]);
+  block_top16<kMergeThreads>(t, s_w, s_best);
+  __syncthreads();
+  const int64_t thr = s_best[k - 1];
+  for (uint64_t i = threadIdx.x; i < m; i += kMergeThreads) {
+    const uint32_t c = cand[i];
+    if (rank[c] < thr) continue;
+    const unsigned long long p = atomicAdd(count, 1ull);
+    if (p < out_cap) out[p] = c;
+  }
+}
+
+// The exact full pass, run only when the sampled selection fell back (the flag is set on
+// the device, so the sequence needs no host round trip and can be captured in a graph).
+__global__ void __launch_bounds__(kT) k_topk_local16_if(const int* fallback, const int64_t* rank,
+                                                        const unsigned long long* live, uint64_t n, uint32_t k,
+                                                        int64_t* out) {
+  if (!*fallback) return;
+  __shared__ int64_t s_w[(kT / 32) * kTopK];
+  __shared__ int64_t s_best[kTopK];
+  int64_t t[kTopK];
+#pragma unroll
+  for (int i = 0; i < kTopK; i++) t[i] = INT64_MIN;
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT)
+    if (__ldg(live + i)) top16_insert(t, __ldg(rank + i));
+  block_top16<kT>(t, s_w, s_best);
+  __syncthreads();
+  if (threadIdx.x < k) out[(uint64_t)blockIdx.x * k + threadIdx.x] = s_best[threadIdx.x];
+}
+__global__ void __launch_bounds__(kMergeThreads) k_topk_merge_if(const int* fallback, const int64_t* best, uint32_t m,
+                                                                 uint32_t k, int64_t* thr) {
+  if (!*fallback) return;
+  __shared__ int64_t s_w[(kMergeThreads / 32) * kTopK];
+  __shared__ int64_t s_best[kTopK];
+  int64_t t[kTopK];
+#pragma unroll
+  for (int i = 0; i < kTopK; i++) t[i] = INT64_MIN;
+  for (uint32_t i = threadIdx.x; i < m; i += kMergeThreads) top16_insert(t, best[i]);
+  block_top16<kMergeThreads>(t, s_w, s_best);
+  __syncthreads();
+  if (threadIdx.x == 0) *thr = s_best[k - 1];
+}
+__global__ void __launch_bounds__(kT) k_topk_collect_if(const int* fallback, const int64_t* rank,
+                                                        const unsigned long long* live, uint64_t n,
+                                                        const int64_t* thr_p, uint32_t* out, uint64_t cap,
+                                                        unsigned long long* count) {
+  if (!*fallback) return;
+  const int64_t thr = *thr_p;
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
+    if (!__ldg(live + i) || __ldg(rank + i) < thr) continue;
+    const unsigned long long p = atomicAdd(count, 1ull);
+    if (p < cap) out[p] = (uint32_t)i;
   }
 }
 
@@ -1252,8 +1349,12 @@ __global__ void __launch_bounds__(kT) k_stage_vec(const __grid_constant__ TmaArg
   for (uint32_t i = threadIdx.x; i < f.nconj * a.nseg; i += kT) s_cs[i] = f.cseg[i];
   for (uint32_t i = threadIdx.x; i < a.nseg; i += kT) s_sp[i] = f.splan[i];
   __syncthreads();
+  // per warp: its survivors' rows within the tile (inline builds), so that the warp then
+  // handles them 32 at a time, one per lane, whatever lanes they came from
+  __shared__ uint16_t s_rows[kMode == 0 ? 1 : kT * kVecRows];
   unsigned long long rows_seen = 0, inserted = 0, survivors = 0;
   HitWriter hw;
+  const uint32_t lane = threadIdx.x & 31;
   const bool probe = t.probe_st >= 0 && a.probe.bits;
   // the current segment, in registers
   uint32_t seg = 0, seg_end = 0, tile0 = 0, nrows = 0;
@@ -1308,65 +1409,62 @@ __global__ void __launch_bounds__(kT) k_stage_vec(const __grid_constant__ TmaArg
       hw.append_blocked(a, live, seg, row0);
       continue;
     }
-    // inline build: key and payload of each survivor read at its row
+    // inline build: the warp's survivors are listed, then handled one per lane; key and
+    // payload are read at each survivor's row
+    uint32_t excl;
+    const uint32_t total = __any_sync(0xffffffffu, live) ? warp_offsets(__popc(live), &excl) : 0;
+    if (!total) continue;
+    uint16_t* wl = s_rows + (threadIdx.x & ~31u) * kVecRows;
+    {
+      uint32_t q = excl;
+      for (uint32_t m = live; m; m &= m - 1, q++) wl[q] = (uint16_t)(threadIdx.x * kVecRows + (__ffs(m) - 1));
+    }
+    __syncwarp();
+    const uint32_t tile_row0 = (tile - tile0) * kTile;
     const alk_colseg& kd = s_cd[t.key_st * a.nseg + seg];
     if (kMode == 1) {
-      uint32_t excl;
-      const uint32_t total = __any_sync(0xffffffffu, live) ? warp_offsets(__popc(live), &excl) : 0;
-      if (!total) continue;
+      // dense table: the key's bit, and the record [position, key, payload...]
       const HitWriter::Room room = hw.reserve(a, total);
-      // record fields one column at a time: the key (with its bit), then each payload
-      // column; a column of at most 32 bits whose base is aligned is read for the
-      // thread's 8 rows with vector loads, a wider one row by row
-      for (uint32_t f = 0; f < 1 + a.build.npay; f++) {
-        const alk_colseg& d = f == 0 ? kd : s_cd[t.pay_st[f - 1] * a.nseg + seg];
-        const bool vec_col = d.bits <= 32 && !((uintptr_t)d.data & (d.bits == 8 ? 7u : 15u));
-        uint32_t v[kVecRows];
-        if (live && vec_col) load8_narrow(d.data, d.bits, row0, n, v);
-        uint32_t i = excl;
-        for (uint32_t m = live; m; m &= m - 1, i++) {
-          const uint32_t k = (uint32_t)(__ffs(m) - 1);
-          const uint32_t r = row0 + k;
-          uint32_t vk = 0;
+      for (uint32_t j = lane; j < total; j += 32) {
+        const uint32_t r = tile_row0 + wl[j];
+        const int64_t key = load_for(kd.data, kd.bits, kd.lower, r);
+        const uint64_t o = (uint64_t)key - (uint64_t)a.build.kmin;
+        if (o < a.build.nbits) atomicOr(a.build.bits + (o >> 5), 1u << (o & 31));
+        else atomicExch(a.build.flags + 3, 1);
+        const uint64_t e = room.at(j);
+        if (e >= a.hit_cap) continue;
+        Hit* rec = a.hits + e * a.hit_words;
+        rec[0] = (uint64_t)seg << 32 | (uint64_t)r;
+        rec[1] = (uint64_t)key;
 #pragma unroll
-          for (uint32_t q = 0; q < kVecRows; q++)
-            if (q == k) vk = v[q];
-          const int64_t val = vec_col ? (int64_t)((uint64_t)vk + (uint64_t)d.lower) : load_for(d.data, d.bits, d.lower, r);
-          const uint64_t e = room.at(i);
-          if (f == 0) {
-            const uint64_t o = (uint64_t)val - (uint64_t)a.build.kmin;
-            if (o < a.build.nbits) atomicOr(a.build.bits + (o >> 5), 1u << (o & 31));
-            else atomicExch(a.build.flags + 3, 1);
-            if (e < a.hit_cap) {
-              Hit* rec = a.hits + e * a.hit_words;
-              rec[0] = (uint64_t)seg << 32 | (uint64_t)r;
-              rec[1] = (uint64_t)val;
-            }
-          } else if (e < a.hit_cap) {
-            a.hits[e * a.hit_words + 1 + f] = (uint64_t)val;
+        for (uint32_t p = 0; p < 8; p++)
+          if (p < a.build.npay) {
+            const alk_colseg& pd = s_cd[t.pay_st[p] * a.nseg + seg];
+            rec[2 + p] = (uint64_t)load_for(pd.data, pd.bits, pd.lower, r);
           }
-        }
       }
-      continue;
-    }
-    survivors += __popc(live);
-    for (uint32_t m = live; m; m &= m - 1) {
-      const uint32_t r = row0 + (uint32_t)(__ffs(m) - 1);
-      const int64_t key = load_for(kd.data, kd.bits, kd.lower, r);
-      int64_t pv[8];
+    } else {
+      // hash table: insert, then the payload at the key's position
+      if (lane == 0) survivors += total;
+      for (uint32_t j = lane; j < total; j += 32) {
+        const uint32_t r = tile_row0 + wl[j];
+        const int64_t key = load_for(kd.data, kd.bits, kd.lower, r);
+        int64_t pv[8];
 #pragma unroll
-      for (uint32_t p = 0; p < 8; p++)
-        if (p < a.build.npay) {
-          const alk_colseg& pd = s_cd[t.pay_st[p] * a.nseg + seg];
-          pv[p] = load_for(pd.data, pd.bits, pd.lower, r);
-        }
-      const int64_t sl = ht_insert(a.build, key);
-      if (sl < 0) continue;
-      inserted++;
+        for (uint32_t p = 0; p < 8; p++)
+          if (p < a.build.npay) {
+            const alk_colseg& pd = s_cd[t.pay_st[p] * a.nseg + seg];
+            pv[p] = load_for(pd.data, pd.bits, pd.lower, r);
+          }
+        const int64_t sl = ht_insert(a.build, key);
+        if (sl < 0) continue;
+        inserted++;
 #pragma unroll
-      for (uint32_t p = 0; p < 8; p++)
-        if (p < a.build.npay) a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = pv[p];
+        for (uint32_t p = 0; p < 8; p++)
+          if (p < a.build.npay) a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = pv[p];
+      }
     }
+    __syncwarp();  // the list is rewritten by the warp's next tile
   }
   hw.finish(a);
   for (int o = 16; o; o >>= 1) {
@@ -1374,7 +1472,6 @@ __global__ void __launch_bounds__(kT) k_stage_vec(const __grid_constant__ TmaArg
     inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
     survivors += __shfl_xor_sync(0xffffffffu, survivors, o);
   }
-  const uint32_t lane = threadIdx.x & 31;
   if (lane == 0 && a.rows_in) atomicAdd(a.rows_in, rows_seen);
   if (lane == 0 && inserted) atomicAdd(a.build.nslots, inserted);
   if (lane == 0 && survivors) atomicAdd(a.hit_rows, survivors);
@@ -2103,18 +2200,33 @@ int alk_topk_select(const int64_t* d_rank, const uint64_t* d_live, uint64_t n, u
   if (!d_count || !d_out || k == 0 || k > (uint32_t)kTopK) return ALK_ERR_ARG;
   CK(cudaMemsetAsync(d_count, 0, 8, s));
   if (n == 0) return ALK_OK;
-  // a few blocks per SM, each over a strided share of the slots: the merge of their lists
-  // stays short
+  const unsigned long long* live = (const unsigned long long*)d_live;
+  // 1. the sampled threshold: per-block lists over every kSampleStride-th slot, merged
+  const uint64_t ns = (n + kSampleStride - 1) / kSampleStride;
+  const int sblocks = (int)std::min<uint64_t>(std::min<uint64_t>((ns + kT - 1) / kT, (uint64_t)kMergeMax / k),
+                                              (uint64_t)sms() * 4);
+  // 2. the exact full pass's per-block lists, should the sampled selection fall back
   const int blocks = (int)std::min<uint64_t>(std::min<uint64_t>((n + kT - 1) / kT, (uint64_t)kMergeMax / k),
                                              (uint64_t)sms() * 4);
+  const uint64_t ccap = kTopKCollect;  // slots collected at or above the sampled threshold
+  const size_t off_sthr = (size_t)sblocks * k, off_lists = off_sthr + 1, off_thr = off_lists + (size_t)blocks * k;
+  const size_t off_ctr = off_thr + 1, off_cand = off_ctr + 2;  // [ncand, fallback flag]
   int64_t* db = nullptr;
-  CK(cudaMallocAsync((void**)&db, ((size_t)blocks * k + 1) * 8, s));
-  k_topk_local16<<<blocks, kT, 0, s>>>(d_rank, (const unsigned long long*)d_live, n, k, db);
-  k_topk_merge<<<1, kMergeThreads, 0, s>>>(db, (uint32_t)blocks * k, k, db + (size_t)blocks * k);
-  k_topk_collect_dev<<<grid_for(n), kT, 0, s>>>(d_rank, (const unsigned long long*)d_live, n,
-                                                db + (size_t)blocks * k, d_out, cap,
-                                                (unsigned long long*)d_count);
-  alk::g_kernel_launches += 3;
+  CK(cudaMallocAsync((void**)&db, (off_cand * 8 + ccap * 4 + 15) & ~size_t(15), s));
+  unsigned long long* ncand = (unsigned long long*)(db + off_ctr);
+  int* fallback = (int*)(db + off_ctr + 1);
+  uint32_t* cand = (uint32_t*)(db + off_cand);
+  CK(cudaMemsetAsync(db + off_ctr, 0, 16, s));
+  k_topk_sample<<<sblocks, kT, 0, s>>>(d_rank, live, n, k, db);
+  k_topk_merge<<<1, kMergeThreads, 0, s>>>(db, (uint32_t)sblocks * k, k, db + off_sthr);
+  k_topk_collect_dev<<<grid_for(n), kT, 0, s>>>(d_rank, live, n, db + off_sthr, cand, ccap, ncand);
+  k_topk_refine<<<1, kMergeThreads, 0, s>>>(d_rank, cand, ncand, ccap, k, d_out, cap,
+                                           (unsigned long long*)d_count, fallback);
+  k_topk_local16_if<<<blocks, kT, 0, s>>>(fallback, d_rank, live, n, k, db + off_lists);
+  k_topk_merge_if<<<1, kMergeThreads, 0, s>>>(fallback, db + off_lists, (uint32_t)blocks * k, k, db + off_thr);
+  k_topk_collect_if<<<grid_for(n), kT, 0, s>>>(fallback, d_rank, live, n, db + off_thr, d_out, cap,
+                                               (unsigned long long*)d_count);
+  alk::g_kernel_launches += 7;
   CK(cudaGetLastError());
   CK(cudaFreeAsync(db, s));
   return ALK_OK;

@@ -744,6 +744,7 @@ def run_three_way(args, torch, dist, world, rank, local):
     clocks = clk.stop()
     sess.set_timing(False)
     fused_out = open(os.path.join(d, out_name), "rb").read()
+    dev_ms = acc["query_dev_ms"] / args.steps
     value = fact_rows * world / (ms / 1000.0)
     plan = {0: "operator-at-a-time", 1: "fused", 2: "fused, replayed from its CUDA graph"}.get(acc["plan"], "?")
 
@@ -754,14 +755,18 @@ def run_three_way(args, torch, dist, world, rank, local):
                               "device_ms_per_step": acc["query_dev_ms"] / args.steps}), flush=True)
         sess.close()
         return
+    sess.close()  # each path below runs alone on the device, with its own resident copy
     # plain operator-at-a-time GPU path, resident (the baseline the fused plan is compared to)
     plain = ab.Session(d, resident=True, plain=True)
     for t in ("lineitem", "orders", "customer"):
         plain.preload(t)
-    for _ in range(2):
+    for _ in range(3):
         plain.execute(script)
-    psteps = max(3, args.steps // 4)
-    pms, _ = timed_steps(plain, script, psteps, torch, dist)
+    # each plain step timed alone (CUDA events on the session's stream); the median step
+    # is the path's figure
+    psteps = max(5, args.steps // 2)
+    plain_steps = [timed_steps(plain, script, 1, torch, dist)[0] for _ in range(psteps)]
+    pms = statistics.median(plain_steps)
     plain.close()
     plain_out = open(os.path.join(d, out_name), "rb").read()
 
@@ -796,7 +801,6 @@ def run_three_way(args, torch, dist, world, rank, local):
                                     "(l_extendedprice + l_discount stored widths)",
                "algorithmic_bytes_per_launch": int(per_launch_bytes), "avg_launch_ms": per_launch_ms,
                "peak_source": f"{peak_kind} hbm_gbs (copy bandwidth measured on this pool)"}
-    dev_ms = acc["query_dev_ms"] / args.steps
     qb = query_bytes(d, fact_rows, {})
     query_roofline = {"bytes_per_query": qb, "device_ms": dev_ms, "achieved": qb / (dev_ms / 1000.0) / 1e9,
                       "peak": peak, "unit": "GB/s", "frac": qb / (dev_ms / 1000.0) / 1e9 / peak,
@@ -810,7 +814,6 @@ def run_three_way(args, torch, dist, world, rank, local):
         except Exception as e:  # test infrastructure: report, do not fail
             cpu = {"value": None, "unit": "rows/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {e}"}
-    sess.close()
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
@@ -819,6 +822,7 @@ def run_three_way(args, torch, dist, world, rank, local):
             "config": workload_config(args.scale, world),
             "plan": plan, "device_ms_per_step": dev_ms,
             "plain_gpu_rows_per_s": fact_rows * world / (pms / 1000.0), "fused_vs_plain": pms / ms,
+            "plain_ms_steps": [round(x, 3) for x in plain_steps],
             "verified": verified,
             "e2e": {"value": fact_rows * world / (ems / 1000.0), "unit": "rows/s",
                     "h2d_bytes_per_step": eacc["h2d"] // esteps, "d2h_bytes_per_step": eacc["d2h"] // esteps},
