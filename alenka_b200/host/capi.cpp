@@ -166,27 +166,41 @@ void alk_session_close(alk_session* s) { delete s; }
 // The reference's flags (bison.y:306-331): -l MB (segment size for stores), -v,
 // -delta, -ssd, -precision N, -i. Only -v changes this engine's behaviour; the data
 // directory is the current directory as in the reference.
-void alenkaInit(char** av) {
+void alenkaInit(char** av) { alk::embed_init(av); }
+int alenkaExecute(char* s) { return alk::embed_execute(s); }
+void alenkaClose(void) { alk::embed_close(); }
+int execute_file(int ac, char** av) { return alk::embed_file(ac, av); }
+}  // extern "C"
+
+namespace alk {
+void embed_init(char** av) {
   if (av)
     for (int i = 0; av[i]; i++)
       if (std::strcmp(av[i], "-v") == 0) g_verbose = true;
   if (!g_session) open_session(".", ALK_SESSION_RESIDENT, &g_session);
 }
 
-int alenkaExecute(char* s) {
-  if (!g_session) alenkaInit(nullptr);
+int embed_execute(char* s) {
+  if (!g_session) embed_init(nullptr);
   if (!g_session || !s) return 1;
   int rc = g_session->eng->execute(s);
   if (rc != ALK_OK) std::fprintf(stderr, "alenka_b200: %s\n", g_session->eng->error().c_str());
   return rc == ALK_OK ? 0 : 1;
 }
 
-void alenkaClose(void) {
+void embed_close() {
   delete g_session;
   g_session = nullptr;
 }
 
-int execute_file(int ac, char** av) {
+// The engine behind the embedding API (alenkaInit's session over the current directory,
+// opened on first use). The reference front end's emit_* boundary runs its scripts here.
+Engine* embedding_engine() {
+  if (!g_session) embed_init(nullptr);
+  return g_session ? g_session->eng.get() : nullptr;
+}
+
+int embed_file(int ac, char** av) {
   if (ac < 2) return 1;
   std::ifstream f(av[ac - 1]);
   if (!f) {
@@ -205,8 +219,7 @@ int execute_file(int ac, char** av) {
   delete s;
   return rc == ALK_OK ? 0 : 1;
 }
-
-}  // extern "C"
+}  // namespace alk
 
 // Text rendering of the parsed statements and their queues (front-end tests).
 extern "C" int alk_parse_dump(const char* script, char* out, int out_len) {

@@ -162,11 +162,19 @@ struct CardStage {
   const ScanPlan* up = nullptr;  // the scan that built the probed table
 };
 
+// The embedding API's implementation (alenka.h:30-35), behind both its C entry points
+// (include/alenka_b200.h) and the C++-linkage ones the reference's own callers bind.
+void embed_init(char** av);
+int embed_execute(char* s);
+void embed_close();
+int embed_file(int ac, char** av);
+
 class Engine {
  public:
   Engine(std::string dir, uint32_t flags);
   ~Engine();
   int execute(const std::string& script);
+  int execute_statements(std::vector<Statement> sts, const std::string& key);
   int execute_batch(const std::vector<std::string>& scripts);
   // A lineitem-shaped table generated in device memory (segments of the given sizes).
   int gen_resident_flat(const std::string& table, const std::vector<uint32_t>& seg_rows, uint64_t seed,

@@ -1622,6 +1622,7 @@ void Engine::emit_store_binary(Statement& st) {
 
 // ------------------------------------------------------------------ script
 void Engine::exec(Statement& st) {
+  if (st.op_case) unsupported("CASE expressions");
   switch (st.kind) {
     case StmtKind::Filter: emit_filter(st); break;
     case StmtKind::Select: emit_select(st); break;
@@ -1837,8 +1838,16 @@ int Engine::execute(const std::string& script) {
     if (parsed_.size() >= 256) parsed_.clear();
     parsed_.emplace(script, sts);
   }
+  return execute_statements(std::move(sts), script);
+}
+
+// Runs parsed statements, as the reference's second pass does (bison.y:346-360): from the
+// engine's own parser, or from the reference's grammar actions through the emit_*
+// boundary. key names the script for the per-script caches (fused graphs, records).
+int Engine::execute_statements(std::vector<Statement> sts, const std::string& key) {
+  err_.clear();
   reset_script_state();
-  cur_script_ = script;
+  cur_script_ = key;
   uint64_t k0 = g_kernel_launches;
   int rc = ALK_OK;
   try {

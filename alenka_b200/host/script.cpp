@@ -31,7 +31,7 @@ const char* kKeywords[] = {
     "LEFT", "RIGHT", "OUTER", "SEMI", "ANTI", "SORT", "SEGMENTS", "PRESORTED", "INSERT", "WHERE",
     "DISPLAY", "CASE", "WHEN", "THEN", "ELSE", "END", "SHOW", "TABLES", "TABLE", "DESCRIBE",
     "DROP", "DELETE", "FROM", "LIKE", "CREATE", "INDEX", "YEAR", "MONTH", "DAY", "CAST_TO_INT",
-    "APPEND", "NO", "ENCODING", "INTERVAL", "PARTITION"};
+    "APPEND", "NO", "ENCODING", "PARTITION"};  // no INTERVAL: fl.l has no such token
 
 struct SyntaxError : std::runtime_error {
   int line;
@@ -393,9 +393,11 @@ class Parser {
           val(n + "." + n2);
         } else if (is_punct('(') && peek(1).t == T::String && peek(2).t == T::Punct && peek(2).sub == ')') {
           take();
-          std::string s = take().text;
           take();
-          emit_string(s);  // emit_string_grp: grp_val is not used on this path
+          take();
+          // emit_string_grp(NAME, STRING) (bison.y:219, operators.cu:92-96) pushes the
+          // NAME as a string value; the literal goes to grp_val, unused on this path
+          emit_string(n);
         } else if (is_punct('{')) {
           var_decl(n);
         } else if (is_kw("ASC")) {
@@ -446,7 +448,7 @@ class Parser {
           expect_kw("ELSE");
           expr();
           expect_kw("END");
-          ty("CASE");
+          cur_->op_case = true;  // emit_case sets a flag and queues nothing
           return;
         }
         break;
@@ -581,7 +583,10 @@ class Parser {
         st.f = expect(T::Name, "source name");
         if (is_kw("JOIN") || is_kw("LEFT") || is_kw("RIGHT") || is_kw("OUTER")) {
           join_list();
-          st.grp_cnt = opt_group();
+          // the grammar passes join_list's value (always 1) as emit_join's third argument,
+          // not the GROUP BY count (bison.y:144-145, 268-275); the group names stay queued
+          opt_group();
+          st.grp_cnt = 1;
           st.kind = StmtKind::Join;
         } else {
           st.grp_cnt = opt_group();
@@ -656,9 +661,48 @@ class Parser {
       st.kind = StmtKind::Display;
       return;
     }
-    // DESCRIBE / SHOW / DROP / INSERT / DELETE / CREATE: recorded, not executed here.
-    while (!is_punct(';') && peek().t != T::End) take();
+    // DESCRIBE / SHOW / DROP / INSERT / DELETE / CREATE: recorded with the names and
+    // queues their emitters receive (bison.y:150-169), not executed here.
     st.kind = StmtKind::Other;
+    if (is_kw("DESCRIBE")) {  // emit_describe_table($2)
+      take();
+      st.s = expect(T::Name, "table name");
+      return;
+    }
+    if (is_kw("DROP") && is_kw("TABLE", 1)) {  // emit_drop_table($3)
+      take();
+      take();
+      st.s = expect(T::Name, "table name");
+      return;
+    }
+    if (is_kw("INSERT")) {  // INSERT INTO t SELECT expr_list FROM s: emit_insert($3, $7)
+      take();
+      expect_kw("INTO");
+      st.f = expect(T::Name, "table name");
+      expect_kw("SELECT");
+      expr_list();
+      expect_kw("FROM");
+      st.s = expect(T::Name, "source name");
+      return;
+    }
+    if (is_kw("DELETE")) {  // DELETE FROM t WHERE expr: emit_delete($3)
+      take();
+      expect_kw("FROM");
+      st.f = expect(T::Name, "table name");
+      expect_kw("WHERE");
+      expr();
+      return;
+    }
+    if (is_kw("CREATE")) {
+      // CREATE INDEX name ON table ...: the emitters take (name, table, ...). The grammar's
+      // CREATE INTERVAL form (bison.y:168) never parses: the lexer (fl.l) has no INTERVAL
+      take();
+      expect_kw("INDEX");
+      st.s = expect(T::Name, "index name");
+      expect_kw("ON");
+      st.f = expect(T::Name, "table name");
+    }
+    while (!is_punct(';') && peek().t != T::End) take();
   }
 };
 

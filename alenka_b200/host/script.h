@@ -33,6 +33,7 @@ struct Statement {
   int grp_cnt = 0;    // number of GROUP BY columns
   bool append = false;
   bool store_sort = false;  // STORE ... BINARY with SORT SEGMENTS BY / PRESORTED BY
+  bool op_case = false;     // a CASE expression was emitted (emit_case, operators.cu:2142)
   std::vector<std::string> op_type, op_value;
   std::vector<int64_t> op_nums;
   std::vector<double> op_nums_f;

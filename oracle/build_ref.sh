@@ -5,6 +5,9 @@
 #                           driven by oracle/ref_driver.cpp to write golden vectors
 #   oracle/_ref/alenka_ref  the whole reference CLI (bison front end, operators, codec)
 #                           under Thrust's OpenMP device system (oracle/ref.mk)
+#   oracle/_ref/alenka_frontend, frontend_dump
+#                           the reference's front end (parser, CLI) linked against
+#                           alenka_b200/libalenka_b200.so instead of its operators
 # The host shims in oracle/ref_shim stand in for the CUDA runtime calls (host memory),
 # Thrust 2.x's removed pinned_allocator and the moderngpu primitives the reference does
 # not vendor. Outputs go to oracle/_ref only.
@@ -24,6 +27,8 @@ g++ $FLAGS -I"$HERE/ref_shim" -I/usr/local/cuda/include -include "$HERE/ref_shim
 g++ -O1 -include cstddef -x c++ -c "$REF/MurmurHash2_64.cu" -o "$OUT/murmur.o"
 g++ -o "$OUT/ref_driver" "$OUT/ref_driver.o" "$OUT/murmur.o"
 echo "built $OUT/ref_driver"
-# the whole reference (bison front end, operators, codec) for the CPU: oracle/_ref/alenka_ref
-make -s -j"$(nproc)" -f "$HERE/ref.mk" REF="$REF"
-echo "built $OUT/alenka_ref"
+# the whole reference (bison front end, operators, codec) for the CPU: oracle/_ref/alenka_ref;
+# and its front end linked against alenka_b200/libalenka_b200.so (built first):
+# oracle/_ref/alenka_frontend and oracle/_ref/frontend_dump
+make -s -j"$(nproc)" -f "$HERE/ref.mk" REF="$REF" "$OUT/alenka_ref" frontend
+echo "built $OUT/alenka_ref, $OUT/alenka_frontend, $OUT/frontend_dump"

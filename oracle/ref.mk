@@ -27,3 +27,19 @@ $(OUT)/obj/%.o: $(REF)/%.cu $(wildcard $(SHIM)/*.h $(SHIM)/moderngpu/src/moderng
 $(OUT)/obj/callbacks.o: $(REF)/callbacks.c
 	@mkdir -p $(OUT)/obj
 	gcc -O2 -w -c $< -o $@
+
+# The reference's own front end (the generated parser bison.cu + lex.yy.c, main.cu and
+# callbacks.c, compiled above, unchanged) linked against this repository's library in
+# place of the reference's operators: the reference CLI running scripts on the engine.
+LIB := $(abspath $(HERE)../alenka_b200/libalenka_b200.so)
+FRONT_LDFLAGS = -Wl,-rpath,'$$ORIGIN/../../alenka_b200' -fopenmp -L$(GCC_LIB) -lgomp -lpthread
+FRONT_OBJS = $(OUT)/obj/bison.o $(OUT)/obj/atof.o $(OUT)/obj/callbacks.o
+$(OUT)/alenka_frontend: $(FRONT_OBJS) $(OUT)/obj/main.o $(LIB)
+	g++ -o $@ $(FRONT_OBJS) $(OUT)/obj/main.o $(LIB) $(FRONT_LDFLAGS)
+
+# The same parser's first pass only, printing what the library's emit_* boundary captured
+$(OUT)/frontend_dump: $(HERE)frontend_dump.cpp $(FRONT_OBJS) $(LIB)
+	g++ -std=c++14 -O1 -o $@ $< $(FRONT_OBJS) $(LIB) $(FRONT_LDFLAGS)
+
+frontend: $(OUT)/alenka_frontend $(OUT)/frontend_dump
+.PHONY: frontend

@@ -89,6 +89,8 @@ def main():
                 got, err = run_reference(d, c["script"], c["out"])
                 entry = {"name": c["name"], "dataset": ds_name, "script": c["script"], "out": c["out"],
                          "mode": c.get("mode", "bytes"), "data_sha256": digest}
+                if "segments_skipped" in c:
+                    entry["segments_skipped"] = c["segments_skipped"]
                 if err is not None:
                     entry["error"] = err
                 elif len(got) <= INLINE_LIMIT:

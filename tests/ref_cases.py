@@ -133,6 +133,25 @@ SCRIPTS = {
         "STORE R INTO 'x.txt' USING ('|');\n"),
 }
 
+# Zone maps over the segments of flat_multi (l_orderkey in order: [1, 24789],
+# [24789, 49806], [49807, 74916]): each filter gives the three segments different
+# verdicts (zone_map.cu:720-1135); name -> (script, segments the verdicts skip)
+ZONE_SCRIPTS = {
+    "zone_n_r_a": (
+        "LF := FILTER lineitem BY l_orderkey > 30000 AND l_orderkey < 80000;\n"
+        "R := SELECT l_returnflag AS f, l_linestatus AS s, SUM(l_quantity) AS q, COUNT(l_orderkey) AS c "
+        "FROM LF GROUP BY l_returnflag, l_linestatus;\n"
+        "STORE R INTO 'z.txt' USING ('|');\n", 1),
+    "zone_r_r_n": (
+        "LF := FILTER lineitem BY l_orderkey >= 24789 AND l_orderkey <= 24789;\n"
+        "R := SELECT l_orderkey AS k, SUM(l_extendedprice) AS p, COUNT(l_orderkey) AS c FROM LF GROUP BY l_orderkey;\n"
+        "STORE R INTO 'z.txt' USING ('|');\n", 1),
+    "zone_r_n_n_or": (
+        "LF := FILTER lineitem BY l_orderkey < 24789 OR l_orderkey > 90000;\n"
+        "R := SELECT l_linestatus AS s, SUM(l_quantity) AS q, COUNT(l_orderkey) AS c FROM LF GROUP BY l_linestatus;\n"
+        "STORE R INTO 'z.txt' USING ('|');\n", 2),
+}
+
 FUSED_PREDICATES = {
     "ge_le": ("l_shipdate >= 19950315", "o_orderdate <= 19950315", 'c_mktsegment == "BUILDING"'),
     "eq_ne": ("l_shipdate == 19950320", "o_orderdate != 19950301", 'c_mktsegment != "MACHINERY"'),
@@ -195,6 +214,15 @@ def _cases():
     for seed in range(1, 7):
         c.append({"name": f"three_way_random_s{seed}", "dataset": "three_way", "script": random_three_way(seed, "qr.txt"),
                   "out": "qr.txt"})
+    for n, (sc, skipped) in sorted(ZONE_SCRIPTS.items()):
+        c.append({"name": f"flat_multi_{n}", "dataset": "flat_multi", "script": sc, "out": "z.txt",
+                  "segments_skipped": skipped})
+    # the fused three-way plan with a fact filter whose zone maps skip two of the three
+    # lineitem segments ([4, 200392], [200392, 400024], [400024, 599664])
+    c.append({"name": "three_way_zone_fact_skip", "dataset": "three_way",
+              "script": three_way_with("l_orderkey < 200000 AND l_shipdate > 19950101", "o_orderdate < 19960101",
+                                       'c_mktsegment == "BUILDING"', "fx.txt", limit=0),
+              "out": "fx.txt", "segments_skipped": 2})
     for n, (sc, out, mode) in sorted(JOIN_SCRIPTS.items()):
         c.append({"name": f"three_way_{n}", "dataset": "three_way", "script": sc, "out": out, "mode": mode})
     # the stated sizes: config 1 (6M rows) and config 2 (60M / 15M / 1.5M)

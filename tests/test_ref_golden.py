@@ -157,7 +157,10 @@ def _engine(case, d, plain):
             assert case["error"] in str(e.value)
             return
         s.execute(script)
+        st = s.stats()
     _check(case, open(os.path.join(d, out), "rb").read())
+    if "segments_skipped" in case:  # segments whose zone-map verdict is N are never read
+        assert st.segments_skipped == case["segments_skipped"], (case["name"], st.segments_skipped)
 
 
 @pytest.mark.gpu
