@@ -249,6 +249,51 @@ __global__ void __launch_bounds__(kT) k_gather(const int64_t* src, const uint32_
     out[i] = __ldg(src + __ldg(idx + i));
 }
 
+__global__ void __launch_bounds__(kT) k_gather_u32(const uint32_t* src, const uint32_t* idx, uint64_t n,
+                                                   uint32_t* out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT)
+    out[i] = __ldg(src + __ldg(idx + i));
+}
+
+// Join forms of emit_multijoin (operators.cu:1288-1399) on the pairs a hash join found.
+// flags[i] = (lcol[pl[i]] == rcol[pr[i]]) (!= when neq): the AND-ed key pairs.
+__global__ void __launch_bounds__(kT) k_pair_match(const uint32_t* pl, const uint32_t* pr, uint64_t n,
+                                                   const int64_t* lcol, const int64_t* rcol, int neq,
+                                                   unsigned long long* flags) {
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
+    const bool eq = lcol[pl[i]] == rcol[pr[i]];
+    flags[i] = (eq != (neq != 0)) ? 1ull : 0ull;
+  }
+}
+// flags[rows[i]] = v: the rows a semi or anti join keeps or drops.
+__global__ void __launch_bounds__(kT) k_rows_mark(const uint32_t* rows, uint64_t n, unsigned long long* flags,
+                                                  unsigned long long v) {
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT)
+    flags[rows[i]] = v;
+}
+// Per segment g (rows [start[g], start[g + 1])), the least and greatest key: out[2g],
+// out[2g + 1] (preset to INT64_MAX / INT64_MIN).
+__global__ void __launch_bounds__(kT) k_seg_minmax(const int64_t* keys, const uint64_t* start, uint32_t nseg,
+                                                   long long* out) {
+  for (uint32_t g = 0; g < nseg; g++) {
+    const uint64_t b = start[g], e = start[g + 1];
+    long long mn = INT64_MAX, mx = INT64_MIN;
+    for (uint64_t i = b + blockIdx.x * (uint64_t)kT + threadIdx.x; i < e; i += (uint64_t)gridDim.x * kT) {
+      const long long k = keys[i];
+      mn = k < mn ? k : mn;
+      mx = k > mx ? k : mx;
+    }
+    for (int o = 16; o; o >>= 1) {
+      mn = min(mn, (long long)__shfl_xor_sync(0xffffffffu, mn, o));
+      mx = max(mx, (long long)__shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0 && b < e) {
+      atomicMin(out + 2 * g, mn);
+      atomicMax(out + 2 * g + 1, mx);
+    }
+  }
+}
+
 // ------------------------------------------------------------ hash group-by
 constexpr int kMaxKeys = 8;
 constexpr int kMaxVals = 16;
@@ -1029,6 +1074,60 @@ int alk_gather(const int64_t* d_src, const uint32_t* d_idx, uint64_t n, int64_t*
   k_gather<<<grid_for(n), kT, 0, (cudaStream_t)stream>>>(d_src, d_idx, n, d_out);
   alk::g_kernel_launches++;
   CK(cudaGetLastError());
+  return ALK_OK;
+}
+
+int alk_gather_u32(const uint32_t* d_src, const uint32_t* d_idx, uint64_t n, uint32_t* d_out, alk_stream stream) {
+  if (n == 0) return ALK_OK;
+  if (!d_src || !d_idx || !d_out) return ALK_ERR_ARG;
+  k_gather_u32<<<grid_for(n), kT, 0, (cudaStream_t)stream>>>(d_src, d_idx, n, d_out);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  return ALK_OK;
+}
+
+int alk_pair_match(const uint32_t* d_pl, const uint32_t* d_pr, uint64_t n, const int64_t* d_lcol,
+                   const int64_t* d_rcol, int neq, uint64_t* d_flags, alk_stream stream) {
+  if (n == 0) return ALK_OK;
+  if (!d_pl || !d_pr || !d_lcol || !d_rcol || !d_flags) return ALK_ERR_ARG;
+  k_pair_match<<<grid_for(n), kT, 0, (cudaStream_t)stream>>>(d_pl, d_pr, n, d_lcol, d_rcol, neq,
+                                                             (unsigned long long*)d_flags);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  return ALK_OK;
+}
+
+int alk_rows_mark(const uint32_t* d_rows, uint64_t n, uint64_t* d_flags, uint64_t value, alk_stream stream) {
+  if (n == 0) return ALK_OK;
+  if (!d_rows || !d_flags) return ALK_ERR_ARG;
+  k_rows_mark<<<grid_for(n), kT, 0, (cudaStream_t)stream>>>(d_rows, n, (unsigned long long*)d_flags, value);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  return ALK_OK;
+}
+
+int alk_seg_minmax(const int64_t* d_keys, const uint64_t* h_start, uint32_t nseg, int64_t* h_out, alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (nseg == 0) return ALK_OK;
+  if (!d_keys || !h_start || !h_out) return ALK_ERR_ARG;
+  Scratch sc(s);
+  cudaError_t e;
+  uint64_t* d_start = sc.get<uint64_t>(nseg + 1, &e);
+  CK(e);
+  long long* d_out = sc.get<long long>(2 * (size_t)nseg, &e);
+  CK(e);
+  std::vector<long long> init(2 * (size_t)nseg);
+  for (uint32_t g = 0; g < nseg; g++) {
+    init[2 * g] = INT64_MAX;
+    init[2 * g + 1] = INT64_MIN;
+  }
+  CK(cudaMemcpyAsync(d_start, h_start, (nseg + 1) * 8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_out, init.data(), init.size() * 8, cudaMemcpyHostToDevice, s));
+  k_seg_minmax<<<grid_for(h_start[nseg]), kT, 0, s>>>(d_keys, d_start, nseg, d_out);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h_out, d_out, init.size() * 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
   return ALK_OK;
 }
 

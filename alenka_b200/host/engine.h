@@ -246,6 +246,11 @@ class Engine {
   alk_program compile_filter(Var* f, Var* src, std::vector<std::string>& slots);
 
   void exec(Statement& st);
+  uint64_t filter_pairs(DevBufP& pl, DevBufP& pr, uint64_t pairs, const DevBufP& lcol, const DevBufP& rcol,
+                        unsigned jac, const std::vector<char>& eq_type);
+  void semi_anti_join(Var* c, Rows& L, Rows& R, const std::string& lkey, const std::string& rkey,
+                      const std::string& f3, const std::string& f4, unsigned jac, const std::vector<char>& eq_type,
+                      char kind);
   void emit_filter(Statement& st);
   void emit_select(Statement& st);
   void select_output(SelectCtx& c);

@@ -1258,6 +1258,133 @@ void Engine::emit_join(Statement& st) {
   }
 }
 
+// The AND-ed key pairs of a join (operators.cu:1288-1348) on its pairs (pl, pr): extra pair
+// m keeps the pairs whose first extra columns compare equal (not equal when the m-th
+// queued equality is '!='). The pairs are compacted in order; returns their count.
+uint64_t Engine::filter_pairs(DevBufP& pl, DevBufP& pr, uint64_t pairs, const DevBufP& lcol, const DevBufP& rcol,
+                              unsigned jac, const std::vector<char>& eq_type) {
+  for (unsigned m = 0; m < jac && pairs; m++) {
+    const int neq = m < eq_type.size() && eq_type[m] == 'N';
+    auto flags = mkbuf(pairs * 8, stream_);
+    check(alk_pair_match(pl->as<uint32_t>(), pr->as<uint32_t>(), pairs, lcol->as<int64_t>(), rcol->as<int64_t>(), neq,
+                         flags->as<uint64_t>(), (alk_stream)stream_),
+          "join AND pair");
+    auto idx = mkbuf(pairs * 4, stream_);
+    uint64_t kept = 0;
+    check(alk_live_compact(flags->as<uint64_t>(), pairs, idx->as<uint32_t>(), &kept, (alk_stream)stream_),
+          "join AND compact");
+    auto npl = mkbuf(std::max<uint64_t>(kept, 1) * 4, stream_), npr = mkbuf(std::max<uint64_t>(kept, 1) * 4, stream_);
+    check(alk_gather_u32(pl->as<uint32_t>(), idx->as<uint32_t>(), kept, npl->as<uint32_t>(), (alk_stream)stream_),
+          "join AND gather");
+    check(alk_gather_u32(pr->as<uint32_t>(), idx->as<uint32_t>(), kept, npr->as<uint32_t>(), (alk_stream)stream_),
+          "join AND gather");
+    pl = npl;
+    pr = npr;
+    pairs = kept;
+  }
+  return pairs;
+}
+
+// Semi and anti joins (operators.cu:1357-1399, 1473-1530): the rows of one side that have
+// (semi) or lack (anti) a partner after the AND-ed pairs, each once.
+//  '1' left semi, '3' left anti: left rows in left order. A left segment whose filtered key
+//     range misses the right side's key range adds nothing, even to an anti join (the
+//     range test skips the segment before the join kinds are told apart,
+//     operators.cu:1215-1220).
+//  '2' right semi, '4' right anti: right rows in the order of the right side sorted by
+//     its key (the reference sorts it for the merge join, stably), across all left segments.
+void Engine::semi_anti_join(Var* c, Rows& L, Rows& R, const std::string& lkey, const std::string& rkey,
+                            const std::string& f3, const std::string& f4, unsigned jac,
+                            const std::vector<char>& eq_type, char kind) {
+  const bool left_rows = kind == '1' || kind == '3';
+  const uint64_t nrows = left_rows ? L.n : R.n;
+  DevBufP pl, pr;
+  uint64_t pairs = 0;
+  if (L.n && R.n) {
+    alk_join_table* t = nullptr;
+    check(alk_join_build(R.col.at(rkey)->as<int64_t>(), R.n, &t, (alk_stream)stream_), "join build");
+    struct TableGuard {
+      alk_join_table* t;
+      cudaStream_t s;
+      ~TableGuard() { alk_join_free(t, (alk_stream)s); }
+    } guard{t, stream_};
+    uint64_t cap = std::max<uint64_t>(L.n, 1024);
+    for (int attempt = 0; attempt < 2; attempt++) {
+      pl = mkbuf(cap * 4, stream_);
+      pr = mkbuf(cap * 4, stream_);
+      int rc = alk_join_probe(t, L.col.at(lkey)->as<int64_t>(), L.n, pl->as<uint32_t>(), pr->as<uint32_t>(), cap,
+                              &pairs, (alk_stream)stream_);
+      if (rc == ALK_ERR_OVERFLOW && attempt == 0) {
+        cap = pairs;
+        continue;
+      }
+      check(rc, "join probe");
+      break;
+    }
+    if (jac) pairs = filter_pairs(pl, pr, pairs, L.col.at(f3), R.col.at(f4), jac, eq_type);
+  }
+  const bool anti = kind == '3' || kind == '4';
+  auto flags = mkbuf(std::max<uint64_t>(nrows, 1) * 8, stream_);
+  if (nrows) check(alk_fill_i64(flags->as<int64_t>(), nrows, anti ? 1 : 0, (alk_stream)stream_), "join flags");
+  if (pairs)
+    check(alk_rows_mark((left_rows ? pl : pr)->as<uint32_t>(), pairs, flags->as<uint64_t>(), anti ? 0 : 1,
+                        (alk_stream)stream_),
+          "join mark");
+  if (kind == '3' && nrows) {
+    // left segments whose key range misses the right side's
+    std::vector<uint64_t> start(L.seg_counts.size() + 1, 0);
+    for (size_t g = 0; g < L.seg_counts.size(); g++) start[g + 1] = start[g] + L.seg_counts[g];
+    int64_t rr[2] = {INT64_MAX, INT64_MIN};
+    if (R.n) {
+      const uint64_t rs[2] = {0, R.n};
+      check(alk_seg_minmax(R.col.at(rkey)->as<int64_t>(), rs, 1, rr, (alk_stream)stream_), "join range");
+    }
+    std::vector<int64_t> lr(2 * L.seg_counts.size());
+    check(alk_seg_minmax(L.col.at(lkey)->as<int64_t>(), start.data(), (uint32_t)L.seg_counts.size(), lr.data(),
+                         (alk_stream)stream_),
+          "join range");
+    for (size_t g = 0; g < L.seg_counts.size(); g++) {
+      if (!L.seg_counts[g]) continue;
+      if (!R.n || lr[2 * g] > rr[1] || lr[2 * g + 1] < rr[0])
+        check(alk_fill_i64(flags->as<int64_t>() + start[g], L.seg_counts[g], 0, (alk_stream)stream_), "join flags");
+    }
+  }
+  // the kept rows, in the side's order (right: sorted by key, stably)
+  DevBufP order;
+  if (!left_rows && nrows) {
+    order = mkbuf(nrows * 4, stream_);
+    const int64_t* keys[1] = {R.col.at(rkey)->as<int64_t>()};
+    const uint8_t asc[1] = {0};
+    check(alk_sort_perm(keys, asc, 1, nrows, order->as<uint32_t>(), (alk_stream)stream_), "join order");
+    auto sorted_flags = mkbuf(nrows * 8, stream_);
+    check(alk_gather(flags->as<int64_t>(), order->as<uint32_t>(), nrows, sorted_flags->as<int64_t>(),
+                     (alk_stream)stream_),
+          "join order");
+    flags = sorted_flags;
+  }
+  auto idx = mkbuf(std::max<uint64_t>(nrows, 1) * 4, stream_);
+  uint64_t kept = 0;
+  if (nrows)
+    check(alk_live_compact(flags->as<uint64_t>(), nrows, idx->as<uint32_t>(), &kept, (alk_stream)stream_),
+          "join compact");
+  if (order && kept) {
+    auto rows = mkbuf(kept * 4, stream_);
+    check(alk_gather_u32(order->as<uint32_t>(), idx->as<uint32_t>(), kept, rows->as<uint32_t>(), (alk_stream)stream_),
+          "join order");
+    idx = rows;
+  }
+  Rows& side = left_rows ? L : R;
+  c->n = kept;
+  for (auto& n : c->columnNames) {
+    auto d = mkbuf(std::max<uint64_t>(kept, 1) * 8, stream_);
+    if (kept)
+      check(alk_gather(side.col.at(n)->as<int64_t>(), idx->as<uint32_t>(), kept, d->as<int64_t>(), (alk_stream)stream_),
+            "join gather");
+    c->data[n] = d;
+  }
+  ck(cudaStreamSynchronize(stream_), "join sync");
+}
+
 // emit_multijoin (operators.cu:940-1582): inner equi-join of a (filtered) left side
 // with a right side; the right side is hashed (MurmurHash64A, linear probing) instead
 // of sorted, so pairs come out as a multiset.
@@ -1277,8 +1404,19 @@ void Engine::multijoin(Statement& st, const std::string& s, const std::string& j
   }
   std::string f1 = op_g.at(gi), f2 = op_g.at(gi + 1);
   unsigned jac = st.join_and_cnt.count(st.join_tab_cnt - tab) ? st.join_and_cnt.at(st.join_tab_cnt - tab) : 0;
-  if (jac) unsupported("multi-column joins");
-  if (st.join_type.at(tab - 1) != 'I') unsupported("outer / semi / anti joins");
+  const char kind = st.join_type.at(tab - 1);
+  if (kind != 'I' && kind != '1' && kind != '2' && kind != '3' && kind != '4')
+    unsupported("outer joins");  // the reference's outer joins are commented out (operators.cu:1242-1260)
+  if ((jac || kind != 'I') && st.join_tab_cnt != 1) unsupported("multi-column / semi / anti joins in a join chain");
+  // AND-ed key pairs (operators.cu:1288-1348): every extra pair tests the first extra pair's
+  // columns (the queue is copied afresh each time), with the equality type of the step's
+  // queued '=' / '!=' in order, the first being the primary key's
+  std::string f3, f4;
+  if (jac) {
+    f3 = op_g.at(gi + 2);
+    f4 = op_g.at(gi + 3);
+    if (!left->has(f3) || !right->has(f4)) unsupported("AND-ed join column outside its side");
+  }
   auto c = std::make_unique<Var>();
   c->kind = Var::Mat;
   c->name = s;
@@ -1305,16 +1443,30 @@ void Engine::multijoin(Statement& st, const std::string& s, const std::string& j
   // char keys are dictionary codes: codes of two different dictionaries do not compare
   if (left->meta[colname1].type == 2 && left->meta[colname1].string_map != right->meta[colname2].string_map)
     unsupported("join on char columns of different dictionaries");
+  // a left semi / anti join outputs left rows only, a right one right rows only (the
+  // reference gathers the other side through pairs it has since reordered)
+  const bool left_rows = kind == '1' || kind == '3', right_rows = kind == '2' || kind == '4';
+  for (auto& n : c->columnNames) {
+    if (left_rows && !left->has(n)) unsupported("right-side column in a left semi / anti join");
+    if (right_rows && !right->has(n)) unsupported("left-side column in a right semi / anti join");
+  }
   std::vector<std::string> rfields, lfields;
   for (auto& n : c->columnNames)
-    if (!left->has(n) && right->has(n)) rfields.push_back(n);
+    if ((right_rows || !left->has(n)) && right->has(n)) rfields.push_back(n);
   rfields.push_back(colname2);
+  if (jac) rfields.push_back(f4);
   for (auto& n : c->columnNames)
-    if (left->has(n)) lfields.push_back(n);
+    if (!right_rows && left->has(n)) lfields.push_back(n);
   lfields.push_back(colname1);
+  if (jac) lfields.push_back(f3);
   Rows R = materialize(right, rfields);
   Rows L = materialize(left, lfields);
   c->n = 0;
+  if (kind != 'I') {
+    semi_anti_join(c.get(), L, R, colname1, colname2, f3, f4, jac, st.join_eq_type, kind);
+    vars_[s] = std::move(c);
+    return;
+  }
   if (R.n && L.n) {
     alk_join_table* t = nullptr;
     check(alk_join_build(R.col.at(colname2)->as<int64_t>(), R.n, &t, (alk_stream)stream_), "join build");
@@ -1337,6 +1489,7 @@ void Engine::multijoin(Statement& st, const std::string& s, const std::string& j
       check(rc, "join probe");
       break;
     }
+    if (jac) pairs = filter_pairs(pl, pr, pairs, L.col.at(f3), R.col.at(f4), jac, st.join_eq_type);
     c->n = pairs;
     for (auto& n : c->columnNames) {
       bool from_left = left->has(n);

@@ -260,6 +260,19 @@ int alk_sort_perm_u64(const uint64_t* d_key, uint64_t n, uint32_t* d_perm, alk_s
  * sorts.cu:87): d_out[i] = d_src[d_idx[i]]. */
 int alk_gather(const int64_t* d_src, const uint32_t* d_idx, uint64_t n, int64_t* d_out,
                alk_stream stream);
+/* Join forms of emit_multijoin beyond the single-key inner join (operators.cu:1288-1399):
+ * d_flags[i] = lcol[pl[i]] == rcol[pr[i]] (!= when neq), the AND-ed key pair test on the
+ * pairs a join found; d_flags[rows[i]] = value, the left or right rows a semi or anti
+ * join keeps; and, per segment g of a concatenation (rows [h_start[g], h_start[g+1]) of
+ * d_keys), the least and greatest key into h_out[2g], h_out[2g+1] (INT64_MAX /
+ * INT64_MIN for an empty segment), for the anti join's per-segment range test
+ * (operators.cu:1215-1220). The last synchronises. alk_gather_u32 is alk_gather for u32
+ * row indices (pairs compacted by an AND-ed pair test). */
+int alk_gather_u32(const uint32_t* d_src, const uint32_t* d_idx, uint64_t n, uint32_t* d_out, alk_stream stream);
+int alk_pair_match(const uint32_t* d_pl, const uint32_t* d_pr, uint64_t n, const int64_t* d_lcol,
+                   const int64_t* d_rcol, int neq, uint64_t* d_flags, alk_stream stream);
+int alk_rows_mark(const uint32_t* d_rows, uint64_t n, uint64_t* d_flags, uint64_t value, alk_stream stream);
+int alk_seg_minmax(const int64_t* d_keys, const uint64_t* h_start, uint32_t nseg, int64_t* h_out, alk_stream stream);
 
 /* Width conversions used by the host engine between index and value columns. */
 int alk_widen_u32(const uint32_t* d_in, uint64_t n, int64_t* d_out, alk_stream stream);

@@ -1515,9 +1515,19 @@ class Engine {
     string f1 = op_g[gi], f2 = op_g[gi + 1];
     gi += 2;
     unsigned jac = st.join_and_cnt.count(st.join_tab_cnt - tab) ? st.join_and_cnt.at(st.join_tab_cnt - tab) : 0;
-    if (jac) throw Error("multi-column joins are not supported by the oracle");
     char kind = st.join_type[tab - 1];
-    if (kind != 'I') throw Error("only inner joins are supported by the oracle");
+    if (kind != 'I' && kind != '1' && kind != '2' && kind != '3' && kind != '4')
+      throw Error("outer joins are not supported by the oracle");
+    if ((jac || kind != 'I') && st.join_tab_cnt != 1)
+      throw Error("multi-column / semi / anti joins in a join chain are not supported by the oracle");
+    // AND-ed pairs (operators.cu:1288-1348): each of the jac checks reads the first extra
+    // pair (the queue is copied afresh) and the m-th queued equality type
+    string f3, f4;
+    if (jac) {
+      f3 = op_g[gi];
+      f4 = op_g[gi + 1];
+    }
+    const bool left_rows = kind == '1' || kind == '3', right_rows = kind == '2' || kind == '4';
     // result layout: CudaSet(right, left, op_sel_s) (cm.cu:3078-3160)
     auto c = std::make_unique<Var>();
     c->name = s;
@@ -1552,6 +1562,11 @@ class Engine {
     for (auto& n : op_sel_s)
       if (right->has(n) && std::find(rfields.begin(), rfields.end(), n) == rfields.end()) rfields.push_back(n);
     if (std::find(rfields.begin(), rfields.end(), f2) == rfields.end()) rfields.push_back(f2);
+    if (jac && std::find(rfields.begin(), rfields.end(), f4) == rfields.end()) rfields.push_back(f4);
+    for (auto& n : c->columnNames) {
+      if (left_rows && !left->has(n)) throw Error("right-side column in a left semi / anti join");
+      if (right_rows && !right->has(n)) throw Error("left-side column in a right semi / anti join");
+    }
     Seg R = load_all(right, rfields);
     size_t cnt_r = R.n;
     const Vec& rk0 = R.c.at(colname2);
@@ -1570,6 +1585,8 @@ class Engine {
     for (auto& n : op_sel_s)
       if (left->has(n) && std::find(lfields.begin(), lfields.end(), n) == lfields.end()) lfields.push_back(n);
     if (std::find(lfields.begin(), lfields.end(), colname1) == lfields.end()) lfields.push_back(colname1);
+    if (jac && std::find(lfields.begin(), lfields.end(), f3) == lfields.end()) lfields.push_back(f3);
+    std::set<u32> ranj;  // right semi / anti: right rows matched over all left segments
     size_t cyc = cycles(left);
     for (size_t i = 0; i < cyc && cnt_r; i++) {
       Seg L = fetch(left, lfields, (unsigned)i);
@@ -1591,6 +1608,30 @@ class Engine {
           pr.push_back((u32)q);
         }
       }
+      for (unsigned m = 0; m < jac; m++) {  // stable: the pairs keep their order
+        const bool neq = m < st.join_eq_type.size() && st.join_eq_type[m] == 'N';
+        const Vec& a = L.c.at(f3);
+        const Vec& b = RS.at(f4);
+        vector<u32> ql, qr;
+        for (size_t q = 0; q < pl.size(); q++)
+          if ((a[pl[q]] == b[pr[q]]) != neq) {
+            ql.push_back(pl[q]);
+            qr.push_back(pr[q]);
+          }
+        pl.swap(ql);
+        pr.swap(qr);
+      }
+      if (right_rows) {  // accumulated; output after every left segment (operators.cu:1376-1399)
+        ranj.insert(pr.begin(), pr.end());
+        continue;
+      }
+      if (left_rows) {  // left semi: matched left rows once; anti: the others; left order
+        vector<char> hit(cnt_l, 0);
+        for (u32 x : pl) hit[x] = 1;
+        pl.clear();
+        for (u32 r = 0; r < cnt_l; r++)
+          if (hit[r] == (kind == '1')) pl.push_back(r);
+      }
       for (auto& n : c->columnNames) {
         Vec& dst = c->h[n];
         if (left->has(n)) {
@@ -1602,6 +1643,17 @@ class Engine {
         }
       }
       c->mRecCount += pl.size();
+    }
+    if (right_rows) {  // right rows in the sorted right side's order
+      vector<u32> rows;
+      for (u32 r = 0; r < cnt_r; r++)
+        if (ranj.count(r) == (size_t)(kind == '2')) rows.push_back(r);
+      for (auto& n : c->columnNames) {
+        Vec& dst = c->h[n];
+        const Vec& src = RS.at(n);
+        for (u32 r : rows) dst.push_back(src[r]);
+      }
+      c->mRecCount = rows.size();
     }
     c->hostRecCount = c->maxRecs = c->mRecCount;
     c->segCount = 1;

@@ -166,6 +166,39 @@ FUSED_PREDICATES = {
                    "o_orderdate >= 19941001", 'c_mktsegment == "BUILDING"'),
 }
 
+# emit_multijoin's other forms (operators.cu:1288-1399); left rows come in left order and
+# right rows in key order, so those outputs are compared byte for byte
+_JF = ("OFI := FILTER orders BY o_orderdate < 19950101;\n"
+       "LF := FILTER lineitem BY l_shipdate < 19950301;\n")
+JOIN_FORMS = {
+    "and_same_pair": (_JF + "J := SELECT l_orderkey AS lk, o_orderdate AS od FROM LF JOIN OFI "
+                            "ON l_orderkey = o_orderkey AND l_orderkey = o_orderkey;\n"
+                            "STORE J INTO 'jf.txt' USING ('|');\n", "multiset"),
+    "and_second_pair": (_JF + "J := SELECT l_orderkey AS lk, l_discount AS d, o_orderdate AS od FROM LF JOIN OFI "
+                              "ON l_orderkey = o_orderkey AND l_discount = o_shippriority;\n"
+                              "STORE J INTO 'jf.txt' USING ('|');\n", "multiset"),
+    "left_semi": (_JF + "K := SELECT l_orderkey AS lk, l_extendedprice AS p FROM LF LEFT SEMI JOIN OFI "
+                        "ON l_orderkey = o_orderkey;\n"
+                        "STORE K INTO 'jf.txt' USING ('|');\n", "bytes"),
+    "left_semi_and": (_JF + "K := SELECT l_orderkey AS lk, l_shipdate AS sd FROM LF LEFT SEMI JOIN OFI "
+                            "ON l_orderkey = o_orderkey AND l_discount = o_shippriority;\n"
+                            "STORE K INTO 'jf.txt' USING ('|');\n", "bytes"),
+    "left_anti": (_JF + "M := SELECT l_orderkey AS lk, l_shipdate AS sd FROM LF LEFT ANTI JOIN OFI "
+                        "ON l_orderkey = o_orderkey;\n"
+                        "STORE M INTO 'jf.txt' USING ('|');\n", "bytes"),
+    "right_semi": (_JF + "R := SELECT o_orderkey AS ok, o_orderdate AS od FROM LF RIGHT SEMI JOIN OFI "
+                         "ON l_orderkey = o_orderkey;\n"
+                         "STORE R INTO 'jf.txt' USING ('|');\n", "bytes"),
+    "right_anti": (_JF + "RA := SELECT o_orderkey AS ok, o_custkey AS ck FROM LF RIGHT ANTI JOIN OFI "
+                         "ON l_orderkey = o_orderkey;\n"
+                         "STORE RA INTO 'jf.txt' USING ('|');\n", "bytes"),
+    "left_semi_grouped": (_JF + "K := SELECT l_orderkey AS lk, l_extendedprice AS p FROM LF LEFT SEMI JOIN OFI "
+                                "ON l_orderkey = o_orderkey;\n"
+                                "G := SELECT lk AS k, SUM(p) AS s, COUNT(lk) AS c FROM K GROUP BY lk;\n"
+                                "O := ORDER G BY s DESC, k ASC;\n"
+                                "STORE O INTO 'jf.txt' USING ('|') LIMIT 20;\n", "bytes"),
+}
+
 JOIN_SCRIPTS = {
     # join output with no ORDER: the reference's row order comes from its sort-merge, so
     # it is compared as a multiset
@@ -223,6 +256,8 @@ def _cases():
               "script": three_way_with("l_orderkey < 200000 AND l_shipdate > 19950101", "o_orderdate < 19960101",
                                        'c_mktsegment == "BUILDING"', "fx.txt", limit=0),
               "out": "fx.txt", "segments_skipped": 2})
+    for n, (sc, mode) in sorted(JOIN_FORMS.items()):
+        c.append({"name": f"three_way_join_{n}", "dataset": "three_way", "script": sc, "out": "jf.txt", "mode": mode})
     for n, (sc, out, mode) in sorted(JOIN_SCRIPTS.items()):
         c.append({"name": f"three_way_{n}", "dataset": "three_way", "script": sc, "out": out, "mode": mode})
     # the stated sizes: config 1 (6M rows) and config 2 (60M / 15M / 1.5M)
