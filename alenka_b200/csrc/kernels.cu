@@ -101,6 +101,55 @@ __global__ void __launch_bounds__(kT) k_decode_delta(DeltaArgs a) {
   }
 }
 
+// ------------------------------------------------------------ ordered flag compaction
+// out = the indices i (ascending) with flags[i] != 0: tiles claimed in increasing order,
+// each thread counting 8 consecutive flags, a block scan and a decoupled look-back for the
+// tile's base (the semi / anti joins keep their side's row order, operators.cu:1357-1399).
+struct CompactArgs {
+  const unsigned long long* flags;
+  uint64_t n;
+  uint32_t ntiles;
+  uint32_t* tflags;
+  uint64_t* aggs;
+  uint64_t* incls;
+  uint32_t* ctr;
+  int* err;
+  uint32_t* out;
+  unsigned long long* count;
+};
+__global__ void __launch_bounds__(kT) k_flags_compact(CompactArgs a) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint64_t s_warp[kT / 32 + 1];
+  __shared__ uint64_t s_base;
+  __shared__ int s_ok;
+  while (true) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(a.ctr, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    __syncthreads();
+    if (tile >= a.ntiles) break;
+    const uint64_t r0 = (uint64_t)tile * kTile + (uint64_t)threadIdx.x * kItems;  // blocked
+    uint32_t m = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; k++)
+      if (r0 + k < a.n && a.flags[r0 + k]) m |= 1u << k;
+    uint64_t tot;
+    const uint64_t excl = block_excl_scan<kT>((uint64_t)__popc(m), s_warp, &tot);
+    if (threadIdx.x == 0) {
+      bool ok;
+      s_base = lookback_u64(a.tflags, a.aggs, a.incls, tile, tot, a.err, &ok);
+      s_ok = ok;
+      if (ok && tile == a.ntiles - 1) *a.count = s_base + tot;
+    }
+    __syncthreads();
+    if (s_ok) {
+      uint64_t o = s_base + excl;
+      for (uint32_t q = m; q; q &= q - 1) a.out[o++] = (uint32_t)(r0 + (uint32_t)(__ffs(q) - 1));
+    }
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------------ fused scan
 struct ScanArgs {
   const alk_colseg* cols;  // [ncols][nseg]
@@ -1083,6 +1132,35 @@ int alk_gather_u32(const uint32_t* d_src, const uint32_t* d_idx, uint64_t n, uin
   k_gather_u32<<<grid_for(n), kT, 0, (cudaStream_t)stream>>>(d_src, d_idx, n, d_out);
   alk::g_kernel_launches++;
   CK(cudaGetLastError());
+  return ALK_OK;
+}
+
+int alk_flags_compact(const uint64_t* d_flags, uint64_t n, uint32_t* d_out, uint64_t* h_count, alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!h_count) return ALK_ERR_ARG;
+  *h_count = 0;
+  if (n == 0) return ALK_OK;
+  if (!d_flags || !d_out || n > 0xffffffffull) return ALK_ERR_ARG;
+  Scratch sc(s);
+  cudaError_t e;
+  const uint32_t ntiles = (uint32_t)((n + kTile - 1) / kTile);
+  uint32_t* tflags = sc.get<uint32_t>(ntiles + 4, &e);
+  CK(e);
+  uint64_t* aggs = sc.get<uint64_t>(2 * (size_t)ntiles + 2, &e);
+  CK(e);
+  CK(cudaMemsetAsync(tflags, 0, (ntiles + 4) * sizeof(uint32_t), s));
+  CompactArgs a{(const unsigned long long*)d_flags, n, ntiles, tflags, aggs, aggs + ntiles, tflags + ntiles,
+                (int*)(tflags + ntiles + 1), d_out, (unsigned long long*)(aggs + 2 * ntiles)};
+  k_flags_compact<<<std::min<int>(ntiles, sm_count() * 4), kT, 0, s>>>(a);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  unsigned long long res[2] = {0, 0};
+  int h_err = 0;
+  CK(cudaMemcpyAsync(res, aggs + 2 * ntiles, 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&h_err, tflags + ntiles + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (h_err) return h_err;
+  *h_count = res[0];
   return ALK_OK;
 }
 

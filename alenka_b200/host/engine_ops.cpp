@@ -1271,7 +1271,7 @@ uint64_t Engine::filter_pairs(DevBufP& pl, DevBufP& pr, uint64_t pairs, const De
           "join AND pair");
     auto idx = mkbuf(pairs * 4, stream_);
     uint64_t kept = 0;
-    check(alk_live_compact(flags->as<uint64_t>(), pairs, idx->as<uint32_t>(), &kept, (alk_stream)stream_),
+    check(alk_flags_compact(flags->as<uint64_t>(), pairs, idx->as<uint32_t>(), &kept, (alk_stream)stream_),
           "join AND compact");
     auto npl = mkbuf(std::max<uint64_t>(kept, 1) * 4, stream_), npr = mkbuf(std::max<uint64_t>(kept, 1) * 4, stream_);
     check(alk_gather_u32(pl->as<uint32_t>(), idx->as<uint32_t>(), kept, npl->as<uint32_t>(), (alk_stream)stream_),
@@ -1365,7 +1365,7 @@ void Engine::semi_anti_join(Var* c, Rows& L, Rows& R, const std::string& lkey, c
   auto idx = mkbuf(std::max<uint64_t>(nrows, 1) * 4, stream_);
   uint64_t kept = 0;
   if (nrows)
-    check(alk_live_compact(flags->as<uint64_t>(), nrows, idx->as<uint32_t>(), &kept, (alk_stream)stream_),
+    check(alk_flags_compact(flags->as<uint64_t>(), nrows, idx->as<uint32_t>(), &kept, (alk_stream)stream_),
           "join compact");
   if (order && kept) {
     auto rows = mkbuf(kept * 4, stream_);

@@ -269,6 +269,9 @@ int alk_gather(const int64_t* d_src, const uint32_t* d_idx, uint64_t n, int64_t*
  * (operators.cu:1215-1220). The last synchronises. alk_gather_u32 is alk_gather for u32
  * row indices (pairs compacted by an AND-ed pair test). */
 int alk_gather_u32(const uint32_t* d_src, const uint32_t* d_idx, uint64_t n, uint32_t* d_out, alk_stream stream);
+/* The indices i < n with d_flags[i] != 0, ascending, into d_out (room for n); the count
+ * into *h_count. Synchronises. (alk_live_compact gives the same set in no set order.) */
+int alk_flags_compact(const uint64_t* d_flags, uint64_t n, uint32_t* d_out, uint64_t* h_count, alk_stream stream);
 int alk_pair_match(const uint32_t* d_pl, const uint32_t* d_pr, uint64_t n, const int64_t* d_lcol,
                    const int64_t* d_rcol, int neq, uint64_t* d_flags, alk_stream stream);
 int alk_rows_mark(const uint32_t* d_rows, uint64_t n, uint64_t* d_flags, uint64_t value, alk_stream stream);
