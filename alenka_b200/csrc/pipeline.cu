@@ -51,6 +51,10 @@ struct HtView {
   // popcount of the bitmap below it (rank[w] = set bits in words < w). Keys and payload
   // are dense over slots [0, nslots); cap is then the slot capacity. Null: hash table.
   uint32_t* rank;
+  // Dense tables only: 0 keys and payload stored at their ranks (build records, rank
+  // prefix, scatter); 1 ranks only (bitmap and rank prefix: slots for accumulators, no
+  // keys or payload stored); 2 membership only (the bitmap).
+  uint32_t dense_mode;
 };
 
 __device__ __forceinline__ bool ht_member(const HtView& h, int64_t k) {
@@ -474,7 +478,12 @@ __global__ void __launch_bounds__(kT) k_stage_hits(const StageArgs a) {
 // set already is a duplicate key; a key outside the bitmap range is flagged).
 __global__ void __launch_bounds__(kT) k_rank_mark(const StageArgs a) {
   const uint64_t n = *(volatile unsigned long long*)a.hit_count;
-  if (n > a.hit_cap) return;  // the scatter pass reports the overflow
+  if (n > a.hit_cap) {
+    // the scatter pass reports the overflow; a table that stores no keys has none
+    if (a.build.dense_mode && blockIdx.x == 0 && threadIdx.x == 0) atomicExch(a.err, ALK_ERR_OVERFLOW);
+    return;
+  }
+  unsigned long long inserted = 0;
   for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
     const Hit h = a.hits[i * a.hit_words];
     if (h == kNoHit) continue;
@@ -494,6 +503,12 @@ __global__ void __launch_bounds__(kT) k_rank_mark(const StageArgs a) {
     }
     const uint32_t bit = 1u << (o & 31);
     if (atomicOr(a.build.bits + (o >> 5), bit) & bit) atomicExch(a.build.flags, 1);
+    else inserted++;
+  }
+  // the key count of a membership-only table (the rank prefix counts the others)
+  if (a.build.dense_mode == 2) {
+    for (int o = 16; o; o >>= 1) inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
+    if ((threadIdx.x & 31) == 0 && inserted) atomicAdd(a.build.nslots, inserted);
   }
 }
 
@@ -1329,7 +1344,8 @@ __device__ __forceinline__ void load8_narrow(const void* p, uint32_t bits, uint3
   }
 }
 
-// kMode: 0 survivors to the hit list, 1 inline dense build, 2 inline hash build.
+// kMode: 0 survivors to the hit list, 1 inline dense build (records), 2 inline hash build,
+// 3 inline dense build of a table that stores no keys (bits only).
 // kConj: the predicate's conjuncts. A block's tiles advance by gridDim.x, so each thread
 // follows its segment incrementally and keeps the segment's column descriptors, conjunct
 // tests and probe plan in registers (no per-tile table lookups).
@@ -1422,7 +1438,22 @@ __global__ void __launch_bounds__(kT) k_stage_vec(const __grid_constant__ TmaArg
     __syncwarp();
     const uint32_t tile_row0 = (tile - tile0) * kTile;
     const alk_colseg& kd = s_cd[t.key_st * a.nseg + seg];
-    if (kMode == 1) {
+    if (kMode == 3) {
+      // dense table without stored keys: the key's bit; a bit found set already is a
+      // duplicate key, a new one counts as an inserted key
+      for (uint32_t j = lane; j < total; j += 32) {
+        const uint32_t r = tile_row0 + wl[j];
+        const int64_t key = load_for(kd.data, kd.bits, kd.lower, r);
+        const uint64_t o = (uint64_t)key - (uint64_t)a.build.kmin;
+        if (o >= a.build.nbits) {
+          atomicExch(a.build.flags + 3, 1);
+          continue;
+        }
+        const uint32_t bit = 1u << (o & 31);
+        if (atomicOr(a.build.bits + (o >> 5), bit) & bit) atomicExch(a.build.flags, 1);
+        else inserted++;
+      }
+    } else if (kMode == 1) {
       // dense table: the key's bit, and the record [position, key, payload...]
       const HitWriter::Room room = hw.reserve(a, total);
       for (uint32_t j = lane; j < total; j += 32) {
@@ -1657,18 +1688,22 @@ cudaError_t launch_stage(FastArgs fa, bool conj, bool narrow_all, const alk_cols
     // settled by the exact key bitmap
     const bool can_inline = kBuild && h_pay_src && !a.need_slot && (a.probe_slot < 0 || a.probe.bits);
     if (narrow_all) vec = (can_inline && plan_vec(true)) || plan_vec(false);
-    if (!vec) tma = (can_inline && plan(true)) || plan(false);
+    // the staged kernel's inline dense build writes records: tables that store no keys
+    // take the survivor list and the bit-marking pass instead
+    const bool tma_inline = can_inline && !(a.build.rank && a.build.dense_mode);
+    if (!vec) tma = (tma_inline && plan(true)) || plan(false);
   }
   const bool inline_build = (tma || vec) && t.inline_build;
   const bool dense = kBuild && a.build.rank != nullptr;
   // a dense build staged inline records [position, key, payload] per survivor
-  a.hit_words = dense && inline_build ? 2 + a.build.npay : 1;
+  a.hit_words = dense && inline_build && !a.build.dense_mode ? 2 + a.build.npay : 1;
   t.f.a.hit_words = a.hit_words;
   int occ = 0;
   // the blocked kernel's mode: hit list, inline dense build, inline hash build
-  void (*vec_kernel)(const TmaArgs) = !inline_build ? vec_kernel_for<0>(fa.nconj)
-                                      : dense         ? vec_kernel_for<1>(fa.nconj)
-                                                      : vec_kernel_for<2>(fa.nconj);
+  void (*vec_kernel)(const TmaArgs) = !inline_build               ? vec_kernel_for<0>(fa.nconj)
+                                      : dense && a.build.dense_mode ? vec_kernel_for<3>(fa.nconj)
+                                      : dense                       ? vec_kernel_for<1>(fa.nconj)
+                                                                    : vec_kernel_for<2>(fa.nconj);
   if (vec) {
     cudaFuncSetAttribute(vec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, vec_smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, vec_kernel, kT, vec_smem);
@@ -1698,16 +1733,22 @@ cudaError_t launch_stage(FastArgs fa, bool conj, bool narrow_all, const alk_cols
   const int hits_grid = sms() * std::max(occ_hits, 1);
   if (dense) {
     // dense build: key bits (from positions, when the scan did not set them), the rank
-    // prefix, then the scatter of keys and payload to their ranks
+    // prefix (unless the table is membership only), then the scatter of keys and payload
+    // to their ranks (only for a table that stores them)
     if (!inline_build) {
       k_rank_mark<<<hits_grid, kT, 0, s>>>(a);
       launches++;
     }
-    k_rank_sums<<<a.rk_tiles, kT, 0, s>>>(a);
-    k_rank_scan_sums<<<1, kRankScanThreads, 0, s>>>(a);
-    k_rank_write<<<a.rk_tiles, kT, 0, s>>>(a);
-    k_stage_hits<kBuild><<<hits_grid, kT, 0, s>>>(a);
-    launches += 4;
+    if (a.build.dense_mode != 2) {
+      k_rank_sums<<<a.rk_tiles, kT, 0, s>>>(a);
+      k_rank_scan_sums<<<1, kRankScanThreads, 0, s>>>(a);
+      k_rank_write<<<a.rk_tiles, kT, 0, s>>>(a);
+      launches += 3;
+    }
+    if (a.build.dense_mode == 0) {
+      k_stage_hits<kBuild><<<hits_grid, kT, 0, s>>>(a);
+      launches++;
+    }
   } else if (!inline_build) {
     k_stage_hits<kBuild><<<hits_grid, kT, 0, s>>>(a);
     launches++;
@@ -1715,6 +1756,109 @@ cudaError_t launch_stage(FastArgs fa, bool conj, bool narrow_all, const alk_cols
   if (timer && timer->on) cudaEventRecordWithFlags((cudaEvent_t)timer->ev1, s, evflags);
   alk::g_kernel_launches += launches;
   return cudaGetLastError();
+}
+
+// Late payload of a ranks-only dense table (keys and payload fetched for a few candidate
+// slots after the aggregation, instead of stored for every key during the build).
+struct LateArgs {
+  HtView h;
+  const uint32_t* cand;             // candidate slots
+  const unsigned long long* count;  // their number (device)
+  uint32_t cap;                     // at most this many are handled
+  uint32_t nseg, npay;
+  const alk_colseg* cols;   // [1 + npay][nseg]: the key column (ascending), then payload
+  const int64_t* seg_lo;    // [nseg] zone bounds of the key column
+  const int64_t* seg_hi;
+  const uint8_t* seg_mode;  // [nseg] segments the build stage scanned
+  int64_t* const* out;      // [1 + npay] slot-indexed columns: key, payload
+  int* status;              // set: a candidate matched no row or more than one
+};
+
+// First index in [lo, hi) whose value is >= key (hi if none), for values nondecreasing
+// in the index; 32-ary: each round the warp tests 32 pivots, so a range of n values takes
+// ceil(log32 n) dependent loads instead of log2 n. Called by all 32 lanes.
+template <class F>
+__device__ __forceinline__ uint64_t warp_lower_bound(uint64_t lo, uint64_t hi, int64_t key, F value) {
+  const uint32_t lane = threadIdx.x & 31;
+  while (hi - lo > 32) {
+    const uint64_t step = (hi - lo + 31) / 32;
+    const uint64_t p = lo + lane * step;
+    const uint32_t c = __popc(__ballot_sync(0xffffffffu, p < hi && value(p) < key));
+    if (c == 0) return lo;
+    // the answer lies after pivot c - 1 and at or before pivot c (or hi)
+    const uint64_t nlo = lo + (uint64_t)(c - 1) * step + 1;
+    hi = min(hi, lo + (uint64_t)c * step);
+    lo = nlo;
+  }
+  return lo + __popc(__ballot_sync(0xffffffffu, lo + lane < hi && value(lo + lane) < key));
+}
+
+// One warp per candidate: its key from the rank prefix (the last bitmap word whose rank
+// is <= slot, then the (slot - rank)-th set bit), then the key's rows by binary search
+// in each scanned segment whose zone holds the key. Exactly one row: its payload is the
+// candidate's; none or several: status.
+__global__ void __launch_bounds__(kT) k_late_rows(const LateArgs a) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t n = (uint32_t)min((unsigned long long)a.cap, *(volatile const unsigned long long*)a.count);
+  const uint64_t nkeys = *(volatile const unsigned long long*)a.h.nslots;
+  const uint64_t nwords = (a.h.nbits + 31) / 32;
+  const uint32_t warps = gridDim.x * (kT / 32);
+  for (uint32_t i = blockIdx.x * (kT / 32) + (threadIdx.x >> 5); i < n; i += warps) {
+    const uint32_t slot = a.cand[i];
+    if (slot >= nkeys || slot >= a.h.slot_cap) {
+      if (lane == 0) atomicExch(a.status, 1);
+      continue;
+    }
+    const uint64_t w =
+        warp_lower_bound(0, nwords, (int64_t)slot + 1, [&](uint64_t x) { return (int64_t)a.h.rank[x]; }) - 1;
+    uint32_t m = a.h.bits[w];
+    for (uint32_t r = slot - a.h.rank[w]; r && m; r--) m &= m - 1;
+    if (!m) {  // the rank prefix and the bitmap disagree
+      if (lane == 0) atomicExch(a.status, 1);
+      continue;
+    }
+    const int64_t key = (int64_t)((uint64_t)a.h.kmin + w * 32 + (uint64_t)(__ffs(m) - 1));
+    if (lane == 0) a.out[0][slot] = key;
+    uint32_t found = 0, fg = 0;
+    uint64_t frow = 0;
+    for (uint32_t g0 = 0; g0 < a.nseg && found < 2; g0 += 32) {
+      const uint32_t g = g0 + lane;
+      uint32_t hit = __ballot_sync(0xffffffffu, g < a.nseg && a.seg_mode[g] && key >= a.seg_lo[g] &&
+                                                    key <= a.seg_hi[g]);
+      for (; hit && found < 2; hit &= hit - 1) {
+        const uint32_t sg = g0 + __ffs(hit) - 1;
+        const alk_colseg kd = a.cols[sg];
+        auto v = [&](uint64_t x) { return load_for(kd.data, kd.bits, kd.lower, x); };
+        const uint64_t lb = warp_lower_bound(0, kd.rows, key, v);
+        uint32_t c = 0;
+        if (lb < kd.rows && v(lb) == key) c = (lb + 1 < kd.rows && v(lb + 1) == key) ? 2 : 1;
+        if (c && !found) {
+          fg = sg;
+          frow = lb;
+        }
+        found += c;
+      }
+    }
+    if (lane != 0) continue;
+    if (found != 1) {
+      atomicExch(a.status, 1);
+      continue;
+    }
+    for (uint32_t p = 0; p < a.npay; p++) {
+      const alk_colseg& pd = a.cols[(uint64_t)(1 + p) * a.nseg + fg];
+      a.out[1 + p][slot] = load_for(pd.data, pd.bits, pd.lower, frow);
+    }
+  }
+}
+
+// Per segment: 1 when a row's value is below its predecessor's.
+__global__ void __launch_bounds__(kT) k_seg_unsorted(const alk_colseg* segs, uint32_t* flags) {
+  const uint32_t g = blockIdx.y;
+  const alk_colseg d = segs[g];
+  int bad = 0;
+  for (uint64_t r = 1 + blockIdx.x * (uint64_t)kT + threadIdx.x; r < d.rows && !bad; r += (uint64_t)gridDim.x * kT)
+    bad = load_for(d.data, d.bits, d.lower, r) < load_for(d.data, d.bits, d.lower, r - 1);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flags + g, 1u);
 }
 
 bool prog_ok(const alk_program& p, uint32_t ncols, uint32_t npay) {
@@ -1800,29 +1944,33 @@ int alk_ht_create_range(uint64_t max_keys, uint32_t npay, int64_t key_min, int64
   return ALK_OK;
 }
 
-int alk_ht_create_dense(uint64_t max_keys, uint32_t npay, int64_t key_min, int64_t key_max, alk_ht** out,
-                        alk_stream stream) {
+int alk_ht_create_dense_mode(uint64_t max_keys, uint32_t npay, int64_t key_min, int64_t key_max, int mode,
+                             alk_ht** out, alk_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (!out || npay > 8 || max_keys >= 0xffffffffull || key_max < key_min) return ALK_ERR_ARG;
+  if (mode < ALK_DENSE_FULL || mode > ALK_DENSE_BITS || (mode != ALK_DENSE_FULL && npay)) return ALK_ERR_ARG;
   const uint64_t span = (uint64_t)key_max - (uint64_t)key_min + 1;
   if (span == 0 || span > ALK_DENSE_MAX_SPAN) return ALK_ERR_UNSUPPORTED;  // no exact bitmap
   const uint64_t cap = std::max<uint64_t>(max_keys, 1);  // slots are ranks: no spare room
   const size_t words = (span + 31) / 32;
-  const size_t off_pay = cap * 8;
-  const size_t off_ctr = off_pay + cap * 8 * npay;
+  // keys and payload only for a table that stores them
+  const size_t off_pay = mode == ALK_DENSE_FULL ? cap * 8 : 0;
+  const size_t off_ctr = off_pay + (mode == ALK_DENSE_FULL ? cap * 8 * npay : 0);
   const size_t off_bits = (off_ctr + 64 + 15) & ~size_t(15);  // 16-byte aligned (vector loads)
   const size_t off_rank = off_bits + ((words * 4 + 15) & ~size_t(15));
+  // a membership-only table keeps a one-word rank array: probes of it never ask for slots
+  const size_t rank_bytes = mode == ALK_DENSE_BITS ? 16 : words * 4;
   auto* h = new alk_ht();
-  cudaError_t e = cudaMallocAsync(&h->mem, off_rank + words * 4, s);
+  cudaError_t e = cudaMallocAsync(&h->mem, off_rank + rank_bytes, s);
   if (e != cudaSuccess) {
     delete h;
     return alk::cuda_fail(e);
   }
-  h->bytes = off_rank + words * 4;
+  h->bytes = off_rank + rank_bytes;
   uint8_t* p = (uint8_t*)h->mem;
   h->v.cap = cap;
-  h->v.key = (int64_t*)p;
-  h->v.payload = (int64_t*)(p + off_pay);
+  h->v.key = mode == ALK_DENSE_FULL ? (int64_t*)p : nullptr;
+  h->v.payload = mode == ALK_DENSE_FULL ? (int64_t*)(p + off_pay) : nullptr;
   h->v.slot_cap = cap;
   h->v.npay = npay;
   h->v.nslots = (unsigned long long*)(p + off_ctr);
@@ -1831,9 +1979,15 @@ int alk_ht_create_dense(uint64_t max_keys, uint32_t npay, int64_t key_min, int64
   h->v.kmin = key_min;
   h->v.nbits = span;
   h->v.rank = (uint32_t*)(p + off_rank);
+  h->v.dense_mode = (uint32_t)mode;
   CK(cudaMemsetAsync(p + off_ctr, 0, off_rank - off_ctr, s));  // counters and bitmap
   *out = h;
   return ALK_OK;
+}
+
+int alk_ht_create_dense(uint64_t max_keys, uint32_t npay, int64_t key_min, int64_t key_max, alk_ht** out,
+                        alk_stream stream) {
+  return alk_ht_create_dense_mode(max_keys, npay, key_min, key_max, ALK_DENSE_FULL, out, stream);
 }
 
 int alk_ht_create(uint64_t max_keys, uint32_t npay, alk_ht** out, alk_stream stream) {
@@ -2067,6 +2221,7 @@ static int pipeline_build(const alk_colseg* cols, uint32_t ncols, uint32_t nseg,
   a.build = build->v;
   for (uint32_t p = 0; p < build->v.npay; p++)
     if (pay_src[p] >= 32) a.need_slot = 1;
+  if (probe && probe->v.dense_mode == ALK_DENSE_BITS && a.need_slot) return ALK_ERR_ARG;  // no slots
   return run_stage<true>(a, prog, cols, seg_mode, hb, off_x, hit_cap, h_rows_in, h_hits, h_status, s, nullptr);
 }
 
@@ -2097,6 +2252,7 @@ static int pipeline_probe_agg(const alk_colseg* cols, uint32_t ncols, uint32_t n
   if (!probe || probe_slot < 0 || (uint32_t)probe_slot >= ncols || ncols == 0 || ncols > kMaxCols || nagg > 7)
     return ALK_ERR_ARG;
   if (acc_stride < probe->v.slot_cap) return ALK_ERR_ARG;  // accumulators indexed by table position
+  if (probe->v.dense_mode == ALK_DENSE_BITS) return ALK_ERR_ARG;  // a membership-only table has no slots
 
   std::vector<alk_program> progs(1 + nagg);
   std::memset(progs.data(), 0, sizeof(alk_program) * progs.size());
@@ -2245,6 +2401,90 @@ int alk_gather_rows(const int64_t* const* d_cols, uint32_t ncols, const uint32_t
       g, ncols, d_idx, (const unsigned long long*)d_count, cap, d_out);
   alk::g_kernel_launches++;
   CK(cudaGetLastError());
+  return ALK_OK;
+}
+
+int alk_ht_late_rows(const alk_ht* h, const uint32_t* d_cand, const uint64_t* d_count, uint32_t cap,
+                     const alk_colseg* cols, uint32_t npay, uint32_t nseg, const uint8_t* seg_mode,
+                     const int64_t* seg_lo, const int64_t* seg_hi, int64_t* const* d_out, int32_t* d_status,
+                     alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!h || h->v.dense_mode != ALK_DENSE_RANKS || !d_cand || !d_count || !cols || !seg_mode || !seg_lo ||
+      !seg_hi || !d_out || !d_status || npay > 8 || nseg == 0)
+    return ALK_ERR_ARG;
+  for (uint32_t c = 0; c <= npay; c++)
+    if (!d_out[c]) return ALK_ERR_ARG;
+  for (uint32_t c = 0; c <= npay; c++)
+    for (uint32_t g = 0; g < nseg; g++) {
+      const alk_colseg& d = cols[(size_t)c * nseg + g];
+      if (d.rows != cols[g].rows || !(d.bits == 8 || d.bits == 16 || d.bits == 32 || d.bits == 64)) return ALK_ERR_ARG;
+      if (seg_mode[g] && d.rows && !d.data) return ALK_ERR_ARG;
+    }
+  if (cap == 0) return ALK_OK;
+  // one upload: descriptors, zone bounds, output addresses, segment verdicts
+  const size_t n_cols = (size_t)(1 + npay) * nseg;
+  const size_t off_lo = (n_cols * sizeof(alk_colseg) + 15) & ~size_t(15);
+  const size_t off_hi = off_lo + 8 * (size_t)nseg;
+  const size_t off_out = off_hi + 8 * (size_t)nseg;
+  const size_t off_mode = off_out + 8 * (size_t)(1 + npay);
+  const size_t up_bytes = (off_mode + nseg + 15) & ~size_t(15);
+  std::vector<uint8_t> up(up_bytes, 0);
+  std::memcpy(up.data(), cols, n_cols * sizeof(alk_colseg));
+  std::memcpy(up.data() + off_lo, seg_lo, 8 * (size_t)nseg);
+  std::memcpy(up.data() + off_hi, seg_hi, 8 * (size_t)nseg);
+  std::memcpy(up.data() + off_out, d_out, 8 * (size_t)(1 + npay));
+  std::memcpy(up.data() + off_mode, seg_mode, nseg);
+  uint8_t* db = nullptr;
+  CK(cudaMallocAsync((void**)&db, up_bytes, s));
+  cudaError_t ue;
+  const void* src = alk::upload_source(up.data(), up.size(), s, &ue);
+  CK(ue);
+  CK(cudaMemcpyAsync(db, src, up.size(), cudaMemcpyHostToDevice, s));
+  LateArgs a{};
+  a.h = h->v;
+  a.cand = d_cand;
+  a.count = (const unsigned long long*)d_count;
+  a.cap = cap;
+  a.nseg = nseg;
+  a.npay = npay;
+  a.cols = (const alk_colseg*)db;
+  a.seg_lo = (const int64_t*)(db + off_lo);
+  a.seg_hi = (const int64_t*)(db + off_hi);
+  a.out = (int64_t* const*)(db + off_out);
+  a.seg_mode = db + off_mode;
+  a.status = d_status;
+  const uint32_t blocks = std::min<uint32_t>((cap + kT / 32 - 1) / (kT / 32), (uint32_t)sms() * 2);
+  k_late_rows<<<blocks, kT, 0, s>>>(a);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  CK(cudaFreeAsync(db, s));
+  return ALK_OK;
+}
+
+int alk_seg_sorted(const alk_colseg* segs, uint32_t nseg, uint8_t* h_sorted, alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (nseg == 0) return ALK_OK;
+  if (!segs || !h_sorted || nseg > 65535) return ALK_ERR_ARG;
+  uint64_t most = 0;
+  for (uint32_t g = 0; g < nseg; g++) {
+    if (!(segs[g].bits == 8 || segs[g].bits == 16 || segs[g].bits == 32 || segs[g].bits == 64)) return ALK_ERR_ARG;
+    if (segs[g].rows && !segs[g].data) return ALK_ERR_ARG;
+    most = std::max<uint64_t>(most, segs[g].rows);
+  }
+  const size_t off_flags = (sizeof(alk_colseg) * (size_t)nseg + 15) & ~size_t(15);
+  uint8_t* db = nullptr;
+  CK(cudaMallocAsync((void**)&db, off_flags + 4 * (size_t)nseg, s));
+  CK(cudaMemcpyAsync(db, segs, sizeof(alk_colseg) * nseg, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(db + off_flags, 0, 4 * (size_t)nseg, s));
+  const uint32_t bx = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((most + kT * 16 - 1) / (kT * 16), 512));
+  k_seg_unsorted<<<dim3(bx, nseg), kT, 0, s>>>((const alk_colseg*)db, (uint32_t*)(db + off_flags));
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  std::vector<uint32_t> f(nseg);
+  CK(cudaMemcpyAsync(f.data(), db + off_flags, 4 * (size_t)nseg, cudaMemcpyDeviceToHost, s));
+  CK(cudaFreeAsync(db, s));
+  CK(cudaStreamSynchronize(s));
+  for (uint32_t g = 0; g < nseg; g++) h_sorted[g] = f[g] ? 0 : 1;
   return ALK_OK;
 }
 

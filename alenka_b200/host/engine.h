@@ -69,6 +69,10 @@ struct BaseCol {
   std::vector<uint8_t*> host_img;     // pinned host copies of the segment files
   std::vector<size_t> host_len;
   std::vector<DevBufP> dev;           // device payload (FOR) or expanded int64 (delta)
+  // per segment: its values in ascending order (1) or not (0), as checked on the device
+  // buffer recorded beside it (a segment uploaded again is checked again)
+  std::vector<std::weak_ptr<DevBuf>> order_buf;
+  std::vector<int8_t> ascending;
   bool headers_read = false;
   bool device_only = false;  // generated in device memory: no files, never released
   // char dictionaries
@@ -142,6 +146,7 @@ struct FusedTail {
   uint64_t small = 0, cand_cap = 0;             // rows returned with the first copy; candidate cap
   std::string first_key, path, sep;
   uint64_t kernels = 0, d2h = 0, rows = 0;      // statistics of one execution
+  std::string late_sig;  // the last build stage fetched its payload late (status to check)
 };
 struct FusedGraph;
 struct SelectCtx;
@@ -241,6 +246,11 @@ class Engine {
   Var* base_table(const std::string& t);
   BaseCol& basecol(Var* base, const std::string& col);
   void read_headers(Var* base, const std::string& col, BaseCol& bc);
+  // Every segment with mode[g] != 0 holds the column's values in ascending order (one
+  // device pass per segment not checked before; none when may_sync is false: unknown
+  // segments then count as unsorted).
+  bool segs_ascending(BaseCol& bc, const std::vector<alk_colseg>& segs, const std::vector<uint8_t>& mode,
+                      bool may_sync);
   void load_dict(Var* base, const std::string& col, BaseCol& bc);
   std::vector<char> zone_maps(Var* f, Var* src);
   alk_program compile_filter(Var* f, Var* src, std::vector<std::string>& slots);
@@ -279,6 +289,7 @@ class Engine {
   std::map<std::string, std::shared_ptr<FusedGraph>> fused_graphs_;
   std::set<std::string> fused_seen_;
   std::set<std::string> fused_nograph_;  // queries whose capture failed
+  std::set<std::string> late_off_;       // build stages whose rows could not name a late candidate
   std::string cur_script_;
   std::unordered_map<std::string, std::vector<Statement>> parsed_;  // script text -> statements
   // a batch's final STOREs: formatted at once, written together after the batch (the

@@ -2049,6 +2049,8 @@ struct RerunFused {
 struct FusedStatus {
   alk_stage_status st[3];  // build stage 1, build stage 2, probe-aggregate
   alk_ht_status ht[2];
+  int32_t late;  // the late payload fetch could not name a candidate's row
+  int32_t pad;
 };
 constexpr uint64_t kSmallCand = 1024;     // candidate rows returned with the first copy
 constexpr uint64_t kCandCap = 1 << 16;    // candidates at most (more ties: operator plan)
@@ -2199,6 +2201,34 @@ bool Engine::try_fused(std::vector<Statement>& sts, size_t& i) {
   return true;
 }
 
+bool Engine::segs_ascending(BaseCol& bc, const std::vector<alk_colseg>& segs, const std::vector<uint8_t>& mode,
+                            bool may_sync) {
+  const size_t nseg = segs.size();
+  if (bc.dev.size() != nseg || mode.size() != nseg) return false;
+  bc.order_buf.resize(nseg);
+  bc.ascending.resize(nseg, 0);
+  std::vector<uint32_t> todo;
+  for (uint32_t g = 0; g < nseg; g++)
+    if (mode[g] && (!bc.dev[g] || bc.order_buf[g].lock() != bc.dev[g])) todo.push_back(g);
+  if (!todo.empty()) {
+    if (!may_sync) return false;
+    std::vector<alk_colseg> d;
+    for (uint32_t g : todo) {
+      if (!bc.dev[g] || segs[g].data != bc.dev[g]->as<void>()) return false;
+      d.push_back(segs[g]);
+    }
+    std::vector<uint8_t> asc(todo.size());
+    check(alk_seg_sorted(d.data(), (uint32_t)d.size(), asc.data(), (alk_stream)stream_), "segment order");
+    for (size_t k = 0; k < todo.size(); k++) {
+      bc.order_buf[todo[k]] = bc.dev[todo[k]];
+      bc.ascending[todo[k]] = (int8_t)asc[k];
+    }
+  }
+  for (uint32_t g = 0; g < nseg; g++)
+    if (mode[g] && !bc.ascending[g]) return false;
+  return true;
+}
+
 void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, const std::string& gkey) {
   cudaStream_t s = stream_;
   // a captured graph of this very query: replay it and do the host part
@@ -2338,6 +2368,7 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     if (o.col_type == 2 && has_col(o.vec)) fallback("row-level expression in a grouped select");
   }
   std::set<std::string> fact_cols;
+  bool agg_reads_build = false;  // an aggregate input reads a build-side column
   for (auto& ag : aggs) {
     if (!ag.input) continue;
     std::vector<AstP> stack = {ag.input};
@@ -2348,13 +2379,24 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
       if (a->k == Ast::Col) {
         const std::string& src = src_of.at(a->col);
         if (origin(src) == fact) fact_cols.insert(src);
-        else need_payload(src);
+        else {
+          need_payload(src);
+          agg_reads_build = true;
+        }
       }
       stack.push_back(a->l);
       stack.push_back(a->r);
     }
   }
   if (payload.size() > 8) fallback("payload width");
+  // the first ORDER key is ranked on the device: a build-side column there needs its
+  // values for every slot
+  bool order_by_build_col = false;
+  if (!O.op_type.empty()) {
+    const std::string name = O.op_type[0] == "NAME" ? O.op_value.at(0) : O.op_type[0];
+    for (auto& o : outs)
+      if (o.name == name && o.col_type == 1) order_by_build_col = true;
+  }
   // ---- build stages
   // Stage sizes come from the exact counts the previous run of the same stage recorded
   // (the counts the engine learns from its own runs): hash tables from the inserted key
@@ -2385,8 +2427,11 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
   // A stage without recorded counts is sized by the learned estimator when it is on;
   // returns the fraction of the key range the table is expected to hold (the exact
   // fraction when recording), a feature of the stage that probes it.
+  auto is_dense = [](std::pair<int64_t, int64_t> range) {
+    return range.second >= range.first && (uint64_t)range.second - (uint64_t)range.first < ALK_DENSE_MAX_SPAN;
+  };
   auto build_stage = [&](HtGuard& g, const std::string& sig, uint64_t upper, uint32_t npay,
-                         std::pair<int64_t, int64_t> range, int idx, const CardStage& cst,
+                         std::pair<int64_t, int64_t> range, int mode, int idx, const CardStage& cst,
                          const std::function<int(alk_ht*, uint64_t, alk_stage_status*)>& run) -> double {
     auto it = card_feedback_.find(sig);
     uint64_t est = it == card_feedback_.end() ? upper : std::min(upper, it->second + it->second / 4 + 1024);
@@ -2402,14 +2447,16 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     // a key range below 2^32 values (the zone maps) takes the dense, rank-addressed
     // table (a bitmap of span/8 bytes plus a u32 rank per bitmap word: 150 MB for the
     // 600M-wide o_orderkey range of a 150M-row orders table); wider ranges the hash table
-    const bool dense = range.second >= range.first &&
-                       (uint64_t)range.second - (uint64_t)range.first < ALK_DENSE_MAX_SPAN;
-    if (dense) check(alk_ht_create_dense(est, npay, range.first, range.second, &g.h, (alk_stream)s), "dense table");
+    const bool dense = is_dense(range);
+    if (dense)
+      check(alk_ht_create_dense_mode(est, npay, range.first, range.second, mode, &g.h, (alk_stream)s),
+            "dense table");
     else check(alk_ht_create_range(est, npay, range.first, range.second, &g.h, (alk_stream)s), "hash table");
     check(run(g.h, hcap, &fs->st[idx]), "build stage");
     check(alk_ht_info_async(g.h, &fs->ht[idx], (alk_stream)s), "hash table");
     tail.pending.push_back({sig, idx, idx, upper});
-    stats_.reserved_bytes += alk_ht_bytes(g.h) + (hcap ? hcap : upper) * 8 * (dense ? 2 + npay : 1);
+    stats_.reserved_bytes +=
+        alk_ht_bytes(g.h) + (hcap ? hcap : upper) * 8 * (dense && mode == ALK_DENSE_FULL ? 2 + npay : 1);
     const double span = range.second >= range.first ? (double)range.second - (double)range.first + 1.0 : 0.0;
     if (span <= 0) return 0.0;
     if (card_record_) {
@@ -2436,6 +2483,50 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
   double last_fill = 0;                      // fraction of its key range the last table holds
   std::pair<int64_t, int64_t> last_range;    // and that key range
   ScanPlan last_scan;                        // the scan that built it
+  // Late payload: when F reads the last table's key and payload columns only as group or
+  // output columns (no aggregate input, not the device-ranked ORDER key), and the build
+  // table's key column is ascending in its segments, that table keeps ranks only; after
+  // the top-k the candidate slots' keys and payload are fetched from the build table's
+  // rows by binary search (alk_ht_late_rows). A key found in no row or in several makes
+  // the query run again with the full table.
+  bool late = false;
+  std::map<std::string, uint32_t> late_pay;  // payload column -> late column 1 + index
+  std::vector<alk_colseg> late_cs;           // [1 + npay][nseg]: key, payload columns
+  std::vector<int64_t> late_lo, late_hi;     // key zone bounds per segment
+  auto late_plan = [&](ScanPlan& p, const std::vector<alk_colseg>& cs, const std::string& sig,
+                       std::pair<int64_t, int64_t> range) -> bool {
+    if (!fast || agg_reads_build || order_by_build_col || late_off_.count(sig) || !is_dense(range)) return false;
+    if (p.src->segCount == 0 || p.src->segCount > 65535) return false;
+    if (cs.size() < (size_t)p.slots.size() * p.src->segCount) return false;
+    for (auto& c : payload)
+      if (!p.src->has(c)) return false;  // carried from the inner table
+    // exact zone bounds: FOR headers hold the segment's minimum and maximum
+    BaseCol& kb = basecol(p.src, build_key);
+    read_headers(p.src, build_key, kb);
+    for (auto& sg : kb.segs)
+      if (sg.m.comp_type != 0) return false;
+    const uint32_t nseg = p.src->segCount;
+    // the candidates' rows are found by binary search: the key column must be ascending
+    // in every scanned segment (checked once per resident segment, outside a capture)
+    std::vector<alk_colseg> kcs(cs.begin() + (size_t)p.slot(build_key) * nseg,
+                                cs.begin() + (size_t)(p.slot(build_key) + 1) * nseg);
+    if (!segs_ascending(kb, kcs, p.mode, !capture)) return false;
+    std::vector<std::string> names = {build_key};
+    names.insert(names.end(), payload.begin(), payload.end());
+    late_cs.clear();
+    for (auto& c : names) {
+      const uint32_t sl = p.slot(c);
+      for (uint32_t g = 0; g < nseg; g++) late_cs.push_back(cs.at((size_t)sl * nseg + g));
+    }
+    late_lo.assign(nseg, 0);
+    late_hi.assign(nseg, 0);
+    for (uint32_t g = 0; g < nseg; g++) {
+      late_lo[g] = kb.segs[g].m.lower;
+      late_hi[g] = kb.segs[g].m.upper;
+    }
+    for (size_t k = 0; k < payload.size(); k++) late_pay[payload[k]] = 1 + (uint32_t)k;
+    return true;
+  };
   if (J.join_tab_cnt == 2) {
     // stage 1: d2 (innermost right) keyed on st1.rkey, carrying the d2 columns needed later
     ScanPlan p1 = plan_scan(d2);
@@ -2453,7 +2544,10 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     c1.cs = &cs1;
     c1.key_slot = (int32_t)k1;
     c1.key_range = range_of(p1.src, st1.rkey);
-    const double fill1 = build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)pay1.size(), range_of(p1.src, st1.rkey), 0, c1,
+    // a table that carries no payload is probed for membership only
+    const int mode1 = pay1.empty() ? ALK_DENSE_BITS : ALK_DENSE_FULL;
+    const double fill1 = build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)pay1.size(), range_of(p1.src, st1.rkey),
+                                     mode1, 0, c1,
                 [&](alk_ht* h, uint64_t cap, alk_stage_status* st) {
                   return alk_pipeline_build_async(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount,
                                                   p1.mode.data(), p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h,
@@ -2488,7 +2582,13 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     c2.up = &p1;
     c2.key_slot = key2;
     c2.key_range = range_of(p2.src, build_key);
-    last_fill = build_stage(ht2, sig2, rows_of(p2, cs2), (uint32_t)payload.size(), range_of(p2.src, build_key), 1, c2,
+    late = late_plan(p2, cs2, sig2, c2.key_range);
+    if (late) {
+      src2.clear();
+      last_pay.clear();
+    }
+    last_fill = build_stage(ht2, sig2, rows_of(p2, cs2), (uint32_t)src2.size(), range_of(p2.src, build_key),
+                            late ? ALK_DENSE_RANKS : ALK_DENSE_FULL, 1, c2,
                 [&](alk_ht* h, uint64_t cap, alk_stage_status* st) {
                   return alk_pipeline_build_async(cs2.data(), (uint32_t)p2.slots.size(), p2.src->segCount,
                                                   p2.mode.data(), p2.has_pred ? &p2.pred : nullptr, ht1.h,
@@ -2513,7 +2613,13 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     c1.cs = &cs1;
     c1.key_slot = (int32_t)k1;
     c1.key_range = range_of(p1.src, build_key);
-    last_fill = build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)payload.size(), range_of(p1.src, build_key), 0, c1,
+    late = late_plan(p1, cs1, sig1, c1.key_range);
+    if (late) {
+      src1.clear();
+      last_pay.clear();
+    }
+    last_fill = build_stage(ht1, sig1, rows_of(p1, cs1), (uint32_t)src1.size(), range_of(p1.src, build_key),
+                            late ? ALK_DENSE_RANKS : ALK_DENSE_FULL, 0, c1,
                 [&](alk_ht* h, uint64_t cap, alk_stage_status* st) {
                   return alk_pipeline_build_async(cs1.data(), (uint32_t)p1.slots.size(), p1.src->segCount,
                                                   p1.mode.data(), p1.has_pred ? &p1.pred : nullptr, nullptr, -1, h,
@@ -2607,8 +2713,16 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     tail.streamed_bytes = scan_bytes(pf, std::vector<uint32_t>(streamed.begin(), streamed.end()));
   }
   // ---- F's columns over slots
+  std::vector<DevBufP> late_buf;  // slot-indexed key and payload columns, written late
+  std::vector<int64_t*> late_ptr;
+  if (late)
+    for (size_t c = 0; c <= payload.size(); c++) {
+      late_buf.push_back(mkbuf(stride * 8, s));
+      late_ptr.push_back(late_buf.back()->as<int64_t>());
+    }
   auto slot_col = [&](const std::string& alias) -> const int64_t* {
     const std::string& src = src_of.at(alias);
+    if (late) return late_ptr.at(src == build_key ? 0 : late_pay.at(src));
     if (src == build_key && !last_pay.count(src)) return alk_ht_keys(last);
     return alk_ht_payload(last, last_pay.at(src));
   };
@@ -2714,6 +2828,17 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     check(alk_topk_select(rank, cnt->as<uint64_t>(), nslots, limit, cand->as<uint32_t>(), kCandCap,
                           dcount->as<uint64_t>(), (alk_stream)s),
           "top-k");
+    if (late) {
+      auto lst = mkbuf(4, s);
+      ck(cudaMemsetAsync(lst->as<void>(), 0, 4, s), "late status");
+      check(alk_ht_late_rows(last, cand->as<uint32_t>(), dcount->as<uint64_t>(), (uint32_t)kCandCap,
+                             late_cs.data(), (uint32_t)payload.size(), last_scan.src->segCount,
+                             last_scan.mode.data(), late_lo.data(), late_hi.data(), late_ptr.data(),
+                             lst->as<int32_t>(), (alk_stream)s),
+            "late rows");
+      ck(cudaMemcpyAsync(&fs->late, lst->as<void>(), 4, cudaMemcpyDeviceToHost, s), "d2h");
+      tail.late_sig = last_sig;
+    }
     check(alk_gather_rows(back_cols.data(), (uint32_t)nback, cand->as<uint32_t>(), dcount->as<uint64_t>(),
                           tail.small, tmp->as<int64_t>(), (alk_stream)s),
           "gather");
@@ -2729,6 +2854,7 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     cand.reset();
     rank_buf.reset();
     keep.clear();
+    late_buf.clear();
     acc.reset();
     cnt.reset();
     ht2.release();
@@ -2815,6 +2941,11 @@ void Engine::finish_fused(const FusedTail& t) {
     }
   }
   if (rerun) throw RerunFused();
+  if (!t.late_sig.empty() && fs->late) {
+    // a candidate key matched no row or several: this stage keeps its payload from now on
+    late_off_.insert(t.late_sig);
+    throw RerunFused();
+  }
   if (timing_ && t.timed) {
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0_, ev1_);

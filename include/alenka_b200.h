@@ -276,6 +276,9 @@ int alk_pair_match(const uint32_t* d_pl, const uint32_t* d_pr, uint64_t n, const
                    const int64_t* d_rcol, int neq, uint64_t* d_flags, alk_stream stream);
 int alk_rows_mark(const uint32_t* d_rows, uint64_t n, uint64_t* d_flags, uint64_t value, alk_stream stream);
 int alk_seg_minmax(const int64_t* d_keys, const uint64_t* h_start, uint32_t nseg, int64_t* h_out, alk_stream stream);
+/* Per column segment (nseg <= 65535 descriptors): 1 when its values are in ascending
+ * order (ties allowed), else 0, into h_sorted[g]. Synchronises. */
+int alk_seg_sorted(const alk_colseg* segs, uint32_t nseg, uint8_t* h_sorted, alk_stream stream);
 
 /* Width conversions used by the host engine between index and value columns. */
 int alk_widen_u32(const uint32_t* d_in, uint64_t n, int64_t* d_out, alk_stream stream);
@@ -318,6 +321,34 @@ int alk_ht_create_range(uint64_t max_keys, uint32_t npay, int64_t key_min, int64
  * flag 2, capacity exceeded). ALK_ERR_UNSUPPORTED for a wider range. */
 int alk_ht_create_dense(uint64_t max_keys, uint32_t npay, int64_t key_min, int64_t key_max, alk_ht** out,
                         alk_stream stream);
+/* What a dense table keeps. FULL: keys and payload at their slots (the build writes one
+ * record per surviving row and scatters it to its rank). RANKS: the bitmap and the rank
+ * prefix only (slots for per-key accumulators; keys and payload are fetched later for a
+ * few slots by alk_ht_late_rows; alk_ht_keys and alk_ht_payload return NULL). BITS: the
+ * bitmap only (membership probes; a stage that asks this table for slots is refused).
+ * In RANKS and BITS a build detects duplicate keys from the bitmap itself. */
+#define ALK_DENSE_FULL 0
+#define ALK_DENSE_RANKS 1
+#define ALK_DENSE_BITS 2
+/* alk_ht_create_dense with a mode; npay must be 0 unless the mode is ALK_DENSE_FULL. */
+int alk_ht_create_dense_mode(uint64_t max_keys, uint32_t npay, int64_t key_min, int64_t key_max, int mode,
+                             alk_ht** out, alk_stream stream);
+/* Keys and payload of a few slots of an ALK_DENSE_RANKS table, after the fact. d_cand
+ * holds candidate slots, their number in device memory d_count (at most cap of them are
+ * handled). Each candidate's key is selected back from the bitmap and rank prefix and
+ * written to d_out[0][slot]; the key's rows are then found by binary search in the build
+ * table's scanned segments (seg_mode != 0) whose key range [seg_lo, seg_hi] (the key
+ * column's zone maps) holds it, and payload p of the one row found is written to
+ * d_out[1 + p][slot]. cols: [1 + npay][nseg] descriptors, the key column first, then the
+ * payload columns; the key column of every scanned segment must be in ascending order
+ * (alk_seg_sorted). A candidate whose key is found in no row or in more than one sets
+ * *d_status to 1 (the rows cannot name the surviving one: build the table FULL). d_out is
+ * a host array of 1 + npay device addresses of slot-indexed columns of alk_ht_slots(h)
+ * values. Asynchronous; no host synchronisation, capturable in a CUDA graph. */
+int alk_ht_late_rows(const alk_ht* h, const uint32_t* d_cand, const uint64_t* d_count, uint32_t cap,
+                     const alk_colseg* cols, uint32_t npay, uint32_t nseg, const uint8_t* seg_mode,
+                     const int64_t* seg_lo, const int64_t* seg_hi, int64_t* const* d_out, int32_t* d_status,
+                     alk_stream stream);
 void alk_ht_free(alk_ht* h, alk_stream stream);
 /* Inserted keys and flags (1 duplicate key, 2 capacity exceeded, 4 wait expired,
  * 8 key outside the declared range). */

@@ -298,3 +298,134 @@ def test_topk_select_and_gather_rows(k):
     idx = d_out.cpu().numpy()[:min(m, small)].astype(np.int64)
     assert np.array_equal(rows[:len(idx)], rank[idx])
     assert np.array_equal(rows[small:small + len(idx)], other[idx])
+
+
+ALK_ERR_ARG, ALK_DENSE_FULL, ALK_DENSE_RANKS, ALK_DENSE_BITS = 1, 0, 1, 2
+
+
+def _lt_pred(slot, c0, conjunctive):
+    """column(slot) < c0; as a single conjunct, or (not a conjunction) OR-ed with
+    column(slot) < -1, which no row meets."""
+    p = Program()
+    p.consts[0] = c0
+    p.ins[0] = Instr(ALK_OP_LT, 0, ALK_K_COL, ALK_K_CONST, slot, 0, 0)
+    if conjunctive:
+        p.n_instr, p.result = 1, 0
+        return p
+    p.consts[1] = -1
+    p.n_instr, p.result = 3, 2
+    p.ins[1] = Instr(ALK_OP_LT, 1, ALK_K_COL, ALK_K_CONST, slot, 1, 0)
+    p.ins[2] = Instr(ALK_OP_OR, 2, ALK_K_REG, ALK_K_REG, 0, 1, 0)
+    return p
+
+
+@pytest.mark.parametrize("route", ["blocked", "positions"])
+@pytest.mark.parametrize("dup", [None, "filtered", "skipped"])
+def test_dense_modes_and_late_rows(route, dup):
+    """Ranks-only and membership-only dense tables, and the late fetch of keys and
+    payload for candidate slots. Three segments of ascending, disjoint key ranges, the
+    middle one skipped; a predicate keeps 60% of the rows. 'blocked': a one-conjunct
+    predicate on narrow columns runs the blocked scan, which sets the bits itself;
+    'positions': a predicate that is not a conjunction goes through the survivor list and
+    the bitmap pass. dup 'filtered': a row the predicate removes repeats a candidate's key,
+    so the late fetch cannot tell the rows apart and reports it; 'skipped': the repeat
+    sits in the skipped segment, which the fetch does not read. alk_seg_sorted tells the
+    ascending segments from a shuffled one."""
+    import torch
+    L = _lib()
+    vp, u32, u64, i32, i64 = c.c_void_p, c.c_uint32, c.c_uint64, c.c_int32, c.c_int64
+    L.alk_ht_create_dense_mode.argtypes = [u64, u32, i64, i64, c.c_int, c.POINTER(vp), vp]
+    L.alk_ht_late_rows.argtypes = [vp, vp, vp, u32, c.POINTER(ColSeg), u32, u32, c.POINTER(c.c_uint8),
+                                   c.POINTER(i64), c.POINTER(i64), c.POINTER(vp), vp, vp]
+    L.alk_seg_sorted.argtypes = [c.POINTER(ColSeg), u32, c.POINTER(c.c_uint8), vp]
+    rng = np.random.default_rng(21)
+    per, nseg = 100_000, 3
+    keys = np.arange(per * nseg, dtype=np.int64) * 3 + 11
+    filt = rng.integers(0, 100, per * nseg).astype(np.int64)
+    pay0 = rng.integers(-(1 << 20), 1 << 20, per * nseg).astype(np.int64)
+    pay1 = rng.integers(-(1 << 50), 1 << 50, per * nseg).astype(np.int64)
+    seg_mode = [2, 0, 2]
+    live = (filt < 60) & np.repeat(np.array(seg_mode) != 0, per)
+    dup_key = None
+    if dup == "filtered":  # the next row, filtered out, repeats a survivor's key (order kept)
+        src = int(np.nonzero(live[:per - 1] & ~live[1:per])[0][5])
+        dup_key = int(keys[src])
+        keys[src + 1] = dup_key
+    elif dup == "skipped":  # the skipped segment's first row repeats a survivor's key
+        src = int(np.nonzero(live[:per])[0][-3])
+        dup_key = int(keys[src])
+        keys[per] = dup_key
+    bufs, segs = [], []
+    for col, bits in ((keys, 32), (filt, 8), (pay0, 32), (pay1, 64)):
+        for g in range(nseg):
+            b, cs = _column(col[g * per:(g + 1) * per], bits)
+            bufs.append(b)
+            segs.append(cs)
+    cols = (ColSeg * len(segs))(*segs)
+    mode = (c.c_uint8 * nseg)(*seg_mode)
+    asc = (c.c_uint8 * (nseg + 1))()
+    b, shuffled = _column(rng.permutation(keys[:per]), 32)
+    bufs.append(b)
+    assert L.alk_seg_sorted((ColSeg * (nseg + 1))(*(segs[:nseg] + [shuffled])), nseg + 1, asc, None) == ALK_OK
+    assert list(asc) == [1, 1, 1, 0]
+    pred = _lt_pred(1, 60, route == "blocked")
+    kmin, kmax = int(keys.min()), int(keys.max())
+    skeys = np.sort(keys[live])
+    want = {int(keys[r]): int(r) for r in np.nonzero(live)[0]}  # key -> its surviving row
+    # membership only: counts and flags, no slots; payload and late fetch refused
+    ht = c.c_void_p()
+    assert L.alk_ht_create_dense_mode(len(keys), 1, kmin, kmax, ALK_DENSE_BITS, c.byref(ht), None) == ALK_ERR_ARG
+    assert L.alk_ht_create_dense_mode(len(keys), 0, kmin, kmax, ALK_DENSE_BITS, c.byref(ht), None) == ALK_OK
+    rows_in, hits = c.c_uint64(), c.c_uint64()
+    ins, fl = c.c_uint64(), c.c_int()
+    try:
+        assert L.alk_pipeline_build(cols, 4, nseg, mode, c.byref(pred), None, -1, ht, 0, None, 0, c.byref(rows_in),
+                                    c.byref(hits), None) == ALK_OK
+        assert L.alk_ht_info(ht, c.byref(ins), c.byref(fl), None) == ALK_OK
+        assert ins.value == len(skeys) and fl.value == 0
+        assert not L.alk_ht_keys(ht) and not L.alk_ht_payload(ht, 0)
+    finally:
+        L.alk_ht_free(ht, None)
+        torch.cuda.synchronize()
+    # ranks only: slots are ranks; the late fetch names every candidate's key and row
+    ht = c.c_void_p()
+    assert L.alk_ht_create_dense_mode(len(keys), 0, kmin, kmax, ALK_DENSE_RANKS, c.byref(ht), None) == ALK_OK
+    try:
+        assert L.alk_pipeline_build(cols, 4, nseg, mode, c.byref(pred), None, -1, ht, 0, None, 0, c.byref(rows_in),
+                                    c.byref(hits), None) == ALK_OK
+        assert L.alk_ht_info(ht, c.byref(ins), c.byref(fl), None) == ALK_OK
+        assert ins.value == len(skeys) and fl.value == 0
+        slots = L.alk_ht_slots(ht)
+        cand = rng.choice(len(skeys), 300, replace=False).astype(np.int64)
+        cand[1] = 0  # the first and the last key
+        cand[2] = len(skeys) - 1
+        if dup_key is not None:
+            cand[0] = int(np.searchsorted(skeys, dup_key))
+        cand = np.unique(cand)
+        d_cand = torch.from_numpy(cand.astype(np.int32)).cuda()
+        d_cnt = torch.tensor([len(cand)], dtype=torch.int64, device="cuda")
+        outs = [torch.full((slots,), -7, dtype=torch.int64, device="cuda") for _ in range(3)]
+        outp = (c.c_void_p * 3)(*[o.data_ptr() for o in outs])
+        st = torch.zeros(1, dtype=torch.int32, device="cuda")
+        late_cols = (ColSeg * (3 * nseg))(*(segs[:nseg] + segs[2 * nseg:]))
+        lo = (c.c_int64 * nseg)(*[int(keys[g * per:(g + 1) * per].min()) for g in range(nseg)])
+        hi = (c.c_int64 * nseg)(*[int(keys[g * per:(g + 1) * per].max()) for g in range(nseg)])
+        rc = L.alk_ht_late_rows(ht, d_cand.data_ptr(), d_cnt.data_ptr(), 1 << 16, late_cols, 2, nseg, mode, lo, hi,
+                                outp, st.data_ptr(), None)
+        assert rc == ALK_OK
+        torch.cuda.synchronize()
+        assert int(st.item()) == (1 if dup == "filtered" else 0)
+        ok = cand
+        if dup == "filtered":  # the ambiguous candidate aside
+            ok = cand[skeys[cand] != dup_key]
+        got = [o.cpu().numpy() for o in outs]
+        assert np.array_equal(got[0][cand], skeys[cand])
+        rows = np.array([want[int(k)] for k in skeys[ok]])
+        assert np.array_equal(got[1][ok], pay0[rows])
+        assert np.array_equal(got[2][ok], pay1[rows])
+        untouched = np.setdiff1d(np.arange(slots), cand)
+        assert (got[0][untouched] == -7).all()
+    finally:
+        L.alk_ht_free(ht, None)
+        torch.cuda.synchronize()
+    del bufs
