@@ -368,6 +368,18 @@ __global__ void __launch_bounds__(kT) k_card_count(const StageArgs a, uint32_t s
 // build-side insert with its payload or the aggregate updates. A list that overflowed
 // its capacity is refused as a whole (nothing is applied), so a rerun with a larger list
 // starts from unchanged tables and accumulators.
+// Per lane, the reduction of v over the lanes [lane, run_end): run_end is the end of the
+// lane's run of equal slots. Warp-wide.
+__device__ __forceinline__ int64_t run_reduce(int64_t v, uint32_t run_end, uint8_t kind) {
+  const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+  for (uint32_t off = 1; off < 32; off <<= 1) {
+    const int64_t o = __shfl_down_sync(0xffffffffu, v, off);
+    if (lane + off < run_end) v = kind == ALK_AGG_MIN ? min(v, o) : kind == ALK_AGG_MAX ? max(v, o) : v + o;
+  }
+  return v;
+}
+
 template <bool kBuild>
 __global__ void __launch_bounds__(kT) k_stage_hits(const StageArgs a) {
   __shared__ alk_instr s_ins[8][ALK_MAX_INSTR];
@@ -390,6 +402,58 @@ __global__ void __launch_bounds__(kT) k_stage_hits(const StageArgs a) {
     }
     __syncthreads();
   }
+  if (!kBuild) {
+    // Probe-aggregate: the warp takes 32 consecutive list entries, which a scan warp
+    // appended in row order, so survivors of one build key (one slot) sit side by side.
+    // Each run of equal slots is folded across its lanes, and its first lane applies it
+    // with one atomic per aggregate.
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint64_t i0 = blockIdx.x * (uint64_t)kT + (threadIdx.x & ~31u); i0 < n; i0 += (uint64_t)gridDim.x * kT) {
+      const uint64_t i = i0 + lane;
+      const Hit h = i < n ? a.hits[i * a.hit_words] : kNoHit;
+      const uint32_t seg = (uint32_t)(h >> 32);
+      const uint64_t row = h & 0xffffffffull;
+      auto col = [&](uint32_t slot, int64_t j) -> int64_t {
+        if (slot >= 32) return __ldg(a.probe.payload + (uint64_t)(slot - 32) * a.probe.slot_cap + j);
+        const alk_colseg* d = a.cols + (uint64_t)slot * a.nseg + seg;
+        const void* data = (const void*)__ldg((const unsigned long long*)&d->data);
+        return load_for(data, __ldg(&d->bits), (int64_t)__ldg((const long long*)&d->lower), row);
+      };
+      int64_t j = -1;
+      if (h != kNoHit) {
+        j = ht_probe(a.probe, col((uint32_t)a.probe_slot, 0));
+        // a dense table with more keys than slots flags it in its prefix pass; no slot
+        // beyond the capacity is touched
+        if ((uint64_t)j >= a.probe.cap) j = -1;
+      }
+      const bool use = j >= 0;
+      const int64_t prev = __shfl_up_sync(0xffffffffu, j, 1);
+      const uint32_t heads = __ballot_sync(0xffffffffu, use && (lane == 0 || prev != j));
+      const uint32_t after = lane == 31 ? 0u : heads & (0xffffffffu << (lane + 1));
+      const uint32_t run_end = after ? (uint32_t)__ffs(after) - 1 : 32u;
+      const bool head = (heads >> lane) & 1u;
+      for (uint32_t g = 0; g < a.nagg; g++) {
+        const uint8_t kind = a.agg_kind[g];
+        int64_t v = kind == ALK_AGG_MIN ? INT64_MAX : kind == ALK_AGG_MAX ? INT64_MIN : 0;
+        if (use)
+          v = kind == ALK_AGG_COUNT ? 1
+                                    : vm_eval<kT>(s_ins[1 + g], s_n[1 + g], s_res[1 + g], s_consts[1 + g],
+                                                  s_regs + threadIdx.x, [&](uint32_t sl) { return col(sl, j); });
+        v = run_reduce(v, run_end, kind);
+        if (!head) continue;
+        unsigned long long* dst = (unsigned long long*)(a.acc + (uint64_t)g * a.acc_stride + j);
+        if (kind == ALK_AGG_SUM || kind == ALK_AGG_COUNT) atomicAdd(dst, (unsigned long long)v);
+        else if (kind == ALK_AGG_MIN) atomicMin((long long*)dst, (long long)v);
+        else atomicMax((long long*)dst, (long long)v);
+      }
+      if (a.cnt) {
+        const int64_t c = run_reduce(use ? 1 : 0, run_end, ALK_AGG_COUNT);
+        if (head) atomicAdd(a.cnt + j, (unsigned long long)c);
+      }
+    }
+    return;
+  }
+  // build stages: one survivor per thread
   unsigned long long inserted = 0;
   for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
     const Hit* e = a.hits + i * a.hit_words;
@@ -416,7 +480,7 @@ __global__ void __launch_bounds__(kT) k_stage_hits(const StageArgs a) {
       } else {
         if (a.probe_slot >= 0 && (a.need_slot || !a.probe.bits)) {  // as the bitmap pass did
           j = ht_probe(a.probe, col((uint32_t)a.probe_slot));
-          if (j < 0) continue;
+          if (j < 0 || (uint64_t)j >= a.probe.cap) continue;  // beyond the slots: flagged overflow
         }
         key = col((uint32_t)a.build_slot);
 #pragma unroll
@@ -435,43 +499,26 @@ __global__ void __launch_bounds__(kT) k_stage_hits(const StageArgs a) {
     }
     if (a.probe_slot >= 0 && (a.need_slot || !a.probe.bits)) {
       j = ht_probe(a.probe, col((uint32_t)a.probe_slot));
-      if (j < 0) continue;
+      // a dense table with more keys than slots flags it in its prefix pass; no slot
+      // beyond the capacity is touched
+      if (j < 0 || (uint64_t)j >= a.probe.cap) continue;
     }
-    if (kBuild) {
-      // the key and every payload value are loaded before the insert, so that one
-      // round trip covers them all
-      const int64_t key = col((uint32_t)a.build_slot);
-      int64_t pv[8];
+    // the key and every payload value are loaded before the insert, so that one round
+    // trip covers them all
+    const int64_t key = col((uint32_t)a.build_slot);
+    int64_t pv[8];
 #pragma unroll
-      for (uint32_t p = 0; p < 8; p++)
-        if (p < a.build.npay) pv[p] = col((uint32_t)a.pay_src[p]);
-      const int64_t sl = ht_insert(a.build, key);
-      if (sl < 0) continue;
-      inserted++;
+    for (uint32_t p = 0; p < 8; p++)
+      if (p < a.build.npay) pv[p] = col((uint32_t)a.pay_src[p]);
+    const int64_t sl = ht_insert(a.build, key);
+    if (sl < 0) continue;
+    inserted++;
 #pragma unroll
-      for (uint32_t p = 0; p < 8; p++)
-        if (p < a.build.npay) a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = pv[p];
-    } else {
-      for (uint32_t g = 0; g < a.nagg; g++) {
-        unsigned long long* dst = (unsigned long long*)(a.acc + (uint64_t)g * a.acc_stride + j);
-        const uint8_t kind = a.agg_kind[g];
-        if (kind == ALK_AGG_COUNT) {
-          atomicAdd(dst, 1ull);
-          continue;
-        }
-        const int64_t v =
-            vm_eval<kT>(s_ins[1 + g], s_n[1 + g], s_res[1 + g], s_consts[1 + g], s_regs + threadIdx.x, col);
-        if (kind == ALK_AGG_SUM) atomicAdd(dst, (unsigned long long)v);
-        else if (kind == ALK_AGG_MIN) atomicMin((long long*)dst, (long long)v);
-        else atomicMax((long long*)dst, (long long)v);
-      }
-      if (a.cnt) atomicAdd(a.cnt + j, 1ull);
-    }
+    for (uint32_t p = 0; p < 8; p++)
+      if (p < a.build.npay) a.build.payload[(uint64_t)p * a.build.slot_cap + sl] = pv[p];
   }
-  if (kBuild) {
-    for (int o = 16; o; o >>= 1) inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
-    if ((threadIdx.x & 31) == 0 && inserted) atomicAdd(a.build.nslots, inserted);
-  }
+  for (int o = 16; o; o >>= 1) inserted += __shfl_xor_sync(0xffffffffu, inserted, o);
+  if ((threadIdx.x & 31) == 0 && inserted) atomicAdd(a.build.nslots, inserted);
 }
 
 // Dense build from a list of survivor positions: set each survivor's key bit (a bit found
@@ -1344,13 +1391,37 @@ __device__ __forceinline__ void load8_narrow(const void* p, uint32_t bits, uint3
   }
 }
 
+// Hint to the copy engine: bring [p, p + bytes) into L2 (p 16-byte aligned, bytes a
+// multiple of 16; no register or completion is involved).
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+// The part of a column's rows [r0, r0 + nr) that starts and ends on 16-byte boundaries
+// inside the rows, prefetched into L2.
+__device__ __forceinline__ void prefetch_rows(const alk_colseg& d, uint32_t r0, uint32_t nr) {
+  const uint32_t w = d.bits / 8;
+  const uintptr_t b = (uintptr_t)d.data + (uintptr_t)r0 * w;
+  const uintptr_t e = (uintptr_t)d.data + (uintptr_t)(r0 + nr) * w;
+  const uintptr_t b16 = (b + 15) & ~(uintptr_t)15, e16 = e & ~(uintptr_t)15;
+  if (e16 > b16) prefetch_l2((const void*)b16, (uint32_t)(e16 - b16));
+}
+
+// Resident blocks of 256 threads per SM that each form of k_stage_vec is compiled for
+// (at most 65536 / (256 x blocks) registers a thread), the most that compile without
+// spills. The loop is latency-bound: with one conjunct, 8 blocks at 32 registers against
+// 6 at 40 took the 600M-row query from 2.12 to 2.09 ms; left to itself the compiler gave
+// the forms with more conjuncts 76-110 registers (2-3 blocks).
+constexpr int vec_min_blocks(int mode, int conj) {
+  return mode == 2 ? (conj <= 2 ? 4 : 3) : conj <= 1 ? 8 : conj == 2 ? 5 : 4;
+}
+
 // kMode: 0 survivors to the hit list, 1 inline dense build (records), 2 inline hash build,
 // 3 inline dense build of a table that stores no keys (bits only).
 // kConj: the predicate's conjuncts. A block's tiles advance by gridDim.x, so each thread
 // follows its segment incrementally and keeps the segment's column descriptors, conjunct
 // tests and probe plan in registers (no per-tile table lookups).
 template <int kMode, int kConj>
-__global__ void __launch_bounds__(kT) k_stage_vec(const __grid_constant__ TmaArgs t) {
+__global__ void __launch_bounds__(kT, vec_min_blocks(kMode, kConj)) k_stage_vec(const __grid_constant__ TmaArgs t) {
   const FastArgs& f = t.f;
   const StageArgs& a = f.a;
   extern __shared__ __align__(16) unsigned char s_dyn[];
@@ -1404,6 +1475,18 @@ __global__ void __launch_bounds__(kT) k_stage_vec(const __grid_constant__ TmaArg
         pbits = d.bits;
         sp = s_sp[seg];
       }
+    }
+    // the columns every row reads, for this block's next tile: into L2 while this tile
+    // is worked on, so that their loads meet L2 latency rather than DRAM's
+    if (threadIdx.x == 0 && tile + gridDim.x < a.ntiles && (kConj > 0 || probe)) {
+      const uint32_t nt = tile + gridDim.x;
+      uint32_t sg = seg;
+      while (nt >= s_tile[sg + 1]) sg++;
+      const uint32_t r0 = (nt - s_tile[sg]) * kTile;
+      const uint32_t nr = min(kTile, s_cd[sg].rows - r0);
+#pragma unroll
+      for (int c = 0; c < kConj; c++) prefetch_rows(s_cd[t.conj_st[c] * a.nseg + sg], r0, nr);
+      if (probe) prefetch_rows(s_cd[t.probe_st * a.nseg + sg], r0, nr);
     }
     const uint32_t row0 = (tile - tile0) * kTile + threadIdx.x * kVecRows;
     const uint32_t n = row0 < nrows ? min(kVecRows, nrows - row0) : 0u;
@@ -1699,7 +1782,7 @@ cudaError_t launch_stage(FastArgs fa, bool conj, bool narrow_all, const alk_cols
   a.hit_words = dense && inline_build && !a.build.dense_mode ? 2 + a.build.npay : 1;
   t.f.a.hit_words = a.hit_words;
   int occ = 0;
-  // the blocked kernel's mode: hit list, inline dense build, inline hash build
+  // the blocked kernel's mode: hit list, inline builds
   void (*vec_kernel)(const TmaArgs) = !inline_build               ? vec_kernel_for<0>(fa.nconj)
                                       : dense && a.build.dense_mode ? vec_kernel_for<3>(fa.nconj)
                                       : dense                       ? vec_kernel_for<1>(fa.nconj)
