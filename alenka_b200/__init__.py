@@ -45,7 +45,7 @@ class Stats(ctypes.Structure):
         ("card_reruns", ctypes.c_uint32),
         ("batch_host_ms", ctypes.c_double * 3),
         ("sort_groupbys", ctypes.c_uint32),
-        ("pad_", ctypes.c_uint32),
+        ("hash_groupbys", ctypes.c_uint32),
     ]
 
 

@@ -1944,6 +1944,240 @@ __global__ void __launch_bounds__(kT) k_seg_unsorted(const alk_colseg* segs, uin
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flags + g, 1u);
 }
 
+// ---- Fused filter + hash GROUP BY over resident segments (emit_select's group-by,
+// select.cu:359-952, with the filter of filter.cu:133-643 in the same pass): each row's
+// predicate, group keys and aggregate inputs are read at their stored widths, the group's
+// slot is found or claimed in an open-addressing table, and lanes of a warp that land on
+// the same slot fold their values before one atomic per aggregate.
+struct GroupTable {
+  uint64_t cap;            // power of two
+  int64_t* keys;           // [nkeys][cap]; one key: kEmptyKey marks a free slot
+  uint32_t* state;         // several keys: 0 free, 1 being written, 2 full
+  int64_t* vals;           // [nagg][cap]
+  uint32_t nkeys;
+  int32_t key_slot[4];
+  int generic;             // the predicate is not a conjunction: run it per row
+  unsigned long long* seg_rows;  // [nseg] surviving rows per segment
+  unsigned long long* groups;    // groups written by the compaction
+  int64_t* const* out_keys;      // [nkeys] compacted keys (device array of addresses)
+  int64_t* const* out_vals;      // [nagg]
+  uint64_t out_cap;
+};
+
+// One conjunct on one stored value x (value = x + lower).
+__device__ __forceinline__ bool conj_pass(const Conj& cj, const ConjSeg& cs, int64_t lower, uint64_t x) {
+  switch (cs.mode) {
+    case kCjAlways: return true;
+    case kCjNever: return false;
+    case kCjIn: return x - cs.lo <= cs.span;
+    case kCjOut: return x - cs.lo > cs.span;
+    default: {
+      const int64_t v = wrap_mul((int64_t)(x + (uint64_t)lower), cj.mul);
+      switch (cj.op) {
+        case ALK_OP_LT: return v < cj.k;
+        case ALK_OP_GT: return v > cj.k;
+        case ALK_OP_LE: return v <= cj.k;
+        case ALK_OP_GE: return v >= cj.k;
+        case ALK_OP_EQ: return v == cj.k;
+        default: return v != cj.k;
+      }
+    }
+  }
+}
+
+// Slot of a one-column group key: found, or claimed with one compare-and-swap on the key
+// word. -1 when the table is full or the key is the free-slot marker (err set).
+__device__ __forceinline__ int64_t group_slot1(const GroupTable& g, int64_t key, int* err) {
+  if (key == kEmptyKey) {
+    atomicExch(err, ALK_ERR_UNSUPPORTED);
+    return -1;
+  }
+  const uint64_t mask = g.cap - 1;
+  uint64_t p = murmur_u64((uint64_t)key) & mask;
+  for (uint64_t n = 0; n <= mask; n++) {
+    const int64_t v = __ldcg(g.keys + p);  // keys only go from free to set
+    if (v == key) return (int64_t)p;
+    if (v == kEmptyKey) {
+      const int64_t old = (int64_t)atomicCAS((unsigned long long*)(g.keys + p), (unsigned long long)kEmptyKey,
+                                             (unsigned long long)key);
+      if (old == kEmptyKey || old == key) return (int64_t)p;
+    }
+    p = (p + 1) & mask;
+  }
+  atomicCAS(err, 0, ALK_ERR_OVERFLOW);
+  return -1;
+}
+
+// Slot of a multi-column group key: a slot's state goes 0 -> 1 (claimed) -> 2 (keys
+// written); a reader that meets 1 waits, with a bound.
+__device__ __forceinline__ int64_t group_slot(const GroupTable& g, const int64_t (&key)[4], int* err) {
+  const uint64_t mask = g.cap - 1;
+  uint64_t h = kSeed ^ ((uint64_t)(8 * g.nkeys) * kMurmurM);
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    if (j < (int)g.nkeys) h = mm_block(h, (uint64_t)key[j]);
+  uint64_t p = mm_final(h) & mask;
+  uint32_t spins = 0;
+  for (uint64_t n = 0; n <= mask;) {
+    const uint32_t st = *((volatile uint32_t*)g.state + p);
+    if (st == 0) {
+      if (atomicCAS(g.state + p, 0u, 1u) == 0u) {
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (j < (int)g.nkeys) g.keys[j * g.cap + p] = key[j];
+        __threadfence();
+        atomicExch(g.state + p, 2u);
+        return (int64_t)p;
+      }
+      continue;  // claimed meanwhile: look again
+    }
+    if (st == 1) {
+      if (++spins > kSpinLimit) {
+        atomicExch(err, ALK_ERR_TIMEOUT);
+        return -1;
+      }
+      continue;
+    }
+    __threadfence();
+    bool eq = true;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+      if (j < (int)g.nkeys && __ldcg(g.keys + j * g.cap + p) != key[j]) eq = false;
+    if (eq) return (int64_t)p;
+    p = (p + 1) & mask;
+    n++;
+  }
+  atomicCAS(err, 0, ALK_ERR_OVERFLOW);
+  return -1;
+}
+
+// Position of the n-th (from 0) set bit of m; 32 when m has fewer.
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t m, uint32_t n) {
+  for (uint32_t i = 0; i < n && m; i++) m &= m - 1;
+  return m ? (uint32_t)__ffs(m) - 1 : 32u;
+}
+
+// Reduction of v over the lanes of `peers` (this lane's group, from __match_any_sync),
+// delivered to the group's lowest lane: a tree over the group's ranks. Warp-wide.
+__device__ __forceinline__ int64_t peer_reduce(int64_t v, uint32_t peers, uint8_t kind) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t rank = __popc(peers & ((1u << lane) - 1u)), cnt = __popc(peers);
+  for (uint32_t s = 1; s < 32; s <<= 1) {
+    if (!__any_sync(0xffffffffu, cnt > s)) break;
+    const bool take = (rank & (2 * s - 1)) == 0 && rank + s < cnt;
+    const uint32_t src = take ? nth_set_bit(peers, rank + s) : lane;
+    const int64_t o = __shfl_sync(0xffffffffu, v, src);
+    if (take) v = kind == ALK_AGG_MIN ? min(v, o) : kind == ALK_AGG_MAX ? max(v, o) : v + o;
+  }
+  return v;
+}
+
+template <bool kOneKey>
+__global__ void __launch_bounds__(kT, 6) k_group_scan(const __grid_constant__ FastArgs f,
+                                                   const __grid_constant__ GroupTable g) {
+  const StageArgs& a = f.a;
+  __shared__ alk_instr s_ins[8][ALK_MAX_INSTR];
+  __shared__ int64_t s_consts[8][ALK_MAX_CONST];
+  __shared__ uint32_t s_n[8], s_res[8];
+  __shared__ uint8_t s_kind[8];
+  __shared__ int64_t s_regs[ALK_MAX_REGS * kT];
+  for (uint32_t p = 0; p < a.nprogs; p++) {
+    for (uint32_t i = threadIdx.x; i < a.progs[p].n_instr; i += kT) s_ins[p][i] = a.progs[p].ins[i];
+    for (uint32_t i = threadIdx.x; i < ALK_MAX_CONST; i += kT) s_consts[p][i] = a.progs[p].consts[i];
+    if (threadIdx.x == 0) {
+      s_n[p] = a.progs[p].n_instr;
+      s_res[p] = a.progs[p].result;
+      s_kind[p] = p ? a.agg_kind[p - 1] : 0;
+    }
+  }
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31;
+  unsigned long long rows_seen = 0;
+  for (uint32_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    const uint32_t seg = tile_segment(a.seg_tile, a.nseg, tile);
+    const uint32_t rows = a.cols[seg].rows;
+    const uint32_t row0 = (tile - a.seg_tile[seg]) * kTile;
+    const bool test = a.seg_mode[seg] == 2;
+    unsigned long long kept = 0;
+    for (int k = 0; k < kItems; k++) {
+      // rows strided by the block: a warp's lanes read consecutive rows
+      const uint32_t r = row0 + k * kT + threadIdx.x;
+      bool live = r < rows;
+      rows_seen += live;
+      auto col = [&](uint32_t sl) -> int64_t {
+        const alk_colseg* d = a.cols + (uint64_t)sl * a.nseg + seg;
+        const void* data = (const void*)__ldg((const unsigned long long*)&d->data);
+        return load_for(data, __ldg(&d->bits), (int64_t)__ldg((const long long*)&d->lower), r);
+      };
+      if (live && test) {
+        if (g.generic) {
+          live = vm_eval<kT>(s_ins[0], s_n[0], s_res[0], s_consts[0], s_regs + threadIdx.x, col) != 0;
+        } else {
+          for (uint32_t c = 0; c < f.nconj && live; c++) {
+            const Conj& cj = f.conj[c];
+            const int64_t lower = (int64_t)__ldg((const long long*)&a.cols[(uint64_t)cj.slot * a.nseg + seg].lower);
+            live = conj_pass(cj, f.cseg[c * a.nseg + seg], lower, (uint64_t)(col(cj.slot) - lower));
+          }
+        }
+      }
+      kept += __popc(__ballot_sync(0xffffffffu, live));
+      int64_t slot = -1;
+      if (live) {
+        if (kOneKey) {
+          slot = group_slot1(g, col((uint32_t)g.key_slot[0]), a.err);
+        } else {
+          int64_t key[4] = {0, 0, 0, 0};
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (j < (int)g.nkeys) key[j] = col((uint32_t)g.key_slot[j]);
+          slot = group_slot(g, key, a.err);
+        }
+      }
+      const bool use = slot >= 0;
+      // lanes on the same slot: fold their values, then the group's lowest lane applies them
+      const uint32_t peers = __match_any_sync(0xffffffffu, use ? (unsigned long long)slot : ~0ull);
+      const bool share = __any_sync(0xffffffffu, use && __popc(peers) > 1);
+      const bool leader = use && (uint32_t)(__ffs(peers) - 1) == lane;
+      for (uint32_t v = 0; v < a.nagg; v++) {
+        const uint8_t kind = s_kind[1 + v];
+        int64_t x = kind == ALK_AGG_MIN ? INT64_MAX : kind == ALK_AGG_MAX ? INT64_MIN : 0;
+        if (use)
+          x = kind == ALK_AGG_COUNT
+                  ? 1
+                  : vm_eval<kT>(s_ins[1 + v], s_n[1 + v], s_res[1 + v], s_consts[1 + v], s_regs + threadIdx.x, col);
+        if (share) x = peer_reduce(x, peers, kind);
+        if (!leader) continue;
+        unsigned long long* dst = (unsigned long long*)(g.vals + (uint64_t)v * g.cap + slot);
+        if (kind == ALK_AGG_SUM || kind == ALK_AGG_COUNT) atomicAdd(dst, (unsigned long long)x);
+        else if (kind == ALK_AGG_MIN) atomicMin((long long*)dst, (long long)x);
+        else atomicMax((long long*)dst, (long long)x);
+      }
+    }
+    if (lane == 0 && kept) atomicAdd(g.seg_rows + seg, kept);
+  }
+  for (int o = 16; o; o >>= 1) rows_seen += __shfl_xor_sync(0xffffffffu, rows_seen, o);
+  if (lane == 0 && rows_seen) atomicAdd(a.rows_in, rows_seen);
+}
+
+// Occupied slots to the output columns (in slot order within a warp, warps in any order).
+__global__ void __launch_bounds__(kT) k_group_compact(const GroupTable g, uint32_t nagg) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (uint64_t h0 = blockIdx.x * (uint64_t)kT + (threadIdx.x & ~31u); h0 < g.cap; h0 += (uint64_t)gridDim.x * kT) {
+    const uint64_t h = h0 + lane;
+    const bool full = h < g.cap && (g.state ? g.state[h] == 2 : g.keys[h] != kEmptyKey);
+    const uint32_t m = __ballot_sync(0xffffffffu, full);
+    if (!m) continue;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(g.groups, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (!full) continue;
+    const uint64_t pos = base + __popc(m & ((1u << lane) - 1u));
+    if (pos >= g.out_cap) continue;  // counted: the caller sees the total and sizes again
+    for (uint32_t j = 0; j < g.nkeys; j++) g.out_keys[j][pos] = g.keys[(uint64_t)j * g.cap + h];
+    for (uint32_t v = 0; v < nagg; v++) g.out_vals[v][pos] = g.vals[(uint64_t)v * g.cap + h];
+  }
+}
+
 bool prog_ok(const alk_program& p, uint32_t ncols, uint32_t npay) {
   if (p.n_instr > ALK_MAX_INSTR || p.result >= ALK_MAX_REGS) return false;
   for (uint32_t i = 0; i < p.n_instr; i++) {
@@ -2569,6 +2803,116 @@ int alk_seg_sorted(const alk_colseg* segs, uint32_t nseg, uint8_t* h_sorted, alk
   CK(cudaStreamSynchronize(s));
   for (uint32_t g = 0; g < nseg; g++) h_sorted[g] = f[g] ? 0 : 1;
   return ALK_OK;
+}
+
+int alk_pipeline_groupby(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
+                         const alk_program* pred, const int32_t* key_slots, uint32_t nkeys,
+                         const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg, uint64_t max_groups,
+                         int64_t* const* d_out_keys, int64_t* const* d_out_vals, uint64_t out_cap,
+                         uint64_t* h_groups, uint64_t* h_seg_rows, uint64_t* h_rows_in, alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!h_groups || ncols == 0 || ncols > kMaxCols || nkeys == 0 || nkeys > 4 || nagg > 7 || !key_slots ||
+      (nagg && (!agg_kind || !d_out_vals)) || !d_out_keys)
+    return ALK_ERR_ARG;
+  *h_groups = 0;
+  for (uint32_t j = 0; j < nkeys; j++)
+    if (key_slots[j] < 0 || (uint32_t)key_slots[j] >= ncols || !d_out_keys[j]) return ALK_ERR_ARG;
+  std::vector<alk_program> progs(1 + nagg);
+  std::memset(progs.data(), 0, sizeof(alk_program) * progs.size());
+  if (pred) progs[0] = *pred;
+  for (uint32_t v = 0; v < nagg; v++) {
+    if (agg_kind[v] > ALK_AGG_MAX || !d_out_vals[v]) return ALK_ERR_ARG;
+    if (agg_kind[v] != ALK_AGG_COUNT) progs[1 + v] = agg_progs[v];
+  }
+  for (auto& p : progs)
+    if (!prog_ok(p, ncols, 0)) return ALK_ERR_ARG;  // scan columns only
+  StageArgs a{};
+  std::vector<uint8_t> hb;
+  size_t off_x;
+  int rc = stage_common(cols, ncols, nseg, seg_mode, progs.data(), (uint32_t)progs.size(), hb, a,
+                        16 + 8 * (size_t)(nkeys + nagg), &off_x);
+  if (rc) return rc;
+  std::memcpy(&hb[off_x], agg_kind, nagg);
+  const size_t off_outp = off_x + 16;
+  std::memcpy(&hb[off_outp], d_out_keys, 8 * (size_t)nkeys);
+  if (nagg) std::memcpy(&hb[off_outp + 8 * (size_t)nkeys], d_out_vals, 8 * (size_t)nagg);
+  FastArgs fa{};
+  const bool conj = as_conjuncts(progs[0], fa.conj, &fa.nconj);
+  std::vector<ConjSeg> cs;
+  if (conj)
+    for (uint32_t c = 0; c < fa.nconj; c++)
+      for (uint32_t g = 0; g < nseg; g++)
+        cs.push_back(seg_mode[g] == 1 ? ConjSeg{0, 0, kCjAlways, 0} : conj_seg(fa.conj[c], cols[fa.conj[c].slot * nseg + g]));
+  // table: at most 0.7 full at max_groups
+  uint64_t cap = 1024;
+  while ((long double)cap * 0.7L < (long double)std::max<uint64_t>(max_groups, 1)) cap <<= 1;
+  const bool one = nkeys == 1;
+  const size_t off_cs = (hb.size() + 15) & ~size_t(15);
+  const size_t off_ctr = (off_cs + cs.size() * sizeof(ConjSeg) + 255) & ~size_t(255);
+  const size_t ctr_bytes = 32 + 8 * (size_t)nseg;  // rows_in, groups, err, pad, seg_rows
+  const size_t off_keys = (off_ctr + ctr_bytes + 255) & ~size_t(255);
+  const size_t off_vals = off_keys + 8 * (size_t)nkeys * cap;
+  const size_t off_state = off_vals + 8 * (size_t)nagg * cap;
+  const size_t total = off_state + (one ? 0 : 4 * (size_t)cap);
+  uint8_t* db = nullptr;
+  CK(cudaMallocAsync((void**)&db, total, s));
+  std::vector<uint8_t> up(off_ctr, 0);
+  std::memcpy(up.data(), hb.data(), hb.size());
+  if (!cs.empty()) std::memcpy(up.data() + off_cs, cs.data(), cs.size() * sizeof(ConjSeg));
+  cudaError_t ue;
+  const void* src = alk::upload_source(up.data(), up.size(), s, &ue);
+  CK(ue);
+  CK(cudaMemcpyAsync(db, src, up.size(), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(db + off_ctr, 0, ctr_bytes, s));
+  if (one) CK(cudaMemsetAsync(db + off_keys, 0x80, 8 * cap, s));  // every key word = kEmptyKey
+  else CK(cudaMemsetAsync(db + off_state, 0, 4 * cap, s));
+  for (uint32_t v = 0; v < nagg; v++) {
+    const int64_t init = agg_kind[v] == ALK_AGG_MIN ? INT64_MAX : agg_kind[v] == ALK_AGG_MAX ? INT64_MIN : 0;
+    k_fill_i64<<<grid_for(cap), kT, 0, s>>>((int64_t*)(db + off_vals) + (uint64_t)v * cap, cap, init);
+    alk::g_kernel_launches++;
+  }
+  patch(a, db);
+  a.agg_kind = db + off_x;
+  a.nagg = nagg;
+  a.rows_in = (unsigned long long*)(db + off_ctr);
+  a.err = (int*)(db + off_ctr + 16);
+  fa.a = a;
+  fa.cseg = (const ConjSeg*)(db + off_cs);
+  GroupTable g{};
+  g.cap = cap;
+  g.keys = (int64_t*)(db + off_keys);
+  g.vals = (int64_t*)(db + off_vals);
+  g.state = one ? nullptr : (uint32_t*)(db + off_state);
+  g.nkeys = nkeys;
+  for (uint32_t j = 0; j < nkeys; j++) g.key_slot[j] = key_slots[j];
+  g.generic = progs[0].n_instr && !conj;
+  g.seg_rows = (unsigned long long*)(db + off_ctr + 32);
+  g.groups = (unsigned long long*)(db + off_ctr + 8);
+  g.out_keys = (int64_t* const*)(db + off_outp);
+  g.out_vals = (int64_t* const*)(db + off_outp + 8 * (size_t)nkeys);
+  g.out_cap = out_cap;
+  if (a.ntiles) {
+    void (*kern)(const FastArgs, const GroupTable) = one ? k_group_scan<true> : k_group_scan<false>;
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kT, 0);
+    const int grid = std::min<int>((int)a.ntiles, sms() * std::max(occ, 1));
+    kern<<<grid, kT, 0, s>>>(fa, g);
+    alk::g_kernel_launches++;
+  }
+  k_group_compact<<<grid_for(cap), kT, 0, s>>>(g, nagg);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  std::vector<unsigned long long> back(4 + nseg);
+  CK(cudaMemcpyAsync(back.data(), db + off_ctr, ctr_bytes, cudaMemcpyDeviceToHost, s));
+  CK(cudaFreeAsync(db, s));
+  CK(cudaStreamSynchronize(s));
+  *h_groups = back[1];
+  if (h_rows_in) *h_rows_in = back[0];
+  if (h_seg_rows)
+    for (uint32_t g2 = 0; g2 < nseg; g2++) h_seg_rows[g2] = back[4 + g2];
+  const int err = (int)(uint32_t)back[2];
+  if (err) return err;
+  return back[1] > out_cap ? ALK_ERR_OVERFLOW : ALK_OK;
 }
 
 int alk_live_compact(const uint64_t* d_live, uint64_t n, uint32_t* d_out, uint64_t* h_count, alk_stream stream) {

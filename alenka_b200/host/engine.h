@@ -268,6 +268,7 @@ class Engine {
   // domains, conjunctive filter, affine-product aggregates): false when the SELECT has
   // another form. Batches run many prepared selects in one launch.
   bool dense_select_prepare(Statement& st, SelectCtx& c);
+  bool hash_select(Statement& st);  // the fused filter + hash GROUP BY
   void dense_select_run(const std::vector<SelectCtx*>& cs);
   void dense_select_finish(SelectCtx& c);
   void emit_join(Statement& st);

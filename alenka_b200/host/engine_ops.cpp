@@ -434,6 +434,7 @@ void Engine::emit_select(Statement& st) {
       return;
     }
   }
+  if (hash_select(st)) return;
   Var* a = var(st.f);
   const int grp_cnt = st.grp_cnt;
   std::vector<std::string> group_cols(st.op_value.end() - grp_cnt, st.op_value.end());
@@ -2198,6 +2199,151 @@ bool Engine::try_fused(std::vector<Statement>& sts, size_t& i) {
   big_fetch_ = false;
   stats_.plan = std::max<uint32_t>(stats_.plan, 1);
   i += 3;
+  return true;
+}
+
+// GROUP BY over a base table or a FILTER of one, with group keys and aggregate inputs
+// among its columns: the filter and the hash aggregation run as one pass over the resident
+// segments (alk_pipeline_groupby), reading every column at its stored width; the groups
+// then take the output path of the materialized forms (select_output: key order for one
+// segment, MurmurHash64A order of the key tuple across segments). The sort-based form
+// keeps the selects whose rows are already in key order (its sort is then skipped), and
+// the ones the session pins to it.
+bool Engine::hash_select(Statement& st) {
+  if ((flags_ & ALK_SESSION_PLAIN) || st.grp_cnt < 1 || st.grp_cnt > 4 || groupby_mode_ == 2) return false;
+  Var* a = vars_.count(st.f) ? var(st.f) : nullptr;
+  if (!a || (a->kind != Var::Filtered && a->kind != Var::Base)) return false;
+  Var* src = a->kind == Var::Filtered ? var(a->source) : a;
+  if (src->kind != Var::Base) return false;
+  std::vector<std::string> group_cols(st.op_value.end() - st.grp_cnt, st.op_value.end());
+  for (auto& g : group_cols)
+    if (!a->has(g) || !src->has(g) || a->meta[g].type > 2) return false;
+  std::vector<OutSpec> outs;
+  std::vector<AggSpec> aggs;
+  bool one_line = false;
+  compile_select(st, a, true, outs, aggs, one_line);
+  for (auto& o : outs) {
+    if (o.col_type == 1 && std::find(group_cols.begin(), group_cols.end(), o.field) == group_cols.end()) return false;
+    if (o.col_type == 2 && has_col(o.vec)) return false;
+  }
+  if (aggs.size() > 7) return false;
+  const uint32_t skipped = stats_.segments_skipped;
+  const uint64_t rows_before = stats_.rows_scanned;
+  ScanPlan p = plan_scan(a);
+  auto fail = [&]() {
+    stats_.segments_skipped = skipped;  // the materialized plan scans again
+    stats_.rows_scanned = rows_before;
+    return false;
+  };
+  std::vector<int32_t> key_slots;
+  for (auto& g : group_cols) key_slots.push_back((int32_t)p.slot(g));
+  std::vector<alk_program> progs(aggs.size());
+  std::vector<uint8_t> kinds(aggs.size());
+  for (size_t k = 0; k < aggs.size(); k++) {
+    kinds[k] = aggs[k].kind;
+    std::memset(&progs[k], 0, sizeof(alk_program));
+    if (aggs[k].kind == ALK_AGG_COUNT) continue;
+    Compiler c;
+    progs[k] = c.finish(aggs[k].input);
+    std::map<std::string, uint32_t> where;
+    for (auto& n : c.slots) {
+      if (!src->has(n) || src->meta[n].type > 2) return fail();
+      where[n] = p.slot(n);
+    }
+    remap(progs[k], c.slots, where);
+  }
+  for (auto& n : p.slots)
+    if (src->meta[n].type > 2) return fail();
+  auto cs = colsegs(p);
+  uint64_t rows = 0;
+  for (uint32_t g = 0; g < src->segCount; g++)
+    if (p.mode[g]) rows += cs[g].rows;
+  uint64_t groups = expected_groups(a, group_cols, std::max<uint64_t>(rows, 1));
+  if (groupby_mode_ == 0 && groups > kHashGroupsMax && group_cols.size() == 1) {
+    // rows in key order across the scanned segments: the sort-based form skips its sort
+    BaseCol& kb = basecol(src, group_cols[0]);
+    const uint32_t ks = (uint32_t)key_slots[0];
+    std::vector<alk_colseg> kcs(cs.begin() + (size_t)ks * src->segCount, cs.begin() + (size_t)(ks + 1) * src->segCount);
+    bool ordered = segs_ascending(kb, kcs, p.mode, true);
+    int64_t prev_hi = INT64_MIN;
+    for (uint32_t g = 0; ordered && g < src->segCount; g++) {
+      if (!p.mode[g]) continue;
+      if (kb.segs[g].m.comp_type != 0 || kb.segs[g].m.lower < prev_hi) ordered = false;
+      prev_hi = kb.segs[g].m.upper;
+    }
+    if (ordered) return fail();
+  }
+  const size_t cycles = cycle_count(a);
+  GroupOut G;
+  std::vector<int64_t*> okeys, ovals;
+  std::vector<uint64_t> seg_rows(src->segCount, 0);
+  uint64_t ng = 0;
+  for (int attempt = 0;; attempt++) {
+    const uint64_t out_cap = std::max<uint64_t>(groups, 1);
+    G.keys.clear();
+    G.vals.clear();
+    okeys.clear();
+    ovals.clear();
+    for (size_t j = 0; j < group_cols.size(); j++) {
+      G.keys.push_back(mkbuf(out_cap * 8, stream_));
+      okeys.push_back(G.keys.back()->as<int64_t>());
+    }
+    for (size_t k = 0; k < aggs.size(); k++) {
+      G.vals.push_back(mkbuf(out_cap * 8, stream_));
+      ovals.push_back(G.vals.back()->as<int64_t>());
+    }
+    if (timing_) cudaEventRecord(ev0_, stream_);
+    const int rc = alk_pipeline_groupby(cs.data(), (uint32_t)p.slots.size(), src->segCount, p.mode.data(),
+                                        p.has_pred ? &p.pred : nullptr, key_slots.data(),
+                                        (uint32_t)key_slots.size(), progs.data(), kinds.data(),
+                                        (uint32_t)aggs.size(), groups, okeys.data(), ovals.data(), out_cap, &ng,
+                                        seg_rows.data(), nullptr, (alk_stream)stream_);
+    if (timing_) {
+      cudaEventRecord(ev1_, stream_);
+      cudaEventSynchronize(ev1_);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ev0_, ev1_);
+      stats_.hot_kernel_ms += ms;
+      stats_.hot_kernel_launches += 1;
+      stats_.hot_kernel_bytes += scan_bytes(p, std::vector<uint32_t>());
+    }
+    if (rc == ALK_ERR_OVERFLOW && attempt < 3) {
+      // more groups than the estimate: size for the count the run reported (or for every
+      // row when the table itself filled up)
+      groups = std::min<uint64_t>(std::max<uint64_t>(rows, 1), std::max(ng > out_cap ? ng : out_cap * 4, groups));
+      continue;
+    }
+    if (rc == ALK_ERR_UNSUPPORTED) return fail();  // a key equal to the free-slot marker
+    check(rc, "hash group-by");
+    break;
+  }
+  stats_.hash_groupbys++;
+  auto out = std::make_unique<Var>();
+  out->kind = Var::Mat;
+  out->name = st.s;
+  uint64_t kept = 0;
+  for (auto n : seg_rows) kept += n;
+  if (kept == 0) {
+    vars_[st.s] = std::move(out);  // no segment produced rows: empty result without columns
+    return true;
+  }
+  // the reference leaves the select-list order reversed when its first segment is empty
+  if (seg_rows[0] == 0) std::reverse(outs.begin(), outs.end());
+  G.g = ng;
+  G.first = mkbuf(std::max<uint64_t>(ng, 1) * 4, stream_);  // no column reads a group's first row
+  ck(cudaMemsetAsync(G.first->as<void>(), 0, std::max<uint64_t>(ng, 1) * 4, stream_), "memset");
+  SelectCtx c;
+  c.st = &st;
+  c.a = a;
+  c.grp_cnt = st.grp_cnt;
+  c.group_cols = group_cols;
+  c.outs = std::move(outs);
+  c.cycles = cycles;
+  c.G = std::move(G);
+  c.okeys = okeys;
+  c.R = nullptr;
+  c.out = std::move(out);
+  select_output(c);
   return true;
 }
 

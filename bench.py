@@ -476,10 +476,12 @@ def run_batched(args, torch):
 
 
 def run_groupby_high(args, torch):
-    """The high-cardinality group-by: FILTER lineitem BY l_shipdate < d; GROUP BY
-    l_orderkey over a lineitem-shaped table generated in device memory (600M rows, 4 rows
-    per key), timed in its hash form and its sort-based form (in key order: no sort), and
-    in the form the engine picks from the expected group count."""
+    """High-cardinality group-by over a lineitem-shaped table generated in device memory
+    (600M rows): FILTER lineitem BY l_shipdate < d, then GROUP BY l_orderkey (rows in key
+    order, 4 rows per key, ~150M keys) and GROUP BY l_extendedprice, l_discount (unsorted,
+    ~95M groups). Each is timed in its fused hash form (filter and hashing in one pass),
+    its sort-based form (the sort runs for the unsorted keys and is skipped for the
+    ordered ones), and the form the engine picks."""
     import alenka_b200 as ab
     from alenka_b200 import workloads as wl
     rows = int(600_000_000 * args.scale)
@@ -489,27 +491,43 @@ def run_groupby_high(args, torch):
     sess = ab.Session(d, resident=True)
     sess.gen_flat_resident("lineitem", segs, args.seed)
     cut = wl.flat_cutoff(args.seed)
-    script = (f"LF := FILTER lineitem BY l_shipdate < {cut};\n"
-              "R := SELECT l_orderkey AS k, SUM(l_quantity) AS q, SUM(l_extendedprice*(1-l_discount)) AS rev, "
-              "COUNT(l_orderkey) AS c FROM LF GROUP BY l_orderkey;\n"
-              "STORE R INTO 'gbh.txt' USING ('|');\n")
+    scripts = {
+        "key_order": (f"LF := FILTER lineitem BY l_shipdate < {cut};\n"
+                      "R := SELECT l_orderkey AS k, SUM(l_quantity) AS q, SUM(l_extendedprice*(1-l_discount)) AS rev, "
+                      "COUNT(l_orderkey) AS c FROM LF GROUP BY l_orderkey;\n"
+                      "STORE R INTO 'gbh.txt' USING ('|');\n"),
+        "unsorted": (f"LF := FILTER lineitem BY l_shipdate < {cut};\n"
+                     "R := SELECT l_extendedprice AS p, l_discount AS d, SUM(l_quantity) AS q, "
+                     "COUNT(l_orderkey) AS c FROM LF GROUP BY l_extendedprice, l_discount;\n"
+                     "STORE R INTO 'gbu.txt' USING ('|');\n"),
+    }
     out = {}
-    for name, mode in (("auto", 0), ("hash", 1), ("sort", 2)):
-        sess.set_groupby(mode)
-        for _ in range(max(1, args.warmup // 2)):
+    steps = max(1, args.steps // 8)
+    for sname, script in scripts.items():
+        outs = {}
+        for name, mode in (("auto", 0), ("hash", 1), ("sort", 2)):
+            sess.set_groupby(mode)
             sess.execute(script)
-        sess.set_timing(True)
-        ms, acc = _steps(sess, lambda: sess.execute(script), max(1, args.steps // 4), torch)
-        sess.set_timing(False)
-        gb_ms = acc["hot_ms"] / max(1, acc["hot_launches"])
-        out[name] = {"ms_per_query": ms, "rows_per_s": rows / (ms / 1000.0), "groupby_ms": gb_ms,
-                     "groupby_rows_per_s": rows / (gb_ms / 1000.0) if gb_ms else None,
-                     "sort_form": bool(sess.stats().sort_groupbys)}
+            sess.set_timing(True)
+            ms, acc = _steps(sess, lambda: sess.execute(script), steps, torch)
+            sess.set_timing(False)
+            gb_ms = acc["hot_ms"] / max(1, acc["hot_launches"])
+            st = sess.stats()
+            outs[name] = {"ms_per_query": ms, "rows_per_s": rows / (ms / 1000.0), "groupby_ms": gb_ms,
+                          "groupby_rows_per_s": rows / (gb_ms / 1000.0) if gb_ms else None,
+                          "form": "sort" if st.sort_groupbys else ("fused hash" if st.hash_groupbys else "other")}
+        out[sname] = outs
+        with open(os.path.join(d, "gbh.txt" if sname == "key_order" else "gbu.txt"), "rb") as f:
+            f.seek(0, 2)
+            outs["stored_bytes"] = f.tell()
     sess.close()
-    print(json.dumps({"metric": "fact rows/s, filter + GROUP BY l_orderkey (high cardinality)",
-                      "value": out["auto"]["rows_per_s"], "unit": "rows/s", "n_gpus": 1, "dtype": "int64",
+    best = min(out["unsorted"]["hash"]["groupby_ms"], out["unsorted"]["sort"]["groupby_ms"])
+    print(json.dumps({"metric": "fact rows/s, filter + GROUP BY (high cardinality), group-by device time",
+                      "value": rows / (best / 1000.0), "unit": "rows/s", "n_gpus": 1, "dtype": "int64",
                       "data": "synthetic (generated in device memory)",
-                      "config": {"workload": f"lineitem {rows} rows, {len(segs)} segments, ~{rows // 4} keys",
+                      "config": {"workload": f"lineitem {rows} rows, {len(segs)} segments; GROUP BY l_orderkey "
+                                             f"(~{rows // 4} keys, key order) and GROUP BY l_extendedprice, "
+                                             "l_discount (unsorted)",
                                  "forms": out}}), flush=True)
 
 

@@ -114,7 +114,50 @@ def test_engine_high_cardinality_groupby(flat, mode):
         s.execute(HIGH)
         st = s.stats()
         assert st.sort_groupbys == (1 if mode == 2 else 0)
+        assert st.hash_groupbys == (0 if mode == 2 else 1)  # the filter and the hashing in one pass
     assert open(os.path.join(flat, "hs.txt"), "rb").read() == want
+
+
+FUSED = {
+    # two unsorted key columns (the multi-column table), MAX and an expression input
+    "two_keys": "LF := FILTER lineitem BY l_shipdate < 19960101 AND l_quantity > 10;\n"
+                "R := SELECT l_extendedprice AS p, l_discount AS d, SUM(l_quantity) AS q, MAX(l_shipdate) AS mx, "
+                "COUNT(l_orderkey) AS c FROM LF GROUP BY l_extendedprice, l_discount;\n"
+                "STORE R INTO 'fz.txt' USING ('|');\n",
+    # a predicate that is not a conjunction runs per row
+    "or_pred": "LF := FILTER lineitem BY l_shipdate < 19930101 OR l_quantity == 7;\n"
+               "R := SELECT l_orderkey AS k, SUM(l_extendedprice*(1-l_discount)) AS rev, MIN(l_quantity) AS mn, "
+               "COUNT(l_orderkey) AS c FROM LF GROUP BY l_orderkey;\n"
+               "STORE R INTO 'fz.txt' USING ('|');\n",
+    # the base table itself, no filter; char-coded keys
+    "base_char": "R := SELECT l_returnflag AS f, l_linestatus AS s, l_quantity AS q, SUM(l_extendedprice) AS p, "
+                 "COUNT(l_orderkey) AS c FROM lineitem GROUP BY l_returnflag, l_linestatus, l_quantity;\n"
+                 "STORE R INTO 'fz.txt' USING ('|');\n",
+    # zone maps skip the first segment: the reference then reverses the select list
+    "first_empty": "LF := FILTER lineitem BY l_orderkey > 30000;\n"
+                   "R := SELECT l_orderkey AS k, SUM(l_quantity) AS q, COUNT(l_orderkey) AS c FROM LF "
+                   "GROUP BY l_orderkey;\nSTORE R INTO 'fz.txt' USING ('|');\n",
+    # nothing survives
+    "empty": "LF := FILTER lineitem BY l_quantity > 60;\n"
+             "R := SELECT l_orderkey AS k, SUM(l_quantity) AS q, COUNT(l_orderkey) AS c FROM LF "
+             "GROUP BY l_orderkey;\nSTORE R INTO 'fz.txt' USING ('|');\n",
+}
+
+
+@pytest.mark.parametrize("name", sorted(FUSED))
+def test_fused_hash_groupby_matches_oracle(flat, name):
+    """The fused filter + hash GROUP BY (alk_pipeline_groupby) through the engine, byte
+    for byte against the oracle: several key columns, predicates that are and are not
+    conjunctions, no filter, a skipped first segment, and an empty result."""
+    from . import _oracle
+    script = FUSED[name]
+    _oracle.execute(flat, script.replace("fz.txt", "oracle_fz.txt"))
+    with ab.Session(flat) as s:
+        s.set_groupby(1)
+        s.execute(script)
+        # with every segment skipped the key range is empty, and the dense form takes it
+        assert s.stats().hash_groupbys == (0 if name == "empty" else 1)
+    assert open(os.path.join(flat, "fz.txt"), "rb").read() == open(os.path.join(flat, "oracle_fz.txt"), "rb").read()
 
 
 def test_engine_sort_form_small_keys(flat):
