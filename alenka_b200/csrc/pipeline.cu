@@ -1950,10 +1950,17 @@ __global__ void __launch_bounds__(kT) k_seg_unsorted(const alk_colseg* segs, uin
 // slot is found or claimed in an open-addressing table, and lanes of a warp that land on
 // the same slot fold their values before one atomic per aggregate.
 struct GroupTable {
-  uint64_t cap;            // power of two
-  int64_t* keys;           // [nkeys][cap]; one key: kEmptyKey marks a free slot
+  uint64_t cap;            // power of two (hash forms); the key space's size (direct form)
+  // One record of rw words per slot: the key columns (hash forms; one key: kEmptyKey
+  // marks a free slot), then the accumulators. A group's key and accumulators share a
+  // record, so its random updates touch one 32-byte sector when rw <= 4.
+  int64_t* rec;
+  uint32_t rw, kw;         // words per record; key words in front (0 in the direct form)
   uint32_t* state;         // several keys: 0 free, 1 being written, 2 full
-  int64_t* vals;           // [nagg][cap]
+  // direct form: slot = sum over j of (key_j - kmin_j) * kstride_j, a slot's presence a bit
+  int64_t kmin[4];
+  uint64_t kspan[4], kstride[4];
+  uint32_t* occ;
   uint32_t nkeys;
   int32_t key_slot[4];
   int generic;             // the predicate is not a conjunction: run it per row
@@ -1995,10 +2002,10 @@ __device__ __forceinline__ int64_t group_slot1(const GroupTable& g, int64_t key,
   const uint64_t mask = g.cap - 1;
   uint64_t p = murmur_u64((uint64_t)key) & mask;
   for (uint64_t n = 0; n <= mask; n++) {
-    const int64_t v = __ldcg(g.keys + p);  // keys only go from free to set
+    const int64_t v = __ldcg(g.rec + p * g.rw);  // keys only go from free to set
     if (v == key) return (int64_t)p;
     if (v == kEmptyKey) {
-      const int64_t old = (int64_t)atomicCAS((unsigned long long*)(g.keys + p), (unsigned long long)kEmptyKey,
+      const int64_t old = (int64_t)atomicCAS((unsigned long long*)(g.rec + p * g.rw), (unsigned long long)kEmptyKey,
                                              (unsigned long long)key);
       if (old == kEmptyKey || old == key) return (int64_t)p;
     }
@@ -2024,7 +2031,7 @@ __device__ __forceinline__ int64_t group_slot(const GroupTable& g, const int64_t
       if (atomicCAS(g.state + p, 0u, 1u) == 0u) {
 #pragma unroll
         for (int j = 0; j < 4; j++)
-          if (j < (int)g.nkeys) g.keys[j * g.cap + p] = key[j];
+          if (j < (int)g.nkeys) g.rec[p * g.rw + j] = key[j];
         __threadfence();
         atomicExch(g.state + p, 2u);
         return (int64_t)p;
@@ -2042,13 +2049,30 @@ __device__ __forceinline__ int64_t group_slot(const GroupTable& g, const int64_t
     bool eq = true;
 #pragma unroll
     for (int j = 0; j < 4; j++)
-      if (j < (int)g.nkeys && __ldcg(g.keys + j * g.cap + p) != key[j]) eq = false;
+      if (j < (int)g.nkeys && __ldcg(g.rec + p * g.rw + j) != key[j]) eq = false;
     if (eq) return (int64_t)p;
     p = (p + 1) & mask;
     n++;
   }
   atomicCAS(err, 0, ALK_ERR_OVERFLOW);
   return -1;
+}
+
+// Slot of a group key in the direct form (keys within the zone maps' ranges); -1 with err
+// set for a key outside them.
+__device__ __forceinline__ int64_t group_slot_direct(const GroupTable& g, const int64_t (&key)[4], int* err) {
+  uint64_t slot = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    if (j < (int)g.nkeys) {
+      const uint64_t o = (uint64_t)key[j] - (uint64_t)g.kmin[j];
+      if (o >= g.kspan[j]) {
+        atomicExch(err, ALK_ERR_UNSUPPORTED);
+        return -1;
+      }
+      slot += o * g.kstride[j];
+    }
+  return (int64_t)slot;
 }
 
 // Position of the n-th (from 0) set bit of m; 32 when m has fewer.
@@ -2072,7 +2096,9 @@ __device__ __forceinline__ int64_t peer_reduce(int64_t v, uint32_t peers, uint8_
   return v;
 }
 
-template <bool kOneKey>
+// kForm: 0 hash table on one key column, 1 hash table on several, 2 direct (the key
+// space, from the zone maps, indexes the accumulators).
+template <int kForm>
 __global__ void __launch_bounds__(kT, 6) k_group_scan(const __grid_constant__ FastArgs f,
                                                    const __grid_constant__ GroupTable g) {
   const StageArgs& a = f.a;
@@ -2123,14 +2149,14 @@ __global__ void __launch_bounds__(kT, 6) k_group_scan(const __grid_constant__ Fa
       kept += __popc(__ballot_sync(0xffffffffu, live));
       int64_t slot = -1;
       if (live) {
-        if (kOneKey) {
+        if (kForm == 0) {
           slot = group_slot1(g, col((uint32_t)g.key_slot[0]), a.err);
         } else {
           int64_t key[4] = {0, 0, 0, 0};
 #pragma unroll
           for (int j = 0; j < 4; j++)
             if (j < (int)g.nkeys) key[j] = col((uint32_t)g.key_slot[j]);
-          slot = group_slot(g, key, a.err);
+          slot = kForm == 1 ? group_slot(g, key, a.err) : group_slot_direct(g, key, a.err);
         }
       }
       const bool use = slot >= 0;
@@ -2138,6 +2164,16 @@ __global__ void __launch_bounds__(kT, 6) k_group_scan(const __grid_constant__ Fa
       const uint32_t peers = __match_any_sync(0xffffffffu, use ? (unsigned long long)slot : ~0ull);
       const bool share = __any_sync(0xffffffffu, use && __popc(peers) > 1);
       const bool leader = use && (uint32_t)(__ffs(peers) - 1) == lane;
+      if (kForm == 2) {
+        // presence bits: the warp's groups in one word (keys in order put them side by
+        // side) are or-ed together first, and one lane applies the word; a word already
+        // showing every bit is left alone
+        const uint64_t word = leader ? (uint64_t)slot >> 5 : ~0ull;
+        const uint32_t wpeers = __match_any_sync(0xffffffffu, word);
+        const uint32_t bits = __reduce_or_sync(wpeers, leader ? 1u << (slot & 31) : 0u);
+        if (leader && (uint32_t)(__ffs(wpeers) - 1) == lane && (__ldcg(g.occ + word) & bits) != bits)
+          atomicOr(g.occ + word, bits);
+      }
       for (uint32_t v = 0; v < a.nagg; v++) {
         const uint8_t kind = s_kind[1 + v];
         int64_t x = kind == ALK_AGG_MIN ? INT64_MAX : kind == ALK_AGG_MAX ? INT64_MIN : 0;
@@ -2147,7 +2183,7 @@ __global__ void __launch_bounds__(kT, 6) k_group_scan(const __grid_constant__ Fa
                   : vm_eval<kT>(s_ins[1 + v], s_n[1 + v], s_res[1 + v], s_consts[1 + v], s_regs + threadIdx.x, col);
         if (share) x = peer_reduce(x, peers, kind);
         if (!leader) continue;
-        unsigned long long* dst = (unsigned long long*)(g.vals + (uint64_t)v * g.cap + slot);
+        unsigned long long* dst = (unsigned long long*)(g.rec + (uint64_t)slot * g.rw + g.kw + v);
         if (kind == ALK_AGG_SUM || kind == ALK_AGG_COUNT) atomicAdd(dst, (unsigned long long)x);
         else if (kind == ALK_AGG_MIN) atomicMin((long long*)dst, (long long)x);
         else atomicMax((long long*)dst, (long long)x);
@@ -2159,12 +2195,60 @@ __global__ void __launch_bounds__(kT, 6) k_group_scan(const __grid_constant__ Fa
   if (lane == 0 && rows_seen) atomicAdd(a.rows_in, rows_seen);
 }
 
+// Every record: free key words (kEmptyKey for the one-key table), accumulators at their
+// kind's identity.
+__global__ void __launch_bounds__(kT) k_group_init(const GroupTable g, uint32_t nagg, uint64_t kinds) {
+  const uint64_t words = g.cap * g.rw;
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < words; i += (uint64_t)gridDim.x * kT) {
+    const uint32_t w = (uint32_t)(i % g.rw);
+    int64_t v = 0;
+    if (w < g.kw) v = kEmptyKey;
+    else if (w - g.kw < nagg) {
+      const uint8_t kind = (uint8_t)(kinds >> (8 * (w - g.kw)));
+      v = kind == ALK_AGG_MIN ? INT64_MAX : kind == ALK_AGG_MAX ? INT64_MIN : 0;
+    }
+    g.rec[i] = v;
+  }
+}
+
+// Direct form: present slots to the output columns, one presence word per thread; the keys
+// are recovered from the slot.
+__global__ void __launch_bounds__(kT) k_group_compact_direct(const GroupTable g, uint32_t nagg) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t nwords = (g.cap + 31) / 32;
+  for (uint64_t w0 = blockIdx.x * (uint64_t)kT + (threadIdx.x & ~31u); w0 < nwords; w0 += (uint64_t)gridDim.x * kT) {
+    const uint64_t w = w0 + lane;
+    uint32_t bits = w < nwords ? g.occ[w] : 0u;
+    const uint32_t n = __popc(bits);
+    uint32_t excl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, excl, o);
+      if (lane >= (uint32_t)o) excl += t;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, excl, 31);
+    excl -= n;
+    if (!total) continue;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(g.groups, (unsigned long long)total);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    uint64_t pos = base + excl;
+    for (; bits; bits &= bits - 1, pos++) {
+      const uint64_t slot = w * 32 + (uint32_t)(__ffs(bits) - 1);
+      if (pos >= g.out_cap) continue;
+      for (uint32_t j = 0; j < g.nkeys; j++)
+        g.out_keys[j][pos] = (int64_t)((uint64_t)g.kmin[j] + (slot / g.kstride[j]) % g.kspan[j]);
+      for (uint32_t v = 0; v < nagg; v++) g.out_vals[v][pos] = g.rec[slot * g.rw + v];
+    }
+  }
+}
+
 // Occupied slots to the output columns (in slot order within a warp, warps in any order).
 __global__ void __launch_bounds__(kT) k_group_compact(const GroupTable g, uint32_t nagg) {
   const uint32_t lane = threadIdx.x & 31;
   for (uint64_t h0 = blockIdx.x * (uint64_t)kT + (threadIdx.x & ~31u); h0 < g.cap; h0 += (uint64_t)gridDim.x * kT) {
     const uint64_t h = h0 + lane;
-    const bool full = h < g.cap && (g.state ? g.state[h] == 2 : g.keys[h] != kEmptyKey);
+    const bool full = h < g.cap && (g.state ? g.state[h] == 2 : g.rec[h * g.rw] != kEmptyKey);
     const uint32_t m = __ballot_sync(0xffffffffu, full);
     if (!m) continue;
     unsigned long long base = 0;
@@ -2173,8 +2257,8 @@ __global__ void __launch_bounds__(kT) k_group_compact(const GroupTable g, uint32
     if (!full) continue;
     const uint64_t pos = base + __popc(m & ((1u << lane) - 1u));
     if (pos >= g.out_cap) continue;  // counted: the caller sees the total and sizes again
-    for (uint32_t j = 0; j < g.nkeys; j++) g.out_keys[j][pos] = g.keys[(uint64_t)j * g.cap + h];
-    for (uint32_t v = 0; v < nagg; v++) g.out_vals[v][pos] = g.vals[(uint64_t)v * g.cap + h];
+    for (uint32_t j = 0; j < g.nkeys; j++) g.out_keys[j][pos] = g.rec[h * g.rw + j];
+    for (uint32_t v = 0; v < nagg; v++) g.out_vals[v][pos] = g.rec[h * g.rw + g.kw + v];
   }
 }
 
@@ -2808,8 +2892,9 @@ int alk_seg_sorted(const alk_colseg* segs, uint32_t nseg, uint8_t* h_sorted, alk
 int alk_pipeline_groupby(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
                          const alk_program* pred, const int32_t* key_slots, uint32_t nkeys,
                          const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg, uint64_t max_groups,
-                         int64_t* const* d_out_keys, int64_t* const* d_out_vals, uint64_t out_cap,
-                         uint64_t* h_groups, uint64_t* h_seg_rows, uint64_t* h_rows_in, alk_stream stream) {
+                         const int64_t* key_min, const int64_t* key_max, int64_t* const* d_out_keys,
+                         int64_t* const* d_out_vals, uint64_t out_cap, uint64_t* h_groups, uint64_t* h_seg_rows,
+                         uint64_t* h_rows_in, alk_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (!h_groups || ncols == 0 || ncols > kMaxCols || nkeys == 0 || nkeys > 4 || nagg > 7 || !key_slots ||
       (nagg && (!agg_kind || !d_out_vals)) || !d_out_keys)
@@ -2843,17 +2928,43 @@ int alk_pipeline_groupby(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, 
     for (uint32_t c = 0; c < fa.nconj; c++)
       for (uint32_t g = 0; g < nseg; g++)
         cs.push_back(seg_mode[g] == 1 ? ConjSeg{0, 0, kCjAlways, 0} : conj_seg(fa.conj[c], cols[fa.conj[c].slot * nseg + g]));
-  // table: at most 0.7 full at max_groups
+  // Direct form when the key ranges are known and their product is small: at most 2^32
+  // slots, no more than 16 per scanned row, and records within 24 GB. Otherwise a
+  // hash table at most 0.7 full at max_groups.
+  uint64_t rows = 0;
+  for (uint32_t g = 0; g < nseg; g++)
+    if (seg_mode[g]) rows += cols[g].rows;
+  bool direct = key_min && key_max;
+  uint64_t space = 1, span[4] = {1, 1, 1, 1};
+  for (uint32_t j = 0; direct && j < nkeys; j++) {
+    if (key_max[j] < key_min[j]) {
+      span[j] = 1;  // nothing scanned: any key lies outside, which the kernel reports
+      continue;
+    }
+    span[j] = (uint64_t)key_max[j] - (uint64_t)key_min[j] + 1;
+    if (span[j] == 0 || span[j] > (1ull << 32) || space > (1ull << 32) / span[j]) direct = false;
+    else space *= span[j];
+  }
+  uint32_t dw = 1;  // record words of the direct form (accumulators, padded)
+  while (dw < nagg) dw <<= 1;
+  if (direct && (space > 16 * std::max<uint64_t>(rows, 1024) || (long double)space * 8.0L * dw > 24.0L * (1ull << 30)))
+    direct = false;
   uint64_t cap = 1024;
-  while ((long double)cap * 0.7L < (long double)std::max<uint64_t>(max_groups, 1)) cap <<= 1;
-  const bool one = nkeys == 1;
+  if (direct) cap = space;
+  else
+    while ((long double)cap * 0.7L < (long double)std::max<uint64_t>(max_groups, 1)) cap <<= 1;
+  const bool one = nkeys == 1 && !direct;
   const size_t off_cs = (hb.size() + 15) & ~size_t(15);
   const size_t off_ctr = (off_cs + cs.size() * sizeof(ConjSeg) + 255) & ~size_t(255);
   const size_t ctr_bytes = 32 + 8 * (size_t)nseg;  // rows_in, groups, err, pad, seg_rows
   const size_t off_keys = (off_ctr + ctr_bytes + 255) & ~size_t(255);
-  const size_t off_vals = off_keys + 8 * (size_t)nkeys * cap;
-  const size_t off_state = off_vals + 8 * (size_t)nagg * cap;
-  const size_t total = off_state + (one ? 0 : 4 * (size_t)cap);
+  // record: key words (hash forms), accumulators; padded to 1, 2, 4 or 8 words when that fits
+  const uint32_t kw = direct ? 0 : nkeys;
+  uint32_t rw = std::max<uint32_t>(kw + nagg, 1);
+  if (rw <= 8) rw = rw <= 1 ? 1 : rw <= 2 ? 2 : rw <= 4 ? 4 : 8;
+  const size_t off_state = (off_keys + 8 * (size_t)rw * cap + 15) & ~size_t(15);  // state words or presence bits
+  const size_t state_bytes = direct ? 4 * ((cap + 31) / 32) : one ? 0 : 4 * (size_t)cap;
+  const size_t total = off_state + state_bytes;
   uint8_t* db = nullptr;
   CK(cudaMallocAsync((void**)&db, total, s));
   std::vector<uint8_t> up(off_ctr, 0);
@@ -2864,13 +2975,7 @@ int alk_pipeline_groupby(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, 
   CK(ue);
   CK(cudaMemcpyAsync(db, src, up.size(), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(db + off_ctr, 0, ctr_bytes, s));
-  if (one) CK(cudaMemsetAsync(db + off_keys, 0x80, 8 * cap, s));  // every key word = kEmptyKey
-  else CK(cudaMemsetAsync(db + off_state, 0, 4 * cap, s));
-  for (uint32_t v = 0; v < nagg; v++) {
-    const int64_t init = agg_kind[v] == ALK_AGG_MIN ? INT64_MAX : agg_kind[v] == ALK_AGG_MAX ? INT64_MIN : 0;
-    k_fill_i64<<<grid_for(cap), kT, 0, s>>>((int64_t*)(db + off_vals) + (uint64_t)v * cap, cap, init);
-    alk::g_kernel_launches++;
-  }
+  if (state_bytes) CK(cudaMemsetAsync(db + off_state, 0, state_bytes, s));
   patch(a, db);
   a.agg_kind = db + off_x;
   a.nagg = nagg;
@@ -2880,10 +2985,21 @@ int alk_pipeline_groupby(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, 
   fa.cseg = (const ConjSeg*)(db + off_cs);
   GroupTable g{};
   g.cap = cap;
-  g.keys = (int64_t*)(db + off_keys);
-  g.vals = (int64_t*)(db + off_vals);
-  g.state = one ? nullptr : (uint32_t*)(db + off_state);
+  g.rec = (int64_t*)(db + off_keys);
+  g.rw = rw;
+  g.kw = kw;
+  g.state = one || direct ? nullptr : (uint32_t*)(db + off_state);
+  g.occ = direct ? (uint32_t*)(db + off_state) : nullptr;
   g.nkeys = nkeys;
+  if (direct) {
+    uint64_t stride = 1;
+    for (int j = (int)nkeys - 1; j >= 0; j--) {  // the last key column varies fastest
+      g.kmin[j] = key_min[j];
+      g.kspan[j] = span[j];
+      g.kstride[j] = stride;
+      stride *= span[j];
+    }
+  }
   for (uint32_t j = 0; j < nkeys; j++) g.key_slot[j] = key_slots[j];
   g.generic = progs[0].n_instr && !conj;
   g.seg_rows = (unsigned long long*)(db + off_ctr + 32);
@@ -2891,15 +3007,20 @@ int alk_pipeline_groupby(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, 
   g.out_keys = (int64_t* const*)(db + off_outp);
   g.out_vals = (int64_t* const*)(db + off_outp + 8 * (size_t)nkeys);
   g.out_cap = out_cap;
+  uint64_t kinds = 0;
+  for (uint32_t v = 0; v < nagg; v++) kinds |= (uint64_t)agg_kind[v] << (8 * v);
+  k_group_init<<<grid_for(cap * rw), kT, 0, s>>>(g, nagg, kinds);
+  alk::g_kernel_launches++;
   if (a.ntiles) {
-    void (*kern)(const FastArgs, const GroupTable) = one ? k_group_scan<true> : k_group_scan<false>;
+    void (*kern)(const FastArgs, const GroupTable) = direct ? k_group_scan<2> : one ? k_group_scan<0> : k_group_scan<1>;
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kT, 0);
     const int grid = std::min<int>((int)a.ntiles, sms() * std::max(occ, 1));
     kern<<<grid, kT, 0, s>>>(fa, g);
     alk::g_kernel_launches++;
   }
-  k_group_compact<<<grid_for(cap), kT, 0, s>>>(g, nagg);
+  if (direct) k_group_compact_direct<<<grid_for((cap + 31) / 32), kT, 0, s>>>(g, nagg);
+  else k_group_compact<<<grid_for(cap), kT, 0, s>>>(g, nagg);
   alk::g_kernel_launches++;
   CK(cudaGetLastError());
   std::vector<unsigned long long> back(4 + nseg);

@@ -2273,6 +2273,18 @@ bool Engine::hash_select(Statement& st) {
     }
     if (ordered) return fail();
   }
+  // key ranges over the scanned segments (zone maps): a small key space indexes the
+  // accumulators directly
+  std::vector<int64_t> kmin(group_cols.size(), INT64_MAX), kmax(group_cols.size(), INT64_MIN);
+  for (size_t j = 0; j < group_cols.size(); j++) {
+    BaseCol& bc = basecol(src, group_cols[j]);
+    read_headers(src, group_cols[j], bc);
+    for (uint32_t g = 0; g < src->segCount; g++) {
+      if (!p.mode[g]) continue;
+      kmin[j] = std::min(kmin[j], std::min(bc.segs[g].m.lower, bc.segs[g].m.upper));
+      kmax[j] = std::max(kmax[j], std::max(bc.segs[g].m.lower, bc.segs[g].m.upper));
+    }
+  }
   const size_t cycles = cycle_count(a);
   GroupOut G;
   std::vector<int64_t*> okeys, ovals;
@@ -2296,7 +2308,8 @@ bool Engine::hash_select(Statement& st) {
     const int rc = alk_pipeline_groupby(cs.data(), (uint32_t)p.slots.size(), src->segCount, p.mode.data(),
                                         p.has_pred ? &p.pred : nullptr, key_slots.data(),
                                         (uint32_t)key_slots.size(), progs.data(), kinds.data(),
-                                        (uint32_t)aggs.size(), groups, okeys.data(), ovals.data(), out_cap, &ng,
+                                        (uint32_t)aggs.size(), groups, kmin.data(), kmax.data(), okeys.data(),
+                                        ovals.data(), out_cap, &ng,
                                         seg_rows.data(), nullptr, (alk_stream)stream_);
     if (timing_) {
       cudaEventRecord(ev1_, stream_);
@@ -2313,7 +2326,9 @@ bool Engine::hash_select(Statement& st) {
       groups = std::min<uint64_t>(std::max<uint64_t>(rows, 1), std::max(ng > out_cap ? ng : out_cap * 4, groups));
       continue;
     }
-    if (rc == ALK_ERR_UNSUPPORTED) return fail();  // a key equal to the free-slot marker
+    // a key equal to the free-slot marker, or outside the zone maps' range (the header
+    // bounds of a FOR-delta segment are its first and last values)
+    if (rc == ALK_ERR_UNSUPPORTED) return fail();
     check(rc, "hash group-by");
     break;
   }

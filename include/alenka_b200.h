@@ -368,19 +368,24 @@ const int64_t* alk_ht_payload(const alk_ht* h, uint32_t p);
  * select.cu:359-952, over the rows emit_filter keeps, filter.cu:133-643). pred (NULL =
  * every row) and the aggregate input programs read scan columns (slots < ncols) at their
  * stored widths; nkeys (1-4) group key columns at key_slots; nagg (<= 7) aggregates of
- * agg_kind. max_groups sizes the table (at most 0.7 full). The groups, in no particular
- * order, go to the device columns d_out_keys[j] / d_out_vals[v] (host arrays of device
- * addresses, out_cap values each); *h_groups is the group count. Surviving rows per
+ * agg_kind. key_min / key_max (host arrays, or NULL) bound the key columns over the
+ * scanned segments (zone maps): when the product of their spans is small (at most 2^32
+ * and 16 per scanned row) the key space itself indexes the accumulators (no hashing, a
+ * presence bit per slot); otherwise max_groups sizes a hash table (at most 0.7 full). The
+ * groups, in no particular order, go to the device columns d_out_keys[j] /
+ * d_out_vals[v] (host arrays of device addresses, out_cap values each); *h_groups is
+ * the group count. Surviving rows per
  * segment go to h_seg_rows[nseg] and rows scanned to *h_rows_in (either may be NULL).
  * Synchronises. ALK_ERR_OVERFLOW: more groups than out_cap (*h_groups tells how many) or
  * a full table (more groups than the table holds: call again with a larger max_groups);
- * ALK_ERR_UNSUPPORTED: a one-column key equal to 0x8080808080808080, the table's
- * free-slot marker. */
+ * ALK_ERR_UNSUPPORTED: a one-column key equal to 0x8080808080808080 (the hash table's
+ * free-slot marker), or a key outside the stated ranges. */
 int alk_pipeline_groupby(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const uint8_t* seg_mode,
                          const alk_program* pred, const int32_t* key_slots, uint32_t nkeys,
                          const alk_program* agg_progs, const uint8_t* agg_kind, uint32_t nagg, uint64_t max_groups,
-                         int64_t* const* d_out_keys, int64_t* const* d_out_vals, uint64_t out_cap,
-                         uint64_t* h_groups, uint64_t* h_seg_rows, uint64_t* h_rows_in, alk_stream stream);
+                         const int64_t* key_min, const int64_t* key_max, int64_t* const* d_out_keys,
+                         int64_t* const* d_out_vals, uint64_t out_cap, uint64_t* h_groups, uint64_t* h_seg_rows,
+                         uint64_t* h_rows_in, alk_stream stream);
 /* Optional CUDA-event timing of the probe-aggregate kernel (cudaEvent_t handles). */
 typedef struct alk_event_timer {
   int on;

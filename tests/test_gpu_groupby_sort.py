@@ -119,7 +119,12 @@ def test_engine_high_cardinality_groupby(flat, mode):
 
 
 FUSED = {
-    # two unsorted key columns (the multi-column table), MAX and an expression input
+    # one key column whose range is too wide to index directly: the one-CAS hash table
+    "wide_key": "LF := FILTER lineitem BY l_shipdate >= 19950101;\n"
+                "R := SELECT l_extendedprice AS p, SUM(l_quantity) AS q, MIN(l_discount) AS mn, "
+                "COUNT(l_orderkey) AS c FROM LF GROUP BY l_extendedprice;\n"
+                "STORE R INTO 'fz.txt' USING ('|');\n",
+    # two unsorted key columns (the multi-column hash table), MAX and an expression input
     "two_keys": "LF := FILTER lineitem BY l_shipdate < 19960101 AND l_quantity > 10;\n"
                 "R := SELECT l_extendedprice AS p, l_discount AS d, SUM(l_quantity) AS q, MAX(l_shipdate) AS mx, "
                 "COUNT(l_orderkey) AS c FROM LF GROUP BY l_extendedprice, l_discount;\n"
@@ -147,8 +152,10 @@ FUSED = {
 @pytest.mark.parametrize("name", sorted(FUSED))
 def test_fused_hash_groupby_matches_oracle(flat, name):
     """The fused filter + hash GROUP BY (alk_pipeline_groupby) through the engine, byte
-    for byte against the oracle: several key columns, predicates that are and are not
-    conjunctions, no filter, a skipped first segment, and an empty result."""
+    for byte against the oracle, in its three forms: the key space indexing the
+    accumulators (l_orderkey; the char-coded keys), a one-column hash table (a key range
+    wider than 16 slots per row) and a multi-column one. Also predicates that are and are
+    not conjunctions, no filter, a skipped first segment, and an empty result."""
     from . import _oracle
     script = FUSED[name]
     _oracle.execute(flat, script.replace("fz.txt", "oracle_fz.txt"))
