@@ -586,6 +586,31 @@ __global__ void __launch_bounds__(kT) k_sortkey_i64(const int64_t* key, const ui
 __global__ void __launch_bounds__(kT) k_widen(const uint32_t* in, uint64_t n, int64_t* out) {
   for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) out[i] = in[i];
 }
+// Frame-of-reference re-encoding: the exact minimum and maximum (one pass), then the
+// values less the minimum at the narrowest of 8/16/32/64 bits (a second pass).
+__global__ void __launch_bounds__(kT) k_minmax_i64(const int64_t* in, uint64_t n, long long* mm) {
+  long long lo = INT64_MAX, hi = INT64_MIN;
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
+    const long long v = in[i];
+    lo = min(lo, v);
+    hi = max(hi, v);
+  }
+  for (int o = 16; o; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(mm, lo);
+    atomicMax(mm + 1, hi);
+  }
+}
+template <typename T>
+__global__ void __launch_bounds__(kT) k_for_narrow(const int64_t* in, uint64_t n, const long long* mm, T* out) {
+  const uint64_t lo = (uint64_t)mm[0];
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT)
+    out[i] = (T)((uint64_t)in[i] - lo);
+}
+
 __global__ void __launch_bounds__(kT) k_narrow(const int64_t* in, uint64_t n, uint32_t* out) {
   for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) out[i] = (uint32_t)in[i];
 }
@@ -1430,6 +1455,42 @@ int alk_widen_u32(const uint32_t* d_in, uint64_t n, int64_t* d_out, alk_stream s
   CK(cudaGetLastError());
   return ALK_OK;
 }
+int alk_for_reencode(const int64_t* d_in, uint64_t n, void* d_out, size_t out_cap, int64_t* h_lower, uint32_t* h_bits,
+                     alk_stream stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!h_lower || !h_bits || (n && (!d_in || !d_out))) return ALK_ERR_ARG;
+  *h_lower = 0;
+  *h_bits = 8;
+  if (n == 0) return ALK_OK;
+  long long* mm = nullptr;
+  CK(cudaMallocAsync((void**)&mm, 16, s));
+  const long long init[2] = {INT64_MAX, INT64_MIN};
+  CK(cudaMemcpyAsync(mm, init, 16, cudaMemcpyHostToDevice, s));
+  k_minmax_i64<<<grid_for(n), kT, 0, s>>>(d_in, n, mm);
+  alk::g_kernel_launches++;
+  long long h[2];
+  CK(cudaMemcpyAsync(h, mm, 16, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const uint64_t span = (uint64_t)h[1] - (uint64_t)h[0];
+  const uint32_t bits = span < (1ull << 8) ? 8 : span < (1ull << 16) ? 16 : span < (1ull << 32) ? 32 : 64;
+  if (out_cap < n * (bits / 8)) {
+    cudaFreeAsync(mm, s);
+    return ALK_ERR_OVERFLOW;
+  }
+  switch (bits) {
+    case 8: k_for_narrow<uint8_t><<<grid_for(n), kT, 0, s>>>(d_in, n, mm, (uint8_t*)d_out); break;
+    case 16: k_for_narrow<uint16_t><<<grid_for(n), kT, 0, s>>>(d_in, n, mm, (uint16_t*)d_out); break;
+    case 32: k_for_narrow<uint32_t><<<grid_for(n), kT, 0, s>>>(d_in, n, mm, (uint32_t*)d_out); break;
+    default: k_for_narrow<uint64_t><<<grid_for(n), kT, 0, s>>>(d_in, n, mm, (uint64_t*)d_out); break;
+  }
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
+  CK(cudaFreeAsync(mm, s));
+  *h_lower = h[0];
+  *h_bits = bits;
+  return ALK_OK;
+}
+
 int alk_narrow_u32(const int64_t* d_in, uint64_t n, uint32_t* d_out, alk_stream stream) {
   if (n == 0) return ALK_OK;
   k_narrow<<<grid_for(n), kT, 0, (cudaStream_t)stream>>>(d_in, n, d_out);

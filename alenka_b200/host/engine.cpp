@@ -339,15 +339,30 @@ void Engine::ensure_base_col(Var* base, const std::string& col, bool device) {
                        stream_),
        "segment upload");
     stats_.h2d_bytes += m.cnt;
+    bc.res_lower.resize(base->segCount, 0);
+    bc.res_bits.resize(base->segCount, 64);
     if (m.comp_type == 1) {
-      // padded like the FOR payloads: bulk tile copies round their length up to 16 bytes
+      // decoded once (bit unpack + prefix sum), then kept as FOR at the narrowest width
+      // over the segment's exact range, padded like the FOR payloads (bulk tile copies
+      // round their length up to 16 bytes); every scan kernel then reads it as FOR
       auto dec = mkbuf((size_t)m.rec_count * 8 + 256, stream_);
       check(alk_decode_segment(buf->as<void>(), 1, m.bits, m.fit_count, m.orig_lower, m.start_val, m.rec_count,
                                dec->as<int64_t>(), (alk_stream)stream_),
             "delta decode");
-      bc.dev[g] = dec;
+      const size_t cap = (size_t)m.rec_count * 8;
+      auto narrow = mkbuf((cap + 255) / 256 * 256 + 256, stream_);
+      int64_t lo = 0;
+      uint32_t bits = 64;
+      check(alk_for_reencode(dec->as<int64_t>(), m.rec_count, narrow->as<void>(), cap, &lo, &bits,
+                             (alk_stream)stream_),
+            "delta re-encode");
+      bc.dev[g] = narrow;
+      bc.res_lower[g] = lo;
+      bc.res_bits[g] = bits;
     } else {
       bc.dev[g] = buf;
+      bc.res_lower[g] = m.orig_lower;
+      bc.res_bits[g] = m.bits;
     }
   }
 }
@@ -826,13 +841,8 @@ Rows Engine::materialize(Var* v, const std::vector<std::string>& fields, bool wa
       alk_colseg& d = cs[c * src->segCount + g];
       d.data = bc.dev[g]->as<void>();
       d.rows = m.rec_count;
-      if (m.comp_type == 1) {
-        d.lower = 0;
-        d.bits = 64;
-      } else {
-        d.lower = m.orig_lower;
-        d.bits = m.bits;
-      }
+      d.lower = bc.res_lower[g];
+      d.bits = bc.res_bits[g];
     }
   }
   for (uint32_t g = 0; g < src->segCount; g++)
@@ -902,8 +912,8 @@ std::vector<alk_colseg> Engine::colsegs(const ScanPlan& p) {
       alk_colseg& d = cs[c * src->segCount + g];
       d.data = bc.dev[g]->as<void>();
       d.rows = m.rec_count;
-      d.lower = m.comp_type == 1 ? 0 : m.orig_lower;
-      d.bits = m.comp_type == 1 ? 64 : m.bits;
+      d.lower = bc.res_lower[g];
+      d.bits = bc.res_bits[g];
     }
   }
   for (uint32_t g = 0; g < src->segCount; g++)
@@ -918,7 +928,7 @@ uint64_t Engine::scan_bytes(const ScanPlan& p, const std::vector<uint32_t>& used
     for (uint32_t g = 0; g < p.src->segCount; g++) {
       if (!p.mode[g]) continue;
       const SegMeta& m = bc.segs[g].m;
-      b += (uint64_t)m.rec_count * (m.comp_type == 1 ? 8 : m.bits / 8);
+      b += (uint64_t)m.rec_count * (bc.res_bits.size() > g ? bc.res_bits[g] / 8 : m.bits / 8);
     }
   }
   return b;

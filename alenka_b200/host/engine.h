@@ -68,7 +68,11 @@ struct BaseCol {
   std::vector<SegInfo> segs;
   std::vector<uint8_t*> host_img;     // pinned host copies of the segment files
   std::vector<size_t> host_len;
-  std::vector<DevBufP> dev;           // device payload (FOR) or expanded int64 (delta)
+  std::vector<DevBufP> dev;           // device payload: FOR as stored; FOR-delta re-encoded as FOR
+  // per segment, the resident encoding: value = stored + res_lower at res_bits (for FOR
+  // segments the file's own; for FOR-delta ones the re-encoding's exact minimum and width)
+  std::vector<int64_t> res_lower;
+  std::vector<uint32_t> res_bits;
   // per segment: its values in ascending order (1) or not (0), as checked on the device
   // buffer recorded beside it (a segment uploaded again is checked again)
   std::vector<std::weak_ptr<DevBuf>> order_buf;

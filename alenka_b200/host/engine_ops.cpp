@@ -2868,7 +2868,7 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
       uint32_t w = 1;
       BaseCol& bc = basecol(pf.src, pf.slots[c]);
       for (uint32_t g = 0; g < pf.src->segCount; g++)
-        if (pf.mode[g]) w = std::max<uint32_t>(w, bc.segs[g].m.comp_type == 1 ? 8 : bc.segs[g].m.bits / 8);
+        if (pf.mode[g]) w = std::max<uint32_t>(w, bc.res_bits.size() > g ? bc.res_bits[g] / 8 : bc.segs[g].m.bits / 8);
       tail.hit_bytes += w;
     }
     tail.streamed_bytes = scan_bytes(pf, std::vector<uint32_t>(streamed.begin(), streamed.end()));

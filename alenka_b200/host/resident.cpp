@@ -77,6 +77,8 @@ int Engine::gen_resident_flat(const std::string& t, const std::vector<uint32_t>&
       bc.host_img.assign(nseg, nullptr);
       bc.host_len.assign(nseg, 0);
       bc.dev.resize(nseg);
+      bc.res_lower.assign(nseg, 0);
+      bc.res_bits.assign(nseg, 64);
       bc.headers_read = true;
       bc.device_only = true;
       for (uint32_t g = 0; g < nseg; g++) {
@@ -92,6 +94,8 @@ int Engine::gen_resident_flat(const std::string& t, const std::vector<uint32_t>&
         s.fit_count = 64 / s.bits;
         s.start_val = 0;
         bc.dev[g] = std::make_shared<DevBuf>(((size_t)s.cnt + 255) / 256 * 256 + 256, stream_);
+        bc.res_lower[g] = lo;
+        bc.res_bits[g] = s.bits;
         alk_colseg& d = cs[(size_t)c * nseg + g];
         d.data = bc.dev[g]->as<void>();
         d.lower = lo;

@@ -283,6 +283,13 @@ int alk_seg_sorted(const alk_colseg* segs, uint32_t nseg, uint8_t* h_sorted, alk
 /* Width conversions used by the host engine between index and value columns. */
 int alk_widen_u32(const uint32_t* d_in, uint64_t n, int64_t* d_out, alk_stream stream);
 int alk_narrow_u32(const int64_t* d_in, uint64_t n, uint32_t* d_out, alk_stream stream);
+/* Frame-of-reference re-encoding of n int64 values: the exact minimum goes to *h_lower,
+ * the narrowest of 8/16/32/64 bits that holds every value less it to *h_bits, and the
+ * values less the minimum at that width to d_out (out_cap bytes; ALK_ERR_OVERFLOW when
+ * too small). The engine keeps FOR-delta segments resident in this form: decoded once
+ * at upload, then read like FOR segments (value = stored + lower). Synchronises. */
+int alk_for_reencode(const int64_t* d_in, uint64_t n, void* d_out, size_t out_cap, int64_t* h_lower, uint32_t* h_bits,
+                     alk_stream stream);
 
 /* Linear-probing hash join on MurmurHash64A keys, replaces the sort-merge join of
  * emit_multijoin (operators.cu:1117-1283, moderngpu inner_join). Build indexes the

@@ -429,3 +429,32 @@ def test_dense_modes_and_late_rows(route, dup):
         L.alk_ht_free(ht, None)
         torch.cuda.synchronize()
     del bufs
+
+
+@pytest.mark.parametrize("span,bits", [(0, 8), (255, 8), (256, 16), (65535, 16), (1 << 20, 32), ((1 << 32) - 1, 32),
+                                       (1 << 40, 64)])
+def test_for_reencode_picks_the_narrowest_width(span, bits):
+    """alk_for_reencode (how FOR-delta segments stay resident): exact minimum, the
+    narrowest width that holds the span, and the values less the minimum at that width;
+    a too small output is refused."""
+    import torch
+    L = ab.lib()
+    L.alk_for_reencode.argtypes = [c.c_void_p, c.c_uint64, c.c_void_p, c.c_size_t, c.POINTER(c.c_int64),
+                                   c.POINTER(c.c_uint32), c.c_void_p]
+    rng = np.random.default_rng(span % 1000 + 3)
+    n = 100_003
+    lo = -(1 << 35) + 17
+    v = lo + rng.integers(0, span + 1, n, dtype=np.int64)
+    v[0], v[-1] = lo, lo + span  # both ends present: the span is exact
+    d_in = torch.from_numpy(v).cuda()
+    out = torch.zeros(n * 8 // 8 + 32, dtype=torch.int64, device="cuda")
+    low, b = c.c_int64(), c.c_uint32()
+    # one byte short of the width it needs: refused
+    assert L.alk_for_reencode(d_in.data_ptr(), n, out.data_ptr(), n * bits // 8 - 1, c.byref(low), c.byref(b),
+                              None) == ALK_ERR_OVERFLOW
+    assert L.alk_for_reencode(d_in.data_ptr(), n, out.data_ptr(), n * 8, c.byref(low), c.byref(b), None) == ALK_OK
+    torch.cuda.synchronize()
+    assert low.value == lo and b.value == bits
+    dt = {8: np.uint8, 16: np.uint16, 32: np.uint32, 64: np.uint64}[bits]
+    got = out.cpu().numpy().view(np.uint8)[:n * bits // 8].view(dt).astype(np.uint64)
+    assert np.array_equal(got, (v - lo).astype(np.uint64))
