@@ -70,6 +70,7 @@ def _declare(L):
     L.alk_gen_lineitem_flat.argtypes = [c.c_char_p, u64, u32, u64, i32, c.c_char_p, i32]
     L.alk_gen_names.argtypes = [c.c_char_p, u64, u32, u32, u64, c.c_char_p, i32]
     L.alk_gen_three_way.argtypes = [c.c_char_p, u64, u64, u64, u32, u64, i32, c.c_char_p, i32]
+    L.alk_gen_three_way_zipf.argtypes = [c.c_char_p, u64, u64, u64, u32, u64, i32, c.c_double, c.c_char_p, i32]
     L.alk_date_add_days.argtypes = [i64, i64]
     L.alk_date_add_days.restype = i64
     L.alk_decode_segment.argtypes = [vp, u32, u32, u32, i64, i64, u32, vp, vp]
@@ -274,10 +275,16 @@ def gen_names(data_dir, rows, distinct, seg_rows, seed):
         raise AlenkaError(rc, err.value.decode())
 
 
-def gen_three_way(data_dir, customers, orders, lineitems, seg_rows, seed, delta=False):
+def gen_three_way(data_dir, customers, orders, lineitems, seg_rows, seed, delta=False, zipf=0.0):
+    """Three-way tables; zipf > 0 draws lineitem's orderkeys from Zipf(zipf) over the
+    orders (in key order)."""
     err = ctypes.create_string_buffer(512)
-    rc = lib().alk_gen_three_way(str(data_dir).encode(), customers, orders, lineitems, seg_rows, seed,
-                                 int(delta), err, 512)
+    if zipf > 0:
+        rc = lib().alk_gen_three_way_zipf(str(data_dir).encode(), customers, orders, lineitems, seg_rows, seed,
+                                          int(delta), float(zipf), err, 512)
+    else:
+        rc = lib().alk_gen_three_way(str(data_dir).encode(), customers, orders, lineitems, seg_rows, seed,
+                                     int(delta), err, 512)
     if rc:
         raise AlenkaError(rc, err.value.decode())
 

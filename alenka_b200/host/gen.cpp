@@ -6,6 +6,7 @@
 // money, int yyyymmdd dates and dictionary-encoded char columns.
 #include <algorithm>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -134,10 +135,13 @@ bool gen_lineitem_flat(const std::string& dir, uint64_t rows, uint32_t seg_rows,
 
 // Three-way workload: customer (custkey dense 1..C, mktsegment of 5 values), orders
 // (orderkey = 4*i, custkey uniform FK, orderdate uniform over 7 years, shippriority 0),
-// lineitem (orderkey FK with 1-7 rows per order in order, shipdate = orderdate +
-// U[1,121] days, extendedprice, discount).
+// lineitem (orderkey FK in key order, shipdate = orderdate + U[1,121] days,
+// extendedprice, discount). Rows per order: 1-7 uniform, or (zipf_s > 0) the skewed join
+// of the compressed config: order i gets round(N F(i)) - round(N F(i - 1)) rows, F the
+// Zipf(s) distribution over the orders (F(k) = H(k, s) / H(orders, s), H the generalised
+// harmonic number), so the keys stay in order and the counts sum to N exactly.
 bool gen_three_way(const std::string& dir, uint64_t customers, uint64_t orders, uint64_t lineitems,
-                   uint32_t seg_rows, uint64_t seed, bool delta, std::string& err) {
+                   uint32_t seg_rows, uint64_t seed, bool delta, double zipf_s, std::string& err) {
   DataDict dd;
   std::string e2;
   load_data_dict(dir + "/data.dictionary", dd, e2);
@@ -180,11 +184,37 @@ bool gen_three_way(const std::string& dir, uint64_t customers, uint64_t orders, 
     for (auto& v : ints) v.resize(lineitems);
     Rng rk(mix(seed, 31)), rs(mix(seed, 32)), rp(mix(seed, 33)), rd(mix(seed, 34));
     uint64_t o = 0;
-    int64_t left = rk.uniform(1, 7);
+    int64_t left = 0;
+    // Zipf: the cumulative row count after order o, from the running harmonic sum
+    long double htotal = 0, hrun = 0;
+    uint64_t emitted_to = 0;  // rows assigned to orders <= o
+    auto zipf_next = [&]() -> int64_t {
+      hrun += std::pow((long double)(o + 1), -(long double)zipf_s);
+      const uint64_t upto = o + 1 >= orders ? lineitems
+                                            : std::min<uint64_t>(lineitems, (uint64_t)std::llround((long double)lineitems * hrun / htotal));
+      const int64_t n = (int64_t)(upto - emitted_to);
+      emitted_to = upto;
+      return n;
+    };
+    if (zipf_s > 0) {
+      for (uint64_t k = 1; k <= orders; k++) htotal += std::pow((long double)k, -(long double)zipf_s);
+      left = zipf_next();
+      while (left == 0 && o + 1 < orders) {
+        o++;
+        left = zipf_next();
+      }
+    } else {
+      left = rk.uniform(1, 7);
+    }
     for (uint64_t i = 0; i < lineitems; i++) {
-      if (left == 0) {
-        o = (o + 1) % orders;  // wraps only when lineitems exceed 7 x orders
-        left = rk.uniform(1, 7);
+      while (left == 0) {
+        if (zipf_s > 0) {
+          o++;  // the counts sum to the row count: o stays below orders
+          left = zipf_next();
+        } else {
+          o = (o + 1) % orders;  // wraps only when lineitems exceed 7 x orders
+          left = rk.uniform(1, 7);
+        }
       }
       left--;
       ints[0][i] = 4 * ((int64_t)o + 1);
@@ -243,7 +273,18 @@ int alk_gen_lineitem_flat(const char* dir, uint64_t rows, uint32_t seg_rows, uin
 int alk_gen_three_way(const char* dir, uint64_t customers, uint64_t orders, uint64_t lineitems,
                       uint32_t seg_rows, uint64_t seed, int delta, char* err, int err_len) {
   std::string e;
-  bool ok = alk::gen_three_way(dir, customers, orders, lineitems, seg_rows, seed, delta != 0, e);
+  bool ok = alk::gen_three_way(dir, customers, orders, lineitems, seg_rows, seed, delta != 0, 0.0, e);
+  if (!ok && err && err_len > 0) std::snprintf(err, (size_t)err_len, "%s", e.c_str());
+  return ok ? 0 : 1;
+}
+int alk_gen_three_way_zipf(const char* dir, uint64_t customers, uint64_t orders, uint64_t lineitems,
+                           uint32_t seg_rows, uint64_t seed, int delta, double zipf_s, char* err, int err_len) {
+  std::string e;
+  if (!(zipf_s > 0) || orders == 0) {
+    if (err && err_len > 0) std::snprintf(err, (size_t)err_len, "zipf exponent and orders must be positive");
+    return 1;
+  }
+  bool ok = alk::gen_three_way(dir, customers, orders, lineitems, seg_rows, seed, delta != 0, zipf_s, e);
   if (!ok && err && err_len > 0) std::snprintf(err, (size_t)err_len, "%s", e.c_str());
   return ok ? 0 : 1;
 }

@@ -99,9 +99,11 @@ def make_flat(data_dir, rows=FLAT_ROWS, seg_rows=2_000_000, seed=1, delta=False)
     gen_lineitem_flat(data_dir, rows, seg_rows, seed, delta)
 
 
-def make_three_way(data_dir, scale=1.0, seg_rows=10_000_000, seed=1, delta=False):
+def make_three_way(data_dir, scale=1.0, seg_rows=10_000_000, seed=1, delta=False, zipf=0.0):
+    """The three-way tables at scale (x the config-2 sizes). The compressed config stores
+    them FOR-delta (delta=True) with Zipf(1.1) join keys (zipf=1.1)."""
     c = max(1, int(THREE_WAY["customers"] * scale))
     o = max(1, int(THREE_WAY["orders"] * scale))
     li = max(1, int(THREE_WAY["lineitems"] * scale))
-    gen_three_way(data_dir, c, o, li, seg_rows, seed, delta)
+    gen_three_way(data_dir, c, o, li, seg_rows, seed, delta, zipf)
     return li

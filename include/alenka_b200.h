@@ -484,6 +484,11 @@ int alk_gen_lineitem_flat(const char* dir, uint64_t rows, uint32_t seg_rows, uin
                           char* err, int err_len);
 int alk_gen_three_way(const char* dir, uint64_t customers, uint64_t orders, uint64_t lineitems,
                       uint32_t seg_rows, uint64_t seed, int delta, char* err, int err_len);
+/* The same tables with skewed join keys: lineitem's orderkeys follow Zipf(zipf_s) over
+ * the orders, in key order (order i gets round(N F(i)) - round(N F(i - 1)) of the N
+ * rows, F the Zipf distribution function over the orders). */
+int alk_gen_three_way_zipf(const char* dir, uint64_t customers, uint64_t orders, uint64_t lineitems,
+                           uint32_t seg_rows, uint64_t seed, int delta, double zipf_s, char* err, int err_len);
 /* Table "names" for string predicates: n_key 1..rows and n_name char(12) drawn from
  * `distinct` generated strings over A, B, X, '.', '%', '_' (lengths 0-12). */
 int alk_gen_names(const char* dir, uint64_t rows, uint32_t distinct, uint32_t seg_rows, uint64_t seed, char* err,

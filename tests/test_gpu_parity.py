@@ -90,6 +90,28 @@ def test_three_way_pipeline_delta_segments(three_way_delta, seed):
     assert o == g
 
 
+@pytest.fixture(scope="module")
+def three_way_skewed(tmp_path_factory):
+    # the compressed config's shape: FOR-delta columns, lineitem's orderkeys Zipf(1.1)
+    # over the orders (the heaviest order holds about 9% of the rows)
+    d = tmp_path_factory.mktemp("three_way_skewed")
+    wl.make_three_way(str(d), scale=0.02, seg_rows=300_000, seed=6, delta=True, zipf=1.1)
+    return str(d)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+@pytest.mark.parametrize("plain", [True, False])
+def test_three_way_skewed_delta(three_way_skewed, seed, plain):
+    """Skewed join keys on FOR-delta segments, through the fused plan and the operator
+    path, byte for byte against the oracle; every group, so the heavy keys' sums show."""
+    o, g, st = _run_both(three_way_skewed, wl.three_way_script(seed, limit=0), "q3.txt", plain=plain)
+    assert o == g
+    assert o.count(b"\n") > 100
+    o, g, st = _run_both(three_way_skewed, wl.three_way_script(seed), "q3.txt", plain=plain)
+    assert o == g
+    assert st.plan == (0 if plain else 1)  # LIMIT 10: the fused plan's device top-k
+
+
 @pytest.mark.parametrize("seed", [1, 2])
 @pytest.mark.parametrize("plain", [True, False])
 def test_three_way_pipeline(three_way, seed, plain):
