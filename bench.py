@@ -670,7 +670,7 @@ def main():
     ap.add_argument("--fused-only", action="store_true",
                     help="time only the resident fused plan (profiling runs)")
     ap.add_argument("--workload", default="three_way",
-                    choices=["three_way", "batched", "groupby_high", "encode", "compressed"],
+                    choices=["three_way", "batched", "groupby_high", "encode", "compressed", "estimator"],
                     help="three_way: the filter -> join -> group-by pipeline (default); batched: many "
                          "single-table filter + group-by queries per step; compressed: the three-way on "
                          "FOR-delta tables with Zipf(1.1) join keys")
@@ -693,10 +693,10 @@ def main():
         return
     import torch
     torch.cuda.set_device(local)
-    if args.workload in ("batched", "groupby_high", "encode", "compressed"):
+    if args.workload in ("batched", "groupby_high", "encode", "compressed", "estimator"):
         if rank == 0:
             {"batched": run_batched, "groupby_high": run_groupby_high, "encode": run_encode,
-             "compressed": run_compressed}[args.workload](args, torch)
+             "compressed": run_compressed, "estimator": run_estimator}[args.workload](args, torch)
         return
     dist = None
     if world > 1:
@@ -747,6 +747,92 @@ def query_bytes(d, fact_rows, counts):
                 g += 1
     return total + 32 * counts.get("probe_rows_beyond_l2", 0) + 64 * counts.get("agg_rows_beyond_l2", 0) \
         + 32 * counts.get("build_rows", 0) + counts.get("output_bytes", 0)
+
+
+def run_estimator(args, torch):
+    """The learned estimator at the config-2 scale: three-way tables of 60M / 15M / 1.5M
+    rows in 1M-row segments, seeded queries of the README shape in record mode until about
+    100k exact (query, segment) records exist, training on the device, then the q-error
+    of held-out records (rows passing filter and probe per segment) for the network and
+    for the classical histogram / independence estimate, and the bytes that 12 new
+    queries' first runs reserve with and without the estimator (results identical)."""
+    import numpy as np
+    import alenka_b200 as ab
+    from alenka_b200 import workloads as wl
+    base = args.data_dir or os.path.join(tempfile.gettempdir(), "alenka_bench")
+    d = os.path.join(base, f"estimator_seed{args.seed}")
+    marker = os.path.join(d, ".complete")
+    if not os.path.exists(marker):
+        os.makedirs(d, exist_ok=True)
+        wl.make_three_way(d, scale=1.0, seg_rows=1_000_000, seed=args.seed)
+        open(marker, "w").close()
+
+    def run(s, script):
+        try:
+            s.execute(script)
+        except ab.AlenkaError as e:  # an empty join stops the reference with an error too
+            return "error: " + str(e)
+        return None
+    want_records, n_test = 100_000, 300
+    t0 = time.perf_counter()
+    with ab.Session(d) as s:
+        s.card_mode(record=True)
+        q = 0
+        while q < 20_000:  # about 100k records; a bound in case the queries skip most segments
+            run(s, wl.card_script(q, out="qc.txt"))
+            q += 1
+            if q % 50 == 0 and len(s.card_records()[1]) >= want_records:
+                break
+        n_train = q
+        split = len(s.card_records()[1])
+        for k in range(n_test):
+            run(s, wl.card_script(n_train + k, out="qc.txt"))
+        record_s = time.perf_counter() - t0
+        x, y, m = s.card_records()
+        t1 = time.perf_counter()
+        l_first = s.card_train(0, split, epochs=1, batch=256, lr=1e-3, seed=3)
+        l_last = s.card_train(0, split, epochs=40, batch=256, lr=1e-3, seed=4)
+        train_s = time.perf_counter() - t1
+        xt, yt, mt = x[split:], y[split:], m[split:]
+        pt = np.minimum(s.card_predict(xt), 0.0)
+        rows = np.exp2(xt[:, 3] * 32) - 1
+        floor = np.log(0.5 / np.maximum(rows, 1))
+        act = yt[:, 0] + yt[:, 1] * mt[:, 1]
+        est = pt[:, 0] + pt[:, 1] * mt[:, 1]
+        classical = np.maximum(np.log(np.maximum(xt[:, 9] * np.where(mt[:, 1] > 0, xt[:, 10], 1.0), 1e-30)), floor)
+        q_mlp, q_cls = np.exp(np.abs(est - act)), np.exp(np.abs(classical - act))
+        first = {}
+        outs = {}
+        for use in (False, True):
+            s.card_mode(record=False, use=use)
+            res, tot, reruns = [], 0, 0
+            for k in range(100_000, 100_012):
+                s.card_forget()
+                err = run(s, wl.card_script(k, out="qc.txt"))
+                st = s.stats()
+                tot += st.reserved_bytes
+                reruns += st.card_reruns
+                with open(os.path.join(d, "qc.txt"), "rb") as f:
+                    res.append(err or f.read())
+            outs[use] = res
+            first["with_estimator" if use else "upper_bound"] = {"reserved_mib": tot / 2**20, "reruns": reruns}
+    if outs[True] != outs[False]:
+        raise SystemExit("bench: estimator sizing changed a result")
+    print(json.dumps({
+        "metric": "q-error of the learned cardinality estimate (rows passing filter and probe per query segment)",
+        "value": float(np.median(q_mlp)), "unit": "q-error (median)", "higher_is_better": False, "n_gpus": 1,
+        "data": "synthetic", "dtype": "bf16 weights, fp32 accumulate",
+        "config": {"workload": "three-way tables 60M / 15M / 1.5M in 1M-row segments (config-2 scale); "
+                               "seeded README-shape queries with varied operators and constants",
+                   "train_queries": n_train, "train_records": int(split), "test_queries": n_test,
+                   "test_records": int(len(act))},
+        "q_error": {"mlp": {"median": float(np.median(q_mlp)), "p95": float(np.percentile(q_mlp, 95)),
+                            "max": float(q_mlp.max())},
+                    "classical": {"median": float(np.median(q_cls)), "p95": float(np.percentile(q_cls, 95)),
+                                  "max": float(q_cls.max())}},
+        "loss": {"first_epoch": l_first, "last_epoch": l_last},
+        "seconds": {"record": record_s, "train": train_s},
+        "first_runs": first, "verified": {"results_identical": True}}), flush=True)
 
 
 def run_compressed(args, torch):
