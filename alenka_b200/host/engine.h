@@ -280,6 +280,7 @@ class Engine {
   void emit_order(Statement& st);
   void emit_store(Statement& st);
   void emit_store_binary(Statement& st);
+  void emit_load(Statement& st);
   DevBufP like_set(Var* base, const std::string& col, const std::string& pattern);
   const DevBufP& dict_ranks(const ColMeta& m);
   std::map<std::string, uint32_t> cnt_counts_;  // largest payload written per column file prefix

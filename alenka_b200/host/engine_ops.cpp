@@ -1774,6 +1774,58 @@ void Engine::emit_store_binary(Statement& st) {
   basecols_.erase(st.f);
 }
 
+// LOAD 'file' USING (sep) AS (...) (emit_load, operators.cu:2565-2589, and the text source
+// CudaSet::LoadBigFile reads, cm.cu:1852-2080): the file is parsed on the device
+// (alk_text_load) into a variable of int64 columns, which the statements after it use
+// like any computed result (STORE ... BINARY writes it as segments). The reference reads
+// the file when a statement first needs the variable; here the LOAD reads it.
+void Engine::emit_load(Statement& st) {
+  if (st.load_cols.empty()) unsupported("LOAD without columns");
+  if (st.load_cols.size() > 32) unsupported("LOAD of more than 32 columns");
+  std::vector<alk_text_col> cols(st.load_cols.size());
+  for (size_t i = 0; i < st.load_cols.size(); i++) {
+    const LoadCol& lc = st.load_cols[i];
+    cols[i].field = (uint32_t)std::max(lc.field, 0);
+    if (lc.type == "int") {
+      cols[i].kind = ALK_TEXT_INT;
+    } else if (lc.type == "decimal") {
+      cols[i].kind = ALK_TEXT_DECIMAL;
+      cols[i].scale = (uint32_t)std::max(lc.size, 0);
+    } else {
+      unsupported("LOAD of " + lc.type + " columns (" + lc.name + ")");
+    }
+  }
+  const std::string path = !st.f.empty() && st.f[0] == '/' ? st.f : dir_ + "/" + st.f;
+  std::vector<uint8_t> text;
+  std::string e;
+  if (!read_file(path, text, e)) throw EngineError(ALK_ERR_IO, "Could not open file " + st.f);
+  uint64_t rows = 0;
+  for (uint8_t b : text) rows += b == '\n';
+  auto out = std::make_unique<Var>();
+  out->kind = Var::Mat;
+  out->name = st.s;
+  out->n = rows;
+  std::vector<int64_t*> dst;
+  for (auto& lc : st.load_cols) {
+    auto b = mkbuf(std::max<uint64_t>(rows, 1) * 8, stream_);
+    out->data[lc.name] = b;
+    dst.push_back(b->as<int64_t>());
+    out->columnNames.push_back(lc.name);
+    ColMeta m;
+    m.type = 0;
+    m.dz = lc.type == "decimal" ? (uint32_t)std::max(lc.size, 0) : 0;  // decimal_zeroes (cm.cu:3000-3005)
+    out->meta[lc.name] = m;
+  }
+  uint64_t got = 0;
+  uint32_t dates = 0;
+  check(alk_text_load((const char*)text.data(), text.size(), st.sep.empty() ? '|' : st.sep[0], cols.data(),
+                      (uint32_t)cols.size(), dst.data(), std::max<uint64_t>(rows, 1), &got, &dates,
+                      (alk_stream)stream_),
+        "text load");
+  stats_.h2d_bytes += text.size();
+  vars_[st.s] = std::move(out);
+}
+
 // ------------------------------------------------------------------ script
 void Engine::exec(Statement& st) {
   if (st.op_case) unsupported("CASE expressions");
@@ -1785,7 +1837,8 @@ void Engine::exec(Statement& st) {
     case StmtKind::Store: emit_store(st); break;
     case StmtKind::StoreBinary: emit_store_binary(st); break;
     case StmtKind::Display: break;
-    default: unsupported("statement kind (LOAD / catalog commands)");
+    case StmtKind::Load: emit_load(st); break;
+    default: unsupported("statement kind (catalog commands)");
   }
 }
 

@@ -162,6 +162,14 @@ void capture(alk::StmtKind kind, const char* s, const char* f, const char* sep, 
     st.join_tab_cnt = join_tab_cnt;
     st.join_and_cnt = join_and_cnt;
     st.op_case = op_case;
+    if (kind == alk::StmtKind::Load)  // the AS list: emit_var / emit_varchar / emit_vardecimal
+      while (!namevars.empty() && !typevars.empty() && !sizevars.empty() && !cols.empty()) {
+        st.load_cols.push_back({namevars.front(), cols.front(), typevars.front(), sizevars.front()});
+        namevars.pop();
+        typevars.pop();
+        sizevars.pop();
+        cols.pop();
+      }
     g_pending.push_back(std::move(st));
   }
   clean_queues();
@@ -177,6 +185,7 @@ string script_key(const std::vector<alk::Statement>& sts) {
     for (auto x : st.op_nums) k += "," + std::to_string(x);
     for (auto x : st.op_nums_precision) k += "," + std::to_string(x);
     for (auto& x : st.op_join) k += "," + x;
+    for (auto& c : st.load_cols) k += "," + c.name + "{" + std::to_string(c.field) + "}" + c.type + std::to_string(c.size);
     k += ";";
   }
   return k;

@@ -459,17 +459,19 @@ class Parser {
 
   // NAME '{' INTNUM '}' ':' NAME ['(' INTNUM [',' INTNUM] ')'] [NO ENCODING] (bison.y:182-185)
   void var_decl(const std::string& n) {
+    LoadCol lc;
+    lc.name = n;
     expect_punct('{');
-    expect_int();
+    lc.field = (int)expect_int();
     expect_punct('}');
     expect_punct(':');
-    expect(T::Name, "type name");
+    lc.type = expect(T::Name, "type name");
     if (is_punct('(')) {
       take();
-      expect_int();
+      lc.size = (int)expect_int();  // emit_varchar: the width
       if (is_punct(',')) {
         take();
-        expect_int();
+        lc.size = (int)expect_int();  // emit_vardecimal: the digits after the point
       }
       expect_punct(')');
     }
@@ -477,7 +479,7 @@ class Parser {
       take();
       expect_kw("ENCODING");
     }
-    (void)n;
+    cur_->load_cols.push_back(lc);
   }
 
   int expr_list() {  // bison.y:223-228

@@ -25,6 +25,17 @@ enum class StmtKind {
   Other         // DESCRIBE / SHOW / DROP / INSERT / DELETE / CREATE
 };
 
+// A column of a LOAD's AS list (NAME{field}:type[(size[, decimals])], bison.y:182-185):
+// what emit_var / emit_varchar / emit_vardecimal queue for the text-source CudaSet
+// (operators.cu:239-286, cm.cu:2965-3015). size: a char column's width, a decimal
+// column's digits after the point (the second number), else 0.
+struct LoadCol {
+  std::string name;
+  int field = 0;
+  std::string type;
+  int size = 0;
+};
+
 struct Statement {
   StmtKind kind = StmtKind::Other;
   std::string s;      // target variable (Store/Display: variable to write)
@@ -42,6 +53,7 @@ struct Statement {
   std::vector<char> join_type, join_eq_type;
   unsigned sel_count = 0, join_tab_cnt = 0;
   std::map<unsigned, unsigned> join_and_cnt;
+  std::vector<LoadCol> load_cols;  // LOAD: the AS list
   int line = 0;
 };
 

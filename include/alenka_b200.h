@@ -283,6 +283,26 @@ int alk_seg_sorted(const alk_colseg* segs, uint32_t nseg, uint8_t* h_sorted, alk
 /* Width conversions used by the host engine between index and value columns. */
 int alk_widen_u32(const uint32_t* d_in, uint64_t n, int64_t* d_out, alk_stream stream);
 int alk_narrow_u32(const int64_t* d_in, uint64_t n, uint32_t* d_out, alk_stream stream);
+/* Text loader (LOAD 'file' USING (sep) AS (...), CudaSet::LoadBigFile, cm.cu:1852-2080):
+ * the records are the text's newline-terminated lines; declared column i reads the i-th
+ * smallest of the declared field numbers (1-based), as the reference maps them. A field
+ * ends at the separator outside double quotes (the quotes stay in it, NUL bytes are
+ * dropped) and is cut to 23 bytes; it is parsed as an integer (ALK_TEXT_INT: leading
+ * spaces, a sign, digits), a decimal of `scale` <= 9 fraction digits (ALK_TEXT_DECIMAL:
+ * value x 10^scale, digits past the scale ignored), or, when the first record's field
+ * has '-' at offset 4, as a yyyy-mm-dd date (yyyymmdd; *h_date_mask bit i). d_out[i]:
+ * int64 device column of out_cap values; *h_rows gets the record count (ALK_ERR_OVERFLOW
+ * when above out_cap). h_text is host memory; synchronises. */
+typedef struct alk_text_col {
+  uint32_t field;  /* 1-based field number as declared */
+  uint32_t kind;   /* ALK_TEXT_INT or ALK_TEXT_DECIMAL */
+  uint32_t scale;  /* decimal: digits after the point */
+  uint32_t pad;
+} alk_text_col;
+#define ALK_TEXT_INT 0
+#define ALK_TEXT_DECIMAL 1
+int alk_text_load(const char* h_text, uint64_t nbytes, char sep, const alk_text_col* cols, uint32_t ncols,
+                  int64_t* const* d_out, uint64_t out_cap, uint64_t* h_rows, uint32_t* h_date_mask, alk_stream stream);
 /* Frame-of-reference re-encoding of n int64 values: the exact minimum goes to *h_lower,
  * the narrowest of 8/16/32/64 bits that holds every value less it to *h_bits, and the
  * values less the minimum at that width to d_out (out_cap bytes; ALK_ERR_OVERFLOW when
