@@ -24,39 +24,42 @@ struct TextArgs {
   char sep;
   uint32_t ncols;
   uint32_t field[kMaxTextCols];  // 0-based field of declared column i (the i-th smallest)
-  uint32_t kind[kMaxTextCols];   // 0 integer, 1 decimal, 2 date
-  uint32_t scale[kMaxTextCols];  // decimal: digits after the point
-  int64_t* out[kMaxTextCols];
+  uint32_t kind[kMaxTextCols];   // 0 integer, 1 decimal, 2 date, 3 fixed-width text
+  uint32_t scale[kMaxTextCols];  // decimal: digits after the point; text: the width
+  void* out[kMaxTextCols];       // int64 values, or width bytes a record
   const unsigned long long* nl;  // newline positions
   uint64_t rows;
 };
 
 // The field walk of parse_functor (cm.h:599-650) for one record starting at pos: each
-// requested field, in increasing field order, is cut into a zero-filled kSlot-byte slot
-// and handed to visit(index, slot). Reads stop at the end of the text (a record missing
-// fields gets zero slots for them).
+// requested field, in increasing field order, is found as the bytes [b, e) up to the
+// separator outside double quotes (the quote state runs on across the record's fields)
+// and handed to visit(index, b, e). Reads stop at the end of the text.
 template <class Visit>
 __host__ __device__ inline void cut_fields(const char* text, uint64_t n, uint64_t pos, char sep, uint32_t ncols,
                                            const uint32_t* field, Visit&& visit) {
   uint32_t cur = 0, want = 0;
   bool quoted = false;
   uint64_t j = pos;
-  char slot[kSlot];
   while (want < ncols) {
-    const bool keep = field[want] == cur;
-    uint32_t t = 0;
-    if (keep)
-      for (uint32_t k = 0; k < kSlot; k++) slot[k] = 0;
+    const uint64_t b = j;
     while (j < n && (text[j] != sep || quoted)) {
-      const char ch = text[j];
-      if (ch == '"') quoted = !quoted;
-      if (keep && ch != 0 && t < kSlot) slot[t++] = ch;
+      if (text[j] == '"') quoted = !quoted;
       j++;
     }
+    if (field[want] == cur) visit(want++, b, j);
     j++;  // past the separator
-    if (keep) visit(want++, slot);
     cur++;
   }
+}
+
+// A field's bytes into a zero-filled slot of w bytes, NUL bytes dropped (the reference's
+// dest slot; bytes beyond w, which it lets run into the next record's slot, are dropped).
+__host__ __device__ inline void fill_slot(const char* text, uint64_t b, uint64_t e, char* slot, uint32_t w) {
+  uint32_t t = 0;
+  for (uint64_t k = b; k < e && t < w; k++)
+    if (text[k] != 0) slot[t++] = text[k];
+  for (; t < w; t++) slot[t] = 0;
 }
 
 // gpu_atoll (cm.h:543-597)
@@ -135,17 +138,50 @@ __host__ __device__ inline int64_t parse_date(const char* s) {
   return (int64_t)acc;
 }
 
-// The first record's slots: a column whose slot has '-' at offset 4 is a date column.
+// The first record's slots: a numeric column whose slot has '-' at offset 4 is a date
+// column.
 struct DateProbe {
+  const char* text;
   uint32_t* kind;
   uint32_t* mask;
-  __host__ __device__ void operator()(uint32_t c, const char* slot) const {
-    if (slot[4] == '-') {
+  __host__ __device__ void operator()(uint32_t c, uint64_t b, uint64_t e) const {
+    char slot[kSlot];
+    fill_slot(text, b, e, slot, kSlot);
+    if (kind[c] != 3 && slot[4] == '-') {
       kind[c] = 2;
       if (mask) *mask |= 1u << c;
     }
   }
 };
+
+// MurmurHash64A (MurmurHash2_64.cu:201-242) of each record's w bytes, halved: the
+// per-row values of a char column's .hash file (compress_char, cm.cu:1808-1812).
+__global__ void __launch_bounds__(kT) k_hash_strings(const uint8_t* chars, uint64_t n, uint32_t w, uint32_t seed,
+                                                     uint64_t* out) {
+  const uint64_t m = 0xc6a4a7935bd1e995ull;
+  for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
+    const uint8_t* p = chars + i * w;
+    uint64_t h = seed ^ ((uint64_t)w * m);
+    uint32_t k = 0;
+    for (; k + 8 <= w; k += 8) {
+      uint64_t x = 0;
+      for (int b = 7; b >= 0; b--) x = (x << 8) | p[k + b];
+      x *= m;
+      x ^= x >> 47;
+      x *= m;
+      h ^= x;
+      h *= m;
+    }
+    if (k < w) {
+      for (int b = (int)(w - k) - 1; b >= 0; b--) h ^= (uint64_t)p[k + b] << (8 * b);
+      h *= m;
+    }
+    h ^= h >> 47;
+    h *= m;
+    h ^= h >> 47;
+    out[i] = h / 2;
+  }
+}
 
 // Newline counts of each thread's kChunk bytes.
 __global__ void __launch_bounds__(kT) k_nl_count(const char* text, uint64_t n, unsigned long long* counts) {
@@ -174,10 +210,16 @@ __global__ void __launch_bounds__(kT) k_nl_write(const char* text, uint64_t n, c
 __global__ void __launch_bounds__(kT) k_text_parse(const __grid_constant__ TextArgs a) {
   for (uint64_t r = blockIdx.x * (uint64_t)kT + threadIdx.x; r < a.rows; r += (uint64_t)gridDim.x * kT) {
     const uint64_t start = r == 0 ? 0 : a.nl[r - 1] + 1;
-    cut_fields(a.text, a.n, start, a.sep, a.ncols, a.field, [&](uint32_t c, const char* slot) {
-      a.out[c][r] = a.kind[c] == 2   ? parse_date(slot)
-                    : a.kind[c] == 1 ? parse_decimal(slot, a.scale[c])
-                                     : parse_int(slot);
+    cut_fields(a.text, a.n, start, a.sep, a.ncols, a.field, [&](uint32_t c, uint64_t b, uint64_t e) {
+      if (a.kind[c] == 3) {
+        fill_slot(a.text, b, e, (char*)a.out[c] + r * a.scale[c], a.scale[c]);
+        return;
+      }
+      char slot[kSlot];
+      fill_slot(a.text, b, e, slot, kSlot);
+      ((int64_t*)a.out[c])[r] = a.kind[c] == 2   ? parse_date(slot)
+                                : a.kind[c] == 1 ? parse_decimal(slot, a.scale[c])
+                                                 : parse_int(slot);
     });
   }
 }
@@ -192,14 +234,15 @@ __global__ void __launch_bounds__(kT) k_text_parse(const __grid_constant__ TextA
 extern "C" {
 
 int alk_text_load(const char* h_text, uint64_t nbytes, char sep, const alk_text_col* cols, uint32_t ncols,
-                  int64_t* const* d_out, uint64_t out_cap, uint64_t* h_rows, uint32_t* h_date_mask, alk_stream stream) {
+                  void* const* d_out, uint64_t out_cap, uint64_t* h_rows, uint32_t* h_date_mask, alk_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (!h_rows || !cols || ncols == 0 || ncols > kMaxTextCols || (nbytes && !h_text) || !d_out) return ALK_ERR_ARG;
   *h_rows = 0;
   if (h_date_mask) *h_date_mask = 0;
   for (uint32_t c = 0; c < ncols; c++) {
-    if (cols[c].field == 0 || cols[c].kind > ALK_TEXT_DECIMAL || !d_out[c]) return ALK_ERR_ARG;
+    if (cols[c].field == 0 || cols[c].kind > ALK_TEXT_CHAR || !d_out[c]) return ALK_ERR_ARG;
     if (cols[c].kind == ALK_TEXT_DECIMAL && cols[c].scale > 9) return ALK_ERR_UNSUPPORTED;
+    if (cols[c].kind == ALK_TEXT_CHAR && cols[c].width == 0) return ALK_ERR_ARG;
   }
   // records: the newline-terminated lines (text after the last newline is not a record)
   uint64_t rows = 0;
@@ -218,12 +261,12 @@ int alk_text_load(const char* h_text, uint64_t nbytes, char sep, const alk_text_
   std::sort(f.begin(), f.end());
   for (uint32_t c = 0; c < ncols; c++) {
     a.field[c] = f[c];
-    a.kind[c] = cols[c].kind == ALK_TEXT_DECIMAL ? 1 : 0;
-    a.scale[c] = cols[c].scale;
+    a.kind[c] = cols[c].kind == ALK_TEXT_CHAR ? 3 : cols[c].kind == ALK_TEXT_DECIMAL ? 1 : 0;
+    a.scale[c] = cols[c].kind == ALK_TEXT_CHAR ? cols[c].width : cols[c].scale;
     a.out[c] = d_out[c];
   }
   // a column is a date column when its first record's slot has '-' at offset 4 (cm.cu:2024-2026)
-  DateProbe probe{a.kind, h_date_mask};
+  DateProbe probe{h_text, a.kind, h_date_mask};
   cut_fields(h_text, nbytes, 0, sep, ncols, a.field, probe);
   const uint64_t threads = (nbytes + kChunk - 1) / kChunk;
   const size_t off_cnt = (nbytes + 255) & ~size_t(255);
@@ -257,6 +300,17 @@ int alk_text_load(const char* h_text, uint64_t nbytes, char sep, const alk_text_
   CK(cudaGetLastError());
   CK(cudaFreeAsync(db, s));
   CK(cudaStreamSynchronize(s));
+  return ALK_OK;
+}
+
+int alk_hash_strings(const uint8_t* d_chars, uint64_t n, uint32_t width, uint32_t seed, uint64_t* d_out,
+                     alk_stream stream) {
+  if (n == 0) return ALK_OK;
+  if (!d_chars || !d_out || width == 0) return ALK_ERR_ARG;
+  const int grid = (int)std::min<uint64_t>((n + kT - 1) / kT, 148ull * 16);
+  k_hash_strings<<<grid, kT, 0, (cudaStream_t)stream>>>(d_chars, n, width, seed, d_out);
+  alk::g_kernel_launches++;
+  CK(cudaGetLastError());
   return ALK_OK;
 }
 

@@ -782,6 +782,7 @@ Rows Engine::materialize(Var* v, const std::vector<std::string>& fields, bool wa
     r.n = v->n;
     for (auto& fl : fields) {
       if (!v->has(fl)) continue;
+      if (v->meta.at(fl).raw) unsupported("the char column " + fl + " of a LOAD is read by STORE ... BINARY only");
       if (!v->data.count(fl) && v->host.count(fl)) {  // a host-held small result column
         const auto& h = v->host.at(fl);
         auto d = mkbuf(std::max<size_t>(h.size(), 1) * 8, stream_);

@@ -54,6 +54,8 @@ struct ColMeta {
   uint32_t dz = 0;     // decimal_zeroes
   uint32_t width = 0;  // char width
   std::string string_map;  // "<table>.<column>" dictionary the codes refer to
+  bool raw = false;          // a LOAD's char column: width bytes a row, no dictionary yet
+  bool no_encoding = false;  // ... declared NO ENCODING
 };
 
 struct SegInfo {
@@ -284,6 +286,9 @@ class Engine {
   DevBufP like_set(Var* base, const std::string& col, const std::string& pattern);
   const DevBufP& dict_ranks(const ColMeta& m);
   std::map<std::string, uint32_t> cnt_counts_;  // largest payload written per column file prefix
+  // codes of a LOAD's char values per column name: hash -> code (key 0: NO ENCODING's
+  // running count), kept for the session as the reference keeps its char_hash
+  std::map<std::string, std::unordered_map<uint64_t, int64_t>> char_codes_;
   bool try_fused(std::vector<Statement>& sts, size_t& i);
   void run_fused(Statement& J, Statement& F, Statement& O, Statement& S, const std::string& gkey);
   // After the synchronisation: check the stages, record their counts, store the rows.

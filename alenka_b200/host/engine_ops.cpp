@@ -1709,10 +1709,16 @@ void Engine::emit_store(Statement& st) {
 void Engine::emit_store_binary(Statement& st) {
   Var* a = var(st.s);
   if (st.store_sort) unsupported("STORE BINARY with SORT SEGMENTS BY / PRESORTED BY");
-  for (auto& c : a->columnNames)
-    if (a->meta[c].type != 0 || !a->meta[c].string_map.empty()) unsupported("STORE BINARY of char columns");
+  std::vector<std::string> icols, ccols;  // integer columns; a LOAD's char columns
+  for (auto& c : a->columnNames) {
+    if (a->meta[c].raw) ccols.push_back(c);
+    else if (a->meta[c].type != 0 || !a->meta[c].string_map.empty()) unsupported("STORE BINARY of char columns");
+    else icols.push_back(c);
+  }
+  if (!ccols.empty() && st.append) unsupported("STORE BINARY APPEND of char columns");
   if (st.f.empty() || st.f.find('/') != std::string::npos) unsupported("STORE BINARY outside the data directory");
-  Rows R = materialize(a, a->columnNames);
+  Rows R = materialize(a, icols);
+  if (icols.empty()) R.n = a->n;
   const size_t limit = st.op_nums.empty() ? 0 : (size_t)st.op_nums[0];
   const uint64_t n = (limit != 0 && limit < R.n) ? limit : R.n;
   if (n > UINT32_MAX) unsupported("a segment of more than 2^32 - 1 rows");
@@ -1736,7 +1742,59 @@ void Engine::emit_store_binary(Statement& st) {
     }
     return;
   }
-  // every column's segment image in one call of the device writer
+  // A LOAD's char columns (compress_char, cm.cu:1765-1844): codes in first-appearance
+  // order of the values' MurmurHash64A / 2 (one code sequence per column name for the
+  // session, as the reference keys its char_hash), or a running count from 1 under NO
+  // ENCODING; the dictionary file gets each new value, the .hash file every row's hash,
+  // and the codes are written as the .idx segment.
+  std::map<std::string, DevBufP> code_cols;
+  for (auto& c : ccols) {
+    const ColMeta& m = a->meta[c];
+    const uint32_t w = m.width;
+    const DevBufP& raw = a->data.at(c);
+    auto dh = mkbuf(n * 8, stream_);
+    check(alk_hash_strings(raw->as<uint8_t>(), n, w, 100, dh->as<uint64_t>(), (alk_stream)stream_), "string hash");
+    std::vector<uint64_t> h(n);
+    std::vector<uint8_t> chars((size_t)n * w);
+    ck(cudaMemcpyAsync(h.data(), dh->as<void>(), n * 8, cudaMemcpyDeviceToHost, stream_), "d2h");
+    ck(cudaMemcpyAsync(chars.data(), raw->as<void>(), (size_t)n * w, cudaMemcpyDeviceToHost, stream_), "d2h");
+    ck(cudaStreamSynchronize(stream_), "d2h");
+    stats_.d2h_bytes += n * 8 + (uint64_t)n * w;
+    std::vector<int64_t> codes(n);
+    std::vector<uint8_t> dict;
+    auto& known = char_codes_[c];
+    if (!m.no_encoding) {
+      for (uint64_t i = 0; i < n; i++) {
+        auto it = known.find(h[i]);
+        if (it == known.end()) {
+          const int64_t code = (int64_t)known.size();
+          known.emplace(h[i], code);
+          dict.insert(dict.end(), chars.begin() + (size_t)i * w, chars.begin() + (size_t)(i + 1) * w);
+          codes[i] = code;
+        } else {
+          codes[i] = it->second;
+        }
+      }
+    } else {
+      int64_t cnt = known.count(0) ? known[0] : 0;
+      for (uint64_t i = 0; i < n; i++) codes[i] = ++cnt;
+      known[0] = cnt;
+      dict = chars;
+    }
+    const std::string prefix = base + "." + c;
+    if (!write_file(prefix, dict.data(), dict.size())) throw EngineError(ALK_ERR_IO, "Could not write " + prefix);
+    std::vector<uint8_t> hf(4 + (size_t)n * 8);
+    const uint32_t n32 = (uint32_t)n;
+    std::memcpy(hf.data(), &n32, 4);
+    std::memcpy(hf.data() + 4, h.data(), (size_t)n * 8);
+    const std::string hp = prefix + "." + std::to_string(seg) + ".hash";
+    if (!write_file(hp, hf.data(), hf.size())) throw EngineError(ALK_ERR_IO, "Could not write " + hp);
+    auto dc = mkbuf(n * 8, stream_);
+    ck(cudaMemcpyAsync(dc->as<void>(), codes.data(), n * 8, cudaMemcpyHostToDevice, stream_), "h2d");
+    ck(cudaStreamSynchronize(stream_), "h2d");
+    code_cols[c] = dc;
+  }
+  // every column's segment image (char columns: their codes) in one call of the device writer
   const size_t ncol = a->columnNames.size();
   const size_t cap = (kSegHeadBytes + (size_t)n * 8 + kSegTailBytes + 255) & ~size_t(255);
   auto imgs = mkbuf(cap * ncol, stream_);
@@ -1745,7 +1803,8 @@ void Engine::emit_store_binary(Statement& st) {
   std::vector<void*> dst(ncol);
   std::vector<size_t> caps(ncol, cap), lens(ncol, 0);
   for (size_t k = 0; k < ncol; k++) {
-    src[k] = R.col.at(a->columnNames[k])->as<int64_t>();
+    const std::string& c = a->columnNames[k];
+    src[k] = code_cols.count(c) ? code_cols[c]->as<int64_t>() : R.col.at(c)->as<int64_t>();
     dst[k] = imgs->as<uint8_t>() + k * cap;
   }
   check(alk_encode_segments_device(src.data(), counts.data(), (uint32_t)ncol, (flags_ & ALK_SESSION_DELTA) ? 2 : 0,
@@ -1760,15 +1819,16 @@ void Engine::emit_store_binary(Statement& st) {
     ck(cudaStreamSynchronize(stream_), "segment d2h");
     stats_.d2h_bytes += len;
     const std::string prefix = base + "." + c;
-    if (!write_file(prefix + "." + std::to_string(seg), host.data(), len))
-      throw EngineError(ALK_ERR_IO, "Could not write " + prefix + "." + std::to_string(seg));
+    const std::string seg_file = prefix + "." + std::to_string(seg) + (code_cols.count(c) ? ".idx" : "");
+    if (!write_file(seg_file, host.data(), len)) throw EngineError(ALK_ERR_IO, "Could not write " + seg_file);
     uint32_t cnt = 0;
     std::memcpy(&cnt, host.data(), 4);
     cnt_counts_[prefix] = std::max(cnt_counts_[prefix], cnt);
     if (!write_col_header(prefix + ".header", ColHeader{total, seg + 1, max_recs, cnt_counts_[prefix]}))
       throw EngineError(ALK_ERR_IO, "Could not write " + prefix + ".header");
   }
-  for (auto& c : a->columnNames) dd_[st.f][c] = ColData{0, a->meta[c].dz};
+  for (auto& c : a->columnNames)
+    dd_[st.f][c] = a->meta[c].raw ? ColData{2, a->meta[c].width} : ColData{0, a->meta[c].dz};
   if (!save_data_dict(dir_ + "/data.dictionary", dd_)) throw EngineError(ALK_ERR_IO, "Could not write data.dictionary");
   bases_.erase(st.f);  // the table is read afresh by the next statement that names it
   basecols_.erase(st.f);
@@ -1791,8 +1851,12 @@ void Engine::emit_load(Statement& st) {
     } else if (lc.type == "decimal") {
       cols[i].kind = ALK_TEXT_DECIMAL;
       cols[i].scale = (uint32_t)std::max(lc.size, 0);
-    } else {
+    } else if (lc.type == "float" || lc.type == "timestamp") {
       unsupported("LOAD of " + lc.type + " columns (" + lc.name + ")");
+    } else {  // every other type name is a char column of the declared width (cm.cu:3006-3012)
+      if (lc.size <= 0) unsupported("LOAD of a char column without a width (" + lc.name + ")");
+      cols[i].kind = ALK_TEXT_CHAR;
+      cols[i].width = (uint32_t)lc.size;
     }
   }
   const std::string path = !st.f.empty() && st.f[0] == '/' ? st.f : dir_ + "/" + st.f;
@@ -1805,15 +1869,20 @@ void Engine::emit_load(Statement& st) {
   out->kind = Var::Mat;
   out->name = st.s;
   out->n = rows;
-  std::vector<int64_t*> dst;
-  for (auto& lc : st.load_cols) {
-    auto b = mkbuf(std::max<uint64_t>(rows, 1) * 8, stream_);
+  std::vector<void*> dst;
+  for (size_t i = 0; i < st.load_cols.size(); i++) {
+    const LoadCol& lc = st.load_cols[i];
+    const bool chr = cols[i].kind == ALK_TEXT_CHAR;
+    auto b = mkbuf(std::max<uint64_t>(rows, 1) * (chr ? cols[i].width : 8), stream_);
     out->data[lc.name] = b;
-    dst.push_back(b->as<int64_t>());
+    dst.push_back(b->as<void>());
     out->columnNames.push_back(lc.name);
     ColMeta m;
-    m.type = 0;
+    m.type = chr ? 2 : 0;
     m.dz = lc.type == "decimal" ? (uint32_t)std::max(lc.size, 0) : 0;  // decimal_zeroes (cm.cu:3000-3005)
+    m.width = chr ? cols[i].width : 0;
+    m.raw = chr;
+    m.no_encoding = chr && lc.no_encoding;
     out->meta[lc.name] = m;
   }
   uint64_t got = 0;

@@ -61,6 +61,7 @@ queue<string> namevars;
 queue<string> typevars;
 queue<int> sizevars;
 queue<int> cols;
+queue<char> encvars;  // emit_varchar's encoding ('N': NO ENCODING), beside the other var queues
 queue<unsigned int> j_col_count;
 unsigned int sel_count = 0;
 unsigned int join_cnt = 0;
@@ -164,7 +165,9 @@ void capture(alk::StmtKind kind, const char* s, const char* f, const char* sep, 
     st.op_case = op_case;
     if (kind == alk::StmtKind::Load)  // the AS list: emit_var / emit_varchar / emit_vardecimal
       while (!namevars.empty() && !typevars.empty() && !sizevars.empty() && !cols.empty()) {
-        st.load_cols.push_back({namevars.front(), cols.front(), typevars.front(), sizevars.front()});
+        const bool no_enc = !encvars.empty() && encvars.front() == 'N';
+        st.load_cols.push_back({namevars.front(), cols.front(), typevars.front(), sizevars.front(), no_enc});
+        if (!encvars.empty()) encvars.pop();
         namevars.pop();
         typevars.pop();
         sizevars.pop();
@@ -290,6 +293,7 @@ void emit_var(const char* s, const int c, const char* f, const char* ref, const 
   typevars.push(f);
   sizevars.push(0);
   cols.push(c);
+  encvars.push(0);
 }
 void emit_var_asc(const char* s) {
   op_type.push(s);
@@ -305,12 +309,14 @@ void emit_varchar(const char* s, const int c, const char* f, const int d, const 
   typevars.push(f);
   sizevars.push(d);
   cols.push(c);
+  encvars.push(encoding ? encoding[0] : 0);
 }
 void emit_vardecimal(const char* s, const int c, const char* f, const int scale, const int precision) {
   namevars.push(s);
   typevars.push(f);
   sizevars.push(precision);
   cols.push(c);
+  encvars.push(0);
 }
 namespace {
 bool g_store_sort = false;  // SORT SEGMENTS BY / PRESORTED BY seen for the current STORE
@@ -371,6 +377,7 @@ void clean_queues() {
   while (!namevars.empty()) namevars.pop();
   while (!typevars.empty()) typevars.pop();
   while (!sizevars.empty()) sizevars.pop();
+  while (!encvars.empty()) encvars.pop();
   while (!cols.empty()) cols.pop();
   while (!op_sort.empty()) op_sort.pop();
   while (!op_presort.empty()) op_presort.pop();

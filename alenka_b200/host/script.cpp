@@ -478,6 +478,7 @@ class Parser {
     if (is_kw("NO")) {
       take();
       expect_kw("ENCODING");
+      lc.no_encoding = true;
     }
     cur_->load_cols.push_back(lc);
   }

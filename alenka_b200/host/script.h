@@ -34,6 +34,7 @@ struct LoadCol {
   int field = 0;
   std::string type;
   int size = 0;
+  bool no_encoding = false;  // varchar(n) NO ENCODING: every value its own code
 };
 
 struct Statement {

@@ -290,19 +290,26 @@ int alk_narrow_u32(const int64_t* d_in, uint64_t n, uint32_t* d_out, alk_stream 
  * dropped) and is cut to 23 bytes; it is parsed as an integer (ALK_TEXT_INT: leading
  * spaces, a sign, digits), a decimal of `scale` <= 9 fraction digits (ALK_TEXT_DECIMAL:
  * value x 10^scale, digits past the scale ignored), or, when the first record's field
- * has '-' at offset 4, as a yyyy-mm-dd date (yyyymmdd; *h_date_mask bit i). d_out[i]:
- * int64 device column of out_cap values; *h_rows gets the record count (ALK_ERR_OVERFLOW
- * when above out_cap). h_text is host memory; synchronises. */
+ * has '-' at offset 4, as a yyyy-mm-dd date (yyyymmdd; *h_date_mask bit i); a char
+ * column (ALK_TEXT_CHAR) keeps the field's bytes, NUL bytes dropped, cut or zero-padded
+ * to its width. d_out[i]: device column of out_cap int64 values, or of out_cap x width
+ * bytes for a char column; *h_rows gets the record count (ALK_ERR_OVERFLOW when above
+ * out_cap). h_text is host memory; synchronises. */
 typedef struct alk_text_col {
   uint32_t field;  /* 1-based field number as declared */
-  uint32_t kind;   /* ALK_TEXT_INT or ALK_TEXT_DECIMAL */
+  uint32_t kind;   /* ALK_TEXT_INT, ALK_TEXT_DECIMAL or ALK_TEXT_CHAR */
   uint32_t scale;  /* decimal: digits after the point */
-  uint32_t pad;
+  uint32_t width;  /* char: bytes a value (the field, NUL bytes dropped, zero-padded) */
 } alk_text_col;
 #define ALK_TEXT_INT 0
 #define ALK_TEXT_DECIMAL 1
+#define ALK_TEXT_CHAR 2
 int alk_text_load(const char* h_text, uint64_t nbytes, char sep, const alk_text_col* cols, uint32_t ncols,
-                  int64_t* const* d_out, uint64_t out_cap, uint64_t* h_rows, uint32_t* h_date_mask, alk_stream stream);
+                  void* const* d_out, uint64_t out_cap, uint64_t* h_rows, uint32_t* h_date_mask, alk_stream stream);
+/* MurmurHash64A(value, width, seed) / 2 of n fixed-width values (the .hash file of a char
+ * column, compress_char cm.cu:1765-1844; the reference hashes with seed 100). */
+int alk_hash_strings(const uint8_t* d_chars, uint64_t n, uint32_t width, uint32_t seed, uint64_t* d_out,
+                     alk_stream stream);
 /* Frame-of-reference re-encoding of n int64 values: the exact minimum goes to *h_lower,
  * the narrowest of 8/16/32/64 bits that holds every value less it to *h_bits, and the
  * values less the minimum at that width to d_out (out_cap bytes; ALK_ERR_OVERFLOW when

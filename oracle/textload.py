@@ -11,18 +11,21 @@ whose first record's slot has '-' at offset 4 is read as yyyy-mm-dd dates."""
 SLOT = 23
 
 
-def _cut(text, pos, sep, fields):
-    """The slots of the requested 0-based fields (ascending) of the record at pos."""
+def _cut(text, pos, sep, fields, widths=None):
+    """The slots of the requested 0-based fields (ascending) of the record at pos: the
+    field's bytes, NUL bytes dropped, cut or zero-padded to the slot's width (23 bytes,
+    or widths[i])."""
     out, cur, want, j, quoted, n = [], 0, 0, pos, False, len(text)
     while want < len(fields):
         keep = fields[want] == cur
-        slot = bytearray(SLOT)
+        w = widths[want] if widths else SLOT
+        slot = bytearray(w)
         t = 0
         while j < n and (text[j] != sep or quoted):
             ch = text[j]
             if ch == 0x22:
                 quoted = not quoted
-            if keep and ch != 0 and t < SLOT:
+            if keep and ch != 0 and t < w:
                 slot[t] = ch
                 t += 1
             j += 1
@@ -87,8 +90,9 @@ def parse_date(s):
 
 
 def load(text, sep, cols):
-    """cols: [(field (1-based), kind 'int' | 'decimal', scale)] in declared order.
-    Returns one list of int64 values per declared column."""
+    """cols: [(field (1-based), kind 'int' | 'decimal' | 'char', scale or width)] in
+    declared order. Returns one list per declared column: int64 values, or the char
+    column's width-byte values."""
     sepb = sep.encode()[0] if isinstance(sep, str) else sep
     fields = sorted(f - 1 for f, _, _ in cols)
     starts, p = [], 0
@@ -98,12 +102,17 @@ def load(text, sep, cols):
             p = i + 1
     if not starts:
         return [[] for _ in cols]
-    first = _cut(text, 0, sepb, fields)
-    date = [first[i][4] == 0x2D for i in range(len(cols))]
+    widths = [scale if kind == "char" else SLOT for _, kind, scale in cols]
+    first = _cut(text, 0, sepb, fields, widths)
+    date = [cols[i][1] != "char" and first[i][4] == 0x2D for i in range(len(cols))]
     out = [[] for _ in cols]
     for st in starts:
-        slots = _cut(text, st, sepb, fields)
+        slots = _cut(text, st, sepb, fields, widths)
         for i, (_, kind, scale) in enumerate(cols):
             s = slots[i]
-            out[i].append(parse_date(s) if date[i] else parse_decimal(s, scale) if kind == "decimal" else parse_int(s))
+            if kind == "char":
+                out[i].append(s)
+            else:
+                out[i].append(parse_date(s) if date[i] else parse_decimal(s, scale) if kind == "decimal"
+                              else parse_int(s))
     return out

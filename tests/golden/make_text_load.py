@@ -42,7 +42,7 @@ def main():
                 raise SystemExit(f"{name}: reference failed: {r.stdout[-400:]} {r.stderr[-400:]}")
         files = {}
         for fn in sorted(os.listdir(d)):
-            if fn.startswith(case["table"] + ".") or fn.endswith("_q.txt"):
+            if fn.startswith(case["table"] + ".") or fn == case["table"] or fn.endswith("_q.txt"):
                 files[fn] = sha(open(os.path.join(d, fn), "rb").read())
         out[name] = {"text_sha256": sha(text), "files": files}
     with open(os.path.join(HERE, "text_load.json"), "w") as f:

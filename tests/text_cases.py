@@ -47,7 +47,37 @@ CASES["field_order"] = {
                 "STORE T INTO 'tord' BINARY;\n"],
     "table": "tord",
 }
+def _char_text(seed, rows):
+    r = random.Random(seed)
+    # quoted values keep their quotes: every value, quotes included, fits the 12-byte width
+    # (a longer one runs past its slot into the next record's in the reference, an
+    # overflow whose outcome depends on the order its threads take the records)
+    names = ["alpha", "beta", "gamma|x", "delta", "", "omega-name", "zeta"]
+    lines = []
+    for i in range(rows):
+        flag = r.choice("ANR")
+        nm = r.choice(names)
+        nm_txt = f'"{nm}"' if "|" in nm or r.random() < 0.2 else nm
+        code = "".join(r.choice("XYZ") for _ in range(r.randint(1, 9)))
+        lines.append(f"{i + 1}|{flag}|{nm_txt}|{r.randint(1, 50)}|{code}|")
+    return "\n".join(lines) + "\n"
+
+
+CASES["chars"] = {
+    # char columns: a flag, names (quoted ones hold the separator; the quotes stay in
+    # the value), a NO ENCODING column
+    "text": lambda: _char_text(10, 3000),
+    "scripts": ["T := LOAD 'chars.tbl' USING ('|') AS (k{1}:int, f{2}:varchar(1), nm{3}:varchar(12), "
+                "q{4}:int, cd{5}:varchar(8) NO ENCODING);\n"
+                "STORE T INTO 'tch' BINARY;\n",
+                "F := FILTER tch BY q > 10;\n"
+                "R := SELECT f AS f, nm AS nm, SUM(q) AS sq, COUNT(k) AS c FROM F GROUP BY f, nm;\n"
+                "STORE R INTO 'tch_q.txt' USING ('|');\n"],
+    "table": "tch",
+}
+
+
 # A file whose last line has no newline: the reference counts 299 records of 300 lines
 # and then aborts in free() (invalid pointer), so there is no golden output for it; the
 # engine's record count for it is tested on its own.
-FILES = {"numeric": "numeric.tbl", "field_order": "order.tbl"}
+FILES = {"numeric": "numeric.tbl", "field_order": "order.tbl", "chars": "chars.tbl"}
