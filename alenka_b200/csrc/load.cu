@@ -244,13 +244,7 @@ int alk_text_load(const char* h_text, uint64_t nbytes, char sep, const alk_text_
     if (cols[c].kind == ALK_TEXT_DECIMAL && cols[c].scale > 9) return ALK_ERR_UNSUPPORTED;
     if (cols[c].kind == ALK_TEXT_CHAR && cols[c].width == 0) return ALK_ERR_ARG;
   }
-  // records: the newline-terminated lines (text after the last newline is not a record)
-  uint64_t rows = 0;
-  for (const char* p = h_text; (p = (const char*)std::memchr(p, '\n', (size_t)(h_text + nbytes - p))) != nullptr; p++)
-    rows++;
-  *h_rows = rows;
-  if (rows > out_cap) return ALK_ERR_OVERFLOW;
-  if (rows == 0) return ALK_OK;
+  if (nbytes == 0) return ALK_OK;
   TextArgs a{};
   a.n = nbytes;
   a.sep = sep;
@@ -273,7 +267,7 @@ int alk_text_load(const char* h_text, uint64_t nbytes, char sep, const alk_text_
   const size_t off_off = off_cnt + ((threads * 8 + 255) & ~size_t(255));
   const size_t off_pos = off_off + ((threads * 8 + 255) & ~size_t(255));
   uint8_t* db = nullptr;
-  CK(cudaMallocAsync((void**)&db, off_pos + rows * 8, s));
+  CK(cudaMallocAsync((void**)&db, off_pos, s));
   CK(cudaMemcpyAsync(db, h_text, nbytes, cudaMemcpyHostToDevice, s));
   a.text = (const char*)db;
   const unsigned blocks = (unsigned)((threads + kT - 1) / kT);
@@ -289,15 +283,25 @@ int alk_text_load(const char* h_text, uint64_t nbytes, char sep, const alk_text_
     x = run;
     run += v;
   }
+  // records: the newline-terminated lines (text after the last newline is not a record)
+  const uint64_t rows = run;
+  *h_rows = rows;
+  if (rows > out_cap || rows == 0) {
+    CK(cudaFreeAsync(db, s));
+    CK(cudaStreamSynchronize(s));
+    return rows > out_cap ? ALK_ERR_OVERFLOW : ALK_OK;
+  }
+  unsigned long long* nl = nullptr;
+  CK(cudaMallocAsync((void**)&nl, rows * 8, s));
   CK(cudaMemcpyAsync(db + off_off, cnt.data(), threads * 8, cudaMemcpyHostToDevice, s));
-  k_nl_write<<<blocks, kT, 0, s>>>(a.text, nbytes, (const unsigned long long*)(db + off_off),
-                                   (unsigned long long*)(db + off_pos));
-  a.nl = (const unsigned long long*)(db + off_pos);
+  k_nl_write<<<blocks, kT, 0, s>>>(a.text, nbytes, (const unsigned long long*)(db + off_off), nl);
+  a.nl = nl;
   a.rows = rows;
   const int grid = (int)std::min<uint64_t>((rows + kT - 1) / kT, 148ull * 16);
   k_text_parse<<<grid, kT, 0, s>>>(a);
   alk::g_kernel_launches += 3;
   CK(cudaGetLastError());
+  CK(cudaFreeAsync(nl, s));
   CK(cudaFreeAsync(db, s));
   CK(cudaStreamSynchronize(s));
   return ALK_OK;

@@ -670,7 +670,7 @@ def main():
     ap.add_argument("--fused-only", action="store_true",
                     help="time only the resident fused plan (profiling runs)")
     ap.add_argument("--workload", default="three_way",
-                    choices=["three_way", "batched", "groupby_high", "encode", "compressed", "estimator"],
+                    choices=["three_way", "batched", "groupby_high", "encode", "compressed", "estimator", "load"],
                     help="three_way: the filter -> join -> group-by pipeline (default); batched: many "
                          "single-table filter + group-by queries per step; compressed: the three-way on "
                          "FOR-delta tables with Zipf(1.1) join keys")
@@ -693,10 +693,10 @@ def main():
         return
     import torch
     torch.cuda.set_device(local)
-    if args.workload in ("batched", "groupby_high", "encode", "compressed", "estimator"):
+    if args.workload in ("batched", "groupby_high", "encode", "compressed", "estimator", "load"):
         if rank == 0:
             {"batched": run_batched, "groupby_high": run_groupby_high, "encode": run_encode,
-             "compressed": run_compressed, "estimator": run_estimator}[args.workload](args, torch)
+             "compressed": run_compressed, "estimator": run_estimator, "load": run_load}[args.workload](args, torch)
         return
     dist = None
     if world > 1:
@@ -833,6 +833,52 @@ def run_estimator(args, torch):
         "loss": {"first_epoch": l_first, "last_epoch": l_last},
         "seconds": {"record": record_s, "train": train_s},
         "first_runs": first, "verified": {"results_identical": True}}), flush=True)
+
+
+def run_load(args, torch):
+    """The text loader: a lineitem-shaped table (60M rows x scale, generated in device
+    memory) is stored as a '|'-separated text file, then each step LOADs it (the file read
+    from the page cache, copied to the device and parsed there: integers, decimals, char
+    columns) and the device part of the load is timed with CUDA events on the session's
+    stream; e2e is the whole LOAD statement's wall time."""
+    import alenka_b200 as ab
+    rows = int(60_000_000 * args.scale)
+    seg = 10_000_000
+    segs = [seg] * (rows // seg) + ([rows % seg] if rows % seg else [])
+    d = tempfile.mkdtemp(prefix="alenka_load_")
+    with ab.Session(d, resident=True) as s:
+        s.gen_flat_resident("lineitem", segs, args.seed)
+        s.execute("STORE lineitem INTO 'lineitem.tbl' USING ('|');\n")
+    nbytes = os.path.getsize(os.path.join(d, "lineitem.tbl"))
+    script = ("T := LOAD 'lineitem.tbl' USING ('|') AS (k{1}:int, q{2}:int, p{3}:decimal(12,2), "
+              "dc{4}:decimal(4,2), sd{5}:int, rf{6}:varchar(1), ls{7}:varchar(1));\n")
+    sess = ab.Session(d, resident=True)
+    for _ in range(max(1, args.warmup)):
+        sess.execute(script)
+    stream = torch.cuda.ExternalStream(sess.stream)
+    steps = max(1, args.steps // 4)
+    walls, devs = [], []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        sess.execute(script)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        walls.append((time.perf_counter() - t0) * 1000.0)
+        devs.append(e0.elapsed_time(e1))
+    sess.close()
+    wall = statistics.median(walls)
+    print(json.dumps({
+        "metric": "text loader: fact rows/s parsed (LOAD ... USING ('|') AS (...))", "value": rows / (wall / 1000.0),
+        "unit": "rows/s", "n_gpus": 1, "steps": steps, "higher_is_better": True, "dtype": "int64 / char",
+        "data": "synthetic (a device-generated lineitem shape stored as text)",
+        "config": {"workload": f"lineitem text, {rows} rows, {nbytes} bytes, 7 columns (2 int, 2 decimal, 1 "
+                               "yyyymmdd int, 2 char(1))"},
+        "ms_per_load": wall, "text_gb_per_s": nbytes / (wall / 1000.0) / 1e9,
+        "note": "the LOAD statement end to end: file read from the page cache, host newline count, copy to the "
+                "device, newline positions and the parse on the device"}), flush=True)
 
 
 def run_compressed(args, torch):
