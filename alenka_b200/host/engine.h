@@ -285,6 +285,7 @@ class Engine {
   void emit_load(Statement& st);
   DevBufP like_set(Var* base, const std::string& col, const std::string& pattern);
   const DevBufP& dict_ranks(const ColMeta& m);
+  DevBufP dict_hashes(const ColMeta& m, uint32_t width);
   std::map<std::string, uint32_t> cnt_counts_;  // largest payload written per column file prefix
   // codes of a LOAD's char values per column name: hash -> code (key 0: NO ENCODING's
   // running count), kept for the session as the reference keeps its char_hash

@@ -1441,9 +1441,14 @@ void Engine::multijoin(Statement& st, const std::string& s, const std::string& j
     throw EngineError(ALK_ERR_ARG, "Couldn't find column " + f1);
   }
   if (left->meta[colname1].type != right->meta[colname2].type) unsupported("join of different column types");
-  // char keys are dictionary codes: codes of two different dictionaries do not compare
-  if (left->meta[colname1].type == 2 && left->meta[colname1].string_map != right->meta[colname2].string_map)
-    unsupported("join on char columns of different dictionaries");
+  // Char keys are dictionary codes. Codes of one dictionary compare as they are; the
+  // reference compares codes of two different dictionaries too, which matches nothing in
+  // particular. Here such keys compare by value: each row's key becomes the
+  // MurmurHash64A / 2 of its value zero-padded to the wider of the two widths (the form
+  // of the reference's .hash files, filter.cu:428-449 and cm.cu:1808-1812).
+  const bool by_value = left->meta[colname1].type == 2 &&
+                        left->meta[colname1].string_map != right->meta[colname2].string_map;
+  if (by_value && kind != 'I') unsupported("semi / anti join on char columns of different dictionaries");
   // a left semi / anti join outputs left rows only, a right one right rows only (the
   // reference gathers the other side through pairs it has since reordered)
   const bool left_rows = kind == '1' || kind == '3', right_rows = kind == '2' || kind == '4';
@@ -1468,9 +1473,22 @@ void Engine::multijoin(Statement& st, const std::string& s, const std::string& j
     vars_[s] = std::move(c);
     return;
   }
+  DevBufP lkey = L.col.count(colname1) ? L.col.at(colname1) : nullptr, rkey = R.col.count(colname2) ? R.col.at(colname2) : nullptr;
+  if (by_value && R.n && L.n) {
+    const uint32_t w = std::max(left->meta[colname1].width, right->meta[colname2].width);
+    auto keyed = [&](const DevBufP& codes, uint64_t n, const ColMeta& m) {
+      DevBufP h = dict_hashes(m, w), k = mkbuf(n * 8, stream_);
+      auto idx = mkbuf(n * 4, stream_);
+      check(alk_narrow_u32(codes->as<int64_t>(), n, idx->as<uint32_t>(), (alk_stream)stream_), "codes");
+      check(alk_gather(h->as<int64_t>(), idx->as<uint32_t>(), n, k->as<int64_t>(), (alk_stream)stream_), "key hash");
+      return k;
+    };
+    lkey = keyed(L.col.at(colname1), L.n, left->meta[colname1]);
+    rkey = keyed(R.col.at(colname2), R.n, right->meta[colname2]);
+  }
   if (R.n && L.n) {
     alk_join_table* t = nullptr;
-    check(alk_join_build(R.col.at(colname2)->as<int64_t>(), R.n, &t, (alk_stream)stream_), "join build");
+    check(alk_join_build(rkey->as<int64_t>(), R.n, &t, (alk_stream)stream_), "join build");
     struct TableGuard {
       alk_join_table* t;
       cudaStream_t s;
@@ -1481,8 +1499,8 @@ void Engine::multijoin(Statement& st, const std::string& s, const std::string& j
     for (int attempt = 0; attempt < 2; attempt++) {
       pl = mkbuf(cap * 4, stream_);
       pr = mkbuf(cap * 4, stream_);
-      int rc = alk_join_probe(t, L.col.at(colname1)->as<int64_t>(), L.n, pl->as<uint32_t>(), pr->as<uint32_t>(), cap,
-                              &pairs, (alk_stream)stream_);
+      int rc = alk_join_probe(t, lkey->as<int64_t>(), L.n, pl->as<uint32_t>(), pr->as<uint32_t>(), cap, &pairs,
+                              (alk_stream)stream_);
       if (rc == ALK_ERR_OVERFLOW && attempt == 0) {
         cap = pairs;
         continue;
@@ -1568,6 +1586,27 @@ void Engine::emit_order(Statement& st) {
     for (auto& n : a->columnNames) b->data[n] = mkbuf(8, stream_);
   }
   vars_[st.s] = std::move(b);
+}
+
+// MurmurHash64A / 2 of a char column's dictionary entries, each zero-padded to `width`
+// bytes, on the device (index: the code): keys that compare two dictionaries' values.
+DevBufP Engine::dict_hashes(const ColMeta& m, uint32_t width) {
+  const auto dot = m.string_map.find('.');
+  Var* b = dot == std::string::npos ? nullptr : base_table(m.string_map.substr(0, dot));
+  if (!b) throw EngineError(ALK_ERR_IO, "missing dictionary " + m.string_map);
+  BaseCol& bc = basecol(b, m.string_map.substr(dot + 1));
+  load_dict(b, m.string_map.substr(dot + 1), bc);
+  const size_t n = bc.dict.size();
+  std::vector<uint8_t> raw(std::max<size_t>(n, 1) * width, 0);
+  for (size_t i = 0; i < n; i++) std::memcpy(&raw[i * width], bc.dict[i].data(), std::min<size_t>(width, bc.dict[i].size()));
+  auto d_raw = mkbuf(raw.size(), stream_);
+  ck(cudaMemcpyAsync(d_raw->as<void>(), raw.data(), raw.size(), cudaMemcpyHostToDevice, stream_), "dictionary h2d");
+  stats_.h2d_bytes += raw.size();
+  auto h = mkbuf(std::max<size_t>(n, 1) * 8, stream_);
+  check(alk_hash_strings(d_raw->as<uint8_t>(), n, width, kHashSeed, h->as<uint64_t>(), (alk_stream)stream_),
+        "dictionary hash");
+  ck(cudaStreamSynchronize(stream_), "dictionary hash");
+  return h;
 }
 
 // Dense ranks of a char column's dictionary entries in byte order (unsigned, full

@@ -104,3 +104,52 @@ def test_records_are_newline_terminated_lines():
     from oracle import textload
     text = b"1|2|\n3|4|\n5|6"
     assert textload.load(text, "|", [(1, "int", 0), (2, "int", 0)]) == [[1, 3], [2, 4]]
+
+
+@pytest.mark.gpu
+def test_join_on_char_keys_of_two_dictionaries(tmp_path):
+    """A string-key join between tables whose char columns have different dictionaries
+    (different names, widths 25 and 20, values first seen in different orders): the
+    engine compares the values (MurmurHash64A of each value padded to the wider width)
+    where the reference would compare the two dictionaries' codes. Checked against the
+    join computed by string equality."""
+    import random
+    import alenka_b200 as ab
+    d = str(tmp_path)
+    r = random.Random(5)
+    alnum = "ABCDEFGHIJKLMNOPQRSTUVWXYZ0123456789"
+    names = ["".join(r.choice(alnum) for _ in range(r.randint(4, 20))) for _ in range(800)]
+    names = sorted(set(names))
+    segs = {n: r.choice(["AUTO", "BUILD", "FURN"]) for n in names}
+    cust = list(names)
+    r.shuffle(cust)
+    with open(os.path.join(d, "cust.tbl"), "w") as f:
+        for n in cust:
+            f.write(f"{n}|{segs[n]}|\n")
+    orders = []
+    with open(os.path.join(d, "ord.tbl"), "w") as f:
+        for i in range(6000):
+            n = r.choice(names) if r.random() < 0.9 else "NOPE" + str(i % 7)
+            amt = r.randint(1, 1000)
+            orders.append((n, amt))
+            f.write(f"{i}|{n}|{amt}|\n")
+    with ab.Session(d) as s:
+        s.execute("C := LOAD 'cust.tbl' USING ('|') AS (c_name{1}:varchar(25), c_seg{2}:varchar(8));\n"
+                  "STORE C INTO 'cust' BINARY;\n"
+                  "O := LOAD 'ord.tbl' USING ('|') AS (o_id{1}:int, o_cname{2}:varchar(20), o_amt{3}:int);\n"
+                  "STORE O INTO 'ord' BINARY;\n")
+    with ab.Session(d) as s:
+        s.execute("J := SELECT c_seg AS seg, o_amt AS amt FROM ord JOIN cust ON o_cname = c_name;\n"
+                  "R := SELECT seg AS seg, SUM(amt) AS s, COUNT(amt) AS c FROM J GROUP BY seg;\n"
+                  "STORE R INTO 'j.txt' USING ('|');\n")
+    got = set()
+    for line in open(os.path.join(d, "j.txt"), "rb").read().decode().splitlines():
+        seg, sm, cnt = line.split("|")[:3]
+        got.add((seg.rstrip("\x00"), int(sm), int(cnt)))
+    want = {}
+    for n, amt in orders:
+        if n in segs:
+            k = segs[n]
+            s_, c_ = want.get(k, (0, 0))
+            want[k] = (s_ + amt, c_ + 1)
+    assert got == {(k, v[0], v[1]) for k, v in want.items()}
