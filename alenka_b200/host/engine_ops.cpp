@@ -2437,7 +2437,8 @@ bool Engine::hash_select(Statement& st) {
     int64_t prev_hi = INT64_MIN;
     for (uint32_t g = 0; ordered && g < src->segCount; g++) {
       if (!p.mode[g]) continue;
-      if (kb.segs[g].m.comp_type != 0 || kb.segs[g].m.lower < prev_hi) ordered = false;
+      // ascending: the header bounds are the segment's first and last values
+      if (kb.segs[g].m.lower < prev_hi) ordered = false;
       prev_hi = kb.segs[g].m.upper;
     }
     if (ordered) return fail();
@@ -2830,11 +2831,10 @@ void Engine::run_fused(Statement& J, Statement& F, Statement& O, Statement& S, c
     if (cs.size() < (size_t)p.slots.size() * p.src->segCount) return false;
     for (auto& c : payload)
       if (!p.src->has(c)) return false;  // carried from the inner table
-    // exact zone bounds: FOR headers hold the segment's minimum and maximum
+    // exact zone bounds: a FOR header holds the segment's minimum and maximum, a FOR-delta
+    // header its first and last value, the same in an ascending segment (checked below)
     BaseCol& kb = basecol(p.src, build_key);
     read_headers(p.src, build_key, kb);
-    for (auto& sg : kb.segs)
-      if (sg.m.comp_type != 0) return false;
     const uint32_t nseg = p.src->segCount;
     // the candidates' rows are found by binary search: the key column must be ascending
     // in every scanned segment (checked once per resident segment, outside a capture)
