@@ -871,6 +871,25 @@ def run_load(args, torch):
         devs.append(e0.elapsed_time(e1))
     sess.close()
     wall = statistics.median(walls)
+    # beside it: the reference's own LOAD + STORE BINARY (built for the CPU) on the file's
+    # first 2M records, the bounded sample
+    cpu = None
+    if os.path.exists(REF_BIN) and not args.no_cpu_baseline:
+        rd = os.path.join(d, "ref")
+        os.makedirs(rd, exist_ok=True)
+        sample = 2_000_000
+        with open(os.path.join(d, "lineitem.tbl"), "rb") as src, open(os.path.join(rd, "lineitem.tbl"), "wb") as dst:
+            for k, line in enumerate(src):
+                if k == sample:
+                    break
+                dst.write(line)
+        ref_script = script + "STORE T INTO 'tl' BINARY;\n"
+        threads = os.cpu_count() or 1
+        run_reference_binary(rd, ref_script, threads)  # page cache warm
+        dt = run_reference_binary(rd, ref_script, threads)
+        cpu = {"value": sample / dt, "unit": "rows/s", "cores": threads, "kind": "reference",
+               "sample": f"the reference's CLI built for the CPU: LOAD + STORE BINARY of the file's first {sample} "
+                         f"records, {dt:.2f} s (the engine's figure above is the LOAD alone)"}
     print(json.dumps({
         "metric": "text loader: fact rows/s parsed (LOAD ... USING ('|') AS (...))", "value": rows / (wall / 1000.0),
         "unit": "rows/s", "n_gpus": 1, "steps": steps, "higher_is_better": True, "dtype": "int64 / char",
@@ -879,7 +898,8 @@ def run_load(args, torch):
                                "yyyymmdd int, 2 char(1))"},
         "ms_per_load": wall, "text_gb_per_s": nbytes / (wall / 1000.0) / 1e9,
         "note": "the LOAD statement end to end: file read from the page cache, host newline count, copy to the "
-                "device, newline positions and the parse on the device"}), flush=True)
+                "device, newline positions and the parse on the device",
+        "cpu_baseline": cpu}), flush=True)
 
 
 def run_compressed(args, torch):
