@@ -17,10 +17,11 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SRCS = ["csrc/kernels.cu", "csrc/pipeline.cu", "csrc/card.cu", "csrc/batch.cu", "csrc/gen.cu",
-            "csrc/encode.cu", "csrc/strings.cu", "csrc/frontend_state.cu", "csrc/load.cu"]
+            "csrc/encode.cu", "csrc/strings.cu", "csrc/frontend_state.cu", "csrc/load.cu",
+            "csrc/star.cu"]
 CPP_SRCS = ["host/format.cpp", "host/script.cpp", "host/engine.cpp", "host/engine_ops.cpp",
             "host/capi.cpp", "host/gen.cpp", "host/card.cpp", "host/resident.cpp", "host/frontend_abi.cpp",
-            "host/frontend_embed.cpp"]
+            "host/frontend_embed.cpp", "host/star.cpp"]
 
 
 def _run(cmd):

@@ -229,7 +229,7 @@ extern "C" int alk_parse_dump(const char* script, char* out, int out_len) {
     if (out && out_len > 0) std::snprintf(out, (size_t)out_len, "ERROR %s", err.c_str());
     return ALK_ERR_PARSE;
   }
-  static const char* kinds[] = {"FILTER", "SELECT", "JOIN", "ORDER", "STORE", "STORE_BINARY", "DISPLAY", "LOAD", "OTHER"};
+  static const char* kinds[] = {"FILTER", "SELECT", "JOIN", "ORDER", "STORE", "STORE_BINARY", "DISPLAY", "LOAD", "OTHER", "CREATE_BITMAP_INDEX"};
   std::string s;
   for (auto& st : sts) {
     s += kinds[(int)st.kind];
@@ -245,6 +245,10 @@ extern "C" int alk_parse_dump(const char* script, char* out, int out_len) {
     for (size_t i = 0; i < st.op_join.size(); i++) s += " " + st.op_join[i] + "/" + std::string(1, st.join_type[i]);
     s += " sel=" + std::to_string(st.sel_count) + " tabs=" + std::to_string(st.join_tab_cnt) + " and:";
     for (auto& kv : st.join_and_cnt) s += " " + std::to_string(kv.first) + "=" + std::to_string(kv.second);
+    if (!st.index_args.empty()) {
+      s += "\n index:";
+      for (auto& x : st.index_args) s += " " + x;
+    }
     s += "\n";
   }
   if (out && out_len > 0) std::snprintf(out, (size_t)out_len, "%s", s.c_str());

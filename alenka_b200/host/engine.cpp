@@ -219,6 +219,7 @@ Engine::Engine(std::string dir, uint32_t flags) : dir_(std::move(dir)), flags_(f
 
 Engine::~Engine() {
   vars_.clear();
+  star_sets_.clear();  // device buffers free on the stream, destroyed below
   for (auto& t : basecols_)
     for (auto& c : t.second) {
       for (auto* h : c.second.host_img)
@@ -297,12 +298,16 @@ Var* Engine::base_table(const std::string& t) {
 
 BaseCol& Engine::basecol(Var* base, const std::string& col) {
   BaseCol& bc = basecols_[base->table][col];
-  bc.meta = base->meta.at(col);
+  if (col.find('.') == std::string::npos) bc.meta = base->meta.at(col);  // else a bitmap index column
   return bc;
 }
 
 void Engine::read_headers(Var* base, const std::string& col, BaseCol& bc) {
   if (bc.headers_read) return;
+  if (col.find('.') != std::string::npos) {  // a bitmap join index column
+    load_star_index(base, col, bc);
+    return;
+  }
   bc.segs.resize(base->segCount);
   bc.host_img.assign(base->segCount, nullptr);
   bc.host_len.assign(base->segCount, 0);
@@ -699,7 +704,15 @@ alk_program Engine::compile_filter(Var* f, Var* src, std::vector<std::string>& s
       } else if ((s1 == "STRING" && s2 == "NAME") || (s1 == "NAME" && s2 == "STRING")) {
         std::string v1 = pop(ev), v2 = pop(ev);
         if (s1 == "NAME") std::swap(v1, v2);  // v1 literal, v2 column
-        if (v2.find('.') != std::string::npos) unsupported("bitmap-index predicates");
+        if (v2.find('.') != std::string::npos) {
+          // a bitmap join index column: the literal's hash looked up in each segment's
+          // dictionary, == keeps its code and any other operator the other codes
+          // (filter.cu:397-415)
+          const DevBufP set = star_set(src, v2, cmp == 4, star_string_key(v2, v1));
+          bools.push_back(b.emit(ALK_OP_INSET, slot(v2), b.konst((int64_t)(uintptr_t)set->as<void>())));
+          et.push_back("NAME");
+          continue;
+        }
         if (cmp != 4 && cmp != 3 && cmp != 7) unsupported("string comparison other than == / != / LIKE");
         if (!src->has(v2) || src->meta[v2].type != 2) unsupported("string compared with a non-char column");
         if (cmp == 7) {
@@ -719,6 +732,16 @@ alk_program Engine::compile_filter(Var* f, Var* src, std::vector<std::string>& s
         auto it = bc.hash_to_code.find(h);
         int64_t code = it == bc.hash_to_code.end() ? -1 : it->second;
         bools.push_back(b.emit(cmp == 4 ? ALK_OP_EQ : ALK_OP_NE, slot(v2), b.konst(code)));
+        et.push_back("NAME");
+      } else if ((s1 == "NUMBER" && s2 == "NAME" && ev.back().find('.') != std::string::npos) ||
+                 (s1 == "NAME" && s2 == "NUMBER" && ev.back().find('.') != std::string::npos)) {
+        // a bitmap join index column against a number: the number itself looked up in each
+        // segment's dictionary (filter.cu:519-535, 560-577); the number's precision stays
+        // on the precision stack, as the reference pops and pushes none there
+        int64_t n1 = pop(en);
+        std::string v = pop(ev);
+        const DevBufP set = star_set(src, v, cmp == 4, n1);
+        bools.push_back(b.emit(ALK_OP_INSET, slot(v), b.konst((int64_t)(uintptr_t)set->as<void>())));
         et.push_back("NAME");
       } else if (s1 == "NUMBER" && s2 == "NAME") {
         int64_t n1 = pop(en);
@@ -807,6 +830,7 @@ Rows Engine::materialize(Var* v, const std::vector<std::string>& fields, bool wa
   bool have_prog = false;
   std::vector<uint8_t> mode(src->segCount, 1);
   if (v->kind == Var::Filtered) {
+    v->scanned = true;
     std::vector<char> zm = zone_maps(v, src);
     prog = compile_filter(v, src, slots);
     have_prog = true;
@@ -891,6 +915,7 @@ ScanPlan Engine::plan_scan(Var* v) {
   if (p.src->kind != Var::Base) throw EngineError(ALK_ERR_UNSUPPORTED, "scan of a materialized result");
   p.mode.assign(p.src->segCount, 1);
   if (v->kind == Var::Filtered) {
+    v->scanned = true;
     std::vector<char> zm = zone_maps(v, p.src);
     p.pred = compile_filter(v, p.src, p.slots);
     p.has_pred = true;

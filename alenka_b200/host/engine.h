@@ -87,6 +87,10 @@ struct BaseCol {
   bool dict_loaded = false;
   std::map<std::string, DevBufP> like_sets;  // LIKE pattern -> its matching codes [n, bits]
   DevBufP ranks;                             // entry -> dense rank in byte order (ORDER BY)
+  // a bitmap join index column ("<dimension>.<column>" of a fact table): per segment its
+  // dictionary (ascending values) and the offset of its codes in the index's code space
+  std::vector<std::vector<int64_t>> idx_dict;
+  std::vector<uint64_t> idx_off;
 };
 
 struct Var {
@@ -109,6 +113,7 @@ struct Var {
   // host copies of small results (dense group-by); data gets a column on first use
   std::map<std::string, std::vector<int64_t>> host;
   std::map<std::string, int> grp_type;
+  bool scanned = false;  // Filtered: an operator has read it (its row list exists)
   bool has(const std::string& c) const;
 };
 
@@ -283,6 +288,16 @@ class Engine {
   void emit_store(Statement& st);
   void emit_store_binary(Statement& st);
   void emit_load(Statement& st);
+  // star join with bitmap join indexes (host/star.cpp)
+  std::string star_table(Var* v);
+  void emit_create_bitmap_index(Statement& st);
+  void load_star_index(Var* base, const std::string& col, BaseCol& bc);
+  DevBufP star_set(Var* base, const std::string& col, bool eq, int64_t key);
+  int64_t star_string_key(const std::string& col, const std::string& lit);
+  bool star_join_applies(Statement& st);
+  void star_join(Statement& st);
+  std::vector<DevBufP> star_sets_;         // the code sets of this script's index comparisons
+  std::set<std::string> star_consumed_;    // variables whose filters a star join has moved
   DevBufP like_set(Var* base, const std::string& col, const std::string& pattern);
   const DevBufP& dict_ranks(const ColMeta& m);
   DevBufP dict_hashes(const ColMeta& m, uint32_t width);

@@ -1221,6 +1221,10 @@ void Engine::dense_select_finish(SelectCtx& c) {
 // ------------------------------------------------------------------ JOIN
 // emit_join (operators.cu:797-924): a chain of emit_multijoin steps, then aliases.
 void Engine::emit_join(Statement& st) {
+  if (star_join_applies(st)) {  // emit_join's star branch (operators.cu:828-832)
+    star_join(st);
+    return;
+  }
   std::vector<std::string> op_m = st.op_value;
   if (st.join_tab_cnt > 1) {
     size_t oi = 0;
@@ -1945,6 +1949,14 @@ void Engine::emit_load(Statement& st) {
 // ------------------------------------------------------------------ script
 void Engine::exec(Statement& st) {
   if (st.op_case) unsupported("CASE expressions");
+  // a star join moved the filter queues of its fact and dimension variables into the
+  // fact's (check_bitmaps_exist, cm.cu:4151-4206); what later statements would see of
+  // them is not restated
+  for (const std::string* n : {&st.f})
+    if (!n->empty() && star_consumed_.count(*n) && st.kind != StmtKind::Store)
+      unsupported("a statement reading " + *n + " after a star join used it");
+  for (auto& j : st.op_join)
+    if (star_consumed_.count(j)) unsupported("a statement reading " + j + " after a star join used it");
   switch (st.kind) {
     case StmtKind::Filter: emit_filter(st); break;
     case StmtKind::Select: emit_select(st); break;
@@ -1954,12 +1966,15 @@ void Engine::exec(Statement& st) {
     case StmtKind::StoreBinary: emit_store_binary(st); break;
     case StmtKind::Display: break;
     case StmtKind::Load: emit_load(st); break;
+    case StmtKind::CreateBitmapIndex: emit_create_bitmap_index(st); break;
     default: unsupported("statement kind (catalog commands)");
   }
 }
 
 void Engine::reset_script_state() {
   vars_.clear();
+  star_sets_.clear();
+  star_consumed_.clear();
   stats_ = alk_stats{};
 }
 
@@ -2136,9 +2151,11 @@ int Engine::execute_batch(const std::vector<std::string>& scripts) {
     }
   if (!(flags_ & ALK_SESSION_RESIDENT)) {
     for (auto& t : basecols_)
-      for (auto& c : t.second)
+      for (auto& c : t.second) {
         if (!c.second.device_only)
           for (auto& d : c.second.dev) d.reset();
+        if (c.first.find('.') != std::string::npos) c.second.headers_read = false;  // index: reread
+      }
   }
   cudaStreamSynchronize(stream_);
   stats_.kernels = g_kernel_launches - k0;
@@ -2174,6 +2191,12 @@ int Engine::execute_statements(std::vector<Statement> sts, const std::string& ke
   uint64_t k0 = g_kernel_launches;
   int rc = ALK_OK;
   try {
+    // the reference's bitmap CREATE INDEX leaves its four names in the argument queues,
+    // and the next statement of another kind reads them as its own (operators.cu:2188-2205
+    // never calls clean_queues)
+    for (size_t i = 0; i + 1 < sts.size(); i++)
+      if (sts[i].kind == StmtKind::CreateBitmapIndex && sts[i + 1].kind != StmtKind::CreateBitmapIndex)
+        unsupported("a statement after CREATE INDEX in the same script (the reference passes it the index's names)");
     std::map<std::string, size_t> last;
     begin_script(sts, last);
     for (size_t i = 0; i < sts.size(); i++) {
@@ -2192,11 +2215,14 @@ int Engine::execute_statements(std::vector<Statement> sts, const std::string& ke
     cudaStreamSynchronize(stream_);
   }
   vars_.clear();
+  star_sets_.clear();
   if (!(flags_ & ALK_SESSION_RESIDENT)) {
     for (auto& t : basecols_)
-      for (auto& c : t.second)
+      for (auto& c : t.second) {
         if (!c.second.device_only)
           for (auto& d : c.second.dev) d.reset();
+        if (c.first.find('.') != std::string::npos) c.second.headers_read = false;  // index: reread
+      }
   }
   cudaStreamSynchronize(stream_);
   stats_.kernels = g_kernel_launches - k0;
@@ -2327,6 +2353,7 @@ bool Engine::try_fused(std::vector<Statement>& sts, size_t& i) {
     }
   }
   if (J.join_tab_cnt < 1 || J.join_tab_cnt > 2) return false;
+  if (star_join_applies(J)) return false;  // the reference runs it as a star join
   for (char t : J.join_type)
     if (t != 'I') return false;
   for (auto& kv : J.join_and_cnt)

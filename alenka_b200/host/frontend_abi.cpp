@@ -356,7 +356,9 @@ void emit_describe_table(const char* table_name) { capture(alk::StmtKind::Other,
 void emit_drop_table(const char* table_name) { capture(alk::StmtKind::Other, table_name, "", "", 0); }
 void emit_create_bitmap_index(const char* index_name, const char* ltable, const char* rtable, const char* rcolumn,
                               const char* lid, const char* rid) {
-  capture(alk::StmtKind::Other, index_name, ltable, "", 0);
+  capture(alk::StmtKind::CreateBitmapIndex, index_name, ltable, "", 0);
+  if (!second_pass() && !g_pending.empty())
+    g_pending.back().index_args = {rtable ? rtable : "", rcolumn ? rcolumn : "", lid ? lid : "", rid ? rid : ""};
 }
 void emit_create_index(const char* index_name, const char* table, const char* column) {
   capture(alk::StmtKind::Other, index_name, table, "", 0);
@@ -431,7 +433,7 @@ void save_col_data(map<string, map<string, col_data> >& dd, string file_name) {
 // parser's (front-end tests compare the two). Returns the bytes written (0 when none).
 extern "C" int alk_frontend_dump(char* out, int out_len) {
   string s;
-  static const char* kinds[] = {"FILTER", "SELECT", "JOIN", "ORDER", "STORE", "STORE_BINARY", "DISPLAY", "LOAD", "OTHER"};
+  static const char* kinds[] = {"FILTER", "SELECT", "JOIN", "ORDER", "STORE", "STORE_BINARY", "DISPLAY", "LOAD", "OTHER", "CREATE_BITMAP_INDEX"};
   for (auto& st : g_pending) {
     s += kinds[(int)st.kind];
     s += " s=" + st.s + " f=" + st.f + " grp=" + std::to_string(st.grp_cnt) + " sep=" + st.sep + "\n type:";
@@ -446,6 +448,10 @@ extern "C" int alk_frontend_dump(char* out, int out_len) {
     for (size_t i = 0; i < st.op_join.size(); i++) s += " " + st.op_join[i] + "/" + string(1, st.join_type[i]);
     s += " sel=" + std::to_string(st.sel_count) + " tabs=" + std::to_string(st.join_tab_cnt) + " and:";
     for (auto& kv : st.join_and_cnt) s += " " + std::to_string(kv.first) + "=" + std::to_string(kv.second);
+    if (!st.index_args.empty()) {
+      s += "\n index:";
+      for (auto& x : st.index_args) s += " " + x;
+    }
     s += "\n";
   }
   if (out && out_len > 0) std::snprintf(out, (size_t)out_len, "%s", s.c_str());

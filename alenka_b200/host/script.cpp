@@ -704,6 +704,30 @@ class Parser {
       st.s = expect(T::Name, "index name");
       expect_kw("ON");
       st.f = expect(T::Name, "table name");
+      // the bitmap join index form (bison.y:164-165): CREATE INDEX s ON f(rtable.rcolumn)
+      // FROM t1, t2 WHERE t3.lid = t4.rid; the FROM and WHERE table names are not passed on
+      if (is_punct('(') && peek(1).t == T::Name && is_punct('.', 2)) {
+        take();
+        std::string rtable = expect(T::Name, "table name");
+        expect_punct('.');
+        std::string rcolumn = expect(T::Name, "column name");
+        expect_punct(')');
+        expect_kw("FROM");
+        expect(T::Name, "table name");
+        expect_punct(',');
+        expect(T::Name, "table name");
+        expect_kw("WHERE");
+        expect(T::Name, "table name");
+        expect_punct('.');
+        std::string lid = expect(T::Name, "column name");
+        if (peek().t != T::Equal) fail("expected =");
+        take();
+        expect(T::Name, "table name");
+        expect_punct('.');
+        std::string rid = expect(T::Name, "column name");
+        st.kind = StmtKind::CreateBitmapIndex;
+        st.index_args = {rtable, rcolumn, lid, rid};
+      }
     }
     while (!is_punct(';') && peek().t != T::End) take();
   }

@@ -22,7 +22,8 @@ enum class StmtKind {
   StoreBinary,  // emit_store_binary(s, file, append)  bison.y:148-150
   Display,      // emit_display(s, sep)           bison.y:156
   Load,         // emit_load (CSV)                bison.y:138
-  Other         // DESCRIBE / SHOW / DROP / INSERT / DELETE / CREATE
+  Other,        // DESCRIBE / SHOW / DROP / INSERT / DELETE / CREATE INDEX name ON t(c)
+  CreateBitmapIndex  // emit_create_bitmap_index(s, f, rtable, rcolumn, lid, rid)  bison.y:164-165
 };
 
 // A column of a LOAD's AS list (NAME{field}:type[(size[, decimals])], bison.y:182-185):
@@ -55,6 +56,9 @@ struct Statement {
   unsigned sel_count = 0, join_tab_cnt = 0;
   std::map<unsigned, unsigned> join_and_cnt;
   std::vector<LoadCol> load_cols;  // LOAD: the AS list
+  // CREATE INDEX s ON f(rtable.rcolumn) FROM f, rtable WHERE f.lid = rtable.rid:
+  // {rtable, rcolumn, lid, rid}
+  std::vector<std::string> index_args;
   int line = 0;
 };
 

@@ -667,6 +667,44 @@ int alk_session_card_load(alk_session* s, const char* path);
  * next run of a query is a first run again. */
 int alk_session_card_forget(alk_session* s);
 
+/* Star join with bitmap join indexes (CREATE INDEX ... ON fact(dim.col) FROM fact, dim
+ * WHERE fact.fk = dim.key, then a join of the fact table with a filtered dimension).
+ *
+ * alk_bitmap_index_build: one index segment, replaces the per-segment body of
+ * emit_create_bitmap_index (operators.cu:2225-2264) and compress_int (cm.cu:4271-4336).
+ * Value i < n is d_vals[lower_bound(d_keys[0..m), d_fk[i])]; the ntail values of d_tail
+ * follow (the char form appends the dimension's row hashes past the fact segment's row
+ * count when the dimension has more rows). Writes the sorted distinct values (h_dict, room
+ * for n + ntail), the codes bit-packed MSB first, 64 / bits a word (h_words, room for
+ * n + ntail words), and bits = ceil(log2(distinct + 1)). ALK_ERR_UNSUPPORTED when a
+ * foreign key lies past the last dimension key (the reference gathers past its key
+ * column there). All pointers but the h_* ones are device memory. Synchronises. */
+int alk_bitmap_index_build(const int64_t* d_fk, uint32_t n, const int64_t* d_keys, uint32_t m, const int64_t* d_vals,
+                           const int64_t* d_tail, uint32_t ntail, int64_t* h_dict, uint32_t* h_dict_n,
+                           uint64_t* h_words, uint32_t* h_words_n, uint32_t* h_bits, alk_stream stream);
+/* The packed codes of an index segment (as loadIndex keeps them, cm.cu:2775-2845, and
+ * cmp_functor_dict reads them, filter.cu:21-65) decoded to one code a row at out_bits
+ * (8, 16 or 32, at least bits) into d_out. Asynchronous. */
+int alk_bitmap_index_decode(const uint64_t* d_words, uint32_t rows, uint32_t bits, uint32_t fit_count, void* d_out,
+                            uint32_t out_bits, alk_stream stream);
+/* The star join's row lists (star_join operators.cu:541-552): d_rowid holds, segment after
+ * segment (h_seg_counts survivors of h_seg_rows rows each), the surviving rows' positions
+ * in their segments. The reference fills each segment's list with copy_if over rows
+ * [0, rows - 1) into a list kept from the previous segment, so a surviving last row keeps
+ * the previous list's entry at that position (0 past its end); this rewrites those
+ * entries the same way. Synchronises. */
+int alk_star_rows_fixup(uint32_t* d_rowid, const uint64_t* h_seg_counts, const uint32_t* h_seg_rows, uint32_t nseg,
+                        alk_stream stream);
+/* One output column of a star join (star_join operators.cu:558-766): for row i, the
+ * value at position d_rowid[i] of segment d_seg[i] of the stored FOR column segs (host
+ * array of nseg descriptors: payload, header lower, rows, bits), read as the reference
+ * reads the segment file (8-bit values through a signed char) plus lower. With d_keys the
+ * column is the foreign key of a dimension: t = (uint32)value, plus (uint32)(lower - 1)
+ * when lower != 1, and d_out[i] = d_vals[lower_bound(d_keys[0..m), t)]. ALK_ERR_UNSUPPORTED
+ * when a row lies past its segment or a key past the last dimension key. Synchronises. */
+int alk_star_gather(const alk_colseg* segs, uint32_t nseg, const uint32_t* d_rowid, const uint32_t* d_seg, uint64_t n,
+                    const int64_t* d_keys, uint32_t m, const int64_t* d_vals, int64_t* d_out, alk_stream stream);
+
 /* Device properties of the current device. */
 int alk_device_info(int* sm_count, int* cc_major, int* cc_minor);
 

@@ -290,7 +290,11 @@ class Engine {
       names.insert(st.s);
       names.insert(st.f);
       for (auto& j : st.op_join) names.insert(j);
+      for (auto& x : st.index_args) names.insert(x);
     }
+    for (size_t i = 0; i + 1 < sts.size(); i++)  // emit_create_bitmap_index leaves its names queued
+      if (sts[i].kind == alk::StmtKind::CreateBitmapIndex && sts[i + 1].kind != alk::StmtKind::CreateBitmapIndex)
+        throw Error("a statement after CREATE INDEX in the same script reads the index's names as its own");
     for (auto& t : dd_) {
       if (!names.count(t.first)) continue;
       load_table(t.first, names);
@@ -691,7 +695,20 @@ class Engine {
         } else if ((s1 == "STRING" && s2 == "NAME") || (s1 == "NAME" && s2 == "STRING")) {
           string v1 = pop(exe_value), v2 = pop(exe_value);
           if (s1 == "NAME" && s2 == "STRING") std::swap(v1, v2);  // v1 literal, v2 column
-          if (v2.find('.') != string::npos) throw Error("bitmap-index predicates are not supported");
+          if (v2.find('.') != string::npos) {
+            // a bitmap join index (filter.cu:397-415): the literal padded (or cut) to the
+            // dimension column's width, hashed and halved, looked up in the segment's
+            // dictionary; cmp_functor_dict keeps the code for == and the others otherwise
+            const auto dot = v2.find('.');
+            const u32 len = dd_[v2.substr(0, dot)][v2.substr(dot + 1)].col_length;
+            string lit = v1;
+            while (lit.size() < len) lit.push_back('\0');
+            const i64 key = (i64)(murmur(lit.data(), (int)len, alk::kHashSeed) / 2);
+            index_compare(a, v2, segment, key, cmp, n, *res);
+            exe_type.push_back("NAME");
+            bools.push_back(res);
+            continue;
+          }
           const ColInfo& ci = a->info.at(v2);
           if (cmp == 7) {
             // LIKE: every dictionary entry is matched once and a row passes when its
@@ -724,6 +741,17 @@ class Engine {
             bool eq = x == hv;
             (*res)[i] = cmp == 4 ? eq : (cmp == 3 ? !eq : 0);
           }
+          exe_type.push_back("NAME");
+          bools.push_back(res);
+        } else if ((s1 == "NUMBER" || s2 == "NUMBER") && (s1 == "NAME" || s2 == "NAME") &&
+                   exe_value.back().find('.') != string::npos) {
+          // a bitmap join index against a number (filter.cu:519-535, 560-577): the number
+          // as it is, looked up in the segment's dictionary; the precision stack is left
+          // as it was
+          if (s1 == "NAME") cmp = reverse_op(cmp);
+          i64 n1 = pop(exe_nums);
+          string v = pop(exe_value);
+          index_compare(a, v, segment, n1, cmp, n, *res);
           exe_type.push_back("NAME");
           bools.push_back(res);
         } else if (s1 == "NUMBER" && s2 == "NAME") {
@@ -901,6 +929,310 @@ class Engine {
     return a->segCount;
   }
 
+  // ---------------- star join with bitmap join indexes ----------------
+  // Index segment <fact>.<dimension>.<column>.<segment> as loadIndex reads it
+  // (cm.cu:2775-2845): the dictionary and every row's code.
+  struct IndexSeg {
+    vector<i64> dict;
+    vector<u32> codes;
+  };
+  map<string, IndexSeg> index_cache_;
+  const IndexSeg& index_seg(Var* a, const string& name, unsigned segment) {
+    const string path = a->load_file_name + "." + name + "." + std::to_string(segment);
+    auto it = index_cache_.find(path);
+    if (it != index_cache_.end()) return it->second;
+    vector<uint8_t> b;
+    string e;
+    if (!alk::read_file(path, b, e)) throw Error(e);
+    IndexSeg x;
+    u32 sz, fit, bits, vals, real;
+    std::memcpy(&sz, b.data(), 4);
+    x.dict.resize(sz);
+    std::memcpy(x.dict.data(), b.data() + 4, (size_t)sz * 8);
+    const size_t h = 4 + (size_t)sz * 8;
+    std::memcpy(&fit, b.data() + h, 4);
+    std::memcpy(&bits, b.data() + h + 4, 4);
+    std::memcpy(&vals, b.data() + h + 8, 4);
+    std::memcpy(&real, b.data() + h + 12, 4);
+    x.codes.resize(real);
+    for (u32 i = 0; i < real; i++) {  // cmp_functor_dict (filter.cu:30-50)
+      uint64_t w;
+      std::memcpy(&w, b.data() + h + 16 + (size_t)(i / fit) * 8, 8);
+      uint64_t t = w >> ((fit - (i % fit)) - 1) * bits;
+      t = t << (64 - bits);
+      t = t >> (64 - bits);
+      x.codes[i] = (u32)t;
+    }
+    return index_cache_[path] = std::move(x);
+  }
+  // filter.cu:397-415 and cmp_functor_dict: key's position in the segment's dictionary;
+  // == keeps that code, every other operator the other codes; a key the dictionary lacks
+  // keeps nothing
+  void index_compare(Var* a, const string& name, unsigned segment, i64 key, i64 cmp, size_t n,
+                     vector<uint8_t>& out) {
+    const IndexSeg& x = index_seg(a, name, segment);
+    if (x.codes.size() != n) throw Error("index " + name + " holds another row count than its segment");
+    auto it = std::find(x.dict.begin(), x.dict.end(), key);
+    if (it == x.dict.end()) {
+      std::fill(out.begin(), out.end(), 0);
+      return;
+    }
+    const u32 idx = (u32)(it - x.dict.begin());
+    for (size_t i = 0; i < n; i++) out[i] = cmp == 4 ? (x.codes[i] == idx) : (x.codes[i] != idx);
+  }
+
+  // std::lower_bound over v[0, m)
+  static size_t lower_bound_pos(const Vec& v, size_t m, i64 key) {
+    return (size_t)(std::lower_bound(v.begin(), v.begin() + m, key) - v.begin());
+  }
+
+  // emit_create_bitmap_index (operators.cu:2188-2268) with compress_int (cm.cu:4271-4336)
+  void create_bitmap_index(alk::Statement& st) {
+    const string& ltable = st.f;
+    const string& rtable = st.index_args.at(0);
+    const string& rcol = st.index_args.at(1);
+    const string& lid = st.index_args.at(2);
+    const string& rid = st.index_args.at(3);
+    Var* left = var(ltable);
+    Var* right = var(rtable);
+    if (right->segCount != 1) throw Error("a bitmap index over a dimension of several segments");
+    Vec keys = decode_col(right, rid, 0);
+    const size_t m = keys.size();
+    const bool chr = right->info.at(rcol).type == 2;
+    Vec rv;
+    if (!chr) {
+      rv = decode_col(right, rcol, 0);
+    } else {
+      const auto& hb = file(right->load_file_name + "." + rcol + ".0.hash");
+      u32 cnt;
+      std::memcpy(&cnt, hb.data(), 4);
+      rv.resize(cnt);
+      std::memcpy(rv.data(), hb.data() + 4, (size_t)cnt * 8);
+    }
+    for (unsigned i = 0; i < left->segCount; i++) {
+      Vec fk = decode_col(left, lid, i);
+      const size_t n = fk.size();
+      // res_h: the segment's values, then (char) the dimension's hashes past n
+      vector<i64> res(chr ? std::max(n, rv.size()) : n, 0);
+      if (chr)
+        for (size_t k = n; k < rv.size(); k++) res[k] = rv[k];
+      for (size_t k = 0; k < n; k++) {
+        const size_t p = lower_bound_pos(keys, m, fk[k]);
+        if (p >= m) throw Error("a foreign key past the dimension's last key");
+        res[k] = rv[p];
+      }
+      // compress_int: dictionary of the distinct values in order, codes, packing
+      std::set<i64> dict_s(res.begin(), res.end());
+      map<i64, u32> d_ordered;
+      u32 c = 0;
+      for (i64 v : dict_s) d_ordered[v] = c++;
+      vector<u32> dict_val;
+      for (i64 v : res) dict_val.push_back(d_ordered[v]);
+      const u32 bits = (u32)std::ceil(std::log2(double(d_ordered.size() + 1)));
+      const u32 sz = (u32)d_ordered.size();
+      string out;
+      auto put = [&](const void* p, size_t k) { out.append((const char*)p, k); };
+      put(&sz, 4);
+      for (auto& kv : d_ordered) put(&kv.first, 8);
+      const u32 fit_count = 64 / bits;
+      put(&fit_count, 4);
+      put(&bits, 4);
+      u32 vals_count = (u32)dict_val.size() / fit_count;
+      if (!vals_count || dict_val.size() % fit_count) vals_count++;
+      put(&vals_count, 4);
+      const u32 real_count = (u32)dict_val.size();
+      put(&real_count, 4);
+      uint64_t val = 0;
+      u32 curr = 1;
+      for (size_t k = 0; k < dict_val.size(); k++) {
+        val = val | dict_val[k];
+        if (curr < fit_count) val = val << bits;
+        if (curr == fit_count || k == dict_val.size() - 1) {
+          if (curr < fit_count) val = val << ((fit_count - curr) - 1) * bits;
+          curr = 1;
+          put(&val, 8);
+          val = 0;
+        } else {
+          curr++;
+        }
+      }
+      const string path = dir_ + "/" + ltable + "." + rtable + "." + rcol + "." + std::to_string(i);
+      if (!alk::write_file(path, out.data(), out.size())) throw Error("cannot write " + path);
+      index_cache_.erase(path);
+    }
+  }
+
+  string table_of(Var* v) {
+    Var* b = v->filtered ? var(v->source_name) : v;
+    if (b->not_compressed) throw Error("a star join over a materialized result");
+    return b->name;
+  }
+  static bool file_exists(const string& p) {
+    FILE* f = std::fopen(p.c_str(), "rb");
+    if (!f) return false;
+    std::fclose(f);
+    return true;
+  }
+  // check_star_join (operators.cu:408-437) with check_bitmap_file_exist (cm.cu:4131-4149)
+  bool check_star_join(alk::Statement& st) {
+    if (st.join_tab_cnt == 0) return false;
+    Var* left = var(st.f);
+    for (size_t k = 2 * (size_t)st.sel_count; k < st.op_value.size(); k += 2)
+      if (!left->has(st.op_value[k])) return false;
+    if (st.join_tab_cnt == 1) {
+      Var* right = var(st.op_join.at(0));
+      if (right->fil_value.empty()) return false;
+      const string lt = table_of(left), rt = table_of(right);
+      for (auto& c : right->fil_value)
+        if (right->has(c) && !file_exists(dir_ + "/" + lt + "." + rt + "." + c + ".0")) return false;
+    }
+    return true;
+  }
+  // the stored value of row r of a FOR segment file as star_join reads it
+  // (operators.cu:594-650): 8-bit values through a signed char, plus the header's lower
+  i64 stored_value(Var* t, const string& col, unsigned seg, u32 r, size_t n) {
+    const auto& img = file(seg_path(t, col, seg));
+    u32 cnt, comp, bits;
+    i64 lower;
+    std::memcpy(&cnt, img.data(), 4);
+    std::memcpy(&lower, img.data() + 4, 8);
+    std::memcpy(&comp, img.data() + 20, 4);
+    std::memcpy(&bits, img.data() + 24 + cnt + 8, 4);
+    if (comp != 0) throw Error("a star join over the FOR-delta column " + col);
+    if (r >= n) throw Error("a star join row past its segment");
+    const uint8_t* p = img.data() + 24;
+    i64 raw;
+    if (bits == 8) raw = (i64)(int8_t)p[r];
+    else if (bits == 16) { uint16_t x; std::memcpy(&x, p + 2 * (size_t)r, 2); raw = x; }
+    else if (bits == 32) { u32 x; std::memcpy(&x, p + 4 * (size_t)r, 4); raw = x; }
+    else std::memcpy(&raw, p + 8 * (size_t)r, 8);
+    return (i64)((uint64_t)raw + (uint64_t)lower);
+  }
+  // star_join (operators.cu:440-794)
+  void star_join(alk::Statement& st) {
+    Var* left = var(st.f);
+    Var* lbase = left->filtered ? var(left->source_name) : left;
+    const string ltab = table_of(left);
+    vector<string> sel;
+    for (unsigned k = 0; k < st.sel_count; k++) {
+      if (st.op_value[2 * k] != st.op_value[2 * k + 1]) throw Error("an alias in a star join");
+      sel.push_back(st.op_value[2 * k]);
+    }
+    Var f = *left;  // the fact's filter with the dimensions' appended (check_bitmaps_exist)
+    f.h.clear();
+    struct Dim {
+      string fk, key;
+      Var* base;
+      Var* r;
+    };
+    map<string, Dim> dims;  // key_map
+    const size_t g0 = 2 * (size_t)st.sel_count;
+    for (unsigned i = 0; i < st.join_tab_cnt; i++) {
+      Dim d;
+      d.fk = st.op_value.at(g0 + 2 * i);
+      d.key = st.op_value.at(g0 + 2 * i + 1);
+      const string jvar = st.op_join.at(st.join_tab_cnt - 1 - i);
+      d.r = var(jvar);
+      d.base = d.r->filtered ? var(d.r->source_name) : d.r;
+      if (d.base->segCount != 1) throw Error("a star join with a dimension of several segments");
+      const string rt = table_of(d.r);
+      if (!d.r->fil_value.empty()) {
+        for (auto& c : d.r->fil_value)
+          if (d.r->has(c) && !file_exists(dir_ + "/" + ltab + "." + rt + "." + c + ".0"))
+            throw Error("Required bitmap on table " + jvar + " doesn't exists");
+        const bool add_and = !f.fil_type.empty();
+        f.fil_nums.insert(f.fil_nums.end(), d.r->fil_nums.begin(), d.r->fil_nums.end());
+        f.fil_prec.insert(f.fil_prec.end(), d.r->fil_prec.begin(), d.r->fil_prec.end());
+        for (auto& c : d.r->fil_value) f.fil_value.push_back(d.r->has(c) ? rt + "." + c : c);
+        f.fil_type.insert(f.fil_type.end(), d.r->fil_type.begin(), d.r->fil_type.end());
+        if (add_and) f.fil_type.push_back("AND");
+      }
+      dims[jvar] = d;
+    }
+    if (f.fil_type.empty()) throw Error("a star join without a filter");
+    auto c = std::make_unique<Var>();
+    c->name = st.s;
+    c->not_compressed = true;
+    for (auto& name : sel) {
+      if (c->has(name)) continue;
+      c->columnNames.push_back(name);
+      if (left->has(name)) c->info[name] = lbase->info.at(name);
+      else {
+        bool found = false;
+        for (auto& kv : dims)
+          if (kv.second.r->has(name)) {
+            c->info[name] = kv.second.base->info.at(name);
+            found = true;
+            break;
+          }
+        if (!found) throw Error("the star join column " + name + " is in no joined table");
+      }
+      if (left->has(name) && c->info[name].type == 2) throw Error("a char fact column in a star join");
+    }
+    map<string, std::pair<Vec, Vec>> dim_cols;  // (key column, value column) per dimension column
+    vector<u32> prm;                              // left->prm_d, kept from segment to segment
+    size_t total = 0;
+    bool seg0_rows = false;
+    for (unsigned g = 0; g < lbase->segCount; g++) {
+      map<string, Vec> cols;
+      size_t n = 0;
+      for (auto& fv : f.fil_value)
+        if (lbase->has(fv) && !cols.count(fv)) {
+          cols[fv] = decode_col(lbase, fv, g);
+          n = cols[fv].size();
+        }
+      if (!n) n = decode_col(lbase, lbase->columnNames.at(0), g).size();
+      rows_scanned += n;
+      vector<uint8_t> mask = filter_eval(&f, lbase, g, cols, n);
+      size_t cnt = 0;
+      for (size_t i = 0; i < n; i++) cnt += mask[i] != 0;
+      if (!cnt) continue;
+      if (g == 0) seg0_rows = true;
+      prm.resize(cnt, 0);
+      size_t w = 0;
+      for (size_t i = 0; i + 1 < n; i++)  // copy_if over [0, n - 1)
+        if (mask[i]) prm[w++] = (u32)i;
+      for (auto& name : sel) {
+        Vec& out = c->h[name];
+        if (out.size() > total) continue;  // a repeated column
+        if (left->has(name)) {
+          for (size_t k = 0; k < cnt; k++) out.push_back(stored_value(lbase, name, g, prm[k], n));
+          continue;
+        }
+        for (auto& kv : dims) {
+          Dim& d = kv.second;
+          if (!d.r->has(name)) continue;
+          auto& dc = dim_cols[kv.first + "." + name];
+          if (dc.first.empty()) {
+            dc.first = decode_col(d.base, d.key, 0);
+            dc.second = decode_col(d.base, name, 0);
+          }
+          const auto& fimg = file(seg_path(lbase, d.fk, g));
+          i64 lower;
+          std::memcpy(&lower, fimg.data() + 4, 8);
+          for (size_t k = 0; k < cnt; k++) {
+            const i64 raw = (i64)((uint64_t)stored_value(lbase, d.fk, g, prm[k], n) - (uint64_t)lower);
+            u32 t = (u32)raw;
+            if (lower != 1) t += (u32)(lower - 1);
+            const size_t p = lower_bound_pos(dc.first, dc.first.size(), (i64)t);
+            if (p >= dc.first.size()) throw Error("a star join key past the dimension's last key");
+            out.push_back(dc.second[p]);
+          }
+          break;
+        }
+      }
+      total += cnt;
+    }
+    // a char dimension column gets its dictionary while the first segment is gathered
+    // (operators.cu:672-677); without rows there it has none
+    for (auto& name : c->columnNames)
+      if (!left->has(name) && c->info[name].type == 2 && total && !seg0_rows)
+        throw Error("a char dimension column whose first fact segment keeps no row");
+    for (auto& name : c->columnNames) c->h[name].resize(total);
+    c->mRecCount = c->hostRecCount = c->maxRecs = total;
+    vars_[st.s] = std::move(c);
+  }
+
   // ---------------- statements ----------------
   void exec(alk::Statement& st) {
     switch (st.kind) {
@@ -910,6 +1242,7 @@ class Engine {
       case alk::StmtKind::Order: emit_order(st); break;
       case alk::StmtKind::Store: emit_store(st); break;
       case alk::StmtKind::Display: break;
+      case alk::StmtKind::CreateBitmapIndex: create_bitmap_index(st); break;
       default: throw Error("statement kind not supported by the oracle");
     }
   }
@@ -1459,6 +1792,10 @@ class Engine {
 
   // emit_join (operators.cu:797-924) and emit_multijoin (operators.cu:940-1582), inner joins.
   void emit_join(alk::Statement& st) {
+    if (check_star_join(st)) {  // emit_join's star branch (operators.cu:828-832)
+      star_join(st);
+      return;
+    }
     vector<string> op_m = st.op_value;
     if (st.join_tab_cnt > 1) {
       vector<string> oj = st.op_join;
