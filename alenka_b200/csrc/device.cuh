@@ -143,6 +143,73 @@ __device__ __forceinline__ uint64_t lookback_u64(volatile uint32_t* flags, volat
   return excl;
 }
 
+// The same look-back run by a whole warp (all 32 lanes call it with the same tile and
+// aggregate): each step reads 32 predecessors' flags at once, waits only while one of them
+// up to the nearest inclusive prefix is still unpublished, and sums their aggregates (and
+// that inclusive prefix) with a warp reduction, so a tile walks back over a run of
+// unresolved tiles 32 at a time. Waits are bounded like lookback_u64's.
+__device__ __forceinline__ uint64_t lookback_warp_u64(volatile uint32_t* flags, volatile uint64_t* aggs,
+                                                      volatile uint64_t* incls, uint32_t tile, uint64_t agg,
+                                                      int* err, bool* ok) {
+  const int lane = threadIdx.x & 31;
+  *ok = true;
+  if (tile == 0) {
+    if (lane == 0) {
+      incls[0] = agg;
+      __threadfence();
+      flags[0] = 2;
+    }
+    __syncwarp();
+    return 0;
+  }
+  if (lane == 0) {
+    aggs[tile] = agg;
+    __threadfence();
+    flags[tile] = 1;
+  }
+  __syncwarp();
+  uint64_t excl = 0;
+  int64_t top = (int64_t)tile - 1;  // nearest predecessor not yet summed
+  uint32_t spins = 0;
+  bool timed_out = false;
+  while (true) {
+    const int64_t j = top - lane;  // lane 0 is the nearest predecessor
+    const uint32_t f = j >= 0 ? flags[j] : 2u;  // before tile 0 counts as an inclusive prefix of 0
+    const uint32_t inc = __ballot_sync(0xffffffffu, f == 2);
+    const uint32_t upto = inc ? ((inc & (0u - inc)) << 1) - 1 : 0xffffffffu;  // lanes up to the first inclusive
+    if (__ballot_sync(0xffffffffu, f == 0) & upto) {
+      if (++spins > kSpinLimit) {
+        timed_out = true;
+        break;
+      }
+      __nanosleep(64);
+      continue;
+    }
+    __threadfence();
+    uint64_t v = 0;
+    if ((upto >> lane) & 1) {
+      if (f == 2) v = j >= 0 ? incls[j] : 0;
+      else v = aggs[j];
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    excl += v;
+    if (inc) break;
+    top -= 32;
+  }
+  if (timed_out) {
+    if (lane == 0) atomicExch(err, ALK_ERR_TIMEOUT);
+    *ok = false;
+  }
+  if (lane == 0) {
+    incls[tile] = excl + agg;
+    __threadfence();
+    flags[tile] = 2;
+  }
+  __syncwarp();
+  return excl;
+}
+
 template <class T>
 __device__ __forceinline__ T warp_incl_scan(T v) {
   const int lane = threadIdx.x & 31;

@@ -85,10 +85,13 @@ __global__ void __launch_bounds__(kT) k_decode_delta(DeltaArgs a) {
     }
     uint64_t tot;
     uint64_t excl = block_excl_scan<kT>(sum, s_warp, &tot);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
       bool ok;
-      s_base = lookback_u64(a.flags, a.aggs, a.incls, tile, tot, a.err, &ok);
-      s_ok = ok;
+      const uint64_t b = lookback_warp_u64(a.flags, a.aggs, a.incls, tile, tot, a.err, &ok);
+      if (threadIdx.x == 0) {
+        s_base = b;
+        s_ok = ok;
+      }
     }
     __syncthreads();
     if (s_ok) {
@@ -135,11 +138,14 @@ __global__ void __launch_bounds__(kT) k_flags_compact(CompactArgs a) {
       if (r0 + k < a.n && a.flags[r0 + k]) m |= 1u << k;
     uint64_t tot;
     const uint64_t excl = block_excl_scan<kT>((uint64_t)__popc(m), s_warp, &tot);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
       bool ok;
-      s_base = lookback_u64(a.tflags, a.aggs, a.incls, tile, tot, a.err, &ok);
-      s_ok = ok;
-      if (ok && tile == a.ntiles - 1) *a.count = s_base + tot;
+      const uint64_t b = lookback_warp_u64(a.tflags, a.aggs, a.incls, tile, tot, a.err, &ok);
+      if (threadIdx.x == 0) {
+        s_base = b;
+        s_ok = ok;
+        if (ok && tile == a.ntiles - 1) *a.count = b + tot;
+      }
     }
     __syncthreads();
     if (s_ok) {
@@ -233,9 +239,10 @@ __global__ void __launch_bounds__(kT) k_scan(ScanArgs a) {
         s_cnt[base + lane] = carry + inc - x;
         carry += __shfl_sync(0xffffffffu, inc, 31);
       }
+      bool ok;
+      const uint64_t b = lookback_warp_u64(a.flags, a.aggs, a.incls, tile, carry, a.err, &ok);
       if (lane == 0) {
-        bool ok;
-        s_base = lookback_u64(a.flags, a.aggs, a.incls, tile, carry, a.err, &ok);
+        s_base = b;
         s_ok = ok;
         if (carry) {
           atomicAdd(a.total, (unsigned long long)carry);

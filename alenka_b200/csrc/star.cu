@@ -47,6 +47,21 @@ __device__ __forceinline__ uint32_t lower_bound_i64(const int64_t* keys, uint32_
   return first;
 }
 
+// The same search over a dimension column stored FOR (value = stored + lower).
+__device__ __forceinline__ uint32_t lower_bound_for(const alk_colseg& keys, int64_t v) {
+  uint32_t first = 0, len = keys.rows;
+  while (len > 0) {
+    const uint32_t half = len >> 1, mid = first + half;
+    if (alkd::load_for(keys.data, keys.bits, keys.lower, mid) < v) {
+      first = mid + 1;
+      len = len - half - 1;
+    } else {
+      len = half;
+    }
+  }
+  return first;
+}
+
 // First position p in [0, d) with heads[p] > i (heads ascending).
 __device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t* heads, uint32_t d, uint32_t i) {
   uint32_t first = 0, len = d;
@@ -155,13 +170,14 @@ __global__ void k_star_fixup(uint32_t* rowid, const uint64_t* offs, const uint64
 // Values of the star join's output rows, read from the stored segment payloads as the
 // star join reads the segment files (operators.cu:576-650, 678-731): 8-bit values through
 // a signed char, 16 and 32-bit ones unsigned, then the header's lower bound added.
-// Without keys, out = that value (a fact column). With keys, the value is a foreign key:
-// t = (uint32)value, plus (uint32)(lower - 1) when lower != 1, and out = vals at
-// lower_bound(keys, t) (a dimension column; star_join's lower_bound path). A row past its
-// segment sets err bit 1, a key past the dimension's keys err bit 0.
+// For a fact column, out = that value. For a dimension column the value is a foreign key:
+// t = (uint32)value, plus (uint32)(lower - 1) when lower != 1, and out = the dimension
+// column's value at lower_bound(dimension keys, t), both read at their stored widths
+// (star_join's lower_bound path). A row past its segment sets err bit 1, a key past the
+// dimension's keys err bit 0.
 __global__ void __launch_bounds__(kT) k_star_gather(const alk_colseg* segs, const uint32_t* rowid,
-                                                    const uint32_t* seg, uint64_t n, const int64_t* keys, uint32_t m,
-                                                    const int64_t* vals, int64_t* out, int* err) {
+                                                    const uint32_t* seg, uint64_t n, bool dim, alk_colseg keys,
+                                                    alk_colseg vals, int64_t* out, int* err) {
   for (uint64_t i = blockIdx.x * (uint64_t)kT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kT) {
     const alk_colseg cs = segs[seg[i]];
     const uint32_t r = rowid[i];
@@ -177,18 +193,18 @@ __global__ void __launch_bounds__(kT) k_star_gather(const alk_colseg* segs, cons
       case 32: raw = (int64_t)((const uint32_t*)cs.data)[r]; break;
       default: raw = ((const int64_t*)cs.data)[r]; break;
     }
-    if (!keys) {
+    if (!dim) {
       out[i] = (int64_t)((uint64_t)raw + (uint64_t)cs.lower);
       continue;
     }
     uint32_t t = (uint32_t)raw;
     if (cs.lower != 1) t += (uint32_t)(cs.lower - 1);
-    const uint32_t p = lower_bound_i64(keys, m, (int64_t)t);
-    if (p >= m) {
+    const uint32_t p = lower_bound_for(keys, (int64_t)t);
+    if (p >= keys.rows) {
       atomicOr(err, 1);
       out[i] = 0;
     } else {
-      out[i] = vals[p];
+      out[i] = alkd::load_for(vals.data, vals.bits, vals.lower, p);
     }
   }
 }
@@ -326,15 +342,21 @@ int alk_star_rows_fixup(uint32_t* d_rowid, const uint64_t* h_seg_counts, const u
 }
 
 int alk_star_gather(const alk_colseg* segs, uint32_t nseg, const uint32_t* d_rowid, const uint32_t* d_seg, uint64_t n,
-                    const int64_t* d_keys, uint32_t m, const int64_t* d_vals, int64_t* d_out, alk_stream stream) {
+                    const alk_colseg* dim_key, const alk_colseg* dim_val, int64_t* d_out, alk_stream stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (n == 0) return ALK_OK;
   if (!segs || nseg == 0 || !d_rowid || !d_seg || !d_out) return ALK_ERR_ARG;
-  if (d_keys && (m == 0 || !d_vals)) return ALK_ERR_ARG;
-  for (uint32_t g = 0; g < nseg; g++) {
-    const uint32_t b = segs[g].bits;
-    if (b != 8 && b != 16 && b != 32 && b != 64) return ALK_ERR_ARG;
-    if (segs[g].rows && !segs[g].data) return ALK_ERR_ARG;
+  if (!dim_key != !dim_val) return ALK_ERR_ARG;
+  auto bad = [](const alk_colseg& c) {
+    return (c.bits != 8 && c.bits != 16 && c.bits != 32 && c.bits != 64) || (c.rows && !c.data);
+  };
+  for (uint32_t g = 0; g < nseg; g++)
+    if (bad(segs[g])) return ALK_ERR_ARG;
+  alk_colseg kd{}, vd{};
+  if (dim_key) {
+    kd = *dim_key;
+    vd = *dim_val;
+    if (bad(kd) || bad(vd) || kd.rows == 0 || vd.rows != kd.rows) return ALK_ERR_ARG;
   }
   Scratch sc(s);
   cudaError_t e;
@@ -344,7 +366,7 @@ int alk_star_gather(const alk_colseg* segs, uint32_t nseg, const uint32_t* d_row
   CK(e);
   CK(cudaMemcpyAsync(ds, segs, (size_t)nseg * sizeof(alk_colseg), cudaMemcpyHostToDevice, s));
   CK(cudaMemsetAsync(err, 0, sizeof(int), s));
-  k_star_gather<<<grid_for(n), kT, 0, s>>>(ds, d_rowid, d_seg, n, d_keys, m, d_vals, d_out, err);
+  k_star_gather<<<grid_for(n), kT, 0, s>>>(ds, d_rowid, d_seg, n, dim_key != nullptr, kd, vd, d_out, err);
   alk::g_kernel_launches++;
   CK(cudaGetLastError());
   int h_err = 0;

@@ -628,6 +628,21 @@ alk_program Engine::compile_filter(Var* f, Var* src, std::vector<std::string>& s
     slots.push_back(c);
     return b.col((uint32_t)slots.size() - 1);
   };
+  // Comparisons with a bitmap index column stay host-side code sets until something other
+  // than AND / OR of sets over the same column consumes them: those fold into one set, so
+  // a filter such as d == x OR d == y OR ... tests one set per row.
+  constexpr uint8_t kPendingSet = 0xFF;
+  std::vector<std::pair<std::string, std::vector<uint32_t>>> psets;
+  auto pending = [&](const std::string& col, std::vector<uint32_t> w) {
+    psets.push_back({col, std::move(w)});
+    return Operand{kPendingSet, (uint16_t)(psets.size() - 1)};
+  };
+  // a pending set as an ALK_OP_INSET test of its index column
+  auto materialize_set = [&](Operand o) -> Operand {
+    if (o.kind != kPendingSet) return o;
+    const DevBufP buf = star_upload(psets[o.idx].second);
+    return b.emit(ALK_OP_INSET, slot(psets[o.idx].first), b.konst((int64_t)(uintptr_t)buf->as<void>()));
+  };
   auto get_dec = [&](const std::string& s) -> uint32_t { return src->has(s) ? src->meta[s].dz : pop(ep); };
   auto get_vec = [&](const std::string& s) -> Operand { return src->has(s) ? slot(s) : pop(evec); };
   for (auto& ss : f->fil_type) {
@@ -708,8 +723,7 @@ alk_program Engine::compile_filter(Var* f, Var* src, std::vector<std::string>& s
           // a bitmap join index column: the literal's hash looked up in each segment's
           // dictionary, == keeps its code and any other operator the other codes
           // (filter.cu:397-415)
-          const DevBufP set = star_set(src, v2, cmp == 4, star_string_key(v2, v1));
-          bools.push_back(b.emit(ALK_OP_INSET, slot(v2), b.konst((int64_t)(uintptr_t)set->as<void>())));
+          bools.push_back(pending(v2, star_set(src, v2, cmp == 4, star_string_key(v2, v1))));
           et.push_back("NAME");
           continue;
         }
@@ -740,8 +754,7 @@ alk_program Engine::compile_filter(Var* f, Var* src, std::vector<std::string>& s
         // on the precision stack, as the reference pops and pushes none there
         int64_t n1 = pop(en);
         std::string v = pop(ev);
-        const DevBufP set = star_set(src, v, cmp == 4, n1);
-        bools.push_back(b.emit(ALK_OP_INSET, slot(v), b.konst((int64_t)(uintptr_t)set->as<void>())));
+        bools.push_back(pending(v, star_set(src, v, cmp == 4, n1)));
         et.push_back("NAME");
       } else if (s1 == "NUMBER" && s2 == "NAME") {
         int64_t n1 = pop(en);
@@ -788,14 +801,24 @@ alk_program Engine::compile_filter(Var* f, Var* src, std::vector<std::string>& s
     if (ss == "AND" || ss == "OR") {
       Operand b3 = pop(bools), b2 = pop(bools);
       et.push_back("NAME");
+      if (b2.kind == kPendingSet && b3.kind == kPendingSet && psets[b2.idx].first == psets[b3.idx].first) {
+        std::vector<uint32_t> w = psets[b2.idx].second;
+        const std::vector<uint32_t>& w3 = psets[b3.idx].second;
+        for (size_t k = 1; k < w.size(); k++) w[k] = ss == "AND" ? (w[k] & w3[k]) : (w[k] | w3[k]);
+        bools.push_back(pending(psets[b2.idx].first, std::move(w)));
+        continue;
+      }
+      b2 = materialize_set(b2);
+      b3 = materialize_set(b3);
       bools.push_back(b.emit(ss == "AND" ? ALK_OP_AND : ALK_OP_OR, b2, b3));
       continue;
     }
     unsupported("operation " + ss + " is not valid in a filter");
   }
   if (bools.empty()) unsupported("filter without a comparison");
+  Operand res = materialize_set(bools.back());
   if (slots.size() > 16) unsupported("filter reads more than 16 columns");
-  return b.finish(bools.back());
+  return b.finish(res);
 }
 
 // ------------------------------------------------------------------ materialization

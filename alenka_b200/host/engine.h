@@ -292,7 +292,8 @@ class Engine {
   std::string star_table(Var* v);
   void emit_create_bitmap_index(Statement& st);
   void load_star_index(Var* base, const std::string& col, BaseCol& bc);
-  DevBufP star_set(Var* base, const std::string& col, bool eq, int64_t key);
+  std::vector<uint32_t> star_set(Var* base, const std::string& col, bool eq, int64_t key);
+  DevBufP star_upload(const std::vector<uint32_t>& words);
   int64_t star_string_key(const std::string& col, const std::string& lit);
   bool star_join_applies(Statement& st);
   void star_join(Statement& st);

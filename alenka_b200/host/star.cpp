@@ -212,8 +212,9 @@ void Engine::load_star_index(Var* base, const std::string& col, BaseCol& bc) {
 // The codes of an index column that a comparison with `key` keeps, as a set over the
 // index's code space (filter.cu:397-415, 519-535, 560-577 with cmp_functor_dict): in a
 // segment whose dictionary holds key, the code of key for ==, every other code for any
-// other operator; in a segment whose dictionary lacks key, no code at all.
-DevBufP Engine::star_set(Var* base, const std::string& col, bool eq, int64_t key) {
+// other operator; in a segment whose dictionary lacks key, no code at all. The words are
+// ALK_OP_INSET's layout: the space's size, then the bits.
+std::vector<uint32_t> Engine::star_set(Var* base, const std::string& col, bool eq, int64_t key) {
   ensure_base_col(base, col, true);
   BaseCol& bc = basecol(base, col);
   uint64_t space = 0;
@@ -232,6 +233,11 @@ DevBufP Engine::star_set(Var* base, const std::string& col, bool eq, int64_t key
       w[1 + b / 32] |= 1u << (b % 32);
     }
   }
+  return w;
+}
+
+// A code set on the device, kept until the script ends.
+DevBufP Engine::star_upload(const std::vector<uint32_t>& w) {
   auto buf = mkbuf(w.size() * 4, stream_);
   ck(cudaMemcpyAsync(buf->as<void>(), w.data(), w.size() * 4, cudaMemcpyHostToDevice, stream_), "index set upload");
   ck(cudaStreamSynchronize(stream_), "index set upload");
@@ -400,7 +406,7 @@ void Engine::star_join(Statement& st) {
       meta = lsrc->meta.at(name);
       if (meta.type == 2) unsupported("a char column of the fact table in a star join");
       std::vector<alk_colseg> v = stored(name);
-      const int rc = alk_star_gather(v.data(), nseg, rowid->as<uint32_t>(), segof->as<uint32_t>(), count, nullptr, 0,
+      const int rc = alk_star_gather(v.data(), nseg, rowid->as<uint32_t>(), segof->as<uint32_t>(), count, nullptr,
                                      nullptr, out->as<int64_t>(), (alk_stream)stream_);
       if (rc == ALK_ERR_UNSUPPORTED)
         unsupported("a star join row reused from a longer segment (the reference reads past the segment)");
@@ -416,10 +422,15 @@ void Engine::star_join(Statement& st) {
       meta = d->base->meta.at(name);
       if (meta.type == 2 && counts[0] == 0 && count)
         unsupported("a char dimension column in a star join whose first fact segment keeps no row");
-      Rows dr = materialize(d->base, {d->key, name});
+      // the dimension's key and value columns at their resident widths (one segment)
+      auto resident = [&](const std::string& col) {
+        ensure_base_col(d->base, col, true);
+        BaseCol& bc = basecol(d->base, col);
+        return alk_colseg{bc.dev[0]->as<void>(), bc.res_lower[0], bc.segs[0].m.rec_count, bc.res_bits[0]};
+      };
+      const alk_colseg dk = resident(d->key), dv = resident(name);
       std::vector<alk_colseg> v = stored(d->fk);
-      const int rc = alk_star_gather(v.data(), nseg, rowid->as<uint32_t>(), segof->as<uint32_t>(), count,
-                                     dr.col.at(d->key)->as<int64_t>(), (uint32_t)dr.n, dr.col.at(name)->as<int64_t>(),
+      const int rc = alk_star_gather(v.data(), nseg, rowid->as<uint32_t>(), segof->as<uint32_t>(), count, &dk, &dv,
                                      out->as<int64_t>(), (alk_stream)stream_);
       if (rc == ALK_ERR_UNSUPPORTED)
         unsupported("a star join row past its segment or a foreign key past the last key of " + d->key);

@@ -698,12 +698,14 @@ int alk_star_rows_fixup(uint32_t* d_rowid, const uint64_t* h_seg_counts, const u
 /* One output column of a star join (star_join operators.cu:558-766): for row i, the
  * value at position d_rowid[i] of segment d_seg[i] of the stored FOR column segs (host
  * array of nseg descriptors: payload, header lower, rows, bits), read as the reference
- * reads the segment file (8-bit values through a signed char) plus lower. With d_keys the
- * column is the foreign key of a dimension: t = (uint32)value, plus (uint32)(lower - 1)
- * when lower != 1, and d_out[i] = d_vals[lower_bound(d_keys[0..m), t)]. ALK_ERR_UNSUPPORTED
- * when a row lies past its segment or a key past the last dimension key. Synchronises. */
+ * reads the segment file (8-bit values through a signed char) plus lower. With dim_key
+ * and dim_val (host pointers to one descriptor each: the dimension's key column and the
+ * column wanted, stored FOR over the same rows) the column is a dimension's foreign key:
+ * t = (uint32)value, plus (uint32)(lower - 1) when lower != 1, and d_out[i] = dim_val at
+ * lower_bound(dim_key, t). ALK_ERR_UNSUPPORTED when a row lies past its segment or a key
+ * past the last dimension key. Synchronises. */
 int alk_star_gather(const alk_colseg* segs, uint32_t nseg, const uint32_t* d_rowid, const uint32_t* d_seg, uint64_t n,
-                    const int64_t* d_keys, uint32_t m, const int64_t* d_vals, int64_t* d_out, alk_stream stream);
+                    const alk_colseg* dim_key, const alk_colseg* dim_val, int64_t* d_out, alk_stream stream);
 
 /* Device properties of the current device. */
 int alk_device_info(int* sm_count, int* cc_major, int* cc_minor);
