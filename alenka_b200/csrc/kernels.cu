@@ -271,6 +271,186 @@ __global__ void __launch_bounds__(kT) k_scan(ScanArgs a) {
   }
 }
 
+// Ordered scan for a filter that is one set test of one column (ALK_OP_INSET: the star
+// join's filter on a bitmap index column, whose comparisons fold into one code set) with
+// no output columns, in two passes without a look-back chain. Every block owns a
+// contiguous run of tiles: k_set_pass<false> counts the run's survivors, k_block_offsets
+// turns the blocks' counts into exclusive offsets, and k_set_pass<true> tests the rows
+// again and writes the survivors' row positions and segments in row order from its
+// block's offset. A block step covers kSetTiles tiles: each thread issues one vector load
+// per tile for its 8 consecutive rows (8, 16 or 32-bit stored values, 16-byte aligned
+// payloads) before testing any, tests them against the set (copied to shared memory when
+// it fits), and one block scan over the threads' per-tile counts packed in 16-bit fields
+// orders all kSetTiles tiles at once.
+constexpr int kSetTiles = 4;
+constexpr uint32_t kSetSmemWords = 4096;
+
+struct SetTile {
+  uint4 w0, w1;
+  int64_t lower;
+  uint32_t seg, row, rows, bits;  // row: this thread's first row; rows: its rows in the tile (0..8)
+  bool all;
+};
+
+// The tile at (row0 of segment seg, descriptor d): this thread's 8 rows, loaded.
+__device__ __forceinline__ SetTile set_tile_load(const alk_colseg& d, uint32_t seg, uint32_t row0, bool all) {
+  SetTile t;
+  t.seg = seg;
+  const uint32_t tile_rows = min((uint32_t)kTile, d.rows - row0);
+  const uint32_t r = (uint32_t)threadIdx.x * kItems;
+  t.row = row0 + r;
+  t.rows = r < tile_rows ? min((uint32_t)kItems, tile_rows - r) : 0;
+  t.bits = d.bits;
+  t.lower = d.lower;
+  t.all = all;
+  t.w0 = t.w1 = make_uint4(0, 0, 0, 0);
+  if (t.rows) {
+    if (d.bits == 8) {
+      const uint2 w = *(const uint2*)((const uint8_t*)d.data + t.row);
+      t.w0.x = w.x;
+      t.w0.y = w.y;
+    } else if (d.bits == 16) {
+      t.w0 = *(const uint4*)((const uint16_t*)d.data + t.row);
+    } else {
+      t.w0 = *(const uint4*)((const uint32_t*)d.data + t.row);
+      if (t.rows > 4) t.w1 = *(const uint4*)((const uint32_t*)d.data + t.row + 4);
+    }
+  }
+  return t;
+}
+
+__device__ __forceinline__ uint32_t set_tile_mask(const SetTile& t, const uint32_t* set, uint64_t nset) {
+  uint32_t v[kItems];
+  if (t.bits == 8) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      v[k] = (t.w0.x >> (8 * k)) & 0xffu;
+      v[k + 4] = (t.w0.y >> (8 * k)) & 0xffu;
+    }
+  } else if (t.bits == 16) {
+    const uint32_t x[4] = {t.w0.x, t.w0.y, t.w0.z, t.w0.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      v[2 * k] = x[k] & 0xffffu;
+      v[2 * k + 1] = x[k] >> 16;
+    }
+  } else {
+    v[0] = t.w0.x, v[1] = t.w0.y, v[2] = t.w0.z, v[3] = t.w0.w;
+    v[4] = t.w1.x, v[5] = t.w1.y, v[6] = t.w1.z, v[7] = t.w1.w;
+  }
+  uint32_t m = 0;
+#pragma unroll
+  for (int k = 0; k < kItems; k++) {
+    if ((uint32_t)k >= t.rows) break;
+    const uint64_t x = (uint64_t)v[k] + (uint64_t)t.lower;
+    const bool pass = t.all || (x < nset && ((set[1 + (x >> 5)] >> (x & 31)) & 1));
+    m |= (uint32_t)pass << k;
+  }
+  return m;
+}
+
+template <bool WRITE>
+__global__ void __launch_bounds__(kT, 3) k_set_pass(ScanArgs a, uint32_t slot, const uint32_t* set,
+                                                 uint64_t* blk /* counts (count pass) or offsets (write pass) */) {
+  __shared__ uint64_t s_warp[kT / 32 + 1];
+  __shared__ uint32_t s_set[kSetSmemWords];
+  const uint64_t nset = __ldg(set);
+  const uint64_t words = 1 + (nset + 31) / 32;
+  const bool in_smem = words <= kSetSmemWords;
+  if (in_smem)
+    for (uint32_t i = threadIdx.x; i < words; i += kT) s_set[i] = __ldg(set + i);
+  __syncthreads();
+  const uint32_t* bits = in_smem ? (const uint32_t*)s_set : set;
+  const uint32_t per = (a.ntiles + gridDim.x - 1) / gridDim.x;
+  const uint32_t t0 = min(a.ntiles, blockIdx.x * per), t1 = min(a.ntiles, t0 + per);
+  uint64_t carry = WRITE ? blk[blockIdx.x] : 0;
+  uint32_t cur_seg = 0;
+  uint64_t seg_sum = 0;  // count pass, thread 0: survivors of the current segment not yet added
+  // The tile list holds each scanned segment's tiles in order, kTile rows apart, so the
+  // next tile is found by arithmetic; the list and the descriptors are read only where a
+  // segment starts.
+  uint32_t seg = 0, row0 = 0;
+  alk_colseg d{};
+  bool all = false;
+  if (t0 < t1) {
+    seg = a.tile_seg[t0];
+    row0 = a.tile_row0[t0];
+    d = a.cols[slot * a.nseg + seg];
+    all = a.seg_mode[seg] == 1;
+  }
+  for (uint32_t tile = t0; tile < t1; tile += kSetTiles) {
+    SetTile t[kSetTiles];
+#pragma unroll
+    for (int j = 0; j < kSetTiles; j++) {
+      if (tile + j < t1) {
+        if (j > 0 || tile > t0) {  // step from the previous tile
+          const uint64_t next = (uint64_t)row0 + kTile;
+          row0 = (uint32_t)next;
+          if (next >= d.rows) {
+            seg = a.tile_seg[tile + j];
+            row0 = a.tile_row0[tile + j];
+            d = a.cols[slot * a.nseg + seg];
+            all = a.seg_mode[seg] == 1;
+          }
+        }
+        t[j] = set_tile_load(d, seg, row0, all);
+      } else {
+        t[j].rows = 0;
+        t[j].seg = 0;
+      }
+    }
+    uint32_t m[kSetTiles];
+    uint64_t packed = 0;
+#pragma unroll
+    for (int j = 0; j < kSetTiles; j++) {
+      m[j] = t[j].rows ? set_tile_mask(t[j], bits, nset) : 0;
+      packed |= (uint64_t)__popc(m[j]) << (16 * j);
+    }
+    uint64_t totp;
+    const uint64_t exclp = block_excl_scan<kT>(packed, s_warp, &totp);
+#pragma unroll
+    for (int j = 0; j < kSetTiles; j++) {
+      const uint64_t tj = (totp >> (16 * j)) & 0xffffu;
+      if (WRITE) {
+        uint64_t o = carry + ((exclp >> (16 * j)) & 0xffffu);
+        for (uint32_t q = m[j]; q && o < a.cap; q &= q - 1, o++) {
+          const uint32_t rr = t[j].row + (uint32_t)(__ffs(q) - 1);
+          if (a.out_rowid) a.out_rowid[o] = rr;
+          if (a.out_seg) a.out_seg[o] = t[j].seg;
+        }
+      } else if (threadIdx.x == 0 && a.seg_counts && tile + j < t1) {
+        if (t[j].seg != cur_seg && seg_sum) {
+          atomicAdd(a.seg_counts + cur_seg, (unsigned long long)seg_sum);
+          seg_sum = 0;
+        }
+        cur_seg = t[j].seg;
+        seg_sum += tj;
+      }
+      carry += tj;
+    }
+  }
+  if (!WRITE && threadIdx.x == 0) {
+    if (a.seg_counts && seg_sum) atomicAdd(a.seg_counts + cur_seg, (unsigned long long)seg_sum);
+    blk[blockIdx.x] = carry;
+  }
+}
+
+// Exclusive offsets of n block counts (in place), by one block; the total goes to *total.
+constexpr int kOffT = 1024;
+__global__ void __launch_bounds__(kOffT) k_block_offsets(uint64_t* blk, uint32_t n, unsigned long long* total) {
+  __shared__ uint64_t s_warp[kOffT / 32 + 1];
+  uint64_t carry = 0;
+  for (uint32_t base = 0; base < n; base += kOffT) {
+    const uint32_t i = base + threadIdx.x;
+    const uint64_t v = i < n ? blk[i] : 0;
+    uint64_t tot;
+    const uint64_t excl = block_excl_scan<kOffT>(v, s_warp, &tot);
+    if (i < n) blk[i] = carry + excl;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
 // ------------------------------------------------------------ expression evaluation
 __global__ void __launch_bounds__(kT) k_eval(const int64_t* const* cols, uint32_t ncols, uint64_t n,
                                              const alk_program* prog, int64_t* out) {
@@ -1112,10 +1292,31 @@ int alk_scan_filter(const alk_colseg* cols, uint32_t ncols, uint32_t nseg, const
   a.aggs = lb;
   a.incls = lb + ntiles;
   a.total = (unsigned long long*)(lb + 2 * (size_t)ntiles);
+  // one set test of one column and no output columns: the vector-load form
+  bool set_form = pred && nout == 0 && pred->n_instr == 1 && pred->ins[0].op == ALK_OP_INSET &&
+                  pred->ins[0].ka == ALK_K_COL && pred->ins[0].kb == ALK_K_CONST && pred->result == pred->ins[0].dst;
+  const uint32_t set_slot = set_form ? pred->ins[0].a : 0;
+  for (uint32_t g = 0; set_form && g < nseg; g++) {
+    if (seg_mode[g] == 0) continue;
+    const alk_colseg& d = cols[set_slot * nseg + g];
+    if ((d.bits != 8 && d.bits != 16 && d.bits != 32) || ((uintptr_t)d.data & 15)) set_form = false;
+  }
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_scan, kT, 0);
-  int grid = std::max(1, std::min<int>((int)ntiles, sm_count() * std::max(occ, 1)));
-  k_scan<<<grid, kT, 0, s>>>(a);
+  if (set_form) {
+    const uint32_t* set = (const uint32_t*)(uintptr_t)pred->consts[pred->ins[0].b];
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_set_pass<true>, kT, 0);
+    const int grid = std::max(1, std::min<int>((int)ntiles, sm_count() * std::max(occ, 1)));
+    uint64_t* blk = sc.get<uint64_t>(grid, &e);
+    CK(e);
+    k_set_pass<false><<<grid, kT, 0, s>>>(a, set_slot, set, blk);
+    k_block_offsets<<<1, kOffT, 0, s>>>(blk, (uint32_t)grid, a.total);
+    k_set_pass<true><<<grid, kT, 0, s>>>(a, set_slot, set, blk);
+    alk::g_kernel_launches += 2;
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_scan, kT, 0);
+    int grid = std::max(1, std::min<int>((int)ntiles, sm_count() * std::max(occ, 1)));
+    k_scan<<<grid, kT, 0, s>>>(a);
+  }
   alk::g_kernel_launches++;
   CK(cudaGetLastError());
   uint64_t res[2];
