@@ -338,15 +338,25 @@ __device__ __forceinline__ uint32_t set_tile_mask(const SetTile& t, const uint32
     v[0] = t.w0.x, v[1] = t.w0.y, v[2] = t.w0.z, v[3] = t.w0.w;
     v[4] = t.w1.x, v[5] = t.w1.y, v[6] = t.w1.z, v[7] = t.w1.w;
   }
+  const uint32_t valid = (1u << t.rows) - 1;  // rows <= 8
+  if (t.all) return valid;
   uint32_t m = 0;
+  if (t.lower >= 0 && (uint64_t)t.lower + (1ull << t.bits) <= 0xFFFFFFFFull && nset <= 0xFFFFFFFFull) {
+    // every value and the set's size fit 32 bits (index codes offset by their segment)
+    const uint32_t lo = (uint32_t)t.lower, n32 = (uint32_t)nset;
 #pragma unroll
-  for (int k = 0; k < kItems; k++) {
-    if ((uint32_t)k >= t.rows) break;
-    const uint64_t x = (uint64_t)v[k] + (uint64_t)t.lower;
-    const bool pass = t.all || (x < nset && ((set[1 + (x >> 5)] >> (x & 31)) & 1));
-    m |= (uint32_t)pass << k;
+    for (int k = 0; k < kItems; k++) {
+      const uint32_t x = v[k] + lo;
+      m |= (uint32_t)(x < n32 && ((set[1 + (x >> 5)] >> (x & 31)) & 1)) << k;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kItems; k++) {
+      const uint64_t x = (uint64_t)v[k] + (uint64_t)t.lower;
+      m |= (uint32_t)(x < nset && ((set[1 + (x >> 5)] >> (x & 31)) & 1)) << k;
+    }
   }
-  return m;
+  return m & valid;
 }
 
 template <bool WRITE>
