@@ -12,6 +12,12 @@ of orders at once; star_b splits orders into three segments and lineitem into tw
 DATASETS = {
     "star_a": {"kind": "three_way", "customers": 1500, "orders": 15000, "rows": 60000, "seg_rows": 15000, "seed": 5},
     "star_b": {"kind": "three_way", "customers": 1500, "orders": 15000, "rows": 60000, "seg_rows": 5000, "seed": 7},
+    # lineitem segments of 200 rows: l_orderkey is stored in 8 bits with values past 127,
+    # which the star join reads through a signed char
+    "star_c": {"kind": "three_way", "customers": 50, "orders": 200, "rows": 800, "seg_rows": 200, "seed": 3},
+    # customer (6000 rows, one segment) longer than the last orders segment (3000 rows):
+    # the char index appends the dimension's remaining hashes to that segment's values
+    "star_d": {"kind": "three_way", "customers": 6000, "orders": 15000, "rows": 24000, "seg_rows": 6000, "seed": 9},
 }
 
 SETUP = {
@@ -25,6 +31,12 @@ SETUP = {
     "star_b": (
         "CREATE INDEX oc ON orders(customer.c_mktsegment) FROM orders, customer "
         "WHERE orders.o_custkey = customer.c_custkey;\n"),
+    "star_c": (
+        "CREATE INDEX lo ON lineitem(orders.o_orderdate) FROM lineitem, orders "
+        "WHERE lineitem.l_orderkey = orders.o_orderkey;\n"),
+    "star_d": (
+        "CREATE INDEX oc ON orders(customer.c_mktsegment) FROM orders, customer "
+        "WHERE orders.o_custkey = customer.c_custkey;\n"),
 }
 
 # the index files each setup writes (fact.dimension.column.segment)
@@ -32,6 +44,8 @@ INDEX_FILES = {
     "star_a": [f"lineitem.orders.{c}.{g}" for c in ("o_orderdate", "o_shippriority") for g in range(4)]
     + ["orders.customer.c_mktsegment.0"],
     "star_b": [f"orders.customer.c_mktsegment.{g}" for g in range(3)],
+    "star_c": [f"lineitem.orders.o_orderdate.{g}" for g in range(4)],
+    "star_d": [f"orders.customer.c_mktsegment.{g}" for g in range(3)],
 }
 
 CASES = [
@@ -89,6 +103,13 @@ CASES = [
         "J := SELECT o_orderkey AS o_orderkey, c_mktsegment AS c_mktsegment, o_custkey AS o_custkey "
         "FROM OF JOIN CF ON o_custkey = c_custkey;\n"
         "STORE J INTO 'b2.txt' USING ('|');\n")},
+    # fact columns only: l_orderkey's 8-bit stored values past 127 come back negative
+    {"name": "c_signed_char", "dataset": "star_c", "out": "c1.txt", "script": (
+        "OF := FILTER orders BY o_orderdate != 19951019 OR o_orderdate != 19950122 OR o_orderdate != 19930423 "
+        "OR o_orderdate != 19950412;\n"
+        "J := SELECT l_orderkey AS l_orderkey, l_extendedprice AS l_extendedprice, l_shipdate AS l_shipdate "
+        "FROM lineitem JOIN OF ON l_orderkey = o_orderkey;\n"
+        "STORE J INTO 'c1.txt' USING ('|');\n")},
 ]
 
 
