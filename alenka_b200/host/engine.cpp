@@ -747,8 +747,8 @@ alk_program Engine::compile_filter(Var* f, Var* src, std::vector<std::string>& s
         int64_t code = it == bc.hash_to_code.end() ? -1 : it->second;
         bools.push_back(b.emit(cmp == 4 ? ALK_OP_EQ : ALK_OP_NE, slot(v2), b.konst(code)));
         et.push_back("NAME");
-      } else if ((s1 == "NUMBER" && s2 == "NAME" && ev.back().find('.') != std::string::npos) ||
-                 (s1 == "NAME" && s2 == "NUMBER" && ev.back().find('.') != std::string::npos)) {
+      } else if (((s1 == "NUMBER" && s2 == "NAME") || (s1 == "NAME" && s2 == "NUMBER")) && !ev.empty() &&
+                 ev.back().find('.') != std::string::npos) {
         // a bitmap join index column against a number: the number itself looked up in each
         // segment's dictionary (filter.cu:519-535, 560-577); the number's precision stays
         // on the precision stack, as the reference pops and pushes none there
