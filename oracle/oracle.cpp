@@ -744,7 +744,7 @@ class Engine {
           exe_type.push_back("NAME");
           bools.push_back(res);
         } else if ((s1 == "NUMBER" || s2 == "NUMBER") && (s1 == "NAME" || s2 == "NAME") &&
-                   exe_value.back().find('.') != string::npos) {
+                   !exe_value.empty() && exe_value.back().find('.') != string::npos) {
           // a bitmap join index against a number (filter.cu:519-535, 560-577): the number
           // as it is, looked up in the segment's dictionary; the precision stack is left
           // as it was
