@@ -690,6 +690,10 @@ def main():
     rank = _env_int("RANK", 0)
     local = _env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
+        if args.workload == "star":
+            if rank == 0:
+                run_reference_star(args)
+            return
         run_reference(args, rank)
         return
     import torch
@@ -967,6 +971,85 @@ def run_compressed(args, torch):
         "clocks": clocks}), flush=True)
 
 
+STAR_METRIC = "fact rows/s, star join through a bitmap join index + GROUP BY + ORDER BY ... LIMIT 10"
+
+
+def star_scripts(seed, out):
+    """The star workload's CREATE INDEX and its query: lineitem indexed on
+    orders.o_orderdate, joined with orders filtered on ten seed-drawn dates, grouped by
+    date, ordered by revenue, top 10."""
+    import random
+    r = random.Random(seed * 31 + 7)
+    dates = sorted({date_add_days(19920101, r.randint(0, 2400)) for _ in range(10)})
+    setup = ("CREATE INDEX lo ON lineitem(orders.o_orderdate) FROM lineitem, orders "
+             "WHERE lineitem.l_orderkey = orders.o_orderkey;\n")
+    script = ("OF := FILTER orders BY " + " OR ".join(f"o_orderdate == {x}" for x in dates) + ";\n"
+              "J := SELECT l_orderkey AS l_orderkey, l_extendedprice AS l_extendedprice, o_orderdate AS o_orderdate "
+              "FROM lineitem JOIN OF ON l_orderkey = o_orderkey;\n"
+              "G := SELECT o_orderdate AS odate, SUM(l_extendedprice) AS rev, COUNT(l_orderkey) AS cnt "
+              "FROM J GROUP BY o_orderdate;\n"
+              "R := ORDER G BY rev DESC;\n"
+              f"STORE R INTO '{out}' USING ('|') LIMIT 10;\n")
+    return setup, script, dates
+
+
+def star_config(scale, seed):
+    z = sizes(scale)
+    _, _, dates = star_scripts(seed, "x")
+    return {"workload": f"lineitem {z['lineitems']} rows in segments of {z['orders']} / orders {z['orders']} / "
+                        f"customer {z['customers']}, one segment each; lineitem indexed on orders.o_orderdate; star "
+                        f"join with orders filtered on {len(dates)} dates, GROUP BY date, ORDER BY revenue DESC "
+                        "LIMIT 10",
+            "dates": dates}
+
+
+def star_reference(base, scale, seed, threads, steps, warmup):
+    """The reference's own CLI (oracle/_ref/alenka_ref, Thrust OpenMP) on the star workload's
+    tables at a bounded scale, written by the numpy writer (nothing of the engine loaded):
+    CREATE INDEX once, then `steps` runs of the query. Returns (seconds of CREATE INDEX,
+    seconds per query, fact rows, sample text)."""
+    from oracle import refdata
+    z = sizes(scale)
+    d = os.path.join(base, f"star_numpy_s{scale}_seed{seed}")
+    marker = os.path.join(d, ".complete")
+    if not os.path.exists(marker):
+        os.makedirs(d, exist_ok=True)
+        refdata.three_way(d, z["customers"], z["orders"], z["lineitems"], z["orders"], seed)
+        with open(marker, "w") as f:
+            f.write(str(z["lineitems"]))
+    setup, script, _ = star_scripts(seed, "ref_star.txt")
+    index_s = run_reference_binary(d, setup, threads)
+    for _ in range(warmup):
+        run_reference_binary(d, script, threads)
+    dt = sum(run_reference_binary(d, script, threads) for _ in range(steps)) / steps
+    sample = (f"the reference's CLI and operators built for the CPU (Thrust OpenMP): CREATE INDEX once, then the "
+              f"star query over lineitem {_m(z['lineitems'])} / orders {_m(z['orders'])} / customer "
+              f"{_m(z['customers'])} (the same generator, scale {scale:g} of the 60M instance), {steps} runs, "
+              f"{dt * steps:.2f} s")
+    return index_s, dt, z["lineitems"], sample
+
+
+def run_reference_star(args):
+    """--impl reference --workload star: the reference's own star join on the host cores."""
+    threads = os.cpu_count() or 1
+    if not os.path.exists(REF_BIN):
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/alenka_ref absent "
+                                                              "(oracle/build_ref.sh needs the reference sources)"}))
+        return
+    base = args.data_dir or os.path.join(tempfile.gettempdir(), "alenka_bench_ref")
+    sc = reference_sample_scale(args.scale)
+    index_s, dt, rows, sample = star_reference(base, sc, args.seed, threads, args.steps, args.warmup)
+    value = rows / dt
+    print(json.dumps({
+        "impl": "reference", "metric": STAR_METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1000, "higher_is_better": True,
+        "dtype": "int64", "data": "synthetic", "config": star_config(args.scale, args.seed),
+        "create_index": {"seconds": index_s, "rows_per_s": rows / index_s},
+        "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
 def run_star(args, torch):
     """Star join through a bitmap join index at the headline fact size: lineitem 600M rows in
     four 150M-row segments, orders 150M and customer 15M rows in one segment each (the
@@ -975,7 +1058,6 @@ def run_star(args, torch):
     runs the star join of lineitem with orders filtered on ten order dates, grouped by date,
     ordered by revenue, top 10. The same script over the same tables without the index runs
     as a hash join (the fused plan): both are timed and their stored rows compared."""
-    import random
     import alenka_b200 as ab
     base = args.data_dir or os.path.join(tempfile.gettempdir(), "alenka_bench")
     z = sizes(args.scale)
@@ -988,17 +1070,7 @@ def run_star(args, torch):
         with open(marker, "w") as f:
             f.write(str(z["lineitems"]))
     rows = z["lineitems"]
-    r = random.Random(args.seed * 31 + 7)
-    dates = sorted({date_add_days(19920101, r.randint(0, 2400)) for _ in range(10)})
-    setup = ("CREATE INDEX lo ON lineitem(orders.o_orderdate) FROM lineitem, orders "
-             "WHERE lineitem.l_orderkey = orders.o_orderkey;\n")
-    script = ("OF := FILTER orders BY " + " OR ".join(f"o_orderdate == {x}" for x in dates) + ";\n"
-              "J := SELECT l_orderkey AS l_orderkey, l_extendedprice AS l_extendedprice, o_orderdate AS o_orderdate "
-              "FROM lineitem JOIN OF ON l_orderkey = o_orderkey;\n"
-              "G := SELECT o_orderdate AS odate, SUM(l_extendedprice) AS rev, COUNT(l_orderkey) AS cnt "
-              "FROM J GROUP BY o_orderdate;\n"
-              "R := ORDER G BY rev DESC;\n"
-              "STORE R INTO 'bench_star.txt' USING ('|') LIMIT 10;\n")
+    setup, script, dates = star_scripts(args.seed, "bench_star.txt")
     idx = [os.path.join(d, f"lineitem.orders.o_orderdate.{g}") for g in range((rows + seg - 1) // seg)]
     sess = ab.Session(d, resident=True)
     for t in ("lineitem", "orders"):
@@ -1032,15 +1104,11 @@ def run_star(args, torch):
     # the star join's rows: the counts of its groups (ten dates, all within the top 10)
     survivors = sum(int(ln.split(b"|")[2]) for ln in star_out.splitlines() if ln) if star_out else 0
     qb = rows * 2
-    print(json.dumps({
-        "metric": "fact rows/s, star join through a bitmap join index + GROUP BY + ORDER BY ... LIMIT 10",
+    line = {
+        "metric": STAR_METRIC,
         "value": rows / (ms / 1000.0), "unit": "rows/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": f"lineitem {rows} rows in segments of {seg} / orders {z['orders']} / customer "
-                               f"{z['customers']}, one segment each; lineitem indexed on orders.o_orderdate; star "
-                               f"join with orders filtered on {len(dates)} dates, GROUP BY date, ORDER BY revenue "
-                               "DESC LIMIT 10",
-                   "dates": dates},
+        "config": star_config(args.scale, args.seed),
         "create_index": {"seconds": index_s, "rows_per_s": rows / index_s, "index_file_bytes": index_bytes},
         "hash_join_ms_per_step": jms, "star_vs_hash_join": jms / ms,
         "hash_join_plan": {0: "operator-at-a-time", 1: "fused", 2: "fused, replayed from its CUDA graph"}.get(
@@ -1052,7 +1120,16 @@ def run_star(args, torch):
                            "achieved": qb / (ms / 1000.0) / 1e9, "peak": peak, "unit": "GB/s",
                            "frac": qb / (ms / 1000.0) / 1e9 / peak, "peak_source": peak_kind},
         "rows_scanned_per_step": st.rows_scanned, "star_join_rows": survivors,
-        "clocks": clocks}), flush=True)
+        "clocks": clocks}
+    if not args.no_cpu_baseline and os.path.exists(REF_BIN):
+        # the reference's own star join on the host cores, a bounded sample (lineitem 60M rows)
+        sc = reference_sample_scale(args.scale)
+        index_s, dt, srows, sample = star_reference(os.path.join(base, "ref"), sc, args.seed, os.cpu_count() or 1,
+                                                    2, 1)
+        line["cpu_baseline"] = {"value": srows / dt, "unit": "rows/s", "cores": os.cpu_count() or 1,
+                                "kind": "reference", "sample": sample,
+                                "create_index_rows_per_s": srows / index_s}
+    print(json.dumps(line), flush=True)
 
 
 def run_three_way(args, torch, dist, world, rank, local):
